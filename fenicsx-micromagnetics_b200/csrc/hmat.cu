@@ -1,0 +1,308 @@
+// H-matrix apply: y = P^-1 [diag o x~ + Near x~ + sum_b U_b (V_b x~_{J_b})],  x~ = x[perm]
+// (HMatrixGPUPackedFused.matvec, lindholm_hmatrix_gpu/backend_fused.py:496-512).
+//
+// B200 layout.  Far factors are packed per block as U^T (k x m, each column of U
+// contiguous) followed by V (k x n, each row of V contiguous) in the storage type TF
+// (FP64, FP32 or BF16).  Near blocks are dense tiles stored column-major (n x m) in
+// TN.  Three kernels, no atomics, every output row written by exactly one CTA:
+//   k_hgather : x~[i] = src[g(perm[i])]             (fused boundary gather + perm)
+//   k_far_z   : z_b = V_b x~_{J_b}, one CTA per far block, lanes over columns
+//   k_rows    : one CTA per leaf row cluster; threads over the cluster's rows walk
+//               the cluster's item list (near tiles and far blocks covering it),
+//               read U^T / tile columns coalesced across rows, add diag o x~, and
+//               scatter y to dst[g(perm[i])].
+// Near tiles may use compensated (Kahan) accumulation in the mixed-precision form.
+#include <algorithm>
+
+#include "hmat.cuh"
+
+namespace spx {
+
+template <class T> __device__ __forceinline__ T from_d(double v) { return static_cast<T>(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) {
+  return __float2bfloat16_rn(static_cast<float>(v));
+}
+template <class T> __device__ __forceinline__ double to_d(T v) { return static_cast<double>(v); }
+template <> __device__ __forceinline__ double to_d<__nv_bfloat16>(__nv_bfloat16 v) {
+  return static_cast<double>(__bfloat162float(v));
+}
+template <class A, class T> __device__ __forceinline__ A cvt(T v) { return static_cast<A>(v); }
+template <> __device__ __forceinline__ float cvt<float, __nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ double cvt<double, __nv_bfloat16>(__nv_bfloat16 v) {
+  return static_cast<double>(__bfloat162float(v));
+}
+
+// ------------------------------------------------------------------ packing
+struct PackFar {
+  int64_t src_u, src_v, dst;  // element offsets
+  int32_t m, n, k;
+};
+template <class TF>
+__global__ void k_pack_far(const PackFar* __restrict__ jobs, const double* __restrict__ pool, TF* __restrict__ out) {
+  const PackFar j = jobs[blockIdx.x];
+  const int64_t lu = (int64_t)j.k * j.m, lv = (int64_t)j.k * j.n;
+  for (int64_t e = threadIdx.x; e < lu; e += blockDim.x) out[j.dst + e] = from_d<TF>(pool[j.src_u + e]);
+  for (int64_t e = threadIdx.x; e < lv; e += blockDim.x) out[j.dst + lu + e] = from_d<TF>(pool[j.src_v + e]);
+}
+struct PackNear {
+  int64_t src, dst;
+  int32_t m, n;
+};
+template <class TN>
+__global__ void k_pack_near(const PackNear* __restrict__ jobs, const double* __restrict__ pool, TN* __restrict__ out) {
+  const PackNear j = jobs[blockIdx.x];
+  const int64_t L = (int64_t)j.m * j.n;
+  // out[c * m + r] = in[r * n + c]
+  for (int64_t e = threadIdx.x; e < L; e += blockDim.x) {
+    const int64_t c = e / j.m, r = e - c * j.m;
+    out[j.dst + e] = from_d<TN>(pool[j.src + r * j.n + c]);
+  }
+}
+
+// ------------------------------------------------------------------ apply kernels
+template <class TS, class TX>
+__global__ void k_hgather(int64_t Nb, const TS* __restrict__ src, const int32_t* __restrict__ gidx,
+                          const int32_t* __restrict__ perm, TX* __restrict__ xp) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= Nb) return;
+  const int32_t b = perm[i];
+  const int64_t o = gidx ? gidx[b] : b;
+  xp[i] = static_cast<TX>(src[o]);
+}
+
+template <class TF, class TA, class TX>
+__global__ void __launch_bounds__(128) k_far_z(const int32_t* __restrict__ meta, const int64_t* __restrict__ voff,
+                                               const int64_t* __restrict__ zoff, const TF* __restrict__ F,
+                                               const TX* __restrict__ xp, TA* __restrict__ z) {
+  const int b = blockIdx.x;
+  const int cs = meta[5 * b + 2], n = meta[5 * b + 3], k = meta[5 * b + 4];
+  const TF* V = F + voff[b];
+  const TX* x = xp + cs;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q = w; q < k; q += nw) {
+    const TF* row = V + (int64_t)q * n;
+    TA acc = 0;
+    for (int j = lane; j < n; j += 32) acc += cvt<TA>(row[j]) * static_cast<TA>(x[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) z[zoff[b] + q] = acc;
+  }
+}
+
+constexpr int ROWS_GROUPS = 2;
+constexpr int ROWS_GSIZE = 64;
+
+template <class TF, class TN, class TA, class TX, class TD>
+__global__ void __launch_bounds__(ROWS_GROUPS * ROWS_GSIZE) k_rows(
+    const int32_t* __restrict__ leaf_start, const int64_t* __restrict__ item_ptr,
+    const int32_t* __restrict__ items, const int32_t* __restrict__ far_meta,
+    const int64_t* __restrict__ far_uoff, const int64_t* __restrict__ far_zoff,
+    const TF* __restrict__ F, const int32_t* __restrict__ near_meta, const int64_t* __restrict__ near_off,
+    const TN* __restrict__ Nt, const TA* __restrict__ z, const TX* __restrict__ xp,
+    const double* __restrict__ diag, const int32_t* __restrict__ perm, const int32_t* __restrict__ gidx,
+    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, int kahan) {
+  extern __shared__ unsigned char smem_raw[];
+  const int leaf = blockIdx.x;
+  const int r0 = leaf_start[leaf], nr = leaf_start[leaf + 1] - r0;
+  TA* acc = reinterpret_cast<TA*>(smem_raw);             // [GROUPS][nr]
+  TA* cmp = acc + ROWS_GROUPS * nr;                       // [GROUPS][nr] Kahan compensation
+  const int g = threadIdx.x / ROWS_GSIZE, t = threadIdx.x % ROWS_GSIZE;
+  for (int r = t; r < nr; r += ROWS_GSIZE) {
+    acc[g * nr + r] = 0;
+    cmp[g * nr + r] = 0;
+  }
+  const int64_t i0 = item_ptr[leaf], i1 = item_ptr[leaf + 1];
+  for (int64_t it = i0 + g; it < i1; it += ROWS_GROUPS) {
+    const int32_t code = items[it];
+    const int32_t bi = code >> 1;
+    if (code & 1) {
+      const int rs = far_meta[5 * bi], m = far_meta[5 * bi + 1], k = far_meta[5 * bi + 4];
+      const TF* Ut = F + far_uoff[bi];
+      const TA* zb = z + far_zoff[bi];
+      for (int r = t; r < nr; r += ROWS_GSIZE) {
+        const int lr = r0 + r - rs;
+        TA s = 0;
+        for (int q = 0; q < k; ++q) s += cvt<TA>(Ut[(int64_t)q * m + lr]) * zb[q];
+        acc[g * nr + r] += s;
+      }
+    } else {
+      const int rs = near_meta[4 * bi], m = near_meta[4 * bi + 1], cs = near_meta[4 * bi + 2],
+                n = near_meta[4 * bi + 3];
+      const TN* tile = Nt + near_off[bi];
+      const TX* x = xp + cs;
+      for (int r = t; r < nr; r += ROWS_GSIZE) {
+        const int lr = r0 + r - rs;
+        TA s = 0;
+        for (int c = 0; c < n; ++c) s += cvt<TA>(tile[(int64_t)c * m + lr]) * static_cast<TA>(x[c]);
+        if (kahan) {
+          const TA y = s - cmp[g * nr + r];
+          const TA tt = acc[g * nr + r] + y;
+          cmp[g * nr + r] = (tt - acc[g * nr + r]) - y;
+          acc[g * nr + r] = tt;
+        } else {
+          acc[g * nr + r] += s;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < nr; r += blockDim.x) {
+    const int64_t i = r0 + r;
+    TA y = static_cast<TA>(diag[i]) * static_cast<TA>(xp[i]);
+    for (int q = 0; q < ROWS_GROUPS; ++q) y += acc[q * nr + r] - cmp[q * nr + r];
+    const int32_t b = perm[i];
+    const int64_t o = gidx ? gidx[b] : b;
+    const TD yv = static_cast<TD>(y);
+    dst[o] = add ? static_cast<TD>(add[o] + yv) : yv;
+    if (yb) yb[b] = yv;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+template <class TF, class TN>
+void do_pack(HMatrix& H, cudaStream_t s) {
+  std::vector<PackFar> pf;
+  std::vector<PackNear> pn;
+  std::vector<int32_t> fmeta, nmeta;
+  std::vector<int64_t> fu, fv, fz, noff;
+  std::vector<int32_t> code_of(H.blocks.size());
+  int64_t fpos = 0, npos = 0, zpos = 0;
+  int32_t nf = 0, nn = 0;
+  for (size_t q = 0; q < H.blocks.size(); ++q) {
+    const HBlock& b = H.blocks[q];
+    const int32_t m = b.re - b.rs, n = b.ce - b.cs;
+    if (b.type == 1) {
+      pf.push_back(PackFar{b.off_u, b.off_v, fpos, m, n, b.rank});
+      fmeta.insert(fmeta.end(), {b.rs, m, b.cs, n, b.rank});
+      fu.push_back(fpos);
+      fv.push_back(fpos + (int64_t)b.rank * m);
+      fz.push_back(zpos);
+      fpos += (int64_t)b.rank * (m + n);
+      zpos += b.rank;
+      code_of[q] = (nf++ << 1) | 1;
+    } else {
+      pn.push_back(PackNear{b.off_u, npos, m, n});
+      nmeta.insert(nmeta.end(), {b.rs, m, b.cs, n});
+      noff.push_back(npos);
+      npos += (int64_t)m * n;
+      code_of[q] = (nn++ << 1);
+    }
+  }
+  H.n_far = nf;
+  H.n_near = nn;
+  H.zlen = zpos;
+  H.far_f.alloc(std::max<int64_t>(fpos, 1) * sizeof(TF));
+  H.near_f.alloc(std::max<int64_t>(npos, 1) * sizeof(TN));
+  H.bytes_far = fpos * (int64_t)sizeof(TF);
+  H.bytes_near = npos * (int64_t)sizeof(TN);
+  for (size_t k0 = 0; k0 < pf.size(); k0 += 65535) {
+    const size_t c = std::min<size_t>(65535, pf.size() - k0);
+    DevBuf<PackFar> d;
+    d.upload(pf.data() + k0, c, s);
+    k_pack_far<TF><<<static_cast<unsigned>(c), 256, 0, s>>>(d.p, H.far_pool64.p, reinterpret_cast<TF*>(H.far_f.p));
+    SPX_LAUNCH_CHECK();
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
+  for (size_t k0 = 0; k0 < pn.size(); k0 += 65535) {
+    const size_t c = std::min<size_t>(65535, pn.size() - k0);
+    DevBuf<PackNear> d;
+    d.upload(pn.data() + k0, c, s);
+    k_pack_near<TN><<<static_cast<unsigned>(c), 256, 0, s>>>(d.p, H.near_pool64.p, reinterpret_cast<TN*>(H.near_f.p));
+    SPX_LAUNCH_CHECK();
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
+  H.far_meta.upload(fmeta, s);
+  H.far_uoff.upload(fu, s);
+  H.far_voff.upload(fv, s);
+  H.far_zoff.upload(fz, s);
+  H.near_meta.upload(nmeta, s);
+  H.near_off.upload(noff, s);
+  // leaf row clusters: tree leaves in permutation order
+  std::vector<int32_t> ls;
+  for (const TreeNode& nd : H.tree.nodes)
+    if (nd.leaf()) ls.push_back(nd.start);
+  std::sort(ls.begin(), ls.end());
+  ls.push_back(static_cast<int32_t>(H.Nb));
+  const int64_t nleaf = static_cast<int64_t>(ls.size()) - 1;
+  std::vector<std::vector<int32_t>> per(nleaf);
+  for (size_t q = 0; q < H.blocks.size(); ++q) {
+    const HBlock& b = H.blocks[q];
+    int64_t l = std::upper_bound(ls.begin(), ls.end(), b.rs) - ls.begin() - 1;
+    for (; l < nleaf && ls[l] < b.re; ++l) per[l].push_back(code_of[q]);
+  }
+  std::vector<int64_t> ip(nleaf + 1, 0);
+  std::vector<int32_t> items;
+  for (int64_t l = 0; l < nleaf; ++l) {
+    items.insert(items.end(), per[l].begin(), per[l].end());
+    ip[l + 1] = static_cast<int64_t>(items.size());
+  }
+  H.nleaf = nleaf;
+  H.leaf_start.upload(ls, s);
+  H.item_ptr.upload(ip, s);
+  H.items.upload(items, s);
+  int max_leaf = 0;
+  for (int64_t l = 0; l < nleaf; ++l) max_leaf = std::max(max_leaf, ls[l + 1] - ls[l]);
+  SPX_CHECK(max_leaf <= 2048, "leaf clusters larger than 2048 rows are not supported by the apply kernel");
+  SPX_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class TF, class TN, class TA, class TX, class TS>
+void do_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS* add, TS* yb, cudaStream_t s) {
+  const int64_t Nb = H.Nb;
+  if (H.xperm.n < Nb * sizeof(TX)) H.xperm.alloc(Nb * sizeof(TX));
+  if (H.z.n < std::max<int64_t>(H.zlen, 1) * sizeof(TA)) H.z.alloc(std::max<int64_t>(H.zlen, 1) * sizeof(TA));
+  TX* xp = reinterpret_cast<TX*>(H.xperm.p);
+  TA* z = reinterpret_cast<TA*>(H.z.p);
+  k_hgather<TS, TX><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, src, gidx, H.perm.p, xp);
+  SPX_LAUNCH_CHECK();
+  if (H.n_far > 0) {
+    k_far_z<TF, TA, TX><<<static_cast<unsigned>(H.n_far), 128, 0, s>>>(
+        H.far_meta.p, H.far_voff.p, H.far_zoff.p, reinterpret_cast<const TF*>(H.far_f.p), xp, z);
+    SPX_LAUNCH_CHECK();
+  }
+  int max_leaf = H.cfg.leaf_size;
+  const size_t smem = 2 * ROWS_GROUPS * static_cast<size_t>(std::max(max_leaf, 1)) * sizeof(TA);
+  k_rows<TF, TN, TA, TX, TS><<<static_cast<unsigned>(H.nleaf), ROWS_GROUPS * ROWS_GSIZE, smem, s>>>(
+      H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
+      reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
+      reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, gidx, dst, add, yb,
+      H.prec == Prec::MIXED ? 1 : 0);
+  SPX_LAUNCH_CHECK();
+}
+}  // namespace
+
+void HMatrix::pack(Prec p, cudaStream_t s) {
+  prec = p;
+  switch (p) {
+    case Prec::F64: do_pack<double, double>(*this, s); break;
+    case Prec::F32: do_pack<float, float>(*this, s); break;
+    case Prec::MIXED: do_pack<__nv_bfloat16, float>(*this, s); break;
+  }
+  packed = true;
+}
+
+template <class T>
+void HMatrix::apply_gather(const T* src, const int32_t* gidx, T* dst, const T* add, T* yb, cudaStream_t s) {
+  SPX_CHECK(packed, "H-matrix is not packed");
+  switch (prec) {
+    case Prec::F64: do_apply<double, double, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
+    case Prec::F32: do_apply<float, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+    case Prec::MIXED: do_apply<__nv_bfloat16, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+  }
+}
+template void HMatrix::apply_gather<double>(const double*, const int32_t*, double*, const double*, double*, cudaStream_t);
+template void HMatrix::apply_gather<float>(const float*, const int32_t*, float*, const float*, float*, cudaStream_t);
+
+void HMatrix::apply_f64(const double* x, double* y, cudaStream_t s) {
+  apply_gather<double>(x, nullptr, y, nullptr, nullptr, s);
+}
+
+int64_t HMatrix::device_bytes() const {
+  return static_cast<int64_t>(far_f.bytes() + near_f.bytes() + far_uoff.bytes() + far_voff.bytes() +
+                              far_zoff.bytes() + far_meta.bytes() + near_off.bytes() + near_meta.bytes() +
+                              leaf_start.bytes() + item_ptr.bytes() + items.bytes() + z.bytes() +
+                              xperm.bytes() + diag_perm.bytes() + perm.bytes());
+}
+
+}  // namespace spx

@@ -1,0 +1,98 @@
+// H-matrix handle: construction (batched GPU fill + full-pivot ACA) and apply.
+#pragma once
+
+#include "spx_internal.cuh"
+
+namespace spx {
+
+struct FillDesc;
+void launch_fill(const FillDesc* d_blocks, const int64_t* d_tile_start, int nb, int64_t ntiles,
+                 const int32_t* rows_pool, const int32_t* cols_pool, const double* Xb,
+                 const int32_t* tri_lid, const double* T, const int32_t* inc_ptr,
+                 const int32_t* inc_tri, int maxinc, int64_t Nb, double* out, cudaStream_t s);
+void launch_lindholm_pairs(int64_t P, const double* x0, const int32_t* tri, const double* T, int64_t Nt, double* w,
+                           cudaStream_t s);
+void launch_add_diag(int64_t Nb, const double* omega_sum, double* B, cudaStream_t s);
+void pack_triangles(const HostBoundary& bd, std::vector<double>& rec);
+
+// Boundary geometry resident on one device.
+struct BoundaryDev {
+  int device = 0;
+  HostBoundary host;
+  DevBuf<double> Xb, T, omega_sum;
+  DevBuf<int32_t> tri_lid, inc_ptr, inc_tri, bverts;
+  int maxinc = 0;
+  void create(const double* X, int64_t N, const int32_t* tets, int64_t E);
+  // fill B[rows, cols] (no diagonal jump) for one block into out (row-major m x n)
+  void fill_block(const int32_t* rows_dev, int64_t m, const int32_t* cols_dev, int64_t n, double* out,
+                  cudaStream_t s) const;
+  void dense_B(double* B, cudaStream_t s) const;
+};
+
+enum class Prec : int { F64 = 0, F32 = 1, MIXED = 2 };
+
+struct HBuildConfig {
+  double epsilon = 1e-5;
+  double eta = 2.0;
+  int leaf_size = 64;
+  int max_rank = -1;  // <0: None
+  int64_t max_temporary_block_bytes = 256ll * 1024 * 1024;
+  double low_rank_storage_factor = 0.95;
+  int64_t batch_bytes = 6ll * 1024 * 1024 * 1024;  // device workspace per fill/ACA batch
+};
+
+struct HStats {
+  int64_t dense_blocks = 0, low_rank_blocks = 0, rejected_low_rank_blocks = 0;
+  int64_t forced_subdivisions_memory = 0, compression_tolerance_subdivisions = 0;
+  int64_t max_observed_rank = 0, sum_observed_rank = 0, block_entry_evaluations = 0;
+  int64_t near_entries = 0, far_entries = 0, n_far = 0, n_near = 0, aca_steps = 0, waves = 0;
+  double build_seconds = 0.0;
+};
+
+struct HBlock {
+  int32_t rs, re, cs, ce;
+  int32_t type;  // 1 far, 0 near
+  int32_t rank;
+  int64_t off_u, off_v;  // far: offsets (FP64 pool) of U^T (k x m) and V (k x n); near: off_u = tile offset
+  double relres;
+};
+
+struct HMatrix {
+  int device = 0;
+  int64_t Nb = 0;
+  HBuildConfig cfg;
+  HStats stats;
+  ClusterTree tree;
+  std::vector<HBlock> blocks;     // partition, in creation order
+  DevBuf<double> far_pool64;      // U^T / V factors, FP64
+  DevBuf<double> near_pool64;     // near tiles, FP64 row-major
+  DevBuf<double> diag_perm;       // diag_jump[perm]
+  DevBuf<int32_t> perm;
+  // apply-side packed data (built by pack())
+  Prec prec = Prec::F64;
+  bool packed = false;
+  DevBuf<char> far_f, near_f;     // factor / tile storage in the packed precision
+  DevBuf<int64_t> far_uoff, far_voff, far_zoff;  // per far block (element offsets)
+  DevBuf<int32_t> far_meta;       // per far block: rs, m, cs, n, k
+  DevBuf<int64_t> near_off;       // per near tile
+  DevBuf<int32_t> near_meta;      // per near tile: rs, m, cs, n
+  DevBuf<int32_t> leaf_start;     // [nleaf+1] row ranges of leaf clusters (perm space)
+  DevBuf<int64_t> item_ptr;       // [nleaf+1]
+  DevBuf<int32_t> items;          // encoded item: (block index << 1) | is_far
+  DevBuf<char> z;                 // far z vectors (accumulation type)
+  DevBuf<char> xperm;             // x in perm order (vector type)
+  int64_t nleaf = 0, zlen = 0, n_far = 0, n_near = 0;
+  int64_t bytes_far = 0, bytes_near = 0;
+
+  void build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s);
+  void pack(Prec p, cudaStream_t s);
+  // y = H x in the original boundary ordering, FP64 vectors
+  void apply_f64(const double* x, double* y, cudaStream_t s);
+  // apply with gather/scatter fused: x_b = src[gidx[i]] (i in boundary order), result written
+  // as dst[gidx[i]] = y_i (+ add[gidx[i]] if add != nullptr).  T is the vector type.
+  template <class T>
+  void apply_gather(const T* src, const int32_t* gidx, T* dst, const T* add, T* yb, cudaStream_t s);
+  int64_t device_bytes() const;
+};
+
+}  // namespace spx

@@ -1,0 +1,36 @@
+"""spinfemx_b200: B200-native demag + LLG hot path of SpinFEMx behind a C ABI.
+
+Lazy facade mirroring ``spinfemx.gpu`` (src/spinfemx/gpu/__init__.py:23-72): the
+public names resolve on first access, so importing the package does not load
+libspx.so or touch a GPU.
+"""
+from __future__ import annotations
+
+import importlib
+
+__version__ = "0.1.0"
+
+_EXPORTS = {
+    "DemagFieldLindholmGPU": ".demag",
+    "EffectiveField": ".llg",
+    "JvContext": ".llg",
+    "LLG_GPU": ".llg",
+    "HMatrixGPUPackedFused": ".hmatrix",
+    "HMatrixBuildConfig": ".hmatrix",
+    "build_or_load_hmatrix": ".hmatrix",
+    "BoundaryGeometry": ".geometry",
+    "kuhn_box": ".geometry",
+    "boundary_data": ".geometry",
+    "fem_assemble": ".geometry",
+    "cluster_tree_perm": ".geometry",
+    "dense_b_apply": ".geometry",
+}
+
+__all__ = sorted(_EXPORTS)
+
+
+def __getattr__(name):
+    if name in _EXPORTS:
+        mod = importlib.import_module(_EXPORTS[name], __name__)
+        return getattr(mod, name)
+    raise AttributeError(name)

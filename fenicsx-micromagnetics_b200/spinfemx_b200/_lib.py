@@ -1,0 +1,155 @@
+"""ctypes binding of libspx.so (the C ABI declared in include/spx.h).
+
+The library is loaded from this package directory.  A missing library raises
+ImportError: there is no CPU fallback for any operation of this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libspx.so"
+
+SPX_OK, SPX_ERR_INVALID, SPX_ERR_CUDA, SPX_ERR_OOM = 0, 1, 2, 3
+SPX_ERR_NOT_CONVERGED, SPX_ERR_TIMEOUT, SPX_ERR_INTERNAL, SPX_ERR_NO_DEVICE = 4, 5, 6, 7
+PREC = {"f64": 0, "fp64": 0, "float64": 0, "f32": 1, "fp32": 1, "float32": 1, "mixed": 2}
+
+c_i32, c_i64, c_dbl, c_vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
+P_i32, P_i64, P_dbl = C.POINTER(c_i32), C.POINTER(c_i64), C.POINTER(c_dbl)
+
+
+class HmatConfig(C.Structure):
+    _fields_ = [("epsilon", c_dbl), ("eta", c_dbl), ("leaf_size", c_i32), ("max_rank", c_i32),
+                ("max_temporary_block_bytes", c_i64), ("precision", c_i32), ("reserved", c_i32),
+                ("batch_bytes", c_i64)]
+
+
+class DemagOptions(C.Structure):
+    _fields_ = [("backend", c_i32), ("precision", c_i32), ("rtol_u1", c_dbl), ("rtol_u2", c_dbl),
+                ("atol", c_dbl), ("maxit_u1", c_i32), ("maxit_u2", c_i32), ("warm_start", c_i32),
+                ("reserved", c_i32), ("hmat", HmatConfig)]
+
+
+class LLGParams(C.Structure):
+    _fields_ = [("Ms", c_dbl), ("gamma", c_dbl), ("alpha", c_dbl), ("do_precess", c_dbl), ("Aex", c_dbl),
+                ("Ku", c_dbl), ("Ku_nodes", c_vp), ("n_ani", c_vp), ("D_int", c_dbl), ("n_int", c_vp),
+                ("H0_nodes", c_vp), ("H0_uniform", c_dbl * 3), ("use_demag", c_i32), ("precision", c_i32)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "spx_last_error": (C.c_char_p, []),
+    "spx_version": (C.c_int, []),
+    "spx_device_count": (C.c_int, [P_i32]),
+    "spx_boundary_sizes": (C.c_int, [c_vp, c_i64, c_vp, c_i64, P_i64, P_i64]),
+    "spx_boundary_data": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_fem_sizes": (C.c_int, [c_vp, c_i64, c_vp, c_i64, P_i64]),
+    "spx_fem_assemble": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_cluster_tree": (C.c_int, [c_vp, c_i64, c_i32, c_vp]),
+    "spx_boundary_create": (C.c_int, [c_vp, c_i64, c_vp, c_i64, C.POINTER(c_vp)]),
+    "spx_boundary_destroy": (C.c_int, [c_vp]),
+    "spx_boundary_info": (C.c_int, [c_vp, P_i64, P_i64, P_i32]),
+    "spx_lindholm_pairs": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp]),
+    "spx_lindholm_fill_block": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, c_vp, c_vp]),
+    "spx_dense_b_assemble": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_dense_b_apply": (C.c_int, [c_vp, c_i64, c_vp, c_vp, c_vp]),
+    "spx_hmat_build": (C.c_int, [c_vp, C.POINTER(HmatConfig), C.POINTER(c_vp)]),
+    "spx_hmat_stats": (C.c_int, [c_vp, P_i64, P_dbl]),
+    "spx_hmat_num_blocks": (C.c_int, [c_vp, P_i64]),
+    "spx_hmat_blocks": (C.c_int, [c_vp, c_vp, c_i64]),
+    "spx_hmat_perm": (C.c_int, [c_vp, c_vp]),
+    "spx_hmat_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_hmat_repack": (C.c_int, [c_vp, c_i32]),
+    "spx_hmat_far_factors": (C.c_int, [c_vp, c_i64, c_vp, c_vp]),
+    "spx_hmat_memory": (C.c_int, [c_vp, P_i64, P_i64, P_i64]),
+    "spx_hmat_destroy": (C.c_int, [c_vp]),
+    "spx_demag_create": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), C.POINTER(c_vp)]),
+    "spx_demag_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_demag_potentials": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_demag_energy": (C.c_int, [c_vp, c_vp, c_vp, P_dbl, c_vp]),
+    "spx_demag_stats": (C.c_int, [c_vp, P_i64, P_i64, P_dbl, P_dbl]),
+    "spx_demag_info": (C.c_int, [c_vp, P_i64, P_i64, P_i64, P_i64]),
+    "spx_demag_hmat": (C.c_int, [c_vp, C.POINTER(c_vp)]),
+    "spx_demag_destroy": (C.c_int, [c_vp]),
+    "spx_llg_create": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, C.POINTER(LLGParams), C.POINTER(c_vp)]),
+    "spx_llg_heff": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_hjac": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_rhs": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_update_jac_state": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_llg_jv": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_pc_build": (C.c_int, [c_vp, c_dbl, c_i32, c_i32, c_vp]),
+    "spx_llg_pc_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_set_state": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_llg_get_state": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_llg_step": (C.c_int, [c_vp, c_dbl, c_i64, c_vp]),
+    "spx_llg_run_host": (C.c_int, [c_vp, c_vp, c_vp, c_dbl, c_i64]),
+    "spx_llg_set_uniform_field": (C.c_int, [c_vp, c_dbl, c_dbl, c_dbl]),
+    "spx_llg_stats": (C.c_int, [c_vp, P_i64, P_i64, P_i64]),
+    "spx_llg_destroy": (C.c_int, [c_vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libspx.so once; raise ImportError if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with fenicsx-micromagnetics_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class SpxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[spx status {code}] {msg}")
+        self.code = code
+
+
+class SpxTimeout(SpxError):
+    pass
+
+
+def check(code: int):
+    if code == SPX_OK:
+        return
+    msg = lib().spx_last_error().decode(errors="replace")
+    if code == SPX_ERR_INVALID:
+        raise ValueError(msg)
+    if code == SPX_ERR_OOM:
+        raise MemoryError(msg)
+    if code == SPX_ERR_TIMEOUT:
+        raise SpxTimeout(code, msg)
+    raise SpxError(code, msg)
+
+
+def call(name, *args):
+    check(getattr(lib(), name)(*args))
+
+
+def ptr(t):
+    """Raw address of a torch tensor or numpy array (None -> NULL)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return t.ctypes.data_as(C.c_void_p)
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return C.c_void_p(s.cuda_stream)
+
+
+def device_count() -> int:
+    n = c_i32(0)
+    lib().spx_device_count(C.byref(n))
+    return int(n.value)

@@ -1,0 +1,142 @@
+"""FEM/BEM demagnetising field (drop-in for DemagFieldLindholmGPU).
+
+Mirrors ``gpu/fields/Demag_Lindholm_GPU.py``: same constructor option names
+(``boundary_backend``, ``ksp_rtol_u1/u2``, ``hmatrix_*``, ``dense_gpu_max_bytes``),
+``compute_vec(m_vec, out_vec)`` (:643-670), ``Energy_lumped_gpu`` (:706-724),
+``boundary_memory_report`` (:672-704) and the ``last_its_u1/u2`` attributes.
+Vectors are CUDA float64 torch tensors of length 3N in AoS order (the layout of
+the reference's PETSc CUDA Vec with block size 3) instead of PETSc Vecs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr
+from .geometry import as_mesh
+from .hmatrix import HMatrixGPUPackedFused
+
+
+class DemagFieldLindholmGPU:
+    def __init__(self, X, tets, Ms, *, ksp_rtol_u1=1e-6, ksp_rtol_u2=1e-6, ksp_atol=1e-12, ksp_maxit_u1=2000,
+                 ksp_maxit_u2=12000, incident_policy="skip", volume_scale=1e27, boundary_backend="dense",
+                 dense_gpu_max_bytes=512 * 1024 ** 2, hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
+                 hmatrix_compressor="fullaca", hmatrix_max_rank=None,
+                 hmatrix_max_temporary_block_bytes=256 * 1024 ** 2, hmatrix_use_fp32=True, precision="f64",
+                 warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False, **unused):
+        if str(incident_policy).lower()[:4] != "skip":
+            raise ValueError("only incident_policy='skip' (the reference default) is implemented")
+        if str(hmatrix_compressor).strip().lower() not in {"fullaca", "aca"}:
+            raise ValueError("the GPU builder implements the 'fullaca' compressor")
+        X, tets = as_mesh(X, tets)
+        self.X, self.tets = X, tets
+        self.N = X.shape[0]
+        self.local_size = 3 * self.N
+        self.Ms = float(Ms)
+        self.mu0 = 4.0 * np.pi * 1e-7
+        self.volume_scale = float(volume_scale)
+        self.precision = precision
+        req = str(boundary_backend).strip().lower()
+        if req not in {"dense", "hmatrix", "auto"}:
+            raise ValueError("boundary_backend must be 'dense', 'hmatrix', or 'auto'.")
+        if req == "auto":
+            Nb = _lib.c_i64()
+            call("spx_boundary_sizes", ptr(X), self.N, ptr(tets), tets.shape[0], C.byref(Nb), None)
+            req = "dense" if Nb.value * Nb.value * 8 <= int(dense_gpu_max_bytes) else "hmatrix"
+        self.boundary_backend = req
+        hprec = precision
+        if req == "hmatrix" and precision == "f64" and hmatrix_use_fp32:
+            hprec = "f64"  # FP64 solvers keep the FP64 factors unless a reduced form is asked for
+        o = _lib.DemagOptions()
+        o.backend = 0 if req == "dense" else 1
+        o.precision = _lib.PREC[precision]
+        o.rtol_u1, o.rtol_u2, o.atol = float(ksp_rtol_u1), float(ksp_rtol_u2), float(ksp_atol)
+        o.maxit_u1, o.maxit_u2 = int(ksp_maxit_u1), int(ksp_maxit_u2)
+        o.warm_start = 1 if warm_start else 0
+        o.hmat = _lib.HmatConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
+                                 leaf_size=int(hmatrix_leaf_size), max_rank=int(hmatrix_max_rank or 0),
+                                 max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
+                                 precision=_lib.PREC[hprec], reserved=0, batch_bytes=int(hmatrix_batch_bytes))
+        self._h = C.c_void_p()
+        call("spx_demag_create", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o), C.byref(self._h))
+        N, Nb, NI, by = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+        call("spx_demag_info", self._h, C.byref(N), C.byref(Nb), C.byref(NI), C.byref(by))
+        self.Nb, self.NI = Nb.value, NI.value
+        self.last_its_u1 = 0
+        self.last_its_u2 = 0
+        self.B_dense_gpu = None
+        self.B_hmatrix_gpu = None
+        if req == "hmatrix":
+            hh = C.c_void_p()
+            call("spx_demag_hmat", self._h, C.byref(hh))
+            self.B_hmatrix_gpu = HMatrixGPUPackedFused.from_handle(hh, self, hprec, self.Nb)
+            if hmatrix_verbose:
+                st = self.B_hmatrix_gpu.stats()
+                print(f"[Demag Lindholm HMatrix b200] built in {st['build_time_seconds']:.2f} s | "
+                      f"far={st['n_far']:,} | rank avg/max={st['average_far_rank']:.1f}/"
+                      f"{st['max_observed_rank']}", flush=True)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _check(self, v, name):
+        import torch
+        if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float64):
+            raise TypeError(f"{name} must be a CUDA float64 tensor")
+        if v.numel() < self.local_size or not v.is_contiguous():
+            raise RuntimeError(f"{name} must be contiguous with at least {self.local_size} entries")
+
+    def compute_vec(self, m_vec, out_vec):
+        """H_demag(m) into out_vec (AoS, length 3N; entries past 3N are zeroed)."""
+        self._check(m_vec, "m_vec")
+        self._check(out_vec, "out_vec")
+        call("spx_demag_apply", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
+        if out_vec.numel() > self.local_size:
+            out_vec[self.local_size:] = 0.0
+        i1, i2, r1, r2 = _lib.c_i64(), _lib.c_i64(), _lib.c_dbl(), _lib.c_dbl()
+        call("spx_demag_stats", self._h, C.byref(i1), C.byref(i2), C.byref(r1), C.byref(r2))
+        self.last_its_u1, self.last_its_u2 = i1.value, i2.value
+        self.last_res_u1, self.last_res_u2 = r1.value, r2.value
+        return out_vec
+
+    def potentials(self):
+        import torch
+        u1 = torch.empty(self.N, dtype=torch.float64, device="cuda")
+        u2 = torch.empty_like(u1)
+        call("spx_demag_potentials", self._h, ptr(u1), ptr(u2), _lib.stream_ptr())
+        return u1, u2
+
+    def Energy_lumped_gpu(self, m_vec, h_vec):
+        self._check(m_vec, "m_vec")
+        self._check(h_vec, "h_vec")
+        E = _lib.c_dbl()
+        call("spx_demag_energy", self._h, ptr(m_vec), ptr(h_vec), C.byref(E), _lib.stream_ptr())
+        return float(E.value) * (1e27 / self.volume_scale)
+
+    def boundary_memory_report(self):
+        N, Nb, NI, by = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+        call("spx_demag_info", self._h, C.byref(N), C.byref(Nb), C.byref(NI), C.byref(by))
+        if self.boundary_backend == "dense":
+            b = Nb.value * Nb.value * 8
+            return {"backend": "dense", "Nb": Nb.value, "accounted_gpu_bytes": b,
+                    "accounted_gpu_mib": b / 2 ** 20, "total_device_bytes": by.value}
+        rep = self.B_hmatrix_gpu.memory_report()
+        rep["Nb"] = Nb.value
+        rep["total_device_bytes"] = by.value
+        return rep
+
+    def print_boundary_memory_report(self):
+        for k, v in self.boundary_memory_report().items():
+            print(f"[Demag Lindholm b200] {k}: {v}", flush=True)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().spx_demag_destroy(h)
+            except Exception:
+                pass
+            self._h = C.c_void_p()

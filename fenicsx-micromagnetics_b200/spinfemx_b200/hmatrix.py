@@ -1,0 +1,242 @@
+"""H-matrix of the Lindholm double-layer operator on the GPU.
+
+Mirrors the reference package ``gpu/fields/lindholm_hmatrix_gpu``:
+
+* ``HMatrixBuildConfig``      builder.py:24-95 (same fields, same validation)
+* ``build_or_load_hmatrix``   builder.py:814-927 (GPU construction; the npz cache
+  format is not implemented: every call builds)
+* ``HMatrixGPUPackedFused``   backend_fused.py:341-646 (``matvec``, ``matvec_numpy``,
+  ``benchmark``, ``benchmark_roundtrip``, ``memory_report``)
+
+Construction (tree, partition, fill, full-pivot ACA) and the apply run in
+libspx; see csrc/hbuild.cu and csrc/hmat.cu.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from time import perf_counter
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr
+from .geometry import BoundaryGeometry
+
+STAT_NAMES = ("dense_blocks", "low_rank_blocks", "rejected_low_rank_blocks", "forced_subdivisions_memory",
+              "compression_tolerance_subdivisions", "max_observed_rank", "sum_observed_rank",
+              "block_entry_evaluations", "near_entries", "far_entries", "n_far", "n_near", "aca_steps", "waves")
+
+
+@dataclass
+class HMatrixBuildConfig:
+    epsilon: float = 1e-6
+    eta: float = 2.0
+    leaf_size: int = 64
+    compressor: str = "fullaca"
+    max_rank: int | None = None
+    max_temporary_block_bytes: int = 256 * 1024 * 1024
+    low_rank_storage_factor: float = 0.95
+    build_backend: str = "gpu"
+    batch_bytes: int = 0
+
+    def __post_init__(self):
+        if self.epsilon <= 0.0:
+            raise ValueError("epsilon must be positive.")
+        if self.eta <= 0.0:
+            raise ValueError("eta must be positive.")
+        if self.leaf_size < 1:
+            raise ValueError("leaf_size must be positive.")
+        if self.max_temporary_block_bytes < 8:
+            raise ValueError("max_temporary_block_bytes is too small.")
+        if not (0.0 < self.low_rank_storage_factor <= 1.0):
+            raise ValueError("low_rank_storage_factor must be in (0, 1].")
+        if self.low_rank_storage_factor != 0.95:
+            raise ValueError("only low_rank_storage_factor=0.95 (the reference default) is supported")
+        c = str(self.compressor).strip().lower()
+        if c == "aca":
+            c = "fullaca"
+        if c != "fullaca":
+            raise ValueError("the GPU builder implements the 'fullaca' compressor")
+        self.compressor = c
+        b = str(self.build_backend).strip().lower()
+        if b not in {"gpu", "auto", "cpu"}:
+            raise ValueError("build_backend must be 'cpu', 'gpu', or 'auto'.")
+        self.build_backend = "gpu"
+
+    def to_c(self, precision="f64"):
+        return _lib.HmatConfig(epsilon=self.epsilon, eta=self.eta, leaf_size=int(self.leaf_size),
+                               max_rank=int(self.max_rank or 0),
+                               max_temporary_block_bytes=int(self.max_temporary_block_bytes),
+                               precision=_lib.PREC[precision], reserved=0, batch_bytes=int(self.batch_bytes))
+
+
+def _precision_name(use_fp32=True, precision=None):
+    if precision is not None:
+        if precision not in _lib.PREC:
+            raise ValueError(f"unknown precision {precision!r}")
+        return precision
+    return "f32" if use_fp32 else "f64"
+
+
+class HMatrixGPUPackedFused:
+    """Packed GPU H-matrix (y = H x in the original boundary ordering).
+
+    ``HMatrixGPUPackedFused(geometry, config, use_fp32=True, precision=None)`` builds
+    the matrix on the device; ``from_handle`` wraps one owned by a demag object.
+    ``use_fp32`` stores factors and near tiles in FP32 (``precision='f64'`` keeps
+    everything in FP64, ``'mixed'`` uses BF16 far factors and FP32 near tiles).
+    """
+
+    backend_name = "packed_fused_b200"
+
+    def __init__(self, geometry: BoundaryGeometry | None = None, config: HMatrixBuildConfig | None = None,
+                 threads_per_block=128, use_fp32=True, precision=None, _handle=None, _owner=None, _size=None):
+        if threads_per_block < 32 or threads_per_block > 1024:
+            raise ValueError("threads_per_block must be between 32 and 1024.")
+        self.precision = _precision_name(use_fp32, precision)
+        self._owner = _owner
+        if _handle is not None:
+            self._h = _handle
+            self._owned = False
+        else:
+            if geometry is None:
+                raise ValueError("a BoundaryGeometry is required")
+            self._geometry = geometry
+            cfg = config or HMatrixBuildConfig()
+            self._h = C.c_void_p()
+            c = cfg.to_c(self.precision)
+            call("spx_hmat_build", geometry.handle, C.byref(c), C.byref(self._h))
+            self._owned = True
+        n = _lib.c_i64()
+        call("spx_hmat_num_blocks", self._h, C.byref(n))
+        self._nblocks = n.value
+        st = self.stats()
+        self.size = int(_size if _size is not None else geometry.Nb)
+        self.n_far_blocks = st["n_far"]
+        self.max_rank = st["max_observed_rank"]
+
+    @classmethod
+    def from_handle(cls, handle, owner, precision, size):
+        return cls(_handle=handle, _owner=owner, precision=precision, _size=size)
+
+    # --------------------------------------------------------------- info
+    def stats(self):
+        v = np.zeros(16, np.int64)
+        secs = _lib.c_dbl()
+        call("spx_hmat_stats", self._h, ptr(v), C.byref(secs))
+        d = {k: int(v[i]) for i, k in enumerate(STAT_NAMES)}
+        d["build_time_seconds"] = float(secs.value)
+        d["average_far_rank"] = d["sum_observed_rank"] / max(d["low_rank_blocks"], 1)
+        return d
+
+    def blocks(self):
+        out = np.zeros((self._nblocks, 6), np.int64)
+        call("spx_hmat_blocks", self._h, ptr(out), self._nblocks)
+        return out
+
+    def partition(self):
+        b = self.blocks()
+        return sorted(tuple(int(v) for v in r[:5]) for r in b)
+
+    def far_factors(self, index):
+        b = self.blocks()[index]
+        m, n, k = int(b[1] - b[0]), int(b[3] - b[2]), int(b[5])
+        Ut = np.empty((k, m))
+        V = np.empty((k, n))
+        call("spx_hmat_far_factors", self._h, int(index), ptr(Ut), ptr(V))
+        return Ut.T.copy(), V
+
+    @property
+    def perm(self):
+        p = np.empty(self.size, np.int32)
+        call("spx_hmat_perm", self._h, ptr(p))
+        return p
+
+    def repack(self, precision):
+        call("spx_hmat_repack", self._h, _lib.PREC[precision])
+        self.precision = precision
+
+    # --------------------------------------------------------------- apply
+    def matvec(self, x_gpu, out=None):
+        import torch
+        if x_gpu.dtype != torch.float64 or not x_gpu.is_cuda:
+            raise TypeError("matvec expects a CUDA float64 tensor")
+        x = x_gpu.contiguous()
+        if out is None:
+            out = torch.empty_like(x)
+        call("spx_hmat_apply", self._h, ptr(x), ptr(out), _lib.stream_ptr())
+        return out
+
+    def matvec_numpy(self, x):
+        import torch
+        xt = torch.as_tensor(np.asarray(x, dtype=np.float64), device="cuda")
+        return self.matvec(xt).cpu().numpy()
+
+    def benchmark(self, x, repeats=20, warmup=3):
+        import torch
+        xt = torch.as_tensor(np.asarray(x, dtype=np.float64), device="cuda")
+        out = torch.empty_like(xt)
+        for _ in range(warmup):
+            self.matvec(xt, out=out)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(repeats):
+            self.matvec(xt, out=out)
+        e.record()
+        e.synchronize()
+        sec = s.elapsed_time(e) * 1e-3
+        return {"timer": "cuda_events", "repeats": int(repeats), "total_seconds": sec,
+                "average_seconds": sec / repeats}
+
+    def benchmark_roundtrip(self, x, repeats=20, warmup=3):
+        import torch
+        for _ in range(warmup):
+            self.matvec_numpy(x)
+        torch.cuda.synchronize()
+        t0 = perf_counter()
+        for _ in range(repeats):
+            self.matvec_numpy(x)
+        torch.cuda.synchronize()
+        el = perf_counter() - t0
+        return {"timer": "perf_counter_roundtrip", "repeats": int(repeats), "total_seconds": el,
+                "average_seconds": el / repeats}
+
+    def memory_report(self):
+        f, n, t = _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+        call("spx_hmat_memory", self._h, C.byref(f), C.byref(n), C.byref(t))
+        st = self.stats()
+        return {"backend": self.backend_name, "n_far_blocks": st["n_far"], "max_rank": st["max_observed_rank"],
+                "precision": self.precision, "far_bytes": f.value, "near_bytes": n.value,
+                "accounted_gpu_bytes": t.value, "accounted_gpu_human": f"{t.value / 2**20:.3f} MiB"}
+
+    def print_memory_report(self, prefix="[HMatrixGPUPackedFused]"):
+        for k, v in self.memory_report().items():
+            print(f"{prefix} {k:28s}: {v}", flush=True)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if getattr(self, "_owned", False) and h is not None and h.value:
+            try:
+                _lib.lib().spx_hmat_destroy(h)
+            except Exception:
+                pass
+            self._h = C.c_void_p()
+
+
+def build_or_load_hmatrix(cache_path, X, tets, config: HMatrixBuildConfig | None = None, *,
+                          precision="f32", force_rebuild=False, verbose=False, geometry=None):
+    """Build the H-matrix of the mesh boundary on the GPU (builder.py:814-927).
+
+    ``cache_path`` is accepted for call compatibility; this build does not write or
+    read the reference's npz cache.
+    """
+    del cache_path, force_rebuild
+    geom = geometry or BoundaryGeometry(X, tets)
+    H = HMatrixGPUPackedFused(geom, config or HMatrixBuildConfig(), precision=precision)
+    if verbose:
+        st = H.stats()
+        print(f"[HMatrix b200] built in {st['build_time_seconds']:.2f} s | far={st['n_far']} near={st['n_near']} "
+              f"| rank avg/max={st['average_far_rank']:.1f}/{st['max_observed_rank']}", flush=True)
+    return H

@@ -1,0 +1,285 @@
+"""Effective field, LLG right-hand side, Jv, block preconditioner and driver.
+
+Mirrors ``gpu/solvers/llg_module_GPU.py``:
+
+* ``EffectiveField`` (:387-1408): ``compute_H_eff_vec``, ``compute_H_jac_vec``,
+  ``llg_rhs_vec``, ``update_jac_state``, ``jac_vec_times_vec``,
+  ``apply_jacobian_field_vec``, ``set_uniform_field``, ``rhs_function``,
+  ``ifunction`` and the ``LLGSteps`` / ``JacSteps`` counters;
+* ``JvContext`` (:1412-1543): ``update_pc_full_fast_gpu``, ``mult``, ``apply``;
+* ``LLG_GPU`` (:1549): ``add_exchange``, ``add_demag``, ``add_anisotropy``,
+  ``add_dmi_interfacial``, ``add_external_field`` and ``run_fixed`` (classic RK4 at a
+  fixed step; the reference drives PETSc TS rk/5dp or BDF instead).
+
+Vectors are CUDA float64 torch tensors of length 3N (AoS).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, ptr
+from .demag import DemagFieldLindholmGPU
+from .geometry import as_mesh
+
+
+def _vec3(a, N, name):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+    if a.size == 3:
+        a = np.tile(a, N)
+    if a.size != 3 * N:
+        raise ValueError(f"{name} must have 3 or 3N entries")
+    return a
+
+
+class EffectiveField:
+    def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani_vec=None, D_bulk=0.0, D_int=0.0, n0_int_vec=None,
+                 gamma=2.211e5, alpha=0.5, do_precess=1, use_demag=False, demag_method="lindholm",
+                 demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64"):
+        if float(D_bulk) != 0.0:
+            raise NotImplementedError("bulk DMI is not part of this build")
+        if str(demag_method).lower() not in {"lindholm", "lindholm_gpu"}:
+            raise NotImplementedError("only the Lindholm FEM/BEM demag method is implemented")
+        X, tets = as_mesh(X, tets)
+        self.X, self.tets = X, tets
+        self.N = X.shape[0]
+        self.local_dofs = self.N
+        self.local_size = 3 * self.N
+        self.Ms, self.gamma, self.alpha = float(Ms), float(gamma), float(alpha)
+        self.do_precess = float(do_precess)
+        self.A, self.Ku, self.D_int = float(Aex), float(Ku), float(D_int)
+        self.prefactorEQ = -self.gamma / (1.0 + self.alpha ** 2)
+        self.Stab = self.Ms * self.gamma / (1.0 + self.alpha ** 2) * 0.5
+        self.LLGSteps = 0
+        self.JacSteps = 0
+        self.current_time = 0.0
+        self.demag_field = None
+        if use_demag:
+            kw = dict(demag_kwargs or {})
+            kw.setdefault("precision", precision)
+            self.demag_field = DemagFieldLindholmGPU(X, tets, self.Ms, **kw)
+            precision = self.demag_field.precision
+        self.precision = precision
+        self._keep = []
+        p = _lib.LLGParams()
+        p.Ms, p.gamma, p.alpha, p.do_precess = self.Ms, self.gamma, self.alpha, self.do_precess
+        p.Aex, p.Ku, p.D_int = self.A, self.Ku, self.D_int
+        n_ani = _vec3(n_ani_vec, self.N, "n_ani_vec")
+        n_int = _vec3(n0_int_vec, self.N, "n0_int_vec")
+        H0 = _vec3(H0_static, self.N, "H0_static")
+        kun = None if Ku_nodes is None else np.ascontiguousarray(Ku_nodes, dtype=np.float64).reshape(-1)
+        if kun is not None and kun.size != self.N:
+            raise ValueError("Ku_nodes must have N entries")
+        if (self.Ku != 0.0 or kun is not None) and n_ani is None:
+            raise ValueError("anisotropy needs n_ani_vec")
+        for a in (n_ani, n_int, H0, kun):
+            if a is not None:
+                self._keep.append(a)
+        p.n_ani = ptr(n_ani).value if n_ani is not None and (self.Ku != 0.0 or kun is not None) else None
+        p.Ku_nodes = ptr(kun).value if kun is not None else None
+        p.n_int = ptr(n_int).value if n_int is not None and self.D_int != 0.0 else None
+        p.H0_nodes = ptr(H0).value if H0 is not None else None
+        self._H0 = H0 if H0 is not None else np.zeros(3 * self.N)
+        p.use_demag = 1 if use_demag else 0
+        p.precision = _lib.PREC[precision]
+        self._h = C.c_void_p()
+        dh = self.demag_field.handle if self.demag_field is not None else None
+        call("spx_llg_create", dh, ptr(X), self.N, ptr(tets), tets.shape[0], C.byref(p), C.byref(self._h))
+        self._H0_dev = None
+
+    # -------------------------------------------------------------- helpers
+    def _chk(self, v, name):
+        import torch
+        if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float64 and v.is_contiguous()):
+            raise TypeError(f"{name} must be a contiguous CUDA float64 tensor")
+        if v.numel() < self.local_size:
+            raise RuntimeError(f"{name} needs {self.local_size} entries")
+
+    def _tail(self, v):
+        if v.numel() > self.local_size:
+            v[self.local_size:] = 0.0
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -------------------------------------------------------------- fields
+    def set_uniform_field(self, Hx, Hy, Hz):
+        call("spx_llg_set_uniform_field", self._h, float(Hx), float(Hy), float(Hz))
+        self._H0 = np.tile([float(Hx), float(Hy), float(Hz)], self.N)
+        self._H0_dev = None
+
+    def compute_H_eff_vec(self, m_vec, out_vec):
+        self._chk(m_vec, "m_vec")
+        self._chk(out_vec, "out_vec")
+        call("spx_llg_heff", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
+        self._tail(out_vec)
+
+    def compute_H_jac_vec(self, m_vec, out_vec):
+        self._chk(m_vec, "m_vec")
+        self._chk(out_vec, "out_vec")
+        call("spx_llg_hjac", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
+        self._tail(out_vec)
+
+    def apply_jacobian_field_vec(self, m_state_vec, v_vec, out_vec):
+        """dH_eff/dm v for the linear terms (exchange, anisotropy, DMI); no demag, no H0."""
+        import torch
+        self.compute_H_jac_vec(v_vec, out_vec)
+        if self._H0_dev is None:
+            self._H0_dev = torch.as_tensor(self._H0, device=out_vec.device)
+        out_vec[: self.local_size] -= self._H0_dev
+
+    def llg_rhs_vec(self, m_vec, out_vec):
+        self.LLGSteps += 1
+        self._chk(m_vec, "m_vec")
+        self._chk(out_vec, "out_vec")
+        call("spx_llg_rhs", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
+        self._tail(out_vec)
+
+    def update_jac_state(self, m_vec):
+        self._chk(m_vec, "m_vec")
+        call("spx_llg_update_jac_state", self._h, ptr(m_vec), _lib.stream_ptr())
+
+    def jac_vec_times_vec(self, v_vec, out_vec):
+        self.JacSteps += 1
+        self._chk(v_vec, "v_vec")
+        self._chk(out_vec, "out_vec")
+        call("spx_llg_jv", self._h, ptr(v_vec), ptr(out_vec), _lib.stream_ptr())
+        self._tail(out_vec)
+
+    # PETSc TS callback shapes (llg_module_GPU.py:1328-1339, 1403-1408)
+    def rhs_function(self, ts, t, y, f):
+        self.current_time = float(t)
+        self.llg_rhs_vec(y, f)
+        return 0
+
+    def ifunction(self, ts, t, y, ydot, f):
+        import torch
+        self.current_time = float(t)
+        r = torch.empty_like(f)
+        self.llg_rhs_vec(y, r)
+        f.copy_(ydot - r)
+        return 0
+
+    # -------------------------------------------------------------- integrator
+    def set_state(self, m_vec):
+        self._chk(m_vec, "m_vec")
+        call("spx_llg_set_state", self._h, ptr(m_vec), _lib.stream_ptr())
+
+    def get_state(self, out_vec=None):
+        import torch
+        if out_vec is None:
+            out_vec = torch.empty(self.local_size, dtype=torch.float64, device="cuda")
+        call("spx_llg_get_state", self._h, ptr(out_vec), _lib.stream_ptr())
+        return out_vec
+
+    def step(self, dt, nsteps=1):
+        call("spx_llg_step", self._h, float(dt), int(nsteps), _lib.stream_ptr())
+
+    def run_host(self, m_host, dt, nsteps, out=None):
+        """End-to-end call on host buffers (numpy or pinned torch CPU tensors)."""
+        if out is None:
+            out = np.empty_like(m_host)
+        call("spx_llg_run_host", self._h, ptr(m_host), ptr(out), float(dt), int(nsteps))
+        return out
+
+    def stats(self):
+        s, r, l = _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
+        call("spx_llg_stats", self._h, C.byref(s), C.byref(r), C.byref(l))
+        return {"steps": s.value, "rhs_evals": r.value, "launches": l.value}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().spx_llg_destroy(h)
+            except Exception:
+                pass
+            self._h = C.c_void_p()
+
+
+class JvContext:
+    """Matrix-free Jacobian context: y = shift x - J x, and the 3x3 block PC."""
+
+    def __init__(self, hef: EffectiveField, eps_reg=1e-14, det_eps=1e-30):
+        if eps_reg != 1e-14 or det_eps != 1e-30:
+            raise ValueError("eps_reg=1e-14 and det_eps=1e-30 are fixed in this build")
+        self.hef = hef
+        self.shift = 0.0
+        self.calls = 0
+        self.callsPre = 0
+        self._pc_ready = False
+        import torch
+        self._jv = torch.empty(hef.local_size, dtype=torch.float64, device="cuda")
+
+    def update_pc_full_fast_gpu(self, shift, include_stab=True, use_abs_kappa=True):
+        self.shift = float(shift)
+        call("spx_llg_pc_build", self.hef.handle, self.shift, int(bool(include_stab)), int(bool(use_abs_kappa)),
+             _lib.stream_ptr())
+        self._pc_ready = True
+
+    def mult(self, A, x, y):
+        self.calls += 1
+        self.hef.jac_vec_times_vec(x, self._jv)
+        y.copy_(self.shift * x - self._jv)
+
+    def apply(self, pc, x, y):
+        self.callsPre += 1
+        if not self._pc_ready:
+            y.copy_(x)
+            return
+        call("spx_llg_pc_apply", self.hef.handle, ptr(x), ptr(y), _lib.stream_ptr())
+
+
+class LLG_GPU:
+    """Builder-style driver (llg_module_GPU.py:1549-1700) with a fixed-step RK4 run."""
+
+    def __init__(self, X, tets, Ms, gamma=2.211e5, alpha=0.5, do_precess=1, precision="f64"):
+        self.X, self.tets = as_mesh(X, tets)
+        self.Ms, self.gamma, self.alpha, self.do_precess = float(Ms), float(gamma), float(alpha), do_precess
+        self.precision = precision
+        self._kw = dict(Aex=0.0, Ku=0.0, n_ani_vec=None, D_int=0.0, n0_int_vec=None, H0_static=None,
+                        Ku_nodes=None)
+        self._demag = None
+        self.hef = None
+
+    def add_exchange(self, Aex):
+        self._kw["Aex"] = float(Aex)
+
+    def add_demag(self, method="lindholm", **kwargs):
+        self._demag = dict(kwargs)
+
+    def add_anisotropy(self, Ku, n_vec, Ku_nodes=None):
+        self._kw.update(Ku=float(Ku), n_ani_vec=n_vec, Ku_nodes=Ku_nodes)
+
+    def add_dmi_interfacial(self, D_int, n0_vec):
+        self._kw.update(D_int=float(D_int), n0_int_vec=n0_vec)
+
+    def add_dmi_bulk(self, D_bulk):
+        raise NotImplementedError("bulk DMI is not part of this build")
+
+    def add_external_field(self, H0_vec=None, H_time_func=None):
+        if H_time_func is not None:
+            raise NotImplementedError("time-dependent fields are not part of this build")
+        self._kw["H0_static"] = H0_vec
+
+    def _build(self):
+        if self.hef is None:
+            self.hef = EffectiveField(self.X, self.tets, self.Ms, gamma=self.gamma, alpha=self.alpha,
+                                      do_precess=self.do_precess, use_demag=self._demag is not None,
+                                      demag_kwargs=self._demag, precision=self.precision, **self._kw)
+        return self.hef
+
+    def run_fixed(self, m0, dt, nsteps):
+        """Integrate nsteps of RK4 at step dt from m0 (3N numpy or CUDA tensor); returns m (CUDA tensor)."""
+        import torch
+        hef = self._build()
+        m = torch.as_tensor(np.asarray(m0, dtype=np.float64) if not isinstance(m0, torch.Tensor) else m0,
+                            dtype=torch.float64, device="cuda").contiguous()
+        hef.set_state(m)
+        hef.step(dt, nsteps)
+        return hef.get_state()

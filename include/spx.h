@@ -1,0 +1,193 @@
+/* libspx: B200 (sm_100a) FEM/BEM demagnetising field and LLG right-hand side.
+ *
+ * Drop-in C ABI for the hot path of the SpinFEMx GPU backend
+ * (NanoPilot1/FEniCSx-Micromagnetics, package src/spinfemx).  Every entry point
+ * is extern "C", takes plain pointers and sizes, returns an int status (SPX_OK
+ * on success) and never throws or exits; the message of the last failure on the
+ * calling thread is returned by spx_last_error().
+ *
+ * Conventions
+ *   - mesh coordinates X [N][3] in nm (the unit the reference's operators assume,
+ *     gpu/fields/Exchange_GPU.py:62), tets [E][4] int32 vertex ids;
+ *   - nodal vectors are AoS FP64 device pointers [N][3], the layout of the
+ *     reference's PETSc CUDA Vec with block size 3 (gpu/solvers/llg_module_GPU.py:25-39);
+ *   - "device" pointers are CUDA device memory of the current device; calls are
+ *     ordered on the given stream (NULL = legacy default stream);
+ *   - handles are not thread-safe; one handle per thread or external locking.
+ */
+#ifndef SPX_H
+#define SPX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SPX_API __attribute__((visibility("default")))
+#else
+#define SPX_API
+#endif
+
+typedef struct CUstream_st* spx_stream_t; /* same type as cudaStream_t */
+
+#define SPX_OK 0
+#define SPX_ERR_INVALID 1
+#define SPX_ERR_CUDA 2
+#define SPX_ERR_OOM 3
+#define SPX_ERR_NOT_CONVERGED 4
+#define SPX_ERR_TIMEOUT 5
+#define SPX_ERR_INTERNAL 6
+#define SPX_ERR_NO_DEVICE 7
+
+#define SPX_PREC_F64 0   /* every vector, factor and tile in FP64                        */
+#define SPX_PREC_F32 1   /* FP32 vectors/solvers, FP32 H-matrix factors and near tiles    */
+#define SPX_PREC_MIXED 2 /* FP32 vectors, BF16 far factors, FP32 near tiles, compensated */
+
+/* ------------------------------------------------------------------ library */
+SPX_API const char* spx_last_error(void);
+SPX_API int spx_version(void);
+/* number of visible CUDA devices (0 without a GPU; never fails) */
+SPX_API int spx_device_count(int32_t* n);
+
+/* ------------------------------------------------------------------ host geometry
+ * Boundary data of build_boundary_data_serial (gpu/fields/Demag_Lindholm.py:177-285):
+ * outward boundary triangles in a canonical order (sorted ascending vertex triples),
+ * Xb in ascending vertex order, omega_sum = sum over tets of |solid angle|. */
+SPX_API int spx_boundary_sizes(const double* X, int64_t N, const int32_t* tets, int64_t E, int64_t* Nb, int64_t* Nt);
+/* any output may be NULL; sizes Nb / Nt from spx_boundary_sizes */
+SPX_API int spx_boundary_data(const double* X, int64_t N, const int32_t* tets, int64_t E, int32_t* bverts,
+                      int32_t* tri_lid, double* Xb, double* ntri, double* area, double* omega_sum);
+/* P1 operators of gpu/fields/Demag_Lindholm_GPU.py:188-261, 554-567 and the lumped
+ * volume of llg_module_GPU.py:469-484 on the scalar node pattern (CSR, sorted columns):
+ * A = int grad u.grad v ; Div[k*3+c] = int d_c(v_i) phi_j (multiply by Ms) ;
+ * G[k*3+c] = -int phi_i d_c(phi_j) ; vol = int phi_i. */
+SPX_API int spx_fem_sizes(const double* X, int64_t N, const int32_t* tets, int64_t E, int64_t* nnz);
+SPX_API int spx_fem_assemble(const double* X, int64_t N, const int32_t* tets, int64_t E, int64_t* rowptr, int32_t* col,
+                     double* A, double* Div, double* G, double* vol);
+/* cluster-tree permutation of gpu/fields/lindholm_hmatrix_gpu/tree.py:41-96 (bit-exact) */
+SPX_API int spx_cluster_tree(const double* pts, int64_t n, int32_t leaf_size, int32_t* perm);
+
+/* ------------------------------------------------------------------ boundary geometry on the device */
+typedef struct spx_boundary_s* spx_boundary;
+SPX_API int spx_boundary_create(const double* X, int64_t N, const int32_t* tets, int64_t E, spx_boundary* out);
+SPX_API int spx_boundary_destroy(spx_boundary b);
+SPX_API int spx_boundary_info(spx_boundary b, int64_t* Nb, int64_t* Nt, int32_t* max_incident);
+/* Lindholm weights (gpu/fields/Lindholm_kernel.py:66-125, CUDA twin
+ * lindholm_hmatrix_gpu/entry_provider_gpu.py:94-203) for P targets x0 [P][3] against
+ * boundary triangles tri [P]; w [P][3].  Device pointers. */
+SPX_API int spx_lindholm_pairs(spx_boundary b, const double* x0, const int32_t* tri, int64_t P, double* w,
+                       spx_stream_t s);
+/* B[rows, cols] without the diagonal jump, row-major m x n (LindholmEntryProviderGPU.fill_block_device,
+ * entry_provider_gpu.py:687-750; CPU entry_provider.py:41-117).  rows/cols: device int32 boundary ids. */
+SPX_API int spx_lindholm_fill_block(spx_boundary b, const int32_t* rows, int64_t m, const int32_t* cols, int64_t n,
+                            double* out, spx_stream_t s);
+/* dense Nb x Nb row-major B including diag Omega/4pi - 1 (assemble_B_rows_owned,
+ * gpu/fields/Demag_Lindholm.py:51-116) */
+SPX_API int spx_dense_b_assemble(spx_boundary b, double* B, spx_stream_t s);
+/* y = B x (cp.matmul in DemagFieldLindholmGPU._apply_B_gpu, Demag_Lindholm_GPU.py:600-605) */
+SPX_API int spx_dense_b_apply(const double* B, int64_t Nb, const double* x, double* y, spx_stream_t s);
+
+/* ------------------------------------------------------------------ H-matrix */
+typedef struct spx_hmat_s* spx_hmat;
+typedef struct {
+  double epsilon;                    /* ACA tolerance (HMatrixBuildConfig.epsilon, builder.py:24-95) */
+  double eta;                        /* admissibility */
+  int32_t leaf_size;
+  int32_t max_rank;                  /* <= 0: no limit */
+  int64_t max_temporary_block_bytes; /* forced subdivision above this dense size */
+  int32_t precision;                 /* SPX_PREC_* of the packed apply data */
+  int32_t reserved;
+  int64_t batch_bytes;               /* device workspace per fill/ACA batch (0: default) */
+} spx_hmat_config;
+/* build: cluster tree, block partition, GPU fill and full-pivot ACA
+ * (HMatrixBuilder.build / build_or_load_hmatrix, builder.py:186-419, 814-927) */
+SPX_API int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out);
+/* stats[16]: dense_blocks, low_rank_blocks, rejected_low_rank_blocks, forced_subdivisions_memory,
+ * compression_tolerance_subdivisions, max_observed_rank, sum_observed_rank, block_entry_evaluations,
+ * near_entries, far_entries, n_far, n_near, aca_steps, waves, 0, 0 */
+SPX_API int spx_hmat_stats(spx_hmat h, int64_t* stats16, double* build_seconds);
+SPX_API int spx_hmat_num_blocks(spx_hmat h, int64_t* n);
+/* blocks [n][6]: row_start, row_stop, col_start, col_stop, is_far, rank (permuted coordinates) */
+SPX_API int spx_hmat_blocks(spx_hmat h, int64_t* out6, int64_t capacity);
+SPX_API int spx_hmat_perm(spx_hmat h, int32_t* perm);
+/* y = H x in the original boundary ordering (HMatrixGPUPackedFused.matvec, backend_fused.py:496-512) */
+SPX_API int spx_hmat_apply(spx_hmat h, const double* x, double* y, spx_stream_t s);
+SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
+/* low-rank factors U^T (k x m) and V (k x n) of far block `index` (as listed by spx_hmat_blocks), FP64 host */
+SPX_API int spx_hmat_far_factors(spx_hmat h, int64_t index, double* Ut, double* V);
+SPX_API int spx_hmat_memory(spx_hmat h, int64_t* far_bytes, int64_t* near_bytes, int64_t* total_bytes);
+SPX_API int spx_hmat_destroy(spx_hmat h);
+
+/* ------------------------------------------------------------------ demag field */
+typedef struct spx_demag_s* spx_demag;
+typedef struct {
+  int32_t backend;   /* 0 dense, 1 hmatrix (DemagFieldLindholmGPU boundary_backend, :319-345) */
+  int32_t precision; /* SPX_PREC_* */
+  double rtol_u1, rtol_u2, atol; /* ksp_rtol_u1/u2 (:216-226, :271-281), atol 1e-12 */
+  int32_t maxit_u1, maxit_u2;    /* 2000 / 12000 in the reference */
+  int32_t warm_start;            /* start each CG from the previous solution */
+  int32_t reserved;
+  spx_hmat_config hmat;
+} spx_demag_options;
+/* DemagFieldLindholmGPU.__init__ (gpu/fields/Demag_Lindholm_GPU.py:101-155) */
+SPX_API int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                     const spx_demag_options* opt, spx_demag* out);
+/* DemagFieldLindholmGPU.compute_vec (:643-670): H = -grad(u1+u2) lumped, AoS FP64 device */
+SPX_API int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s);
+/* potentials of the last apply (FP64 device, N each) */
+SPX_API int spx_demag_potentials(spx_demag d, double* u1, double* u2, spx_stream_t s);
+/* Energy_lumped_gpu (:706-724): E = -1/2 mu0 Ms sum V_i m.H / 1e27  (J) */
+SPX_API int spx_demag_energy(spx_demag d, const double* m, const double* H, double* E, spx_stream_t s);
+/* last_its_u1 / last_its_u2 and the relative residuals of the last apply */
+SPX_API int spx_demag_stats(spx_demag d, int64_t* its_u1, int64_t* its_u2, double* res_u1, double* res_u2);
+SPX_API int spx_demag_info(spx_demag d, int64_t* N, int64_t* Nb, int64_t* NI, int64_t* device_bytes);
+/* H-matrix of an hmatrix-backend demag (borrowed; valid while d lives) */
+SPX_API int spx_demag_hmat(spx_demag d, spx_hmat* h);
+SPX_API int spx_demag_destroy(spx_demag d);
+
+/* ------------------------------------------------------------------ LLG */
+typedef struct spx_llg_s* spx_llg;
+typedef struct {
+  double Ms, gamma, alpha, do_precess; /* LLG_GPU(mesh, Ms, gamma, alpha, do_precess), llg_module_GPU.py:1549 */
+  double Aex;                          /* add_exchange */
+  double Ku;                           /* add_anisotropy (uniform) */
+  const double* Ku_nodes;              /* [N] per-node Ku, or NULL */
+  const double* n_ani;                 /* [N][3] easy axes, or NULL */
+  double D_int;                        /* add_dmi_interfacial */
+  const double* n_int;                 /* [N][3] interface normal, or NULL */
+  const double* H0_nodes;              /* [N][3] static field (A/m), or NULL */
+  double H0_uniform[3];                /* set_uniform_field */
+  int32_t use_demag;
+  int32_t precision;                   /* used when d == NULL; otherwise the demag's precision */
+} spx_llg_params;
+/* EffectiveField.__init__ (llg_module_GPU.py:388-724); d may be NULL (no demag) */
+SPX_API int spx_llg_create(spx_demag d, const double* X, int64_t N, const int32_t* tets, int64_t E,
+                   const spx_llg_params* p, spx_llg* out);
+SPX_API int spx_llg_heff(spx_llg l, const double* m, double* H, spx_stream_t s);   /* compute_H_eff_vec  :972-1006 */
+SPX_API int spx_llg_hjac(spx_llg l, const double* m, double* H, spx_stream_t s);   /* compute_H_jac_vec  :1232-1257 */
+SPX_API int spx_llg_rhs(spx_llg l, const double* m, double* rhs, spx_stream_t s);  /* llg_rhs_vec        :1261-1285 */
+SPX_API int spx_llg_update_jac_state(spx_llg l, const double* m, spx_stream_t s); /* update_jac_state  :1287-1290 */
+SPX_API int spx_llg_jv(spx_llg l, const double* v, double* out, spx_stream_t s);   /* jac_vec_times_vec  :1293-1323 */
+/* JvContext.update_pc_full_fast_gpu (:1449-1507) and apply (:1519-1543) */
+SPX_API int spx_llg_pc_build(spx_llg l, double shift, int32_t include_stab, int32_t use_abs_kappa, spx_stream_t s);
+SPX_API int spx_llg_pc_apply(spx_llg l, const double* x, double* y, spx_stream_t s);
+/* integrator state (FP64 device AoS) and fixed-step classic RK4 (4 RHS evaluations per step);
+ * the reference steps with PETSc TS rk/5dp or BDF (llg_module_GPU.py:1724-1787, 2052-2181) */
+SPX_API int spx_llg_set_state(spx_llg l, const double* m, spx_stream_t s);
+SPX_API int spx_llg_get_state(spx_llg l, double* m, spx_stream_t s);
+SPX_API int spx_llg_step(spx_llg l, double dt, int64_t nsteps, spx_stream_t s);
+/* end-to-end call with HOST buffers: copy m_in to the device, run nsteps, copy the
+ * result back (pinned host memory gives full PCIe/C2C bandwidth) */
+SPX_API int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, int64_t nsteps);
+/* EffectiveField.set_uniform_field (llg_module_GPU.py:897-904): replace the static field by a uniform one */
+SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz);
+/* steps, RHS evaluations, LLG kernel launches */
+SPX_API int spx_llg_stats(spx_llg l, int64_t* steps, int64_t* rhs_evals, int64_t* launches);
+SPX_API int spx_llg_destroy(spx_llg l);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPX_H */
