@@ -1,0 +1,464 @@
+#!/usr/bin/env python
+"""LLG steps/s on the 0.48M-node film with the FEM/BEM (H-matrix) demag field.
+
+Workload (one "step" = one fixed-dt RK4 step = 4 effective-field/RHS evaluations):
+  film 1000 x 1000 x 5 nm, 400 x 400 x 2 cubes of 2.5 nm, 6 tets per cube
+  (1.92M tets, 482,403 nodes, 323,202 boundary nodes); Ms 8e5 A/m, A 1.3e-11 J/m,
+  alpha 0.02, uniform 25 mT at 170 deg in plane; m0 = x + N(0, 0.05^2) renormalised
+  (seeded); dt 50 fs.  Demag: u1 / u2 Poisson solves (rtol 1e-6) and the Lindholm
+  double layer as an H-matrix (ACA 1e-5, leaf 64, eta 2) built on the GPU in FP64.
+  Synthetic mesh and magnetisation (no dataset is involved).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: the film does not shard (one boundary operator couples every boundary
+node), so N GPUs run N independent replicas ("replicas only"); value = N x steps/s.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (str(ROOT), str(ROOT / "fenicsx-micromagnetics_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "LLG steps/s at 0.48M nodes, demag err<=1e-5 (film 400x400x2 @2.5nm, H-matrix ACA 1e-5, RK4 dt 50 fs)"
+MU0 = 4e-7 * math.pi
+
+
+def workload(nx, ny, nz, h, seed):
+    from spinfemx_b200.geometry import kuhn_box
+    X, T = kuhn_box(nx, ny, nz, h)
+    N = X.shape[0]
+    rng = np.random.default_rng(seed)
+    m = np.tile([1.0, 0.0, 0.0], (N, 1)) + rng.normal(0.0, 0.05, (N, 3))
+    m /= np.linalg.norm(m, axis=1)[:, None]
+    th = math.radians(170.0)
+    H0 = (0.025 / MU0) * np.array([math.cos(th), math.sin(th), 0.0])
+    return X, T, m.ravel(), H0
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(n_gpus):
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, ws, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def bytes_model(st, nnz, N, Nb, NI, nnzI, counters, H):
+    """Algorithmic bytes per launch for each kernel group (FP32 working precision)."""
+    wv, wm = 4, 4
+    # u1 / u2 refinement solves: per inner iteration one SELL SpMV + 7 vector passes
+    # (nnz (w_m + 4) + 4 (N+1) + 7 N w_v); per refinement step an FP64 residual SpMV.
+    def cg_bytes(c, n, z):
+        if c[2] == 0:
+            return 0.0
+        inner = c[0] * (z * (wm + 4) + 4 * (n + 1) + 7 * n * wv)
+        outer = c[1] * (z * (8 + 4) + 4 * (n + 1) + 3 * n * 8)
+        return (inner + outer) / c[2]
+    return {
+        "u1_solve": cg_bytes(counters[0], N, nnz),
+        "u2_solve": cg_bytes(counters[1], NI, nnzI),
+        # far factors + near tiles + x gather (Nb w_v) + scatter of phi and g (2 Nb w_v)
+        "boundary_apply": H["far_bytes"] + H["near_bytes"] + 4 * Nb * wv,
+        # Div: nnz (3 w_m + 4) + 3N w_v + N w_v
+        "div": nnz * (3 * wm + 4) + 4 * N * wv,
+        # fused stage: nnz (w_m exchange + 3 w_m G + 4 index) + m gather (3N) + phi (N)
+        #             + acc/mn/out (3 x 3N read/write)
+        "stage": nnz * (4 * wm + 4) + 4 * N * wv + 12 * N * wv,
+    }
+
+
+def run_ours(a):
+    import torch
+    import spinfemx_b200 as spx
+    from spinfemx_b200 import _lib
+
+    rank, ws, local = dist_init(a.gpus)
+    dev = torch.cuda.current_device()
+    X, T, m0, H0 = workload(a.nx, a.ny, a.nz, a.h, 2000 + rank)
+    N = X.shape[0]
+    t0 = time.time()
+    hef = spx.EffectiveField(
+        X, T, 8e5, Aex=1.3e-11, alpha=0.02, gamma=2.211e5, H0_static=H0, use_demag=True,
+        precision=a.precision,
+        demag_kwargs=dict(boundary_backend="hmatrix", hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
+                          ksp_rtol_u1=1e-6, ksp_rtol_u2=1e-6, warm_start=a.warm_start, precision=a.precision))
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    dm = hef.demag_field
+    Hst = dm.B_hmatrix_gpu.stats()
+    Hmem = dm.B_hmatrix_gpu.memory_report()
+    m = torch.as_tensor(m0, device="cuda")
+    hef.set_state(m)
+    # warm-up
+    hef.step(a.dt, a.warmup)
+    torch.cuda.synchronize()
+    c_before = counters(dm)
+    sampler = ClockSampler(dev) if rank == 0 else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    _lib.call("spx_demag_profile_begin", dm.handle)
+    st0 = hef.stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    hef.step(a.dt, a.steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms_cat = np.zeros(8)
+    nl_cat = np.zeros(8, np.int64)
+    ng_cat = np.zeros(8, np.int64)
+    _lib.call("spx_demag_profile_end", dm.handle, _lib.ptr(ms_cat), _lib.ptr(nl_cat), _lib.ptr(ng_cat))
+    barrier(ws)
+    clocks = sampler.stop() if sampler else None
+    st1 = hef.stats()
+    c_after = counters(dm)
+    ms_max = allmax(ms, ws)
+    sps = a.steps / (ms_max * 1e-3)
+    # demag accuracy of the final state against an FP64 evaluation (same GPU operator)
+    mfin = hef.get_state()
+    err = None
+    if rank == 0 and a.check_error:
+        err = demag_error(spx, X, T, mfin, dm, a)
+    # end-to-end through the host-buffer entry point (pinned), one step per call
+    e2e = None
+    if not a.no_e2e:
+        hin = torch.empty(3 * N, dtype=torch.float64).pin_memory()
+        hout = torch.empty(3 * N, dtype=torch.float64).pin_memory()
+        hin.copy_(mfin.cpu())
+        ke = max(1, min(a.steps, a.e2e_steps))
+        hef.run_host(hin, a.dt, 1, out=hout)  # warm
+        barrier(ws)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(ke):
+            hef.run_host(hin, a.dt, 1, out=hout)
+            hin, hout = hout, hin
+        torch.cuda.synchronize()
+        el = allmax(time.perf_counter() - t1, ws)
+        e2e = {"value": ws * ke / el, "unit": "steps/s", "h2d_bytes_per_step": 3 * N * 8,
+               "d2h_bytes_per_step": 3 * N * 8, "steps": ke}
+    if rank != 0:
+        finish(ws)
+        return
+    # roofline of the dominant kernel group
+    cats = ["div", "u1_solve", "boundary_apply", "u2_rhs", "u2_solve", "phi", "stage"]
+    dc = [c_after[0][k] - c_before[0][k] for k in range(3)], [c_after[1][k] - c_before[1][k] for k in range(3)]
+    nnz, nnzI = fem_nnz(spx, X, T, dm)
+    bm = bytes_model(Hst, nnz, N, dm.Nb, dm.NI, nnzI, dc, Hmem)
+    per = {}
+    for k, name in enumerate(cats):
+        if ng_cat[k] == 0:
+            continue
+        avg_ms = ms_cat[k] / ng_cat[k]
+        b = bm.get(name)
+        per[name] = {"ms_total": round(float(ms_cat[k]), 3), "executions": int(ng_cat[k]),
+                     "kernel_launches": int(nl_cat[k]),
+                     "avg_ms": round(float(avg_ms), 4), "share": round(float(ms_cat[k] / ms), 4)}
+        if b:
+            per[name]["algorithmic_bytes"] = float(b)
+            per[name]["achieved_GBps"] = round(b / (avg_ms * 1e-3) / 1e9, 1)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max((k for k in per if "achieved_GBps" in per[k]), key=lambda k: per[k]["ms_total"])
+    roof = {"bound": "hbm", "kernel": dom, "achieved": per[dom]["achieved_GBps"], "peak": peak,
+            "peak_source": peak_src, "unit": "GB/s", "frac": round(per[dom]["achieved_GBps"] / peak, 4),
+            "traffic": a.traffic.get(dom) if a.traffic else None}
+    launches = int(sum(int(x) for x in nl_cat[:7]))
+    line = {
+        "metric": METRIC, "value": round(ws * sps, 4), "unit": "steps/s", "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp32+bf16"}[a.precision],
+        "data": "synthetic (seeded Kuhn-box film and magnetisation)",
+        "config": {"workload": f"film {a.nx}x{a.ny}x{a.nz} cubes @{a.h}nm, N={N}, Nb={dm.Nb}, H-matrix ACA 1e-5 "
+                               f"leaf 64 eta 2, RK4 dt {a.dt:g}s, {a.precision}",
+                   "nodes": N, "boundary_nodes": dm.Nb, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (H-matrix factors %.1f GB per apply)" % (
+                       (Hmem["far_bytes"] + Hmem["near_bytes"]) / 1e9),
+                   "warm_start": bool(a.warm_start), "demag_rel_err_vs_fp64": err},
+        "e2e": e2e,
+        "roofline": roof,
+        "kernels": per,
+        "hmatrix": {"build_s": round(Hst["build_time_seconds"], 2), "n_far": Hst["n_far"], "n_near": Hst["n_near"],
+                    "avg_rank": round(Hst["average_far_rank"], 2), "max_rank": Hst["max_observed_rank"],
+                    "far_entries": Hst["far_entries"], "near_entries": Hst["near_entries"]},
+        "cg": {"u1_iters_per_solve": round(dc[0][0] / max(dc[0][2], 1), 1),
+               "u1_refinements_per_solve": round(dc[0][1] / max(dc[0][2], 1), 2),
+               "u2_iters_per_solve": round(dc[1][0] / max(dc[1][2], 1), 1)},
+        "setup_s": round(setup_s, 1),
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if a.cpu_baseline and ws == 1:
+        line["cpu_baseline"] = cpu_baseline(a, bounded=True)
+    print(json.dumps(line), flush=True)
+    finish(ws)
+
+
+def counters(dm):
+    from spinfemx_b200 import _lib
+    c1 = np.zeros(4, np.int64)
+    c2 = np.zeros(4, np.int64)
+    _lib.call("spx_demag_counters", dm.handle, _lib.ptr(c1), _lib.ptr(c2))
+    return c1.tolist(), c2.tolist()
+
+
+def fem_nnz(spx, X, T, dm):
+    f = spx.fem_assemble(X, T)
+    nnz = int(f["rowptr"][-1])
+    bd = np.zeros(X.shape[0], bool)
+    bd[spx.boundary_data(X, T)["bverts"]] = True
+    rows = np.repeat(np.arange(X.shape[0]), np.diff(f["rowptr"]))
+    nnzI = int(np.count_nonzero(~bd[rows] & ~bd[f["col"]]))
+    return nnz, nnzI
+
+
+def demag_error(spx, X, T, m, dm, a):
+    """Relative L2 error of the working-precision demag field against an FP64 solve
+    (FP64 H-matrix factors, rtol 1e-10) at the final state."""
+    import torch
+    if a.precision == "f64":
+        return None
+    ref = spx.DemagFieldLindholmGPU(X, T, 8e5, boundary_backend="hmatrix", hmatrix_epsilon=1e-5, precision="f64",
+                                    ksp_rtol_u1=1e-10, ksp_rtol_u2=1e-10, ksp_maxit_u1=50000, ksp_maxit_u2=50000,
+                                    ksp_atol=0.0)
+    Hr = torch.empty_like(m)
+    ref.compute_vec(m, Hr)
+    Hw = torch.empty_like(m)
+    dm.compute_vec(m, Hw)
+    e = float(torch.linalg.norm(Hw - Hr) / torch.linalg.norm(Hr))
+    del ref
+    torch.cuda.synchronize()
+    return e
+
+
+def finish(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------- CPU (oracle)
+class OracleCPU:
+    """The oracle's FP64 CPU pipeline on the same film (test infrastructure): u1/u2 by
+    sparse direct solves (factorised once), Div / G / exchange SpMVs, the LLG RHS and RK4.
+    The boundary double layer is not applied: no CPU H-matrix of Nb = 323k boundary nodes
+    can be built within the run (the reference's CPU builder needs hours), so the measured
+    CPU steps/s is an upper bound for the reference CPU path."""
+
+    def __init__(self, a, seed=2000):
+        import scipy.sparse.linalg as spla
+        from oracle import fem, lindholm, llg, mesh
+        X, T = mesh.kuhn_box(a.nx, a.ny, a.nz, a.h)
+        self.N = N = X.shape[0]
+        rng = np.random.default_rng(seed)
+        m = np.tile([1.0, 0.0, 0.0], (N, 1)) + rng.normal(0.0, 0.05, (N, 3))
+        m /= np.linalg.norm(m, axis=1)[:, None]
+        self.m = m.ravel()
+        th = math.radians(170.0)
+        self.H0 = np.tile((0.025 / MU0) * np.array([math.cos(th), math.sin(th), 0.0]), N)
+        tris, _ = lindholm.boundary_facets(X, T)
+        bv = np.unique(tris.ravel())
+        self.A = fem.stiffness(X, T).tocsr()
+        self.Div = fem.divergence(X, T, 8e5).tocsr()
+        self.G = fem.gradient_op(X, T).tocsr()
+        self.vol = fem.lumped_volume(X, T)
+        self.K = fem.exchange_matrix(X, T, 1.3e-11, 8e5, self.vol).tocsr()
+        inter = np.ones(N, bool)
+        inter[bv] = False
+        self.I = np.nonzero(inter)[0]
+        self.lu1 = spla.splu(self.A[1:, 1:].tocsc())
+        self.lu2 = spla.splu(self.A[self.I][:, self.I].tocsc())
+        self.AIB = self.A[self.I][:, bv].tocsr()
+        self.bv = bv
+        self.pref, self.stab = llg.constants(8e5, 2.211e5, 0.02)
+        self.llg = llg
+
+    def rhs(self, m):
+        b = self.Div @ m
+        b -= b.mean()
+        u = np.zeros(self.N)
+        u[1:] = self.lu1.solve(b[1:])
+        u -= u.mean()
+        g = u[self.bv]  # boundary operator omitted (see class docstring)
+        u2 = np.zeros(self.N)
+        u2[self.bv] = g
+        u2[self.I] = self.lu2.solve(-(self.AIB @ g))
+        H = (self.G @ (u + u2)).reshape(-1, 3) / self.vol[:, None]
+        H = H.ravel() + self.K @ m + self.H0
+        return self.llg.rhs(m, H, self.pref, 0.02, 1.0, self.stab)
+
+    def step(self, dt):
+        self.m = self.llg.rk4_step(self.rhs, self.m, dt)
+
+
+def cpu_baseline(a, bounded=True):
+    o = OracleCPU(a)
+    o.step(a.dt)  # warm
+    t = time.perf_counter()
+    n = 0
+    while True:
+        o.step(a.dt)
+        n += 1
+        if time.perf_counter() - t > a.cpu_seconds or not bounded:
+            break
+    el = time.perf_counter() - t
+    return {"value": round(n / el, 5), "unit": "steps/s", "cores": 1, "kind": "port",
+            "sample": f"{n} RK4 step(s) of the oracle FP64 CPU pipeline on the full film "
+                      f"(direct u1/u2 solves, boundary double layer omitted: CPU upper bound), "
+                      f"{el:.1f} s"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    o = OracleCPU(a)
+    for _ in range(a.warmup):
+        o.step(a.dt)
+    t = time.perf_counter()
+    for _ in range(a.steps):
+        o.step(a.dt)
+    el = time.perf_counter() - t
+    v = a.steps / el
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "steps/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1e3 * el / a.steps, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic (seeded Kuhn-box film and magnetisation)",
+            "config": {"workload": f"film {a.nx}x{a.ny}x{a.nz} cubes @{a.h}nm, oracle FP64 CPU pipeline, "
+                                   f"RK4 dt {a.dt:g}s (boundary double layer omitted)", "parallelism": "cpu"},
+            "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": 1, "kind": "port",
+                             "sample": f"{a.steps} RK4 steps, oracle FP64 CPU pipeline (direct Poisson solves; the "
+                                       f"reference CPU H-matrix builder cannot finish at Nb=323k in the run, so "
+                                       f"the boundary apply is omitted)"},
+            "e2e": {"value": round(v, 5), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64", "mixed"])
+    ap.add_argument("--nx", type=int, default=400)
+    ap.add_argument("--ny", type=int, default=400)
+    ap.add_argument("--nz", type=int, default=2)
+    ap.add_argument("--h", type=float, default=2.5)
+    ap.add_argument("--dt", type=float, default=5e-14)
+    ap.add_argument("--warm-start", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--check-error", type=int, default=1)
+    ap.add_argument("--cpu-baseline", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--traffic", type=json.loads, default=None,
+                    help='per-group DRAM bytes per launch from an ncu capture, e.g. {"u1_solve": 1.2e9}')
+    a = ap.parse_args()
+    if a.warmup < 0 or a.steps < 1:
+        ap.error("steps >= 1 and warmup >= 0")
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -511,6 +511,38 @@ int spx_demag_hmat(spx_demag d, spx_hmat* h) {
   API_END
 }
 
+int spx_demag_profile_begin(spx_demag d) {
+  API_BEGIN
+  REQUIRE(d);
+  if (d->d64) d->d64->prof.begin();
+  else d->d32->prof.begin();
+  API_END
+}
+
+int spx_demag_profile_end(spx_demag d, double* ms8, int64_t* l8, int64_t* g8) {
+  API_BEGIN
+  REQUIRE(d); REQUIRE(ms8); REQUIRE(l8); REQUIRE(g8);
+  if (d->d64) d->d64->prof.end(ms8, l8, g8);
+  else d->d32->prof.end(ms8, l8, g8);
+  API_END
+}
+
+int spx_demag_counters(spx_demag d, int64_t* c1, int64_t* c2) {
+  API_BEGIN
+  REQUIRE(d);
+  unsigned long long a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
+  auto rd = [](DevBuf<unsigned long long>& src, unsigned long long* dst) {
+    if (src.n) SPX_CUDA(cudaMemcpy(dst, src.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  };
+  if (d->d64) { rd(d->d64->cg1.iters_acc, a); rd(d->d64->cg2.iters_acc, b); }
+  else { rd(d->d32->cg1.iters_acc, a); rd(d->d32->cg2.iters_acc, b); }
+  for (int k = 0; k < 4; ++k) {
+    if (c1) c1[k] = static_cast<int64_t>(a[k]);
+    if (c2) c2[k] = static_cast<int64_t>(b[k]);
+  }
+  API_END
+}
+
 int spx_demag_destroy(spx_demag d) {
   API_BEGIN
   delete d;

@@ -143,6 +143,7 @@ struct CgParams {
   int* err;
   int* iters;
   double* resid;
+  unsigned long long* iters_acc;  // [0] inner iterations, [1] outer steps, [2] solves (accumulated)
   double rtol, atol;
   int maxit, warm, project;
 };
@@ -306,9 +307,215 @@ __global__ void __launch_bounds__(256) k_cg(CgParams<T> P) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *P.iters = it;
     *P.resid = bb > 0.0 ? sqrt(rho / bb) : 0.0;
+    atomicAdd(P.iters_acc, (unsigned long long)it);
+    atomicAdd(P.iters_acc + 1, 1ull);
+    atomicAdd(P.iters_acc + 2, 1ull);
   }
 #undef ROWS_BEGIN
 #undef ROWS_END
+}
+
+// ------------------------------------------------------------------ mixed-precision IR solve
+// FP32 systems: FP64 outer iterative refinement (true residual with FP64 values, FP64
+// solution kept between calls for warm starts) around an FP32 inner single-reduction
+// (Chronopoulos-Gear) CG, all inside one cooperative launch.  Per inner iteration two
+// grid barriers; per outer iteration three.
+struct CgIrParams {
+  int64_t n, nslices;
+  const int64_t* sp;
+  const int32_t* col;
+  const float* v32;
+  const double* v64;
+  const double* sdinv;
+  const double* diag;
+  const float* b;
+  float* x;
+  double *bh, *y;
+  float *r, *p, *q, *s, *d;
+  double* red;  // [0] sum b, [1] ||b||^2, [2] sum x, [4..5] outer rho, [8..13] inner (gamma, delta) x 3
+  unsigned int* bar;
+  int* err;
+  int* iters;
+  double* resid;
+  unsigned long long* iters_acc;
+  double rtol, atol, inner_rtol;
+  int maxit, max_outer, inner_maxit, warm, project;
+};
+
+__global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
+  __shared__ double sh[32];
+  const unsigned nb = gridDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  unsigned int* cnt = P.bar;
+  unsigned int* gen = P.bar + 1;
+  const int64_t n = P.n;
+#define IR_ROWS_BEGIN                                               \
+  for (int64_t sl = gw; sl < P.nslices; sl += nw) {                 \
+    const int64_t row = sl * 32 + lane;                             \
+    const int64_t base = P.sp[sl];                                  \
+    const int width = static_cast<int>((P.sp[sl + 1] - base) >> 5); \
+    (void)base; (void)width;                                        \
+    if (row < n) {
+#define IR_ROWS_END \
+  }                 \
+  }
+  if (P.project) {
+    double part = 0.0;
+    IR_ROWS_BEGIN part += static_cast<double>(P.b[row]);
+    IR_ROWS_END
+    part = block_sum(part, sh);
+    if (threadIdx.x == 0) atomicAdd(P.red + 0, part);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
+  const double meanb = P.project ? P.red[0] / static_cast<double>(n) : 0.0;
+  {
+    double bb = 0.0;
+    IR_ROWS_BEGIN
+      const double bv = static_cast<double>(P.b[row]) - meanb;
+      P.bh[row] = bv * P.sdinv[row];
+      if (!P.warm) P.y[row] = 0.0;
+      bb += bv * bv;
+    IR_ROWS_END
+    bb = block_sum(bb, sh);
+    if (threadIdx.x == 0) atomicAdd(P.red + 1, bb);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
+  const double bb = P.red[1];
+  const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
+  int total = 0;
+  double rho = 0.0;
+  int outers = 0;
+  for (int outer = 0; outer < P.max_outer; ++outer) {
+    ++outers;
+    const int so = 4 + (outer & 1);
+    // true residual in FP64; inner start r = p = r64 (float), d = 0
+    {
+      double rh = 0.0, g = 0.0;
+      if (blockIdx.x == 0 && threadIdx.x == 0) P.red[4 + ((outer + 1) & 1)] = 0.0;
+      IR_ROWS_BEGIN
+        double acc = 0.0;
+        for (int k = 0; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += P.v64[idx] * P.y[P.col[idx]];
+        }
+        const double r64 = P.bh[row] - acc;
+        rh += P.diag[row] * r64 * r64;
+        const float rf = static_cast<float>(r64);
+        P.r[row] = rf;
+        P.d[row] = 0.0f;
+        g += static_cast<double>(rf) * rf;
+      IR_ROWS_END
+      rh = block_sum(rh, sh);
+      if (threadIdx.x == 0) atomicAdd(P.red + so, rh);
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    }
+    rho = P.red[so];
+    if (rho <= tol2 || total >= P.maxit) break;
+    // s = A r, slot 0 <- (r,r), (r,s)
+    {
+      double g = 0.0, dl = 0.0;
+      IR_ROWS_BEGIN
+        float acc = 0.0f;
+        for (int k = 0; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += P.v32[idx] * P.r[P.col[idx]];
+        }
+        P.s[row] = acc;
+        const double rv = P.r[row];
+        g += rv * rv;
+        dl += rv * static_cast<double>(acc);
+      IR_ROWS_END
+      g = block_sum(g, sh);
+      dl = block_sum(dl, sh);
+      if (threadIdx.x == 0) {
+        atomicAdd(P.red + 8, g);
+        atomicAdd(P.red + 9, dl);
+      }
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    }
+    const double g0 = P.red[8];
+    const double itol2 = P.inner_rtol * P.inner_rtol * g0;
+    double gprev = 1.0, aprev = 1.0;
+    for (int it = 0;; ++it) {
+      const int sl = it % 3;
+      const double gm = P.red[8 + 2 * sl], dl = P.red[9 + 2 * sl];
+      if (gm <= itol2 || it >= P.inner_maxit || total >= P.maxit || !(gm > 0.0) || !(dl > 0.0)) break;
+      if (blockIdx.x == 0 && threadIdx.x < 2) P.red[8 + 2 * ((it + 2) % 3) + threadIdx.x] = 0.0;
+      double beta, alpha;
+      if (it == 0) {
+        beta = 0.0;
+        alpha = gm / dl;
+      } else {
+        beta = gm / gprev;
+        alpha = gm / (dl - beta * gm / aprev);
+      }
+      const float a = static_cast<float>(alpha), bt = static_cast<float>(beta);
+      IR_ROWS_BEGIN
+        const float rv = P.r[row], sv = P.s[row];
+        const float pv = (it == 0) ? rv : rv + bt * P.p[row];
+        const float qv = (it == 0) ? sv : sv + bt * P.q[row];
+        P.p[row] = pv;
+        P.q[row] = qv;
+        P.d[row] += a * pv;
+        P.r[row] = rv - a * qv;
+      IR_ROWS_END
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      double g2 = 0.0, d2 = 0.0;
+      IR_ROWS_BEGIN
+        float acc = 0.0f;
+        for (int k = 0; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += P.v32[idx] * P.r[P.col[idx]];
+        }
+        P.s[row] = acc;
+        const double rv = P.r[row];
+        g2 += rv * rv;
+        d2 += rv * static_cast<double>(acc);
+      IR_ROWS_END
+      g2 = block_sum(g2, sh);
+      d2 = block_sum(d2, sh);
+      if (threadIdx.x == 0) {
+        const int ns = (it + 1) % 3;
+        atomicAdd(P.red + 8 + 2 * ns, g2);
+        atomicAdd(P.red + 9 + 2 * ns, d2);
+      }
+      gprev = gm;
+      aprev = alpha;
+      ++total;
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    }
+    // y += d ; reset the inner slots for the next refinement step
+    if (blockIdx.x == 0 && threadIdx.x < 6) P.red[8 + threadIdx.x] = 0.0;
+    IR_ROWS_BEGIN P.y[row] += static_cast<double>(P.d[row]);
+    IR_ROWS_END
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
+  double sx = 0.0;
+  IR_ROWS_BEGIN sx += P.y[row] * P.sdinv[row];
+  IR_ROWS_END
+  double mx = 0.0;
+  if (P.project) {
+    sx = block_sum(sx, sh);
+    if (threadIdx.x == 0) atomicAdd(P.red + 2, sx);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    mx = P.red[2] / static_cast<double>(n);
+  }
+  IR_ROWS_BEGIN
+    const double xv = P.y[row] * P.sdinv[row] - mx;
+    P.x[row] = static_cast<float>(xv);
+    P.y[row] = xv / P.sdinv[row];
+  IR_ROWS_END
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *P.iters = total;
+    *P.resid = bb > 0.0 ? sqrt(rho / bb) : 0.0;
+    atomicAdd(P.iters_acc, (unsigned long long)total);
+    atomicAdd(P.iters_acc + 1, (unsigned long long)outers);
+    atomicAdd(P.iters_acc + 2, 1ull);
+  }
+#undef IR_ROWS_BEGIN
+#undef IR_ROWS_END
 }
 
 template <class T>
@@ -337,7 +544,29 @@ void CgSystem<T>::setup(const HostSell& s, const std::vector<double>& vals_sell,
   sdinv.upload(sd);
   diag.upload(dd);
   work.alloc(7 * static_cast<size_t>(n));
+  if (sizeof(T) == sizeof(float)) {
+    std::vector<double> v64(v.size()), sd64(n), d64(d.begin(), d.begin() + n);
+    for (int64_t i = 0; i < n; ++i) sd64[i] = 1.0 / std::sqrt(d[i]);
+    for (int64_t sl = 0; sl < s.nslices; ++sl) {
+      const int64_t w = (s.slice_ptr[sl + 1] - s.slice_ptr[sl]) / SELL_C;
+      for (int64_t k = 0; k < w; ++k)
+        for (int l = 0; l < SELL_C; ++l) {
+          const int64_t idx = s.slice_ptr[sl] + k * SELL_C + l;
+          const int64_t row = sl * SELL_C + l;
+          v64[idx] = (row < n) ? vals_sell[idx] / std::sqrt(d[row] * d[s.col[idx]]) : 0.0;
+        }
+    }
+    vals64.upload(v64);
+    sdinv64.upload(sd64);
+    diag64.upload(d64);
+    y64.alloc(n);
+    y64.zero();
+    bh64.alloc(n);
+  }
   red.alloc(16);
+  red.zero();
+  iters_acc.alloc(4);
+  iters_acc.zero();
   bar.alloc(2);
   err.alloc(1);
   iters.alloc(1);
@@ -346,6 +575,11 @@ void CgSystem<T>::setup(const HostSell& s, const std::vector<double>& vals_sell,
   SPX_CUDA(cudaGetDevice(&dev));
   int per_sm = 0;
   SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg<T>, 256, 0));
+  if (sizeof(T) == sizeof(float)) {
+    int per_sm_ir = 0;
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ir, k_cg_ir, 256, 0));
+    per_sm = std::min(per_sm, per_sm_ir);
+  }
   SPX_CHECK(per_sm > 0, "CG kernel cannot be resident");
   const int64_t want = (s.nslices * 32 + 255) / 256;
   grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * num_sms(dev))));
@@ -371,6 +605,7 @@ CgStats CgSystem<T>::solve(const T* b, T* x, double rtol, double atol, int maxit
   p.err = err.p;
   p.iters = iters.p;
   p.resid = resid.p;
+  p.iters_acc = iters_acc.p;
   p.rtol = rtol;
   p.atol = atol;
   p.maxit = maxit;
@@ -379,8 +614,25 @@ CgStats CgSystem<T>::solve(const T* b, T* x, double rtol, double atol, int maxit
   SPX_CUDA(cudaMemsetAsync(red.p, 0, red.bytes(), st));
   SPX_CUDA(cudaMemsetAsync(bar.p, 0, bar.bytes(), st));
   SPX_CUDA(cudaMemsetAsync(err.p, 0, err.bytes(), st));
-  void* args[] = {&p};
-  SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg<T>), dim3(grid), dim3(256), args, 0, st));
+  if (sizeof(T) == sizeof(float)) {
+    CgIrParams q;
+    q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
+    q.v32 = reinterpret_cast<const float*>(vals.p); q.v64 = vals64.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
+    q.b = reinterpret_cast<const float*>(b); q.x = reinterpret_cast<float*>(x);
+    q.bh = bh64.p; q.y = y64.p;
+    float* Wf = reinterpret_cast<float*>(work.p);
+    q.r = Wf; q.p = Wf + n; q.q = Wf + 2 * n; q.s = Wf + 3 * n; q.d = Wf + 4 * n;
+    q.red = red.p; q.bar = bar.p; q.err = err.p; q.iters = iters.p; q.resid = resid.p;
+    q.iters_acc = iters_acc.p;
+    q.rtol = rtol; q.atol = atol; q.inner_rtol = inner_rtol;
+    q.maxit = maxit; q.max_outer = max_outer; q.inner_maxit = maxit; q.warm = warm ? 1 : 0;
+    q.project = project ? 1 : 0;
+    void* a2[] = {&q};
+    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_ir), dim3(grid), dim3(256), a2, 0, st));
+  } else {
+    void* args[] = {&p};
+    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg<T>), dim3(grid), dim3(256), args, 0, st));
+  }
   CgStats out;
   if (sync_stats) {
     int h_err = 0, h_it = 0;
@@ -493,28 +745,47 @@ template <class T>
 void DemagCtx<T>::potential(const T* m, cudaStream_t s, bool sync_stats) {
   const int threads = 256;
   const unsigned gsl = grid_for(P.nslices * 32, threads);
-  SPX_CUDA(cudaMemsetAsync(sum.p, 0, sizeof(double), s));
+  prof.mark(PC_DIV, s);
   k_div<T><<<gsl, threads, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Div.p, P.len, m, b.p, nullptr);
   SPX_LAUNCH_CHECK();
+  prof.mark(PC_DIV, s);
+  prof.launches[PC_DIV] += 1;
+  prof.mark(PC_CG1, s);
   last1 = cg1.solve(b.p, u1.p, opt.rtol_u1, opt.atol, opt.maxit_u1, opt.warm_start != 0, true, s, sync_stats);
+  prof.mark(PC_CG1, s);
+  prof.launches[PC_CG1] += 1;
+  prof.mark(PC_BND, s);
   if (opt.backend == 0) {
     k_gather_idx<T><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, bverts.p, u1.p, xb.p);
     SPX_LAUNCH_CHECK();
     k_dense_gemv<T><<<grid_for(Nb * 32, 256), 256, 0, s>>>(Nb, Bdense.p, xb.p, bverts.p, u1.p, phi.p, gB.p);
     SPX_LAUNCH_CHECK();
+    prof.launches[PC_BND] += 2;
   } else {
     H.apply_gather<T>(u1.p, bverts.p, phi.p, u1.p, gB.p, s);
+    prof.launches[PC_BND] += H.n_far > 0 ? 3 : 2;
   }
+  prof.mark(PC_BND, s);
   if (NI > 0) {
+    prof.mark(PC_U2RHS, s);
     k_u2rhs<T><<<grid_for(PIB.nslices * 32, threads), threads, 0, s>>>(NI, PIB.nslices, PIB.slice_ptr.p,
                                                                          PIB.col.p, AIB.p, gB.p, bI.p);
     SPX_LAUNCH_CHECK();
+    prof.mark(PC_U2RHS, s);
+    prof.launches[PC_U2RHS] += 1;
     // ||b|| of the reference's full u2 system includes the boundary rows (b[bnd] = g);
     // the interior test is slightly stricter, which only tightens the solve.
+    prof.mark(PC_CG2, s);
     last2 = cg2.solve(bI.p, xI.p, opt.rtol_u2, opt.atol, opt.maxit_u2, opt.warm_start != 0, false, s, sync_stats);
+    prof.mark(PC_CG2, s);
+    prof.launches[PC_CG2] += 1;
+    prof.mark(PC_PHI, s);
     k_phi_interior<T><<<grid_for(NI, 256), 256, 0, s>>>(NI, interior.p, u1.p, xI.p, phi.p);
     SPX_LAUNCH_CHECK();
+    prof.mark(PC_PHI, s);
+    prof.launches[PC_PHI] += 1;
   }
+  launches += 4 + (opt.backend == 0 ? 2 : (H.n_far > 0 ? 3 : 2)) + (NI > 0 ? 3 : 0) - 1;
   ++applies;
 }
 

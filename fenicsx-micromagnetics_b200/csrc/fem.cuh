@@ -26,11 +26,60 @@ struct CgSystem {
   DevBuf<int> err;
   DevBuf<int> iters;
   DevBuf<double> resid;
+  DevBuf<unsigned long long> iters_acc;
+  // FP32 systems: FP64 values and state for the iterative-refinement solve
+  DevBuf<double> vals64, sdinv64, diag64, y64, bh64;
+  double inner_rtol = 1e-3;
+  int max_outer = 8;
   int grid = 0;
   void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
   // solve A x = b; x holds the initial guess if warm; project: remove the constant null space
   CgStats solve(const T* b, T* x, double rtol, double atol, int maxit, bool warm, bool project,
                 cudaStream_t st, bool sync_stats = true);
+};
+
+// Per-category CUDA-event timing of the demag/LLG pipeline (enabled on demand; events
+// are recorded on the launching stream around each kernel group).
+enum ProfCat : int { PC_DIV = 0, PC_CG1 = 1, PC_BND = 2, PC_U2RHS = 3, PC_CG2 = 4, PC_PHI = 5, PC_STAGE = 6, PC_N = 8 };
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  std::vector<int> cat;
+  size_t used = 0;
+  int64_t launches[PC_N] = {};
+  int64_t groups[PC_N] = {};
+  void mark(int c, cudaStream_t s) {  // call before and after a group: pairs (start, stop)
+    if (!on) return;
+    if ((used & 1) == 0) groups[c]++;
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      SPX_CUDA(cudaEventCreate(&e));
+      pool.push_back(e);
+      cat.push_back(c);
+    }
+    cat[used] = c;
+    SPX_CUDA(cudaEventRecord(pool[used++], s));
+  }
+  void begin() {
+    on = true;
+    used = 0;
+    for (auto& l : launches) l = 0;
+    for (auto& g : groups) g = 0;
+  }
+  void end(double* ms, int64_t* nl, int64_t* ng) {
+    for (int c = 0; c < PC_N; ++c) { ms[c] = 0.0; nl[c] = launches[c]; ng[c] = groups[c]; }
+    if (used) SPX_CUDA(cudaEventSynchronize(pool[used - 1]));
+    for (size_t k = 0; k + 1 < used; k += 2) {
+      float t = 0.f;
+      SPX_CUDA(cudaEventElapsedTime(&t, pool[k], pool[k + 1]));
+      ms[cat[k]] += t;
+    }
+    on = false;
+    used = 0;
+  }
+  ~Profiler() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
 };
 
 struct DemagOptions {
@@ -67,6 +116,8 @@ struct DemagCtx {
   DevBuf<double> sum;
   CgStats last1, last2;
   int64_t applies = 0;
+  Profiler prof;
+  int64_t launches = 0;
   void create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms, const DemagOptions& o,
               cudaStream_t s);
   // potential phi = u1 + u2 for magnetisation m (AoS, T)

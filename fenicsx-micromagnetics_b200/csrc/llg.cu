@@ -454,7 +454,13 @@ void LLGCtx<T>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
       a.c_next = cnext[st];
       a.w_acc = wacc[st];
       a.dt6 = h / T(6);
+      Profiler* pf = use_demag ? &demag->prof : nullptr;
+      if (pf) pf->mark(PC_STAGE, s);
       launch_stage(a, use_demag, s);
+      if (pf) {
+        pf->mark(PC_STAGE, s);
+        pf->launches[PC_STAGE] += 1;
+      }
       ++rhs_evals;
     }
     ++steps;

@@ -55,7 +55,7 @@ SIGNATURES = {
     "spx_dense_b_assemble": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_dense_b_apply": (C.c_int, [c_vp, c_i64, c_vp, c_vp, c_vp]),
     "spx_hmat_build": (C.c_int, [c_vp, C.POINTER(HmatConfig), C.POINTER(c_vp)]),
-    "spx_hmat_stats": (C.c_int, [c_vp, P_i64, P_dbl]),
+    "spx_hmat_stats": (C.c_int, [c_vp, c_vp, P_dbl]),
     "spx_hmat_num_blocks": (C.c_int, [c_vp, P_i64]),
     "spx_hmat_blocks": (C.c_int, [c_vp, c_vp, c_i64]),
     "spx_hmat_perm": (C.c_int, [c_vp, c_vp]),
@@ -72,6 +72,9 @@ SIGNATURES = {
     "spx_demag_info": (C.c_int, [c_vp, P_i64, P_i64, P_i64, P_i64]),
     "spx_demag_hmat": (C.c_int, [c_vp, C.POINTER(c_vp)]),
     "spx_demag_destroy": (C.c_int, [c_vp]),
+    "spx_demag_profile_begin": (C.c_int, [c_vp]),
+    "spx_demag_profile_end": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_demag_counters": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_create": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, C.POINTER(LLGParams), C.POINTER(c_vp)]),
     "spx_llg_heff": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_hjac": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),

@@ -133,10 +133,14 @@ class DemagFieldLindholmGPU:
             print(f"[Demag Lindholm b200] {k}: {v}", flush=True)
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            try:
-                _lib.lib().spx_demag_destroy(h)
-            except Exception:
-                pass
-            self._h = C.c_void_p()
+        try:
+            h = getattr(self, "_h", None)
+            if h is not None and h.value:
+                try:
+                    _lib.lib().spx_demag_destroy(h)
+                except Exception:
+                    pass
+                self._h = C.c_void_p()
+
+        except Exception:
+            pass

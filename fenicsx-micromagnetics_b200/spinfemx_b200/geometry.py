@@ -124,13 +124,16 @@ class BoundaryGeometry:
         return B
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            try:
-                _lib.lib().spx_boundary_destroy(h)
-            except Exception:
-                pass
-            self._h = C.c_void_p()
+        try:
+            h = getattr(self, "_h", None)
+            if h is not None and h.value:
+                try:
+                    _lib.lib().spx_boundary_destroy(h)
+                except Exception:
+                    pass
+                self._h = C.c_void_p()
+        except Exception:
+            pass
 
 
 def dense_b_apply(B, x, out=None):

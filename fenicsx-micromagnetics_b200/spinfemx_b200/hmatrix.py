@@ -216,13 +216,16 @@ class HMatrixGPUPackedFused:
             print(f"{prefix} {k:28s}: {v}", flush=True)
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if getattr(self, "_owned", False) and h is not None and h.value:
-            try:
-                _lib.lib().spx_hmat_destroy(h)
-            except Exception:
-                pass
-            self._h = C.c_void_p()
+        try:
+            h = getattr(self, "_h", None)
+            if getattr(self, "_owned", False) and h is not None and h.value:
+                try:
+                    _lib.lib().spx_hmat_destroy(h)
+                except Exception:
+                    pass
+                self._h = C.c_void_p()
+        except Exception:
+            pass
 
 
 def build_or_load_hmatrix(cache_path, X, tets, config: HMatrixBuildConfig | None = None, *,

@@ -193,13 +193,16 @@ class EffectiveField:
         return {"steps": s.value, "rhs_evals": r.value, "launches": l.value}
 
     def __del__(self):
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            try:
-                _lib.lib().spx_llg_destroy(h)
-            except Exception:
-                pass
-            self._h = C.c_void_p()
+        try:
+            h = getattr(self, "_h", None)
+            if h is not None and h.value:
+                try:
+                    _lib.lib().spx_llg_destroy(h)
+                except Exception:
+                    pass
+                self._h = C.c_void_p()
+        except Exception:
+            pass
 
 
 class JvContext:

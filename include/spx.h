@@ -183,6 +183,14 @@ SPX_API int spx_llg_step(spx_llg l, double dt, int64_t nsteps, spx_stream_t s);
 SPX_API int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, int64_t nsteps);
 /* EffectiveField.set_uniform_field (llg_module_GPU.py:897-904): replace the static field by a uniform one */
 SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz);
+/* CUDA-event timing of the pipeline by kernel group, recorded on the launching stream
+ * between begin and end.  ms[8] / kernel launches[8] / group executions[8] per group: 0 Div SpMV, 1 u1 solve,
+ * 2 boundary operator (gather + far + rows, or dense GEMV), 3 u2 right-hand side,
+ * 4 u2 solve, 5 potential assembly, 6 fused field/RHS/RK stage, 7 unused.
+ * counters[4]: CG inner iterations, refinement steps, solves (since create), 0. */
+SPX_API int spx_demag_profile_begin(spx_demag d);
+SPX_API int spx_demag_profile_end(spx_demag d, double* ms8, int64_t* launches8, int64_t* groups8);
+SPX_API int spx_demag_counters(spx_demag d, int64_t* u1_counters4, int64_t* u2_counters4);
 /* steps, RHS evaluations, LLG kernel launches */
 SPX_API int spx_llg_stats(spx_llg l, int64_t* steps, int64_t* rhs_evals, int64_t* launches);
 SPX_API int spx_llg_destroy(spx_llg l);
