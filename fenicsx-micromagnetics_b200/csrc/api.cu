@@ -336,6 +336,15 @@ int spx_hmat_apply(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   API_END
 }
 
+int spx_hmat_apply_noalloc(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(hm);
+  REQUIRE(x);
+  REQUIRE(y);
+  hmat_apply_noalloc(hm->h, x, y, S(s));
+  API_END
+}
+
 int spx_hmat_repack(spx_hmat hm, int32_t precision) {
   API_BEGIN
   REQUIRE(hm);

@@ -13,6 +13,8 @@
 //               scatter y to dst[g(perm[i])].
 // Near tiles may use compensated (Kahan) accumulation in the mixed-precision form.
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "hmat.cuh"
 
@@ -303,6 +305,74 @@ int64_t HMatrix::device_bytes() const {
                               far_zoff.bytes() + far_meta.bytes() + near_off.bytes() + near_meta.bytes() +
                               leaf_start.bytes() + item_ptr.bytes() + items.bytes() + z.bytes() +
                               xperm.bytes() + diag_perm.bytes() + perm.bytes());
+}
+
+}  // namespace spx
+
+// ------------------------------------------------------------------ apply without allocation
+// spx_hmat_apply_noalloc runs the same three kernels as spx_hmat_apply, but its scratch
+// (x in permuted order, then the far-field z vectors) lives in this fixed device array
+// instead of buffers allocated on first use.  Every device that loads the library holds
+// the array until the process exits.  In host code the symbol is only a stand-in: the
+// device address comes from cudaGetSymbolAddress, looked up once per device.
+namespace spx {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+void* noalloc_scratch_address() {
+  static std::mutex mu;
+  static std::vector<void*> addr;
+  int dev = 0;
+  SPX_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (static_cast<size_t>(dev) >= addr.size()) addr.resize(dev + 1, nullptr);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    SPX_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    addr[dev] = p;
+  }
+  return addr[dev];
+}
+
+template <class TF, class TN, class TA, class TX>
+void apply_noalloc_impl(HMatrix& H, const double* x, double* y, cudaStream_t s) {
+  const int64_t Nb = H.Nb;
+  const size_t xbytes = ((static_cast<size_t>(Nb) * sizeof(TX) + 255) / 256) * 256;
+  const size_t zbytes = static_cast<size_t>(std::max<int64_t>(H.zlen, 1)) * sizeof(TA);
+  if (xbytes + zbytes > kNoAllocScratchBytes)
+    throw Error(ERR_INVALID, "H-matrix too large for the 32 MiB static scratch of spx_hmat_apply_noalloc "
+                             "(needs " + std::to_string(xbytes + zbytes) + " bytes); use spx_hmat_apply");
+  unsigned char* base = static_cast<unsigned char*>(noalloc_scratch_address());
+  TX* xp = reinterpret_cast<TX*>(base);
+  TA* z = reinterpret_cast<TA*>(base + xbytes);
+  k_hgather<double, TX><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, x, nullptr, H.perm.p, xp);
+  SPX_LAUNCH_CHECK();
+  if (H.n_far > 0) {
+    k_far_z<TF, TA, TX><<<static_cast<unsigned>(H.n_far), 128, 0, s>>>(
+        H.far_meta.p, H.far_voff.p, H.far_zoff.p, reinterpret_cast<const TF*>(H.far_f.p), xp, z);
+    SPX_LAUNCH_CHECK();
+  }
+  const size_t smem = 2 * ROWS_GROUPS * static_cast<size_t>(std::max(H.cfg.leaf_size, 1)) * sizeof(TA);
+  k_rows<TF, TN, TA, TX, double><<<static_cast<unsigned>(H.nleaf), ROWS_GROUPS * ROWS_GSIZE, smem, s>>>(
+      H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
+      reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
+      reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, nullptr, y, nullptr, nullptr,
+      H.prec == Prec::MIXED ? 1 : 0);
+  SPX_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s) {
+  SPX_CHECK(H.packed, "H-matrix is not packed");
+  switch (H.prec) {
+    case Prec::F64: apply_noalloc_impl<double, double, double, double>(H, x, y, s); break;
+    case Prec::F32: apply_noalloc_impl<float, float, float, float>(H, x, y, s); break;
+    case Prec::MIXED: apply_noalloc_impl<__nv_bfloat16, float, float, float>(H, x, y, s); break;
+  }
 }
 
 }  // namespace spx

@@ -95,4 +95,8 @@ struct HMatrix {
   int64_t device_bytes() const;
 };
 
+// y = H x (original boundary ordering, FP64) using the library's static device scratch
+// instead of allocated buffers (see spx_hmat_apply_noalloc in include/spx.h).
+void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s);
+
 }  // namespace spx

@@ -168,6 +168,19 @@ class HMatrixGPUPackedFused:
         call("spx_hmat_apply", self._h, ptr(x), ptr(out), _lib.stream_ptr())
         return out
 
+    def matvec_noalloc(self, x_gpu, out):
+        """y = H x through spx_hmat_apply_noalloc: no device allocation inside the call
+        (the scratch is the library's fixed 32 MiB device array, shared by every call, so
+        calls must not overlap on the GPU).  ``out`` must be a preallocated CUDA float64
+        tensor of length Nb."""
+        import torch
+        if x_gpu.dtype != torch.float64 or not x_gpu.is_cuda or not x_gpu.is_contiguous():
+            raise TypeError("matvec_noalloc expects a contiguous CUDA float64 tensor")
+        if out.dtype != torch.float64 or not out.is_cuda or not out.is_contiguous() or out.numel() != self.size:
+            raise TypeError("out must be a contiguous CUDA float64 tensor of length Nb")
+        call("spx_hmat_apply_noalloc", self._h, ptr(x_gpu), ptr(out), _lib.stream_ptr())
+        return out
+
     def matvec_numpy(self, x):
         import torch
         xt = torch.as_tensor(np.asarray(x, dtype=np.float64), device="cuda")

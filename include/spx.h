@@ -115,6 +115,19 @@ SPX_API int spx_hmat_perm(spx_hmat h, int32_t* perm);
 /* y = H x in the original boundary ordering (HMatrixGPUPackedFused.matvec, backend_fused.py:496-512) */
 SPX_API int spx_hmat_apply(spx_hmat h, const double* x, double* y, spx_stream_t s);
 SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
+/* y = H x like spx_hmat_apply, for callers that cannot allocate device memory while they
+ * run: a solver callback whose device memory is owned by another allocator (a PETSc or
+ * framework memory pool that must not be bypassed), or a loop that may not stall on
+ * cudaMalloc.  No counterpart in the reference.  This entry point allocates nothing: its
+ * scratch (x in permuted order plus the far-field z vectors, Nb + sum of ranks elements in
+ * the packed precision, 256-byte aligned) lives in one fixed 32 MiB device array that every
+ * GPU loading libspx holds until exit; larger H-matrices are rejected with SPX_ERR_INVALID.
+ * The first call on a device looks up that array's device address with
+ * cudaGetSymbolAddress, so make the first call on each device before any stream capture.
+ * All calls share the array and overwrite it completely (nothing in it has to start at
+ * zero), so calls that overlap on the GPU (other streams, other threads) race; serialise
+ * them.  x, y: FP64 device vectors of length Nb. */
+SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_stream_t s);
 /* low-rank factors U^T (k x m) and V (k x n) of far block `index` (as listed by spx_hmat_blocks), FP64 host */
 SPX_API int spx_hmat_far_factors(spx_hmat h, int64_t index, double* Ut, double* V);
 SPX_API int spx_hmat_memory(spx_hmat h, int64_t* far_bytes, int64_t* near_bytes, int64_t* total_bytes);

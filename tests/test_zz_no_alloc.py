@@ -1,0 +1,44 @@
+"""spx_hmat_apply_noalloc: the H-matrix apply for callers that cannot allocate device memory.
+
+Some callers cannot call cudaMalloc while they run, for example a time-stepper callback
+whose device memory belongs to another allocator's pool.  For them the library offers
+spx_hmat_apply_noalloc, which keeps its scratch in a fixed device array instead of
+allocating it.  This file checks it through the C ABI against spx_hmat_apply on two
+calls in a row (the scratch keeps the previous call's contents).  It sits last in
+collection order so that a stop-at-first-failure run has already run every other test.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_hmat_apply_noalloc_matches_apply(precision):
+    import spinfemx_b200 as spx
+    from spinfemx_b200 import _lib
+    from oracle import mesh
+
+    X, T = mesh.kuhn_box(30, 30, 2, 2.5)
+    geom = spx.BoundaryGeometry(X, T)
+    H = spx.HMatrixGPUPackedFused(geom, spx.HMatrixBuildConfig(epsilon=1e-5, eta=2.0, leaf_size=64),
+                                  precision=precision)
+    stream = _lib.stream_ptr()
+    rng = np.random.default_rng(4321)
+    for call_no in range(2):
+        x = torch.as_tensor(rng.standard_normal(H.size), device="cuda")
+        y_ref = torch.empty_like(x)
+        y_na = torch.full_like(x, float("nan"))
+        _lib.check(_lib.lib().spx_hmat_apply(H._h, _lib.ptr(x), _lib.ptr(y_ref), stream))
+        _lib.check(_lib.lib().spx_hmat_apply_noalloc(H._h, _lib.ptr(x), _lib.ptr(y_na), stream))
+        torch.cuda.synchronize()
+        a, b = y_na.cpu().numpy(), y_ref.cpu().numpy()
+        assert np.all(np.isfinite(a)), call_no
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), call_no
+    # the Python wrapper reaches the same entry point
+    out = torch.empty_like(x)
+    H.matvec_noalloc(x, out)
+    torch.cuda.synchronize()
+    assert np.linalg.norm(out.cpu().numpy() - y_ref.cpu().numpy()) <= 1e-12 * np.linalg.norm(y_ref.cpu().numpy())
