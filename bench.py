@@ -173,7 +173,9 @@ def run_ours(a):
         X, T, 8e5, Aex=1.3e-11, alpha=0.02, gamma=2.211e5, H0_static=H0, use_demag=True,
         precision=a.precision,
         demag_kwargs=dict(boundary_backend="hmatrix", hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
-                          ksp_rtol_u1=1e-6, ksp_rtol_u2=1e-6, warm_start=a.warm_start, precision=a.precision))
+                          ksp_rtol_u1=1e-6, ksp_rtol_u2=1e-6, precision=a.precision,
+                          hmatrix_precision=a.hmatrix_precision,
+                          warm_start={0: False, 1: True, 2: "extrapolate"}[a.warm_start]))
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     dm = hef.demag_field
@@ -262,14 +264,16 @@ def run_ours(a):
     line = {
         "metric": METRIC, "value": round(ws * sps, 4), "unit": "steps/s", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp32+bf16"}[a.precision],
+        "scaling": "weak", "vs_baseline": None, "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp64 vectors / fp32 operators"}[a.precision],
         "data": "synthetic (seeded Kuhn-box film and magnetisation)",
         "config": {"workload": f"film {a.nx}x{a.ny}x{a.nz} cubes @{a.h}nm, N={N}, Nb={dm.Nb}, H-matrix ACA 1e-5 "
-                               f"leaf 64 eta 2, RK4 dt {a.dt:g}s, {a.precision}",
+                               f"leaf 64 eta 2, RK4 dt {a.dt:g}s, {a.precision} "
+                               f"(H factors {dm.hmatrix_precision})",
                    "nodes": N, "boundary_nodes": dm.Nb, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (H-matrix factors %.1f GB per apply)" % (
                        (Hmem["far_bytes"] + Hmem["near_bytes"]) / 1e9),
-                   "warm_start": bool(a.warm_start), "demag_rel_err_vs_fp64": err},
+                   "cg_start": {0: "zero", 1: "previous", 2: "extrapolated per RK stage"}[a.warm_start],
+                   "demag_rel_err_vs_fp64": err},
         "e2e": e2e,
         "roofline": roof,
         "kernels": per,
@@ -311,11 +315,9 @@ def demag_error(spx, X, T, m, dm, a):
     """Relative L2 error of the working-precision demag field against an FP64 solve
     (FP64 H-matrix factors, rtol 1e-10) at the final state."""
     import torch
-    if a.precision == "f64":
-        return None
     ref = spx.DemagFieldLindholmGPU(X, T, 8e5, boundary_backend="hmatrix", hmatrix_epsilon=1e-5, precision="f64",
                                     ksp_rtol_u1=1e-10, ksp_rtol_u2=1e-10, ksp_maxit_u1=50000, ksp_maxit_u2=50000,
-                                    ksp_atol=0.0)
+                                    ksp_atol=0.0, hmatrix_precision="f64")
     Hr = torch.empty_like(m)
     ref.compute_vec(m, Hr)
     Hw = torch.empty_like(m)
@@ -437,13 +439,14 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="f32", choices=["f32", "f64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["f32", "f64", "mixed"])
+    ap.add_argument("--hmatrix-precision", default=None, choices=["f64", "f32", "bf16"])
     ap.add_argument("--nx", type=int, default=400)
     ap.add_argument("--ny", type=int, default=400)
     ap.add_argument("--nz", type=int, default=2)
     ap.add_argument("--h", type=float, default=2.5)
     ap.add_argument("--dt", type=float, default=5e-14)
-    ap.add_argument("--warm-start", type=int, default=1)
+    ap.add_argument("--warm-start", type=int, default=2, help="0 zero, 1 previous, 2 extrapolated per RK stage")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--check-error", type=int, default=1)

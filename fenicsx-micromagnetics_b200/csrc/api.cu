@@ -77,19 +77,173 @@ struct spx_boundary_s {
 struct spx_hmat_s {
   HMatrix h;
 };
-struct spx_demag_s {
-  Prec prec = Prec::F64;
-  std::unique_ptr<DemagCtx<double>> d64;
-  std::unique_ptr<DemagCtx<float>> d32;
-  DevBuf<float> tm, th;  // FP32 staging of FP64 API vectors
-  int64_t N() const { return d64 ? d64->N : d32->N; }
+// ---- type-erased demag / LLG handles (precision chosen at create)
+struct DemagBase {
+  virtual ~DemagBase() = default;
+  virtual int64_t N() const = 0;
+  virtual void apply(const double* m, double* H, cudaStream_t s) = 0;
+  virtual void potentials(double* u1, double* phi, cudaStream_t s) = 0;
+  virtual double energy(const double* m, const double* H, cudaStream_t s) = 0;
+  virtual CgStats last1() const = 0;
+  virtual CgStats last2() const = 0;
+  virtual void info(int64_t* N, int64_t* Nb, int64_t* NI, int64_t* bytes) const = 0;
+  virtual HMatrix* hmat() = 0;
+  virtual Profiler& prof() = 0;
+  virtual void counters(unsigned long long a[4], unsigned long long b[4]) = 0;
+  virtual void residuals(double a[2], double b[2]) = 0;
+  virtual void set_tolerances(double r1, double r2, double at, int m1, int m2) = 0;
 };
-struct spx_llg_s {
-  bool f32 = false;
-  std::unique_ptr<LLGCtx<double>> l64;
-  std::unique_ptr<LLGCtx<float>> l32;
-  DevBuf<float> ta, tb;
+
+template <class TV, class TM>
+struct DemagImpl : DemagBase {
+  DemagCtx<TV, TM> d;
+  DevBuf<TV> tm, th;
+  int64_t N() const override { return d.N; }
+  void apply(const double* m, double* H, cudaStream_t s) override {
+    if (sizeof(TV) == sizeof(double)) {
+      d.potential(reinterpret_cast<const TV*>(m), s, true);
+      d.field(reinterpret_cast<TV*>(H), s);
+    } else {
+      const int64_t n3 = 3 * d.N;
+      if (!tm.n) { tm.alloc(n3); th.alloc(n3); }
+      convert<double, TV>(n3, m, tm.p, s);
+      d.potential(tm.p, s, true);
+      d.field(th.p, s);
+      convert<TV, double>(n3, th.p, H, s);
+    }
+  }
+  void potentials(double* u1, double* phi, cudaStream_t s) override {
+    if (u1) convert<TV, double>(d.N, d.u1.p, u1, s);
+    if (phi) convert<TV, double>(d.N, d.phi.p, phi, s);
+  }
+  double energy(const double* m, const double* H, cudaStream_t s) override {
+    if (sizeof(TV) == sizeof(double))
+      return demag_energy<TV, TM>(d, reinterpret_cast<const TV*>(m), reinterpret_cast<const TV*>(H), s);
+    const int64_t n3 = 3 * d.N;
+    if (!tm.n) { tm.alloc(n3); th.alloc(n3); }
+    convert<double, TV>(n3, m, tm.p, s);
+    convert<double, TV>(n3, H, th.p, s);
+    return demag_energy<TV, TM>(d, tm.p, th.p, s);
+  }
+  CgStats last1() const override { return d.last1; }
+  CgStats last2() const override { return d.last2; }
+  void info(int64_t* N, int64_t* Nb, int64_t* NI, int64_t* bytes) const override {
+    if (N) *N = d.N;
+    if (Nb) *Nb = d.Nb;
+    if (NI) *NI = d.NI;
+    if (bytes) *bytes = d.device_bytes();
+  }
+  HMatrix* hmat() override { return d.opt.backend == 1 ? &d.H : nullptr; }
+  Profiler& prof() override { return d.prof; }
+  void counters(unsigned long long a[4], unsigned long long b[4]) override {
+    auto rd = [](DevBuf<unsigned long long>& src, unsigned long long* dst) {
+      if (src.n) SPX_CUDA(cudaMemcpy(dst, src.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    };
+    rd(d.cg1.iters_acc, a);
+    rd(d.cg2.iters_acc, b);
+  }
+  void residuals(double a[2], double b[2]) override {
+    auto rd = [](DevBuf<double>& src, double* dst) {
+      if (src.n) SPX_CUDA(cudaMemcpy(dst, src.p, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+    };
+    rd(d.cg1.res_acc, a);
+    rd(d.cg2.res_acc, b);
+  }
+  void set_tolerances(double r1, double r2, double at, int m1, int m2) override {
+    d.opt.rtol_u1 = r1; d.opt.rtol_u2 = r2; d.opt.atol = at;
+    d.opt.maxit_u1 = m1; d.opt.maxit_u2 = m2;
+  }
+};
+
+struct spx_demag_s {
+  std::unique_ptr<DemagBase> impl;
+};
+
+struct LLGBase {
+  virtual ~LLGBase() = default;
+  virtual void heff(const double* m, double* H, bool with_demag, cudaStream_t s) = 0;
+  virtual void rhs(const double* m, double* r, cudaStream_t s) = 0;
+  virtual void update_jac_state(const double* m, cudaStream_t s) = 0;
+  virtual void jv(const double* v, double* o, cudaStream_t s) = 0;
+  virtual void pc_build(double shift, int inc, int absk, cudaStream_t s) = 0;
+  virtual void pc_apply(const double* x, double* y, cudaStream_t s) = 0;
+  virtual void set_state(const double* m, cudaStream_t s) = 0;
+  virtual void get_state(double* m, cudaStream_t s) = 0;
+  virtual void step(double dt, int64_t n, cudaStream_t s) = 0;
+  virtual void run_host(const double* in, double* out, double dt, int64_t n) = 0;
+  virtual void set_uniform_field(double x, double y, double z) = 0;
+  virtual void stats(int64_t* steps, int64_t* rhs, int64_t* launches) const = 0;
+};
+
+template <class TV, class TM>
+struct LLGImpl : LLGBase {
+  LLGCtx<TV, TM> l;
+  DevBuf<TV> ta, tb;
   DevBuf<double> hstage;
+  static constexpr bool f64 = sizeof(TV) == sizeof(double);
+  const TV* in(const double* p, cudaStream_t s) {
+    if (f64) return reinterpret_cast<const TV*>(p);
+    if (!ta.n) ta.alloc(3 * l.N);
+    convert<double, TV>(3 * l.N, p, ta.p, s);
+    return ta.p;
+  }
+  TV* outbuf(double* p) {
+    if (f64) return reinterpret_cast<TV*>(p);
+    if (!tb.n) tb.alloc(3 * l.N);
+    return tb.p;
+  }
+  void out(double* p, cudaStream_t s) {
+    if (!f64) convert<TV, double>(3 * l.N, tb.p, p, s);
+  }
+  void heff(const double* m, double* H, bool wd, cudaStream_t s) override {
+    TV* o = outbuf(H);
+    l.heff(in(m, s), o, wd, s);
+    out(H, s);
+  }
+  void rhs(const double* m, double* r, cudaStream_t s) override {
+    TV* o = outbuf(r);
+    l.rhs(in(m, s), o, s);
+    out(r, s);
+  }
+  void update_jac_state(const double* m, cudaStream_t s) override { l.update_jac_state(in(m, s), s); }
+  void jv(const double* v, double* o, cudaStream_t s) override {
+    TV* q = outbuf(o);
+    l.jv(in(v, s), q, s);
+    out(o, s);
+  }
+  void pc_build(double shift, int inc, int absk, cudaStream_t s) override { l.pc_build(shift, inc, absk, s); }
+  void pc_apply(const double* x, double* y, cudaStream_t s) override {
+    TV* q = outbuf(y);
+    l.pc_apply(in(x, s), q, s);
+    out(y, s);
+  }
+  void set_state(const double* m, cudaStream_t s) override { convert<double, TV>(3 * l.N, m, l.m.p, s); }
+  void get_state(double* m, cudaStream_t s) override { convert<TV, double>(3 * l.N, l.m.p, m, s); }
+  void step(double dt, int64_t n, cudaStream_t s) override { l.step_rk4(dt, n, s); }
+  void run_host(const double* hin, double* hout, double dt, int64_t n) override {
+    const int64_t n3 = 3 * l.N;
+    cudaStream_t s = 0;
+    if (!hstage.n) hstage.alloc(n3);
+    SPX_CUDA(cudaMemcpyAsync(hstage.p, hin, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
+    convert<double, TV>(n3, hstage.p, l.m.p, s);
+    l.step_rk4(dt, n, s);
+    convert<TV, double>(n3, l.m.p, hstage.p, s);
+    SPX_CUDA(cudaMemcpyAsync(hout, hstage.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
+  void set_uniform_field(double x, double y, double z) override {
+    l.H0.release();
+    l.h0[0] = x; l.h0[1] = y; l.h0[2] = z;
+  }
+  void stats(int64_t* st, int64_t* r, int64_t* la) const override {
+    if (st) *st = l.steps;
+    if (r) *r = l.rhs_evals;
+    if (la) *la = l.launches;
+  }
+};
+
+struct spx_llg_s {
+  std::unique_ptr<LLGBase> impl;
   int64_t N = 0;
 };
 
@@ -109,17 +263,18 @@ __global__ void k_gemv_rows(int64_t Nb, const double* __restrict__ B, const doub
 }
 }  // namespace spx
 
-// run op on FP64 API vectors: in -> (convert) -> op -> (convert) -> out
-template <class F64, class F32>
-static void llg_call(spx_llg l, const double* in, double* outp, spx_stream_t s, F64 f64, F32 f32) {
-  if (!l->f32) {
-    f64(*l->l64, in, outp);
-  } else {
-    const int64_t n3 = 3 * l->N;
-    if (in) convert<double, float>(n3, in, l->ta.p, S(s));
-    f32(*l->l32, in ? l->ta.p : nullptr, outp ? l->tb.p : nullptr);
-    if (outp) convert<float, double>(n3, l->tb.p, outp, S(s));
+template <class TV, class TM>
+static std::unique_ptr<LLGBase> make_llg(spx_demag d, const double* X, int64_t N, const int32_t* tets, int64_t E,
+                                         const LLGParams& q) {
+  auto l = std::make_unique<LLGImpl<TV, TM>>();
+  DemagCtx<TV, TM>* dm = nullptr;
+  if (d) {
+    auto* impl = dynamic_cast<DemagImpl<TV, TM>*>(d->impl.get());
+    SPX_CHECK(impl != nullptr, "internal: demag precision mismatch");
+    dm = &impl->d;
   }
+  l->l.create(dm, X, N, tets, E, q, 0);
+  return l;
 }
 
 
@@ -390,8 +545,10 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
   DemagOptions o;
   if (opt) {
     SPX_CHECK(opt->backend == 0 || opt->backend == 1, "backend must be 0 (dense) or 1 (hmatrix)");
+    SPX_CHECK(opt->warm_start >= 0 && opt->warm_start <= 2, "warm_start must be 0, 1 or 2");
     o.backend = opt->backend;
     o.prec = to_prec(opt->precision);
+    o.hprec = to_prec(opt->hmat.precision);
     if (opt->rtol_u1 > 0) o.rtol_u1 = opt->rtol_u1;
     if (opt->rtol_u2 > 0) o.rtol_u2 = opt->rtol_u2;
     if (opt->atol >= 0) o.atol = opt->atol;
@@ -401,15 +558,25 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
     o.hcfg = to_hcfg(&opt->hmat);
   }
   auto d = std::make_unique<spx_demag_s>();
-  d->prec = o.prec;
-  if (o.prec == Prec::F64) {
-    d->d64 = std::make_unique<DemagCtx<double>>();
-    d->d64->create(X, N, tets, E, Ms, o, 0);
-  } else {
-    d->d32 = std::make_unique<DemagCtx<float>>();
-    d->d32->create(X, N, tets, E, Ms, o, 0);
-    d->tm.alloc(3 * N);
-    d->th.alloc(3 * N);
+  switch (o.prec) {
+    case Prec::F64: {
+      auto p = std::make_unique<DemagImpl<double, double>>();
+      p->d.create(X, N, tets, E, Ms, o, 0);
+      d->impl = std::move(p);
+      break;
+    }
+    case Prec::F32: {
+      auto p = std::make_unique<DemagImpl<float, float>>();
+      p->d.create(X, N, tets, E, Ms, o, 0);
+      d->impl = std::move(p);
+      break;
+    }
+    case Prec::MIXED: {
+      auto p = std::make_unique<DemagImpl<double, float>>();
+      p->d.create(X, N, tets, E, Ms, o, 0);
+      d->impl = std::move(p);
+      break;
+    }
   }
   *out = d.release();
   API_END
@@ -417,75 +584,41 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
 
 int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s) {
   API_BEGIN
-  REQUIRE(d);
-  REQUIRE(m);
-  REQUIRE(H);
-  if (d->d64) {
-    d->d64->potential(m, S(s), true);
-    d->d64->field(H, S(s));
-  } else {
-    const int64_t n3 = 3 * d->d32->N;
-    convert<double, float>(n3, m, d->tm.p, S(s));
-    d->d32->potential(d->tm.p, S(s), true);
-    d->d32->field(d->th.p, S(s));
-    convert<float, double>(n3, d->th.p, H, S(s));
-  }
+  REQUIRE(d); REQUIRE(m); REQUIRE(H);
+  d->impl->apply(m, H, S(s));
   API_END
 }
 
 int spx_demag_potentials(spx_demag d, double* u1, double* u2, spx_stream_t s) {
   API_BEGIN
   REQUIRE(d);
-  const int64_t N = d->N();
-  DevBuf<double> t(N);
-  if (d->d64) {
-    if (u1) SPX_CUDA(cudaMemcpyAsync(u1, d->d64->u1.p, N * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
-    if (u2) {
-      SPX_CUDA(cudaMemcpyAsync(u2, d->d64->phi.p, N * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
-    }
-  } else {
-    if (u1) convert<float, double>(N, d->d32->u1.p, u1, S(s));
-    if (u2) convert<float, double>(N, d->d32->phi.p, u2, S(s));
-  }
-  // u2 = phi - u1
+  const int64_t N = d->impl->N();
+  DevBuf<double> a(N);
+  d->impl->potentials(a.p, u2, S(s));  // u2 temporarily holds phi
+  if (u1) SPX_CUDA(cudaMemcpyAsync(u1, a.p, N * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
   if (u2) {
-    std::vector<double> a(N), b(N);
-    if (d->d64) SPX_CUDA(cudaMemcpyAsync(a.data(), d->d64->u1.p, N * sizeof(double), cudaMemcpyDeviceToHost, S(s)));
-    else {
-      convert<float, double>(N, d->d32->u1.p, t.p, S(s));
-      SPX_CUDA(cudaMemcpyAsync(a.data(), t.p, N * sizeof(double), cudaMemcpyDeviceToHost, S(s)));
-    }
-    SPX_CUDA(cudaMemcpyAsync(b.data(), u2, N * sizeof(double), cudaMemcpyDeviceToHost, S(s)));
+    std::vector<double> ha(N), hb(N);
+    SPX_CUDA(cudaMemcpyAsync(ha.data(), a.p, N * sizeof(double), cudaMemcpyDeviceToHost, S(s)));
+    SPX_CUDA(cudaMemcpyAsync(hb.data(), u2, N * sizeof(double), cudaMemcpyDeviceToHost, S(s)));
     SPX_CUDA(cudaStreamSynchronize(S(s)));
-    for (int64_t i = 0; i < N; ++i) b[i] -= a[i];
-    SPX_CUDA(cudaMemcpyAsync(u2, b.data(), N * sizeof(double), cudaMemcpyHostToDevice, S(s)));
-    SPX_CUDA(cudaStreamSynchronize(S(s)));
+    for (int64_t i = 0; i < N; ++i) hb[i] -= ha[i];
+    SPX_CUDA(cudaMemcpyAsync(u2, hb.data(), N * sizeof(double), cudaMemcpyHostToDevice, S(s)));
   }
+  SPX_CUDA(cudaStreamSynchronize(S(s)));
   API_END
 }
 
 int spx_demag_energy(spx_demag d, const double* m, const double* H, double* E, spx_stream_t s) {
   API_BEGIN
-  REQUIRE(d);
-  REQUIRE(m);
-  REQUIRE(H);
-  REQUIRE(E);
-  if (d->d64) {
-    *E = demag_energy<double>(*d->d64, m, H, S(s));
-  } else {
-    const int64_t n3 = 3 * d->d32->N;
-    convert<double, float>(n3, m, d->tm.p, S(s));
-    convert<double, float>(n3, H, d->th.p, S(s));
-    *E = demag_energy<float>(*d->d32, d->tm.p, d->th.p, S(s));
-  }
+  REQUIRE(d); REQUIRE(m); REQUIRE(H); REQUIRE(E);
+  *E = d->impl->energy(m, H, S(s));
   API_END
 }
 
 int spx_demag_stats(spx_demag d, int64_t* i1, int64_t* i2, double* r1, double* r2) {
   API_BEGIN
   REQUIRE(d);
-  const CgStats a = d->d64 ? d->d64->last1 : d->d32->last1;
-  const CgStats b = d->d64 ? d->d64->last2 : d->d32->last2;
+  const CgStats a = d->impl->last1(), b = d->impl->last2();
   if (i1) *i1 = a.iterations;
   if (i2) *i2 = b.iterations;
   if (r1) *r1 = a.rel_residual;
@@ -496,17 +629,7 @@ int spx_demag_stats(spx_demag d, int64_t* i1, int64_t* i2, double* r1, double* r
 int spx_demag_info(spx_demag d, int64_t* N, int64_t* Nb, int64_t* NI, int64_t* bytes) {
   API_BEGIN
   REQUIRE(d);
-  if (d->d64) {
-    if (N) *N = d->d64->N;
-    if (Nb) *Nb = d->d64->Nb;
-    if (NI) *NI = d->d64->NI;
-    if (bytes) *bytes = d->d64->device_bytes();
-  } else {
-    if (N) *N = d->d32->N;
-    if (Nb) *Nb = d->d32->Nb;
-    if (NI) *NI = d->d32->NI;
-    if (bytes) *bytes = d->d32->device_bytes();
-  }
+  d->impl->info(N, Nb, NI, bytes);
   API_END
 }
 
@@ -514,25 +637,23 @@ int spx_demag_hmat(spx_demag d, spx_hmat* h) {
   API_BEGIN
   REQUIRE(d);
   REQUIRE(h);
-  const int be = d->d64 ? d->d64->opt.backend : d->d32->opt.backend;
-  SPX_CHECK(be == 1, "demag uses the dense boundary operator");
-  *h = reinterpret_cast<spx_hmat>(d->d64 ? &d->d64->H : &d->d32->H);
+  HMatrix* H = d->impl->hmat();
+  SPX_CHECK(H != nullptr, "demag uses the dense boundary operator");
+  *h = reinterpret_cast<spx_hmat>(H);
   API_END
 }
 
 int spx_demag_profile_begin(spx_demag d) {
   API_BEGIN
   REQUIRE(d);
-  if (d->d64) d->d64->prof.begin();
-  else d->d32->prof.begin();
+  d->impl->prof().begin();
   API_END
 }
 
 int spx_demag_profile_end(spx_demag d, double* ms8, int64_t* l8, int64_t* g8) {
   API_BEGIN
   REQUIRE(d); REQUIRE(ms8); REQUIRE(l8); REQUIRE(g8);
-  if (d->d64) d->d64->prof.end(ms8, l8, g8);
-  else d->d32->prof.end(ms8, l8, g8);
+  d->impl->prof().end(ms8, l8, g8);
   API_END
 }
 
@@ -540,15 +661,33 @@ int spx_demag_counters(spx_demag d, int64_t* c1, int64_t* c2) {
   API_BEGIN
   REQUIRE(d);
   unsigned long long a[4] = {0, 0, 0, 0}, b[4] = {0, 0, 0, 0};
-  auto rd = [](DevBuf<unsigned long long>& src, unsigned long long* dst) {
-    if (src.n) SPX_CUDA(cudaMemcpy(dst, src.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-  };
-  if (d->d64) { rd(d->d64->cg1.iters_acc, a); rd(d->d64->cg2.iters_acc, b); }
-  else { rd(d->d32->cg1.iters_acc, a); rd(d->d32->cg2.iters_acc, b); }
+  d->impl->counters(a, b);
   for (int k = 0; k < 4; ++k) {
     if (c1) c1[k] = static_cast<int64_t>(a[k]);
     if (c2) c2[k] = static_cast<int64_t>(b[k]);
   }
+  API_END
+}
+
+int spx_demag_residuals(spx_demag d, double* r1, double* r2) {
+  API_BEGIN
+  REQUIRE(d);
+  double a[2] = {0, 0}, b[2] = {0, 0};
+  d->impl->residuals(a, b);
+  for (int k = 0; k < 2; ++k) {
+    if (r1) r1[k] = a[k];
+    if (r2) r2[k] = b[k];
+  }
+  API_END
+}
+
+int spx_demag_set_tolerances(spx_demag d, double rtol_u1, double rtol_u2, double atol, int32_t maxit_u1,
+                             int32_t maxit_u2) {
+  API_BEGIN
+  REQUIRE(d);
+  SPX_CHECK(rtol_u1 > 0.0 && rtol_u2 > 0.0 && atol >= 0.0, "tolerances must be positive");
+  SPX_CHECK(maxit_u1 > 0 && maxit_u2 > 0, "iteration limits must be positive");
+  d->impl->set_tolerances(rtol_u1, rtol_u2, atol, maxit_u1, maxit_u2);
   API_END
 }
 
@@ -581,18 +720,18 @@ int spx_llg_create(spx_demag d, const double* X, int64_t N, const int32_t* tets,
   LLGParams q = to_params(p);
   auto l = std::make_unique<spx_llg_s>();
   l->N = N;
-  const bool f32 = d ? (d->d32 != nullptr) : (p->precision != 0);
-  l->f32 = f32;
-  if (!f32) {
-    l->l64 = std::make_unique<LLGCtx<double>>();
-    l->l64->create(d ? d->d64.get() : nullptr, X, N, tets, E, q, 0);
-  } else {
-    l->l32 = std::make_unique<LLGCtx<float>>();
-    l->l32->create(d ? d->d32.get() : nullptr, X, N, tets, E, q, 0);
-    l->ta.alloc(3 * N);
-    l->tb.alloc(3 * N);
+  int prec = p->precision;
+  if (d) {
+    if (dynamic_cast<DemagImpl<double, double>*>(d->impl.get())) prec = 0;
+    else if (dynamic_cast<DemagImpl<float, float>*>(d->impl.get())) prec = 1;
+    else prec = 2;
+    SPX_CHECK(d->impl->N() == N, "demag and LLG meshes differ");
   }
-  l->hstage.alloc(3 * N);
+  switch (to_prec(prec)) {
+    case Prec::F64: l->impl = make_llg<double, double>(d, X, N, tets, E, q); break;
+    case Prec::F32: l->impl = make_llg<float, float>(d, X, N, tets, E, q); break;
+    case Prec::MIXED: l->impl = make_llg<double, float>(d, X, N, tets, E, q); break;
+  }
   *out = l.release();
   API_END
 }
@@ -600,72 +739,63 @@ int spx_llg_create(spx_demag d, const double* X, int64_t N, const int32_t* tets,
 int spx_llg_heff(spx_llg l, const double* m, double* H, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m); REQUIRE(H);
-  llg_call(l, m, H, s, [&](LLGCtx<double>& c, const double* a, double* b) { c.heff(a, b, true, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float* b) { c.heff(a, b, true, S(s)); });
+  l->impl->heff(m, H, true, S(s));
   API_END
 }
 
 int spx_llg_hjac(spx_llg l, const double* m, double* H, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m); REQUIRE(H);
-  llg_call(l, m, H, s, [&](LLGCtx<double>& c, const double* a, double* b) { c.heff(a, b, false, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float* b) { c.heff(a, b, false, S(s)); });
+  l->impl->heff(m, H, false, S(s));
   API_END
 }
 
 int spx_llg_rhs(spx_llg l, const double* m, double* r, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m); REQUIRE(r);
-  llg_call(l, m, r, s, [&](LLGCtx<double>& c, const double* a, double* b) { c.rhs(a, b, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float* b) { c.rhs(a, b, S(s)); });
+  l->impl->rhs(m, r, S(s));
   API_END
 }
 
 int spx_llg_update_jac_state(spx_llg l, const double* m, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m);
-  llg_call(l, m, nullptr, s, [&](LLGCtx<double>& c, const double* a, double*) { c.update_jac_state(a, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float*) { c.update_jac_state(a, S(s)); });
+  l->impl->update_jac_state(m, S(s));
   API_END
 }
 
 int spx_llg_jv(spx_llg l, const double* v, double* o, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(v); REQUIRE(o);
-  llg_call(l, v, o, s, [&](LLGCtx<double>& c, const double* a, double* b) { c.jv(a, b, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float* b) { c.jv(a, b, S(s)); });
+  l->impl->jv(v, o, S(s));
   API_END
 }
 
 int spx_llg_pc_build(spx_llg l, double shift, int32_t include_stab, int32_t use_abs_kappa, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l);
-  if (!l->f32) l->l64->pc_build(shift, include_stab, use_abs_kappa, S(s));
-  else l->l32->pc_build(shift, include_stab, use_abs_kappa, S(s));
+  l->impl->pc_build(shift, include_stab, use_abs_kappa, S(s));
   API_END
 }
 
 int spx_llg_pc_apply(spx_llg l, const double* x, double* y, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(x); REQUIRE(y);
-  llg_call(l, x, y, s, [&](LLGCtx<double>& c, const double* a, double* b) { c.pc_apply(a, b, S(s)); },
-           [&](LLGCtx<float>& c, const float* a, float* b) { c.pc_apply(a, b, S(s)); });
+  l->impl->pc_apply(x, y, S(s));
   API_END
 }
 
 int spx_llg_set_state(spx_llg l, const double* m, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m);
-  if (!l->f32) SPX_CUDA(cudaMemcpyAsync(l->l64->m.p, m, 3 * l->N * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
-  else convert<double, float>(3 * l->N, m, l->l32->m.p, S(s));
+  l->impl->set_state(m, S(s));
   API_END
 }
 
 int spx_llg_get_state(spx_llg l, double* m, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l); REQUIRE(m);
-  if (!l->f32) SPX_CUDA(cudaMemcpyAsync(m, l->l64->m.p, 3 * l->N * sizeof(double), cudaMemcpyDeviceToDevice, S(s)));
-  else convert<float, double>(3 * l->N, l->l32->m.p, m, S(s));
+  l->impl->get_state(m, S(s));
   API_END
 }
 
@@ -674,8 +804,7 @@ int spx_llg_step(spx_llg l, double dt, int64_t nsteps, spx_stream_t s) {
   REQUIRE(l);
   SPX_CHECK(nsteps >= 0, "nsteps must be non-negative");
   SPX_CHECK(dt > 0.0, "dt must be positive");
-  if (!l->f32) l->l64->step_rk4(dt, nsteps, S(s));
-  else l->l32->step_rk4(dt, nsteps, S(s));
+  l->impl->step(dt, nsteps, S(s));
   API_END
 }
 
@@ -683,48 +812,21 @@ int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, in
   API_BEGIN
   REQUIRE(l); REQUIRE(m_in); REQUIRE(m_out);
   SPX_CHECK(dt > 0.0 && nsteps >= 0, "dt must be positive and nsteps non-negative");
-  const int64_t n3 = 3 * l->N;
-  cudaStream_t s = 0;
-  SPX_CUDA(cudaMemcpyAsync(l->hstage.p, m_in, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
-  if (!l->f32) {
-    SPX_CUDA(cudaMemcpyAsync(l->l64->m.p, l->hstage.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    l->l64->step_rk4(dt, nsteps, s);
-    SPX_CUDA(cudaMemcpyAsync(l->hstage.p, l->l64->m.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  } else {
-    convert<double, float>(n3, l->hstage.p, l->l32->m.p, s);
-    l->l32->step_rk4(dt, nsteps, s);
-    convert<float, double>(n3, l->l32->m.p, l->hstage.p, s);
-  }
-  SPX_CUDA(cudaMemcpyAsync(m_out, l->hstage.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  SPX_CUDA(cudaStreamSynchronize(s));
+  l->impl->run_host(m_in, m_out, dt, nsteps);
   API_END
 }
 
 int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz) {
   API_BEGIN
   REQUIRE(l);
-  if (!l->f32) {
-    l->l64->H0.release();
-    l->l64->h0[0] = hx; l->l64->h0[1] = hy; l->l64->h0[2] = hz;
-  } else {
-    l->l32->H0.release();
-    l->l32->h0[0] = hx; l->l32->h0[1] = hy; l->l32->h0[2] = hz;
-  }
+  l->impl->set_uniform_field(hx, hy, hz);
   API_END
 }
 
 int spx_llg_stats(spx_llg l, int64_t* steps, int64_t* rhs, int64_t* launches) {
   API_BEGIN
   REQUIRE(l);
-  if (!l->f32) {
-    if (steps) *steps = l->l64->steps;
-    if (rhs) *rhs = l->l64->rhs_evals;
-    if (launches) *launches = l->l64->launches;
-  } else {
-    if (steps) *steps = l->l32->steps;
-    if (rhs) *rhs = l->l32->rhs_evals;
-    if (launches) *launches = l->l32->launches;
-  }
+  l->impl->stats(steps, rhs, launches);
   API_END
 }
 

@@ -1,15 +1,19 @@
-// FEM operators, persistent CG and the FEM/BEM demag pipeline on the device.
+// FEM operators, persistent CG solvers and the FEM/BEM demag pipeline on the device.
 //
 // Pipeline per call (DemagFieldLindholmGPU.compute_vec, gpu/fields/Demag_Lindholm_GPU.py:643-670):
-//   b  = Ms int grad v . m                      k_div   (+ sum b for the null space)
-//   u1 : A u1 = b - mean(b), u1 -= mean(u1)     k_cg    (:569-582; PETSc CG+GAMG there)
+//   b  = Ms int grad v . m                      k_div   (difference form)
+//   u1 : A u1 = b - mean(b), u1 -= mean(u1)     k_cg / k_cg_ir  (:569-582; PETSc CG+GAMG there)
 //   g  = B u1|bnd                               dense GEMV or H-matrix (:585-616)
-//   u2 : A_II u_I = -A_IB g, u2|bnd = g          k_cg    (:618-640)
+//   u2 : A_II u_I = -A_IB g, u2|bnd = g          k_u2rhs + k_cg / k_cg_ir  (:618-640)
 //   phi = u1 + u2 ;  H = G phi / V_i            k_grad  (:659-670)
-// The Dirichlet problem is solved on the interior unknowns only; DOLFINx's identity
-// rows for the boundary dofs (assemble_matrix with bcs) give the same interior
-// solution.  CG stops when ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned
-// residual, the KSP default test with a zero initial guess) or after maxit.
+// The Dirichlet problem is solved on the interior unknowns only; DOLFINx's identity rows for
+// the boundary dofs (assemble_matrix with bcs) give the same interior solution.  CG stops when
+// ||r||_2 <= max(rtol ||b||_2, atol) (unpreconditioned residual, the KSP default test with a
+// zero initial guess) or after maxit.
+//
+// Persistent solvers: one cooperative launch per solve, one CTA of 1024 threads per SM.  Each
+// reduction writes one partial per CTA; after the grid barrier every CTA sums the partials in
+// the same order (deterministic, no contended atomics).  Every barrier wait is bounded.
 #include <algorithm>
 #include <cmath>
 
@@ -32,40 +36,42 @@ namespace spx {
     }                                                                                   \
   }
 
-template <class T>
+// b_i = sum_j D_ij . (m_j - m_i) + Dsum_i . m_i
+template <class TV, class TM>
 __global__ void k_div(int64_t n, int64_t nslices, const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
-                      const T* __restrict__ D, int64_t L, const T* __restrict__ m, T* __restrict__ b,
-                      double* __restrict__ bsum) {
-  __shared__ double sh[32];
-  double part = 0.0;
+                      const TM* __restrict__ D, int64_t L, const double* __restrict__ Dsum, const TV* __restrict__ m,
+                      TV* __restrict__ b) {
   SELL_ROW_LOOP(nslices, {
     if (row < n) {
-      T acc = 0;
+      const TV mx = m[3 * row], my = m[3 * row + 1], mz = m[3 * row + 2];
+      TV acc = 0;
       for (int k = 0; k < width; ++k) {
         const int64_t idx = base_ + ((int64_t)k << 5) + lane_;
         const int64_t j = col[idx];
-        acc += D[idx] * m[3 * j] + D[L + idx] * m[3 * j + 1] + D[2 * L + idx] * m[3 * j + 2];
+        acc += static_cast<TV>(D[idx]) * (m[3 * j] - mx) + static_cast<TV>(D[L + idx]) * (m[3 * j + 1] - my) +
+               static_cast<TV>(D[2 * L + idx]) * (m[3 * j + 2] - mz);
       }
+      acc += static_cast<TV>(Dsum[row]) * mx + static_cast<TV>(Dsum[n + row]) * my +
+             static_cast<TV>(Dsum[2 * n + row]) * mz;
       b[row] = acc;
-      part += static_cast<double>(acc);
     }
   })
-  const double t = block_sum(part, sh);
-  if (threadIdx.x == 0 && bsum) atomicAdd(bsum, t);
 }
 
-template <class T>
+// H_i = sum_j Gv_ij (phi_j - phi_i)
+template <class TV, class TM>
 __global__ void k_grad(int64_t n, int64_t nslices, const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
-                       const T* __restrict__ Gv, int64_t L, const T* __restrict__ phi, T* __restrict__ H) {
+                       const TM* __restrict__ Gv, int64_t L, const TV* __restrict__ phi, TV* __restrict__ H) {
   SELL_ROW_LOOP(nslices, {
     if (row < n) {
-      T hx = 0, hy = 0, hz = 0;
+      const TV pi = phi[row];
+      TV hx = 0, hy = 0, hz = 0;
       for (int k = 0; k < width; ++k) {
         const int64_t idx = base_ + ((int64_t)k << 5) + lane_;
-        const T p = phi[col[idx]];
-        hx += Gv[idx] * p;
-        hy += Gv[L + idx] * p;
-        hz += Gv[2 * L + idx] * p;
+        const TV p = phi[col[idx]] - pi;
+        hx += static_cast<TV>(Gv[idx]) * p;
+        hy += static_cast<TV>(Gv[L + idx]) * p;
+        hz += static_cast<TV>(Gv[2 * L + idx]) * p;
       }
       H[3 * row] = hx;
       H[3 * row + 1] = hy;
@@ -74,24 +80,24 @@ __global__ void k_grad(int64_t n, int64_t nslices, const int64_t* __restrict__ s
   })
 }
 
-template <class T>
+template <class TV>
 __global__ void k_u2rhs(int64_t n, int64_t nslices, const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
-                        const T* __restrict__ v, const T* __restrict__ g, T* __restrict__ b) {
+                        const double* __restrict__ v, const TV* __restrict__ g, TV* __restrict__ b) {
   SELL_ROW_LOOP(nslices, {
     if (row < n) {
-      T acc = 0;
+      double acc = 0;
       for (int k = 0; k < width; ++k) {
         const int64_t idx = base_ + ((int64_t)k << 5) + lane_;
-        acc += v[idx] * g[col[idx]];
+        acc += v[idx] * static_cast<double>(g[col[idx]]);
       }
-      b[row] = -acc;
+      b[row] = static_cast<TV>(-acc);
     }
   })
 }
 
-template <class T>
-__global__ void k_phi_interior(int64_t NI, const int32_t* __restrict__ interior, const T* __restrict__ u1,
-                               const T* __restrict__ xI, T* __restrict__ phi) {
+template <class TV>
+__global__ void k_phi_interior(int64_t NI, const int32_t* __restrict__ interior, const TV* __restrict__ u1,
+                               const TV* __restrict__ xI, TV* __restrict__ phi) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < NI) {
     const int32_t g = interior[i];
@@ -106,10 +112,10 @@ __global__ void k_gather_idx(int64_t n, const int32_t* __restrict__ idx, const T
 }
 
 // dense B (FP64, row-major Nb x Nb): warp per row; g = B xb ; phi[bverts] = u1 + g
-template <class T>
-__global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const T* __restrict__ xb,
-                             const int32_t* __restrict__ bverts, const T* __restrict__ u1, T* __restrict__ phi,
-                             T* __restrict__ gB) {
+template <class TV>
+__global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const TV* __restrict__ xb,
+                             const int32_t* __restrict__ bverts, const TV* __restrict__ u1, TV* __restrict__ phi,
+                             TV* __restrict__ gB) {
   const int lane = threadIdx.x & 31;
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
@@ -119,38 +125,110 @@ __global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const T* 
     for (int64_t j = lane; j < Nb; j += 32) acc += row[j] * static_cast<double>(xb[j]);
     acc = warp_sum(acc);
     if (lane == 0) {
-      const T y = static_cast<T>(acc);
+      const TV y = static_cast<TV>(acc);
       gB[i] = y;
       if (phi) phi[bverts[i]] = u1[bverts[i]] + y;
     }
   }
 }
 
-// ------------------------------------------------------------------ persistent pipelined CG
+// starting guess: quadratic / linear / constant extrapolation of stored solutions
 template <class T>
+__global__ void k_extrap(int64_t n, const double* __restrict__ h0, const double* __restrict__ h1,
+                         const double* __restrict__ h2, int cnt, T* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v;
+  if (cnt >= 3) v = 3.0 * h0[i] - 3.0 * h1[i] + h2[i];
+  else if (cnt == 2) v = 2.0 * h0[i] - h1[i];
+  else v = h0[i];
+  out[i] = static_cast<T>(v);
+}
+
+// ------------------------------------------------------------------ CTA reductions
+constexpr int CG_BLOCK = 1024;
+
+// sum of up to 4 values over the CTA; result valid in every thread (sh >= 4*32+4 doubles)
+__device__ __forceinline__ void cta_sum4(double v[4], double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 4; ++q) sh[4 * wid + q] = v[q];
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double t = (lane < nw) ? sh[4 * lane + q] : 0.0;
+      t = warp_sum(t);
+      if (lane == 0) sh[128 + q] = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = sh[128 + q];
+  __syncthreads();
+}
+
+// write this CTA's partials of slot s
+__device__ __forceinline__ void cta_partial(double* part, int s, double a, double b, double c, double d,
+                                            double* sh) {
+  double v[4] = {a, b, c, d};
+  cta_sum4(v, sh);
+  if (threadIdx.x < 4) part[(static_cast<int64_t>(s) * gridDim.x + blockIdx.x) * 4 + threadIdx.x] = v[threadIdx.x];
+}
+
+// total of slot s over all CTAs, same order in every CTA (call after a grid barrier)
+__device__ __forceinline__ void cta_total(const double* part, int s, double out[4], double* sh) {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int c = threadIdx.x; c < static_cast<int>(gridDim.x); c += blockDim.x) {
+    const double* p = part + (static_cast<int64_t>(s) * gridDim.x + c) * 4;
+    v[0] += p[0];
+    v[1] += p[1];
+    v[2] += p[2];
+    v[3] += p[3];
+  }
+  cta_sum4(v, sh);
+  for (int q = 0; q < 4; ++q) out[q] = v[q];
+}
+
+#define CG_ROWS_BEGIN                                               \
+  for (int64_t sl = gw; sl < P.nslices; sl += nw) {                 \
+    const int64_t row = sl * 32 + lane;                             \
+    const int64_t base = P.sp[sl];                                  \
+    const int width = static_cast<int>((P.sp[sl + 1] - base) >> 5); \
+    (void)base; (void)width;                                        \
+    if (row < n) {
+#define CG_ROWS_END \
+  }                 \
+  }
+
+// ------------------------------------------------------------------ pipelined FP64 CG
 struct CgParams {
   int64_t n, nslices;
   const int64_t* sp;
   const int32_t* col;
-  const T* val;
-  const T* sdinv;
-  const T* diag;
-  const T* b;
-  T* x;
-  T *r, *w0, *w1, *p, *s, *z, *y;
-  double* red;  // [0..11] 3 slots x (gamma, delta, rho, -); [12] sum b; [13] ||b||^2; [14] sum x
+  const double* val;
+  const double* sdinv;
+  const double* diag;
+  const double* b;
+  double* x;
+  double *r, *w0, *w1, *p, *s, *z, *y;
+  double* part;
   unsigned int* bar;
   int* err;
   int* iters;
   double* resid;
-  unsigned long long* iters_acc;  // [0] inner iterations, [1] outer steps, [2] solves (accumulated)
+  unsigned long long* iters_acc;
+  double* res_acc;
   double rtol, atol;
   int maxit, warm, project;
 };
 
-template <class T>
-__device__ __forceinline__ T spmv_row(const CgParams<T>& P, int64_t base, int width, int lane, const T* v) {
-  T acc = 0;
+__device__ __forceinline__ double spmv64(const CgParams& P, int64_t base, int width, int lane, const double* v) {
+  double acc = 0;
   for (int k = 0; k < width; ++k) {
     const int64_t idx = base + ((int64_t)k << 5) + lane;
     acc += P.val[idx] * v[P.col[idx]];
@@ -158,9 +236,8 @@ __device__ __forceinline__ T spmv_row(const CgParams<T>& P, int64_t base, int wi
   return acc;
 }
 
-template <class T>
-__global__ void __launch_bounds__(256) k_cg(CgParams<T> P) {
-  __shared__ double sh[32];
+__global__ void __launch_bounds__(CG_BLOCK, 1) k_cg(CgParams P) {
+  __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -168,77 +245,57 @@ __global__ void __launch_bounds__(256) k_cg(CgParams<T> P) {
   unsigned int* cnt = P.bar;
   unsigned int* gen = P.bar + 1;
   const int64_t n = P.n;
-#define ROWS_BEGIN                                                  \
-  for (int64_t sl = gw; sl < P.nslices; sl += nw) {                 \
-    const int64_t row = sl * 32 + lane;                             \
-    const int64_t base = P.sp[sl];                                  \
-    const int width = static_cast<int>((P.sp[sl + 1] - base) >> 5); \
-    (void)base; (void)width;                                        \
-    if (row < n) {
-#define ROWS_END \
-  }              \
-  }
-
-  // phase 0: sum of b (null space)
+  double tot[4];
+  double meanb = 0.0;
   if (P.project) {
     double part = 0.0;
-    ROWS_BEGIN part += static_cast<double>(P.b[row]);
-    ROWS_END
-    const double t = block_sum(part, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 12, t);
+    CG_ROWS_BEGIN part += P.b[row];
+    CG_ROWS_END
+    cta_partial(P.part, 0, part, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    cta_total(P.part, 0, tot, sh);
+    meanb = tot[0] / static_cast<double>(n);
   }
-  const double meanb = P.project ? P.red[12] / static_cast<double>(n) : 0.0;
-  // phase 1: b^ (kept in r), y0, ||b||^2
   {
     double bb = 0.0;
-    ROWS_BEGIN
-      const double bv = static_cast<double>(P.b[row]) - meanb;
-      P.r[row] = static_cast<T>(bv) * P.sdinv[row];
-      P.y[row] = P.warm ? P.x[row] / P.sdinv[row] : T(0);
+    CG_ROWS_BEGIN
+      const double bv = P.b[row] - meanb;
+      P.r[row] = bv * P.sdinv[row];
+      P.y[row] = P.warm ? P.x[row] / P.sdinv[row] : 0.0;
       bb += bv * bv;
-    ROWS_END
-    const double t = block_sum(bb, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 13, t);
+    CG_ROWS_END
+    cta_partial(P.part, 1, bb, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  // phase 2: r0 = b^ - A^ y0
+  cta_total(P.part, 1, tot, sh);
+  const double bb = tot[0];
   if (P.warm) {
-    ROWS_BEGIN P.r[row] -= spmv_row(P, base, width, lane, P.y);
-    ROWS_END
+    CG_ROWS_BEGIN P.r[row] -= spmv64(P, base, width, lane, P.y);
+    CG_ROWS_END
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  // phase 3: w0 = A^ r0, slot 0 <- (r,r), (w,r), rho
   {
     double g = 0.0, dl = 0.0, rh = 0.0;
-    ROWS_BEGIN
-      const T w = spmv_row(P, base, width, lane, P.r);
+    CG_ROWS_BEGIN
+      const double w = spmv64(P, base, width, lane, P.r);
       P.w0[row] = w;
-      const double rv = static_cast<double>(P.r[row]);
+      const double rv = P.r[row];
       g += rv * rv;
-      dl += static_cast<double>(w) * rv;
-      rh += static_cast<double>(P.diag[row]) * rv * rv;
-    ROWS_END
-    g = block_sum(g, sh);
-    dl = block_sum(dl, sh);
-    rh = block_sum(rh, sh);
-    if (threadIdx.x == 0) {
-      atomicAdd(P.red + 0, g);
-      atomicAdd(P.red + 1, dl);
-      atomicAdd(P.red + 2, rh);
-    }
+      dl += w * rv;
+      rh += P.diag[row] * rv * rv;
+    CG_ROWS_END
+    cta_partial(P.part, 2, g, dl, rh, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  const double bb = P.red[13];
   const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
-  double gprev = 1.0, aprev = 1.0, rho = 0.0;
+  double gprev = 1.0, aprev = 1.0, rho = 0.0, rho0 = -1.0;
   int it = 0;
   for (;; ++it) {
-    const int sl = it % 3;
-    const double gm = P.red[4 * sl], dl = P.red[4 * sl + 1];
-    rho = P.red[4 * sl + 2];
+    cta_total(P.part, 2 + (it & 1), tot, sh);
+    const double gm = tot[0], dl = tot[1];
+    rho = tot[2];
+    if (rho0 < 0.0) rho0 = rho;
     if (rho <= tol2 || it >= P.maxit || !(gm > 0.0)) break;
-    if (blockIdx.x == 0 && threadIdx.x < 4) P.red[4 * ((it + 2) % 3) + threadIdx.x] = 0.0;
     double beta, alpha;
     if (it == 0) {
       beta = 0.0;
@@ -247,62 +304,52 @@ __global__ void __launch_bounds__(256) k_cg(CgParams<T> P) {
       beta = gm / gprev;
       alpha = gm / (dl - beta * gm / aprev);
     }
-    const T a = static_cast<T>(alpha), bt = static_cast<T>(beta);
-    const T* wc = (it & 1) ? P.w1 : P.w0;
-    T* wn = (it & 1) ? P.w0 : P.w1;
+    const double* wc = (it & 1) ? P.w1 : P.w0;
+    double* wn = (it & 1) ? P.w0 : P.w1;
     double g2 = 0.0, d2 = 0.0, r2 = 0.0;
-    ROWS_BEGIN
-      const T nv = spmv_row(P, base, width, lane, wc);
-      const T wv = wc[row];
-      const T rv = P.r[row];
-      T zv, sv, pv;
+    CG_ROWS_BEGIN
+      const double nv = spmv64(P, base, width, lane, wc);
+      const double wv = wc[row];
+      const double rv = P.r[row];
+      double zv, sv, pv;
       if (it == 0) {
         zv = nv; sv = wv; pv = rv;
       } else {
-        zv = nv + bt * P.z[row];
-        sv = wv + bt * P.s[row];
-        pv = rv + bt * P.p[row];
+        zv = nv + beta * P.z[row];
+        sv = wv + beta * P.s[row];
+        pv = rv + beta * P.p[row];
       }
       P.z[row] = zv;
       P.s[row] = sv;
       P.p[row] = pv;
-      P.y[row] += a * pv;
-      const T rn = rv - a * sv;
-      const T wnv = wv - a * zv;
+      P.y[row] += alpha * pv;
+      const double rn = rv - alpha * sv;
+      const double wnv = wv - alpha * zv;
       P.r[row] = rn;
       wn[row] = wnv;
-      const double rd = static_cast<double>(rn);
-      g2 += rd * rd;
-      d2 += static_cast<double>(wnv) * rd;
-      r2 += static_cast<double>(P.diag[row]) * rd * rd;
-    ROWS_END
-    g2 = block_sum(g2, sh);
-    d2 = block_sum(d2, sh);
-    r2 = block_sum(r2, sh);
-    if (threadIdx.x == 0) {
-      const int ns = (it + 1) % 3;
-      atomicAdd(P.red + 4 * ns, g2);
-      atomicAdd(P.red + 4 * ns + 1, d2);
-      atomicAdd(P.red + 4 * ns + 2, r2);
-    }
+      g2 += rn * rn;
+      d2 += wnv * rn;
+      r2 += P.diag[row] * rn * rn;
+    CG_ROWS_END
+    // slot 2 + ((it + 1) & 1) was last read at the top of iteration it - 1, a barrier ago
+    cta_partial(P.part, 2 + ((it + 1) & 1), g2, d2, r2, 0.0, sh);
     gprev = gm;
     aprev = alpha;
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  // epilogue: x = D^-1/2 y (- mean)
   double sx = 0.0;
-  ROWS_BEGIN
-    const T xv = P.y[row] * P.sdinv[row];
+  CG_ROWS_BEGIN
+    const double xv = P.y[row] * P.sdinv[row];
     P.x[row] = xv;
-    sx += static_cast<double>(xv);
-  ROWS_END
+    sx += xv;
+  CG_ROWS_END
   if (P.project) {
-    sx = block_sum(sx, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 14, sx);
+    cta_partial(P.part, 0, sx, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
-    const T mx = static_cast<T>(P.red[14] / static_cast<double>(n));
-    ROWS_BEGIN P.x[row] -= mx;
-    ROWS_END
+    cta_total(P.part, 0, tot, sh);
+    const double mx = tot[0] / static_cast<double>(n);
+    CG_ROWS_BEGIN P.x[row] -= mx;
+    CG_ROWS_END
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *P.iters = it;
@@ -310,16 +357,15 @@ __global__ void __launch_bounds__(256) k_cg(CgParams<T> P) {
     atomicAdd(P.iters_acc, (unsigned long long)it);
     atomicAdd(P.iters_acc + 1, 1ull);
     atomicAdd(P.iters_acc + 2, 1ull);
+    if (bb > 0.0) {
+      atomicAdd(P.res_acc, sqrt(fmax(rho0, 0.0) / bb));
+      atomicAdd(P.res_acc + 1, sqrt(rho / bb));
+    }
   }
-#undef ROWS_BEGIN
-#undef ROWS_END
 }
 
-// ------------------------------------------------------------------ mixed-precision IR solve
-// FP32 systems: FP64 outer iterative refinement (true residual with FP64 values, FP64
-// solution kept between calls for warm starts) around an FP32 inner single-reduction
-// (Chronopoulos-Gear) CG, all inside one cooperative launch.  Per inner iteration two
-// grid barriers; per outer iteration three.
+// ------------------------------------------------------------------ FP32 CG inside FP64 refinement
+template <class TV>
 struct CgIrParams {
   int64_t n, nslices;
   const int64_t* sp;
@@ -328,22 +374,24 @@ struct CgIrParams {
   const double* v64;
   const double* sdinv;
   const double* diag;
-  const float* b;
-  float* x;
+  const TV* b;
+  TV* x;
   double *bh, *y;
   float *r, *p, *q, *s, *d;
-  double* red;  // [0] sum b, [1] ||b||^2, [2] sum x, [4..5] outer rho, [8..13] inner (gamma, delta) x 3
+  double* part;
   unsigned int* bar;
   int* err;
   int* iters;
   double* resid;
   unsigned long long* iters_acc;
+  double* res_acc;  // [0] sum of initial relative residuals, [1] sum of final ones
   double rtol, atol, inner_rtol;
   int maxit, max_outer, inner_maxit, warm, project;
 };
 
-__global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
-  __shared__ double sh[32];
+template <class TV>
+__global__ void __launch_bounds__(CG_BLOCK, 1) k_cg_ir(CgIrParams<TV> P) {
+  __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -351,50 +399,39 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
   unsigned int* cnt = P.bar;
   unsigned int* gen = P.bar + 1;
   const int64_t n = P.n;
-#define IR_ROWS_BEGIN                                               \
-  for (int64_t sl = gw; sl < P.nslices; sl += nw) {                 \
-    const int64_t row = sl * 32 + lane;                             \
-    const int64_t base = P.sp[sl];                                  \
-    const int width = static_cast<int>((P.sp[sl + 1] - base) >> 5); \
-    (void)base; (void)width;                                        \
-    if (row < n) {
-#define IR_ROWS_END \
-  }                 \
-  }
+  double tot[4];
+  double meanb = 0.0;
   if (P.project) {
     double part = 0.0;
-    IR_ROWS_BEGIN part += static_cast<double>(P.b[row]);
-    IR_ROWS_END
-    part = block_sum(part, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 0, part);
+    CG_ROWS_BEGIN part += static_cast<double>(P.b[row]);
+    CG_ROWS_END
+    cta_partial(P.part, 0, part, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    cta_total(P.part, 0, tot, sh);
+    meanb = tot[0] / static_cast<double>(n);
   }
-  const double meanb = P.project ? P.red[0] / static_cast<double>(n) : 0.0;
   {
     double bb = 0.0;
-    IR_ROWS_BEGIN
+    CG_ROWS_BEGIN
       const double bv = static_cast<double>(P.b[row]) - meanb;
       P.bh[row] = bv * P.sdinv[row];
       if (!P.warm) P.y[row] = 0.0;
       bb += bv * bv;
-    IR_ROWS_END
-    bb = block_sum(bb, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 1, bb);
+    CG_ROWS_END
+    cta_partial(P.part, 1, bb, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  const double bb = P.red[1];
+  cta_total(P.part, 1, tot, sh);
+  const double bb = tot[0];
   const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
-  int total = 0;
-  double rho = 0.0;
-  int outers = 0;
+  int total = 0, outers = 0;
+  double rho = 0.0, rho0 = -1.0;
   for (int outer = 0; outer < P.max_outer; ++outer) {
     ++outers;
-    const int so = 4 + (outer & 1);
-    // true residual in FP64; inner start r = p = r64 (float), d = 0
+    // true residual in FP64; inner start r = r64 (FP32), d = 0
     {
-      double rh = 0.0, g = 0.0;
-      if (blockIdx.x == 0 && threadIdx.x == 0) P.red[4 + ((outer + 1) & 1)] = 0.0;
-      IR_ROWS_BEGIN
+      double rh = 0.0;
+      CG_ROWS_BEGIN
         double acc = 0.0;
         for (int k = 0; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
@@ -402,21 +439,24 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
         }
         const double r64 = P.bh[row] - acc;
         rh += P.diag[row] * r64 * r64;
-        const float rf = static_cast<float>(r64);
-        P.r[row] = rf;
+        P.r[row] = static_cast<float>(r64);
         P.d[row] = 0.0f;
-        g += static_cast<double>(rf) * rf;
-      IR_ROWS_END
-      rh = block_sum(rh, sh);
-      if (threadIdx.x == 0) atomicAdd(P.red + so, rh);
+      CG_ROWS_END
+      cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
     }
-    rho = P.red[so];
+    cta_total(P.part, 0, tot, sh);
+    rho = tot[0];
+    if (rho0 < 0.0) rho0 = rho;
     if (rho <= tol2 || total >= P.maxit) break;
-    // s = A r, slot 0 <- (r,r), (r,s)
+    // reduce the residual only as far as the target needs (with a 0.3 margin), at most
+    // by inner_rtol per refinement step (the FP32 inner solve's reliable range)
+    const double need = 0.3 * sqrt(tol2 / rho);
+    const double itol = fmax(P.inner_rtol, fmin(need, 0.5));
+    // s = A r, slot 2 <- (r,r), (r,s)
     {
       double g = 0.0, dl = 0.0;
-      IR_ROWS_BEGIN
+      CG_ROWS_BEGIN
         float acc = 0.0f;
         for (int k = 0; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
@@ -426,23 +466,18 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
         const double rv = P.r[row];
         g += rv * rv;
         dl += rv * static_cast<double>(acc);
-      IR_ROWS_END
-      g = block_sum(g, sh);
-      dl = block_sum(dl, sh);
-      if (threadIdx.x == 0) {
-        atomicAdd(P.red + 8, g);
-        atomicAdd(P.red + 9, dl);
-      }
+      CG_ROWS_END
+      cta_partial(P.part, 2, g, dl, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
     }
-    const double g0 = P.red[8];
-    const double itol2 = P.inner_rtol * P.inner_rtol * g0;
-    double gprev = 1.0, aprev = 1.0;
+    double g0 = 0.0, gprev = 1.0, aprev = 1.0;
     for (int it = 0;; ++it) {
-      const int sl = it % 3;
-      const double gm = P.red[8 + 2 * sl], dl = P.red[9 + 2 * sl];
-      if (gm <= itol2 || it >= P.inner_maxit || total >= P.maxit || !(gm > 0.0) || !(dl > 0.0)) break;
-      if (blockIdx.x == 0 && threadIdx.x < 2) P.red[8 + 2 * ((it + 2) % 3) + threadIdx.x] = 0.0;
+      cta_total(P.part, 2 + (it & 1), tot, sh);
+      const double gm = tot[0], dl = tot[1];
+      if (it == 0) g0 = gm;
+      if (gm <= itol * itol * g0 || it >= P.inner_maxit || total >= P.maxit || !(gm > 0.0) ||
+          !(dl > 0.0))
+        break;
       double beta, alpha;
       if (it == 0) {
         beta = 0.0;
@@ -452,7 +487,7 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
         alpha = gm / (dl - beta * gm / aprev);
       }
       const float a = static_cast<float>(alpha), bt = static_cast<float>(beta);
-      IR_ROWS_BEGIN
+      CG_ROWS_BEGIN
         const float rv = P.r[row], sv = P.s[row];
         const float pv = (it == 0) ? rv : rv + bt * P.p[row];
         const float qv = (it == 0) ? sv : sv + bt * P.q[row];
@@ -460,10 +495,10 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
         P.q[row] = qv;
         P.d[row] += a * pv;
         P.r[row] = rv - a * qv;
-      IR_ROWS_END
+      CG_ROWS_END
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
       double g2 = 0.0, d2 = 0.0;
-      IR_ROWS_BEGIN
+      CG_ROWS_BEGIN
         float acc = 0.0f;
         for (int k = 0; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
@@ -473,61 +508,55 @@ __global__ void __launch_bounds__(256) k_cg_ir(CgIrParams P) {
         const double rv = P.r[row];
         g2 += rv * rv;
         d2 += rv * static_cast<double>(acc);
-      IR_ROWS_END
-      g2 = block_sum(g2, sh);
-      d2 = block_sum(d2, sh);
-      if (threadIdx.x == 0) {
-        const int ns = (it + 1) % 3;
-        atomicAdd(P.red + 8 + 2 * ns, g2);
-        atomicAdd(P.red + 9 + 2 * ns, d2);
-      }
+      CG_ROWS_END
+      // slot 2 + ((it+1)&1) was last read at the top of iteration it-1, two barriers ago
+      cta_partial(P.part, 2 + ((it + 1) & 1), g2, d2, 0.0, 0.0, sh);
       gprev = gm;
       aprev = alpha;
       ++total;
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
     }
-    // y += d ; reset the inner slots for the next refinement step
-    if (blockIdx.x == 0 && threadIdx.x < 6) P.red[8 + threadIdx.x] = 0.0;
-    IR_ROWS_BEGIN P.y[row] += static_cast<double>(P.d[row]);
-    IR_ROWS_END
+    CG_ROWS_BEGIN P.y[row] += static_cast<double>(P.d[row]);
+    CG_ROWS_END
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
   }
-  double sx = 0.0;
-  IR_ROWS_BEGIN sx += P.y[row] * P.sdinv[row];
-  IR_ROWS_END
   double mx = 0.0;
   if (P.project) {
-    sx = block_sum(sx, sh);
-    if (threadIdx.x == 0) atomicAdd(P.red + 2, sx);
+    double sx = 0.0;
+    CG_ROWS_BEGIN sx += P.y[row] * P.sdinv[row];
+    CG_ROWS_END
+    cta_partial(P.part, 1, sx, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
-    mx = P.red[2] / static_cast<double>(n);
+    cta_total(P.part, 1, tot, sh);
+    mx = tot[0] / static_cast<double>(n);
   }
-  IR_ROWS_BEGIN
+  CG_ROWS_BEGIN
     const double xv = P.y[row] * P.sdinv[row] - mx;
-    P.x[row] = static_cast<float>(xv);
+    P.x[row] = static_cast<TV>(xv);
     P.y[row] = xv / P.sdinv[row];
-  IR_ROWS_END
+  CG_ROWS_END
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *P.iters = total;
     *P.resid = bb > 0.0 ? sqrt(rho / bb) : 0.0;
     atomicAdd(P.iters_acc, (unsigned long long)total);
     atomicAdd(P.iters_acc + 1, (unsigned long long)outers);
     atomicAdd(P.iters_acc + 2, 1ull);
+    if (bb > 0.0) {
+      atomicAdd(P.res_acc, sqrt(fmax(rho0, 0.0) / bb));
+      atomicAdd(P.res_acc + 1, sqrt(rho / bb));
+    }
   }
-#undef IR_ROWS_BEGIN
-#undef IR_ROWS_END
 }
 
-template <class T>
-void CgSystem<T>::setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d) {
+// ------------------------------------------------------------------ CgSystem
+template <class TM>
+void CgSystem<TM>::setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d) {
   n = s.nrows;
   P.upload(s);
-  // scaled values: A_ij / sqrt(d_i d_j); rows are SELL rows, columns are system indices
-  std::vector<T> v(vals_sell.size()), sd(n), dd(n);
+  std::vector<double> v64(vals_sell.size(), 0.0), sd(n);
   for (int64_t i = 0; i < n; ++i) {
     SPX_CHECK(d[i] > 0.0, "CG system has a non-positive diagonal");
-    sd[i] = static_cast<T>(1.0 / std::sqrt(d[i]));
-    dd[i] = static_cast<T>(d[i]);
+    sd[i] = 1.0 / std::sqrt(d[i]);
   }
   for (int64_t sl = 0; sl < s.nslices; ++sl) {
     const int64_t w = (s.slice_ptr[sl + 1] - s.slice_ptr[sl]) / SELL_C;
@@ -535,103 +564,101 @@ void CgSystem<T>::setup(const HostSell& s, const std::vector<double>& vals_sell,
       for (int l = 0; l < SELL_C; ++l) {
         const int64_t idx = s.slice_ptr[sl] + k * SELL_C + l;
         const int64_t row = sl * SELL_C + l;
-        if (row >= n) { v[idx] = T(0); continue; }
-        const int64_t c = s.col[idx];
-        v[idx] = static_cast<T>(vals_sell[idx] / std::sqrt(d[row] * d[c]));
+        v64[idx] = (row < n) ? vals_sell[idx] * sd[row] * sd[s.col[idx]] : 0.0;
       }
   }
-  vals.upload(v);
-  sdinv.upload(sd);
-  diag.upload(dd);
-  work.alloc(7 * static_cast<size_t>(n));
-  if (sizeof(T) == sizeof(float)) {
-    std::vector<double> v64(v.size()), sd64(n), d64(d.begin(), d.begin() + n);
-    for (int64_t i = 0; i < n; ++i) sd64[i] = 1.0 / std::sqrt(d[i]);
-    for (int64_t sl = 0; sl < s.nslices; ++sl) {
-      const int64_t w = (s.slice_ptr[sl + 1] - s.slice_ptr[sl]) / SELL_C;
-      for (int64_t k = 0; k < w; ++k)
-        for (int l = 0; l < SELL_C; ++l) {
-          const int64_t idx = s.slice_ptr[sl] + k * SELL_C + l;
-          const int64_t row = sl * SELL_C + l;
-          v64[idx] = (row < n) ? vals_sell[idx] / std::sqrt(d[row] * d[s.col[idx]]) : 0.0;
-        }
-    }
+  std::vector<TM> vt(v64.begin(), v64.end());
+  vals.upload(vt);
+  sdinv64.upload(sd);
+  diag64.upload(d.data(), static_cast<size_t>(n));
+  if (sizeof(TM) == sizeof(float)) {
     vals64.upload(v64);
-    sdinv64.upload(sd64);
-    diag64.upload(d64);
     y64.alloc(n);
     y64.zero();
     bh64.alloc(n);
+    work.alloc(5 * static_cast<size_t>(n) * sizeof(float));
+  } else {
+    work.alloc(7 * static_cast<size_t>(n) * sizeof(double));
   }
-  red.alloc(16);
-  red.zero();
-  iters_acc.alloc(4);
-  iters_acc.zero();
   bar.alloc(2);
   err.alloc(1);
   iters.alloc(1);
   resid.alloc(1);
+  iters_acc.alloc(4);
+  iters_acc.zero();
+  res_acc.alloc(2);
+  res_acc.zero();
   int dev;
   SPX_CUDA(cudaGetDevice(&dev));
   int per_sm = 0;
-  SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg<T>, 256, 0));
-  if (sizeof(T) == sizeof(float)) {
-    int per_sm_ir = 0;
-    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ir, k_cg_ir, 256, 0));
-    per_sm = std::min(per_sm, per_sm_ir);
-  }
+  block = CG_BLOCK;
+  if (sizeof(TM) == sizeof(float))
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_ir<double>, CG_BLOCK, 0));
+  else
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg, CG_BLOCK, 0));
   SPX_CHECK(per_sm > 0, "CG kernel cannot be resident");
-  const int64_t want = (s.nslices * 32 + 255) / 256;
-  grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)per_sm * num_sms(dev))));
+  const int64_t want = (s.nslices * 32 + CG_BLOCK - 1) / CG_BLOCK;
+  grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, num_sms(dev))));
+  part.alloc(4 * 4 * static_cast<size_t>(grid));
 }
 
-template <class T>
-CgStats CgSystem<T>::solve(const T* b, T* x, double rtol, double atol, int maxit, bool warm, bool project,
-                           cudaStream_t st, bool sync_stats) {
-  CgParams<T> p;
-  p.n = n;
-  p.nslices = P.nslices;
-  p.sp = P.slice_ptr.p;
-  p.col = P.col.p;
-  p.val = vals.p;
-  p.sdinv = sdinv.p;
-  p.diag = diag.p;
-  p.b = b;
-  p.x = x;
-  T* W = work.p;
-  p.r = W; p.w0 = W + n; p.w1 = W + 2 * n; p.p = W + 3 * n; p.s = W + 4 * n; p.z = W + 5 * n; p.y = W + 6 * n;
-  p.red = red.p;
-  p.bar = bar.p;
-  p.err = err.p;
-  p.iters = iters.p;
-  p.resid = resid.p;
-  p.iters_acc = iters_acc.p;
-  p.rtol = rtol;
-  p.atol = atol;
-  p.maxit = maxit;
-  p.warm = warm ? 1 : 0;
-  p.project = project ? 1 : 0;
-  SPX_CUDA(cudaMemsetAsync(red.p, 0, red.bytes(), st));
+template <class TM>
+template <class TV>
+CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project,
+                            int slot, cudaStream_t st, bool sync_stats) {
+  const bool ir = sizeof(TM) == sizeof(float);
+  SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
+  if (slot >= 0) {
+    SPX_CHECK(slot < 4, "extrapolation slot out of range");
+    for (int k = 0; k < 3; ++k)
+      if (!hist[slot][k].n) hist[slot][k].alloc(n);
+    if (hcount[slot] > 0) {
+      const int h0 = (hhead[slot] + 2) % 3, h1 = (hhead[slot] + 1) % 3, h2 = hhead[slot];
+      double* target = ir ? y64.p : reinterpret_cast<double*>(x);
+      k_extrap<double><<<grid_for(n, 256), 256, 0, st>>>(n, hist[slot][h0].p, hist[slot][h1].p, hist[slot][h2].p,
+                                                         hcount[slot], target);
+      SPX_LAUNCH_CHECK();
+      warm = true;
+    }
+  }
   SPX_CUDA(cudaMemsetAsync(bar.p, 0, bar.bytes(), st));
   SPX_CUDA(cudaMemsetAsync(err.p, 0, err.bytes(), st));
-  if (sizeof(T) == sizeof(float)) {
-    CgIrParams q;
+  if (ir) {
+    CgIrParams<TV> q;
     q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
     q.v32 = reinterpret_cast<const float*>(vals.p); q.v64 = vals64.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
-    q.b = reinterpret_cast<const float*>(b); q.x = reinterpret_cast<float*>(x);
+    q.b = b; q.x = x;
     q.bh = bh64.p; q.y = y64.p;
     float* Wf = reinterpret_cast<float*>(work.p);
     q.r = Wf; q.p = Wf + n; q.q = Wf + 2 * n; q.s = Wf + 3 * n; q.d = Wf + 4 * n;
-    q.red = red.p; q.bar = bar.p; q.err = err.p; q.iters = iters.p; q.resid = resid.p;
+    q.part = part.p; q.bar = bar.p; q.err = err.p; q.iters = iters.p; q.resid = resid.p;
     q.iters_acc = iters_acc.p;
+    q.res_acc = res_acc.p;
     q.rtol = rtol; q.atol = atol; q.inner_rtol = inner_rtol;
     q.maxit = maxit; q.max_outer = max_outer; q.inner_maxit = maxit; q.warm = warm ? 1 : 0;
     q.project = project ? 1 : 0;
     void* a2[] = {&q};
-    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_ir), dim3(grid), dim3(256), a2, 0, st));
+    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_ir<TV>), dim3(grid), dim3(block), a2, 0, st));
   } else {
+    CgParams p;
+    p.n = n; p.nslices = P.nslices; p.sp = P.slice_ptr.p; p.col = P.col.p;
+    p.val = reinterpret_cast<const double*>(vals.p); p.sdinv = sdinv64.p; p.diag = diag64.p;
+    p.b = reinterpret_cast<const double*>(b); p.x = reinterpret_cast<double*>(x);
+    double* W = reinterpret_cast<double*>(work.p);
+    p.r = W; p.w0 = W + n; p.w1 = W + 2 * n; p.p = W + 3 * n; p.s = W + 4 * n; p.z = W + 5 * n; p.y = W + 6 * n;
+    p.part = part.p; p.bar = bar.p; p.err = err.p; p.iters = iters.p; p.resid = resid.p;
+    p.iters_acc = iters_acc.p;
+    p.res_acc = res_acc.p;
+    p.rtol = rtol; p.atol = atol; p.maxit = maxit; p.warm = warm ? 1 : 0; p.project = project ? 1 : 0;
     void* args[] = {&p};
-    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg<T>), dim3(grid), dim3(256), args, 0, st));
+    SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg), dim3(grid), dim3(block), args, 0, st));
+  }
+  if (slot >= 0) {
+    double* dst = hist[slot][hhead[slot]].p;
+    const double* src = ir ? y64.p : reinterpret_cast<const double*>(x);
+    SPX_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    hhead[slot] = (hhead[slot] + 1) % 3;
+    hcount[slot] = std::min(3, hcount[slot] + 1);
   }
   CgStats out;
   if (sync_stats) {
@@ -651,11 +678,17 @@ CgStats CgSystem<T>::solve(const T* b, T* x, double rtol, double atol, int maxit
 
 template struct CgSystem<double>;
 template struct CgSystem<float>;
+template CgStats CgSystem<double>::solve<double>(const double*, double*, double, double, int, bool, bool, int,
+                                                 cudaStream_t, bool);
+template CgStats CgSystem<float>::solve<double>(const double*, double*, double, double, int, bool, bool, int,
+                                                cudaStream_t, bool);
+template CgStats CgSystem<float>::solve<float>(const float*, float*, double, double, int, bool, bool, int,
+                                               cudaStream_t, bool);
 
 // ------------------------------------------------------------------ demag context
-template <class T>
-void DemagCtx<T>::create(const double* X, int64_t N_, const int32_t* tets, int64_t E_, double Ms_,
-                         const DemagOptions& o, cudaStream_t s) {
+template <class TV, class TM>
+void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, int64_t E_, double Ms_,
+                              const DemagOptions& o, cudaStream_t s) {
   SPX_CUDA(cudaGetDevice(&device));
   N = N_;
   E = E_;
@@ -665,26 +698,27 @@ void DemagCtx<T>::create(const double* X, int64_t N_, const int32_t* tets, int64
   Nb = bd.host.Nb;
   assemble_fem(X, N, tets, E, fem);
   const int64_t nnz = fem.rowptr[N];
-  // full pattern
   std::vector<int32_t> all(N);
   for (int64_t i = 0; i < N; ++i) all[i] = static_cast<int32_t>(i);
   build_sell(fem.rowptr, fem.col, all, nullptr, hsell);
   P.upload(hsell, s);
-  const int64_t L = hsell.slice_ptr.back();
   {
-    std::vector<T> v;
-    sell_values<T>(hsell, fem.Div.data(), 3, true, nnz, Ms, v);
+    std::vector<TM> v;
+    sell_values<TM>(hsell, fem.Div.data(), 3, true, nnz, Ms, v);
     Div.upload(v, s);
-    // G / vol_i : scale per CSR row
+    std::vector<double> ds(3 * N, 0.0);
+    for (int64_t i = 0; i < N; ++i)
+      for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
+        for (int c = 0; c < 3; ++c) ds[c * N + i] += Ms * fem.Div[3 * k + c];
+    Dsum.upload(ds, s);
     std::vector<double> g = fem.G;
     for (int64_t i = 0; i < N; ++i)
       for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
         for (int c = 0; c < 3; ++c) g[3 * k + c] /= fem.vol[i];
-    sell_values<T>(hsell, g.data(), 3, true, nnz, 1.0, v);
+    sell_values<TM>(hsell, g.data(), 3, true, nnz, 1.0, v);
     Gv.upload(v, s);
   }
   vol.upload(fem.vol, s);
-  // u1 system: full stiffness
   {
     std::vector<double> a;
     sell_values<double>(hsell, fem.A.data(), 1, true, nnz, 1.0, a);
@@ -694,7 +728,6 @@ void DemagCtx<T>::create(const double* X, int64_t N_, const int32_t* tets, int64
         if (fem.col[k] == i) d[i] = fem.A[k];
     cg1.setup(hsell, a, d);
   }
-  // interior / boundary split for u2
   std::vector<int32_t> bmap(N, -1), imap(N, -1), inter;
   for (int64_t k = 0; k < Nb; ++k) bmap[bd.host.bverts[k]] = static_cast<int32_t>(k);
   for (int64_t i = 0; i < N; ++i)
@@ -711,8 +744,7 @@ void DemagCtx<T>::create(const double* X, int64_t N_, const int32_t* tets, int64
     build_sell(fem.rowptr, fem.col, inter, &bmap, sIB);
     std::vector<double> aII, aIB;
     sell_values<double>(sII, fem.A.data(), 1, true, nnz, 1.0, aII);
-    std::vector<T> vIB;
-    sell_values<T>(sIB, fem.A.data(), 1, true, nnz, 1.0, vIB);
+    sell_values<double>(sIB, fem.A.data(), 1, true, nnz, 1.0, aIB);
     std::vector<double> d(NI);
     for (int64_t q = 0; q < NI; ++q) {
       const int64_t i = inter[q];
@@ -721,97 +753,94 @@ void DemagCtx<T>::create(const double* X, int64_t N_, const int32_t* tets, int64
     }
     cg2.setup(sII, aII, d);
     PIB.upload(sIB, s);
-    AIB.upload(vIB, s);
+    AIB.upload(aIB, s);
   }
-  // boundary operator
   if (opt.backend == 0) {
     SPX_CHECK(Nb * Nb * 8 <= (int64_t)64 * 1024 * 1024 * 1024, "dense boundary operator too large");
     Bdense.alloc(static_cast<size_t>(Nb * Nb));
     bd.dense_B(Bdense.p, s);
   } else {
     H.build(bd, opt.hcfg, s);
-    H.pack(opt.prec, s);
+    H.pack(opt.hprec, s);
   }
-  b.alloc(N); u1.alloc(N); phi.alloc(N); gB.alloc(Nb); xb.alloc(Nb); yb.alloc(Nb);
+  b.alloc(N); u1.alloc(N); phi.alloc(N); gB.alloc(Nb); xb.alloc(Nb);
   bI.alloc(std::max<int64_t>(NI, 1));
   xI.alloc(std::max<int64_t>(NI, 1));
   u1.zero(s);
   xI.zero(s);
-  sum.alloc(4);
   SPX_CUDA(cudaStreamSynchronize(s));
 }
 
-template <class T>
-void DemagCtx<T>::potential(const T* m, cudaStream_t s, bool sync_stats) {
+template <class TV, class TM>
+void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, int slot) {
   const int threads = 256;
-  const unsigned gsl = grid_for(P.nslices * 32, threads);
+  const bool warm = opt.warm_start != 0;
+  const int sl = (opt.warm_start == 2) ? slot : -1;
   prof.mark(PC_DIV, s);
-  k_div<T><<<gsl, threads, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Div.p, P.len, m, b.p, nullptr);
+  k_div<TV, TM><<<grid_for(P.nslices * 32, threads), threads, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Div.p,
+                                                                     P.len, Dsum.p, m, b.p);
   SPX_LAUNCH_CHECK();
   prof.mark(PC_DIV, s);
   prof.launches[PC_DIV] += 1;
   prof.mark(PC_CG1, s);
-  last1 = cg1.solve(b.p, u1.p, opt.rtol_u1, opt.atol, opt.maxit_u1, opt.warm_start != 0, true, s, sync_stats);
+  last1 = cg1.template solve<TV>(b.p, u1.p, opt.rtol_u1, opt.atol, opt.maxit_u1, warm, true, sl, s, sync_stats);
   prof.mark(PC_CG1, s);
-  prof.launches[PC_CG1] += 1;
+  prof.launches[PC_CG1] += 1 + (sl >= 0 && cg1.hcount[sl] > 1 ? 1 : 0);
   prof.mark(PC_BND, s);
   if (opt.backend == 0) {
-    k_gather_idx<T><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, bverts.p, u1.p, xb.p);
+    k_gather_idx<TV><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, bverts.p, u1.p, xb.p);
     SPX_LAUNCH_CHECK();
-    k_dense_gemv<T><<<grid_for(Nb * 32, 256), 256, 0, s>>>(Nb, Bdense.p, xb.p, bverts.p, u1.p, phi.p, gB.p);
+    k_dense_gemv<TV><<<grid_for(Nb * 32, 256), 256, 0, s>>>(Nb, Bdense.p, xb.p, bverts.p, u1.p, phi.p, gB.p);
     SPX_LAUNCH_CHECK();
     prof.launches[PC_BND] += 2;
   } else {
-    H.apply_gather<T>(u1.p, bverts.p, phi.p, u1.p, gB.p, s);
+    H.apply_gather<TV>(u1.p, bverts.p, phi.p, u1.p, gB.p, s);
     prof.launches[PC_BND] += H.n_far > 0 ? 3 : 2;
   }
   prof.mark(PC_BND, s);
   if (NI > 0) {
     prof.mark(PC_U2RHS, s);
-    k_u2rhs<T><<<grid_for(PIB.nslices * 32, threads), threads, 0, s>>>(NI, PIB.nslices, PIB.slice_ptr.p,
-                                                                         PIB.col.p, AIB.p, gB.p, bI.p);
+    k_u2rhs<TV><<<grid_for(PIB.nslices * 32, threads), threads, 0, s>>>(NI, PIB.nslices, PIB.slice_ptr.p,
+                                                                          PIB.col.p, AIB.p, gB.p, bI.p);
     SPX_LAUNCH_CHECK();
     prof.mark(PC_U2RHS, s);
     prof.launches[PC_U2RHS] += 1;
     // ||b|| of the reference's full u2 system includes the boundary rows (b[bnd] = g);
     // the interior test is slightly stricter, which only tightens the solve.
     prof.mark(PC_CG2, s);
-    last2 = cg2.solve(bI.p, xI.p, opt.rtol_u2, opt.atol, opt.maxit_u2, opt.warm_start != 0, false, s, sync_stats);
+    last2 = cg2.template solve<TV>(bI.p, xI.p, opt.rtol_u2, opt.atol, opt.maxit_u2, warm, false, sl, s,
+                                   sync_stats);
     prof.mark(PC_CG2, s);
-    prof.launches[PC_CG2] += 1;
+    prof.launches[PC_CG2] += 1 + (sl >= 0 && cg2.hcount[sl] > 1 ? 1 : 0);
     prof.mark(PC_PHI, s);
-    k_phi_interior<T><<<grid_for(NI, 256), 256, 0, s>>>(NI, interior.p, u1.p, xI.p, phi.p);
+    k_phi_interior<TV><<<grid_for(NI, 256), 256, 0, s>>>(NI, interior.p, u1.p, xI.p, phi.p);
     SPX_LAUNCH_CHECK();
     prof.mark(PC_PHI, s);
     prof.launches[PC_PHI] += 1;
   }
-  launches += 4 + (opt.backend == 0 ? 2 : (H.n_far > 0 ? 3 : 2)) + (NI > 0 ? 3 : 0) - 1;
   ++applies;
 }
 
-template <class T>
-void DemagCtx<T>::field(T* Hout, cudaStream_t s) {
-  k_grad<T><<<grid_for(P.nslices * 32, 256), 256, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Gv.p, P.len,
-                                                           phi.p, Hout);
+template <class TV, class TM>
+void DemagCtx<TV, TM>::field(TV* Hout, cudaStream_t s) {
+  k_grad<TV, TM><<<grid_for(P.nslices * 32, 256), 256, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Gv.p, P.len,
+                                                               phi.p, Hout);
   SPX_LAUNCH_CHECK();
 }
 
-template <class T>
-int64_t DemagCtx<T>::device_bytes() const {
+template <class TV, class TM>
+int64_t DemagCtx<TV, TM>::device_bytes() const {
   int64_t tot = 0;
-  tot += P.slice_ptr.bytes() + P.col.bytes() + Div.bytes() + Gv.bytes() + vol.bytes();
-  tot += cg1.vals.bytes() + cg1.work.bytes() + cg1.P.col.bytes() + cg2.vals.bytes() + cg2.work.bytes() +
-         cg2.P.col.bytes();
+  tot += P.slice_ptr.bytes() + P.col.bytes() + Div.bytes() + Dsum.bytes() + Gv.bytes() + vol.bytes();
+  tot += cg1.vals.bytes() + cg1.vals64.bytes() + cg1.work.bytes() + cg1.P.col.bytes();
+  tot += cg2.vals.bytes() + cg2.vals64.bytes() + cg2.work.bytes() + cg2.P.col.bytes();
   tot += AIB.bytes() + PIB.col.bytes() + Bdense.bytes();
   tot += H.device_bytes();
   return tot;
 }
 
-template struct DemagCtx<double>;
-template struct DemagCtx<float>;
-
-// explicit instantiations used by llg.cu
-template __global__ void k_gather_idx<double>(int64_t, const int32_t*, const double*, double*);
-template __global__ void k_gather_idx<float>(int64_t, const int32_t*, const float*, float*);
+template struct DemagCtx<double, double>;
+template struct DemagCtx<float, float>;
+template struct DemagCtx<double, float>;
 
 }  // namespace spx

@@ -1,4 +1,13 @@
-// FEM operators on the device, the persistent CG solver and the demag pipeline.
+// FEM operators on the device, the persistent CG solvers and the demag pipeline.
+//
+// Precision: DemagCtx<TV, TM> keeps nodal vectors (m, u1, u2, phi, b, g) in TV and the large
+// matrices (Div, G/V, the CG values) in TM.
+//   <double, double>  FP64 everywhere, pipelined FP64 CG
+//   <float,  float>   plain FP32 (FP32 CG inside FP64 iterative refinement, FP32 vectors)
+//   <double, float>   mixed: FP64 vectors, FP32 matrices, FP32 inner CG + FP64 refinement
+// Operators whose rows sum to zero (G, exchange) are applied in difference form
+// sum_j a_ij (v_j - v_i), and Div as sum_j D_ij (m_j - m_i) + (sum_j D_ij) m_i, so a
+// rounded matrix value multiplies a small nodal difference instead of a large value.
 #pragma once
 
 #include "hmat.cuh"
@@ -9,33 +18,6 @@ struct CgStats {
   int64_t iterations = 0;
   double rel_residual = 0.0;
   int converged = 0;
-};
-
-// Scaled SPD system  A^ = D^-1/2 A D^-1/2  on a SELL-32 pattern, solved by a pipelined
-// CG (one grid barrier per iteration) in one cooperative launch.
-template <class T>
-struct CgSystem {
-  int64_t n = 0;
-  DevSell<T> P;
-  DevBuf<T> vals;    // scaled values
-  DevBuf<T> sdinv;   // 1/sqrt(d)
-  DevBuf<T> diag;    // d (for the unscaled residual norm)
-  DevBuf<T> work;    // 7 vectors of n
-  DevBuf<double> red;
-  DevBuf<unsigned int> bar;
-  DevBuf<int> err;
-  DevBuf<int> iters;
-  DevBuf<double> resid;
-  DevBuf<unsigned long long> iters_acc;
-  // FP32 systems: FP64 values and state for the iterative-refinement solve
-  DevBuf<double> vals64, sdinv64, diag64, y64, bh64;
-  double inner_rtol = 1e-3;
-  int max_outer = 8;
-  int grid = 0;
-  void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
-  // solve A x = b; x holds the initial guess if warm; project: remove the constant null space
-  CgStats solve(const T* b, T* x, double rtol, double atol, int maxit, bool warm, bool project,
-                cudaStream_t st, bool sync_stats = true);
 };
 
 // Per-category CUDA-event timing of the demag/LLG pipeline (enabled on demand; events
@@ -82,16 +64,57 @@ struct Profiler {
   }
 };
 
+// Scaled SPD system  A^ = D^-1/2 A D^-1/2  on a SELL-32 pattern solved in one cooperative
+// launch: TM = double -> pipelined FP64 CG (one grid barrier per iteration); TM = float ->
+// FP32 single-reduction CG inside FP64 iterative refinement (FP64 values kept for the
+// true residual, FP64 solution state kept between calls).
+//
+// Starting guesses: with `slot` >= 0 the solver keeps the last three solutions returned
+// for that slot (e.g. one slot per RK stage) and starts from their quadratic
+// extrapolation 3 x1 - 3 x2 + x3 (linear / constant while fewer are stored).  The stopping
+// rule does not change; only the iteration count does.
+template <class TM>
+struct CgSystem {
+  int64_t n = 0;
+  DevSell<TM> P;
+  DevBuf<TM> vals;     // scaled values
+  DevBuf<double> vals64, sdinv64, diag64, y64, bh64;  // FP64 data of the refinement solve
+  DevBuf<TM> sdinv;    // 1/sqrt(d) (pipelined FP64 path)
+  DevBuf<TM> diag;
+  DevBuf<char> work;   // solver vectors
+  DevBuf<double> part;  // per-CTA partial sums [3 slots][grid][4]
+  DevBuf<double> red;   // scalars
+  DevBuf<unsigned int> bar;
+  DevBuf<int> err;
+  DevBuf<int> iters;
+  DevBuf<double> resid;
+  DevBuf<unsigned long long> iters_acc;  // [0] inner iterations, [1] refinement steps, [2] solves
+  DevBuf<double> res_acc;                // [0] sum of initial, [1] sum of final relative residuals
+  DevBuf<double> hist[4][3];
+  int hcount[4] = {0, 0, 0, 0}, hhead[4] = {0, 0, 0, 0};
+  double inner_rtol = 1e-3;
+  int max_outer = 10;
+  int grid = 0, block = 0;
+  void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
+  template <class TV>
+  CgStats solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, int slot,
+                cudaStream_t st, bool sync_stats);
+  void reset_history() {
+    for (int s = 0; s < 4; ++s) hcount[s] = hhead[s] = 0;
+  }
+};
+
 struct DemagOptions {
   int backend = 0;          // 0 dense, 1 hmatrix
-  Prec prec = Prec::F64;    // vector / solver precision (F64 or F32) and H storage
+  Prec prec = Prec::F64;    // vector / matrix precision of the pipeline
+  Prec hprec = Prec::F64;   // storage precision of the H-matrix factors
   double rtol_u1 = 1e-6, rtol_u2 = 1e-6, atol = 1e-12;
   int maxit_u1 = 2000, maxit_u2 = 12000;
-  int warm_start = 0;
+  int warm_start = 0;       // 0 zero start, 1 previous solution, 2 extrapolated per RK stage
   HBuildConfig hcfg;
 };
 
-template <class T>
+template <class TV, class TM>
 struct DemagCtx {
   int device = 0;
   int64_t N = 0, E = 0, Nb = 0, NI = 0;
@@ -99,31 +122,29 @@ struct DemagCtx {
   DemagOptions opt;
   BoundaryDev bd;
   HostFem fem;
-  // full pattern (all nodes)
   HostSell hsell;
-  DevSell<T> P;
-  DevBuf<T> Div;        // 3 planes, Ms * int grad v . m
-  DevBuf<T> Gv;         // 3 planes, G / vol_i  (H = Gv phi)
-  DevBuf<double> vol;   // lumped nodal volume
+  DevSell<TM> P;
+  DevBuf<TM> Div;        // 3 planes, Ms * int grad v . m
+  DevBuf<double> Dsum;   // [3][N] row sums of Div (boundary flux terms)
+  DevBuf<TM> Gv;         // 3 planes, G / vol_i
+  DevBuf<double> vol;
   DevBuf<int32_t> interior, bverts;
-  CgSystem<T> cg1, cg2;
-  DevSell<T> PIB;       // interior rows x boundary columns
-  DevBuf<T> AIB;
+  CgSystem<TM> cg1, cg2;
+  DevSell<TM> PIB;
+  DevBuf<double> AIB;    // interior rows x boundary columns, FP64
   DevBuf<double> Bdense;
   HMatrix H;
-  // work
-  DevBuf<T> b, u1, phi, gB, bI, xI, xb, yb;
-  DevBuf<double> sum;
+  DevBuf<TV> b, u1, phi, gB, bI, xI, xb;
   CgStats last1, last2;
   int64_t applies = 0;
   Profiler prof;
   int64_t launches = 0;
   void create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms, const DemagOptions& o,
               cudaStream_t s);
-  // potential phi = u1 + u2 for magnetisation m (AoS, T)
-  void potential(const T* m, cudaStream_t s, bool sync_stats);
+  // potential phi = u1 + u2 for magnetisation m (AoS, TV); slot: RK stage for extrapolated starts
+  void potential(const TV* m, cudaStream_t s, bool sync_stats, int slot = -1);
   // H_demag = G phi / vol (AoS)
-  void field(T* H, cudaStream_t s);
+  void field(TV* H, cudaStream_t s);
   int64_t device_bytes() const;
 };
 

@@ -36,15 +36,19 @@ template <> __device__ __forceinline__ double cvt<double, __nv_bfloat16>(__nv_bf
 
 // ------------------------------------------------------------------ packing
 struct PackFar {
-  int64_t src_u, src_v, dst;  // element offsets
-  int32_t m, n, k;
+  int64_t src_u, src_v, dst_u, dst_v;  // element offsets
+  int32_t m, n, k, ldv;
 };
+// U^T (k x m) as is; V (k x n) into rows of ldv elements (ldv = n rounded up to 8), zero padded
 template <class TF>
 __global__ void k_pack_far(const PackFar* __restrict__ jobs, const double* __restrict__ pool, TF* __restrict__ out) {
   const PackFar j = jobs[blockIdx.x];
-  const int64_t lu = (int64_t)j.k * j.m, lv = (int64_t)j.k * j.n;
-  for (int64_t e = threadIdx.x; e < lu; e += blockDim.x) out[j.dst + e] = from_d<TF>(pool[j.src_u + e]);
-  for (int64_t e = threadIdx.x; e < lv; e += blockDim.x) out[j.dst + lu + e] = from_d<TF>(pool[j.src_v + e]);
+  const int64_t lu = (int64_t)j.k * j.m, lv = (int64_t)j.k * j.ldv;
+  for (int64_t e = threadIdx.x; e < lu; e += blockDim.x) out[j.dst_u + e] = from_d<TF>(pool[j.src_u + e]);
+  for (int64_t e = threadIdx.x; e < lv; e += blockDim.x) {
+    const int64_t q = e / j.ldv, c = e - q * j.ldv;
+    out[j.dst_v + e] = (c < j.n) ? from_d<TF>(pool[j.src_v + q * j.n + c]) : from_d<TF>(0.0);
+  }
 }
 struct PackNear {
   int64_t src, dst;
@@ -72,26 +76,82 @@ __global__ void k_hgather(int64_t Nb, const TS* __restrict__ src, const int32_t*
   xp[i] = static_cast<TX>(src[o]);
 }
 
+// 16-byte vector loads of far factors
+template <class TF> struct V16;
+template <> struct V16<double> { using T = double2; static constexpr int E = 2; };
+template <> struct V16<float> { using T = float4; static constexpr int E = 4; };
+template <> struct V16<__nv_bfloat16> { using T = uint4; static constexpr int E = 8; };
+
+template <class TA, class TF>
+__device__ __forceinline__ void v16_elems(const typename V16<TF>::T& v, TA out[V16<TF>::E]);
+template <>
+__device__ __forceinline__ void v16_elems<double, double>(const double2& v, double out[2]) { out[0] = v.x; out[1] = v.y; }
+template <>
+__device__ __forceinline__ void v16_elems<float, double>(const double2& v, float out[2]) {
+  out[0] = static_cast<float>(v.x); out[1] = static_cast<float>(v.y);
+}
+template <>
+__device__ __forceinline__ void v16_elems<double, float>(const float4& v, double out[4]) {
+  out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void v16_elems<float, float>(const float4& v, float out[4]) {
+  out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+}
+template <class TA>
+__device__ __forceinline__ void bf16x8(const uint4& v, TA out[8]) {
+  const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    out[2 * q] = static_cast<TA>(__uint_as_float(w[q] << 16));
+    out[2 * q + 1] = static_cast<TA>(__uint_as_float(w[q] & 0xffff0000u));
+  }
+}
+template <>
+__device__ __forceinline__ void v16_elems<double, __nv_bfloat16>(const uint4& v, double out[8]) { bf16x8<double>(v, out); }
+template <>
+__device__ __forceinline__ void v16_elems<float, __nv_bfloat16>(const uint4& v, float out[8]) { bf16x8<float>(v, out); }
+
+// z_b = V_b x~_{J_b}: one CTA per far block; V rows (ldv elements, zero padded, 16-byte aligned)
+// are read as 16-byte vectors by groups of G lanes (G = chunks per row rounded to a power of
+// two, at most 32), groups reduce with shuffles.
 template <class TF, class TA, class TX>
 __global__ void __launch_bounds__(128) k_far_z(const int32_t* __restrict__ meta, const int64_t* __restrict__ voff,
                                                const int64_t* __restrict__ zoff, const TF* __restrict__ F,
                                                const TX* __restrict__ xp, TA* __restrict__ z) {
+  constexpr int E = V16<TF>::E;
+  using VT = typename V16<TF>::T;
   const int b = blockIdx.x;
-  const int cs = meta[5 * b + 2], n = meta[5 * b + 3], k = meta[5 * b + 4];
-  const TF* V = F + voff[b];
+  const int cs = meta[6 * b + 2], n = meta[6 * b + 3], k = meta[6 * b + 4], ldv = meta[6 * b + 5];
+  const VT* V = reinterpret_cast<const VT*>(F + voff[b]);
   const TX* x = xp + cs;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int q = w; q < k; q += nw) {
-    const TF* row = V + (int64_t)q * n;
+  const int nch = ldv / E;
+  int G = 1;
+  while (G < nch && G < 32) G <<= 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int gpw = 32 / G;                // groups per warp
+  const int gl = lane % G, gw = lane / G;
+  for (int qb = warp * gpw; qb < k; qb += nwarps * gpw) {
+    const int q = qb + gw;
     TA acc = 0;
-    for (int j = lane; j < n; j += 32) acc += cvt<TA>(row[j]) * static_cast<TA>(x[j]);
+    if (q < k) {
+      const VT* row = V + (int64_t)q * nch;
+      for (int c = gl; c < nch; c += G) {
+        const VT v = row[c];
+        TA e[E];
+        v16_elems<TA, TF>(v, e);
+        const int j0 = c * E;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) z[zoff[b] + q] = acc;
+        for (int t = 0; t < E; ++t)
+          if (j0 + t < n) acc += e[t] * static_cast<TA>(x[j0 + t]);
+      }
+    }
+    for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (q < k && gl == 0) z[zoff[b] + q] = acc;
   }
 }
 
-constexpr int ROWS_GROUPS = 2;
+constexpr int ROWS_GROUPS = 4;
 constexpr int ROWS_GSIZE = 64;
 
 template <class TF, class TN, class TA, class TX, class TD>
@@ -118,14 +178,21 @@ __global__ void __launch_bounds__(ROWS_GROUPS * ROWS_GSIZE) k_rows(
     const int32_t code = items[it];
     const int32_t bi = code >> 1;
     if (code & 1) {
-      const int rs = far_meta[5 * bi], m = far_meta[5 * bi + 1], k = far_meta[5 * bi + 4];
+      const int rs = far_meta[6 * bi], m = far_meta[6 * bi + 1], k = far_meta[6 * bi + 4];
       const TF* Ut = F + far_uoff[bi];
       const TA* zb = z + far_zoff[bi];
       for (int r = t; r < nr; r += ROWS_GSIZE) {
-        const int lr = r0 + r - rs;
-        TA s = 0;
-        for (int q = 0; q < k; ++q) s += cvt<TA>(Ut[(int64_t)q * m + lr]) * zb[q];
-        acc[g * nr + r] += s;
+        const TF* u = Ut + (r0 + r - rs);
+        TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int q = 0;
+        for (; q + 4 <= k; q += 4) {
+          s0 += cvt<TA>(u[(int64_t)q * m]) * zb[q];
+          s1 += cvt<TA>(u[(int64_t)(q + 1) * m]) * zb[q + 1];
+          s2 += cvt<TA>(u[(int64_t)(q + 2) * m]) * zb[q + 2];
+          s3 += cvt<TA>(u[(int64_t)(q + 3) * m]) * zb[q + 3];
+        }
+        for (; q < k; ++q) s0 += cvt<TA>(u[(int64_t)q * m]) * zb[q];
+        acc[g * nr + r] += (s0 + s1) + (s2 + s3);
       }
     } else {
       const int rs = near_meta[4 * bi], m = near_meta[4 * bi + 1], cs = near_meta[4 * bi + 2],
@@ -133,9 +200,17 @@ __global__ void __launch_bounds__(ROWS_GROUPS * ROWS_GSIZE) k_rows(
       const TN* tile = Nt + near_off[bi];
       const TX* x = xp + cs;
       for (int r = t; r < nr; r += ROWS_GSIZE) {
-        const int lr = r0 + r - rs;
-        TA s = 0;
-        for (int c = 0; c < n; ++c) s += cvt<TA>(tile[(int64_t)c * m + lr]) * static_cast<TA>(x[c]);
+        const TN* u = tile + (r0 + r - rs);
+        TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int c = 0;
+        for (; c + 4 <= n; c += 4) {
+          s0 += cvt<TA>(u[(int64_t)c * m]) * static_cast<TA>(x[c]);
+          s1 += cvt<TA>(u[(int64_t)(c + 1) * m]) * static_cast<TA>(x[c + 1]);
+          s2 += cvt<TA>(u[(int64_t)(c + 2) * m]) * static_cast<TA>(x[c + 2]);
+          s3 += cvt<TA>(u[(int64_t)(c + 3) * m]) * static_cast<TA>(x[c + 3]);
+        }
+        for (; c < n; ++c) s0 += cvt<TA>(u[(int64_t)c * m]) * static_cast<TA>(x[c]);
+        const TA s = (s0 + s1) + (s2 + s3);
         if (kahan) {
           const TA y = s - cmp[g * nr + r];
           const TA tt = acc[g * nr + r] + y;
@@ -175,12 +250,15 @@ void do_pack(HMatrix& H, cudaStream_t s) {
     const HBlock& b = H.blocks[q];
     const int32_t m = b.re - b.rs, n = b.ce - b.cs;
     if (b.type == 1) {
-      pf.push_back(PackFar{b.off_u, b.off_v, fpos, m, n, b.rank});
-      fmeta.insert(fmeta.end(), {b.rs, m, b.cs, n, b.rank});
-      fu.push_back(fpos);
-      fv.push_back(fpos + (int64_t)b.rank * m);
+      const int32_t ldv = (n + 7) / 8 * 8;
+      const int64_t pu = fpos;
+      const int64_t pv = (pu + (int64_t)b.rank * m + 7) / 8 * 8;  // 16-byte aligned V rows
+      pf.push_back(PackFar{b.off_u, b.off_v, pu, pv, m, n, b.rank, ldv});
+      fmeta.insert(fmeta.end(), {b.rs, m, b.cs, n, b.rank, ldv});
+      fu.push_back(pu);
+      fv.push_back(pv);
       fz.push_back(zpos);
-      fpos += (int64_t)b.rank * (m + n);
+      fpos = pv + (int64_t)b.rank * ldv;
       zpos += b.rank;
       code_of[q] = (nf++ << 1) | 1;
     } else {
@@ -269,7 +347,7 @@ void do_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS*
       H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
       reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
       reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, gidx, dst, add, yb,
-      H.prec == Prec::MIXED ? 1 : 0);
+      (H.prec == Prec::MIXED && sizeof(TA) == sizeof(float)) ? 1 : 0);
   SPX_LAUNCH_CHECK();
 }
 }  // namespace
@@ -287,10 +365,19 @@ void HMatrix::pack(Prec p, cudaStream_t s) {
 template <class T>
 void HMatrix::apply_gather(const T* src, const int32_t* gidx, T* dst, const T* add, T* yb, cudaStream_t s) {
   SPX_CHECK(packed, "H-matrix is not packed");
-  switch (prec) {
-    case Prec::F64: do_apply<double, double, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
-    case Prec::F32: do_apply<float, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
-    case Prec::MIXED: do_apply<__nv_bfloat16, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+  // FP64 vectors accumulate in FP64 whatever the factor storage; FP32 vectors in FP32
+  if (sizeof(T) == sizeof(double)) {
+    switch (prec) {
+      case Prec::F64: do_apply<double, double, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::F32: do_apply<float, float, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::MIXED: do_apply<__nv_bfloat16, float, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
+    }
+  } else {
+    switch (prec) {
+      case Prec::F64: do_apply<double, double, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::F32: do_apply<float, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::MIXED: do_apply<__nv_bfloat16, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+    }
   }
 }
 template void HMatrix::apply_gather<double>(const double*, const int32_t*, double*, const double*, double*, cudaStream_t);
@@ -360,7 +447,7 @@ void apply_noalloc_impl(HMatrix& H, const double* x, double* y, cudaStream_t s) 
       H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
       reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
       reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, nullptr, y, nullptr, nullptr,
-      H.prec == Prec::MIXED ? 1 : 0);
+      (H.prec == Prec::MIXED && sizeof(TA) == sizeof(float)) ? 1 : 0);
   SPX_LAUNCH_CHECK();
 }
 
@@ -370,8 +457,8 @@ void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s) 
   SPX_CHECK(H.packed, "H-matrix is not packed");
   switch (H.prec) {
     case Prec::F64: apply_noalloc_impl<double, double, double, double>(H, x, y, s); break;
-    case Prec::F32: apply_noalloc_impl<float, float, float, float>(H, x, y, s); break;
-    case Prec::MIXED: apply_noalloc_impl<__nv_bfloat16, float, float, float>(H, x, y, s); break;
+    case Prec::F32: apply_noalloc_impl<float, float, double, double>(H, x, y, s); break;
+    case Prec::MIXED: apply_noalloc_impl<__nv_bfloat16, float, double, double>(H, x, y, s); break;
   }
 }
 

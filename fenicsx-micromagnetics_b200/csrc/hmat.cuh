@@ -73,7 +73,7 @@ struct HMatrix {
   bool packed = false;
   DevBuf<char> far_f, near_f;     // factor / tile storage in the packed precision
   DevBuf<int64_t> far_uoff, far_voff, far_zoff;  // per far block (element offsets)
-  DevBuf<int32_t> far_meta;       // per far block: rs, m, cs, n, k
+  DevBuf<int32_t> far_meta;       // per far block: rs, m, cs, n, k, ldv (padded V row length)
   DevBuf<int64_t> near_off;       // per near tile
   DevBuf<int32_t> near_meta;      // per near tile: rs, m, cs, n
   DevBuf<int32_t> leaf_start;     // [nleaf+1] row ranges of leaf clusters (perm space)

@@ -10,10 +10,10 @@
 //   interfacial DMI (gpu/fields/DMI_Interfacial_GPU.py:140-172), nodal uniaxial
 //   anisotropy H = 2Ku/(mu0 Ms) (m.n) n (gpu/fields/Anisotropy_GPU.py:317-342)
 //
-// k_stage fuses, per node and in one pass over the shared SELL pattern: the exchange
-// (and DMI) SpMV on m, the demag gradient G phi / V_i, anisotropy, Zeeman, the LLG
-// RHS and the RK4 stage combination.  The only other per-stage work is the demag
-// potential (Div SpMV, two CG solves, boundary operator).
+// k_stage fuses, per node and in one pass over the shared SELL pattern: the exchange and
+// DMI SpMVs on m and the demag gradient G phi / V_i (all in difference form, see fem.cuh),
+// anisotropy, Zeeman, the LLG RHS and the RK4 stage combination.  The only other per-stage
+// work is the demag potential (Div SpMV, two CG solves, boundary operator).
 #include <algorithm>
 #include <cmath>
 
@@ -21,32 +21,33 @@
 
 namespace spx {
 
-template <class T>
+template <class TV, class TM>
 struct StageArgs {
   int64_t n, nslices;
   const int64_t* sp;
   const int32_t* col;
   int64_t L;
-  const T* Kex;   // [L] exchange, row-scaled
-  const T* Kd;    // [9L] DMI blocks, row-scaled (or null)
-  const T* Gv;    // [3L] G / vol (or null: no demag)
-  const T* phi;   // potential (or null)
-  const T* ani_n; // [3n] unit axes (or null)
-  const T* ani_p; // [n] per-node prefactor 2Ku/(mu0 Ms) (or null)
-  T ani_p0;       // scalar prefactor when ani_p == null
-  const T* H0;    // [3n] (or null)
-  T h0x, h0y, h0z;
-  const T* m;     // stage input (AoS)
-  T* out;         // mode 0: H ; mode 1: rhs ; mode 2: next stage m
-  T* mn;          // RK state (mode 2)
-  T* acc;         // RK accumulator (mode 2)
-  T pref, alpha, precess, stab;
-  T c_next, w_acc, dt6;
+  const TM* Kex;     // [L] exchange, row-scaled
+  const TM* Kd;      // [9L] DMI blocks, row-scaled (or null)
+  const double* Ksum;  // [9n] DMI row sums
+  const TM* Gv;      // [3L] G / vol (or null: no demag)
+  const TV* phi;     // potential (or null)
+  const TV* ani_n;   // [3n] unit axes (or null)
+  const TV* ani_p;   // [n] per-node prefactor 2Ku/(mu0 Ms) (or null)
+  TV ani_p0;         // scalar prefactor when ani_p == null
+  const TV* H0;      // [3n] (or null)
+  TV h0x, h0y, h0z;
+  const TV* m;       // stage input (AoS)
+  TV* out;           // mode 0: H ; mode 1: rhs ; mode 2: next stage m
+  TV* mn;            // RK state (mode 2)
+  TV* acc;           // RK accumulator (mode 2)
+  TV pref, alpha, precess, stab;
+  TV c_next, w_acc, dt6;
   int mode, stage;
 };
 
-template <class T, bool DMI, bool DEMAG, bool ANI>
-__global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
+template <class TV, class TM, bool DMI, bool DEMAG, bool ANI>
+__global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
@@ -55,33 +56,41 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
     if (i >= a.n) continue;
     const int64_t base = a.sp[sl];
     const int width = static_cast<int>((a.sp[sl + 1] - base) >> 5);
-    T hx = 0, hy = 0, hz = 0;
+    const TV mx = a.m[3 * i], my = a.m[3 * i + 1], mz = a.m[3 * i + 2];
+    const TV pi = DEMAG ? a.phi[i] : TV(0);
+    TV hx = 0, hy = 0, hz = 0;
     for (int k = 0; k < width; ++k) {
       const int64_t idx = base + ((int64_t)k << 5) + lane;
       const int64_t j = a.col[idx];
-      const T mx = a.m[3 * j], my = a.m[3 * j + 1], mz = a.m[3 * j + 2];
-      const T e = a.Kex[idx];
-      hx += e * mx;
-      hy += e * my;
-      hz += e * mz;
+      const TV dx = a.m[3 * j] - mx, dy = a.m[3 * j + 1] - my, dz = a.m[3 * j + 2] - mz;
+      const TV e = static_cast<TV>(a.Kex[idx]);
+      hx += e * dx;
+      hy += e * dy;
+      hz += e * dz;
       if (DMI) {
-        const T* K = a.Kd + idx;
+        const TM* K = a.Kd + idx;
         const int64_t L = a.L;
-        hx += K[0] * mx + K[L] * my + K[2 * L] * mz;
-        hy += K[3 * L] * mx + K[4 * L] * my + K[5 * L] * mz;
-        hz += K[6 * L] * mx + K[7 * L] * my + K[8 * L] * mz;
+        hx += static_cast<TV>(K[0]) * dx + static_cast<TV>(K[L]) * dy + static_cast<TV>(K[2 * L]) * dz;
+        hy += static_cast<TV>(K[3 * L]) * dx + static_cast<TV>(K[4 * L]) * dy + static_cast<TV>(K[5 * L]) * dz;
+        hz += static_cast<TV>(K[6 * L]) * dx + static_cast<TV>(K[7 * L]) * dy + static_cast<TV>(K[8 * L]) * dz;
       }
       if (DEMAG) {
-        const T p = a.phi[j];
-        hx += a.Gv[idx] * p;
-        hy += a.Gv[a.L + idx] * p;
-        hz += a.Gv[2 * a.L + idx] * p;
+        const TV p = a.phi[j] - pi;
+        hx += static_cast<TV>(a.Gv[idx]) * p;
+        hy += static_cast<TV>(a.Gv[a.L + idx]) * p;
+        hz += static_cast<TV>(a.Gv[2 * a.L + idx]) * p;
       }
     }
-    const T mx = a.m[3 * i], my = a.m[3 * i + 1], mz = a.m[3 * i + 2];
+    if (DMI) {
+      const double* S = a.Ksum;
+      const int64_t n = a.n;
+      hx += static_cast<TV>(S[i]) * mx + static_cast<TV>(S[n + i]) * my + static_cast<TV>(S[2 * n + i]) * mz;
+      hy += static_cast<TV>(S[3 * n + i]) * mx + static_cast<TV>(S[4 * n + i]) * my + static_cast<TV>(S[5 * n + i]) * mz;
+      hz += static_cast<TV>(S[6 * n + i]) * mx + static_cast<TV>(S[7 * n + i]) * my + static_cast<TV>(S[8 * n + i]) * mz;
+    }
     if (ANI) {
-      const T nx = a.ani_n[3 * i], ny = a.ani_n[3 * i + 1], nz = a.ani_n[3 * i + 2];
-      const T c = (a.ani_p ? a.ani_p[i] : a.ani_p0) * (mx * nx + my * ny + mz * nz);
+      const TV nx = a.ani_n[3 * i], ny = a.ani_n[3 * i + 1], nz = a.ani_n[3 * i + 2];
+      const TV c = (a.ani_p ? a.ani_p[i] : a.ani_p0) * (mx * nx + my * ny + mz * nz);
       hx += c * nx;
       hy += c * ny;
       hz += c * nz;
@@ -101,12 +110,12 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
       a.out[3 * i + 2] = hz;
       continue;
     }
-    const T cx = my * hz - mz * hy, cy = mz * hx - mx * hz, cz = mx * hy - my * hx;
-    const T ccx = my * cz - mz * cy, ccy = mz * cx - mx * cz, ccz = mx * cy - my * cx;
-    const T s = a.stab * (T(1) - (mx * mx + my * my + mz * mz));
-    const T rx = a.pref * (a.precess * cx + a.alpha * ccx) + s * mx;
-    const T ry = a.pref * (a.precess * cy + a.alpha * ccy) + s * my;
-    const T rz = a.pref * (a.precess * cz + a.alpha * ccz) + s * mz;
+    const TV cx = my * hz - mz * hy, cy = mz * hx - mx * hz, cz = mx * hy - my * hx;
+    const TV ccx = my * cz - mz * cy, ccy = mz * cx - mx * cz, ccz = mx * cy - my * cx;
+    const TV s = a.stab * (TV(1) - (mx * mx + my * my + mz * mz));
+    const TV rx = a.pref * (a.precess * cx + a.alpha * ccx) + s * mx;
+    const TV ry = a.pref * (a.precess * cy + a.alpha * ccy) + s * my;
+    const TV rz = a.pref * (a.precess * cz + a.alpha * ccz) + s * mz;
     if (a.mode == 1) {
       a.out[3 * i] = rx;
       a.out[3 * i + 1] = ry;
@@ -114,8 +123,8 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
       continue;
     }
     // RK4 stage update
-    T* A = a.acc + 3 * i;
-    T* M = a.mn + 3 * i;
+    TV* A = a.acc + 3 * i;
+    TV* M = a.mn + 3 * i;
     if (a.stage == 0) {
       A[0] = rx; A[1] = ry; A[2] = rz;
     } else if (a.stage < 3) {
@@ -134,9 +143,10 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<T> a) {
 }
 
 // J v with the linear field H_v = K_lin v (+ anisotropy of v)
-template <class T, bool DMI, bool ANI>
-__global__ void __launch_bounds__(256) k_jv(StageArgs<T> a, const T* __restrict__ Ms, const T* __restrict__ Hm,
-                                            const T* __restrict__ v, T* __restrict__ out, T gamma) {
+template <class TV, class TM, bool DMI, bool ANI>
+__global__ void __launch_bounds__(256) k_jv(StageArgs<TV, TM> a, const TV* __restrict__ Ms,
+                                            const TV* __restrict__ Hm, const TV* __restrict__ v,
+                                            TV* __restrict__ out, TV gamma) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
@@ -145,52 +155,59 @@ __global__ void __launch_bounds__(256) k_jv(StageArgs<T> a, const T* __restrict_
     if (i >= a.n) continue;
     const int64_t base = a.sp[sl];
     const int width = static_cast<int>((a.sp[sl + 1] - base) >> 5);
-    T hvx = 0, hvy = 0, hvz = 0;
+    const TV vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
+    TV hvx = 0, hvy = 0, hvz = 0;
     for (int k = 0; k < width; ++k) {
       const int64_t idx = base + ((int64_t)k << 5) + lane;
       const int64_t j = a.col[idx];
-      const T x = v[3 * j], y = v[3 * j + 1], z = v[3 * j + 2];
-      const T e = a.Kex[idx];
+      const TV x = v[3 * j] - vx, y = v[3 * j + 1] - vy, z = v[3 * j + 2] - vz;
+      const TV e = static_cast<TV>(a.Kex[idx]);
       hvx += e * x; hvy += e * y; hvz += e * z;
       if (DMI) {
-        const T* K = a.Kd + idx;
+        const TM* K = a.Kd + idx;
         const int64_t L = a.L;
-        hvx += K[0] * x + K[L] * y + K[2 * L] * z;
-        hvy += K[3 * L] * x + K[4 * L] * y + K[5 * L] * z;
-        hvz += K[6 * L] * x + K[7 * L] * y + K[8 * L] * z;
+        hvx += static_cast<TV>(K[0]) * x + static_cast<TV>(K[L]) * y + static_cast<TV>(K[2 * L]) * z;
+        hvy += static_cast<TV>(K[3 * L]) * x + static_cast<TV>(K[4 * L]) * y + static_cast<TV>(K[5 * L]) * z;
+        hvz += static_cast<TV>(K[6 * L]) * x + static_cast<TV>(K[7 * L]) * y + static_cast<TV>(K[8 * L]) * z;
       }
     }
-    const T vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
+    if (DMI) {
+      const double* S = a.Ksum;
+      const int64_t n = a.n;
+      hvx += static_cast<TV>(S[i]) * vx + static_cast<TV>(S[n + i]) * vy + static_cast<TV>(S[2 * n + i]) * vz;
+      hvy += static_cast<TV>(S[3 * n + i]) * vx + static_cast<TV>(S[4 * n + i]) * vy + static_cast<TV>(S[5 * n + i]) * vz;
+      hvz += static_cast<TV>(S[6 * n + i]) * vx + static_cast<TV>(S[7 * n + i]) * vy + static_cast<TV>(S[8 * n + i]) * vz;
+    }
     if (ANI) {
-      const T nx = a.ani_n[3 * i], ny = a.ani_n[3 * i + 1], nz = a.ani_n[3 * i + 2];
-      const T c = (a.ani_p ? a.ani_p[i] : a.ani_p0) * (vx * nx + vy * ny + vz * nz);
+      const TV nx = a.ani_n[3 * i], ny = a.ani_n[3 * i + 1], nz = a.ani_n[3 * i + 2];
+      const TV c = (a.ani_p ? a.ani_p[i] : a.ani_p0) * (vx * nx + vy * ny + vz * nz);
       hvx += c * nx; hvy += c * ny; hvz += c * nz;
     }
-    const T mx = Ms[3 * i], my = Ms[3 * i + 1], mz = Ms[3 * i + 2];
-    const T hx = Hm[3 * i], hy = Hm[3 * i + 1], hz = Hm[3 * i + 2];
-    const T cvx = vy * hz - vz * hy, cvy = vz * hx - vx * hz, cvz = vx * hy - vy * hx;
-    const T cmx = my * hvz - mz * hvy, cmy = mz * hvx - mx * hvz, cmz = mx * hvy - my * hvx;
-    const T mdHm = mx * hx + my * hy + mz * hz;
-    const T mdHv = mx * hvx + my * hvy + mz * hvz;
-    const T vdHm = vx * hx + vy * hy + vz * hz;
-    const T mdv = mx * vx + my * vy + mz * vz;
-    const T mdmm = mx * mx + my * my + mz * mz;
-    const T common = vdHm + mdHv;
-    const T dampx = vx * mdHm - T(2) * hx * mdv + mx * common - hvx * mdmm;
-    const T dampy = vy * mdHm - T(2) * hy * mdv + my * common - hvy * mdmm;
-    const T dampz = vz * mdHm - T(2) * hz * mdv + mz * common - hvz * mdmm;
-    const T coef = -gamma / (T(1) + a.alpha * a.alpha);
-    const T sc = a.stab * (T(1) - mdmm);
-    out[3 * i] = coef * (a.precess * (cvx + cmx) + a.alpha * dampx) + sc * vx - T(2) * a.stab * mx * mdv;
-    out[3 * i + 1] = coef * (a.precess * (cvy + cmy) + a.alpha * dampy) + sc * vy - T(2) * a.stab * my * mdv;
-    out[3 * i + 2] = coef * (a.precess * (cvz + cmz) + a.alpha * dampz) + sc * vz - T(2) * a.stab * mz * mdv;
+    const TV mx = Ms[3 * i], my = Ms[3 * i + 1], mz = Ms[3 * i + 2];
+    const TV hx = Hm[3 * i], hy = Hm[3 * i + 1], hz = Hm[3 * i + 2];
+    const TV cvx = vy * hz - vz * hy, cvy = vz * hx - vx * hz, cvz = vx * hy - vy * hx;
+    const TV cmx = my * hvz - mz * hvy, cmy = mz * hvx - mx * hvz, cmz = mx * hvy - my * hvx;
+    const TV mdHm = mx * hx + my * hy + mz * hz;
+    const TV mdHv = mx * hvx + my * hvy + mz * hvz;
+    const TV vdHm = vx * hx + vy * hy + vz * hz;
+    const TV mdv = mx * vx + my * vy + mz * vz;
+    const TV mdmm = mx * mx + my * my + mz * mz;
+    const TV common = vdHm + mdHv;
+    const TV dampx = vx * mdHm - TV(2) * hx * mdv + mx * common - hvx * mdmm;
+    const TV dampy = vy * mdHm - TV(2) * hy * mdv + my * common - hvy * mdmm;
+    const TV dampz = vz * mdHm - TV(2) * hz * mdv + mz * common - hvz * mdmm;
+    const TV coef = -gamma / (TV(1) + a.alpha * a.alpha);
+    const TV sc = a.stab * (TV(1) - mdmm);
+    out[3 * i] = coef * (a.precess * (cvx + cmx) + a.alpha * dampx) + sc * vx - TV(2) * a.stab * mx * mdv;
+    out[3 * i + 1] = coef * (a.precess * (cvy + cmy) + a.alpha * dampy) + sc * vy - TV(2) * a.stab * my * mdv;
+    out[3 * i + 2] = coef * (a.precess * (cvz + cmz) + a.alpha * dampz) + sc * vz - TV(2) * a.stab * mz * mdv;
   }
 }
 
-template <class T>
-__global__ void k_pc_build(int64_t n, const T* __restrict__ M, const T* __restrict__ H, const T* __restrict__ D,
+template <class TV>
+__global__ void k_pc_build(int64_t n, const TV* __restrict__ M, const TV* __restrict__ H, const TV* __restrict__ D,
                            int include_stab, int use_abs_kappa, double shift, double eps_reg, double det_eps,
-                           double c1, double c2, double Stab, T* __restrict__ inv) {
+                           double c1, double c2, double Stab, TV* __restrict__ inv) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double mx = M[3 * i], my = M[3 * i + 1], mz = M[3 * i + 2];
@@ -223,32 +240,32 @@ __global__ void k_pc_build(int64_t n, const T* __restrict__ M, const T* __restri
                A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
   if (fabs(det) < det_eps) det += ((det + det_eps) > 0.0 ? 1.0 : -1.0) * det_eps;
   const double id = 1.0 / det;
-  T* o = inv + 9 * i;
-  o[0] = static_cast<T>((A[1][1] * A[2][2] - A[1][2] * A[2][1]) * id);
-  o[1] = static_cast<T>(-(A[0][1] * A[2][2] - A[0][2] * A[2][1]) * id);
-  o[2] = static_cast<T>((A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id);
-  o[3] = static_cast<T>(-(A[1][0] * A[2][2] - A[1][2] * A[2][0]) * id);
-  o[4] = static_cast<T>((A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id);
-  o[5] = static_cast<T>(-(A[0][0] * A[1][2] - A[0][2] * A[1][0]) * id);
-  o[6] = static_cast<T>((A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id);
-  o[7] = static_cast<T>(-(A[0][0] * A[2][1] - A[0][1] * A[2][0]) * id);
-  o[8] = static_cast<T>((A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id);
+  TV* o = inv + 9 * i;
+  o[0] = static_cast<TV>((A[1][1] * A[2][2] - A[1][2] * A[2][1]) * id);
+  o[1] = static_cast<TV>(-(A[0][1] * A[2][2] - A[0][2] * A[2][1]) * id);
+  o[2] = static_cast<TV>((A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id);
+  o[3] = static_cast<TV>(-(A[1][0] * A[2][2] - A[1][2] * A[2][0]) * id);
+  o[4] = static_cast<TV>((A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id);
+  o[5] = static_cast<TV>(-(A[0][0] * A[1][2] - A[0][2] * A[1][0]) * id);
+  o[6] = static_cast<TV>((A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id);
+  o[7] = static_cast<TV>(-(A[0][0] * A[2][1] - A[0][1] * A[2][0]) * id);
+  o[8] = static_cast<TV>((A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id);
 }
 
-template <class T>
-__global__ void k_pc_apply(int64_t n, const T* __restrict__ inv, const T* __restrict__ x, T* __restrict__ y) {
+template <class TV>
+__global__ void k_pc_apply(int64_t n, const TV* __restrict__ inv, const TV* __restrict__ x, TV* __restrict__ y) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const T* o = inv + 9 * i;
-  const T a = x[3 * i], b = x[3 * i + 1], c = x[3 * i + 2];
+  const TV* o = inv + 9 * i;
+  const TV a = x[3 * i], b = x[3 * i + 1], c = x[3 * i + 2];
   y[3 * i] = o[0] * a + o[1] * b + o[2] * c;
   y[3 * i + 1] = o[3] * a + o[4] * b + o[5] * c;
   y[3 * i + 2] = o[6] * a + o[7] * b + o[8] * c;
 }
 
 // sum_i w_i m_i . H_i  (w = nodal volume)
-template <class T>
-__global__ void k_mdoth(int64_t n, const double* __restrict__ w, const T* __restrict__ m, const T* __restrict__ H,
+template <class TV>
+__global__ void k_mdoth(int64_t n, const double* __restrict__ w, const TV* __restrict__ m, const TV* __restrict__ H,
                         double* __restrict__ out) {
   __shared__ double sh[32];
   double s = 0.0;
@@ -276,9 +293,9 @@ template void convert<float, double>(int64_t, const float*, double*, cudaStream_
 template void convert<double, double>(int64_t, const double*, double*, cudaStream_t);
 
 // ------------------------------------------------------------------ LLG context
-template <class T>
-void LLGCtx<T>::create(DemagCtx<T>* dm, const double* X, int64_t N_, const int32_t* tets, int64_t E,
-                       const LLGParams& p, cudaStream_t s) {
+template <class TV, class TM>
+void LLGCtx<TV, TM>::create(DemagCtx<TV, TM>* dm, const double* X, int64_t N_, const int32_t* tets, int64_t E,
+                            const LLGParams& p, cudaStream_t s) {
   SPX_CUDA(cudaGetDevice(&device));
   prm = p;
   N = N_;
@@ -314,8 +331,8 @@ void LLGCtx<T>::create(DemagCtx<T>* dm, const double* X, int64_t N_, const int32
         for (int c = 0; c < 3; ++c) diag[3 * i + c] += kex[k];
     }
   }
-  std::vector<T> v;
-  sell_values<T>(*hs, kex.data(), 1, true, nnz, 1.0, v);
+  std::vector<TM> v;
+  sell_values<TM>(*hs, kex.data(), 1, true, nnz, 1.0, v);
   Kex.upload(v, s);
   has_dmi = (p.D_int != 0.0);
   if (has_dmi) {
@@ -326,59 +343,63 @@ void LLGCtx<T>::create(DemagCtx<T>* dm, const double* X, int64_t N_, const int32
     else { build_boundary(X, N, tets, E, bhost); bh = &bhost; }
     std::vector<double> b9;
     assemble_dmi_interfacial(X, tets, E, *fem, *bh, p.n_int, b9);
+    std::vector<double> ks(9 * N, 0.0);
     for (int64_t i = 0; i < N; ++i) {
       const double sc = -2.0 * p.D_int / (mu0 * p.Ms) / 1e-9 / fem->vol[i];
       for (int64_t k = fem->rowptr[i]; k < fem->rowptr[i + 1]; ++k) {
-        for (int q = 0; q < 9; ++q) b9[9 * k + q] *= sc;
+        for (int q = 0; q < 9; ++q) {
+          b9[9 * k + q] *= sc;
+          ks[q * N + i] += b9[9 * k + q];
+        }
         if (fem->col[k] == i)
           for (int c = 0; c < 3; ++c) diag[3 * i + c] += b9[9 * k + 4 * c];
       }
     }
-    sell_values<T>(*hs, b9.data(), 9, true, nnz, 1.0, v);
+    sell_values<TM>(*hs, b9.data(), 9, true, nnz, 1.0, v);
     Kd.upload(v, s);
+    Ksum.upload(ks, s);
   }
-  // anisotropy (per-node prefactor allowed)
   has_ani = false;
   if (p.n_ani && (p.Ku != 0.0 || p.Ku_nodes)) {
     has_ani = true;
-    std::vector<T> nn(3 * N);
+    std::vector<TV> nn(3 * N);
     for (int64_t i = 0; i < N; ++i) {
-      double a = p.n_ani[3 * i], b = p.n_ani[3 * i + 1], c = p.n_ani[3 * i + 2];
+      const double a = p.n_ani[3 * i], b = p.n_ani[3 * i + 1], c = p.n_ani[3 * i + 2];
       const double r = std::max(std::sqrt(a * a + b * b + c * c), 1e-300);
-      nn[3 * i] = static_cast<T>(a / r);
-      nn[3 * i + 1] = static_cast<T>(b / r);
-      nn[3 * i + 2] = static_cast<T>(c / r);
+      const double u[3] = {a / r, b / r, c / r};
       const double pr = 2.0 * (p.Ku_nodes ? p.Ku_nodes[i] : p.Ku) / (mu0 * p.Ms);
-      for (int q = 0; q < 3; ++q) diag[3 * i + q] += pr * (a / r) * (a / r) * (q == 0) + pr * (b / r) * (b / r) * (q == 1) +
-                                                     pr * (c / r) * (c / r) * (q == 2);
+      for (int q = 0; q < 3; ++q) {
+        nn[3 * i + q] = static_cast<TV>(u[q]);
+        diag[3 * i + q] += pr * u[q] * u[q];
+      }
     }
     ani_n.upload(nn, s);
     ani_p0 = 2.0 * p.Ku / (mu0 * p.Ms);
     if (p.Ku_nodes) {
-      std::vector<T> pp(N);
-      for (int64_t i = 0; i < N; ++i) pp[i] = static_cast<T>(2.0 * p.Ku_nodes[i] / (mu0 * p.Ms));
+      std::vector<TV> pp(N);
+      for (int64_t i = 0; i < N; ++i) pp[i] = static_cast<TV>(2.0 * p.Ku_nodes[i] / (mu0 * p.Ms));
       ani_p.upload(pp, s);
     }
   }
-  std::vector<T> dg(diag.begin(), diag.end());
+  std::vector<TV> dg(diag.begin(), diag.end());
   diagK.upload(dg, s);
   if (p.H0_nodes) {
-    std::vector<T> h(p.H0_nodes, p.H0_nodes + 3 * N);
+    std::vector<TV> h(p.H0_nodes, p.H0_nodes + 3 * N);
     H0.upload(h, s);
   }
   h0[0] = p.H0_uniform[0];
   h0[1] = p.H0_uniform[1];
   h0[2] = p.H0_uniform[2];
   use_demag = (dm != nullptr) && p.use_demag;
-  m.alloc(3 * N); ms0.alloc(3 * N); ms1.alloc(3 * N); acc.alloc(3 * N); tmp.alloc(3 * N); tmp2.alloc(3 * N);
+  m.alloc(3 * N); ms0.alloc(3 * N); ms1.alloc(3 * N); acc.alloc(3 * N);
   Mstate.alloc(3 * N); Hm.alloc(3 * N); pcinv.alloc(9 * N);
   red.alloc(2);
   SPX_CUDA(cudaStreamSynchronize(s));
 }
 
-template <class T>
-StageArgs<T> LLGCtx<T>::args(const T* min, T* out, int mode, bool with_demag) const {
-  StageArgs<T> a{};
+template <class TV, class TM>
+StageArgs<TV, TM> LLGCtx<TV, TM>::args(const TV* min, TV* out, int mode, bool with_demag) const {
+  StageArgs<TV, TM> a{};
   a.n = N;
   a.nslices = P.nslices;
   a.sp = P.slice_ptr.p;
@@ -386,30 +407,31 @@ StageArgs<T> LLGCtx<T>::args(const T* min, T* out, int mode, bool with_demag) co
   a.L = P.len;
   a.Kex = Kex.p;
   a.Kd = has_dmi ? Kd.p : nullptr;
+  a.Ksum = has_dmi ? Ksum.p : nullptr;
   a.Gv = with_demag ? demag->Gv.p : nullptr;
   a.phi = with_demag ? demag->phi.p : nullptr;
   a.ani_n = has_ani ? ani_n.p : nullptr;
   a.ani_p = (has_ani && ani_p.n) ? ani_p.p : nullptr;
-  a.ani_p0 = static_cast<T>(ani_p0);
+  a.ani_p0 = static_cast<TV>(ani_p0);
   a.H0 = H0.n ? H0.p : nullptr;
-  a.h0x = static_cast<T>(h0[0]);
-  a.h0y = static_cast<T>(h0[1]);
-  a.h0z = static_cast<T>(h0[2]);
+  a.h0x = static_cast<TV>(h0[0]);
+  a.h0y = static_cast<TV>(h0[1]);
+  a.h0z = static_cast<TV>(h0[2]);
   a.m = min;
   a.out = out;
-  a.pref = static_cast<T>(pref);
-  a.alpha = static_cast<T>(prm.alpha);
-  a.precess = static_cast<T>(prm.do_precess);
-  a.stab = static_cast<T>(stab);
+  a.pref = static_cast<TV>(pref);
+  a.alpha = static_cast<TV>(prm.alpha);
+  a.precess = static_cast<TV>(prm.do_precess);
+  a.stab = static_cast<TV>(stab);
   a.mode = mode;
   return a;
 }
 
-template <class T>
-void LLGCtx<T>::launch_stage(const StageArgs<T>& a, bool with_demag, cudaStream_t s) const {
+template <class TV, class TM>
+void LLGCtx<TV, TM>::launch_stage(const StageArgs<TV, TM>& a, bool with_demag, cudaStream_t s) const {
   const unsigned g = grid_for(a.nslices * 32, 256);
   const bool d = has_dmi, an = has_ani;
-#define SPX_STAGE(DM, DE, AN) k_stage<T, DM, DE, AN><<<g, 256, 0, s>>>(a)
+#define SPX_STAGE(DM, DE, AN) k_stage<TV, TM, DM, DE, AN><<<g, 256, 0, s>>>(a)
   if (d && with_demag && an) SPX_STAGE(true, true, true);
   else if (d && with_demag) SPX_STAGE(true, true, false);
   else if (d && an) SPX_STAGE(true, false, true);
@@ -423,37 +445,37 @@ void LLGCtx<T>::launch_stage(const StageArgs<T>& a, bool with_demag, cudaStream_
   ++launches;
 }
 
-template <class T>
-void LLGCtx<T>::heff(const T* min, T* Hout, bool with_demag, cudaStream_t s) {
+template <class TV, class TM>
+void LLGCtx<TV, TM>::heff(const TV* min, TV* Hout, bool with_demag, cudaStream_t s) {
   const bool dm = with_demag && use_demag;
   if (dm) demag->potential(min, s, true);
   launch_stage(args(min, Hout, 0, dm), dm, s);
 }
 
-template <class T>
-void LLGCtx<T>::rhs(const T* min, T* out, cudaStream_t s) {
+template <class TV, class TM>
+void LLGCtx<TV, TM>::rhs(const TV* min, TV* out, cudaStream_t s) {
   if (use_demag) demag->potential(min, s, true);
   launch_stage(args(min, out, 1, use_demag), use_demag, s);
   ++rhs_evals;
 }
 
-template <class T>
-void LLGCtx<T>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
-  const T h = static_cast<T>(dt);
+template <class TV, class TM>
+void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
+  const TV h = static_cast<TV>(dt);
   for (int64_t it = 0; it < nsteps; ++it) {
-    const T* in[4] = {m.p, ms0.p, ms1.p, ms0.p};
-    T* out[4] = {ms0.p, ms1.p, ms0.p, nullptr};
-    const T cnext[4] = {T(0.5) * h, T(0.5) * h, h, T(0)};
-    const T wacc[4] = {T(1), T(2), T(2), T(0)};
+    const TV* in[4] = {m.p, ms0.p, ms1.p, ms0.p};
+    TV* out[4] = {ms0.p, ms1.p, ms0.p, nullptr};
+    const TV cnext[4] = {TV(0.5) * h, TV(0.5) * h, h, TV(0)};
+    const TV wacc[4] = {TV(1), TV(2), TV(2), TV(0)};
     for (int st = 0; st < 4; ++st) {
-      if (use_demag) demag->potential(in[st], s, false);
-      StageArgs<T> a = args(in[st], out[st], 2, use_demag);
+      if (use_demag) demag->potential(in[st], s, false, st);
+      StageArgs<TV, TM> a = args(in[st], out[st], 2, use_demag);
       a.mn = m.p;
       a.acc = acc.p;
       a.stage = st;
       a.c_next = cnext[st];
       a.w_acc = wacc[st];
-      a.dt6 = h / T(6);
+      a.dt6 = h / TV(6);
       Profiler* pf = use_demag ? &demag->prof : nullptr;
       if (pf) pf->mark(PC_STAGE, s);
       launch_stage(a, use_demag, s);
@@ -467,68 +489,59 @@ void LLGCtx<T>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
   }
 }
 
-template <class T>
-void LLGCtx<T>::update_jac_state(const T* min, cudaStream_t s) {
-  SPX_CUDA(cudaMemcpyAsync(Mstate.p, min, 3 * N * sizeof(T), cudaMemcpyDeviceToDevice, s));
+template <class TV, class TM>
+void LLGCtx<TV, TM>::update_jac_state(const TV* min, cudaStream_t s) {
+  SPX_CUDA(cudaMemcpyAsync(Mstate.p, min, 3 * N * sizeof(TV), cudaMemcpyDeviceToDevice, s));
   launch_stage(args(Mstate.p, Hm.p, 0, false), false, s);
 }
 
-template <class T>
-void LLGCtx<T>::jv(const T* v, T* out, cudaStream_t s) {
-  StageArgs<T> a = args(Mstate.p, out, 0, false);
+template <class TV, class TM>
+void LLGCtx<TV, TM>::jv(const TV* v, TV* out, cudaStream_t s) {
+  StageArgs<TV, TM> a = args(Mstate.p, out, 0, false);
   const unsigned g = grid_for(a.nslices * 32, 256);
-  const T gam = static_cast<T>(prm.gamma);
-  if (has_dmi && has_ani) k_jv<T, true, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else if (has_dmi) k_jv<T, true, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else if (has_ani) k_jv<T, false, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else k_jv<T, false, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
+  const TV gam = static_cast<TV>(prm.gamma);
+  if (has_dmi && has_ani) k_jv<TV, TM, true, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
+  else if (has_dmi) k_jv<TV, TM, true, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
+  else if (has_ani) k_jv<TV, TM, false, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
+  else k_jv<TV, TM, false, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
   SPX_LAUNCH_CHECK();
 }
 
-template <class T>
-void LLGCtx<T>::pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s) {
-  k_pc_build<T><<<grid_for(N, 256), 256, 0, s>>>(N, Mstate.p, Hm.p, diagK.p, include_stab, use_abs_kappa, shift,
-                                                 1e-14, 1e-30, c1, c2, stab, pcinv.p);
+template <class TV, class TM>
+void LLGCtx<TV, TM>::pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s) {
+  k_pc_build<TV><<<grid_for(N, 256), 256, 0, s>>>(N, Mstate.p, Hm.p, diagK.p, include_stab, use_abs_kappa, shift,
+                                                  1e-14, 1e-30, c1, c2, stab, pcinv.p);
   SPX_LAUNCH_CHECK();
   pc_ready = true;
 }
 
-template <class T>
-void LLGCtx<T>::pc_apply(const T* x, T* y, cudaStream_t s) {
+template <class TV, class TM>
+void LLGCtx<TV, TM>::pc_apply(const TV* x, TV* y, cudaStream_t s) {
   if (!pc_ready) {
-    SPX_CUDA(cudaMemcpyAsync(y, x, 3 * N * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    SPX_CUDA(cudaMemcpyAsync(y, x, 3 * N * sizeof(TV), cudaMemcpyDeviceToDevice, s));
     return;
   }
-  k_pc_apply<T><<<grid_for(N, 256), 256, 0, s>>>(N, pcinv.p, x, y);
+  k_pc_apply<TV><<<grid_for(N, 256), 256, 0, s>>>(N, pcinv.p, x, y);
   SPX_LAUNCH_CHECK();
 }
 
-template <class T>
-double LLGCtx<T>::mdoth(const double* w, const T* a, const T* b, cudaStream_t s) {
-  SPX_CUDA(cudaMemsetAsync(red.p, 0, sizeof(double), s));
-  k_mdoth<T><<<std::min<unsigned>(grid_for(N, 256), 1184), 256, 0, s>>>(N, w, a, b, red.p);
-  SPX_LAUNCH_CHECK();
-  double h = 0.0;
-  SPX_CUDA(cudaMemcpyAsync(&h, red.p, sizeof(double), cudaMemcpyDeviceToHost, s));
-  SPX_CUDA(cudaStreamSynchronize(s));
-  return h;
-}
+template struct LLGCtx<double, double>;
+template struct LLGCtx<float, float>;
+template struct LLGCtx<double, float>;
 
-template struct LLGCtx<double>;
-template struct LLGCtx<float>;
-
-template <class T>
-double demag_energy(DemagCtx<T>& d, const T* m, const T* H, cudaStream_t s) {
+template <class TV, class TM>
+double demag_energy(DemagCtx<TV, TM>& d, const TV* m, const TV* H, cudaStream_t s) {
   DevBuf<double> r(1);
   r.zero(s);
-  k_mdoth<T><<<std::min<unsigned>(grid_for(d.N, 256), 1184), 256, 0, s>>>(d.N, d.vol.p, m, H, r.p);
+  k_mdoth<TV><<<std::min<unsigned>(grid_for(d.N, 256), 1184), 256, 0, s>>>(d.N, d.vol.p, m, H, r.p);
   SPX_LAUNCH_CHECK();
   double h = 0.0;
   SPX_CUDA(cudaMemcpyAsync(&h, r.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   SPX_CUDA(cudaStreamSynchronize(s));
   return -0.5 * d.mu0 * d.Ms * h / 1e27;
 }
-template double demag_energy<double>(DemagCtx<double>&, const double*, const double*, cudaStream_t);
-template double demag_energy<float>(DemagCtx<float>&, const float*, const float*, cudaStream_t);
+template double demag_energy<double, double>(DemagCtx<double, double>&, const double*, const double*, cudaStream_t);
+template double demag_energy<float, float>(DemagCtx<float, float>&, const float*, const float*, cudaStream_t);
+template double demag_energy<double, float>(DemagCtx<double, float>&, const double*, const double*, cudaStream_t);
 
 }  // namespace spx

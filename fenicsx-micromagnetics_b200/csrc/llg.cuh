@@ -18,44 +18,46 @@ struct LLGParams {
   int use_demag = 1;
 };
 
-template <class T> struct StageArgs;
+template <class TV, class TM> struct StageArgs;
 
-template <class T>
+// TV: nodal vector type, TM: operator value type (see DemagCtx)
+template <class TV, class TM>
 struct LLGCtx {
   int device = 0;
   int64_t N = 0;
   LLGParams prm;
-  DemagCtx<T>* demag = nullptr;
+  DemagCtx<TV, TM>* demag = nullptr;
   HostFem own_fem;
   HostSell own_sell;
-  DevSell<T> P;
-  DevBuf<T> Kex, Kd, ani_n, ani_p, H0, diagK;
+  DevSell<TM> P;
+  DevBuf<TM> Kex, Kd;        // exchange (difference form) and DMI 3x3 blocks
+  DevBuf<double> Ksum;       // [9][N] row sums of the DMI blocks
+  DevBuf<TV> ani_n, ani_p, H0, diagK;
   double ani_p0 = 0.0, h0[3] = {0, 0, 0};
   double pref = 0, stab = 0, c1 = 0, c2 = 0;
   bool has_dmi = false, has_ani = false, use_demag = false, pc_ready = false;
-  DevBuf<T> m, ms0, ms1, acc, tmp, tmp2, Mstate, Hm, pcinv;
+  DevBuf<TV> m, ms0, ms1, acc, Mstate, Hm, pcinv;
   DevBuf<double> red;
   int64_t steps = 0, rhs_evals = 0;
   mutable int64_t launches = 0;
 
-  void create(DemagCtx<T>* dm, const double* X, int64_t N, const int32_t* tets, int64_t E, const LLGParams& p,
-              cudaStream_t s);
-  StageArgs<T> args(const T* min, T* out, int mode, bool with_demag) const;
-  void launch_stage(const StageArgs<T>& a, bool with_demag, cudaStream_t s) const;
-  void heff(const T* m, T* H, bool with_demag, cudaStream_t s);
-  void rhs(const T* m, T* out, cudaStream_t s);
+  void create(DemagCtx<TV, TM>* dm, const double* X, int64_t N, const int32_t* tets, int64_t E,
+              const LLGParams& p, cudaStream_t s);
+  StageArgs<TV, TM> args(const TV* min, TV* out, int mode, bool with_demag) const;
+  void launch_stage(const StageArgs<TV, TM>& a, bool with_demag, cudaStream_t s) const;
+  void heff(const TV* m, TV* H, bool with_demag, cudaStream_t s);
+  void rhs(const TV* m, TV* out, cudaStream_t s);
   void step_rk4(double dt, int64_t nsteps, cudaStream_t s);
-  void update_jac_state(const T* m, cudaStream_t s);
-  void jv(const T* v, T* out, cudaStream_t s);
+  void update_jac_state(const TV* m, cudaStream_t s);
+  void jv(const TV* v, TV* out, cudaStream_t s);
   void pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s);
-  void pc_apply(const T* x, T* y, cudaStream_t s);
-  double mdoth(const double* w, const T* a, const T* b, cudaStream_t s);
+  void pc_apply(const TV* x, TV* y, cudaStream_t s);
 };
 
 template <class A, class B>
 void convert(int64_t n, const A* src, B* dst, cudaStream_t s);
 
-template <class T>
-double demag_energy(DemagCtx<T>& d, const T* m, const T* H, cudaStream_t s);
+template <class TV, class TM>
+double demag_energy(DemagCtx<TV, TM>& d, const TV* m, const TV* H, cudaStream_t s);
 
 }  // namespace spx

@@ -243,7 +243,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* 
           atomicCAS(err, 0, ERR_TIMEOUT);
           break;
         }
-        __nanosleep(64);
+        if (it > 4096) __nanosleep(32);
       }
     }
     __threadfence();

@@ -13,7 +13,7 @@ LIB_PATH = _HERE / "libspx.so"
 
 SPX_OK, SPX_ERR_INVALID, SPX_ERR_CUDA, SPX_ERR_OOM = 0, 1, 2, 3
 SPX_ERR_NOT_CONVERGED, SPX_ERR_TIMEOUT, SPX_ERR_INTERNAL, SPX_ERR_NO_DEVICE = 4, 5, 6, 7
-PREC = {"f64": 0, "fp64": 0, "float64": 0, "f32": 1, "fp32": 1, "float32": 1, "mixed": 2}
+PREC = {"f64": 0, "fp64": 0, "float64": 0, "f32": 1, "fp32": 1, "float32": 1, "mixed": 2, "bf16": 2}
 
 c_i32, c_i64, c_dbl, c_vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 P_i32, P_i64, P_dbl = C.POINTER(c_i32), C.POINTER(c_i64), C.POINTER(c_dbl)
@@ -76,6 +76,8 @@ SIGNATURES = {
     "spx_demag_profile_begin": (C.c_int, [c_vp]),
     "spx_demag_profile_end": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_demag_counters": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_demag_residuals": (C.c_int, [c_vp, c_vp, c_vp]),
+    "spx_demag_set_tolerances": (C.c_int, [c_vp, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32]),
     "spx_llg_create": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, C.POINTER(LLGParams), C.POINTER(c_vp)]),
     "spx_llg_heff": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_hjac": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),

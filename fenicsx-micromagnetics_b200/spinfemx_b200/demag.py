@@ -25,7 +25,16 @@ class DemagFieldLindholmGPU:
                  dense_gpu_max_bytes=512 * 1024 ** 2, hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
                  hmatrix_compressor="fullaca", hmatrix_max_rank=None,
                  hmatrix_max_temporary_block_bytes=256 * 1024 ** 2, hmatrix_use_fp32=True, precision="f64",
-                 warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False, **unused):
+                 hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False, **unused):
+        """Options as in the reference, plus:
+
+        precision          'f64' | 'f32' (plain FP32) | 'mixed' (FP64 vectors, FP32 matrices,
+                           FP32 CG inside FP64 iterative refinement)
+        hmatrix_precision  factor storage 'f64' | 'f32' | 'bf16' (default: 'f64' for
+                           precision='f64', 'f32' otherwise)
+        warm_start         False: zero start (the reference); True: previous solution;
+                           'extrapolate': per-RK-stage quadratic extrapolation (time loop)
+        """
         if str(incident_policy).lower()[:4] != "skip":
             raise ValueError("only incident_policy='skip' (the reference default) is implemented")
         if str(hmatrix_compressor).strip().lower() not in {"fullaca", "aca"}:
@@ -46,15 +55,23 @@ class DemagFieldLindholmGPU:
             call("spx_boundary_sizes", ptr(X), self.N, ptr(tets), tets.shape[0], C.byref(Nb), None)
             req = "dense" if Nb.value * Nb.value * 8 <= int(dense_gpu_max_bytes) else "hmatrix"
         self.boundary_backend = req
-        hprec = precision
-        if req == "hmatrix" and precision == "f64" and hmatrix_use_fp32:
-            hprec = "f64"  # FP64 solvers keep the FP64 factors unless a reduced form is asked for
+        if precision not in ("f64", "f32", "mixed"):
+            raise ValueError("precision must be 'f64', 'f32' or 'mixed'")
+        hprec = hmatrix_precision or ("f64" if precision == "f64" else "f32")
+        if hprec not in ("f64", "f32", "bf16"):
+            raise ValueError("hmatrix_precision must be 'f64', 'f32' or 'bf16'")
+        self.hmatrix_precision = hprec
+        ws = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, "extrapolate": 2}.get(warm_start)
+        if ws is None:
+            raise ValueError("warm_start must be False, True or 'extrapolate'")
         o = _lib.DemagOptions()
         o.backend = 0 if req == "dense" else 1
         o.precision = _lib.PREC[precision]
         o.rtol_u1, o.rtol_u2, o.atol = float(ksp_rtol_u1), float(ksp_rtol_u2), float(ksp_atol)
         o.maxit_u1, o.maxit_u2 = int(ksp_maxit_u1), int(ksp_maxit_u2)
-        o.warm_start = 1 if warm_start else 0
+        self.ksp_rtol_u1, self.ksp_rtol_u2, self.ksp_atol = o.rtol_u1, o.rtol_u2, o.atol
+        self.ksp_maxit_u1, self.ksp_maxit_u2 = o.maxit_u1, o.maxit_u2
+        o.warm_start = ws
         o.hmat = _lib.HmatConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
                                  leaf_size=int(hmatrix_leaf_size), max_rank=int(hmatrix_max_rank or 0),
                                  max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
@@ -71,7 +88,8 @@ class DemagFieldLindholmGPU:
         if req == "hmatrix":
             hh = C.c_void_p()
             call("spx_demag_hmat", self._h, C.byref(hh))
-            self.B_hmatrix_gpu = HMatrixGPUPackedFused.from_handle(hh, self, hprec, self.Nb)
+            self.B_hmatrix_gpu = HMatrixGPUPackedFused.from_handle(hh, self, {"bf16": "mixed"}.get(hprec, hprec),
+                                                                   self.Nb)
             if hmatrix_verbose:
                 st = self.B_hmatrix_gpu.stats()
                 print(f"[Demag Lindholm HMatrix b200] built in {st['build_time_seconds']:.2f} s | "
@@ -115,6 +133,30 @@ class DemagFieldLindholmGPU:
         E = _lib.c_dbl()
         call("spx_demag_energy", self._h, ptr(m_vec), ptr(h_vec), C.byref(E), _lib.stream_ptr())
         return float(E.value) * (1e27 / self.volume_scale)
+
+    def set_tolerances(self, *, ksp_rtol_u1=None, ksp_rtol_u2=None, ksp_atol=None, ksp_maxit_u1=None,
+                       ksp_maxit_u2=None):
+        """Change the Krylov tolerances after construction (KSP.setTolerances in the reference)."""
+        self.ksp_rtol_u1 = self.ksp_rtol_u1 if ksp_rtol_u1 is None else float(ksp_rtol_u1)
+        self.ksp_rtol_u2 = self.ksp_rtol_u2 if ksp_rtol_u2 is None else float(ksp_rtol_u2)
+        self.ksp_atol = self.ksp_atol if ksp_atol is None else float(ksp_atol)
+        self.ksp_maxit_u1 = self.ksp_maxit_u1 if ksp_maxit_u1 is None else int(ksp_maxit_u1)
+        self.ksp_maxit_u2 = self.ksp_maxit_u2 if ksp_maxit_u2 is None else int(ksp_maxit_u2)
+        call("spx_demag_set_tolerances", self._h, self.ksp_rtol_u1, self.ksp_rtol_u2, self.ksp_atol,
+             self.ksp_maxit_u1, self.ksp_maxit_u2)
+
+    def solver_counters(self):
+        """Totals since construction: inner iterations, refinement steps, solves, and the sums of
+        the relative residuals at the starting guess and at return, for the u1 and u2 solves."""
+        c1, c2 = (_lib.c_i64 * 4)(), (_lib.c_i64 * 4)()
+        r1, r2 = (_lib.c_dbl * 2)(), (_lib.c_dbl * 2)()
+        call("spx_demag_counters", self._h, c1, c2)
+        call("spx_demag_residuals", self._h, r1, r2)
+        out = {}
+        for name, c, r in (("u1", c1, r1), ("u2", c2, r2)):
+            out[name] = {"iterations": c[0], "refinements": c[1], "solves": c[2],
+                         "initial_rel_residual_sum": r[0], "final_rel_residual_sum": r[1]}
+        return out
 
     def boundary_memory_report(self):
         N, Nb, NI, by = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()

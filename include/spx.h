@@ -204,6 +204,14 @@ SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz
 SPX_API int spx_demag_profile_begin(spx_demag d);
 SPX_API int spx_demag_profile_end(spx_demag d, double* ms8, int64_t* launches8, int64_t* groups8);
 SPX_API int spx_demag_counters(spx_demag d, int64_t* u1_counters4, int64_t* u2_counters4);
+/* sums over all solves since create of the relative residual ||b - A x0||/||b|| at the
+ * starting guess ([0]) and at return ([1]), for the u1 and u2 solves (no counterpart in
+ * the reference: its KSP solves, Demag_Lindholm_GPU.py:577 and :640, report nothing) */
+SPX_API int spx_demag_residuals(spx_demag d, double* u1_res2, double* u2_res2);
+/* change the Krylov tolerances / iteration limits after create (the reference fixes them
+ * with KSP.setTolerances, Demag_Lindholm_GPU.py:219 and :274) */
+SPX_API int spx_demag_set_tolerances(spx_demag d, double rtol_u1, double rtol_u2, double atol, int32_t maxit_u1,
+                                     int32_t maxit_u2);
 /* steps, RHS evaluations, LLG kernel launches */
 SPX_API int spx_llg_stats(spx_llg l, int64_t* steps, int64_t* rhs_evals, int64_t* launches);
 SPX_API int spx_llg_destroy(spx_llg l);

@@ -268,3 +268,39 @@ def test_cg_iteration_cap_reports_not_converged(spx, c1_oracle):
     d = spx.DemagFieldLindholmGPU(o.X, o.tets, 8e5, ksp_maxit_u1=3)
     d.compute_vec(mt, out)
     assert d.last_its_u1 == 3 and d.last_res_u1 > 1e-6
+
+
+def test_demag_mixed_vs_oracle(spx, c1_oracle):
+    # FP64 vectors, FP32 matrices, FP32 CG inside FP64 refinement, difference-form operators
+    o = c1_oracle
+    m = _m0(o.N)
+    Href = o.compute(m)
+    mt = torch.as_tensor(m, device=DEV)
+    out = torch.empty_like(mt)
+    d = spx.DemagFieldLindholmGPU(o.X, o.tets, 8e5, boundary_backend="dense", precision="mixed",
+                                  ksp_rtol_u1=1e-10, ksp_rtol_u2=1e-10, ksp_atol=0.0, ksp_maxit_u1=20000)
+    d.compute_vec(mt, out)
+    assert rel(out.cpu().numpy(), Href) < 1e-7
+    d6 = spx.DemagFieldLindholmGPU(o.X, o.tets, 8e5, boundary_backend="dense", precision="mixed")
+    d6.compute_vec(mt, out)
+    assert rel(out.cpu().numpy(), Href) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_rk4_extrapolated_starts_vs_oracle(spx, c1_oracle, precision):
+    # per-RK-stage extrapolated CG starts change iteration counts, not the trajectory
+    o = c1_oracle
+    m0 = _m0(o.N)
+    ohef = ollg.EffectiveFieldOracle(o.X, o.tets, 8e5, Aex=1.3e-11, alpha=0.5, demag=o)
+    nsteps = 12
+    m = m0.copy()
+    for _ in range(nsteps):
+        m = ollg.rk4_step(ohef.llg_rhs, m, 1e-14)
+    hef = spx.EffectiveField(o.X, o.tets, 8e5, Aex=1.3e-11, alpha=0.5, use_demag=True,
+                             demag_kwargs=dict(boundary_backend="dense", ksp_rtol_u1=1e-11, ksp_rtol_u2=1e-11,
+                                               ksp_atol=0.0, ksp_maxit_u1=20000, precision=precision,
+                                               warm_start="extrapolate"))
+    hef.set_state(torch.as_tensor(m0, device=DEV))
+    hef.step(1e-14, nsteps)
+    mg = hef.get_state().cpu().numpy()
+    assert np.abs(mg - m).max() < (1e-8 if precision == "f64" else 1e-7)
