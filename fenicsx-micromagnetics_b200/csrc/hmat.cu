@@ -1,17 +1,31 @@
 // H-matrix apply: y = P^-1 [diag o x~ + Near x~ + sum_b U_b (V_b x~_{J_b})],  x~ = x[perm]
 // (HMatrixGPUPackedFused.matvec, lindholm_hmatrix_gpu/backend_fused.py:496-512).
 //
-// B200 layout.  Far factors are packed per block as U^T (k x m, each column of U
-// contiguous) followed by V (k x n, each row of V contiguous) in the storage type TF
-// (FP64, FP32 or BF16).  Near blocks are dense tiles stored column-major (n x m) in
-// TN.  Three kernels, no atomics, every output row written by exactly one CTA:
+// B200 layout (built by pack() from the FP64 pools of the builder, in the storage type TF of
+// the far factors -- FP64, FP32 or BF16 -- and TN of the near tiles -- FP64 or FP32):
+//   * row segments: the leaf clusters in permutation order, split into pieces of at most
+//     64 rows; every output row belongs to exactly one segment.
+//   * V_b (k x n) of each far block: k rows of ldv = n rounded up to a 16-byte multiple.
+//   * U_b of each far block, cut at the segments it covers: per segment a tile of k rows of
+//     ld = rows rounded up to a 16-byte multiple (row q holds U[rows, q]).
+//   * near blocks, cut the same way: per segment a tile of n columns of ld entries.
+// Every tile and row starts 16-byte aligned and is zero padded, so all factor traffic is
+// 16-byte vector loads of contiguous memory.
+//
+// Kernels (no atomics on data, every output written by exactly one warp or CTA):
 //   k_hgather : x~[i] = src[g(perm[i])]             (fused boundary gather + perm)
-//   k_far_z   : z_b = V_b x~_{J_b}, one CTA per far block, lanes over columns
-//   k_rows    : one CTA per leaf row cluster; threads over the cluster's rows walk
-//               the cluster's item list (near tiles and far blocks covering it),
-//               read U^T / tile columns coalesced across rows, add diag o x~, and
-//               scatter y to dst[g(perm[i])].
-// Near tiles may use compensated (Kahan) accumulation in the mixed-precision form.
+//   k_far_z   : z_b = V_b x~_{J_b}.  Persistent warps; the work is cut into units of at most
+//               8 rows x 1024 columns of one V_b and dealt to warps in contiguous, byte-balanced
+//               ranges.  A lane keeps its x~ values in registers for all rows of the unit.  Rows
+//               longer than 1024 columns are cut into pieces whose partial sums the last
+//               arriving piece (per-group arrival counter, reset by that piece) adds in piece
+//               order, so z does not depend on scheduling.
+//   k_rows    : one CTA per row segment; its warps take the segment's items (U tiles with z_b,
+//               near tiles with x~) round-robin, lanes over 16-byte row vectors x phases over
+//               the tile rows, then a fixed-order sum over warps, + diag o x~, scattered to
+//               dst[g(perm[i])].
+// Near tiles use compensated (Kahan) accumulation when FP32 accumulates BF16/FP32 data in
+// the mixed-precision form.
 #include <algorithm>
 #include <mutex>
 #include <string>
@@ -34,34 +48,33 @@ template <> __device__ __forceinline__ double cvt<double, __nv_bfloat16>(__nv_bf
   return static_cast<double>(__bfloat162float(v));
 }
 
+
 // ------------------------------------------------------------------ packing
-struct PackFar {
-  int64_t src_u, src_v, dst_u, dst_v;  // element offsets
-  int32_t m, n, k, ldv;
-};
-// U^T (k x m) as is; V (k x n) into rows of ldv elements (ldv = n rounded up to 8), zero padded
-template <class TF>
-__global__ void k_pack_far(const PackFar* __restrict__ jobs, const double* __restrict__ pool, TF* __restrict__ out) {
-  const PackFar j = jobs[blockIdx.x];
-  const int64_t lu = (int64_t)j.k * j.m, lv = (int64_t)j.k * j.ldv;
-  for (int64_t e = threadIdx.x; e < lu; e += blockDim.x) out[j.dst_u + e] = from_d<TF>(pool[j.src_u + e]);
-  for (int64_t e = threadIdx.x; e < lv; e += blockDim.x) {
-    const int64_t q = e / j.ldv, c = e - q * j.ldv;
-    out[j.dst_v + e] = (c < j.n) ? from_d<TF>(pool[j.src_v + q * j.n + c]) : from_d<TF>(0.0);
-  }
-}
-struct PackNear {
+namespace {
+constexpr int ZROWS = 8;        // V rows per far_z unit
+constexpr int ZCOLS = 1024;     // columns per far_z unit piece
+constexpr int Z_WARPS = 8;      // warps per far_z CTA
+constexpr int Z_CTAS_PER_SM = 4;
+constexpr int SEG_MAX = 64;     // rows per segment
+constexpr int ROWS_WARPS = 8;   // warps per k_rows CTA
+inline int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+}  // namespace
+
+// dst[q * ld + r] = pool[src + q * sq + r * sr] for r < nr, 0 for nr <= r < ld, q < nq
+struct PackJob {
   int64_t src, dst;
-  int32_t m, n;
+  int32_t nq, nr, ld, sq, sr;
 };
-template <class TN>
-__global__ void k_pack_near(const PackNear* __restrict__ jobs, const double* __restrict__ pool, TN* __restrict__ out) {
-  const PackNear j = jobs[blockIdx.x];
-  const int64_t L = (int64_t)j.m * j.n;
-  // out[c * m + r] = in[r * n + c]
-  for (int64_t e = threadIdx.x; e < L; e += blockDim.x) {
-    const int64_t c = e / j.m, r = e - c * j.m;
-    out[j.dst + e] = from_d<TN>(pool[j.src + r * j.n + c]);
+template <class T>
+__global__ void k_pack(const PackJob* __restrict__ jobs, int64_t njobs, const double* __restrict__ pool,
+                       T* __restrict__ out) {
+  for (int64_t jb = blockIdx.x; jb < njobs; jb += gridDim.x) {
+    const PackJob j = jobs[jb];
+    const int64_t L = static_cast<int64_t>(j.nq) * j.ld;
+    for (int64_t e = threadIdx.x; e < L; e += blockDim.x) {
+      const int64_t q = e / j.ld, r = e - q * j.ld;
+      out[j.dst + e] = r < j.nr ? from_d<T>(pool[j.src + q * j.sq + r * j.sr]) : from_d<T>(0.0);
+    }
   }
 }
 
@@ -112,121 +125,203 @@ __device__ __forceinline__ void v16_elems<double, __nv_bfloat16>(const uint4& v,
 template <>
 __device__ __forceinline__ void v16_elems<float, __nv_bfloat16>(const uint4& v, float out[8]) { bf16x8<float>(v, out); }
 
-// z_b = V_b x~_{J_b}: one CTA per far block; V rows (ldv elements, zero padded, 16-byte aligned)
-// are read as 16-byte vectors by groups of G lanes (G = chunks per row rounded to a power of
-// two, at most 32), groups reduce with shuffles.
+
+__device__ __forceinline__ int log2_ceil_le5(int n) {
+  int l = 0;
+  while ((1 << l) < n && l < 5) ++l;
+  return l;
+}
+
 template <class TF, class TA, class TX>
-__global__ void __launch_bounds__(128) k_far_z(const int32_t* __restrict__ meta, const int64_t* __restrict__ voff,
-                                               const int64_t* __restrict__ zoff, const TF* __restrict__ F,
-                                               const TX* __restrict__ xp, TA* __restrict__ z) {
+__global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
+    k_far_z(const FarUnit* __restrict__ units, const int32_t* __restrict__ warp_first, int nwarps,
+            const TF* __restrict__ F, const TX* __restrict__ xp, TA* __restrict__ z, TA* __restrict__ zpart,
+            const FarGroup* __restrict__ groups, unsigned int* __restrict__ gcnt) {
   constexpr int E = V16<TF>::E;
   using VT = typename V16<TF>::T;
-  const int b = blockIdx.x;
-  const int cs = meta[6 * b + 2], n = meta[6 * b + 3], k = meta[6 * b + 4], ldv = meta[6 * b + 5];
-  const VT* V = reinterpret_cast<const VT*>(F + voff[b]);
-  const TX* x = xp + cs;
-  const int nch = ldv / E;
-  int G = 1;
-  while (G < nch && G < 32) G <<= 1;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int gpw = 32 / G;                // groups per warp
-  const int gl = lane % G, gw = lane / G;
-  for (int qb = warp * gpw; qb < k; qb += nwarps * gpw) {
-    const int q = qb + gw;
-    TA acc = 0;
-    if (q < k) {
-      const VT* row = V + (int64_t)q * nch;
-      for (int c = gl; c < nch; c += G) {
-        const VT v = row[c];
-        TA e[E];
-        v16_elems<TA, TF>(v, e);
-        const int j0 = c * E;
+  const int wg = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
+  if (wg >= nwarps) return;  // uniform per warp
+  const int lane = threadIdx.x & 31;
+  const int u1 = warp_first[wg + 1];
+  int u = warp_first[wg];
+  FarUnit nxt;
+  if (u < u1) nxt = units[u];
+  for (; u < u1; ++u) {
+    const FarUnit U = nxt;
+    if (u + 1 < u1) nxt = units[u + 1];  // descriptor of the next unit in flight
+    const int nvec = (U.nc + E - 1) / E;
+    const int lg = log2_ceil_le5(nvec);
+    const int G = 1 << lg, NG = 32 >> lg;
+    const int gl = lane & (G - 1), g = lane >> lg;
+    const int rpg = (U.nrows + NG - 1) / NG;  // rows per lane group, uniform over the warp
+    const int ldv = U.ldv / E;
+    const VT* base = reinterpret_cast<const VT*>(F + U.voff);
+    const TX* x = xp + U.xc;
+    TA acc[ZROWS];
 #pragma unroll
-        for (int t = 0; t < E; ++t)
-          if (j0 + t < n) acc += e[t] * static_cast<TA>(x[j0 + t]);
+    for (int j = 0; j < ZROWS; ++j) acc[j] = TA(0);
+    for (int v = gl; v < nvec; v += G) {
+      TA xv[E];
+#pragma unroll
+      for (int t = 0; t < E; ++t) {
+        const int c = v * E + t;
+        xv[t] = c < U.nc ? static_cast<TA>(x[c]) : TA(0);
+      }
+#pragma unroll
+      for (int j = 0; j < ZROWS; ++j) {
+        const int r = g + j * NG;
+        if (j < rpg && r < U.nrows) {
+          const VT w = base[static_cast<int64_t>(r) * ldv + v];
+          TA e[E];
+          v16_elems<TA, TF>(w, e);
+          TA s = TA(0);
+#pragma unroll
+          for (int t = 0; t < E; ++t) s += e[t] * xv[t];
+          acc[j] += s;
+        }
       }
     }
-    for (int o = G >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (q < k && gl == 0) z[zoff[b] + q] = acc;
+#pragma unroll
+    for (int j = 0; j < ZROWS; ++j)
+      if (j < rpg)
+        for (int o = G >> 1; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+    TA* out = U.grp < 0 ? z : zpart;
+    if (gl == 0) {
+#pragma unroll
+      for (int j = 0; j < ZROWS; ++j) {
+        const int r = g + j * NG;
+        if (j < rpg && r < U.nrows) out[U.zout + r] = acc[j];
+      }
+    }
+    if (U.grp >= 0) {  // column piece of a long row batch: the last piece to arrive sums all
+      __threadfence();
+      __syncwarp();
+      unsigned last = 0;
+      if (lane == 0)
+        last = atomicAdd(gcnt + U.grp, 1u) == static_cast<unsigned>(groups[U.grp].npieces) - 1u ? 1u : 0u;
+      last = __shfl_sync(0xffffffffu, last, 0);
+      if (last) {
+        __threadfence();
+        const FarGroup Gp = groups[U.grp];
+        if (lane < Gp.nrows) {
+          TA s = TA(0);
+          for (int p = 0; p < Gp.npieces; ++p) s += __ldcg(zpart + Gp.pbase + p * ZROWS + lane);
+          z[Gp.zdst + lane] = s;
+        }
+        if (lane == 0) atomicExch(gcnt + U.grp, 0u);
+      }
+    }
   }
 }
 
-constexpr int ROWS_GROUPS = 4;
-constexpr int ROWS_GSIZE = 64;
-
-template <class TF, class TN, class TA, class TX, class TD>
-__global__ void __launch_bounds__(ROWS_GROUPS * ROWS_GSIZE) k_rows(
-    const int32_t* __restrict__ leaf_start, const int64_t* __restrict__ item_ptr,
-    const int32_t* __restrict__ items, const int32_t* __restrict__ far_meta,
-    const int64_t* __restrict__ far_uoff, const int64_t* __restrict__ far_zoff,
-    const TF* __restrict__ F, const int32_t* __restrict__ near_meta, const int64_t* __restrict__ near_off,
-    const TN* __restrict__ Nt, const TA* __restrict__ z, const TX* __restrict__ xp,
-    const double* __restrict__ diag, const int32_t* __restrict__ perm, const int32_t* __restrict__ gidx,
-    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, int kahan) {
-  extern __shared__ unsigned char smem_raw[];
-  const int leaf = blockIdx.x;
-  const int r0 = leaf_start[leaf], nr = leaf_start[leaf + 1] - r0;
-  TA* acc = reinterpret_cast<TA*>(smem_raw);             // [GROUPS][nr]
-  TA* cmp = acc + ROWS_GROUPS * nr;                       // [GROUPS][nr] Kahan compensation
-  const int g = threadIdx.x / ROWS_GSIZE, t = threadIdx.x % ROWS_GSIZE;
-  for (int r = t; r < nr; r += ROWS_GSIZE) {
-    acc[g * nr + r] = 0;
-    cmp[g * nr + r] = 0;
-  }
-  const int64_t i0 = item_ptr[leaf], i1 = item_ptr[leaf + 1];
-  for (int64_t it = i0 + g; it < i1; it += ROWS_GROUPS) {
-    const int32_t code = items[it];
-    const int32_t bi = code >> 1;
-    if (code & 1) {
-      const int rs = far_meta[6 * bi], m = far_meta[6 * bi + 1], k = far_meta[6 * bi + 4];
-      const TF* Ut = F + far_uoff[bi];
-      const TA* zb = z + far_zoff[bi];
-      for (int r = t; r < nr; r += ROWS_GSIZE) {
-        const TF* u = Ut + (r0 + r - rs);
-        TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int q = 0;
-        for (; q + 4 <= k; q += 4) {
-          s0 += cvt<TA>(u[(int64_t)q * m]) * zb[q];
-          s1 += cvt<TA>(u[(int64_t)(q + 1) * m]) * zb[q + 1];
-          s2 += cvt<TA>(u[(int64_t)(q + 2) * m]) * zb[q + 2];
-          s3 += cvt<TA>(u[(int64_t)(q + 3) * m]) * zb[q + 3];
-        }
-        for (; q < k; ++q) s0 += cvt<TA>(u[(int64_t)q * m]) * zb[q];
-        acc[g * nr + r] += (s0 + s1) + (s2 + s3);
+// Accumulate one warp's share of a segment's items: item it covers tile rows q < len of
+// ld = round_up(nr, E) entries; row q is multiplied by vs[item.src + q].
+template <class T, class TA, class TV>
+__device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, int64_t first, int64_t end,
+                                           const T* __restrict__ base, const TV* __restrict__ vs, int nr,
+                                           TA* __restrict__ part, int lane, bool kahan) {
+  constexpr int E = V16<T>::E;
+  using VT = typename V16<T>::T;
+  const int nvec = (nr + E - 1) / E;
+  const int lg = log2_ceil_le5(nvec);
+  const int G = 1 << lg, P = 32 >> lg;
+  const int vl = lane & (G - 1), ph = lane >> lg;
+  TA acc[E], cmp[E];
+#pragma unroll
+  for (int t = 0; t < E; ++t) acc[t] = cmp[t] = TA(0);
+  const bool active = vl < nvec;
+  RowItem nxt;
+  if (first < end) nxt = items[first];
+  for (int64_t it = first; it < end; it += ROWS_WARPS) {
+    const RowItem I = nxt;
+    if (it + ROWS_WARPS < end) nxt = items[it + ROWS_WARPS];
+    if (!active) continue;
+    const VT* tile = reinterpret_cast<const VT*>(base + I.off) + vl;
+    const TV* v = vs + I.src;
+    int q = ph;
+    for (; q + 3 * P < I.len; q += 4 * P) {
+      VT w[4];
+      TA a[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        w[u] = tile[static_cast<int64_t>(q + u * P) * nvec];
+        a[u] = static_cast<TA>(v[q + u * P]);
       }
-    } else {
-      const int rs = near_meta[4 * bi], m = near_meta[4 * bi + 1], cs = near_meta[4 * bi + 2],
-                n = near_meta[4 * bi + 3];
-      const TN* tile = Nt + near_off[bi];
-      const TX* x = xp + cs;
-      for (int r = t; r < nr; r += ROWS_GSIZE) {
-        const TN* u = tile + (r0 + r - rs);
-        TA s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int c = 0;
-        for (; c + 4 <= n; c += 4) {
-          s0 += cvt<TA>(u[(int64_t)c * m]) * static_cast<TA>(x[c]);
-          s1 += cvt<TA>(u[(int64_t)(c + 1) * m]) * static_cast<TA>(x[c + 1]);
-          s2 += cvt<TA>(u[(int64_t)(c + 2) * m]) * static_cast<TA>(x[c + 2]);
-          s3 += cvt<TA>(u[(int64_t)(c + 3) * m]) * static_cast<TA>(x[c + 3]);
-        }
-        for (; c < n; ++c) s0 += cvt<TA>(u[(int64_t)c * m]) * static_cast<TA>(x[c]);
-        const TA s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        TA e[E];
+        v16_elems<TA, T>(w[u], e);
         if (kahan) {
-          const TA y = s - cmp[g * nr + r];
-          const TA tt = acc[g * nr + r] + y;
-          cmp[g * nr + r] = (tt - acc[g * nr + r]) - y;
-          acc[g * nr + r] = tt;
+#pragma unroll
+          for (int t = 0; t < E; ++t) {
+            const TA y = e[t] * a[u] - cmp[t];
+            const TA s = acc[t] + y;
+            cmp[t] = (s - acc[t]) - y;
+            acc[t] = s;
+          }
         } else {
-          acc[g * nr + r] += s;
+#pragma unroll
+          for (int t = 0; t < E; ++t) acc[t] += e[t] * a[u];
         }
       }
     }
+    for (; q < I.len; q += P) {
+      const VT w = tile[static_cast<int64_t>(q) * nvec];
+      const TA a = static_cast<TA>(v[q]);
+      TA e[E];
+      v16_elems<TA, T>(w, e);
+      if (kahan) {
+#pragma unroll
+        for (int t = 0; t < E; ++t) {
+          const TA y = e[t] * a - cmp[t];
+          const TA s = acc[t] + y;
+          cmp[t] = (s - acc[t]) - y;
+          acc[t] = s;
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < E; ++t) acc[t] += e[t] * a;
+      }
+    }
   }
+#pragma unroll
+  for (int t = 0; t < E; ++t) {
+    TA y = acc[t] - cmp[t];
+    for (int o = G; o < 32; o <<= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    acc[t] = y;
+  }
+  if (ph == 0 && active) {
+#pragma unroll
+    for (int t = 0; t < E; ++t) {
+      const int r = vl * E + t;
+      if (r < nr) part[r] += acc[t];
+    }
+  }
+  __syncwarp();
+}
+
+template <class TF, class TN, class TA, class TX, class TD>
+__global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
+    const int32_t* __restrict__ seg_start, const int64_t* __restrict__ item_ptr,
+    const int64_t* __restrict__ near_begin, const RowItem* __restrict__ items, const TF* __restrict__ F,
+    const TN* __restrict__ Nt, const TA* __restrict__ z, const TX* __restrict__ xp,
+    const double* __restrict__ diag, const int32_t* __restrict__ perm, const int32_t* __restrict__ gidx,
+    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, int kahan) {
+  __shared__ TA part[ROWS_WARPS][SEG_MAX];
+  const int sgm = blockIdx.x;
+  const int r0 = seg_start[sgm], nr = seg_start[sgm + 1] - r0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = lane; r < SEG_MAX; r += 32) part[warp][r] = TA(0);
+  __syncwarp();
+  const int64_t i0 = item_ptr[sgm], im = near_begin[sgm], i1 = item_ptr[sgm + 1];
+  rows_items<TF, TA, TA>(items, i0 + warp, im, F, z, nr, part[warp], lane, false);
+  rows_items<TN, TA, TX>(items, im + warp, i1, Nt, xp, nr, part[warp], lane, kahan != 0);
   __syncthreads();
   for (int r = threadIdx.x; r < nr; r += blockDim.x) {
     const int64_t i = r0 + r;
     TA y = static_cast<TA>(diag[i]) * static_cast<TA>(xp[i]);
-    for (int q = 0; q < ROWS_GROUPS; ++q) y += acc[q * nr + r] - cmp[q * nr + r];
+#pragma unroll
+    for (int w = 0; w < ROWS_WARPS; ++w) y += part[w][r];
     const int32_t b = perm[i];
     const int64_t o = gidx ? gidx[b] : b;
     const TD yv = static_cast<TD>(y);
@@ -237,94 +332,168 @@ __global__ void __launch_bounds__(ROWS_GROUPS * ROWS_GSIZE) k_rows(
 
 // ------------------------------------------------------------------ host side
 namespace {
+
+void run_pack_jobs_f(const std::vector<PackJob>& jobs, const double* pool, char* out, Prec p, bool near,
+                     cudaStream_t s) {
+  if (jobs.empty()) return;
+  constexpr size_t CH = size_t(1) << 20;
+  for (size_t k0 = 0; k0 < jobs.size(); k0 += CH) {
+    const size_t c = std::min(CH, jobs.size() - k0);
+    DevBuf<PackJob> d;
+    d.upload(jobs.data() + k0, c, s);
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>(c, 65535));
+    if (p == Prec::F64)
+      k_pack<double><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool, reinterpret_cast<double*>(out));
+    else if (p == Prec::F32 || near)
+      k_pack<float><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool, reinterpret_cast<float*>(out));
+    else
+      k_pack<__nv_bfloat16><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool,
+                                                 reinterpret_cast<__nv_bfloat16*>(out));
+    SPX_LAUNCH_CHECK();
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
 template <class TF, class TN>
 void do_pack(HMatrix& H, cudaStream_t s) {
-  std::vector<PackFar> pf;
-  std::vector<PackNear> pn;
-  std::vector<int32_t> fmeta, nmeta;
-  std::vector<int64_t> fu, fv, fz, noff;
-  std::vector<int32_t> code_of(H.blocks.size());
-  int64_t fpos = 0, npos = 0, zpos = 0;
-  int32_t nf = 0, nn = 0;
-  for (size_t q = 0; q < H.blocks.size(); ++q) {
-    const HBlock& b = H.blocks[q];
-    const int32_t m = b.re - b.rs, n = b.ce - b.cs;
-    if (b.type == 1) {
-      const int32_t ldv = (n + 7) / 8 * 8;
-      const int64_t pu = fpos;
-      const int64_t pv = (pu + (int64_t)b.rank * m + 7) / 8 * 8;  // 16-byte aligned V rows
-      pf.push_back(PackFar{b.off_u, b.off_v, pu, pv, m, n, b.rank, ldv});
-      fmeta.insert(fmeta.end(), {b.rs, m, b.cs, n, b.rank, ldv});
-      fu.push_back(pu);
-      fv.push_back(pv);
-      fz.push_back(zpos);
-      fpos = pv + (int64_t)b.rank * ldv;
-      zpos += b.rank;
-      code_of[q] = (nf++ << 1) | 1;
-    } else {
-      pn.push_back(PackNear{b.off_u, npos, m, n});
-      nmeta.insert(nmeta.end(), {b.rs, m, b.cs, n});
-      noff.push_back(npos);
-      npos += (int64_t)m * n;
-      code_of[q] = (nn++ << 1);
-    }
-  }
-  H.n_far = nf;
-  H.n_near = nn;
-  H.zlen = zpos;
-  H.far_f.alloc(std::max<int64_t>(fpos, 1) * sizeof(TF));
-  H.near_f.alloc(std::max<int64_t>(npos, 1) * sizeof(TN));
-  H.bytes_far = fpos * (int64_t)sizeof(TF);
-  H.bytes_near = npos * (int64_t)sizeof(TN);
-  for (size_t k0 = 0; k0 < pf.size(); k0 += 65535) {
-    const size_t c = std::min<size_t>(65535, pf.size() - k0);
-    DevBuf<PackFar> d;
-    d.upload(pf.data() + k0, c, s);
-    k_pack_far<TF><<<static_cast<unsigned>(c), 256, 0, s>>>(d.p, H.far_pool64.p, reinterpret_cast<TF*>(H.far_f.p));
-    SPX_LAUNCH_CHECK();
-    SPX_CUDA(cudaStreamSynchronize(s));
-  }
-  for (size_t k0 = 0; k0 < pn.size(); k0 += 65535) {
-    const size_t c = std::min<size_t>(65535, pn.size() - k0);
-    DevBuf<PackNear> d;
-    d.upload(pn.data() + k0, c, s);
-    k_pack_near<TN><<<static_cast<unsigned>(c), 256, 0, s>>>(d.p, H.near_pool64.p, reinterpret_cast<TN*>(H.near_f.p));
-    SPX_LAUNCH_CHECK();
-    SPX_CUDA(cudaStreamSynchronize(s));
-  }
-  H.far_meta.upload(fmeta, s);
-  H.far_uoff.upload(fu, s);
-  H.far_voff.upload(fv, s);
-  H.far_zoff.upload(fz, s);
-  H.near_meta.upload(nmeta, s);
-  H.near_off.upload(noff, s);
-  // leaf row clusters: tree leaves in permutation order
+  constexpr int EF = 16 / static_cast<int>(sizeof(TF));
+  constexpr int EN = 16 / static_cast<int>(sizeof(TN));
+  // row segments: leaf clusters in permutation order, cut into pieces of <= SEG_MAX rows
   std::vector<int32_t> ls;
   for (const TreeNode& nd : H.tree.nodes)
     if (nd.leaf()) ls.push_back(nd.start);
   std::sort(ls.begin(), ls.end());
   ls.push_back(static_cast<int32_t>(H.Nb));
-  const int64_t nleaf = static_cast<int64_t>(ls.size()) - 1;
-  std::vector<std::vector<int32_t>> per(nleaf);
-  for (size_t q = 0; q < H.blocks.size(); ++q) {
-    const HBlock& b = H.blocks[q];
-    int64_t l = std::upper_bound(ls.begin(), ls.end(), b.rs) - ls.begin() - 1;
-    for (; l < nleaf && ls[l] < b.re; ++l) per[l].push_back(code_of[q]);
+  std::vector<int32_t> seg;
+  for (size_t l = 0; l + 1 < ls.size(); ++l) {
+    const int32_t a = ls[l], n = ls[l + 1] - ls[l];
+    const int32_t pieces = (n + SEG_MAX - 1) / SEG_MAX;
+    for (int32_t p = 0; p < pieces; ++p) seg.push_back(a + static_cast<int32_t>((int64_t)n * p / pieces));
   }
-  std::vector<int64_t> ip(nleaf + 1, 0);
-  std::vector<int32_t> items;
-  for (int64_t l = 0; l < nleaf; ++l) {
-    items.insert(items.end(), per[l].begin(), per[l].end());
-    ip[l + 1] = static_cast<int64_t>(items.size());
+  seg.push_back(static_cast<int32_t>(H.Nb));
+  const int64_t nseg = static_cast<int64_t>(seg.size()) - 1;
+
+  std::vector<PackJob> jf, jn;
+  std::vector<FarUnit> units;
+  std::vector<FarGroup> groups;
+  std::vector<std::vector<RowItem>> far_items(nseg), near_items(nseg);
+  int64_t fpos = 0, npos = 0, zpos = 0, ppos = 0, nf = 0, nn = 0;
+  for (const HBlock& b : H.blocks) {
+    const int32_t m = b.re - b.rs, n = b.ce - b.cs;
+    int64_t sg = std::upper_bound(seg.begin(), seg.end(), b.rs) - seg.begin() - 1;
+    SPX_CHECK(sg >= 0 && seg[sg] == b.rs, "block rows do not start at a segment boundary");
+    if (b.type == 1) {
+      const int32_t k = b.rank;
+      const int32_t ldv = static_cast<int32_t>(round_up(n, EF));
+      const int64_t pv = fpos;
+      jf.push_back(PackJob{b.off_v, pv, k, n, ldv, n, 1});
+      fpos = round_up(pv + (int64_t)k * ldv, EF);
+      const int32_t P = (n + ZCOLS - 1) / ZCOLS;
+      for (int32_t q0 = 0; q0 < k; q0 += ZROWS) {
+        const int32_t nrows = std::min(ZROWS, k - q0);
+        if (P == 1) {
+          units.push_back(FarUnit{pv + (int64_t)q0 * ldv, ldv, n, b.cs, nrows, static_cast<int32_t>(zpos + q0), -1});
+        } else {
+          const int32_t g = static_cast<int32_t>(groups.size());
+          groups.push_back(FarGroup{static_cast<int32_t>(ppos), P, static_cast<int32_t>(zpos + q0), nrows});
+          for (int32_t p = 0; p < P; ++p) {
+            const int32_t c0 = p * ZCOLS;
+            units.push_back(FarUnit{pv + (int64_t)q0 * ldv + c0, ldv, std::min(ZCOLS, n - c0), b.cs + c0, nrows,
+                                    static_cast<int32_t>(ppos + (int64_t)p * ZROWS), g});
+          }
+          ppos += (int64_t)P * ZROWS;
+        }
+      }
+      for (; sg < nseg && seg[sg] < b.re; ++sg) {
+        const int32_t a = seg[sg], nr = seg[sg + 1] - seg[sg];
+        const int32_t ld = static_cast<int32_t>(round_up(nr, EF));
+        jf.push_back(PackJob{b.off_u + (a - b.rs), fpos, k, nr, ld, m, 1});
+        far_items[sg].push_back(RowItem{fpos, k, static_cast<int32_t>(zpos)});
+        fpos = round_up(fpos + (int64_t)k * ld, EF);
+      }
+      zpos += k;
+      ++nf;
+    } else {
+      for (; sg < nseg && seg[sg] < b.re; ++sg) {
+        const int32_t a = seg[sg], nr = seg[sg + 1] - seg[sg];
+        const int32_t ld = static_cast<int32_t>(round_up(nr, EN));
+        jn.push_back(PackJob{b.off_u + (int64_t)(a - b.rs) * n, npos, n, nr, ld, 1, n});
+        near_items[sg].push_back(RowItem{npos, n, b.cs});
+        npos = round_up(npos + (int64_t)n * ld, EN);
+      }
+      ++nn;
+    }
   }
-  H.nleaf = nleaf;
-  H.leaf_start.upload(ls, s);
+  SPX_CHECK(zpos < (int64_t(1) << 31) && ppos < (int64_t(1) << 31), "far-field rank sum exceeds 2^31");
+  H.n_far = nf;
+  H.n_near = nn;
+  H.zlen = zpos;
+  H.zpart_len = ppos;
+  H.far_f.alloc(std::max<int64_t>(fpos, 1) * sizeof(TF));
+  H.near_f.alloc(std::max<int64_t>(npos, 1) * sizeof(TN));
+  H.bytes_far = fpos * (int64_t)sizeof(TF);
+  H.bytes_near = npos * (int64_t)sizeof(TN);
+  run_pack_jobs_f(jf, H.far_pool64.p, H.far_f.p, H.prec, false, s);
+  run_pack_jobs_f(jn, H.near_pool64.p, H.near_f.p, H.prec, true, s);
+
+  // far_z units dealt to warps in contiguous ranges of about equal cost
+  const int nsm = num_sms(H.device);
+  const int64_t nw = static_cast<int64_t>(nsm) * Z_CTAS_PER_SM * Z_WARPS;
+  std::vector<double> cost(units.size() + 1, 0.0);
+  for (size_t u = 0; u < units.size(); ++u) {
+    const FarUnit& U = units[u];
+    cost[u + 1] = cost[u] + (double)U.nrows * round_up(U.nc, EF) * sizeof(TF) + 8.0 * U.nc + 1024.0;
+  }
+  std::vector<int32_t> wf(nw + 1, 0);
+  size_t u = 0;
+  for (int64_t w = 0; w <= nw; ++w) {
+    const double target = cost.back() * static_cast<double>(w) / static_cast<double>(nw);
+    while (u < units.size() && cost[u] < target) ++u;
+    wf[w] = static_cast<int32_t>(u);
+  }
+  wf[nw] = static_cast<int32_t>(units.size());
+  H.nunits = static_cast<int64_t>(units.size());
+  H.nwarps_z = nw;
+  H.units.upload(units, s);
+  H.warp_first.upload(wf, s);
+  H.groups.upload(groups, s);
+  H.gcnt.alloc(std::max<size_t>(groups.size(), 1));
+  H.gcnt.zero(s);
+
+  std::vector<int64_t> ip(nseg + 1, 0), nb(nseg, 0);
+  std::vector<RowItem> items;
+  for (int64_t g = 0; g < nseg; ++g) {
+    items.insert(items.end(), far_items[g].begin(), far_items[g].end());
+    nb[g] = static_cast<int64_t>(items.size());
+    items.insert(items.end(), near_items[g].begin(), near_items[g].end());
+    ip[g + 1] = static_cast<int64_t>(items.size());
+  }
+  H.nseg = nseg;
+  H.seg_start.upload(seg, s);
   H.item_ptr.upload(ip, s);
+  H.near_begin.upload(nb, s);
   H.items.upload(items, s);
-  int max_leaf = 0;
-  for (int64_t l = 0; l < nleaf; ++l) max_leaf = std::max(max_leaf, ls[l + 1] - ls[l]);
-  SPX_CHECK(max_leaf <= 2048, "leaf clusters larger than 2048 rows are not supported by the apply kernel");
   SPX_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class TF, class TN, class TA, class TX, class TS>
+void launch_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS* add, TS* yb, TX* xp, TA* z,
+                  TA* zpart, cudaStream_t s) {
+  const int64_t Nb = H.Nb;
+  k_hgather<TS, TX><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, src, gidx, H.perm.p, xp);
+  SPX_LAUNCH_CHECK();
+  if (H.nunits > 0) {
+    const unsigned ctas = static_cast<unsigned>((H.nwarps_z + Z_WARPS - 1) / Z_WARPS);
+    k_far_z<TF, TA, TX><<<ctas, Z_WARPS * 32, 0, s>>>(H.units.p, H.warp_first.p, static_cast<int>(H.nwarps_z),
+                                                       reinterpret_cast<const TF*>(H.far_f.p), xp, z, zpart,
+                                                       H.groups.p, H.gcnt.p);
+    SPX_LAUNCH_CHECK();
+  }
+  k_rows<TF, TN, TA, TX, TS><<<static_cast<unsigned>(H.nseg), ROWS_WARPS * 32, 0, s>>>(
+      H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TF*>(H.far_f.p),
+      reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, gidx, dst, add, yb,
+      (H.prec != Prec::F64 && sizeof(TA) == sizeof(float)) ? 1 : 0);
+  SPX_LAUNCH_CHECK();
 }
 
 template <class TF, class TN, class TA, class TX, class TS>
@@ -332,23 +501,10 @@ void do_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS*
   const int64_t Nb = H.Nb;
   if (H.xperm.n < Nb * sizeof(TX)) H.xperm.alloc(Nb * sizeof(TX));
   if (H.z.n < std::max<int64_t>(H.zlen, 1) * sizeof(TA)) H.z.alloc(std::max<int64_t>(H.zlen, 1) * sizeof(TA));
-  TX* xp = reinterpret_cast<TX*>(H.xperm.p);
-  TA* z = reinterpret_cast<TA*>(H.z.p);
-  k_hgather<TS, TX><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, src, gidx, H.perm.p, xp);
-  SPX_LAUNCH_CHECK();
-  if (H.n_far > 0) {
-    k_far_z<TF, TA, TX><<<static_cast<unsigned>(H.n_far), 128, 0, s>>>(
-        H.far_meta.p, H.far_voff.p, H.far_zoff.p, reinterpret_cast<const TF*>(H.far_f.p), xp, z);
-    SPX_LAUNCH_CHECK();
-  }
-  int max_leaf = H.cfg.leaf_size;
-  const size_t smem = 2 * ROWS_GROUPS * static_cast<size_t>(std::max(max_leaf, 1)) * sizeof(TA);
-  k_rows<TF, TN, TA, TX, TS><<<static_cast<unsigned>(H.nleaf), ROWS_GROUPS * ROWS_GSIZE, smem, s>>>(
-      H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
-      reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
-      reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, gidx, dst, add, yb,
-      (H.prec == Prec::MIXED && sizeof(TA) == sizeof(float)) ? 1 : 0);
-  SPX_LAUNCH_CHECK();
+  if (H.zpart.n < std::max<int64_t>(H.zpart_len, 1) * sizeof(TA))
+    H.zpart.alloc(std::max<int64_t>(H.zpart_len, 1) * sizeof(TA));
+  launch_apply<TF, TN, TA, TX, TS>(H, src, gidx, dst, add, yb, reinterpret_cast<TX*>(H.xperm.p),
+                                   reinterpret_cast<TA*>(H.z.p), reinterpret_cast<TA*>(H.zpart.p), s);
 }
 }  // namespace
 
@@ -388,20 +544,21 @@ void HMatrix::apply_f64(const double* x, double* y, cudaStream_t s) {
 }
 
 int64_t HMatrix::device_bytes() const {
-  return static_cast<int64_t>(far_f.bytes() + near_f.bytes() + far_uoff.bytes() + far_voff.bytes() +
-                              far_zoff.bytes() + far_meta.bytes() + near_off.bytes() + near_meta.bytes() +
-                              leaf_start.bytes() + item_ptr.bytes() + items.bytes() + z.bytes() +
-                              xperm.bytes() + diag_perm.bytes() + perm.bytes());
+  return static_cast<int64_t>(far_f.bytes() + near_f.bytes() + units.bytes() + warp_first.bytes() + groups.bytes() +
+                              gcnt.bytes() + seg_start.bytes() + item_ptr.bytes() + near_begin.bytes() +
+                              items.bytes() + z.bytes() + zpart.bytes() + xperm.bytes() + diag_perm.bytes() +
+                              perm.bytes());
 }
 
 }  // namespace spx
 
 // ------------------------------------------------------------------ apply without allocation
 // spx_hmat_apply_noalloc runs the same three kernels as spx_hmat_apply, but its scratch
-// (x in permuted order, then the far-field z vectors) lives in this fixed device array
-// instead of buffers allocated on first use.  Every device that loads the library holds
-// the array until the process exits.  In host code the symbol is only a stand-in: the
-// device address comes from cudaGetSymbolAddress, looked up once per device.
+// (x in permuted order, the far-field z vectors and the partial sums of long rows) lives in
+// this fixed device array instead of buffers allocated on first use.  Every device that
+// loads the library holds the array until the process exits.  In host code the symbol is
+// only a stand-in: the device address comes from cudaGetSymbolAddress, looked up once per
+// device.
 namespace spx {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
@@ -428,27 +585,15 @@ template <class TF, class TN, class TA, class TX>
 void apply_noalloc_impl(HMatrix& H, const double* x, double* y, cudaStream_t s) {
   const int64_t Nb = H.Nb;
   const size_t xbytes = ((static_cast<size_t>(Nb) * sizeof(TX) + 255) / 256) * 256;
-  const size_t zbytes = static_cast<size_t>(std::max<int64_t>(H.zlen, 1)) * sizeof(TA);
-  if (xbytes + zbytes > kNoAllocScratchBytes)
+  const size_t zbytes = ((static_cast<size_t>(std::max<int64_t>(H.zlen, 1)) * sizeof(TA) + 255) / 256) * 256;
+  const size_t pbytes = static_cast<size_t>(std::max<int64_t>(H.zpart_len, 1)) * sizeof(TA);
+  if (xbytes + zbytes + pbytes > kNoAllocScratchBytes)
     throw Error(ERR_INVALID, "H-matrix too large for the 32 MiB static scratch of spx_hmat_apply_noalloc "
-                             "(needs " + std::to_string(xbytes + zbytes) + " bytes); use spx_hmat_apply");
+                             "(needs " + std::to_string(xbytes + zbytes + pbytes) + " bytes); use spx_hmat_apply");
   unsigned char* base = static_cast<unsigned char*>(noalloc_scratch_address());
-  TX* xp = reinterpret_cast<TX*>(base);
-  TA* z = reinterpret_cast<TA*>(base + xbytes);
-  k_hgather<double, TX><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, x, nullptr, H.perm.p, xp);
-  SPX_LAUNCH_CHECK();
-  if (H.n_far > 0) {
-    k_far_z<TF, TA, TX><<<static_cast<unsigned>(H.n_far), 128, 0, s>>>(
-        H.far_meta.p, H.far_voff.p, H.far_zoff.p, reinterpret_cast<const TF*>(H.far_f.p), xp, z);
-    SPX_LAUNCH_CHECK();
-  }
-  const size_t smem = 2 * ROWS_GROUPS * static_cast<size_t>(std::max(H.cfg.leaf_size, 1)) * sizeof(TA);
-  k_rows<TF, TN, TA, TX, double><<<static_cast<unsigned>(H.nleaf), ROWS_GROUPS * ROWS_GSIZE, smem, s>>>(
-      H.leaf_start.p, H.item_ptr.p, H.items.p, H.far_meta.p, H.far_uoff.p, H.far_zoff.p,
-      reinterpret_cast<const TF*>(H.far_f.p), H.near_meta.p, H.near_off.p,
-      reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, nullptr, y, nullptr, nullptr,
-      (H.prec == Prec::MIXED && sizeof(TA) == sizeof(float)) ? 1 : 0);
-  SPX_LAUNCH_CHECK();
+  launch_apply<TF, TN, TA, TX, double>(H, x, nullptr, y, nullptr, nullptr, reinterpret_cast<TX*>(base),
+                                       reinterpret_cast<TA*>(base + xbytes),
+                                       reinterpret_cast<TA*>(base + xbytes + zbytes), s);
 }
 
 }  // namespace

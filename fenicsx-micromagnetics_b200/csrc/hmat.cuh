@@ -57,6 +57,22 @@ struct HBlock {
   double relres;
 };
 
+// Apply-side records (see hmat.cu).  FarUnit: rows [zout, zout + nrows) of z (or of the
+// partial-sum buffer when grp >= 0) from V rows starting at element voff (row stride ldv),
+// columns [xc, xc + nc) of x~.  RowItem: a tile of len rows at element off, row q scaled by
+// z[src + q] (far) or x~[src + q] (near).
+struct FarUnit {
+  int64_t voff;
+  int32_t ldv, nc, xc, nrows, zout, grp;
+};
+struct FarGroup {
+  int32_t pbase, npieces, zdst, nrows;
+};
+struct RowItem {
+  int64_t off;
+  int32_t len, src;
+};
+
 struct HMatrix {
   int device = 0;
   int64_t Nb = 0;
@@ -72,16 +88,17 @@ struct HMatrix {
   Prec prec = Prec::F64;
   bool packed = false;
   DevBuf<char> far_f, near_f;     // factor / tile storage in the packed precision
-  DevBuf<int64_t> far_uoff, far_voff, far_zoff;  // per far block (element offsets)
-  DevBuf<int32_t> far_meta;       // per far block: rs, m, cs, n, k, ldv (padded V row length)
-  DevBuf<int64_t> near_off;       // per near tile
-  DevBuf<int32_t> near_meta;      // per near tile: rs, m, cs, n
-  DevBuf<int32_t> leaf_start;     // [nleaf+1] row ranges of leaf clusters (perm space)
-  DevBuf<int64_t> item_ptr;       // [nleaf+1]
-  DevBuf<int32_t> items;          // encoded item: (block index << 1) | is_far
-  DevBuf<char> z;                 // far z vectors (accumulation type)
+  DevBuf<FarUnit> units;          // k_far_z work units
+  DevBuf<int32_t> warp_first;     // [nwarps_z + 1] unit range of each k_far_z warp
+  DevBuf<FarGroup> groups;        // row batches cut into column pieces
+  DevBuf<unsigned int> gcnt;      // per group: pieces arrived (reset by the last one)
+  DevBuf<int32_t> seg_start;      // [nseg + 1] row segments (perm space)
+  DevBuf<int64_t> item_ptr;       // [nseg + 1] items of each segment: far ones, then near ones
+  DevBuf<int64_t> near_begin;     // [nseg] first near item of each segment
+  DevBuf<RowItem> items;
+  DevBuf<char> z, zpart;          // far z vectors and partial sums (accumulation type)
   DevBuf<char> xperm;             // x in perm order (vector type)
-  int64_t nleaf = 0, zlen = 0, n_far = 0, n_near = 0;
+  int64_t nseg = 0, zlen = 0, zpart_len = 0, n_far = 0, n_near = 0, nunits = 0, nwarps_z = 0;
   int64_t bytes_far = 0, bytes_near = 0;
 
   void build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s);

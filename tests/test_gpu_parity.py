@@ -111,6 +111,33 @@ def test_hmatrix_build_vs_reference(spx, golden, name):
     assert rel(Hx, B @ g["x"]) < 1e-5
 
 
+def test_hmatrix_long_rows_vs_dense(spx):
+    """A film whose partition has far blocks wider than one k_far_z column piece (1024
+    columns): every packed precision against the dense operator, bitwise-repeatable
+    applies, and the no-allocation entry point equal to the allocating one."""
+    X, T = omesh.kuhn_box(100, 100, 2, 2.5)
+    geom = spx.BoundaryGeometry(X, T)
+    H = spx.HMatrixGPUPackedFused(geom, spx.HMatrixBuildConfig(epsilon=1e-5), precision="f64")
+    b = H.blocks()
+    far = b[b[:, 4] == 1]
+    assert (far[:, 3] - far[:, 2]).max() > 1024
+    g = torch.Generator(device=DEV).manual_seed(7)
+    x = torch.randn(H.size, dtype=torch.float64, device=DEV, generator=g)
+    B = geom.dense_B()
+    yd = B @ x
+    del B
+    torch.cuda.empty_cache()
+    for prec, tol in (("f64", 1e-5), ("f32", 1e-5), ("mixed", 1e-3)):
+        H.repack(prec)
+        y1 = H.matvec(x).clone()
+        y2 = H.matvec(x).clone()
+        assert torch.equal(y1, y2)
+        assert float(torch.linalg.norm(y1 - yd) / torch.linalg.norm(yd)) < tol, prec
+        yn = torch.empty_like(x)
+        H.matvec_noalloc(x, yn)
+        assert torch.equal(yn, y1)
+
+
 def test_hmatrix_reduced_precisions(spx, golden):
     g = golden("hmat_film48.npz")
     X, T = omesh.kuhn_box(*CASES["film48"])
