@@ -1,0 +1,84 @@
+// Smoothed-aggregation algebraic multigrid for the scalar P1 Poisson systems.
+//
+// The reference preconditions its u1 Krylov solve with PETSc GAMG
+// (gpu/fields/Demag_Lindholm_GPU.py:215-222: KSP "cg", PC "gamg").  This is a restatement
+// of the same method family, set up on the host once per mesh and cycled on the device:
+//   * strength of connection |a_ij| > theta sqrt(a_ii a_jj), three-pass greedy aggregation
+//     (root + strong neighbours; attach leftovers to a neighbouring aggregate; group the
+//     rest), in vertex order;
+//   * tentative prolongator from the near-null vector w (piecewise w / ||w_aggregate||),
+//     smoothed once: P = (I - omega D^-1 A) P0, omega = 4 / (3 lambda_max(D^-1 A));
+//   * Galerkin coarse operators A_c = P^T A P, down to at most `coarse_max` unknowns, whose
+//     dense inverse (with a rank-one term w w^T when the system is singular) is applied
+//     exactly;
+//   * V(2,2) cycle with Chebyshev-Jacobi smoothing on [0.1, 1.1] x lambda_max(D^-1 A)
+//     (PETSc's default eigenvalue transform for GAMG level smoothers).
+// The cycle runs in FP32 inside an FP64 preconditioned CG (k_pcg_amg in amg.cu).
+#pragma once
+
+#include "spx_internal.cuh"
+
+namespace spx {
+
+struct CsrHost {
+  int64_t n = 0, ncols = 0;
+  std::vector<int64_t> rp;
+  std::vector<int32_t> ci;
+  std::vector<double> v;
+};
+
+struct AmgOptions {
+  double theta = 0.0;      // strength threshold (0: every nonzero off-diagonal is strong)
+  int64_t coarse_max = 256;
+  int max_levels = 10;
+  int power_iters = 20;
+};
+
+struct AmgHostLevel {
+  CsrHost A, P, R;         // P: n x n_next, R = P^T
+  std::vector<double> dinv;
+  double lmax = 0.0;       // estimate of lambda_max(D^-1 A)
+};
+
+struct AmgHost {
+  std::vector<AmgHostLevel> lv;   // lv.back() is the dense coarsest level (no P/R)
+  std::vector<double> coarse_inv; // n_c x n_c, row-major
+};
+
+// A: symmetric positive (semi)definite CSR with sorted columns; null: its near-null vector
+// (A null = 0 when singular).
+void amg_build(const CsrHost& A, const std::vector<double>& null, bool singular, const AmgOptions& o,
+               AmgHost& out);
+
+// Device side ---------------------------------------------------------------------------
+struct AmgLevelDev {
+  int64_t n, nslices;
+  const int64_t* sp;
+  const int32_t* col;
+  const float* val;
+  const float* dinv;
+  int64_t p_nslices, r_nslices;
+  const int64_t* p_sp;
+  const int32_t* p_col;
+  const float* p_val;
+  const int64_t* r_sp;
+  const int32_t* r_col;
+  const float* r_val;
+  float *b, *x, *x2, *d, *r;
+  float theta, delta, sigma;
+  int cta;  // 1: the level is cycled by CTA 0 alone
+};
+
+struct AmgDevice {
+  int nlev = 0, nlev_grid = 0;
+  int64_t n0 = 0, nc = 0;
+  std::vector<DevSell<float>> A, P, R;
+  std::vector<DevBuf<float>> val, pval, rval, dinv, vec;
+  DevBuf<AmgLevelDev> lv;
+  DevBuf<float> cinv;
+  std::vector<int64_t> sizes, nnz;
+  void upload(const AmgHost& h, cudaStream_t s);
+  int64_t device_bytes() const;
+};
+
+}  // namespace spx

@@ -555,6 +555,9 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
     if (opt->maxit_u1 > 0) o.maxit_u1 = opt->maxit_u1;
     if (opt->maxit_u2 > 0) o.maxit_u2 = opt->maxit_u2;
     o.warm_start = opt->warm_start;
+    SPX_CHECK(opt->u1_preconditioner == 0 || opt->u1_preconditioner == 1,
+              "u1_preconditioner must be 0 (AMG) or 1 (Jacobi)");
+    o.u1_pc = opt->u1_preconditioner;
     o.hcfg = to_hcfg(&opt->hmat);
   }
   auto d = std::make_unique<spx_demag_s>();

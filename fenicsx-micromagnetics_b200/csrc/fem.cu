@@ -145,54 +145,7 @@ __global__ void k_extrap(int64_t n, const double* __restrict__ h0, const double*
   out[i] = static_cast<T>(v);
 }
 
-// ------------------------------------------------------------------ CTA reductions
 constexpr int CG_BLOCK = 1024;
-
-// sum of up to 4 values over the CTA; result valid in every thread (sh >= 4*32+4 doubles)
-__device__ __forceinline__ void cta_sum4(double v[4], double* sh) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
-  __syncthreads();
-  if (lane == 0)
-    for (int q = 0; q < 4; ++q) sh[4 * wid + q] = v[q];
-  __syncthreads();
-  const int nw = (blockDim.x + 31) >> 5;
-  if (wid == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      double t = (lane < nw) ? sh[4 * lane + q] : 0.0;
-      t = warp_sum(t);
-      if (lane == 0) sh[128 + q] = t;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 4; ++q) v[q] = sh[128 + q];
-  __syncthreads();
-}
-
-// write this CTA's partials of slot s
-__device__ __forceinline__ void cta_partial(double* part, int s, double a, double b, double c, double d,
-                                            double* sh) {
-  double v[4] = {a, b, c, d};
-  cta_sum4(v, sh);
-  if (threadIdx.x < 4) part[(static_cast<int64_t>(s) * gridDim.x + blockIdx.x) * 4 + threadIdx.x] = v[threadIdx.x];
-}
-
-// total of slot s over all CTAs, same order in every CTA (call after a grid barrier)
-__device__ __forceinline__ void cta_total(const double* part, int s, double out[4], double* sh) {
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int c = threadIdx.x; c < static_cast<int>(gridDim.x); c += blockDim.x) {
-    const double* p = part + (static_cast<int64_t>(s) * gridDim.x + c) * 4;
-    v[0] += p[0];
-    v[1] += p[1];
-    v[2] += p[2];
-    v[3] += p[3];
-  }
-  cta_sum4(v, sh);
-  for (int q = 0; q < 4; ++q) out[q] = v[q];
-}
 
 #define CG_ROWS_BEGIN                                               \
   for (int64_t sl = gw; sl < P.nslices; sl += nw) {                 \
@@ -606,7 +559,8 @@ template <class TM>
 template <class TV>
 CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project,
                             int slot, cudaStream_t st, bool sync_stats) {
-  const bool ir = sizeof(TM) == sizeof(float);
+  const bool use_amg = static_cast<bool>(amg);
+  const bool ir = sizeof(TM) == sizeof(float) || use_amg;  // solution state kept in y64
   SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
   if (slot >= 0) {
     SPX_CHECK(slot < 4, "extrapolation slot out of range");
@@ -623,7 +577,9 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   }
   SPX_CUDA(cudaMemsetAsync(bar.p, 0, bar.bytes(), st));
   SPX_CUDA(cudaMemsetAsync(err.p, 0, err.bytes(), st));
-  if (ir) {
+  if (use_amg) {
+    launch_amg<TV>(b, x, rtol, atol, maxit, warm, project, st);
+  } else if (sizeof(TM) == sizeof(float)) {
     CgIrParams<TV> q;
     q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
     q.v32 = reinterpret_cast<const float*>(vals.p); q.v64 = vals64.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
@@ -727,6 +683,7 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
       for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
         if (fem.col[k] == i) d[i] = fem.A[k];
     cg1.setup(hsell, a, d);
+    if (opt.u1_pc == 0) cg1.enable_amg(fem.rowptr, fem.col, fem.A, d, true, s);
   }
   std::vector<int32_t> bmap(N, -1), imap(N, -1), inter;
   for (int64_t k = 0; k < Nb; ++k) bmap[bd.host.bverts[k]] = static_cast<int32_t>(k);
@@ -832,7 +789,8 @@ template <class TV, class TM>
 int64_t DemagCtx<TV, TM>::device_bytes() const {
   int64_t tot = 0;
   tot += P.slice_ptr.bytes() + P.col.bytes() + Div.bytes() + Dsum.bytes() + Gv.bytes() + vol.bytes();
-  tot += cg1.vals.bytes() + cg1.vals64.bytes() + cg1.work.bytes() + cg1.P.col.bytes();
+  tot += cg1.vals.bytes() + cg1.vals64.bytes() + cg1.work.bytes() + cg1.P.col.bytes() + cg1.amg_work.bytes();
+  if (cg1.amg) tot += cg1.amg->device_bytes();
   tot += cg2.vals.bytes() + cg2.vals64.bytes() + cg2.work.bytes() + cg2.P.col.bytes();
   tot += AIB.bytes() + PIB.col.bytes() + Bdense.bytes();
   tot += H.device_bytes();

@@ -10,6 +10,9 @@
 // rounded matrix value multiplies a small nodal difference instead of a large value.
 #pragma once
 
+#include <memory>
+
+#include "amg.cuh"
 #include "hmat.cuh"
 
 namespace spx {
@@ -95,7 +98,18 @@ struct CgSystem {
   double inner_rtol = 1e-3;
   int max_outer = 10;
   int grid = 0, block = 0;
+  // AMG-preconditioned FP64 CG (k_pcg_amg) instead of the Jacobi solvers when enabled
+  std::unique_ptr<AmgDevice> amg;
+  DevBuf<double> amg_work;  // r, p, q
+  double amg_ww = 0.0;
+  bool amg_singular = false;
+  int amg_grid = 0;
   void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
+  // build the AMG hierarchy of D^-1/2 A D^-1/2 from the CSR of A (same rows as setup)
+  void enable_amg(const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col, const std::vector<double>& a,
+                  const std::vector<double>& d, bool singular, cudaStream_t s);
+  template <class TV>
+  void launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, cudaStream_t st);
   template <class TV>
   CgStats solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, int slot,
                 cudaStream_t st, bool sync_stats);
@@ -111,6 +125,7 @@ struct DemagOptions {
   double rtol_u1 = 1e-6, rtol_u2 = 1e-6, atol = 1e-12;
   int maxit_u1 = 2000, maxit_u2 = 12000;
   int warm_start = 0;       // 0 zero start, 1 previous solution, 2 extrapolated per RK stage
+  int u1_pc = 0;            // u1 preconditioner: 0 smoothed-aggregation AMG, 1 Jacobi
   HBuildConfig hcfg;
 };
 

@@ -253,6 +253,54 @@ __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* 
   return s_ok != 0;
 }
 
+// ------------------------------------------------------------------ CTA reductions
+// sum of up to 4 values over the CTA; result valid in every thread (sh >= 4*32+4 doubles)
+__device__ __forceinline__ void cta_sum4(double v[4], double* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = warp_sum(v[q]);
+  __syncthreads();
+  if (lane == 0)
+    for (int q = 0; q < 4; ++q) sh[4 * wid + q] = v[q];
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      double t = (lane < nw) ? sh[4 * lane + q] : 0.0;
+      t = warp_sum(t);
+      if (lane == 0) sh[128 + q] = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = sh[128 + q];
+  __syncthreads();
+}
+
+// write this CTA's partials of slot s
+__device__ __forceinline__ void cta_partial(double* part, int s, double a, double b, double c, double d,
+                                            double* sh) {
+  double v[4] = {a, b, c, d};
+  cta_sum4(v, sh);
+  if (threadIdx.x < 4) part[(static_cast<int64_t>(s) * gridDim.x + blockIdx.x) * 4 + threadIdx.x] = v[threadIdx.x];
+}
+
+// total of slot s over all CTAs, same order in every CTA (call after a grid barrier)
+__device__ __forceinline__ void cta_total(const double* part, int s, double out[4], double* sh) {
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int c = threadIdx.x; c < static_cast<int>(gridDim.x); c += blockDim.x) {
+    const double* p = part + (static_cast<int64_t>(s) * gridDim.x + c) * 4;
+    v[0] += p[0];
+    v[1] += p[1];
+    v[2] += p[2];
+    v[3] += p[3];
+  }
+  cta_sum4(v, sh);
+  for (int q = 0; q < 4; ++q) out[q] = v[q];
+}
+
+
 // precision helpers
 template <class T> __device__ __forceinline__ float to_f(T v) { return static_cast<float>(v); }
 template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }

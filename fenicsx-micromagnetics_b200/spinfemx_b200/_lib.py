@@ -28,7 +28,7 @@ class HmatConfig(C.Structure):
 class DemagOptions(C.Structure):
     _fields_ = [("backend", c_i32), ("precision", c_i32), ("rtol_u1", c_dbl), ("rtol_u2", c_dbl),
                 ("atol", c_dbl), ("maxit_u1", c_i32), ("maxit_u2", c_i32), ("warm_start", c_i32),
-                ("reserved", c_i32), ("hmat", HmatConfig)]
+                ("u1_preconditioner", c_i32), ("hmat", HmatConfig)]
 
 
 class LLGParams(C.Structure):

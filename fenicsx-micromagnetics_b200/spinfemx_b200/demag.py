@@ -25,7 +25,8 @@ class DemagFieldLindholmGPU:
                  dense_gpu_max_bytes=512 * 1024 ** 2, hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
                  hmatrix_compressor="fullaca", hmatrix_max_rank=None,
                  hmatrix_max_temporary_block_bytes=256 * 1024 ** 2, hmatrix_use_fp32=True, precision="f64",
-                 hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False, **unused):
+                 hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False,
+                 u1_preconditioner="amg", **unused):
         """Options as in the reference, plus:
 
         precision          'f64' | 'f32' (plain FP32) | 'mixed' (FP64 vectors, FP32 matrices,
@@ -34,6 +35,8 @@ class DemagFieldLindholmGPU:
                            precision='f64', 'f32' otherwise)
         warm_start         False: zero start (the reference); True: previous solution;
                            'extrapolate': per-RK-stage quadratic extrapolation (time loop)
+        u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or
+                           'jacobi'
         """
         if str(incident_policy).lower()[:4] != "skip":
             raise ValueError("only incident_policy='skip' (the reference default) is implemented")
@@ -72,6 +75,11 @@ class DemagFieldLindholmGPU:
         self.ksp_rtol_u1, self.ksp_rtol_u2, self.ksp_atol = o.rtol_u1, o.rtol_u2, o.atol
         self.ksp_maxit_u1, self.ksp_maxit_u2 = o.maxit_u1, o.maxit_u2
         o.warm_start = ws
+        pcs = {"amg": 0, "gamg": 0, "jacobi": 1}
+        if str(u1_preconditioner).lower() not in pcs:
+            raise ValueError("u1_preconditioner must be 'amg' or 'jacobi'")
+        o.u1_preconditioner = pcs[str(u1_preconditioner).lower()]
+        self.u1_preconditioner = str(u1_preconditioner).lower()
         o.hmat = _lib.HmatConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
                                  leaf_size=int(hmatrix_leaf_size), max_rank=int(hmatrix_max_rank or 0),
                                  max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),

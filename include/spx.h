@@ -140,8 +140,8 @@ typedef struct {
   int32_t precision; /* SPX_PREC_* */
   double rtol_u1, rtol_u2, atol; /* ksp_rtol_u1/u2 (:216-226, :271-281), atol 1e-12 */
   int32_t maxit_u1, maxit_u2;    /* 2000 / 12000 in the reference */
-  int32_t warm_start;            /* start each CG from the previous solution */
-  int32_t reserved;
+  int32_t warm_start;            /* 0 zero start (reference), 1 previous solution, 2 extrapolated per RK stage */
+  int32_t u1_preconditioner;     /* 0 smoothed-aggregation AMG (the reference's PC "gamg", :219-222), 1 Jacobi */
   spx_hmat_config hmat;
 } spx_demag_options;
 /* DemagFieldLindholmGPU.__init__ (gpu/fields/Demag_Lindholm_GPU.py:101-155) */
