@@ -1,22 +1,23 @@
 // Device side of the smoothed-aggregation AMG (amg.cuh): level upload, the FP32 V-cycle
 // and the FP64 preconditioned CG that uses it, in one persistent cooperative kernel.
 //
-// Level layout: every level matrix (A_l, P_l, R_l = P_l^T) is SELL-32 (one thread per row,
-// 32 rows per slice, padding entries point at column 0 with value 0), FP32 values, FP32
-// vectors b, x, x2, d, r per level.  Levels with many nonzeros are swept by the whole grid
-// (grid barrier between phases); small levels and the dense coarsest solve are swept by
-// CTA 0 alone (__syncthreads between phases) while the other CTAs wait at the next grid
-// barrier.
+// Level layout: A_l and P_l are SELL-32 (one thread per row, 32 rows per slice, padding
+// entries point at column 0 with value 0); R_l = P_l^T is CSR swept by `r_lanes` lanes per
+// row (its rows are long); FP32 values; FP32 vectors b, D^-1 b, x, x2, d, r per level.  Every
+// phase is swept by the whole grid with a grid barrier after it; the dense coarsest level
+// (at most a few thousand unknowns) is one GEMV with its precomputed inverse, a warp per row.
 //
-// PCG (FP64 vectors, scaled system A^ = D^-1/2 A D^-1/2, FP64 values):
+// PCG (FP64 vectors, scaled system A^ = D^-1/2 A D^-1/2):
 //   z = V(r);  beta = (r,z)/(r,z)_old;  c = (w,z)/(w,w) (singular systems: remove the
 //   null-vector component w = D^1/2 1 from z);  p = z - c w + beta p;
-//   q = A^ z + beta q  (A^ w = 0, so q = A^ p without a second SpMV);  alpha = (r,z)/(p,q);
-//   y += alpha p;  r -= alpha q.
-// The recurrence residual is confirmed against the true FP64 residual before returning;
-// stopping rule ||b - A x|| <= max(rtol ||b||, atol) in the unscaled norm, as the IR solver.
+//   q = A^ z + beta q  (A^ w = 0, so q = A^ p without a second SpMV), with A^ z evaluated as
+//   D^-1/2 [sum_j a_ij (u_j - u_i) + (sum_j a_ij) u_i], u = D^-1/2 z, FP32 a_ij, FP64 sums;
+//   alpha = (r,z)/(p,q);  y += alpha p;  r -= alpha q.
+// The recurrence residual is confirmed against the true FP64 residual (FP64 values) before
+// returning; stopping rule ||b - A x|| <= max(rtol ||b||, atol) in the unscaled norm.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "amg.cuh"
 #include "fem.cuh"
@@ -50,91 +51,117 @@ void csr_to_sell(const CsrHost& A, HostSell& s, std::vector<float>& val) {
   s.map.clear();
 }
 
+// in-place Gauss-Jordan inverse of an SPD matrix (no pivoting), one pivot per step
+__global__ void k_gj_pivot(double* __restrict__ M, double* __restrict__ colk, int64_t n, int64_t k) {
+  const double p = M[k * n + k];
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) colk[i] = M[i * n + k];
+  __syncthreads();
+  for (int64_t j = threadIdx.x; j < n; j += blockDim.x) M[k * n + j] = (j == k) ? 1.0 / p : M[k * n + j] / p;
+}
+__global__ void k_gj_update(double* __restrict__ M, const double* __restrict__ colk, int64_t n, int64_t k) {
+  const int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (e >= n * n) return;
+  const int64_t i = e / n, j = e - i * n;
+  if (i == k) return;
+  const double f = colk[i];
+  if (j == k)
+    M[e] = -f * M[k * n + k];
+  else
+    M[e] -= f * M[k * n + j];
+}
+__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (i < n) b[i] = static_cast<float>(a[i]);
+}
+
 }  // namespace
 
 void AmgDevice::upload(const AmgHost& h, cudaStream_t s) {
   nlev = static_cast<int>(h.lv.size());
   n0 = h.lv[0].A.n;
   nc = h.lv.back().A.n;
-  A.clear(); P.clear(); R.clear(); val.clear(); pval.clear(); rval.clear(); dinv.clear(); vec.clear();
-  A.resize(nlev); P.resize(nlev); R.resize(nlev);
+  A.clear(); P.clear(); rrp.clear(); rcol.clear();
+  val.clear(); pval.clear(); rval.clear(); dinv.clear(); vec.clear();
+  A.resize(nlev); P.resize(nlev); rrp.resize(nlev); rcol.resize(nlev);
   val.resize(nlev); pval.resize(nlev); rval.resize(nlev); dinv.resize(nlev); vec.resize(nlev);
   sizes.assign(nlev, 0);
   nnz.assign(nlev, 0);
   std::vector<AmgLevelDev> d(nlev);
-  // grid levels: from the top while the level has enough nonzeros to fill the GPU
-  nlev_grid = 0;
-  for (int l = 0; l + 1 < nlev; ++l) {
-    if (static_cast<int64_t>(h.lv[l].A.ci.size()) < 200000) break;
-    nlev_grid = l + 1;
-  }
   for (int l = 0; l < nlev; ++l) {
     const AmgHostLevel& L = h.lv[l];
     sizes[l] = L.A.n;
     nnz[l] = static_cast<int64_t>(L.A.ci.size());
-    HostSell hs;
-    std::vector<float> v;
+    AmgLevelDev& D = d[l];
+    std::memset(&D, 0, sizeof(D));
+    D.n = L.A.n;
+    std::vector<float> di(L.dinv.begin(), L.dinv.end());
+    dinv[l].upload(di, s);
+    D.dinv = dinv[l].p;
+    vec[l].alloc(6 * static_cast<size_t>(L.A.n));
+    vec[l].zero(s);
+    D.b = vec[l].p;
+    D.db = vec[l].p + L.A.n;
+    D.x = vec[l].p + 2 * L.A.n;
+    D.x2 = vec[l].p + 3 * L.A.n;
+    D.d = vec[l].p + 4 * L.A.n;
+    D.r = vec[l].p + 5 * L.A.n;
+    if (l + 1 == nlev) break;  // dense coarsest: vectors only
+    HostSell hs, hp;
+    std::vector<float> v, vp;
     csr_to_sell(L.A, hs, v);
     A[l].upload(hs, s);
     val[l].upload(v, s);
-    std::vector<float> di(L.dinv.begin(), L.dinv.end());
-    dinv[l].upload(di, s);
-    vec[l].alloc(5 * static_cast<size_t>(L.A.n));
-    vec[l].zero(s);
-    AmgLevelDev& D = d[l];
-    D.n = L.A.n;
     D.nslices = hs.nslices;
     D.sp = A[l].slice_ptr.p;
     D.col = A[l].col.p;
     D.val = val[l].p;
-    D.dinv = dinv[l].p;
-    D.b = vec[l].p;
-    D.x = vec[l].p + L.A.n;
-    D.x2 = vec[l].p + 2 * L.A.n;
-    D.d = vec[l].p + 3 * L.A.n;
-    D.r = vec[l].p + 4 * L.A.n;
-    D.p_nslices = D.r_nslices = 0;
-    D.p_sp = D.r_sp = nullptr;
-    D.p_col = D.r_col = nullptr;
-    D.p_val = D.r_val = nullptr;
-    if (l + 1 < nlev) {
-      HostSell hp, hr;
-      std::vector<float> vp, vr;
-      csr_to_sell(L.P, hp, vp);
-      csr_to_sell(L.R, hr, vr);
-      P[l].upload(hp, s);
-      R[l].upload(hr, s);
-      pval[l].upload(vp, s);
-      rval[l].upload(vr, s);
-      D.p_nslices = hp.nslices;
-      D.p_sp = P[l].slice_ptr.p;
-      D.p_col = P[l].col.p;
-      D.p_val = pval[l].p;
-      D.r_nslices = hr.nslices;
-      D.r_sp = R[l].slice_ptr.p;
-      D.r_col = R[l].col.p;
-      D.r_val = rval[l].p;
-      const double b = 1.1 * L.lmax, a = 0.1 * L.lmax;
-      D.theta = static_cast<float>(0.5 * (b + a));
-      D.delta = static_cast<float>(0.5 * (b - a));
-      D.sigma = static_cast<float>((b + a) / (b - a));
-    } else {
-      D.theta = D.delta = D.sigma = 1.0f;
-    }
-    D.cta = l >= nlev_grid ? 1 : 0;
+    csr_to_sell(L.P, hp, vp);
+    P[l].upload(hp, s);
+    pval[l].upload(vp, s);
+    D.p_nslices = hp.nslices;
+    D.p_sp = P[l].slice_ptr.p;
+    D.p_col = P[l].col.p;
+    D.p_val = pval[l].p;
+    rrp[l].upload(L.R.rp, s);
+    rcol[l].upload(L.R.ci, s);
+    std::vector<float> vr(L.R.v.begin(), L.R.v.end());
+    rval[l].upload(vr, s);
+    D.r_rp = rrp[l].p;
+    D.r_col = rcol[l].p;
+    D.r_val = rval[l].p;
+    const double avg = static_cast<double>(L.R.ci.size()) / std::max<int64_t>(L.R.n, 1);
+    int lanes = 1;
+    while (lanes < 32 && lanes < avg / 2.0) lanes <<= 1;
+    D.r_lanes = lanes;
+    const double b = 1.1 * L.lmax, a = 0.1 * L.lmax;
+    D.theta = static_cast<float>(0.5 * (b + a));
+    D.delta = static_cast<float>(0.5 * (b - a));
+    D.sigma = static_cast<float>((b + a) / (b - a));
   }
   lv.upload(d, s);
-  std::vector<float> ci(h.coarse_inv.begin(), h.coarse_inv.end());
-  cinv.upload(ci, s);
-  SPX_CUDA(cudaStreamSynchronize(s));
+  // coarsest inverse: FP64 Gauss-Jordan on the device, stored FP32
+  {
+    DevBuf<double> M, colk;
+    M.upload(h.coarse_dense, s);
+    colk.alloc(std::max<int64_t>(nc, 1));
+    const int64_t nn = nc * nc;
+    for (int64_t k = 0; k < nc; ++k) {
+      k_gj_pivot<<<1, 1024, 0, s>>>(M.p, colk.p, nc, k);
+      k_gj_update<<<grid_for(nn, 256), 256, 0, s>>>(M.p, colk.p, nc, k);
+    }
+    SPX_LAUNCH_CHECK();
+    cinv.alloc(std::max<int64_t>(nn, 1));
+    k_to_float<<<grid_for(nn, 256), 256, 0, s>>>(M.p, cinv.p, nn);
+    SPX_LAUNCH_CHECK();
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
 }
 
 int64_t AmgDevice::device_bytes() const {
   int64_t t = cinv.bytes() + lv.bytes();
   for (int l = 0; l < nlev; ++l) {
-    t += A[l].slice_ptr.bytes() + A[l].col.bytes() + P[l].slice_ptr.bytes() + P[l].col.bytes() +
-         R[l].slice_ptr.bytes() + R[l].col.bytes() + val[l].bytes() + pval[l].bytes() + rval[l].bytes() +
-         dinv[l].bytes() + vec[l].bytes();
+    t += A[l].slice_ptr.bytes() + A[l].col.bytes() + P[l].slice_ptr.bytes() + P[l].col.bytes() + rrp[l].bytes() +
+         rcol[l].bytes() + val[l].bytes() + pval[l].bytes() + rval[l].bytes() + dinv[l].bytes() + vec[l].bytes();
   }
   return t;
 }
@@ -154,40 +181,44 @@ __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const 
                                           const float* __restrict__ v) {
   const int64_t base = sp[sl];
   const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
-  float acc = 0.0f;
+  const float* vv = val + base + lane;
+  const int32_t* cc = col + base + lane;
+  float a0 = 0.0f, a1 = 0.0f;
   int k = 0;
+  for (; k + 8 <= width; k += 8) {  // eight gathers in flight per thread
+    float w[8];
+    int32_t c[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      w[u] = vv[(k + u) * 32];
+      c[u] = cc[(k + u) * 32];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+      a0 += w[u] * v[c[u]];
+      a1 += w[u + 1] * v[c[u + 1]];
+    }
+  }
   for (; k + 2 <= width; k += 2) {
-    const int64_t i0 = base + (static_cast<int64_t>(k) << 5) + lane;
-    const int64_t i1 = i0 + 32;
-    const float a0 = val[i0], a1 = val[i1];
-    const int32_t c0 = col[i0], c1 = col[i1];
-    acc += a0 * v[c0];
-    acc += a1 * v[c1];
+    const float w0 = vv[k * 32], w1 = vv[(k + 1) * 32];
+    const int32_t c0 = cc[k * 32], c1 = cc[(k + 1) * 32];
+    a0 += w0 * v[c0];
+    a1 += w1 * v[c1];
   }
-  if (k < width) {
-    const int64_t i0 = base + (static_cast<int64_t>(k) << 5) + lane;
-    acc += val[i0] * v[col[i0]];
-  }
-  return acc;
+  if (k < width) a0 += vv[k * 32] * v[cc[k * 32]];
+  return a0 + a1;
 }
 
-// pre-smoothing from x = 0, Chebyshev step 1 and 2 (one SpMV: A d0, d0 = D^-1 b / theta)
+// pre-smoothing from x = 0, Chebyshev steps 1 and 2 (one SpMV: A d0, d0 = D^-1 b / theta)
 __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const int64_t base = L.sp[sl];
-    const int width = static_cast<int>((L.sp[sl + 1] - base) >> 5);
-    float t = 0.0f;
-    for (int k = 0; k < width; ++k) {
-      const int64_t idx = base + (static_cast<int64_t>(k) << 5) + rr.lane;
-      const int32_t c = L.col[idx];
-      t += L.val[idx] * (L.dinv[c] * L.b[c]);
-    }
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db);
     if (i < L.n) {
-      const float di = L.dinv[i], bi = L.b[i];
-      const float d0 = di * bi / L.theta;
-      const float r1 = di * (bi - t / L.theta);
+      const float di = L.dinv[i];
+      const float d0 = L.db[i] / L.theta;
+      const float r1 = L.db[i] - di * t / L.theta;
       const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
       L.x[i] = d0 + d1;
       L.d[i] = d1;
@@ -208,11 +239,25 @@ __device__ void pre_b(const AmgLevelDev& L, RowRange rr) {
   }
 }
 
+// b_c = R r (CSR rows, `r_lanes` lanes per row), db_c = D_c^-1 b_c
 __device__ void restrict_to(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
-  for (int64_t sl = rr.gw; sl < L.r_nslices; sl += rr.nw) {
-    const int64_t a = sl * 32 + rr.lane;
-    const float t = sell_dot(L.r_sp, L.r_col, L.r_val, sl, rr.lane, L.r);
-    if (a < C.n) C.b[a] = t;
+  const int G = L.r_lanes;
+  const int gl = rr.lane & (G - 1);
+  const int64_t rows_per_warp = 32 / G;
+  const int64_t first = rr.gw * rows_per_warp + rr.lane / G, stride = rr.nw * rows_per_warp;
+  const int64_t nrows_pad = (C.n + rows_per_warp - 1) / rows_per_warp * rows_per_warp;
+  for (int64_t a = first - rr.lane / G; a < nrows_pad; a += stride) {  // uniform per warp
+    const int64_t row = a + rr.lane / G;
+    float t = 0.0f;
+    if (row < C.n) {
+      const int64_t k1 = L.r_rp[row + 1];
+      for (int64_t k = L.r_rp[row] + gl; k < k1; k += G) t += L.r_val[k] * L.r[L.r_col[k]];
+    }
+    for (int o = G >> 1; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (row < C.n && gl == 0) {
+      C.b[row] = t;
+      C.db[row] = C.dinv[row] * t;
+    }
   }
 }
 
@@ -230,7 +275,7 @@ __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
     const int64_t i = sl * 32 + rr.lane;
     const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x);
     if (i < L.n) {
-      const float r0 = L.dinv[i] * (L.b[i] - t);
+      const float r0 = L.db[i] - L.dinv[i] * t;
       const float d0 = r0 / L.theta;
       L.x2[i] = L.x[i] + d0;
       L.d[i] = d0;
@@ -239,9 +284,11 @@ __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
   }
 }
 
-// post-smoothing step 2; optionally the partial dots (r64, z) and (w, z) of the FP64 PCG
+// post-smoothing step 2; on the top level also u = D^-1/2 z (FP64) and the partial dots
+// (r64, z), (w, z) of the PCG
 __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
-                       const double* __restrict__ sdinv, double& rz, double& wz, bool dots) {
+                       const double* __restrict__ sdinv, double* __restrict__ u, double& rz, double& wz,
+                       bool top) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
@@ -251,22 +298,24 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
       const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;
       const float z = L.x2[i] + d1;
       L.x[i] = z;
-      if (dots) {
-        rz += r64[i] * static_cast<double>(z);
-        wz += static_cast<double>(z) / sdinv[i];
+      if (top) {
+        const double zd = static_cast<double>(z);
+        u[i] = zd * sdinv[i];
+        rz += r64[i] * zd;
+        wz += zd / sdinv[i];
       }
     }
   }
 }
 
-// x = C^-1 b on the dense coarsest level (warps over rows, lanes over columns)
-__device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int64_t i = warp; i < nc; i += nw) {
+// x = C^-1 b on the dense coarsest level: a warp per row over the grid
+__device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, RowRange rr) {
+  for (int64_t i = rr.gw; i < nc; i += rr.nw) {
+    const float* row = cinv + i * nc;
     float s = 0.0f;
-    for (int64_t j = lane; j < nc; j += 32) s += cinv[i * nc + j] * L.b[j];
+    for (int64_t j = rr.lane; j < nc; j += 32) s += row[j] * L.b[j];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) L.x[i] = s;
+    if (rr.lane == 0) L.x[i] = s;
   }
 }
 
@@ -275,12 +324,14 @@ struct PcgParams {
   int64_t n, nslices;
   const int64_t* sp;
   const int32_t* col;
-  const double* v64;
+  const double* v64;   // scaled FP64 values (true residual)
+  const float* a32;    // unscaled FP32 values (difference-form SpMV)
+  const double* rsum;  // row sums of the unscaled matrix
   const double* sdinv;
   const double* diag;
   const TV* b;
   TV* x;
-  double *bh, *y, *r, *p, *q;
+  double *bh, *y, *r, *p, *q, *u;
   double* part;
   unsigned int* bar;
   int* err;
@@ -291,7 +342,7 @@ struct PcgParams {
   double rtol, atol, ww;
   int maxit, max_outer, warm, project;
   const AmgLevelDev* lv;
-  int nlev, nlev_grid;
+  int nlev;
   const float* cinv;
   int64_t nc;
 };
@@ -307,64 +358,37 @@ struct PcgParams {
   }                  \
   }
 
-// z = V(r): lv[0].b holds r (FP32) on entry, lv[0].x holds z on exit; when the top level is
-// a grid level its last phase also writes the partial dots (r, z), (w, z) to `slot`.
+// z = V(r): lv[0].b / lv[0].db hold r (FP32) on entry, lv[0].x holds z on exit, P.u holds
+// D^-1/2 z, and slot `slot` of the partials holds (r, z), (w, z).  nlev >= 2.
 template <class TV>
-__device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh, bool& dots_done) {
+__device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
   const unsigned nb = gridDim.x;
   unsigned int* cnt = P.bar;
   unsigned int* gen = P.bar + 1;
-  const int lane = threadIdx.x & 31;
-  const RowRange grid_rr{static_cast<int64_t>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5),
-                         static_cast<int64_t>((gridDim.x * static_cast<int64_t>(blockDim.x)) >> 5), lane};
-  const RowRange cta_rr{static_cast<int64_t>(threadIdx.x >> 5), static_cast<int64_t>(blockDim.x >> 5), lane};
-  const int G = P.nlev_grid, NL = P.nlev;
-  for (int l = 0; l < G; ++l) {
+  const RowRange rr{static_cast<int64_t>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5),
+                    static_cast<int64_t>((gridDim.x * static_cast<int64_t>(blockDim.x)) >> 5),
+                    static_cast<int>(threadIdx.x & 31)};
+  const int NL = P.nlev;
+  for (int l = 0; l + 1 < NL; ++l) {
     const AmgLevelDev& L = P.lv[l];
-    pre_a(L, grid_rr);
+    pre_a(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
-    pre_b(L, grid_rr);
+    pre_b(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
-    restrict_to(L, P.lv[l + 1], grid_rr);
+    restrict_to(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
   }
-  if (blockIdx.x == 0) {
-    for (int l = G; l + 1 < NL; ++l) {
-      const AmgLevelDev& L = P.lv[l];
-      pre_a(L, cta_rr);
-      __syncthreads();
-      pre_b(L, cta_rr);
-      __syncthreads();
-      restrict_to(L, P.lv[l + 1], cta_rr);
-      __syncthreads();
-    }
-    coarse_solve(P.lv[NL - 1], P.cinv, P.nc);
-    __syncthreads();
-    for (int l = NL - 2; l >= G; --l) {
-      const AmgLevelDev& L = P.lv[l];
-      prolong_from(L, P.lv[l + 1], cta_rr);
-      __syncthreads();
-      post_c(L, cta_rr);
-      __syncthreads();
-      double a = 0.0, b = 0.0;
-      post_d(L, cta_rr, nullptr, nullptr, a, b, false);
-      __syncthreads();
-    }
-  }
+  coarse_solve(P.lv[NL - 1], P.cinv, P.nc, rr);
   if (!grid_barrier(cnt, gen, nb, P.err)) return false;
-  dots_done = false;
-  for (int l = G - 1; l >= 0; --l) {
+  for (int l = NL - 2; l >= 0; --l) {
     const AmgLevelDev& L = P.lv[l];
-    prolong_from(L, P.lv[l + 1], grid_rr);
+    prolong_from(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
-    post_c(L, grid_rr);
+    post_c(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
     double rz = 0.0, wz = 0.0;
-    post_d(L, grid_rr, P.r, P.sdinv, rz, wz, l == 0);
-    if (l == 0) {
-      cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
-      dots_done = true;
-    }
+    post_d(L, rr, P.r, P.sdinv, P.u, rz, wz, l == 0);
+    if (l == 0) cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
   }
   return true;
@@ -381,7 +405,8 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
   unsigned int* gen = P.bar + 1;
   const int64_t n = P.n;
   float* b0 = P.lv[0].b;
-  const float* z0 = P.lv[0].x;
+  float* db0 = P.lv[0].db;
+  const float* dinv0 = P.lv[0].dinv;
   double tot[4];
   double meanb = 0.0;
   if (P.project) {
@@ -415,14 +440,22 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
     {
       double rh = 0.0;
       PCG_ROWS_BEGIN
-        double acc = 0.0;
-        for (int k = 0; k < width; ++k) {
+        double acc = 0.0, acc2 = 0.0;
+        int k = 0;
+        for (; k + 2 <= width; k += 2) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += P.v64[idx] * P.y[P.col[idx]];
+          acc2 += P.v64[idx + 32] * P.y[P.col[idx + 32]];
+        }
+        if (k < width) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
           acc += P.v64[idx] * P.y[P.col[idx]];
         }
-        const double r = P.bh[row] - acc;
+        const double r = P.bh[row] - (acc + acc2);
         P.r[row] = r;
-        b0[row] = static_cast<float>(r);
+        const float rf = static_cast<float>(r);
+        b0[row] = rf;
+        db0[row] = dinv0[row] * rf;
         rh += P.diag[row] * r * r;
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
@@ -434,29 +467,31 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
     if (rr <= tol2 || total >= P.maxit) break;
     double rz_old = 1.0;
     for (int it = 0;; ++it) {
-      bool dots = false;
-      if (!vcycle(P, 2, sh, dots)) return;
-      if (!dots) {  // no grid level: dots over the whole grid after the CTA-0 cycle
-        double rz = 0.0, wz = 0.0;
-        PCG_ROWS_BEGIN
-          const double z = static_cast<double>(z0[row]);
-          rz += P.r[row] * z;
-          wz += z / P.sdinv[row];
-        PCG_ROWS_END
-        cta_partial(P.part, 2, rz, wz, 0.0, 0.0, sh);
-        if (!grid_barrier(cnt, gen, nb, P.err)) return;
-      }
+      if (!vcycle(P, 2, sh)) return;
       cta_total(P.part, 2, tot, sh);
       const double rz = tot[0];
       const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
       const double beta = it == 0 ? 0.0 : rz / rz_old;
+      const float* z0 = P.lv[0].x;
       double pq = 0.0;
       PCG_ROWS_BEGIN
-        double acc = 0.0;
-        for (int k = 0; k < width; ++k) {
-          const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += P.v64[idx] * static_cast<double>(z0[P.col[idx]]);
+        const double ui = P.u[row];
+        double acc = 0.0, acc2 = 0.0;
+        int k = 0;
+        for (; k + 4 <= width; k += 4) {
+          const int64_t i0 = base + ((int64_t)k << 5) + lane;
+          const float w0 = P.a32[i0], w1 = P.a32[i0 + 32], w2 = P.a32[i0 + 64], w3 = P.a32[i0 + 96];
+          const int32_t c0 = P.col[i0], c1 = P.col[i0 + 32], c2 = P.col[i0 + 64], c3 = P.col[i0 + 96];
+          acc += static_cast<double>(w0) * (P.u[c0] - ui);
+          acc2 += static_cast<double>(w1) * (P.u[c1] - ui);
+          acc += static_cast<double>(w2) * (P.u[c2] - ui);
+          acc2 += static_cast<double>(w3) * (P.u[c3] - ui);
         }
+        for (; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += static_cast<double>(P.a32[idx]) * (P.u[P.col[idx]] - ui);
+        }
+        acc = (acc + acc2 + P.rsum[row] * ui) * P.sdinv[row];
         const double z = static_cast<double>(z0[row]);
         const double w = 1.0 / P.sdinv[row];
         const double pv = (z - c * w) + (it == 0 ? 0.0 : beta * P.p[row]);
@@ -476,7 +511,9 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
         P.y[row] += alpha * P.p[row];
         const double r = P.r[row] - alpha * P.q[row];
         P.r[row] = r;
-        b0[row] = static_cast<float>(r);
+        const float rf = static_cast<float>(r);
+        b0[row] = rf;
+        db0[row] = dinv0[row] * rf;
         rh += P.diag[row] * r * r;
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
@@ -521,7 +558,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
 
 // ------------------------------------------------------------------ host entry
 template <class TM>
-void CgSystem<TM>::enable_amg(const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col,
+void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col,
                               const std::vector<double>& a, const std::vector<double>& d, bool singular,
                               cudaStream_t s) {
   CsrHost Ah;
@@ -540,6 +577,10 @@ void CgSystem<TM>::enable_amg(const std::vector<int64_t>& rowptr, const std::vec
   }
   AmgHost h;
   amg_build(Ah, w, singular, AmgOptions{}, h);
+  if (h.lv.size() < 2) {  // no coarsening possible: keep the Jacobi solver
+    amg.reset();
+    return;
+  }
   amg = std::make_unique<AmgDevice>();
   amg->upload(h, s);
   amg_ww = ww;
@@ -549,19 +590,31 @@ void CgSystem<TM>::enable_amg(const std::vector<int64_t>& rowptr, const std::vec
     y64.zero(s);
   }
   if (!bh64.n) bh64.alloc(n);
-  amg_work.alloc(3 * static_cast<size_t>(n));
+  amg_work.alloc(4 * static_cast<size_t>(n));
+  amg_work.zero(s);
   if (!vals64.n) {  // FP64 scaled values (the FP64 CG keeps them in vals)
     std::vector<double> v(P.len);
     SPX_CUDA(cudaMemcpy(v.data(), vals.p, P.len * sizeof(double), cudaMemcpyDeviceToHost));
     vals64.upload(v, s);
+  }
+  // unscaled FP32 values on the SELL pattern and FP64 row sums (difference-form SpMV)
+  {
+    std::vector<float> v(P.len, 0.0f);
+    std::vector<double> rs(n, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        rs[i] += a[k];
+        if (hs.map[k] >= 0) v[hs.map[k]] = static_cast<float>(a[k]);
+      }
+    amg_a32.upload(v, s);
+    amg_rsum.upload(rs, s);
   }
   int per_sm = 0;
   SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_amg<double>, PCG_BLOCK, 0));
   SPX_CHECK(per_sm > 0, "AMG PCG kernel cannot be resident");
   int dev;
   SPX_CUDA(cudaGetDevice(&dev));
-  const int64_t want = (P.nslices * 32 + PCG_BLOCK - 1) / PCG_BLOCK;
-  amg_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, num_sms(dev))));
+  amg_grid = num_sms(dev);
   if (part.n < 4 * 4 * static_cast<size_t>(amg_grid)) part.alloc(4 * 4 * static_cast<size_t>(amg_grid));
   SPX_CUDA(cudaStreamSynchronize(s));
 }
@@ -572,24 +625,24 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
                               cudaStream_t st) {
   PcgParams<TV> q;
   q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
-  q.v64 = vals64.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
+  q.v64 = vals64.p; q.a32 = amg_a32.p; q.rsum = amg_rsum.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
   q.b = b; q.x = x;
   q.bh = bh64.p; q.y = y64.p;
-  q.r = amg_work.p; q.p = amg_work.p + n; q.q = amg_work.p + 2 * n;
+  q.r = amg_work.p; q.p = amg_work.p + n; q.q = amg_work.p + 2 * n; q.u = amg_work.p + 3 * n;
   q.part = part.p; q.bar = bar.p; q.err = err.p; q.iters = iters.p; q.resid = resid.p;
   q.iters_acc = iters_acc.p; q.res_acc = res_acc.p;
   q.rtol = rtol; q.atol = atol; q.ww = amg_singular ? amg_ww : 0.0;
   q.maxit = maxit; q.max_outer = max_outer; q.warm = warm ? 1 : 0; q.project = project ? 1 : 0;
-  q.lv = amg->lv.p; q.nlev = amg->nlev; q.nlev_grid = amg->nlev_grid; q.cinv = amg->cinv.p; q.nc = amg->nc;
+  q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc;
   void* args[] = {&q};
   SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_pcg_amg<TV>), dim3(amg_grid), dim3(PCG_BLOCK),
                                        args, 0, st));
 }
 
-template void CgSystem<double>::enable_amg(const std::vector<int64_t>&, const std::vector<int32_t>&,
+template void CgSystem<double>::enable_amg(const HostSell&, const std::vector<int64_t>&, const std::vector<int32_t>&,
                                            const std::vector<double>&, const std::vector<double>&, bool,
                                            cudaStream_t);
-template void CgSystem<float>::enable_amg(const std::vector<int64_t>&, const std::vector<int32_t>&,
+template void CgSystem<float>::enable_amg(const HostSell&, const std::vector<int64_t>&, const std::vector<int32_t>&,
                                           const std::vector<double>&, const std::vector<double>&, bool,
                                           cudaStream_t);
 template void CgSystem<double>::launch_amg<double>(const double*, double*, double, double, int, bool, bool,

@@ -9,8 +9,8 @@
 //   * tentative prolongator from the near-null vector w (piecewise w / ||w_aggregate||),
 //     smoothed once: P = (I - omega D^-1 A) P0, omega = 4 / (3 lambda_max(D^-1 A));
 //   * Galerkin coarse operators A_c = P^T A P, down to at most `coarse_max` unknowns, whose
-//     dense inverse (with a rank-one term w w^T when the system is singular) is applied
-//     exactly;
+//     dense inverse (with a rank-one term w w^T when the system is singular; Gauss-Jordan in
+//     FP64 on the device at set-up) is applied exactly as a GEMV;
 //   * V(2,2) cycle with Chebyshev-Jacobi smoothing on [0.1, 1.1] x lambda_max(D^-1 A)
 //     (PETSc's default eigenvalue transform for GAMG level smoothers).
 // The cycle runs in FP32 inside an FP64 preconditioned CG (k_pcg_amg in amg.cu).
@@ -28,8 +28,8 @@ struct CsrHost {
 };
 
 struct AmgOptions {
-  double theta = 0.0;      // strength threshold (0: every nonzero off-diagonal is strong)
-  int64_t coarse_max = 256;
+  double theta = 0.0;         // strength threshold (0: every nonzero off-diagonal is strong)
+  int64_t coarse_max = 2500;  // dense coarsest level (inverted once, applied as a GEMV)
   int max_levels = 10;
   int power_iters = 20;
 };
@@ -41,8 +41,8 @@ struct AmgHostLevel {
 };
 
 struct AmgHost {
-  std::vector<AmgHostLevel> lv;   // lv.back() is the dense coarsest level (no P/R)
-  std::vector<double> coarse_inv; // n_c x n_c, row-major
+  std::vector<AmgHostLevel> lv;      // lv.back() is the dense coarsest level (no P/R)
+  std::vector<double> coarse_dense;  // n_c x n_c, row-major, SPD
 };
 
 // A: symmetric positive (semi)definite CSR with sorted columns; null: its near-null vector
@@ -53,26 +53,28 @@ void amg_build(const CsrHost& A, const std::vector<double>& null, bool singular,
 // Device side ---------------------------------------------------------------------------
 struct AmgLevelDev {
   int64_t n, nslices;
-  const int64_t* sp;
+  const int64_t* sp;       // A: SELL-32
   const int32_t* col;
   const float* val;
   const float* dinv;
-  int64_t p_nslices, r_nslices;
+  int64_t p_nslices;       // P: SELL-32, n rows
   const int64_t* p_sp;
   const int32_t* p_col;
   const float* p_val;
-  const int64_t* r_sp;
+  const int64_t* r_rp;     // R = P^T: CSR, rows of the next level, `r_lanes` lanes per row
   const int32_t* r_col;
   const float* r_val;
-  float *b, *x, *x2, *d, *r;
+  int r_lanes;
+  float *b, *db, *x, *x2, *d, *r;  // db = D^-1 b
   float theta, delta, sigma;
-  int cta;  // 1: the level is cycled by CTA 0 alone
 };
 
 struct AmgDevice {
-  int nlev = 0, nlev_grid = 0;
+  int nlev = 0;            // levels 0..nlev-2 are cycled, level nlev-1 is the dense coarsest
   int64_t n0 = 0, nc = 0;
-  std::vector<DevSell<float>> A, P, R;
+  std::vector<DevSell<float>> A, P;
+  std::vector<DevBuf<int64_t>> rrp;
+  std::vector<DevBuf<int32_t>> rcol;
   std::vector<DevBuf<float>> val, pval, rval, dinv, vec;
   DevBuf<AmgLevelDev> lv;
   DevBuf<float> cinv;

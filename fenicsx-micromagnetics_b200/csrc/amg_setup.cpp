@@ -146,40 +146,6 @@ void transpose(const CsrHost& A, CsrHost& T) {
     }
 }
 
-// in-place inverse of an SPD matrix (row-major) by Cholesky
-void spd_inverse(std::vector<double>& M, int64_t n) {
-  std::vector<double> L(n * n, 0.0);
-  for (int64_t j = 0; j < n; ++j) {
-    double s = M[j * n + j];
-    for (int64_t k = 0; k < j; ++k) s -= L[j * n + k] * L[j * n + k];
-    SPX_CHECK(s > 0.0, "AMG coarsest matrix is not positive definite");
-    const double ljj = std::sqrt(s);
-    L[j * n + j] = ljj;
-    for (int64_t i = j + 1; i < n; ++i) {
-      double t = M[i * n + j];
-      for (int64_t k = 0; k < j; ++k) t -= L[i * n + k] * L[j * n + k];
-      L[i * n + j] = t / ljj;
-    }
-  }
-  // inverse = L^-T L^-1, column by column
-  std::vector<double> e(n), y(n);
-  for (int64_t c = 0; c < n; ++c) {
-    std::fill(e.begin(), e.end(), 0.0);
-    e[c] = 1.0;
-    for (int64_t i = 0; i < n; ++i) {  // L y = e
-      double t = e[i];
-      for (int64_t k = 0; k < i; ++k) t -= L[i * n + k] * y[k];
-      y[i] = t / L[i * n + i];
-    }
-    for (int64_t i = n - 1; i >= 0; --i) {  // L^T x = y
-      double t = y[i];
-      for (int64_t k = i + 1; k < n; ++k) t -= L[k * n + i] * e[k];
-      e[i] = t / L[i * n + i];
-    }
-    for (int64_t i = 0; i < n; ++i) M[i * n + c] = e[i];
-  }
-}
-
 }  // namespace
 
 void amg_build(const CsrHost& A0, const std::vector<double>& null0, bool singular, const AmgOptions& o,
@@ -196,7 +162,8 @@ void amg_build(const CsrHost& A0, const std::vector<double>& null0, bool singula
       SPX_CHECK(d > 0.0, "AMG level matrix has a non-positive diagonal");
       L.dinv[i] = 1.0 / d;
     }
-    const bool last = A.n <= o.coarse_max || level + 1 >= o.max_levels;
+    // the top level is always smoothed (at least one coarsening), unless it is tiny
+    const bool last = (A.n <= o.coarse_max && (level > 0 || A.n <= 64)) || level + 1 >= o.max_levels;
     if (last) {
       out.lv.push_back(std::move(L));
       break;
@@ -273,10 +240,10 @@ void amg_build(const CsrHost& A0, const std::vector<double>& null0, bool singula
     A = std::move(Ac);
     w = std::move(wn);
   }
-  // coarsest: dense inverse of A_c (+ rank-one term on the null vector when singular)
+  // coarsest: dense A_c (+ rank-one term on the null vector when singular), inverted on the device
   const CsrHost& C = out.lv.back().A;
   const int64_t nc = C.n;
-  SPX_CHECK(nc <= 4096, "AMG coarsest level is too large for a dense inverse");
+  SPX_CHECK(nc <= 8192, "AMG coarsest level is too large for a dense inverse");
   std::vector<double> M(nc * nc, 0.0);
   double dsum = 0.0;
   for (int64_t i = 0; i < nc; ++i)
@@ -291,8 +258,7 @@ void amg_build(const CsrHost& A0, const std::vector<double>& null0, bool singula
     for (int64_t i = 0; i < nc; ++i)
       for (int64_t j = 0; j < nc; ++j) M[i * nc + j] += tau * w[i] * w[j];
   }
-  spd_inverse(M, nc);
-  out.coarse_inv = std::move(M);
+  out.coarse_dense = std::move(M);
 }
 
 }  // namespace spx

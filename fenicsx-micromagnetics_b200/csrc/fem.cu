@@ -683,7 +683,7 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
       for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
         if (fem.col[k] == i) d[i] = fem.A[k];
     cg1.setup(hsell, a, d);
-    if (opt.u1_pc == 0) cg1.enable_amg(fem.rowptr, fem.col, fem.A, d, true, s);
+    if (opt.u1_pc == 0) cg1.enable_amg(hsell, fem.rowptr, fem.col, fem.A, d, true, s);
   }
   std::vector<int32_t> bmap(N, -1), imap(N, -1), inter;
   for (int64_t k = 0; k < Nb; ++k) bmap[bd.host.bverts[k]] = static_cast<int32_t>(k);
@@ -790,7 +790,7 @@ int64_t DemagCtx<TV, TM>::device_bytes() const {
   int64_t tot = 0;
   tot += P.slice_ptr.bytes() + P.col.bytes() + Div.bytes() + Dsum.bytes() + Gv.bytes() + vol.bytes();
   tot += cg1.vals.bytes() + cg1.vals64.bytes() + cg1.work.bytes() + cg1.P.col.bytes() + cg1.amg_work.bytes();
-  if (cg1.amg) tot += cg1.amg->device_bytes();
+  if (cg1.amg) tot += cg1.amg->device_bytes() + cg1.amg_a32.bytes() + cg1.amg_rsum.bytes();
   tot += cg2.vals.bytes() + cg2.vals64.bytes() + cg2.work.bytes() + cg2.P.col.bytes();
   tot += AIB.bytes() + PIB.col.bytes() + Bdense.bytes();
   tot += H.device_bytes();

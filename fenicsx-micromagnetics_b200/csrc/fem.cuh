@@ -100,13 +100,15 @@ struct CgSystem {
   int grid = 0, block = 0;
   // AMG-preconditioned FP64 CG (k_pcg_amg) instead of the Jacobi solvers when enabled
   std::unique_ptr<AmgDevice> amg;
-  DevBuf<double> amg_work;  // r, p, q
+  DevBuf<double> amg_work;  // r, p, q, u
+  DevBuf<float> amg_a32;    // unscaled values on the SELL pattern (FP32)
+  DevBuf<double> amg_rsum;  // row sums of the unscaled matrix
   double amg_ww = 0.0;
   bool amg_singular = false;
   int amg_grid = 0;
   void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
   // build the AMG hierarchy of D^-1/2 A D^-1/2 from the CSR of A (same rows as setup)
-  void enable_amg(const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col, const std::vector<double>& a,
+  void enable_amg(const HostSell& hs, const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col, const std::vector<double>& a,
                   const std::vector<double>& d, bool singular, cudaStream_t s);
   template <class TV>
   void launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, cudaStream_t st);
