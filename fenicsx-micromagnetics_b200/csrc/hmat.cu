@@ -24,6 +24,10 @@
 //               near tiles with x~) round-robin, lanes over 16-byte row vectors x phases over
 //               the tile rows, then a fixed-order sum over warps, + diag o x~, scattered to
 //               dst[g(perm[i])].
+// Each warp keeps the factor data of its next units / items moving into L2 with
+// cp.async.bulk.prefetch.L2 (a few units ahead), so its own 16-byte loads mostly hit L2.
+// FP32 and BF16 factors form each 16-byte vector's partial sum in FP32 (the factors carry
+// FP32 rounding already) before it is added to the FP64 accumulator.
 // Near tiles use compensated (Kahan) accumulation when FP32 accumulates BF16/FP32 data in
 // the mixed-precision form.
 #include <algorithm>
@@ -132,6 +136,27 @@ __device__ __forceinline__ int log2_ceil_le5(int n) {
   return l;
 }
 
+// asynchronous prefetch of a contiguous range into L2 (cp.async.bulk.prefetch.L2; 16-byte
+// aligned address, size a multiple of 16)
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Per-vector partial sums: FP32 factors (or BF16) against FP64 vectors form each 16-byte
+// vector's partial in FP32 (the factors carry FP32 rounding already) and accumulate in TA.
+template <class TF, class TA> struct Partial { using T = TA; };
+template <> struct Partial<float, double> { using T = float; };
+template <> struct Partial<__nv_bfloat16, double> { using T = float; };
+
+#ifndef SPX_Z_PF
+#define SPX_Z_PF 2
+#endif
+#ifndef SPX_R_PF
+#define SPX_R_PF 2
+#endif
+constexpr int Z_PF = SPX_Z_PF;  // units prefetched ahead by each far_z warp
+constexpr int R_PF = SPX_R_PF;  // items prefetched ahead by each rows warp
+
 template <class TF, class TA, class TX>
 __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
     k_far_z(const FarUnit* __restrict__ units, const int32_t* __restrict__ warp_first, int nwarps,
@@ -142,13 +167,24 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
   const int wg = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
   if (wg >= nwarps) return;  // uniform per warp
   const int lane = threadIdx.x & 31;
+  using TP = typename Partial<TF, TA>::T;
   const int u1 = warp_first[wg + 1];
   int u = warp_first[wg];
   FarUnit nxt;
   if (u < u1) nxt = units[u];
+  // the first units' V rows into L2
+  for (int k = 0; k < Z_PF && u + k < u1; ++k) {
+    const FarUnit P = units[u + k];
+    if (lane < P.nrows)
+      prefetch_l2(F + P.voff + static_cast<int64_t>(lane) * P.ldv,
+                  static_cast<uint32_t>(((P.nc + E - 1) / E) * 16));
+  }
   for (; u < u1; ++u) {
     const FarUnit U = nxt;
     if (u + 1 < u1) nxt = units[u + 1];  // descriptor of the next unit in flight
+    FarUnit pf;
+    const bool do_pf = u + Z_PF < u1;
+    if (do_pf) pf = units[u + Z_PF];    // its rows are prefetched after this unit's loads
     const int nvec = (U.nc + E - 1) / E;
     const int lg = log2_ceil_le5(nvec);
     const int G = 1 << lg, NG = 32 >> lg;
@@ -161,26 +197,29 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
 #pragma unroll
     for (int j = 0; j < ZROWS; ++j) acc[j] = TA(0);
     for (int v = gl; v < nvec; v += G) {
-      TA xv[E];
+      TP xv[E];
 #pragma unroll
       for (int t = 0; t < E; ++t) {
         const int c = v * E + t;
-        xv[t] = c < U.nc ? static_cast<TA>(x[c]) : TA(0);
+        xv[t] = c < U.nc ? static_cast<TP>(x[c]) : TP(0);
       }
 #pragma unroll
       for (int j = 0; j < ZROWS; ++j) {
         const int r = g + j * NG;
         if (j < rpg && r < U.nrows) {
           const VT w = base[static_cast<int64_t>(r) * ldv + v];
-          TA e[E];
-          v16_elems<TA, TF>(w, e);
-          TA s = TA(0);
+          TP e[E];
+          v16_elems<TP, TF>(w, e);
+          TP s = TP(0);
 #pragma unroll
           for (int t = 0; t < E; ++t) s += e[t] * xv[t];
-          acc[j] += s;
+          acc[j] += static_cast<TA>(s);
         }
       }
     }
+    if (do_pf && lane < pf.nrows)
+      prefetch_l2(F + pf.voff + static_cast<int64_t>(lane) * pf.ldv,
+                  static_cast<uint32_t>(((pf.nc + E - 1) / E) * 16));
 #pragma unroll
     for (int j = 0; j < ZROWS; ++j)
       if (j < rpg)
@@ -229,12 +268,25 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
   TA acc[E], cmp[E];
 #pragma unroll
   for (int t = 0; t < E; ++t) acc[t] = cmp[t] = TA(0);
+  using TP = typename Partial<T, TA>::T;
   const bool active = vl < nvec;
   RowItem nxt;
   if (first < end) nxt = items[first];
+  if (lane < R_PF) {  // the first items' tiles into L2
+    const int64_t f = first + static_cast<int64_t>(lane) * ROWS_WARPS;
+    if (f < end) {
+      const RowItem P = items[f];
+      prefetch_l2(base + P.off, static_cast<uint32_t>(P.len) * static_cast<uint32_t>(nvec) * 16u);
+    }
+  }
   for (int64_t it = first; it < end; it += ROWS_WARPS) {
     const RowItem I = nxt;
     if (it + ROWS_WARPS < end) nxt = items[it + ROWS_WARPS];
+    const int64_t fp = it + static_cast<int64_t>(R_PF) * ROWS_WARPS;
+    if (lane == 0 && fp < end) {
+      const RowItem P = items[fp];
+      prefetch_l2(base + P.off, static_cast<uint32_t>(P.len) * static_cast<uint32_t>(nvec) * 16u);
+    }
     if (!active) continue;
     const VT* tile = reinterpret_cast<const VT*>(base + I.off) + vl;
     const TV* v = vs + I.src;
@@ -247,11 +299,11 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
         w[u] = tile[static_cast<int64_t>(q + u * P) * nvec];
         a[u] = static_cast<TA>(v[q + u * P]);
       }
+      if (kahan) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        TA e[E];
-        v16_elems<TA, T>(w[u], e);
-        if (kahan) {
+        for (int u = 0; u < 4; ++u) {
+          TA e[E];
+          v16_elems<TA, T>(w[u], e);
 #pragma unroll
           for (int t = 0; t < E; ++t) {
             const TA y = e[t] * a[u] - cmp[t];
@@ -259,10 +311,21 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
             cmp[t] = (s - acc[t]) - y;
             acc[t] = s;
           }
-        } else {
-#pragma unroll
-          for (int t = 0; t < E; ++t) acc[t] += e[t] * a[u];
         }
+      } else {
+        TP ps[E];
+#pragma unroll
+        for (int t = 0; t < E; ++t) ps[t] = TP(0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          TP e[E];
+          v16_elems<TP, T>(w[u], e);
+          const TP au = static_cast<TP>(a[u]);
+#pragma unroll
+          for (int t = 0; t < E; ++t) ps[t] += e[t] * au;
+        }
+#pragma unroll
+        for (int t = 0; t < E; ++t) acc[t] += static_cast<TA>(ps[t]);
       }
     }
     for (; q < I.len; q += P) {
