@@ -5,7 +5,8 @@
 // the far factors -- FP64, FP32 or BF16 -- and TN of the near tiles -- FP64 or FP32):
 //   * row segments: the leaf clusters in permutation order, split into pieces of at most
 //     64 rows; every output row belongs to exactly one segment.
-//   * V_b (k x n) of each far block: k rows of ldv = n rounded up to a 16-byte multiple.
+//   * V_b^T of each far block: n rows of ldk = k rounded up to 16 bytes (row c holds
+//     V_b[0..k-1, c]), cut into units of at most ~16 KB of rows.
 //   * U_b of each far block, cut at the segments it covers: per segment a tile of k rows of
 //     ld = rows rounded up to a 16-byte multiple (row q holds U[rows, q]).
 //   * near blocks, cut the same way: per segment a tile of n columns of ld entries.
@@ -14,12 +15,13 @@
 //
 // Kernels (no atomics on data, every output written by exactly one warp or CTA):
 //   k_hgather : x~[i] = src[g(perm[i])]             (fused boundary gather + perm)
-//   k_far_z   : z_b = V_b x~_{J_b}.  Persistent warps; the work is cut into units of at most
-//               8 rows x 1024 columns of one V_b and dealt to warps in contiguous, byte-balanced
-//               ranges.  A lane keeps its x~ values in registers for all rows of the unit.  Rows
-//               longer than 1024 columns are cut into pieces whose partial sums the last
-//               arriving piece (per-group arrival counter, reset by that piece) adds in piece
-//               order, so z does not depend on scheduling.
+//   k_far_z   : z_b = V_b x~_{J_b} = sum_c x~_c V_b^T[c, :].  Persistent warps over contiguous,
+//               byte-balanced unit ranges; lanes = (16-byte vector of outputs q, phase over
+//               rows c), accumulating in registers across the units of a block; at the
+//               block's last unit in the warp a shuffle sum over the phases writes z_b.  A
+//               block shared by several warps (only at range ends) adds the warps' partials
+//               through an arrival counter: the last arriving warp sums them in contributor
+//               order and resets the counter, so z does not depend on scheduling.
 //   k_rows    : one CTA per row segment; its warps take the segment's items (U tiles with z_b,
 //               near tiles with x~) round-robin, lanes over 16-byte row vectors x phases over
 //               the tile rows, then a fixed-order sum over warps, + diag o x~, scattered to
@@ -55,8 +57,6 @@ template <> __device__ __forceinline__ double cvt<double, __nv_bfloat16>(__nv_bf
 
 // ------------------------------------------------------------------ packing
 namespace {
-constexpr int ZROWS = 8;        // V rows per far_z unit
-constexpr int ZCOLS = 1024;     // columns per far_z unit piece
 constexpr int Z_WARPS = 8;      // warps per far_z CTA
 constexpr int Z_CTAS_PER_SM = 4;
 constexpr int SEG_MAX = 64;     // rows per segment
@@ -149,10 +149,10 @@ template <> struct Partial<float, double> { using T = float; };
 template <> struct Partial<__nv_bfloat16, double> { using T = float; };
 
 #ifndef SPX_Z_PF
-#define SPX_Z_PF 2
+#define SPX_Z_PF 1
 #endif
 #ifndef SPX_R_PF
-#define SPX_R_PF 2
+#define SPX_R_PF 1
 #endif
 constexpr int Z_PF = SPX_Z_PF;  // units prefetched ahead by each far_z warp
 constexpr int R_PF = SPX_R_PF;  // items prefetched ahead by each rows warp
@@ -164,88 +164,91 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
             const FarGroup* __restrict__ groups, unsigned int* __restrict__ gcnt) {
   constexpr int E = V16<TF>::E;
   using VT = typename V16<TF>::T;
+  using TP = typename Partial<TF, TA>::T;
   const int wg = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
   if (wg >= nwarps) return;  // uniform per warp
   const int lane = threadIdx.x & 31;
-  using TP = typename Partial<TF, TA>::T;
   const int u1 = warp_first[wg + 1];
   int u = warp_first[wg];
   FarUnit nxt;
-  if (u < u1) nxt = units[u];
-  // the first units' V rows into L2
-  for (int k = 0; k < Z_PF && u + k < u1; ++k) {
-    const FarUnit P = units[u + k];
-    if (lane < P.nrows)
-      prefetch_l2(F + P.voff + static_cast<int64_t>(lane) * P.ldv,
-                  static_cast<uint32_t>(((P.nc + E - 1) / E) * 16));
+  if (u < u1) {
+    nxt = units[u];
+    if (lane == 0) prefetch_l2(F + nxt.voff, static_cast<uint32_t>(nxt.nc) * nxt.ldk * sizeof(TF));
   }
+  TA acc[E];
+#pragma unroll
+  for (int t = 0; t < E; ++t) acc[t] = TA(0);
   for (; u < u1; ++u) {
     const FarUnit U = nxt;
     if (u + 1 < u1) nxt = units[u + 1];  // descriptor of the next unit in flight
-    FarUnit pf;
-    const bool do_pf = u + Z_PF < u1;
-    if (do_pf) pf = units[u + Z_PF];    // its rows are prefetched after this unit's loads
-    const int nvec = (U.nc + E - 1) / E;
-    const int lg = log2_ceil_le5(nvec);
-    const int G = 1 << lg, NG = 32 >> lg;
-    const int gl = lane & (G - 1), g = lane >> lg;
-    const int rpg = (U.nrows + NG - 1) / NG;  // rows per lane group, uniform over the warp
-    const int ldv = U.ldv / E;
-    const VT* base = reinterpret_cast<const VT*>(F + U.voff);
-    const TX* x = xp + U.xc;
-    TA acc[ZROWS];
+    const int nvq = U.ldk / E;
+    const int lg = log2_ceil_le5(nvq);
+    const int G = 1 << lg, P = 32 >> lg;
+    const int vl = lane & (G - 1), ph = lane >> lg;
+    if (vl < nvq) {
+      const VT* tile = reinterpret_cast<const VT*>(F + U.voff) + vl;
+      const TX* x = xp + U.xc;
+      int c = ph;
+      for (; c + 3 * P < U.nc; c += 4 * P) {
+        VT w[4];
+        TP a[4];
 #pragma unroll
-    for (int j = 0; j < ZROWS; ++j) acc[j] = TA(0);
-    for (int v = gl; v < nvec; v += G) {
-      TP xv[E];
+        for (int i = 0; i < 4; ++i) {
+          w[i] = tile[static_cast<int64_t>(c + i * P) * nvq];
+          a[i] = static_cast<TP>(x[c + i * P]);
+        }
+        TP ps[E];
+#pragma unroll
+        for (int t = 0; t < E; ++t) ps[t] = TP(0);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          TP e[E];
+          v16_elems<TP, TF>(w[i], e);
+#pragma unroll
+          for (int t = 0; t < E; ++t) ps[t] += e[t] * a[i];
+        }
+#pragma unroll
+        for (int t = 0; t < E; ++t) acc[t] += static_cast<TA>(ps[t]);
+      }
+      for (; c < U.nc; c += P) {
+        TP e[E];
+        v16_elems<TP, TF>(tile[static_cast<int64_t>(c) * nvq], e);
+        const TP a = static_cast<TP>(x[c]);
+#pragma unroll
+        for (int t = 0; t < E; ++t) acc[t] += static_cast<TA>(e[t] * a);
+      }
+    }
+    if (lane == 0 && u + 1 < u1)  // the next unit's V^T rows into L2
+      prefetch_l2(F + nxt.voff, static_cast<uint32_t>(nxt.nc) * nxt.ldk * sizeof(TF));
+    const int fl = U.flags & 3;
+    if (fl == 0) continue;
+    // the block ends in this warp: sum over the phases, write its k rows
+#pragma unroll
+    for (int t = 0; t < E; ++t)
+      for (int o = G; o < 32; o <<= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], o);
+    TA* out = fl == 1 ? z : zpart;
+    if (ph == 0 && vl < nvq) {
 #pragma unroll
       for (int t = 0; t < E; ++t) {
-        const int c = v * E + t;
-        xv[t] = c < U.nc ? static_cast<TP>(x[c]) : TP(0);
-      }
-#pragma unroll
-      for (int j = 0; j < ZROWS; ++j) {
-        const int r = g + j * NG;
-        if (j < rpg && r < U.nrows) {
-          const VT w = base[static_cast<int64_t>(r) * ldv + v];
-          TP e[E];
-          v16_elems<TP, TF>(w, e);
-          TP s = TP(0);
-#pragma unroll
-          for (int t = 0; t < E; ++t) s += e[t] * xv[t];
-          acc[j] += static_cast<TA>(s);
-        }
+        const int q = vl * E + t;
+        if (q < U.k) out[U.zout + q] = acc[t];
       }
     }
-    if (do_pf && lane < pf.nrows)
-      prefetch_l2(F + pf.voff + static_cast<int64_t>(lane) * pf.ldv,
-                  static_cast<uint32_t>(((pf.nc + E - 1) / E) * 16));
 #pragma unroll
-    for (int j = 0; j < ZROWS; ++j)
-      if (j < rpg)
-        for (int o = G >> 1; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
-    TA* out = U.grp < 0 ? z : zpart;
-    if (gl == 0) {
-#pragma unroll
-      for (int j = 0; j < ZROWS; ++j) {
-        const int r = g + j * NG;
-        if (j < rpg && r < U.nrows) out[U.zout + r] = acc[j];
-      }
-    }
-    if (U.grp >= 0) {  // column piece of a long row batch: the last piece to arrive sums all
+    for (int t = 0; t < E; ++t) acc[t] = TA(0);
+    if (fl == 2) {  // block shared between warps: the last contributor sums the partials in order
       __threadfence();
       __syncwarp();
+      const FarGroup Gp = groups[U.grp];
       unsigned last = 0;
-      if (lane == 0)
-        last = atomicAdd(gcnt + U.grp, 1u) == static_cast<unsigned>(groups[U.grp].npieces) - 1u ? 1u : 0u;
+      if (lane == 0) last = atomicAdd(gcnt + U.grp, 1u) == static_cast<unsigned>(Gp.ncontrib) - 1u ? 1u : 0u;
       last = __shfl_sync(0xffffffffu, last, 0);
       if (last) {
         __threadfence();
-        const FarGroup Gp = groups[U.grp];
-        if (lane < Gp.nrows) {
-          TA s = TA(0);
-          for (int p = 0; p < Gp.npieces; ++p) s += __ldcg(zpart + Gp.pbase + p * ZROWS + lane);
-          z[Gp.zdst + lane] = s;
+        for (int q = lane; q < Gp.k; q += 32) {
+          TA sum = TA(0);
+          for (int cc = 0; cc < Gp.ncontrib; ++cc) sum += __ldcg(zpart + Gp.pbase + cc * U.ldk + q);
+          z[Gp.zdst + q] = sum;
         }
         if (lane == 0) atomicExch(gcnt + U.grp, 0u);
       }
@@ -438,34 +441,24 @@ void do_pack(HMatrix& H, cudaStream_t s) {
 
   std::vector<PackJob> jf, jn;
   std::vector<FarUnit> units;
-  std::vector<FarGroup> groups;
   std::vector<std::vector<RowItem>> far_items(nseg), near_items(nseg);
-  int64_t fpos = 0, npos = 0, zpos = 0, ppos = 0, nf = 0, nn = 0;
+  int64_t fpos = 0, npos = 0, zpos = 0, nf = 0, nn = 0;
   for (const HBlock& b : H.blocks) {
     const int32_t m = b.re - b.rs, n = b.ce - b.cs;
     int64_t sg = std::upper_bound(seg.begin(), seg.end(), b.rs) - seg.begin() - 1;
     SPX_CHECK(sg >= 0 && seg[sg] == b.rs, "block rows do not start at a segment boundary");
     if (b.type == 1) {
       const int32_t k = b.rank;
-      const int32_t ldv = static_cast<int32_t>(round_up(n, EF));
+      const int32_t ldk = static_cast<int32_t>(round_up(std::max(k, 1), EF));
       const int64_t pv = fpos;
-      jf.push_back(PackJob{b.off_v, pv, k, n, ldv, n, 1});
-      fpos = round_up(pv + (int64_t)k * ldv, EF);
-      const int32_t P = (n + ZCOLS - 1) / ZCOLS;
-      for (int32_t q0 = 0; q0 < k; q0 += ZROWS) {
-        const int32_t nrows = std::min(ZROWS, k - q0);
-        if (P == 1) {
-          units.push_back(FarUnit{pv + (int64_t)q0 * ldv, ldv, n, b.cs, nrows, static_cast<int32_t>(zpos + q0), -1});
-        } else {
-          const int32_t g = static_cast<int32_t>(groups.size());
-          groups.push_back(FarGroup{static_cast<int32_t>(ppos), P, static_cast<int32_t>(zpos + q0), nrows});
-          for (int32_t p = 0; p < P; ++p) {
-            const int32_t c0 = p * ZCOLS;
-            units.push_back(FarUnit{pv + (int64_t)q0 * ldv + c0, ldv, std::min(ZCOLS, n - c0), b.cs + c0, nrows,
-                                    static_cast<int32_t>(ppos + (int64_t)p * ZROWS), g});
-          }
-          ppos += (int64_t)P * ZROWS;
-        }
+      // V^T: n rows of ldk (row c = V[0..k-1, c]); units of at most ~16 KB of rows
+      jf.push_back(PackJob{b.off_v, pv, n, k, ldk, 1, n});
+      fpos = pv + static_cast<int64_t>(n) * ldk;
+      if (k > 0) {
+        const int32_t uc = std::max<int32_t>(8, static_cast<int32_t>(16384 / (static_cast<int64_t>(ldk) * sizeof(TF))));
+        for (int32_t c0 = 0; c0 < n; c0 += uc)
+          units.push_back(FarUnit{pv + static_cast<int64_t>(c0) * ldk, ldk, std::min(uc, n - c0), b.cs + c0, k,
+                                  static_cast<int32_t>(zpos), -1, 0, 0});
       }
       for (; sg < nseg && seg[sg] < b.re; ++sg) {
         const int32_t a = seg[sg], nr = seg[sg + 1] - seg[sg];
@@ -487,11 +480,10 @@ void do_pack(HMatrix& H, cudaStream_t s) {
       ++nn;
     }
   }
-  SPX_CHECK(zpos < (int64_t(1) << 31) && ppos < (int64_t(1) << 31), "far-field rank sum exceeds 2^31");
+  SPX_CHECK(zpos < (int64_t(1) << 31), "far-field rank sum exceeds 2^31");
   H.n_far = nf;
   H.n_near = nn;
   H.zlen = zpos;
-  H.zpart_len = ppos;
   H.far_f.alloc(std::max<int64_t>(fpos, 1) * sizeof(TF));
   H.near_f.alloc(std::max<int64_t>(npos, 1) * sizeof(TN));
   H.bytes_far = fpos * (int64_t)sizeof(TF);
@@ -501,22 +493,66 @@ void do_pack(HMatrix& H, cudaStream_t s) {
 
   // far_z units dealt to warps in contiguous ranges of about equal cost
   const int nsm = num_sms(H.device);
-  const int64_t nw = static_cast<int64_t>(nsm) * Z_CTAS_PER_SM * Z_WARPS;
+  const int64_t nw = std::max<int64_t>(1, std::min<int64_t>(static_cast<int64_t>(nsm) * Z_CTAS_PER_SM * Z_WARPS,
+                                                            static_cast<int64_t>(units.size())));
   std::vector<double> cost(units.size() + 1, 0.0);
   for (size_t u = 0; u < units.size(); ++u) {
     const FarUnit& U = units[u];
-    cost[u + 1] = cost[u] + (double)U.nrows * round_up(U.nc, EF) * sizeof(TF) + 8.0 * U.nc + 1024.0;
+    cost[u + 1] = cost[u] + static_cast<double>(U.nc) * U.ldk * sizeof(TF) + 8.0 * U.nc + 512.0;
   }
   std::vector<int32_t> wf(nw + 1, 0);
-  size_t u = 0;
-  for (int64_t w = 0; w <= nw; ++w) {
-    const double target = cost.back() * static_cast<double>(w) / static_cast<double>(nw);
-    while (u < units.size() && cost[u] < target) ++u;
-    wf[w] = static_cast<int32_t>(u);
+  {
+    size_t u = 0;
+    for (int64_t w = 0; w <= nw; ++w) {
+      const double target = cost.back() * static_cast<double>(w) / static_cast<double>(nw);
+      while (u < units.size() && cost[u] < target) ++u;
+      wf[w] = static_cast<int32_t>(u);
+    }
+    wf[nw] = static_cast<int32_t>(units.size());
   }
-  wf[nw] = static_cast<int32_t>(units.size());
+  // the last unit of a block in each warp writes the block: directly when one warp holds
+  // the whole block, else as contributor c of a group
+  std::vector<FarGroup> groups;
+  int64_t ppos = 0;
+  {
+    std::vector<int32_t> warp_of(units.size());
+    for (int64_t w = 0; w < nw; ++w)
+      for (int32_t u = wf[w]; u < wf[w + 1]; ++u) warp_of[u] = static_cast<int32_t>(w);
+    size_t u = 0;
+    while (u < units.size()) {
+      size_t e = u;
+      while (e < units.size() && units[e].zout == units[u].zout) ++e;  // block = units [u, e)
+      std::vector<size_t> lasts;
+      for (size_t v = u; v < e; ++v)
+        if (v + 1 == e || warp_of[v + 1] != warp_of[v]) lasts.push_back(v);
+      if (lasts.size() == 1) {
+        units[lasts[0]].flags = 1;
+      } else {
+        const int32_t g = static_cast<int32_t>(groups.size());
+        groups.push_back(FarGroup{static_cast<int32_t>(ppos), static_cast<int32_t>(lasts.size()), units[u].zout,
+                                  units[u].k});
+        for (size_t c = 0; c < lasts.size(); ++c) {
+          FarUnit& L = units[lasts[c]];
+          L.flags = 2;
+          L.grp = g;
+          L.zout = static_cast<int32_t>(ppos + static_cast<int64_t>(c) * L.ldk);
+        }
+        ppos += static_cast<int64_t>(lasts.size()) * units[u].ldk;
+      }
+      u = e;
+    }
+  }
+  SPX_CHECK(ppos < (int64_t(1) << 31), "far-field partial slots exceed 2^31");
+  for (const FarUnit& U : units)
+    SPX_CHECK(U.voff % EF == 0 && U.nc >= 1 && U.k >= 1 && U.ldk % EF == 0 && U.ldk >= U.k &&
+                  U.voff + static_cast<int64_t>(U.nc) * U.ldk <= fpos && U.xc >= 0 &&
+                  U.xc + static_cast<int64_t>(U.nc) <= H.Nb &&
+                  ((U.flags & 3) != 2 || (U.grp >= 0 && U.grp < static_cast<int64_t>(groups.size()) &&
+                                          U.zout + static_cast<int64_t>(U.k) <= ppos)),
+              "far_z plan: unit out of range");
+  H.zpart_len = ppos;
   H.nunits = static_cast<int64_t>(units.size());
-  H.nwarps_z = nw;
+  H.nwarps_z = units.empty() ? 0 : nw;
   H.units.upload(units, s);
   H.warp_first.upload(wf, s);
   H.groups.upload(groups, s);

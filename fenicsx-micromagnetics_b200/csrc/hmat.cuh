@@ -57,16 +57,18 @@ struct HBlock {
   double relres;
 };
 
-// Apply-side records (see hmat.cu).  FarUnit: rows [zout, zout + nrows) of z (or of the
-// partial-sum buffer when grp >= 0) from V rows starting at element voff (row stride ldv),
-// columns [xc, xc + nc) of x~.  RowItem: a tile of len rows at element off, row q scaled by
-// z[src + q] (far) or x~[src + q] (near).
+// Apply-side records (see hmat.cu).  FarUnit: columns [xc, xc + nc) of far block V^T rows
+// (nc rows of ldk elements at element voff: row c holds V[0..k-1, c]); flags & 3 at the last
+// unit of the block in a warp: 1 write z[zout + q], 2 write partial slot zout + q of group
+// grp.  FarGroup: a block whose units several warps share: partials at pbase + c * ldk + q
+// for contributor c < ncontrib, result z[zdst + q], q < k.  RowItem: a tile of len rows at
+// element off, row q scaled by z[src + q] (far) or x~[src + q] (near).
 struct FarUnit {
   int64_t voff;
-  int32_t ldv, nc, xc, nrows, zout, grp;
+  int32_t ldk, nc, xc, k, zout, grp, flags, pad;
 };
 struct FarGroup {
-  int32_t pbase, npieces, zdst, nrows;
+  int32_t pbase, ncontrib, zdst, k;
 };
 struct RowItem {
   int64_t off;
@@ -90,8 +92,8 @@ struct HMatrix {
   DevBuf<char> far_f, near_f;     // factor / tile storage in the packed precision
   DevBuf<FarUnit> units;          // k_far_z work units
   DevBuf<int32_t> warp_first;     // [nwarps_z + 1] unit range of each k_far_z warp
-  DevBuf<FarGroup> groups;        // row batches cut into column pieces
-  DevBuf<unsigned int> gcnt;      // per group: pieces arrived (reset by the last one)
+  DevBuf<FarGroup> groups;        // far blocks shared by several k_far_z warps
+  DevBuf<unsigned int> gcnt;      // per group: contributors arrived (reset by the last one)
   DevBuf<int32_t> seg_start;      // [nseg + 1] row segments (perm space)
   DevBuf<int64_t> item_ptr;       // [nseg + 1] items of each segment: far ones, then near ones
   DevBuf<int64_t> near_begin;     // [nseg] first near item of each segment
