@@ -28,8 +28,6 @@
 //               dst[g(perm[i])].
 // Each warp keeps the factor data of its next units / items moving into L2 with
 // cp.async.bulk.prefetch.L2 (a few units ahead), so its own 16-byte loads mostly hit L2.
-// FP32 and BF16 factors form each 16-byte vector's partial sum in FP32 (the factors carry
-// FP32 rounding already) before it is added to the FP64 accumulator.
 // Near tiles use compensated (Kahan) accumulation when FP32 accumulates BF16/FP32 data in
 // the mixed-precision form.
 #include <algorithm>
@@ -142,12 +140,6 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// Per-vector partial sums: FP32 factors (or BF16) against FP64 vectors form each 16-byte
-// vector's partial in FP32 (the factors carry FP32 rounding already) and accumulate in TA.
-template <class TF, class TA> struct Partial { using T = TA; };
-template <> struct Partial<float, double> { using T = float; };
-template <> struct Partial<__nv_bfloat16, double> { using T = float; };
-
 #ifndef SPX_Z_PF
 #define SPX_Z_PF 1
 #endif
@@ -164,7 +156,7 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
             const FarGroup* __restrict__ groups, unsigned int* __restrict__ gcnt) {
   constexpr int E = V16<TF>::E;
   using VT = typename V16<TF>::T;
-  using TP = typename Partial<TF, TA>::T;
+  using TP = TA;
   const int wg = static_cast<int>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5);
   if (wg >= nwarps) return;  // uniform per warp
   const int lane = threadIdx.x & 31;
@@ -271,7 +263,7 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
   TA acc[E], cmp[E];
 #pragma unroll
   for (int t = 0; t < E; ++t) acc[t] = cmp[t] = TA(0);
-  using TP = typename Partial<T, TA>::T;
+  using TP = TA;
   const bool active = vl < nvec;
   RowItem nxt;
   if (first < end) nxt = items[first];
