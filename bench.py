@@ -137,10 +137,29 @@ def allmax(x, ws):
     return float(t.item())
 
 
-def bytes_model(st, nnz, N, Nb, NI, nnzI, counters, H):
+def amg_iter_bytes(levels, n0, nnz0):
+    """Algorithmic bytes of one AMG-preconditioned PCG iteration (k_pcg_amg): every V-cycle
+    phase reads its matrix once (FP32 value + int32 column per nonzero) and its FP32 level
+    vectors; the coarsest level is a dense FP32 GEMV; the PCG phases read the FP32 unscaled
+    matrix and FP64 vectors (u gather, p, q, r, y, diagonal scalings)."""
+    total = 0.0
+    for l in range(len(levels) - 1):
+        n, a, p, r = levels[l]["rows"], levels[l]["nnz_A"], levels[l]["nnz_P"], levels[l]["nnz_R"]
+        nc = levels[l + 1]["rows"]
+        total += (8 * a + 20 * n) + (8 * a + 16 * n) + (8 * r + 4 * n + 20 * nc)  # pre-smooth, residual, restrict
+        total += (8 * p + 4 * nc + 8 * n) + (8 * a + 24 * n) + (8 * a + 20 * n)  # prolong, post-smooth x2
+    ncs = levels[-1]["rows"]
+    total += 4 * ncs * ncs + 8 * ncs
+    total += 24 * n0  # top level: u (FP64) write, r (FP64) read, D^-1/2 read
+    total += 8 * nnz0 + 60 * n0  # A z in difference form + p, q updates
+    total += 68 * n0  # y, r updates, level-0 right-hand side
+    return total
+
+
+def bytes_model(st, nnz, N, Nb, NI, nnzI, counters, H, amg_levels=None):
     """Algorithmic bytes per launch for each kernel group (FP32 working precision)."""
     wv, wm = 4, 4
-    # u1 / u2 refinement solves: per inner iteration one SELL SpMV + 7 vector passes
+    # Jacobi refinement solves: per inner iteration one SELL SpMV + 7 vector passes
     # (nnz (w_m + 4) + 4 (N+1) + 7 N w_v); per refinement step an FP64 residual SpMV.
     def cg_bytes(c, n, z):
         if c[2] == 0:
@@ -148,8 +167,14 @@ def bytes_model(st, nnz, N, Nb, NI, nnzI, counters, H):
         inner = c[0] * (z * (wm + 4) + 4 * (n + 1) + 7 * n * wv)
         outer = c[1] * (z * (8 + 4) + 4 * (n + 1) + 3 * n * 8)
         return (inner + outer) / c[2]
+
+    def amg_bytes(c, n, z):
+        if c[2] == 0:
+            return 0.0
+        outer = c[1] * (z * (8 + 4) + 4 * (n + 1) + 3 * n * 8 + 8 * n)
+        return (c[0] * amg_iter_bytes(amg_levels, n, z) + outer) / c[2]
     return {
-        "u1_solve": cg_bytes(counters[0], N, nnz),
+        "u1_solve": amg_bytes(counters[0], N, nnz) if amg_levels else cg_bytes(counters[0], N, nnz),
         "u2_solve": cg_bytes(counters[1], NI, nnzI),
         # far factors + near tiles + x gather (Nb w_v) + scatter of phi and g (2 Nb w_v)
         "boundary_apply": H["far_bytes"] + H["near_bytes"] + 4 * Nb * wv,
@@ -242,7 +267,8 @@ def run_ours(a):
     cats = ["div", "u1_solve", "boundary_apply", "u2_rhs", "u2_solve", "phi", "stage"]
     dc = [c_after[0][k] - c_before[0][k] for k in range(3)], [c_after[1][k] - c_before[1][k] for k in range(3)]
     nnz, nnzI = fem_nnz(spx, X, T, dm)
-    bm = bytes_model(Hst, nnz, N, dm.Nb, dm.NI, nnzI, dc, Hmem)
+    levels = dm.amg_levels()
+    bm = bytes_model(Hst, nnz, N, dm.Nb, dm.NI, nnzI, dc, Hmem, levels)
     per = {}
     for k, name in enumerate(cats):
         if ng_cat[k] == 0:
@@ -283,6 +309,7 @@ def run_ours(a):
         "hmatrix": {"build_s": round(Hst["build_time_seconds"], 2), "n_far": Hst["n_far"], "n_near": Hst["n_near"],
                     "avg_rank": round(Hst["average_far_rank"], 2), "max_rank": Hst["max_observed_rank"],
                     "far_entries": Hst["far_entries"], "near_entries": Hst["near_entries"]},
+        "amg_levels": [[lv["rows"], lv["nnz_A"]] for lv in levels],
         "cg": {"u1_iters_per_solve": round(dc[0][0] / max(dc[0][2], 1), 1),
                "u1_refinements_per_solve": round(dc[0][1] / max(dc[0][2], 1), 2),
                "u2_iters_per_solve": round(dc[1][0] / max(dc[1][2], 1), 1),

@@ -86,11 +86,15 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s) {
   val.resize(nlev); pval.resize(nlev); rval.resize(nlev); dinv.resize(nlev); vec.resize(nlev);
   sizes.assign(nlev, 0);
   nnz.assign(nlev, 0);
+  pnnz.assign(nlev, 0);
+  rnnz.assign(nlev, 0);
   std::vector<AmgLevelDev> d(nlev);
   for (int l = 0; l < nlev; ++l) {
     const AmgHostLevel& L = h.lv[l];
     sizes[l] = L.A.n;
     nnz[l] = static_cast<int64_t>(L.A.ci.size());
+    pnnz[l] = static_cast<int64_t>(L.P.ci.size());
+    rnnz[l] = static_cast<int64_t>(L.R.ci.size());
     AmgLevelDev& D = d[l];
     std::memset(&D, 0, sizeof(D));
     D.n = L.A.n;

@@ -78,7 +78,7 @@ struct AmgDevice {
   std::vector<DevBuf<float>> val, pval, rval, dinv, vec;
   DevBuf<AmgLevelDev> lv;
   DevBuf<float> cinv;
-  std::vector<int64_t> sizes, nnz;
+  std::vector<int64_t> sizes, nnz, pnnz, rnnz;  // per level: rows, nonzeros of A, P, R
   void upload(const AmgHost& h, cudaStream_t s);
   int64_t device_bytes() const;
 };

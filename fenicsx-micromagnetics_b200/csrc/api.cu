@@ -91,6 +91,7 @@ struct DemagBase {
   virtual Profiler& prof() = 0;
   virtual void counters(unsigned long long a[4], unsigned long long b[4]) = 0;
   virtual void residuals(double a[2], double b[2]) = 0;
+  virtual int amg_levels(int64_t* out, int maxl) = 0;
   virtual void set_tolerances(double r1, double r2, double at, int m1, int m2) = 0;
 };
 
@@ -148,6 +149,17 @@ struct DemagImpl : DemagBase {
     };
     rd(d.cg1.res_acc, a);
     rd(d.cg2.res_acc, b);
+  }
+  int amg_levels(int64_t* out, int maxl) override {
+    const AmgDevice* a = d.cg1.amg.get();
+    if (!a) return 0;
+    for (int l = 0; l < a->nlev && l < maxl; ++l) {
+      out[4 * l + 0] = a->sizes[l];
+      out[4 * l + 1] = a->nnz[l];
+      out[4 * l + 2] = a->pnnz[l];
+      out[4 * l + 3] = a->rnnz[l];
+    }
+    return a->nlev;
   }
   void set_tolerances(double r1, double r2, double at, int m1, int m2) override {
     d.opt.rtol_u1 = r1; d.opt.rtol_u2 = r2; d.opt.atol = at;
@@ -681,6 +693,15 @@ int spx_demag_residuals(spx_demag d, double* r1, double* r2) {
     if (r1) r1[k] = a[k];
     if (r2) r2[k] = b[k];
   }
+  API_END
+}
+
+int spx_demag_amg_levels(spx_demag d, int64_t* levels4, int32_t max_levels, int32_t* nlev) {
+  API_BEGIN
+  REQUIRE(d);
+  REQUIRE(nlev);
+  SPX_CHECK(max_levels >= 0 && (levels4 || max_levels == 0), "levels4 must hold 4 * max_levels entries");
+  *nlev = d->impl->amg_levels(levels4, max_levels);
   API_END
 }
 

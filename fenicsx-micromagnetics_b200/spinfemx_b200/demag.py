@@ -166,6 +166,14 @@ class DemagFieldLindholmGPU:
                          "initial_rel_residual_sum": r[0], "final_rel_residual_sum": r[1]}
         return out
 
+    def amg_levels(self):
+        """Rows and nonzeros (A, P, R) per level of the u1 AMG hierarchy ([] without AMG)."""
+        out = np.zeros(4 * 16, np.int64)
+        nl = _lib.c_i32()
+        call("spx_demag_amg_levels", self._h, ptr(out), 16, C.byref(nl))
+        return [dict(rows=int(out[4 * l]), nnz_A=int(out[4 * l + 1]), nnz_P=int(out[4 * l + 2]),
+                     nnz_R=int(out[4 * l + 3])) for l in range(nl.value)]
+
     def boundary_memory_report(self):
         N, Nb, NI, by = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
         call("spx_demag_info", self._h, C.byref(N), C.byref(Nb), C.byref(NI), C.byref(by))

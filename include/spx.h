@@ -208,6 +208,10 @@ SPX_API int spx_demag_counters(spx_demag d, int64_t* u1_counters4, int64_t* u2_c
  * starting guess ([0]) and at return ([1]), for the u1 and u2 solves (no counterpart in
  * the reference: its KSP solves, Demag_Lindholm_GPU.py:577 and :640, report nothing) */
 SPX_API int spx_demag_residuals(spx_demag d, double* u1_res2, double* u2_res2);
+/* levels of the u1 AMG hierarchy (0 when u1 uses the Jacobi solver): per level rows,
+ * nonzeros of A, P and R = P^T (the last level is the dense coarsest one; the reference's
+ * PETSc GAMG hierarchy, Demag_Lindholm_GPU.py:219-222, is not exposed) */
+SPX_API int spx_demag_amg_levels(spx_demag d, int64_t* levels4, int32_t max_levels, int32_t* nlev);
 /* change the Krylov tolerances / iteration limits after create (the reference fixes them
  * with KSP.setTolerances, Demag_Lindholm_GPU.py:219 and :274) */
 SPX_API int spx_demag_set_tolerances(spx_demag d, double rtol_u1, double rtol_u2, double atol, int32_t maxit_u1,
