@@ -134,8 +134,8 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s) {
     D.r_col = rcol[l].p;
     D.r_val = rval[l].p;
     const double avg = static_cast<double>(L.R.ci.size()) / std::max<int64_t>(L.R.n, 1);
-    int lanes = 1;
-    while (lanes < 32 && lanes < avg / 2.0) lanes <<= 1;
+    int lanes = 1;  // about eight entries per lane
+    while (lanes < 32 && lanes < avg / 8.0) lanes <<= 1;
     D.r_lanes = lanes;
     const double b = 1.1 * L.lmax, a = 0.1 * L.lmax;
     D.theta = static_cast<float>(0.5 * (b + a));
@@ -255,7 +255,13 @@ __device__ void restrict_to(const AmgLevelDev& L, const AmgLevelDev& C, RowRange
     float t = 0.0f;
     if (row < C.n) {
       const int64_t k1 = L.r_rp[row + 1];
-      for (int64_t k = L.r_rp[row] + gl; k < k1; k += G) t += L.r_val[k] * L.r[L.r_col[k]];
+      int64_t k = L.r_rp[row] + gl;
+      for (; k + 3 * G < k1; k += 4 * G) {  // four gathers in flight per lane
+        const float w0 = L.r_val[k], w1 = L.r_val[k + G], w2 = L.r_val[k + 2 * G], w3 = L.r_val[k + 3 * G];
+        const int32_t c0 = L.r_col[k], c1 = L.r_col[k + G], c2 = L.r_col[k + 2 * G], c3 = L.r_col[k + 3 * G];
+        t += w0 * L.r[c0] + w1 * L.r[c1] + w2 * L.r[c2] + w3 * L.r[c3];
+      }
+      for (; k < k1; k += G) t += L.r_val[k] * L.r[L.r_col[k]];
     }
     for (int o = G >> 1; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
     if (row < C.n && gl == 0) {
