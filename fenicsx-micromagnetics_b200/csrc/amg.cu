@@ -11,7 +11,9 @@
 //   z = V(r);  beta = (r,z)/(r,z)_old;  c = (w,z)/(w,w) (singular systems: remove the
 //   null-vector component w = D^1/2 1 from z);  p = z - c w + beta p;
 //   q = A^ z + beta q  (A^ w = 0, so q = A^ p without a second SpMV), with A^ z evaluated as
-//   D^-1/2 [sum_j a_ij (u_j - u_i) + (sum_j a_ij) u_i], u = D^-1/2 z, FP32 a_ij, FP64 sums;
+//   D^-1/2 [sum_j a_ij (u_j - u_i) + (sum_j a_ij) u_i], u = D^-1/2 z, FP32 a_ij, FP64 sums
+//   (the level-0 cycle works on the unscaled A and returns u directly, reading the same
+//   FP32 a_ij and columns);
 //   alpha = (r,z)/(p,q);  y += alpha p;  r -= alpha q.
 // The recurrence residual is confirmed against the true FP64 residual (FP64 values) before
 // returning; stopping rule ||b - A x|| <= max(rtol ||b||, atol) in the unscaled norm.
@@ -76,7 +78,8 @@ __global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, 
 
 }  // namespace
 
-void AmgDevice::upload(const AmgHost& h, cudaStream_t s) {
+void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, const int32_t* col0, const float* val0,
+                       int64_t nslices0) {
   nlev = static_cast<int>(h.lv.size());
   n0 = h.lv[0].A.n;
   nc = h.lv.back().A.n;
@@ -112,13 +115,20 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s) {
     if (l + 1 == nlev) break;  // dense coarsest: vectors only
     HostSell hs, hp;
     std::vector<float> v, vp;
-    csr_to_sell(L.A, hs, v);
-    A[l].upload(hs, s);
-    val[l].upload(v, s);
-    D.nslices = hs.nslices;
-    D.sp = A[l].slice_ptr.p;
-    D.col = A[l].col.p;
-    D.val = val[l].p;
+    if (l == 0 && sp0) {
+      D.nslices = nslices0;
+      D.sp = sp0;
+      D.col = col0;
+      D.val = val0;
+    } else {
+      csr_to_sell(L.A, hs, v);
+      A[l].upload(hs, s);
+      val[l].upload(v, s);
+      D.nslices = hs.nslices;
+      D.sp = A[l].slice_ptr.p;
+      D.col = A[l].col.p;
+      D.val = val[l].p;
+    }
     csr_to_sell(L.P, hp, vp);
     P[l].upload(hp, s);
     pval[l].upload(vp, s);
@@ -294,11 +304,9 @@ __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
   }
 }
 
-// post-smoothing step 2; on the top level also u = D^-1/2 z (FP64) and the partial dots
-// (r64, z), (w, z) of the PCG
+// post-smoothing step 2; on the top level also the partial dots (r64, z^), (w, z^) of the PCG
 __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
-                       const double* __restrict__ sdinv, double* __restrict__ u, double& rz, double& wz,
-                       bool top) {
+                       const double* __restrict__ sdinv, double& rz, double& wz, bool top) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
@@ -308,11 +316,10 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
       const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;
       const float z = L.x2[i] + d1;
       L.x[i] = z;
-      if (top) {
-        const double zd = static_cast<double>(z);
-        u[i] = zd * sdinv[i];
-        rz += r64[i] * zd;
-        wz += zd / sdinv[i];
+      if (top) {  // level 0 runs unscaled: z is u = D^-1/2 z^, z^ = u / sdinv
+        const double zh = static_cast<double>(z) / sdinv[i];
+        rz += r64[i] * zh;
+        wz += zh / sdinv[i];
       }
     }
   }
@@ -341,7 +348,7 @@ struct PcgParams {
   const double* diag;
   const TV* b;
   TV* x;
-  double *bh, *y, *r, *p, *q, *u;
+  double *bh, *y, *r, *p, *q;
   double* part;
   unsigned int* bar;
   int* err;
@@ -368,8 +375,8 @@ struct PcgParams {
   }                  \
   }
 
-// z = V(r): lv[0].b / lv[0].db hold r (FP32) on entry, lv[0].x holds z on exit, P.u holds
-// D^-1/2 z, and slot `slot` of the partials holds (r, z), (w, z).  nlev >= 2.
+// z^ = V(r^): lv[0].b / lv[0].db hold the unscaled residual D^1/2 r^ (FP32) on entry, lv[0].x
+// holds u = D^-1/2 z^ on exit, and slot `slot` of the partials holds (r^, z^), (w, z^).  nlev >= 2.
 template <class TV>
 __device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
   const unsigned nb = gridDim.x;
@@ -397,7 +404,7 @@ __device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
     post_c(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
     double rz = 0.0, wz = 0.0;
-    post_d(L, rr, P.r, P.sdinv, P.u, rz, wz, l == 0);
+    post_d(L, rr, P.r, P.sdinv, rz, wz, l == 0);
     if (l == 0) cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
   }
@@ -463,7 +470,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
         }
         const double r = P.bh[row] - (acc + acc2);
         P.r[row] = r;
-        const float rf = static_cast<float>(r);
+        const float rf = static_cast<float>(r / P.sdinv[row]);
         b0[row] = rf;
         db0[row] = dinv0[row] * rf;
         rh += P.diag[row] * r * r;
@@ -482,27 +489,27 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       const double rz = tot[0];
       const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
       const double beta = it == 0 ? 0.0 : rz / rz_old;
-      const float* z0 = P.lv[0].x;
+      const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ from the unscaled level-0 cycle
       double pq = 0.0;
       PCG_ROWS_BEGIN
-        const double ui = P.u[row];
+        const double ui = static_cast<double>(u0[row]);
         double acc = 0.0, acc2 = 0.0;
         int k = 0;
         for (; k + 4 <= width; k += 4) {
           const int64_t i0 = base + ((int64_t)k << 5) + lane;
           const float w0 = P.a32[i0], w1 = P.a32[i0 + 32], w2 = P.a32[i0 + 64], w3 = P.a32[i0 + 96];
           const int32_t c0 = P.col[i0], c1 = P.col[i0 + 32], c2 = P.col[i0 + 64], c3 = P.col[i0 + 96];
-          acc += static_cast<double>(w0) * (P.u[c0] - ui);
-          acc2 += static_cast<double>(w1) * (P.u[c1] - ui);
-          acc += static_cast<double>(w2) * (P.u[c2] - ui);
-          acc2 += static_cast<double>(w3) * (P.u[c3] - ui);
+          acc += static_cast<double>(w0) * (static_cast<double>(u0[c0]) - ui);
+          acc2 += static_cast<double>(w1) * (static_cast<double>(u0[c1]) - ui);
+          acc += static_cast<double>(w2) * (static_cast<double>(u0[c2]) - ui);
+          acc2 += static_cast<double>(w3) * (static_cast<double>(u0[c3]) - ui);
         }
         for (; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += static_cast<double>(P.a32[idx]) * (P.u[P.col[idx]] - ui);
+          acc += static_cast<double>(P.a32[idx]) * (static_cast<double>(u0[P.col[idx]]) - ui);
         }
         acc = (acc + acc2 + P.rsum[row] * ui) * P.sdinv[row];
-        const double z = static_cast<double>(z0[row]);
+        const double z = ui / P.sdinv[row];
         const double w = 1.0 / P.sdinv[row];
         const double pv = (z - c * w) + (it == 0 ? 0.0 : beta * P.p[row]);
         const double qv = acc + (it == 0 ? 0.0 : beta * P.q[row]);
@@ -521,7 +528,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
         P.y[row] += alpha * P.p[row];
         const double r = P.r[row] - alpha * P.q[row];
         P.r[row] = r;
-        const float rf = static_cast<float>(r);
+        const float rf = static_cast<float>(r / P.sdinv[row]);
         b0[row] = rf;
         db0[row] = dinv0[row] * rf;
         rh += P.diag[row] * r * r;
@@ -591,23 +598,8 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
     amg.reset();
     return;
   }
-  amg = std::make_unique<AmgDevice>();
-  amg->upload(h, s);
-  amg_ww = ww;
-  amg_singular = singular;
-  if (!y64.n) {
-    y64.alloc(n);
-    y64.zero(s);
-  }
-  if (!bh64.n) bh64.alloc(n);
-  amg_work.alloc(4 * static_cast<size_t>(n));
-  amg_work.zero(s);
-  if (!vals64.n) {  // FP64 scaled values (the FP64 CG keeps them in vals)
-    std::vector<double> v(P.len);
-    SPX_CUDA(cudaMemcpy(v.data(), vals.p, P.len * sizeof(double), cudaMemcpyDeviceToHost));
-    vals64.upload(v, s);
-  }
-  // unscaled FP32 values on the SELL pattern and FP64 row sums (difference-form SpMV)
+  // unscaled FP32 values on the SELL pattern and FP64 row sums (difference-form SpMV); the
+  // finest level of the cycle uses the same values
   {
     std::vector<float> v(P.len, 0.0f);
     std::vector<double> rs(n, 0.0);
@@ -618,6 +610,30 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
       }
     amg_a32.upload(v, s);
     amg_rsum.upload(rs, s);
+  }
+  // level 0 in the unscaled space: D^-1 of A, P_0 = D^-1/2 P^_0, R_0 = P^_0^T D^-1/2
+  {
+    AmgHostLevel& L0 = h.lv[0];
+    for (int64_t i = 0; i < n; ++i) L0.dinv[i] = 1.0 / d[i];
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = L0.P.rp[i]; k < L0.P.rp[i + 1]; ++k) L0.P.v[k] /= std::sqrt(d[i]);
+    for (int64_t k = 0; k < static_cast<int64_t>(L0.R.v.size()); ++k) L0.R.v[k] /= std::sqrt(d[L0.R.ci[k]]);
+  }
+  amg = std::make_unique<AmgDevice>();
+  amg->upload(h, s, P.slice_ptr.p, P.col.p, amg_a32.p, P.nslices);
+  amg_ww = ww;
+  amg_singular = singular;
+  if (!y64.n) {
+    y64.alloc(n);
+    y64.zero(s);
+  }
+  if (!bh64.n) bh64.alloc(n);
+  amg_work.alloc(3 * static_cast<size_t>(n));
+  amg_work.zero(s);
+  if (!vals64.n) {  // FP64 scaled values (the FP64 CG keeps them in vals)
+    std::vector<double> v(P.len);
+    SPX_CUDA(cudaMemcpy(v.data(), vals.p, P.len * sizeof(double), cudaMemcpyDeviceToHost));
+    vals64.upload(v, s);
   }
   int per_sm = 0;
   SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_amg<double>, PCG_BLOCK, 0));
@@ -638,7 +654,7 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   q.v64 = vals64.p; q.a32 = amg_a32.p; q.rsum = amg_rsum.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
   q.b = b; q.x = x;
   q.bh = bh64.p; q.y = y64.p;
-  q.r = amg_work.p; q.p = amg_work.p + n; q.q = amg_work.p + 2 * n; q.u = amg_work.p + 3 * n;
+  q.r = amg_work.p; q.p = amg_work.p + n; q.q = amg_work.p + 2 * n;
   q.part = part.p; q.bar = bar.p; q.err = err.p; q.iters = iters.p; q.resid = resid.p;
   q.iters_acc = iters_acc.p; q.res_acc = res_acc.p;
   q.rtol = rtol; q.atol = atol; q.ww = amg_singular ? amg_ww : 0.0;

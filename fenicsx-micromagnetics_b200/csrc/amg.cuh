@@ -13,7 +13,10 @@
 //     FP64 on the device at set-up) is applied exactly as a GEMV;
 //   * V(2,2) cycle with Chebyshev-Jacobi smoothing on [0.1, 1.1] x lambda_max(D^-1 A)
 //     (PETSc's default eigenvalue transform for GAMG level smoothers).
-// The cycle runs in FP32 inside an FP64 preconditioned CG (k_pcg_amg in amg.cu).
+// The cycle runs in FP32 inside an FP64 preconditioned CG (k_pcg_amg in amg.cu).  The
+// hierarchy is built for the Jacobi-scaled matrix D^-1/2 A D^-1/2; its finest level is cycled
+// on the unscaled A (P_0 and R_0 absorb D^-1/2), so that the PCG and the cycle read one copy
+// of the level-0 matrix.
 #pragma once
 
 #include "spx_internal.cuh"
@@ -79,7 +82,10 @@ struct AmgDevice {
   DevBuf<AmgLevelDev> lv;
   DevBuf<float> cinv;
   std::vector<int64_t> sizes, nnz, pnnz, rnnz;  // per level: rows, nonzeros of A, P, R
-  void upload(const AmgHost& h, cudaStream_t s);
+  // top0: when set, level 0's matrix is this SELL-32 (slice pointers, columns, FP32 values of
+  // nslices0 slices) owned by the caller instead of a copy of lv[0].A
+  void upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0 = nullptr, const int32_t* col0 = nullptr,
+              const float* val0 = nullptr, int64_t nslices0 = 0);
   int64_t device_bytes() const;
 };
 

@@ -100,7 +100,7 @@ struct CgSystem {
   int grid = 0, block = 0;
   // AMG-preconditioned FP64 CG (k_pcg_amg) instead of the Jacobi solvers when enabled
   std::unique_ptr<AmgDevice> amg;
-  DevBuf<double> amg_work;  // r, p, q, u
+  DevBuf<double> amg_work;  // r, p, q
   DevBuf<float> amg_a32;    // unscaled values on the SELL pattern (FP32)
   DevBuf<double> amg_rsum;  // row sums of the unscaled matrix
   double amg_ww = 0.0;
