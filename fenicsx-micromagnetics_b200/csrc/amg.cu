@@ -71,9 +71,12 @@ __global__ void k_gj_update(double* __restrict__ M, const double* __restrict__ c
   else
     M[e] -= f * M[k * n + j];
 }
-__global__ void k_to_float(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
-  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (i < n) b[i] = static_cast<float>(a[i]);
+// FP32 copy of an n x n matrix into rows of ld >= n entries (zero padded)
+__global__ void k_to_float_rows(const double* __restrict__ a, float* __restrict__ b, int64_t n, int64_t ld) {
+  const int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (e >= n * ld) return;
+  const int64_t i = e / ld, j = e - i * ld;
+  b[e] = j < n ? static_cast<float>(a[i * n + j]) : 0.0f;
 }
 
 }  // namespace
@@ -164,8 +167,9 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, con
       k_gj_update<<<grid_for(nn, 256), 256, 0, s>>>(M.p, colk.p, nc, k);
     }
     SPX_LAUNCH_CHECK();
-    cinv.alloc(std::max<int64_t>(nn, 1));
-    k_to_float<<<grid_for(nn, 256), 256, 0, s>>>(M.p, cinv.p, nn);
+    ldc = (nc + 3) / 4 * 4;  // rows of 16-byte vectors
+    cinv.alloc(std::max<int64_t>(nc * ldc, 1));
+    k_to_float_rows<<<grid_for(nc * ldc, 256), 256, 0, s>>>(M.p, cinv.p, nc, ldc);
     SPX_LAUNCH_CHECK();
     SPX_CUDA(cudaStreamSynchronize(s));
   }
@@ -325,12 +329,20 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
   }
 }
 
-// x = C^-1 b on the dense coarsest level: a warp per row over the grid
-__device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, RowRange rr) {
+// x = C^-1 b on the dense coarsest level: a warp per row over the grid, 16-byte loads of the
+// zero-padded rows (ld = nc rounded up to 4; b is read up to ld, inside the level's vectors)
+__device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, int64_t ldc,
+                             RowRange rr) {
+  const int64_t nv = ldc / 4;
   for (int64_t i = rr.gw; i < nc; i += rr.nw) {
-    const float* row = cinv + i * nc;
+    const float4* row = reinterpret_cast<const float4*>(cinv + i * ldc);
     float s = 0.0f;
-    for (int64_t j = rr.lane; j < nc; j += 32) s += row[j] * L.b[j];
+#pragma unroll 4
+    for (int64_t j = rr.lane; j < nv; j += 32) {
+      const float4 c = row[j];
+      const float* b = L.b + 4 * j;
+      s += c.x * b[0] + c.y * b[1] + c.z * b[2] + c.w * b[3];
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (rr.lane == 0) L.x[i] = s;
   }
@@ -361,7 +373,7 @@ struct PcgParams {
   const AmgLevelDev* lv;
   int nlev;
   const float* cinv;
-  int64_t nc;
+  int64_t nc, ldc;
 };
 
 #define PCG_ROWS_BEGIN                                              \
@@ -395,7 +407,7 @@ __device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
     restrict_to(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
   }
-  coarse_solve(P.lv[NL - 1], P.cinv, P.nc, rr);
+  coarse_solve(P.lv[NL - 1], P.cinv, P.nc, P.ldc, rr);
   if (!grid_barrier(cnt, gen, nb, P.err)) return false;
   for (int l = NL - 2; l >= 0; --l) {
     const AmgLevelDev& L = P.lv[l];
@@ -659,7 +671,7 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   q.iters_acc = iters_acc.p; q.res_acc = res_acc.p;
   q.rtol = rtol; q.atol = atol; q.ww = amg_singular ? amg_ww : 0.0;
   q.maxit = maxit; q.max_outer = max_outer; q.warm = warm ? 1 : 0; q.project = project ? 1 : 0;
-  q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc;
+  q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc; q.ldc = amg->ldc;
   void* args[] = {&q};
   SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_pcg_amg<TV>), dim3(amg_grid), dim3(PCG_BLOCK),
                                        args, 0, st));

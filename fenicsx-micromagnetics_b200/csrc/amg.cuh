@@ -74,7 +74,7 @@ struct AmgLevelDev {
 
 struct AmgDevice {
   int nlev = 0;            // levels 0..nlev-2 are cycled, level nlev-1 is the dense coarsest
-  int64_t n0 = 0, nc = 0;
+  int64_t n0 = 0, nc = 0, ldc = 0;  // ldc: row stride of the coarsest inverse (cinv)
   std::vector<DevSell<float>> A, P;
   std::vector<DevBuf<int64_t>> rrp;
   std::vector<DevBuf<int32_t>> rcol;

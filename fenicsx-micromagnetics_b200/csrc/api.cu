@@ -76,6 +76,9 @@ struct spx_boundary_s {
 };
 struct spx_hmat_s {
   HMatrix h;
+  // near field as CSR, computed by spx_hmat_export_sizes for spx_hmat_export
+  std::vector<int32_t> near_indptr, near_indices;
+  std::vector<double> near_data;
 };
 // ---- type-erased demag / LLG handles (precision chosen at create)
 struct DemagBase {
@@ -449,6 +452,61 @@ int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out) {
   API_END
 }
 
+int spx_hmat_export_sizes(spx_hmat hm, int64_t* nfar, int64_t* u_entries, int64_t* v_entries, int64_t* near_nnz) {
+  API_BEGIN
+  REQUIRE(hm);
+  int64_t f = 0, u = 0, v = 0;
+  hmat_far_sizes(hm->h, f, u, v);
+  hmat_near_csr(hm->h, hm->near_indptr, hm->near_indices, hm->near_data);
+  if (nfar) *nfar = f;
+  if (u_entries) *u_entries = u;
+  if (v_entries) *v_entries = v;
+  if (near_nnz) *near_nnz = static_cast<int64_t>(hm->near_data.size());
+  API_END
+}
+
+int spx_hmat_export(spx_hmat hm, int32_t* perm, double* diag_jump, int64_t* far_meta5, double* relres, double* U,
+                    double* V, int32_t* near_indptr, int32_t* near_indices, double* near_data) {
+  API_BEGIN
+  REQUIRE(hm);
+  const HMatrix& H = hm->h;
+  SPX_CHECK(hm->near_indptr.size() == static_cast<size_t>(H.Nb + 1),
+            "call spx_hmat_export_sizes before spx_hmat_export");
+  if (perm) std::memcpy(perm, H.tree.perm.data(), H.Nb * sizeof(int32_t));
+  if (diag_jump) {  // original boundary order
+    std::vector<double> dp(H.Nb);
+    SPX_CUDA(cudaMemcpy(dp.data(), H.diag_perm.p, H.Nb * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < H.Nb; ++i) diag_jump[H.tree.perm[i]] = dp[i];
+  }
+  hmat_export_far(H, far_meta5, relres, U, V);
+  if (near_indptr) std::memcpy(near_indptr, hm->near_indptr.data(), hm->near_indptr.size() * sizeof(int32_t));
+  if (near_indices) std::memcpy(near_indices, hm->near_indices.data(), hm->near_indices.size() * sizeof(int32_t));
+  if (near_data) std::memcpy(near_data, hm->near_data.data(), hm->near_data.size() * sizeof(double));
+  hm->near_indptr.clear();
+  hm->near_indices.clear();
+  hm->near_data.clear();
+  API_END
+}
+
+int spx_hmat_import(spx_boundary b, const spx_hmat_config* cfg, const int32_t* perm, const double* diag_jump,
+                    int64_t nfar, const int64_t* far_meta5, const double* relres, const double* U, const double* V,
+                    const int32_t* near_indptr, const int32_t* near_indices, const double* near_data,
+                    spx_hmat* out) {
+  API_BEGIN
+  REQUIRE(b);
+  REQUIRE(out);
+  *out = nullptr;
+  REQUIRE(near_indptr);
+  SPX_CHECK(nfar >= 0 && (nfar == 0 || (far_meta5 && U && V)), "far blocks need meta, U and V");
+  SPX_CHECK(near_indptr[0] == 0 && (near_indptr[b->bd.host.Nb] == 0 || (near_indices && near_data)),
+            "near CSR needs indices and data");
+  auto h = std::make_unique<spx_hmat_s>();
+  hmat_import(h->h, b->bd, to_hcfg(cfg), to_prec(cfg ? cfg->precision : 0), nfar, far_meta5, relres, U, V,
+              near_indptr, near_indices, near_data, perm, diag_jump, 0);
+  *out = h.release();
+  API_END
+}
+
 int spx_hmat_stats(spx_hmat hm, int64_t* st, double* secs) {
   API_BEGIN
   REQUIRE(hm);
@@ -546,8 +604,8 @@ int spx_hmat_destroy(spx_hmat hm) {
   API_END
 }
 
-int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
-                     const spx_demag_options* opt, spx_demag* out) {
+static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                        const spx_demag_options* opt, HMatrix* preset, spx_demag* out) {
   API_BEGIN
   REQUIRE(out);
   *out = nullptr;
@@ -572,6 +630,10 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
     o.u1_pc = opt->u1_preconditioner;
     o.hcfg = to_hcfg(&opt->hmat);
   }
+  if (preset) {
+    SPX_CHECK(o.backend == 1, "an H-matrix can only be given to the hmatrix backend");
+    o.preset = preset;
+  }
   auto d = std::make_unique<spx_demag_s>();
   switch (o.prec) {
     case Prec::F64: {
@@ -595,6 +657,20 @@ int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E,
   }
   *out = d.release();
   API_END
+}
+
+int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                     const spx_demag_options* opt, spx_demag* out) {
+  return demag_create(X, N, tets, E, Ms, opt, nullptr, out);
+}
+
+int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                               const spx_demag_options* opt, spx_hmat hm, spx_demag* out) {
+  if (!hm) {
+    spx::set_last_error("null H-matrix handle");
+    return SPX_ERR_INVALID;
+  }
+  return demag_create(X, N, tets, E, Ms, opt, &hm->h, out);
 }
 
 int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s) {

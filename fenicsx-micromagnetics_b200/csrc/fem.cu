@@ -717,8 +717,15 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
     Bdense.alloc(static_cast<size_t>(Nb * Nb));
     bd.dense_B(Bdense.p, s);
   } else {
-    H.build(bd, opt.hcfg, s);
-    H.pack(opt.hprec, s);
+    if (opt.preset) {
+      SPX_CHECK(opt.preset->Nb == Nb && opt.preset->packed, "the given H-matrix does not belong to this boundary");
+      H = std::move(*opt.preset);
+      opt.preset = nullptr;
+      if (H.prec != opt.hprec) H.pack(opt.hprec, s);
+    } else {
+      H.build(bd, opt.hcfg, s);
+      H.pack(opt.hprec, s);
+    }
   }
   b.alloc(N); u1.alloc(N); phi.alloc(N); gB.alloc(Nb); xb.alloc(Nb);
   bI.alloc(std::max<int64_t>(NI, 1));

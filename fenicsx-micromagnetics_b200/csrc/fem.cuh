@@ -128,6 +128,7 @@ struct DemagOptions {
   int maxit_u1 = 2000, maxit_u2 = 12000;
   int warm_start = 0;       // 0 zero start, 1 previous solution, 2 extrapolated per RK stage
   int u1_pc = 0;            // u1 preconditioner: 0 smoothed-aggregation AMG, 1 Jacobi
+  HMatrix* preset = nullptr;  // hmatrix backend: adopt this H-matrix (moved in) instead of building
   HBuildConfig hcfg;
 };
 

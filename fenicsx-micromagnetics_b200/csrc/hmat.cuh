@@ -114,6 +114,17 @@ struct HMatrix {
   int64_t device_bytes() const;
 };
 
+// The reference's cache representation (hio.cu): near field as CSR in permutation space
+// (zeros dropped), far blocks as meta (rs, re, cs, ce, k), relres, U (m x k), V (k x n).
+void hmat_near_csr(const HMatrix& H, std::vector<int32_t>& indptr, std::vector<int32_t>& indices,
+                   std::vector<double>& data);
+void hmat_far_sizes(const HMatrix& H, int64_t& nfar, int64_t& u_entries, int64_t& v_entries);
+void hmat_export_far(const HMatrix& H, int64_t* meta5, double* relres, double* U, double* V);
+void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec p, int64_t nfar, const int64_t* meta5,
+                 const double* relres, const double* U, const double* V, const int32_t* indptr,
+                 const int32_t* indices, const double* data, const int32_t* perm_in, const double* diag_jump,
+                 cudaStream_t s);
+
 // y = H x (original boundary ordering, FP64) using the library's static device scratch
 // instead of allocated buffers (see spx_hmat_apply_noalloc in include/spx.h).
 void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s);

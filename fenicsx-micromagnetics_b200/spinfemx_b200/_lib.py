@@ -78,6 +78,12 @@ SIGNATURES = {
     "spx_demag_counters": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_demag_residuals": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_demag_amg_levels": (C.c_int, [c_vp, c_vp, C.c_int32, c_vp]),
+    "spx_demag_create_with_hmat": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), c_vp,
+                                             C.POINTER(c_vp)]),
+    "spx_hmat_export_sizes": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_hmat_export": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_hmat_import": (C.c_int, [c_vp, C.POINTER(HmatConfig), c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                  c_vp, C.POINTER(c_vp)]),
     "spx_demag_set_tolerances": (C.c_int, [c_vp, C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int32]),
     "spx_llg_create": (C.c_int, [c_vp, c_vp, c_i64, c_vp, c_i64, C.POINTER(LLGParams), C.POINTER(c_vp)]),
     "spx_llg_heff": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),

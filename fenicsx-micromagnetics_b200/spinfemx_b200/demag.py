@@ -26,7 +26,8 @@ class DemagFieldLindholmGPU:
                  hmatrix_compressor="fullaca", hmatrix_max_rank=None,
                  hmatrix_max_temporary_block_bytes=256 * 1024 ** 2, hmatrix_use_fp32=True, precision="f64",
                  hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False,
-                 u1_preconditioner="amg", **unused):
+                 u1_preconditioner="amg", hmatrix_cache_path=None, hmatrix_cache_dir="./hmatrix_cache",
+                 cache_tag=None, hmatrix_force_rebuild=False, hmatrix_cache_compressed=False, **unused):
         """Options as in the reference, plus:
 
         precision          'f64' | 'f32' (plain FP32) | 'mixed' (FP64 vectors, FP32 matrices,
@@ -37,6 +38,11 @@ class DemagFieldLindholmGPU:
                            'extrapolate': per-RK-stage quadratic extrapolation (time loop)
         u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or
                            'jacobi'
+        hmatrix_cache_path / cache_tag
+                           npz cache of the H-matrix in the reference's schema
+                           (Demag_Lindholm_GPU.py:353-377 naming in hmatrix_cache_dir or
+                           $DEMAG_HMATRIX_CACHE_DIR when only cache_tag is given).  Without either,
+                           the H-matrix is built on the GPU and no file is written.
         """
         if str(incident_policy).lower()[:4] != "skip":
             raise ValueError("only incident_policy='skip' (the reference default) is implemented")
@@ -85,7 +91,33 @@ class DemagFieldLindholmGPU:
                                  max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
                                  precision=_lib.PREC[hprec], reserved=0, batch_bytes=int(hmatrix_batch_bytes))
         self._h = C.c_void_p()
-        call("spx_demag_create", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o), C.byref(self._h))
+        self.hmatrix_cache_path = None
+        if req == "hmatrix" and (hmatrix_cache_path is not None or cache_tag is not None):
+            import os
+            from pathlib import Path
+            from .hmatrix import HMatrixBuildConfig, build_or_load_hmatrix
+            if hmatrix_cache_path is None:
+                root = Path(os.environ.get("DEMAG_HMATRIX_CACHE_DIR", hmatrix_cache_dir))
+                eps_tag = f"{float(hmatrix_epsilon):.0e}".replace("+", "")
+                eta_tag = f"{float(hmatrix_eta):g}".replace(".", "p")
+                comp = str(hmatrix_compressor).strip().lower().replace("-", "_")
+                hmatrix_cache_path = root / (f"{cache_tag}_eps{eps_tag}_eta{eta_tag}_leaf{int(hmatrix_leaf_size)}_"
+                                             f"{comp}_gpu.npz")
+            self.hmatrix_cache_path = str(hmatrix_cache_path)
+            cfg = HMatrixBuildConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
+                                     leaf_size=int(hmatrix_leaf_size), max_rank=hmatrix_max_rank,
+                                     max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
+                                     batch_bytes=int(hmatrix_batch_bytes))
+            Hc = build_or_load_hmatrix(self.hmatrix_cache_path, X, tets, cfg, precision=hprec,
+                                       force_rebuild=bool(hmatrix_force_rebuild), verbose=bool(hmatrix_verbose),
+                                       cache_compressed=bool(hmatrix_cache_compressed))
+            self.hmatrix_metadata = Hc.metadata
+            call("spx_demag_create_with_hmat", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o),
+                 Hc.handle, C.byref(self._h))
+            del Hc  # its data moved into the demag object
+        else:
+            call("spx_demag_create", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o),
+                 C.byref(self._h))
         N, Nb, NI, by = _lib.c_i64(), _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
         call("spx_demag_info", self._h, C.byref(N), C.byref(Nb), C.byref(NI), C.byref(by))
         self.Nb, self.NI = Nb.value, NI.value

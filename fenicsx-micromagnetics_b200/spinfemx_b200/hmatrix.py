@@ -3,8 +3,9 @@
 Mirrors the reference package ``gpu/fields/lindholm_hmatrix_gpu``:
 
 * ``HMatrixBuildConfig``      builder.py:24-95 (same fields, same validation)
-* ``build_or_load_hmatrix``   builder.py:814-927 (GPU construction; the npz cache
-  format is not implemented: every call builds)
+* ``build_or_load_hmatrix``   builder.py:814-927 (GPU construction; npz cache in the
+  reference's ``HMatrixCPUData.save/load`` schema, storage.py:72-209, with the same
+  geometry-hash / build-config / provider-signature validation)
 * ``HMatrixGPUPackedFused``   backend_fused.py:341-646 (``matvec``, ``matvec_numpy``,
   ``benchmark``, ``benchmark_roundtrip``, ``memory_report``)
 
@@ -14,14 +15,35 @@ libspx; see csrc/hbuild.cu and csrc/hmat.cu.
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass
+import json
+from dataclasses import asdict, dataclass
+from hashlib import sha256
+from pathlib import Path
 from time import perf_counter
 
 import numpy as np
 
 from . import _lib
 from ._lib import call, ptr
-from .geometry import BoundaryGeometry
+from .geometry import BoundaryGeometry, boundary_data
+
+HMATRIX_CONSTRUCTION_VERSION = "lindholm-hmatrix-build-v2-b200"
+# cache signature of the device entry provider (the reference's providers report theirs,
+# entry_provider.py:177-185, entry_provider_gpu.py:473-486)
+PROVIDER_SIGNATURE = {"provider": "LindholmEntryProviderB200", "kernel_version": "lindholm-tiles-sm100a-v1",
+                      "incident_policy": 0}
+FAR_META_DTYPE = np.dtype([("row_start", np.int64), ("row_stop", np.int64), ("col_start", np.int64),
+                           ("col_stop", np.int64), ("rank", np.int64), ("u_offset", np.int64), ("u_size", np.int64),
+                           ("v_offset", np.int64), ("v_size", np.int64), ("relative_residual", np.float64)])
+
+
+def geometry_hash(Xb, tri_lid=None) -> str:
+    """sha256 of the boundary points (and triangles), as builder.py:98-103."""
+    digest = sha256()
+    digest.update(np.ascontiguousarray(Xb, dtype=np.float64).view(np.uint8))
+    if tri_lid is not None:
+        digest.update(np.ascontiguousarray(tri_lid, dtype=np.int32).view(np.uint8))
+    return digest.hexdigest()
 
 STAT_NAMES = ("dense_blocks", "low_rank_blocks", "rejected_low_rank_blocks", "forced_subdivisions_memory",
               "compression_tolerance_subdivisions", "max_observed_rank", "sum_observed_rank",
@@ -96,6 +118,7 @@ class HMatrixGPUPackedFused:
             raise ValueError("threads_per_block must be between 32 and 1024.")
         self.precision = _precision_name(use_fp32, precision)
         self._owner = _owner
+        self.metadata = {}
         if _handle is not None:
             self._h = _handle
             self._owned = False
@@ -119,6 +142,10 @@ class HMatrixGPUPackedFused:
     @classmethod
     def from_handle(cls, handle, owner, precision, size):
         return cls(_handle=handle, _owner=owner, precision=precision, _size=size)
+
+    @property
+    def handle(self):
+        return self._h
 
     # --------------------------------------------------------------- info
     def stats(self):
@@ -216,6 +243,84 @@ class HMatrixGPUPackedFused:
         return {"timer": "perf_counter_roundtrip", "repeats": int(repeats), "total_seconds": el,
                 "average_seconds": el / repeats}
 
+    # --------------------------------------------------------------- cache
+    def cache_arrays(self):
+        """The reference's HMatrixCPUData arrays (storage.py:72-149) of this H-matrix."""
+        nf, nu, nv, nz = (_lib.c_i64() for _ in range(4))
+        call("spx_hmat_export_sizes", self._h, C.byref(nf), C.byref(nu), C.byref(nv), C.byref(nz))
+        nf, nu, nv, nz = nf.value, nu.value, nv.value, nz.value
+        perm = np.empty(self.size, np.int32)
+        diag = np.empty(self.size)
+        meta5 = np.empty((nf, 5), np.int64)
+        relres = np.empty(nf)
+        U = np.empty(nu)
+        V = np.empty(nv)
+        indptr = np.empty(self.size + 1, np.int32)
+        indices = np.empty(nz, np.int32)
+        data = np.empty(nz)
+        call("spx_hmat_export", self._h, ptr(perm), ptr(diag), ptr(meta5), ptr(relres), ptr(U), ptr(V), ptr(indptr),
+             ptr(indices), ptr(data))
+        m = meta5[:, 1] - meta5[:, 0]
+        n = meta5[:, 3] - meta5[:, 2]
+        k = meta5[:, 4]
+        far_meta = np.zeros(nf, FAR_META_DTYPE)
+        for i, name in enumerate(("row_start", "row_stop", "col_start", "col_stop", "rank")):
+            far_meta[name] = meta5[:, i]
+        far_meta["u_size"] = m * k
+        far_meta["v_size"] = k * n
+        far_meta["u_offset"] = np.concatenate([[0], np.cumsum(m * k)[:-1]]) if nf else []
+        far_meta["v_offset"] = np.concatenate([[0], np.cumsum(k * n)[:-1]]) if nf else []
+        far_meta["relative_residual"] = relres
+        return dict(perm=perm, diag_jump=diag, near_data=data, near_indices=indices, near_indptr=indptr,
+                    near_shape=np.array([self.size, self.size], np.int64), far_meta=far_meta, far_U_flat=U,
+                    far_V_flat=V)
+
+    def save(self, path, *, compressed=True, metadata=None):
+        """Write the reference's npz cache (HMatrixCPUData.save, storage.py:72-149)."""
+        path = Path(path)
+        path.parent.mkdir(parents=True, exist_ok=True)
+        arrays = self.cache_arrays()
+        arrays["metadata_json"] = np.asarray(json.dumps(metadata or {}))
+        with path.open("wb") as f:
+            (np.savez_compressed if compressed else np.savez)(f, **arrays)
+
+    @classmethod
+    def load(cls, path, geometry: BoundaryGeometry, config: HMatrixBuildConfig | None = None, precision="f32"):
+        """Read an npz cache in the reference's schema (HMatrixCPUData.load, storage.py:151-209)
+        onto the device.  The cluster tree is rebuilt from ``geometry`` and must reproduce the
+        cached permutation.  Returns (H, metadata)."""
+        a = np.load(Path(path), allow_pickle=False)
+        perm = np.ascontiguousarray(a["perm"], dtype=np.int32)
+        if perm.size != geometry.Nb:
+            raise ValueError(f"cache has {perm.size} boundary nodes, the geometry {geometry.Nb}")
+        fm = a["far_meta"]
+        meta5 = np.ascontiguousarray(np.stack([fm[k] for k in ("row_start", "row_stop", "col_start", "col_stop",
+                                                               "rank")], 1).astype(np.int64)).reshape(-1, 5)
+        U_all = np.asarray(a["far_U_flat"], dtype=np.float64)
+        V_all = np.asarray(a["far_V_flat"], dtype=np.float64)
+        # factors in block order, contiguous (the offsets of the file may have any order)
+        if fm.size:
+            U = np.concatenate([U_all[o:o + z] for o, z in zip(fm["u_offset"], fm["u_size"])])
+            V = np.concatenate([V_all[o:o + z] for o, z in zip(fm["v_offset"], fm["v_size"])])
+        else:
+            U = V = np.empty(0)
+        relres = np.ascontiguousarray(fm["relative_residual"], dtype=np.float64) if fm.size else np.empty(0)
+        indptr = np.ascontiguousarray(a["near_indptr"], dtype=np.int32)
+        indices = np.ascontiguousarray(a["near_indices"], dtype=np.int32)
+        data = np.ascontiguousarray(a["near_data"], dtype=np.float64)
+        diag = np.ascontiguousarray(a["diag_jump"], dtype=np.float64)
+        raw = str(np.asarray(a["metadata_json"]).item())
+        metadata = json.loads(raw) if raw else {}
+        cfg = config or HMatrixBuildConfig(leaf_size=int(metadata.get("build_config", {}).get("leaf_size", 64)))
+        c = cfg.to_c(precision)
+        h = C.c_void_p()
+        call("spx_hmat_import", geometry.handle, C.byref(c), ptr(perm), ptr(diag), meta5.shape[0], ptr(meta5),
+             ptr(relres), ptr(U), ptr(V), ptr(indptr), ptr(indices), ptr(data), C.byref(h))
+        H = cls(_handle=h, _owner=None, precision=precision, _size=geometry.Nb)
+        H._owned = True
+        H._geometry = geometry
+        return H, metadata
+
     def memory_report(self):
         f, n, t = _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
         call("spx_hmat_memory", self._h, C.byref(f), C.byref(n), C.byref(t))
@@ -241,18 +346,54 @@ class HMatrixGPUPackedFused:
             pass
 
 
-def build_or_load_hmatrix(cache_path, X, tets, config: HMatrixBuildConfig | None = None, *,
-                          precision="f32", force_rebuild=False, verbose=False, geometry=None):
-    """Build the H-matrix of the mesh boundary on the GPU (builder.py:814-927).
+def _cache_build_config(config: HMatrixBuildConfig) -> dict:
+    value = asdict(config)
+    value["resolved_build_backend"] = "gpu"
+    value["construction_version"] = HMATRIX_CONSTRUCTION_VERSION
+    return json.loads(json.dumps(value, sort_keys=True))
 
-    ``cache_path`` is accepted for call compatibility; this build does not write or
-    read the reference's npz cache.
-    """
-    del cache_path, force_rebuild
+
+def build_or_load_hmatrix(cache_path, X, tets, config: HMatrixBuildConfig | None = None, *,
+                          precision="f32", force_rebuild=False, verbose=False, geometry=None, cache_compressed=True):
+    """Build the H-matrix of the mesh boundary on the GPU, or load it from an npz cache
+    (builder.py:814-927).  A cache is used when its metadata carries the same geometry hash
+    (boundary points and triangles), build configuration and provider signature; else the
+    matrix is built and the cache (re)written.  ``cache_path=None`` builds without a file.
+    The returned object carries ``metadata`` (cache_loaded, cache_file_bytes, ...)."""
     geom = geometry or BoundaryGeometry(X, tets)
-    H = HMatrixGPUPackedFused(geom, config or HMatrixBuildConfig(), precision=precision)
+    cfg = config or HMatrixBuildConfig()
+    bd = boundary_data(X, tets)
+    expected = {"geometry_hash": geometry_hash(bd["Xb"], bd["tri_lid"]), "build_config": _cache_build_config(cfg),
+                "provider_signature": dict(PROVIDER_SIGNATURE)}
+    path = Path(cache_path) if cache_path is not None else None
+    if path is not None and path.exists() and not force_rebuild:
+        try:
+            H, meta = HMatrixGPUPackedFused.load(path, geom, cfg, precision=precision)
+        except (ValueError, KeyError, RuntimeError, OSError) as exc:
+            H, meta = None, {"load_error": str(exc)}
+        if H is not None and all(meta.get(k) == v for k, v in expected.items()):
+            meta["cache_loaded"] = True
+            meta["cache_file_bytes"] = int(path.stat().st_size)
+            H.metadata = meta
+            if verbose:
+                print(f"[HMatrix b200] loaded cache: {path}", flush=True)
+            return H
+        if verbose:
+            print("[HMatrix b200] cache metadata changed; rebuilding.", flush=True)
+        del H
+    H = HMatrixGPUPackedFused(geom, cfg, precision=precision)
+    st = H.stats()
+    meta = {"Nb": geom.Nb, **expected, "build_time_seconds": st["build_time_seconds"],
+            "average_far_rank": st["average_far_rank"], "resolved_build_backend": "gpu",
+            "construction_version": HMATRIX_CONSTRUCTION_VERSION,
+            **{k: st[k] for k in STAT_NAMES}, "cache_compressed": bool(cache_compressed), "cache_loaded": False}
+    if path is not None:
+        t0 = perf_counter()
+        H.save(path, compressed=cache_compressed, metadata=meta)
+        meta["cache_write_seconds"] = perf_counter() - t0
+        meta["cache_file_bytes"] = int(path.stat().st_size)
+    H.metadata = meta
     if verbose:
-        st = H.stats()
         print(f"[HMatrix b200] built in {st['build_time_seconds']:.2f} s | far={st['n_far']} near={st['n_near']} "
               f"| rank avg/max={st['average_far_rank']:.1f}/{st['max_observed_rank']}", flush=True)
     return H

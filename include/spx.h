@@ -132,6 +132,24 @@ SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_s
 SPX_API int spx_hmat_far_factors(spx_hmat h, int64_t index, double* Ut, double* V);
 SPX_API int spx_hmat_memory(spx_hmat h, int64_t* far_bytes, int64_t* near_bytes, int64_t* total_bytes);
 SPX_API int spx_hmat_destroy(spx_hmat h);
+/* The reference's cache contents (HMatrixCPUData, lindholm_hmatrix_gpu/storage.py:29-325; the
+ * npz file itself is read and written by numpy in the Python layer):
+ *   perm[Nb]; diag_jump[Nb] (original order); near field as CSR in permutation space with exact
+ *   zeros dropped (indptr[Nb+1], indices, data); far blocks as far_meta5[nfar][5] =
+ *   (row_start, row_stop, col_start, col_stop, rank), relres[nfar], U_flat (m x k row-major
+ *   per block), V_flat (k x n row-major per block), blocks in the same order.
+ * export_sizes computes the near CSR and must precede export (HMatrixCPUData.save, :72-149). */
+SPX_API int spx_hmat_export_sizes(spx_hmat h, int64_t* nfar, int64_t* u_entries, int64_t* v_entries,
+                                  int64_t* near_nnz);
+SPX_API int spx_hmat_export(spx_hmat h, int32_t* perm, double* diag_jump, int64_t* far_meta5, double* relres,
+                            double* U, double* V, int32_t* near_indptr, int32_t* near_indices, double* near_data);
+/* HMatrixCPUData.load (:151-209) + upload: the cluster tree is rebuilt from the boundary and
+ * must reproduce `perm`; the near CSR becomes dense leaf x leaf tiles; packed in
+ * cfg->precision.  diag_jump may be NULL (then taken from the boundary's solid angles). */
+SPX_API int spx_hmat_import(spx_boundary b, const spx_hmat_config* cfg, const int32_t* perm, const double* diag_jump,
+                            int64_t nfar, const int64_t* far_meta5, const double* relres, const double* U,
+                            const double* V, const int32_t* near_indptr, const int32_t* near_indices,
+                            const double* near_data, spx_hmat* out);
 
 /* ------------------------------------------------------------------ demag field */
 typedef struct spx_demag_s* spx_demag;
@@ -148,6 +166,12 @@ typedef struct {
 SPX_API int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                      const spx_demag_options* opt, spx_demag* out);
 /* DemagFieldLindholmGPU.compute_vec (:643-670): H = -grad(u1+u2) lumped, AoS FP64 device */
+/* DemagFieldLindholmGPU with an H-matrix from build_or_load_hmatrix (Demag_Lindholm_GPU.py:
+ * 377-430): opt->backend must be 1; the H-matrix is moved into the demag object (h keeps no
+ * data afterwards and is still destroyed by the caller) and repacked if opt->hmat.precision
+ * differs from its packing */
+SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                                       const spx_demag_options* opt, spx_hmat h, spx_demag* out);
 SPX_API int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s);
 /* potentials of the last apply (FP64 device, N each) */
 SPX_API int spx_demag_potentials(spx_demag d, double* u1, double* u2, spx_stream_t s);

@@ -14,6 +14,8 @@ Each fixture holds seeded inputs and the outputs of the REFERENCE's own code:
 * ``trees.npz``  lindholm_hmatrix_gpu/tree.py permutations.
 * ``hmat_<case>.npz``  lindholm_hmatrix_gpu/builder.py ``HMatrixBuilder``
   (CPU, full-pivot ACA): block partition, ranks, near nnz, H @ x.
+* ``hcache_film14.npz``  the reference's own npz cache (``HMatrixCPUData.save``,
+  storage.py:72-149) of a 14x14x2 film H-matrix (eps 1e-4, leaf 16), for the cache reader.
 * ``llg_kernels.npz``  the reference's per-node CUDA-C kernel bodies compiled
   with gcc by ``oracle/ref_build.py`` plus the CPU numba Jv kernel.
 
@@ -127,6 +129,21 @@ def make_hmatrix(mods, name, bd, eps=1e-5, eta=2.0, leaf=64):
     return data
 
 
+CACHE_CASE = (14, 14, 2, 2.5)  # with eps 1e-4, eta 2, leaf 16
+
+
+def make_cache(mods):
+    """The reference's npz cache of an H-matrix, written by its own HMatrixCPUData.save."""
+    X, T = mesh.kuhn_box(*CACHE_CASE)
+    bd = lindholm.boundary_data(X, T)
+    bl = mods["builder"]
+    dj = bd["omega_sum"] / (4.0 * math.pi) - 1.0
+    cfg = bl.HMatrixBuildConfig(epsilon=1e-4, eta=2.0, leaf_size=16, compressor="fullaca", build_backend="cpu")
+    data = bl.HMatrixBuilder(bd["Xb"], dj, provider_for(mods, bd), cfg).build()
+    data.save(OUT / "hcache_film14.npz", compressed=True)
+    return data
+
+
 def make_aca(mods):
     cp = mods["compressors"]
     rng = np.random.default_rng(1004)
@@ -219,6 +236,7 @@ def main():
     for name in CASES:
         d = make_hmatrix(mods, name, bds[name])
         print(name, "far", len(d.far_blocks), "near nnz", d.near_csr.nnz, flush=True)
+    make_cache(mods)
 
 
 if __name__ == "__main__":
