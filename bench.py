@@ -202,7 +202,7 @@ def run_ours(a):
         demag_kwargs=dict(boundary_backend="hmatrix", hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64,
                           ksp_rtol_u1=a.rtol_u1, ksp_rtol_u2=a.rtol_u2, precision=a.precision,
                           hmatrix_precision=a.hmatrix_precision,
-                          warm_start={0: False, 1: True, 2: "extrapolate"}[a.warm_start]))
+                          warm_start={0: False, 1: True, 2: "extrapolate", 3: "extrapolate_corrected"}[a.warm_start]))
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     dm = hef.demag_field
@@ -300,7 +300,8 @@ def run_ours(a):
                    "nodes": N, "boundary_nodes": dm.Nb, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (H-matrix factors %.1f GB per apply)" % (
                        (Hmem["far_bytes"] + Hmem["near_bytes"]) / 1e9),
-                   "cg_start": {0: "zero", 1: "previous", 2: "extrapolated per RK stage"}[a.warm_start],
+                   "cg_start": {0: "zero", 1: "previous", 2: "extrapolated per RK stage",
+                                3: "extrapolated per RK stage, corrected by stage 1"}[a.warm_start],
                    "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2,
                    "demag_rel_err_vs_fp64": err},
         "e2e": e2e,
@@ -486,7 +487,7 @@ def main():
     ap.add_argument("--dt", type=float, default=5e-14)
     ap.add_argument("--rtol-u1", type=float, default=1e-8)
     ap.add_argument("--rtol-u2", type=float, default=1e-8)
-    ap.add_argument("--warm-start", type=int, default=2, help="0 zero, 1 previous, 2 extrapolated per RK stage")
+    ap.add_argument("--warm-start", type=int, default=3, help="0 zero, 1 previous, 2 extrapolated per RK stage, 3 extrapolated and corrected")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--check-error", type=int, default=1)

@@ -615,7 +615,7 @@ static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t
   DemagOptions o;
   if (opt) {
     SPX_CHECK(opt->backend == 0 || opt->backend == 1, "backend must be 0 (dense) or 1 (hmatrix)");
-    SPX_CHECK(opt->warm_start >= 0 && opt->warm_start <= 2, "warm_start must be 0, 1 or 2");
+    SPX_CHECK(opt->warm_start >= 0 && opt->warm_start <= 3, "warm_start must be 0, 1, 2 or 3");
     o.backend = opt->backend;
     o.prec = to_prec(opt->precision);
     o.hprec = to_prec(opt->hmat.precision);

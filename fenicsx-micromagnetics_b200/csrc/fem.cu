@@ -133,6 +133,13 @@ __global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const TV*
 }
 
 // starting guess: quadratic / linear / constant extrapolation of stored solutions
+__global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ out, int mode) {  // mode 0: out = a - b; 1: out += a
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = mode == 0 ? a[i] - b[i] : out[i] + a[i];
+}
+
 template <class T>
 __global__ void k_extrap(int64_t n, const double* __restrict__ h0, const double* __restrict__ h1,
                          const double* __restrict__ h2, int cnt, T* __restrict__ out) {
@@ -573,6 +580,16 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
                                                          hcount[slot], target);
       SPX_LAUNCH_CHECK();
       warm = true;
+      if (stage_correct) {
+        if (slot == 0) {
+          if (!pred0.n) pred0.alloc(n);
+          SPX_CUDA(cudaMemcpyAsync(pred0.p, target, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+          have_pred0 = true;
+        } else if (have_delta) {
+          k_axpy_sub<<<grid_for(n, 256), 256, 0, st>>>(n, delta.p, nullptr, target, 1);
+          SPX_LAUNCH_CHECK();
+        }
+      }
     }
   }
   SPX_CUDA(cudaMemsetAsync(bar.p, 0, bar.bytes(), st));
@@ -608,6 +625,14 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     p.rtol = rtol; p.atol = atol; p.maxit = maxit; p.warm = warm ? 1 : 0; p.project = project ? 1 : 0;
     void* args[] = {&p};
     SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg), dim3(grid), dim3(block), args, 0, st));
+  }
+  if (slot == 0 && stage_correct && have_pred0) {  // stage 1's prediction error
+    if (!delta.n) delta.alloc(n);
+    k_axpy_sub<<<grid_for(n, 256), 256, 0, st>>>(n, ir ? y64.p : reinterpret_cast<const double*>(x), pred0.p,
+                                                 delta.p, 0);
+    SPX_LAUNCH_CHECK();
+    have_delta = true;
+    have_pred0 = false;
   }
   if (slot >= 0) {
     double* dst = hist[slot][hhead[slot]].p;
@@ -683,6 +708,7 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
       for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
         if (fem.col[k] == i) d[i] = fem.A[k];
     cg1.setup(hsell, a, d);
+    cg1.stage_correct = opt.warm_start == 3;
     if (opt.u1_pc == 0) cg1.enable_amg(hsell, fem.rowptr, fem.col, fem.A, d, true, s);
   }
   std::vector<int32_t> bmap(N, -1), imap(N, -1), inter;
@@ -709,6 +735,7 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
         if (fem.col[k] == i) d[q] = fem.A[k];
     }
     cg2.setup(sII, aII, d);
+    cg2.stage_correct = opt.warm_start == 3;
     PIB.upload(sIB, s);
     AIB.upload(aIB, s);
   }
@@ -739,7 +766,7 @@ template <class TV, class TM>
 void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, int slot) {
   const int threads = 256;
   const bool warm = opt.warm_start != 0;
-  const int sl = (opt.warm_start == 2) ? slot : -1;
+  const int sl = (opt.warm_start >= 2) ? slot : -1;
   prof.mark(PC_DIV, s);
   k_div<TV, TM><<<grid_for(P.nslices * 32, threads), threads, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Div.p,
                                                                      P.len, Dsum.p, m, b.p);

@@ -95,6 +95,9 @@ struct CgSystem {
   DevBuf<double> res_acc;                // [0] sum of initial, [1] sum of final relative residuals
   DevBuf<double> hist[4][3];
   int hcount[4] = {0, 0, 0, 0}, hhead[4] = {0, 0, 0, 0};
+  // stage correction: slots 1..3 add slot 0's last prediction error (solution - guess)
+  bool stage_correct = false, have_pred0 = false, have_delta = false;
+  DevBuf<double> pred0, delta;
   double inner_rtol = 1e-3;
   int max_outer = 10;
   int grid = 0, block = 0;
@@ -117,6 +120,7 @@ struct CgSystem {
                 cudaStream_t st, bool sync_stats);
   void reset_history() {
     for (int s = 0; s < 4; ++s) hcount[s] = hhead[s] = 0;
+    have_pred0 = have_delta = false;
   }
 };
 
@@ -126,7 +130,8 @@ struct DemagOptions {
   Prec hprec = Prec::F64;   // storage precision of the H-matrix factors
   double rtol_u1 = 1e-6, rtol_u2 = 1e-6, atol = 1e-12;
   int maxit_u1 = 2000, maxit_u2 = 12000;
-  int warm_start = 0;       // 0 zero start, 1 previous solution, 2 extrapolated per RK stage
+  int warm_start = 0;       // 0 zero start, 1 previous solution, 2 extrapolated per RK stage,
+                            // 3 as 2, stages 2-4 corrected by stage 1's prediction error
   int u1_pc = 0;            // u1 preconditioner: 0 smoothed-aggregation AMG, 1 Jacobi
   HMatrix* preset = nullptr;  // hmatrix backend: adopt this H-matrix (moved in) instead of building
   HBuildConfig hcfg;

@@ -35,7 +35,9 @@ class DemagFieldLindholmGPU:
         hmatrix_precision  factor storage 'f64' | 'f32' | 'bf16' (default: 'f64' for
                            precision='f64', 'f32' otherwise)
         warm_start         False: zero start (the reference); True: previous solution;
-                           'extrapolate': per-RK-stage quadratic extrapolation (time loop)
+                           'extrapolate': per-RK-stage quadratic extrapolation (time loop);
+                           'extrapolate_corrected': the same, stages 2-4 shifted by stage 1's
+                           prediction error
         u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or
                            'jacobi'
         hmatrix_cache_path / cache_tag
@@ -70,9 +72,9 @@ class DemagFieldLindholmGPU:
         if hprec not in ("f64", "f32", "bf16"):
             raise ValueError("hmatrix_precision must be 'f64', 'f32' or 'bf16'")
         self.hmatrix_precision = hprec
-        ws = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, "extrapolate": 2}.get(warm_start)
+        ws = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, 3: 3, "extrapolate": 2, "extrapolate_corrected": 3}.get(warm_start)
         if ws is None:
-            raise ValueError("warm_start must be False, True or 'extrapolate'")
+            raise ValueError("warm_start must be False, True, 'extrapolate' or 'extrapolate_corrected'")
         o = _lib.DemagOptions()
         o.backend = 0 if req == "dense" else 1
         o.precision = _lib.PREC[precision]

@@ -158,7 +158,8 @@ typedef struct {
   int32_t precision; /* SPX_PREC_* */
   double rtol_u1, rtol_u2, atol; /* ksp_rtol_u1/u2 (:216-226, :271-281), atol 1e-12 */
   int32_t maxit_u1, maxit_u2;    /* 2000 / 12000 in the reference */
-  int32_t warm_start;            /* 0 zero start (reference), 1 previous solution, 2 extrapolated per RK stage */
+  int32_t warm_start;            /* 0 zero start (reference), 1 previous solution, 2 extrapolated per RK stage,
+                                    3 as 2 with stages 2-4 corrected by stage 1's prediction error */
   int32_t u1_preconditioner;     /* 0 smoothed-aggregation AMG (the reference's PC "gamg", :219-222), 1 Jacobi */
   spx_hmat_config hmat;
 } spx_demag_options;
