@@ -223,28 +223,25 @@ __device__ __forceinline__ double block_sum(double v, double* smem) {
 __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen,
                                              unsigned int nblocks, int* err,
                                              long long limit = (1ll << 26)) {
+  // One monotonic arrival counter (zeroed before the launch): a CTA adds 1 and waits until
+  // the counter reaches the next multiple of nblocks.  `gen` is not used.
+  (void)gen;
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = gen;
+    volatile unsigned int* vc = count;
     volatile int* verr = err;
-    const unsigned int g = *vgen;
     __threadfence();
-    const unsigned int arrived = atomicAdd(count, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(count, 0u);
-      __threadfence();
-      atomicAdd(gen, 1u);
-    } else {
-      long long it = 0;
-      while (*vgen == g) {
-        if (*verr != 0) break;
-        if (++it > limit) {
-          atomicCAS(err, 0, ERR_TIMEOUT);
-          break;
-        }
-        if (it > 4096) __nanosleep(32);
+    const unsigned int old = atomicAdd(count, 1u);
+    const unsigned int target = (old / nblocks + 1u) * nblocks;
+    long long it = 0;
+    while (static_cast<int>(*vc - target) < 0) {
+      if (*verr != 0) break;
+      if (++it > limit) {
+        atomicCAS(err, 0, ERR_TIMEOUT);
+        break;
       }
+      if (it > 4096) __nanosleep(32);
     }
     __threadfence();
     s_ok = (*verr == 0);
