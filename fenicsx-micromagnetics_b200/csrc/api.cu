@@ -96,6 +96,7 @@ struct DemagBase {
   virtual void residuals(double a[2], double b[2]) = 0;
   virtual int amg_levels(int64_t* out, int maxl) = 0;
   virtual void set_tolerances(double r1, double r2, double at, int m1, int m2) = 0;
+  virtual void apply_transpose(const double* w, double* out, cudaStream_t s) = 0;
 };
 
 template <class TV, class TM>
@@ -168,6 +169,17 @@ struct DemagImpl : DemagBase {
     d.opt.rtol_u1 = r1; d.opt.rtol_u2 = r2; d.opt.atol = at;
     d.opt.maxit_u1 = m1; d.opt.maxit_u2 = m2;
   }
+  void apply_transpose(const double* w, double* out, cudaStream_t s) override {
+    if (sizeof(TV) == sizeof(double)) {
+      d.apply_transpose(reinterpret_cast<const TV*>(w), reinterpret_cast<TV*>(out), false, -1, s);
+    } else {
+      const int64_t n3 = 3 * d.N;
+      if (!tm.n) { tm.alloc(n3); th.alloc(n3); }
+      convert<double, TV>(n3, w, tm.p, s);
+      d.apply_transpose(tm.p, th.p, false, -1, s);
+      convert<TV, double>(n3, th.p, out, s);
+    }
+  }
 };
 
 struct spx_demag_s {
@@ -188,6 +200,12 @@ struct LLGBase {
   virtual void run_host(const double* in, double* out, double dt, int64_t n) = 0;
   virtual void set_uniform_field(double x, double y, double z) = 0;
   virtual void stats(int64_t* steps, int64_t* rhs, int64_t* launches) const = 0;
+  virtual void rhs_vjp(const double* m, const double* w, double* out, double* gKu, double* gH0, cudaStream_t s) = 0;
+  virtual void step_vjp(const double* mn, double dt, const double* lin, double* lout, double* gKu, double* gH0,
+                        cudaStream_t s) = 0;
+  virtual void step_jvp(const double* mn, const double* dm, const double* dKu, const double* dH0, double dt,
+                        double* mo, double* dmo, cudaStream_t s) = 0;
+  virtual void set_ku_map(const double* ku) = 0;
 };
 
 template <class TV, class TM>
@@ -255,6 +273,49 @@ struct LLGImpl : LLGBase {
     if (r) *r = l.rhs_evals;
     if (la) *la = l.launches;
   }
+  DevBuf<TV> tc, td, te;
+  TV* scratch(DevBuf<TV>& b) {
+    if (!b.n) b.alloc(3 * l.N);
+    return b.p;
+  }
+  // FP64 -> TV copy into a given scratch (FP64 pipelines use the caller's buffer)
+  const TV* in_to(const double* p, DevBuf<TV>& b, cudaStream_t s) {
+    if (f64) return reinterpret_cast<const TV*>(p);
+    convert<double, TV>(3 * l.N, p, scratch(b), s);
+    return b.p;
+  }
+  TV* out_of(double* p, DevBuf<TV>& b) { return f64 ? reinterpret_cast<TV*>(p) : scratch(b); }
+  void back(double* p, DevBuf<TV>& b, cudaStream_t s) {
+    if (!f64) convert<TV, double>(3 * l.N, b.p, p, s);
+  }
+  void rhs_vjp(const double* m, const double* w, double* o, double* gKu, double* gH0, cudaStream_t s) override {
+    l.adjoint_setup(s);
+    const TV* mm = in_to(m, ta, s);
+    const TV* ww = in_to(w, tc, s);
+    TV* oo = out_of(o, tb);
+    l.heff(mm, l.adj.Hs[0].p, true, s);
+    l.rhs_vjp(mm, l.adj.Hs[0].p, ww, oo, gKu, gH0, -1, s);
+    back(o, tb, s);
+  }
+  void step_vjp(const double* mn, double dt, const double* lin, double* lout, double* gKu, double* gH0,
+                cudaStream_t s) override {
+    const TV* mm = in_to(mn, ta, s);
+    const TV* li = in_to(lin, tc, s);
+    TV* lo = out_of(lout, tb);
+    l.step_vjp(mm, dt, li, lo, gKu, gH0, s);
+    back(lout, tb, s);
+  }
+  void step_jvp(const double* mn, const double* dm, const double* dKu, const double* dH0, double dt, double* mo,
+                double* dmo, cudaStream_t s) override {
+    const TV* mm = in_to(mn, ta, s);
+    const TV* dd = in_to(dm, tc, s);
+    TV* o1 = out_of(mo, tb);
+    TV* o2 = out_of(dmo, td);
+    l.step_jvp(mm, dd, dKu, dH0, dt, o1, o2, s);
+    back(mo, tb, s);
+    back(dmo, td, s);
+  }
+  void set_ku_map(const double* ku) override { l.set_ku_map(ku, 0); }
 };
 
 struct spx_llg_s {
@@ -561,6 +622,15 @@ int spx_hmat_apply(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   API_END
 }
 
+int spx_hmat_apply_transpose(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(hm);
+  REQUIRE(x);
+  REQUIRE(y);
+  hm->h.transposed(S(s)).apply_f64(x, y, S(s));
+  API_END
+}
+
 int spx_hmat_apply_noalloc(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   API_BEGIN
   REQUIRE(hm);
@@ -791,6 +861,13 @@ int spx_demag_set_tolerances(spx_demag d, double rtol_u1, double rtol_u2, double
   API_END
 }
 
+int spx_demag_apply_transpose(spx_demag d, const double* w, double* out, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(d); REQUIRE(w); REQUIRE(out);
+  d->impl->apply_transpose(w, out, S(s));
+  API_END
+}
+
 int spx_demag_destroy(spx_demag d) {
   API_BEGIN
   delete d;
@@ -927,6 +1004,39 @@ int spx_llg_stats(spx_llg l, int64_t* steps, int64_t* rhs, int64_t* launches) {
   API_BEGIN
   REQUIRE(l);
   l->impl->stats(steps, rhs, launches);
+  API_END
+}
+
+int spx_llg_set_anisotropy_map(spx_llg l, const double* Ku_nodes) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(Ku_nodes);
+  l->impl->set_ku_map(Ku_nodes);
+  API_END
+}
+
+int spx_llg_rhs_vjp(spx_llg l, const double* m, const double* w, double* mbar, double* gKu, double* gH0,
+                    spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m); REQUIRE(w); REQUIRE(mbar);
+  l->impl->rhs_vjp(m, w, mbar, gKu, gH0, S(s));
+  API_END
+}
+
+int spx_llg_step_vjp(spx_llg l, const double* m_n, double dt, const double* lam_in, double* lam_out, double* gKu,
+                     double* gH0, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m_n); REQUIRE(lam_in); REQUIRE(lam_out);
+  SPX_CHECK(dt > 0.0, "dt must be positive");
+  l->impl->step_vjp(m_n, dt, lam_in, lam_out, gKu, gH0, S(s));
+  API_END
+}
+
+int spx_llg_step_jvp(spx_llg l, const double* m_n, const double* dm, const double* dKu, const double* dH0, double dt,
+                     double* m_out, double* dm_out, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m_n); REQUIRE(dm); REQUIRE(m_out); REQUIRE(dm_out);
+  SPX_CHECK(dt > 0.0, "dt must be positive");
+  l->impl->step_jvp(m_n, dm, dKu, dH0, dt, m_out, dm_out, S(s));
   API_END
 }
 

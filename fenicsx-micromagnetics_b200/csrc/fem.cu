@@ -570,7 +570,7 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   const bool ir = sizeof(TM) == sizeof(float) || use_amg;  // solution state kept in y64
   SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
   if (slot >= 0) {
-    SPX_CHECK(slot < 4, "extrapolation slot out of range");
+    SPX_CHECK(slot < CG_SLOTS, "extrapolation slot out of range");
     for (int k = 0; k < 3; ++k)
       if (!hist[slot][k].n) hist[slot][k].alloc(n);
     if (hcount[slot] > 0) {
@@ -585,7 +585,7 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
           if (!pred0.n) pred0.alloc(n);
           SPX_CUDA(cudaMemcpyAsync(pred0.p, target, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
           have_pred0 = true;
-        } else if (have_delta) {
+        } else if (slot < 4 && have_delta) {
           k_axpy_sub<<<grid_for(n, 256), 256, 0, st>>>(n, delta.p, nullptr, target, 1);
           SPX_LAUNCH_CHECK();
         }

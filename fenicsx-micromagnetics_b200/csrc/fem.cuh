@@ -75,7 +75,10 @@ struct Profiler {
 // Starting guesses: with `slot` >= 0 the solver keeps the last three solutions returned
 // for that slot (e.g. one slot per RK stage) and starts from their quadratic
 // extrapolation 3 x1 - 3 x2 + x3 (linear / constant while fewer are stored).  The stopping
-// rule does not change; only the iteration count does.
+// rule does not change; only the iteration count does.  Slots 0-3: forward RK stages,
+// 4-7: adjoint stages, 8-11: tangent stages (CG_SLOTS).
+constexpr int CG_SLOTS = 12;
+
 template <class TM>
 struct CgSystem {
   int64_t n = 0;
@@ -93,8 +96,8 @@ struct CgSystem {
   DevBuf<double> resid;
   DevBuf<unsigned long long> iters_acc;  // [0] inner iterations, [1] refinement steps, [2] solves
   DevBuf<double> res_acc;                // [0] sum of initial, [1] sum of final relative residuals
-  DevBuf<double> hist[4][3];
-  int hcount[4] = {0, 0, 0, 0}, hhead[4] = {0, 0, 0, 0};
+  DevBuf<double> hist[CG_SLOTS][3];
+  int hcount[CG_SLOTS] = {}, hhead[CG_SLOTS] = {};
   // stage correction: slots 1..3 add slot 0's last prediction error (solution - guess)
   bool stage_correct = false, have_pred0 = false, have_delta = false;
   DevBuf<double> pred0, delta;
@@ -119,7 +122,7 @@ struct CgSystem {
   CgStats solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, int slot,
                 cudaStream_t st, bool sync_stats);
   void reset_history() {
-    for (int s = 0; s < 4; ++s) hcount[s] = hhead[s] = 0;
+    for (int s = 0; s < CG_SLOTS; ++s) hcount[s] = hhead[s] = 0;
     have_pred0 = have_delta = false;
   }
 };
@@ -135,6 +138,20 @@ struct DemagOptions {
   int u1_pc = 0;            // u1 preconditioner: 0 smoothed-aggregation AMG, 1 Jacobi
   HMatrix* preset = nullptr;  // hmatrix backend: adopt this H-matrix (moved in) instead of building
   HBuildConfig hcfg;
+};
+
+// Transposed operators of the demag map m -> H, built on first use of
+// DemagCtx::apply_transpose (adjoint.cu).
+template <class TV, class TM>
+struct DemagAdjoint {
+  bool ready = false;
+  DevBuf<TM> GvT;          // 3 planes: GvT_c(j, i) = Gv_c(i, j)
+  DevBuf<double> GvTsum;   // [3][N] row sums of GvT
+  DevBuf<TM> DivT;         // 3 planes: DivT_c(j, i) = Div(i, (j, c)); rows sum to zero
+  DevSell<double> PBI;     // boundary rows (bverts order) x interior columns of A
+  DevBuf<double> ABI;
+  DevBuf<double> part;     // dense B^T partial sums
+  DevBuf<TV> psi, bIbar, xIbar, gbar, yb, u1bar, bbar;
 };
 
 template <class TV, class TM>
@@ -168,6 +185,10 @@ struct DemagCtx {
   void potential(const TV* m, cudaStream_t s, bool sync_stats, int slot = -1);
   // H_demag = G phi / vol (AoS)
   void field(TV* H, cudaStream_t s);
+  // out (+)= D^T w for the linear map D: m -> H_demag (AoS, 3N); slot: adjoint RK stage (4-7)
+  // or -1.  The two Poisson solves are the forward ones (symmetric), with their own slots.
+  DemagAdjoint<TV, TM> adj;
+  void apply_transpose(const TV* w, TV* out, bool accumulate, int slot, cudaStream_t s);
   int64_t device_bytes() const;
 };
 

@@ -6,6 +6,11 @@
 // The npz file itself is written and read by the Python layer (numpy); this file moves the
 // arrays between the host and the device pools of an HMatrix.
 //
+// Transpose (HMatrix::transposed): B^T has the same cluster tree and the transposed block
+// partition.  A far block U V (U: m x k, V: k x n) becomes V^T U^T, whose "U^T" is V (k x n,
+// already stored) and whose "V" is U^T (k x m, already stored): the far pool is copied as is
+// and only the offsets swap.  Near tiles are transposed element by element.
+//
 // Import: the cluster tree is rebuilt from the boundary points (bit-exact), and the cached
 // permutation must equal it.  Far blocks keep their ranges; the near CSR is split into dense
 // leaf x leaf tiles (every tile row and column range is a leaf cluster), which is all the
@@ -192,6 +197,48 @@ void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec 
   H.stats.n_near = H.stats.dense_blocks;
   SPX_CUDA(cudaStreamSynchronize(s));
   H.pack(p, s);
+}
+
+HMatrix& HMatrix::transposed(cudaStream_t s) {
+  if (tr) return *tr;
+  SPX_CHECK(packed, "H-matrix is not packed");
+  auto T = std::make_unique<HMatrix>();
+  T->device = device;
+  T->Nb = Nb;
+  T->cfg = cfg;
+  T->stats = stats;
+  T->tree = tree;
+  T->perm.upload(tree.perm, s);
+  T->diag_perm.alloc(diag_perm.n);
+  if (diag_perm.n)
+    SPX_CUDA(cudaMemcpyAsync(T->diag_perm.p, diag_perm.p, diag_perm.bytes(), cudaMemcpyDeviceToDevice, s));
+  T->far_pool64.alloc(far_pool64.n);
+  if (far_pool64.n)
+    SPX_CUDA(cudaMemcpyAsync(T->far_pool64.p, far_pool64.p, far_pool64.bytes(), cudaMemcpyDeviceToDevice, s));
+  std::vector<double> near(near_pool64.n), neart(near_pool64.n, 0.0);
+  if (!near.empty()) {
+    SPX_CUDA(cudaMemcpyAsync(near.data(), near_pool64.p, near.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SPX_CUDA(cudaStreamSynchronize(s));
+  }
+  T->blocks.reserve(blocks.size());
+  for (const HBlock& b : blocks) {
+    HBlock t = b;
+    t.rs = b.cs; t.re = b.ce; t.cs = b.rs; t.ce = b.re;
+    if (b.type == 1) {
+      t.off_u = b.off_v;
+      t.off_v = b.off_u;
+    } else {
+      const int64_t m = b.re - b.rs, n = b.ce - b.cs;
+      for (int64_t i = 0; i < m; ++i)
+        for (int64_t j = 0; j < n; ++j) neart[b.off_u + j * m + i] = near[b.off_u + i * n + j];
+    }
+    T->blocks.push_back(t);
+  }
+  T->near_pool64.upload(neart, s);
+  SPX_CUDA(cudaStreamSynchronize(s));
+  T->pack(prec, s);
+  tr = std::move(T);
+  return *tr;
 }
 
 }  // namespace spx

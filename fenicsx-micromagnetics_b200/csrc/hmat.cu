@@ -600,6 +600,7 @@ void do_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS*
 }  // namespace
 
 void HMatrix::pack(Prec p, cudaStream_t s) {
+  tr.reset();
   prec = p;
   switch (p) {
     case Prec::F64: do_pack<double, double>(*this, s); break;

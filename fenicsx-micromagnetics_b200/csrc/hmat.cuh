@@ -1,6 +1,8 @@
 // H-matrix handle: construction (batched GPU fill + full-pivot ACA) and apply.
 #pragma once
 
+#include <memory>
+
 #include "spx_internal.cuh"
 
 namespace spx {
@@ -102,6 +104,7 @@ struct HMatrix {
   DevBuf<char> xperm;             // x in perm order (vector type)
   int64_t nseg = 0, zlen = 0, zpart_len = 0, n_far = 0, n_near = 0, nunits = 0, nwarps_z = 0;
   int64_t bytes_far = 0, bytes_near = 0;
+  std::unique_ptr<HMatrix> tr;    // H^T (same tree; built on first use by transposed())
 
   void build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s);
   void pack(Prec p, cudaStream_t s);
@@ -112,6 +115,9 @@ struct HMatrix {
   template <class T>
   void apply_gather(const T* src, const int32_t* gidx, T* dst, const T* add, T* yb, cudaStream_t s);
   int64_t device_bytes() const;
+  // H^T packed in the same precision: far blocks keep their factors with the roles of U^T and
+  // V exchanged, near tiles are transposed (hio.cu).  Built once, kept in `tr`.
+  HMatrix& transposed(cudaStream_t s);
 };
 
 // The reference's cache representation (hio.cu): near field as CSR in permutation space

@@ -21,30 +21,6 @@
 
 namespace spx {
 
-template <class TV, class TM>
-struct StageArgs {
-  int64_t n, nslices;
-  const int64_t* sp;
-  const int32_t* col;
-  int64_t L;
-  const TM* Kex;     // [L] exchange, row-scaled
-  const TM* Kd;      // [9L] DMI blocks, row-scaled (or null)
-  const double* Ksum;  // [9n] DMI row sums
-  const TM* Gv;      // [3L] G / vol (or null: no demag)
-  const TV* phi;     // potential (or null)
-  const TV* ani_n;   // [3n] unit axes (or null)
-  const TV* ani_p;   // [n] per-node prefactor 2Ku/(mu0 Ms) (or null)
-  TV ani_p0;         // scalar prefactor when ani_p == null
-  const TV* H0;      // [3n] (or null)
-  TV h0x, h0y, h0z;
-  const TV* m;       // stage input (AoS)
-  TV* out;           // mode 0: H ; mode 1: rhs ; mode 2: next stage m
-  TV* mn;            // RK state (mode 2)
-  TV* acc;           // RK accumulator (mode 2)
-  TV pref, alpha, precess, stab;
-  TV c_next, w_acc, dt6;
-  int mode, stage;
-};
 
 template <class TV, class TM, bool DMI, bool DEMAG, bool ANI>
 __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
@@ -358,6 +334,12 @@ void LLGCtx<TV, TM>::create(DemagCtx<TV, TM>* dm, const double* X, int64_t N_, c
     sell_values<TM>(*hs, b9.data(), 9, true, nnz, 1.0, v);
     Kd.upload(v, s);
     Ksum.upload(ks, s);
+  }
+  diag_lin_host = diag;
+  if (has_dmi) {
+    X_host.assign(X, X + 3 * N);
+    tets_host.assign(tets, tets + 4 * E);
+    n_int_host.assign(p.n_int, p.n_int + 3 * N);
   }
   has_ani = false;
   if (p.n_ani && (p.Ku != 0.0 || p.Ku_nodes)) {

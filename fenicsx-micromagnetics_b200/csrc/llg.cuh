@@ -18,7 +18,41 @@ struct LLGParams {
   int use_demag = 1;
 };
 
-template <class TV, class TM> struct StageArgs;
+// Arguments of the fused stage kernel k_stage (llg.cu)
+template <class TV, class TM>
+struct StageArgs {
+  int64_t n, nslices;
+  const int64_t* sp;
+  const int32_t* col;
+  int64_t L;
+  const TM* Kex;     // [L] exchange, row-scaled
+  const TM* Kd;      // [9L] DMI blocks, row-scaled (or null)
+  const double* Ksum;  // [9n] DMI row sums
+  const TM* Gv;      // [3L] G / vol (or null: no demag)
+  const TV* phi;     // potential (or null)
+  const TV* ani_n;   // [3n] unit axes (or null)
+  const TV* ani_p;   // [n] per-node prefactor 2Ku/(mu0 Ms) (or null)
+  TV ani_p0;         // scalar prefactor when ani_p == null
+  const TV* H0;      // [3n] (or null)
+  TV h0x, h0y, h0z;
+  const TV* m;       // stage input (AoS)
+  TV* out;           // mode 0: H ; mode 1: rhs ; mode 2: next stage m
+  TV* mn;            // RK state (mode 2)
+  TV* acc;           // RK accumulator (mode 2)
+  TV pref, alpha, precess, stab;
+  TV c_next, w_acc, dt6;
+  int mode, stage;
+};
+
+// Work data of the adjoint and tangent products (adjoint.cu), built on first use.
+template <class TV, class TM>
+struct LLGAdjoint {
+  bool ready = false;
+  DevBuf<TM> KexT, KdT;            // transposed exchange (1 plane) and DMI (9 planes)
+  DevBuf<double> KexTsum, KdTsum;  // their row sums
+  DevBuf<TV> Y[4], Hs[4], dY[2], u, w, a, ap, lam, acc, K, dK, dH;
+  DevBuf<double> part;
+};
 
 // TV: nodal vector type, TM: operator value type (see DemagCtx)
 template <class TV, class TM>
@@ -40,6 +74,10 @@ struct LLGCtx {
   DevBuf<double> red;
   int64_t steps = 0, rhs_evals = 0;
   mutable int64_t launches = 0;
+  std::vector<double> diag_lin_host;        // [3N] diagonal of exchange + DMI (no anisotropy)
+  std::vector<double> X_host, n_int_host;   // kept when DMI is on (adjoint set-up)
+  std::vector<int32_t> tets_host;
+  LLGAdjoint<TV, TM> adj;
 
   void create(DemagCtx<TV, TM>* dm, const double* X, int64_t N, const int32_t* tets, int64_t E,
               const LLGParams& p, cudaStream_t s);
@@ -52,6 +90,17 @@ struct LLGCtx {
   void jv(const TV* v, TV* out, cudaStream_t s);
   void pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s);
   void pc_apply(const TV* x, TV* y, cudaStream_t s);
+  // adjoint / tangent products (adjoint.cu).  gKu [N] and gH0 [3] are FP64 device
+  // accumulators (+=), either may be null.
+  void adjoint_setup(cudaStream_t s);
+  // out = J(m)^T w for the field H = H_eff(m) given; slot: CG slot of the demag solves
+  void rhs_vjp(const TV* m, const TV* H, const TV* w, TV* out, double* gKu, double* gH0, int slot, cudaStream_t s);
+  // lam_out = (d m_(n+1) / d m_n)^T lam_in for one RK4 step of size dt from mn
+  void step_vjp(const TV* mn, double dt, const TV* lam_in, TV* lam_out, double* gKu, double* gH0, cudaStream_t s);
+  // one RK4 step of the primal and of the tangent: m_out = step(mn), dm_out = d step . (dm, dKu, dH0)
+  void step_jvp(const TV* mn, const TV* dm, const double* dKu, const double dH0[3], double dt, TV* m_out, TV* dm_out,
+                cudaStream_t s);
+  void set_ku_map(const double* Ku_nodes, cudaStream_t s);
 };
 
 template <class A, class B>

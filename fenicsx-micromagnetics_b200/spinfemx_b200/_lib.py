@@ -62,11 +62,13 @@ SIGNATURES = {
     "spx_hmat_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_repack": (C.c_int, [c_vp, c_i32]),
     "spx_hmat_apply_noalloc": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_hmat_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_far_factors": (C.c_int, [c_vp, c_i64, c_vp, c_vp]),
     "spx_hmat_memory": (C.c_int, [c_vp, P_i64, P_i64, P_i64]),
     "spx_hmat_destroy": (C.c_int, [c_vp]),
     "spx_demag_create": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), C.POINTER(c_vp)]),
     "spx_demag_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_demag_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_demag_potentials": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_demag_energy": (C.c_int, [c_vp, c_vp, c_vp, P_dbl, c_vp]),
     "spx_demag_stats": (C.c_int, [c_vp, P_i64, P_i64, P_dbl, P_dbl]),
@@ -96,6 +98,10 @@ SIGNATURES = {
     "spx_llg_set_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_get_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_step": (C.c_int, [c_vp, c_dbl, c_i64, c_vp]),
+    "spx_llg_set_anisotropy_map": (C.c_int, [c_vp, c_vp]),
+    "spx_llg_rhs_vjp": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_step_vjp": (C.c_int, [c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_step_jvp": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp]),
     "spx_llg_run_host": (C.c_int, [c_vp, c_vp, c_vp, c_dbl, c_i64]),
     "spx_llg_set_uniform_field": (C.c_int, [c_vp, c_dbl, c_dbl, c_dbl]),
     "spx_llg_stats": (C.c_int, [c_vp, P_i64, P_i64, P_i64]),

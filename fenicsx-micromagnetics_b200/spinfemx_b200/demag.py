@@ -162,6 +162,15 @@ class DemagFieldLindholmGPU:
         self.last_res_u1, self.last_res_u2 = r1.value, r2.value
         return out_vec
 
+    def compute_vec_transpose(self, w_vec, out_vec):
+        """out = D^T w for the linear map D: m -> H_demag (adjoint of compute_vec)."""
+        self._check(w_vec, "w_vec")
+        self._check(out_vec, "out_vec")
+        call("spx_demag_apply_transpose", self._h, ptr(w_vec), ptr(out_vec), _lib.stream_ptr())
+        if out_vec.numel() > self.local_size:
+            out_vec[self.local_size:] = 0.0
+        return out_vec
+
     def potentials(self):
         import torch
         u1 = torch.empty(self.N, dtype=torch.float64, device="cuda")

@@ -195,6 +195,17 @@ class HMatrixGPUPackedFused:
         call("spx_hmat_apply", self._h, ptr(x), ptr(out), _lib.stream_ptr())
         return out
 
+    def rmatvec(self, x_gpu, out=None):
+        """y = H^T x (transposed apply; the transposed H-matrix is packed on the first call)."""
+        import torch
+        if x_gpu.dtype != torch.float64 or not x_gpu.is_cuda:
+            raise TypeError("rmatvec expects a CUDA float64 tensor")
+        x = x_gpu.contiguous()
+        if out is None:
+            out = torch.empty_like(x)
+        call("spx_hmat_apply_transpose", self._h, ptr(x), ptr(out), _lib.stream_ptr())
+        return out
+
     def matvec_noalloc(self, x_gpu, out):
         """y = H x through spx_hmat_apply_noalloc: no device allocation inside the call
         (the scratch is the library's fixed 32 MiB device array, shared by every call, so

@@ -187,6 +187,41 @@ class EffectiveField:
         call("spx_llg_run_host", self._h, ptr(m_host), ptr(out), float(dt), int(nsteps))
         return out
 
+    # -------------------------------------------------------------- gradients
+    # Adjoint / tangent products (not in the reference).  gKu (N) and gH0 (3) are CUDA float64
+    # accumulators that the calls add to.
+    def set_anisotropy_map(self, Ku_nodes):
+        """Replace the nodal Ku map (J/m^3); the anisotropy axis must have been given."""
+        ku = np.ascontiguousarray(np.asarray(Ku_nodes, dtype=np.float64).reshape(-1))
+        if ku.size != self.N:
+            raise ValueError("Ku_nodes must have N entries")
+        call("spx_llg_set_anisotropy_map", self._h, ptr(ku))
+
+    def rhs_vjp(self, m_vec, w_vec, out_vec, gKu=None, gH0=None):
+        """out = J(m)^T w, J the Jacobian of llg_rhs_vec at m (demag included)."""
+        for v, n in ((m_vec, "m_vec"), (w_vec, "w_vec"), (out_vec, "out_vec")):
+            self._chk(v, n)
+        call("spx_llg_rhs_vjp", self._h, ptr(m_vec), ptr(w_vec), ptr(out_vec), ptr(gKu), ptr(gH0),
+             _lib.stream_ptr())
+        return out_vec
+
+    def step_vjp(self, m_n, dt, lam_in, lam_out, gKu=None, gH0=None):
+        """lam_out = (d m_(n+1) / d m_n)^T lam_in for one RK4 step from m_n."""
+        for v, n in ((m_n, "m_n"), (lam_in, "lam_in"), (lam_out, "lam_out")):
+            self._chk(v, n)
+        call("spx_llg_step_vjp", self._h, ptr(m_n), float(dt), ptr(lam_in), ptr(lam_out), ptr(gKu), ptr(gH0),
+             _lib.stream_ptr())
+        return lam_out
+
+    def step_jvp(self, m_n, dm, dt, m_out, dm_out, dKu=None, dH0=None):
+        """One RK4 step of the state and its tangent along (dm, dKu, dH0)."""
+        for v, n in ((m_n, "m_n"), (dm, "dm"), (m_out, "m_out"), (dm_out, "dm_out")):
+            self._chk(v, n)
+        h0 = None if dH0 is None else np.ascontiguousarray(np.asarray(dH0, dtype=np.float64).reshape(3))
+        call("spx_llg_step_jvp", self._h, ptr(m_n), ptr(dm), ptr(dKu), ptr(h0), float(dt), ptr(m_out),
+             ptr(dm_out), _lib.stream_ptr())
+        return m_out, dm_out
+
     def stats(self):
         s, r, l = _lib.c_i64(), _lib.c_i64(), _lib.c_i64()
         call("spx_llg_stats", self._h, C.byref(s), C.byref(r), C.byref(l))

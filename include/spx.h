@@ -128,6 +128,12 @@ SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
  * zero), so calls that overlap on the GPU (other streams, other threads) race; serialise
  * them.  x, y: FP64 device vectors of length Nb. */
 SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_stream_t s);
+/* y = H^T x (original boundary ordering, FP64 device vectors of length Nb).  No counterpart
+ * in the reference (its H-matrix backends apply H only); the adjoint of the demag operator
+ * needs it.  The transposed H-matrix (same cluster tree, transposed partition, far factors
+ * shared with U^T and V exchanged, near tiles transposed) is packed in the same precision on
+ * the first call and kept with the handle; spx_hmat_repack drops it. */
+SPX_API int spx_hmat_apply_transpose(spx_hmat h, const double* x, double* y, spx_stream_t s);
 /* low-rank factors U^T (k x m) and V (k x n) of far block `index` (as listed by spx_hmat_blocks), FP64 host */
 SPX_API int spx_hmat_far_factors(spx_hmat h, int64_t index, double* Ut, double* V);
 SPX_API int spx_hmat_memory(spx_hmat h, int64_t* far_bytes, int64_t* near_bytes, int64_t* total_bytes);
@@ -174,6 +180,13 @@ SPX_API int spx_demag_create(const double* X, int64_t N, const int32_t* tets, in
 SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                        const spx_demag_options* opt, spx_hmat h, spx_demag* out);
 SPX_API int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s);
+/* out = D^T w for the linear demag map D: m -> H of spx_demag_apply (AoS FP64 device,
+ * length 3N).  No counterpart in the reference.  Evaluated as
+ * Div^T Pi A^+ Pi (psi + E^T B^T (psi_B - A_BI A_II^-1 psi_I)) with psi = (G/V)^T w: the
+ * same two CG solves as the forward map (symmetric systems) and B^T (transposed dense GEMV
+ * or spx_hmat_apply_transpose's operator); the transposed value planes are built on the
+ * first call. */
+SPX_API int spx_demag_apply_transpose(spx_demag d, const double* w, double* out, spx_stream_t s);
 /* potentials of the last apply (FP64 device, N each) */
 SPX_API int spx_demag_potentials(spx_demag d, double* u1, double* u2, spx_stream_t s);
 /* Energy_lumped_gpu (:706-724): E = -1/2 mu0 Ms sum V_i m.H / 1e27  (J) */
@@ -221,6 +234,26 @@ SPX_API int spx_llg_step(spx_llg l, double dt, int64_t nsteps, spx_stream_t s);
 SPX_API int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, int64_t nsteps);
 /* EffectiveField.set_uniform_field (llg_module_GPU.py:897-904): replace the static field by a uniform one */
 SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz);
+/* Adjoint and tangent products (no counterpart in the reference, which has no gradients).
+ * Vectors are FP64 device AoS of length 3N.  gKu (length N) and gH0 (length 3) are FP64
+ * device accumulators: the call ADDS dL/dKu_i (J/m^3, per node) and dL/dH0 (A/m, uniform
+ * applied field) to them; either may be NULL.  gKu needs an anisotropy axis given at
+ * creation.
+ *   spx_llg_set_anisotropy_map: replace the nodal Ku map (host, N values, J/m^3).
+ *   spx_llg_rhs_vjp:  mbar = J(m)^T w, J the Jacobian of llg_rhs_vec (demag included).
+ *   spx_llg_step_vjp: lam_out = (d m_{n+1}/d m_n)^T lam_in for one classic RK4 step of
+ *                     size dt from m_n (the four stages are recomputed); lam_out may be
+ *                     lam_in.
+ *   spx_llg_step_jvp: one RK4 step of the state and of its tangent: m_out = step(m_n),
+ *                     dm_out = d step . (dm, dKu, dH0); dKu: device N or NULL, dH0: host 3
+ *                     or NULL. */
+SPX_API int spx_llg_set_anisotropy_map(spx_llg l, const double* Ku_nodes);
+SPX_API int spx_llg_rhs_vjp(spx_llg l, const double* m, const double* w, double* mbar, double* gKu, double* gH0,
+                            spx_stream_t s);
+SPX_API int spx_llg_step_vjp(spx_llg l, const double* m_n, double dt, const double* lam_in, double* lam_out,
+                             double* gKu, double* gH0, spx_stream_t s);
+SPX_API int spx_llg_step_jvp(spx_llg l, const double* m_n, const double* dm, const double* dKu, const double* dH0,
+                             double dt, double* m_out, double* dm_out, spx_stream_t s);
 /* CUDA-event timing of the pipeline by kernel group, recorded on the launching stream
  * between begin and end.  ms[8] / kernel launches[8] / group executions[8] per group: 0 Div SpMV, 1 u1 solve,
  * 2 boundary operator (gather + far + rows, or dense GEMV), 3 u2 right-hand side,
