@@ -430,8 +430,10 @@ void DemagCtx<TV, TM>::apply_transpose(const TV* w, TV* out, bool accumulate, in
     SPX_CUDA(cudaStreamSynchronize(s));
     A.ready = true;
   }
-  const bool warm = opt.warm_start != 0;
-  const int sl = (opt.warm_start >= 2) ? slot : -1;
+  // adjoint solves start from the extrapolation of earlier adjoint solutions of the same RK
+  // stage (slots 4-7) when warm starts are on, from zero otherwise
+  const int sl = (opt.warm_start != 0 && slot >= 0) ? slot : -1;
+  const bool warm = sl >= 0;
   const unsigned gs = grid_for(P.nslices * 32, 256);
   // psi = Gv^T w
   k_planes3_to1<TV, TM><<<gs, 256, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, A.GvT.p, P.len, A.GvTsum.p, w,
@@ -441,7 +443,7 @@ void DemagCtx<TV, TM>::apply_transpose(const TV* w, TV* out, bool accumulate, in
   if (NI > 0) {
     k_gather<TV><<<grid_for(NI, 256), 256, 0, s>>>(NI, interior.p, A.psi.p, A.bIbar.p);
     SPX_LAUNCH_CHECK();
-    cg2.template solve<TV>(A.bIbar.p, A.xIbar.p, opt.rtol_u2, opt.atol, opt.maxit_u2, warm, false, sl, s, false);
+    cg2.template solve<TV>(A.bIbar.p, A.xIbar.p, opt.rtol_u2, opt.atol, opt.maxit_u2, warm, false, sl, s, false, 1);
     k_bnd_adj<TV><<<grid_for(A.PBI.nslices * 32, 256), 256, 0, s>>>(Nb, A.PBI.nslices, A.PBI.slice_ptr.p,
                                                                      A.PBI.col.p, A.ABI.p, A.xIbar.p, A.psi.p,
                                                                      bverts.p, A.gbar.p);
@@ -466,7 +468,7 @@ void DemagCtx<TV, TM>::apply_transpose(const TV* w, TV* out, bool accumulate, in
   SPX_CUDA(cudaMemcpyAsync(A.u1bar.p, A.psi.p, N * sizeof(TV), cudaMemcpyDeviceToDevice, s));
   k_scatter_add<TV><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, bverts.p, A.yb.p, A.u1bar.p);
   SPX_LAUNCH_CHECK();
-  cg1.template solve<TV>(A.u1bar.p, A.bbar.p, opt.rtol_u1, opt.atol, opt.maxit_u1, warm, true, sl, s, false);
+  cg1.template solve<TV>(A.u1bar.p, A.bbar.p, opt.rtol_u1, opt.atol, opt.maxit_u1, warm, true, sl, s, false, 1);
   k_planes1_to3<TV, TM><<<gs, 256, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, A.DivT.p, P.len, A.bbar.p, out,
                                             accumulate ? 1 : 0);
   SPX_LAUNCH_CHECK();

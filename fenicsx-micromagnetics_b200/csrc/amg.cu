@@ -460,6 +460,11 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
   }
   cta_total(P.part, 1, tot, sh);
   const double bb = tot[0];
+  if (P.warm && !(bb > 0.0)) {  // b = 0: the solution is 0
+    PCG_ROWS_BEGIN P.y[row] = 0.0;
+    PCG_ROWS_END
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
   const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
   int total = 0, outers = 0;
   double rr = 0.0, rr0 = -1.0;

@@ -229,7 +229,13 @@ __global__ void __launch_bounds__(CG_BLOCK, 1) k_cg(CgParams P) {
   }
   cta_total(P.part, 1, tot, sh);
   const double bb = tot[0];
-  if (P.warm) {
+  // b = 0: the solution is 0 (a warm start would only iterate on rounding noise)
+  const bool warm = P.warm && bb > 0.0;
+  if (P.warm && !warm) {
+    CG_ROWS_BEGIN P.y[row] = 0.0;
+    CG_ROWS_END
+  }
+  if (warm) {
     CG_ROWS_BEGIN P.r[row] -= spmv64(P, base, width, lane, P.y);
     CG_ROWS_END
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
@@ -383,6 +389,11 @@ __global__ void __launch_bounds__(CG_BLOCK, 1) k_cg_ir(CgIrParams<TV> P) {
   }
   cta_total(P.part, 1, tot, sh);
   const double bb = tot[0];
+  if (P.warm && !(bb > 0.0)) {  // b = 0: the solution is 0
+    CG_ROWS_BEGIN P.y[row] = 0.0;
+    CG_ROWS_END
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
   const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
   int total = 0, outers = 0;
   double rho = 0.0, rho0 = -1.0;
@@ -565,7 +576,10 @@ void CgSystem<TM>::setup(const HostSell& s, const std::vector<double>& vals_sell
 template <class TM>
 template <class TV>
 CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project,
-                            int slot, cudaStream_t st, bool sync_stats) {
+                            int slot, cudaStream_t st, bool sync_stats, int kind) {
+  if (kind < 0) kind = slot < 4 ? 0 : (slot < 8 ? 1 : 2);
+  if (kind != last_kind) warm = false;
+  last_kind = kind;
   const bool use_amg = static_cast<bool>(amg);
   const bool ir = sizeof(TM) == sizeof(float) || use_amg;  // solution state kept in y64
   SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
@@ -660,11 +674,11 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
 template struct CgSystem<double>;
 template struct CgSystem<float>;
 template CgStats CgSystem<double>::solve<double>(const double*, double*, double, double, int, bool, bool, int,
-                                                 cudaStream_t, bool);
+                                                 cudaStream_t, bool, int);
 template CgStats CgSystem<float>::solve<double>(const double*, double*, double, double, int, bool, bool, int,
-                                                cudaStream_t, bool);
+                                                cudaStream_t, bool, int);
 template CgStats CgSystem<float>::solve<float>(const float*, float*, double, double, int, bool, bool, int,
-                                               cudaStream_t, bool);
+                                               cudaStream_t, bool, int);
 
 // ------------------------------------------------------------------ demag context
 template <class TV, class TM>
@@ -767,6 +781,7 @@ void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, i
   const int threads = 256;
   const bool warm = opt.warm_start != 0;
   const int sl = (opt.warm_start >= 2) ? slot : -1;
+  const int kind = slot < 4 ? 0 : (slot < 8 ? 1 : 2);  // forward (slot -1 included), adjoint, tangent
   prof.mark(PC_DIV, s);
   k_div<TV, TM><<<grid_for(P.nslices * 32, threads), threads, 0, s>>>(N, P.nslices, P.slice_ptr.p, P.col.p, Div.p,
                                                                      P.len, Dsum.p, m, b.p);
@@ -774,7 +789,7 @@ void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, i
   prof.mark(PC_DIV, s);
   prof.launches[PC_DIV] += 1;
   prof.mark(PC_CG1, s);
-  last1 = cg1.template solve<TV>(b.p, u1.p, opt.rtol_u1, opt.atol, opt.maxit_u1, warm, true, sl, s, sync_stats);
+  last1 = cg1.template solve<TV>(b.p, u1.p, opt.rtol_u1, opt.atol, opt.maxit_u1, warm, true, sl, s, sync_stats, kind);
   prof.mark(PC_CG1, s);
   prof.launches[PC_CG1] += 1 + (sl >= 0 && cg1.hcount[sl] > 1 ? 1 : 0);
   prof.mark(PC_BND, s);
@@ -800,7 +815,7 @@ void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, i
     // the interior test is slightly stricter, which only tightens the solve.
     prof.mark(PC_CG2, s);
     last2 = cg2.template solve<TV>(bI.p, xI.p, opt.rtol_u2, opt.atol, opt.maxit_u2, warm, false, sl, s,
-                                   sync_stats);
+                                   sync_stats, kind);
     prof.mark(PC_CG2, s);
     prof.launches[PC_CG2] += 1 + (sl >= 0 && cg2.hcount[sl] > 1 ? 1 : 0);
     prof.mark(PC_PHI, s);

@@ -100,6 +100,10 @@ struct CgSystem {
   int hcount[CG_SLOTS] = {}, hhead[CG_SLOTS] = {};
   // stage correction: slots 1..3 add slot 0's last prediction error (solution - guess)
   bool stage_correct = false, have_pred0 = false, have_delta = false;
+  // kind of the last solve (0 forward, 1 adjoint, 2 tangent): a warm start from the solver
+  // state (y64 or x) is taken only from a solve of the same kind, whose right-hand sides
+  // have the same scale; otherwise the solve starts from zero
+  int last_kind = 0;
   DevBuf<double> pred0, delta;
   double inner_rtol = 1e-3;
   int max_outer = 10;
@@ -118,9 +122,10 @@ struct CgSystem {
                   const std::vector<double>& d, bool singular, cudaStream_t s);
   template <class TV>
   void launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, cudaStream_t st);
+  // kind: 0 forward, 1 adjoint, 2 tangent; -1 derives it from the slot (0-3, 4-7, 8-11)
   template <class TV>
   CgStats solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, int slot,
-                cudaStream_t st, bool sync_stats);
+                cudaStream_t st, bool sync_stats, int kind = -1);
   void reset_history() {
     for (int s = 0; s < CG_SLOTS; ++s) hcount[s] = hhead[s] = 0;
     have_pred0 = have_delta = false;

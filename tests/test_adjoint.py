@@ -153,10 +153,11 @@ def test_hmat_transpose_apply(spx, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("backend", ["dense", "hmatrix"])
-def test_demag_transpose_vs_oracle(spx, prob, backend):
+@pytest.mark.parametrize("backend,warm_start", [("dense", False), ("hmatrix", False),
+                                                ("dense", "extrapolate_corrected")])
+def test_demag_transpose_vs_oracle(spx, prob, backend, warm_start):
     D = prob["D"]
-    kw = dict(boundary_backend=backend, precision="f64", **TIGHT)
+    kw = dict(boundary_backend=backend, precision="f64", warm_start=warm_start, **TIGHT)
     if backend == "hmatrix":
         kw.update(hmatrix_epsilon=1e-8, hmatrix_leaf_size=8)
     d = spx.DemagFieldLindholmGPU(prob["X"], prob["T"], prob["kw"]["Ms"], **kw)
@@ -169,6 +170,8 @@ def test_demag_transpose_vs_oracle(spx, prob, backend):
     assert rel(g, oadj.demag_transpose(D, w)) < (1e-9 if backend == "dense" else 1e-6)
     Hv = torch.empty_like(out)
     d.compute_vec(_t(v), Hv)
+    d.compute_vec_transpose(_t(w), out)  # after a forward solve of another scale
+    assert rel(out.cpu().numpy(), g) < 1e-9
     lhs = w @ Hv.cpu().numpy()
     assert abs(lhs - g @ v) <= 1e-9 * abs(lhs)
 
@@ -215,16 +218,21 @@ def test_step_vjp_and_jvp_vs_oracle(spx, prob):
 
 
 @pytest.mark.gpu
-def test_trajectory_gradient_vs_oracle_fd_and_tangent(spx, prob):
+@pytest.mark.parametrize("warm_start,precision", [(False, "f64"), ("extrapolate_corrected", "f64"),
+                                                  ("extrapolate_corrected", "mixed")])
+def test_trajectory_gradient_vs_oracle_fd_and_tangent(spx, prob, warm_start, precision):
     """Gradients of ||m(T) - m_target||^2 through the autograd Function (checkpoints every 3 of
     8 steps) against central finite differences of the FP64 oracle (h = 1e-4 relative),
-    and against the CUDA tangent."""
+    and against the CUDA tangent.  Warm-started solves keep separate states for the forward,
+    adjoint and tangent solves (their right-hand sides differ in scale by many orders)."""
     F, m0, N = prob["F"], prob["m"], prob["N"]
     nsteps, dt = 8, 2e-14
     L, _ = _loss_and_target(prob, nsteps, dt)
     mt = oadj.trajectory(F, _unit(np.random.default_rng(99), N), dt, nsteps)[-1]
     Ku0, H00 = prob["Ku"].copy(), prob["H0"].copy()
-    hef = _gpu_field(spx, prob)
+    tight = precision == "f64"
+    hef = _gpu_field(spx, prob, warm_start=warm_start, precision=precision,
+                     **({} if tight else dict(ksp_rtol_u1=1e-11, ksp_rtol_u2=1e-11)))
     m0t = _t(m0).requires_grad_(True)
     Kut = _t(Ku0).requires_grad_(True)
     H0t = _t(H00).requires_grad_(True)
@@ -232,7 +240,7 @@ def test_trajectory_gradient_vs_oracle_fd_and_tangent(spx, prob):
     loss = torch.sum((mT - _t(mt)) ** 2)
     loss.backward()
     oadj.set_params(F, Ku0, H00)
-    assert abs(loss.item() - L(oadj.trajectory(F, m0, dt, nsteps)[-1])) <= 1e-9 * loss.item()
+    assert abs(loss.item() - L(oadj.trajectory(F, m0, dt, nsteps)[-1])) <= (1e-9 if tight else 1e-6) * loss.item()
     rng = np.random.default_rng(8)
     dirs = {"Ku": rng.normal(size=N) * Ku0, "H0": rng.normal(size=3) * 1e4, "m0": rng.normal(size=3 * N)}
     grads = {"Ku": Kut.grad.cpu().numpy(), "H0": H0t.grad.cpu().numpy(), "m0": m0t.grad.cpu().numpy()}
@@ -257,4 +265,4 @@ def test_trajectory_gradient_vs_oracle_fd_and_tangent(spx, prob):
         kw = {"Ku": dict(dKu=d), "H0": dict(dH0=d), "m0": dict(dm0=d)}[name]
         mT2, dmT = spx.trajectory_tangent(hef, m0, dt, nsteps, Ku=Ku0, H0=H00, **kw)
         tan = float(torch.sum(2.0 * (mT2 - _t(mt)) * dmT).item())
-        assert abs(tan - g) <= 1e-8 * abs(g), (name, tan, g)
+        assert abs(tan - g) <= (1e-8 if tight else 1e-6) * abs(g), (name, tan, g)
