@@ -462,6 +462,117 @@ def run_adjoint(a):
     finish(ws)
 
 
+def ensemble_boxes(n, seed):
+    """BASELINE config 4 shapes: lateral sides U[20, 120] nm and thickness in {4, 6, 8, 10} nm,
+    snapped to 2 nm cubes (Kuhn split)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = (int(round(rng.uniform(20.0, 120.0) / 2.0)) for _ in range(2))
+        nz = int(rng.choice([4, 6, 8, 10])) // 2
+        out.append((max(nx, 1), max(ny, 1), nz))
+    return out
+
+
+def run_ensemble(a):
+    """Sample-steps/s of a batched ensemble of independent boxes."""
+    import torch
+    import spinfemx_b200 as spx
+    rank, ws, local = dist_init(a.gpus)
+    boxes = ensemble_boxes(a.samples, 7000 + rank)
+    meshes = [spx.kuhn_box(nx, ny, nz, 2.0) for nx, ny, nz in boxes]
+    rng = np.random.default_rng(7100 + rank)
+    Bz = rng.uniform(-0.5, 0.5, size=len(meshes))
+    m0 = []
+    for X, _ in meshes:
+        m = rng.normal(size=(X.shape[0], 3))
+        m0.append((m / np.linalg.norm(m, axis=1)[:, None]).ravel())
+    mat = dict(Aex=1.6e-11, Ku=8e5, D_int=3e-3, alpha=0.3)
+    dk = dict(hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64, ksp_rtol_u1=a.rtol_u1,
+              ksp_rtol_u2=a.rtol_u2, warm_start={0: False, 1: True, 2: "extrapolate", 3: "extrapolate_corrected"}[
+                  a.warm_start])
+    t0 = time.time()
+    ens = spx.LLGEnsemble(meshes, 1.1e6, H0=[[0.0, 0.0, b / MU0] for b in Bz], dense_max_nb=4096,
+                          precision=a.precision, demag_kwargs=dk, **mat)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    dm = ens.hef.demag_field
+    dt = 20e-15
+    ens.set_state(m0)
+    ens.step(dt, a.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    barrier(ws)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.step(dt, a.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = allmax(e0.elapsed_time(e1), ws)
+    clocks = sampler.stop() if sampler else None
+    st = ens.hef.stats()
+    # the same samples one by one (separate field objects, same options), a few of them timed
+    seq = None
+    if a.ens_compare and rank == 0:
+        per = []
+        nchk = min(a.ens_compare, len(meshes))
+        idx = np.linspace(0, len(meshes) - 1, nchk).astype(int)
+        for k in idx:
+            X, T = meshes[k]
+            kw = dict(dk, boundary_backend="dense" if dm_nb(spx, X, T) <= 4096 else "hmatrix", precision=a.precision)
+            hef = spx.EffectiveField(X, T, 1.1e6, n_ani_vec=[0.0, 0.0, 1.0], n0_int_vec=[0.0, 0.0, 1.0],
+                                     H0_static=[0.0, 0.0, Bz[k] / MU0], use_demag=True, demag_kwargs=kw, **mat)
+            hef.set_state(torch.as_tensor(m0[k], device="cuda"))
+            hef.step(dt, a.warmup)
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record()
+            hef.step(dt, a.steps)
+            f1.record()
+            torch.cuda.synchronize()
+            per.append((int(k), f0.elapsed_time(f1) / a.steps, int(X.shape[0])))
+        # sequential time for all samples: per-node cost interpolated from the timed samples
+        tn = np.array([p[1] for p in per])
+        nn = np.array([p[2] for p in per], dtype=np.float64)
+        coef = np.polyfit(nn, tn, 1) if len(per) > 1 else np.array([0.0, tn[0]])
+        est = float(sum(max(np.polyval(coef, X.shape[0]), tn.min()) for X, _ in meshes))
+        seq = {"timed_samples": [{"sample": p[0], "nodes": p[2], "ms_per_step": round(p[1], 4)} for p in per],
+               "est_ms_per_ensemble_step": round(est, 3),
+               "est_sample_steps_per_s": round(len(meshes) * 1e3 / est, 1)}
+    if rank != 0:
+        finish(ws)
+        return
+    nodes = int(ens.N)
+    blk = {"dense": int(sum(1 for X, T in meshes if dm_nb(spx, X, T) <= 4096))}
+    blk["hmatrix"] = len(meshes) - blk["dense"]
+    line = {
+        "metric": "ensemble sample-steps/s: 64 independent boxes (BASELINE config 4 shapes), one launch per phase",
+        "value": round(ws * len(meshes) * a.steps / (ms * 1e-3), 2), "unit": "sample-steps/s", "n_gpus": ws,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp64 vectors / fp32 operators"}[a.precision],
+        "data": "synthetic (seeded box sizes, fields and magnetisations)",
+        "config": {"workload": f"{len(meshes)} boxes, sides U[20,120] nm, thickness {{4,6,8,10}} nm @2 nm, "
+                               f"{nodes} nodes in total, Ms 1.1e6, A 1.6e-11, Ku 8e5 z, D_int 3e-3, alpha 0.3, "
+                               f"Bz U[-0.5,0.5] T, RK4 dt 20 fs",
+                   "nodes": nodes, "boundary_nodes": int(dm.Nb), "boundary_blocks": blk,
+                   "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2, "parallelism": f"samples sharded, {ws} rank(s)"},
+        "launches_per_step": round(st["launches"] / max(st["steps"], 1), 1),
+        "unbatched": seq,
+        "setup_s": round(setup_s, 1),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    finish(ws)
+
+
+def dm_nb(spx, X, T):
+    return int(spx.boundary_data(X, T)["bverts"].shape[0])
+
+
 def counters(dm):
     from spinfemx_b200 import _lib
     c1 = np.zeros(4, np.int64)
@@ -628,7 +739,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--traffic", type=json.loads, default=None,
                     help='per-group DRAM bytes per launch from an ncu capture, e.g. {"u1_solve": 1.2e9}')
-    ap.add_argument("--workload", default="film", choices=["film", "adjoint"],
+    ap.add_argument("--samples", type=int, default=64)
+    ap.add_argument("--ens-compare", type=int, default=6, help="ensemble: samples also timed one by one")
+    ap.add_argument("--workload", default="film", choices=["film", "adjoint", "ensemble"],
                     help="film: LLG steps/s on the 0.48M-node film (the headline); adjoint: trajectory gradient "
                          "on the 100x100x2 film")
     ap.add_argument("--adj-steps", type=int, default=400)
@@ -641,6 +754,8 @@ def main():
         run_reference(a)
     elif a.workload == "adjoint":
         run_adjoint(a)
+    elif a.workload == "ensemble":
+        run_ensemble(a)
     else:
         run_ours(a)
 

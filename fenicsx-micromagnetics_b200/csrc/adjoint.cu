@@ -389,6 +389,7 @@ template <class TV, class TM>
 void DemagCtx<TV, TM>::apply_transpose(const TV* w, TV* out, bool accumulate, int slot, cudaStream_t s) {
   DemagAdjoint<TV, TM>& A = adj;
   const int64_t nnz = fem.rowptr[N];
+  SPX_CHECK(opt.backend != 2, "the ensemble backend has no transposed boundary operator");
   if (!A.ready) {
     const std::vector<int64_t> tp = transpose_positions(fem.rowptr, fem.col);
     std::vector<double> gt(3 * nnz), dt(3 * nnz), gsum(3 * N, 0.0);

@@ -370,6 +370,7 @@ struct PcgParams {
   double* res_acc;
   double rtol, atol, ww;
   int maxit, max_outer, warm, project;
+  int bh_given;  // bh already holds the scaled, projected right-hand side (FP64)
   const AmgLevelDev* lv;
   int nlev;
   const float* cinv;
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
   const float* dinv0 = P.lv[0].dinv;
   double tot[4];
   double meanb = 0.0;
-  if (P.project) {
+  if (P.project && !P.bh_given) {
     double part = 0.0;
     PCG_ROWS_BEGIN part += static_cast<double>(P.b[row]);
     PCG_ROWS_END
@@ -450,8 +451,13 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
   {
     double bb = 0.0;
     PCG_ROWS_BEGIN
-      const double bv = static_cast<double>(P.b[row]) - meanb;
-      P.bh[row] = bv * P.sdinv[row];
+      double bv;
+      if (P.bh_given) {
+        bv = P.bh[row] / P.sdinv[row];
+      } else {
+        bv = static_cast<double>(P.b[row]) - meanb;
+        P.bh[row] = bv * P.sdinv[row];
+      }
       if (!P.warm) P.y[row] = 0.0;
       bb += bv * bv;
     PCG_ROWS_END
@@ -665,7 +671,7 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
 template <class TM>
 template <class TV>
 void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project,
-                              cudaStream_t st) {
+                              cudaStream_t st, bool bh_given) {
   PcgParams<TV> q;
   q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
   q.v64 = vals64.p; q.a32 = amg_a32.p; q.rsum = amg_rsum.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
@@ -676,6 +682,7 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   q.iters_acc = iters_acc.p; q.res_acc = res_acc.p;
   q.rtol = rtol; q.atol = atol; q.ww = amg_singular ? amg_ww : 0.0;
   q.maxit = maxit; q.max_outer = max_outer; q.warm = warm ? 1 : 0; q.project = project ? 1 : 0;
+  q.bh_given = bh_given ? 1 : 0;
   q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc; q.ldc = amg->ldc;
   void* args[] = {&q};
   SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_pcg_amg<TV>), dim3(amg_grid), dim3(PCG_BLOCK),
@@ -689,10 +696,10 @@ template void CgSystem<float>::enable_amg(const HostSell&, const std::vector<int
                                           const std::vector<double>&, const std::vector<double>&, bool,
                                           cudaStream_t);
 template void CgSystem<double>::launch_amg<double>(const double*, double*, double, double, int, bool, bool,
-                                                   cudaStream_t);
+                                                   cudaStream_t, bool);
 template void CgSystem<float>::launch_amg<double>(const double*, double*, double, double, int, bool, bool,
-                                                  cudaStream_t);
+                                                  cudaStream_t, bool);
 template void CgSystem<float>::launch_amg<float>(const float*, float*, double, double, int, bool, bool,
-                                                 cudaStream_t);
+                                                 cudaStream_t, bool);
 
 }  // namespace spx

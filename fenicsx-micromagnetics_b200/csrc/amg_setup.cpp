@@ -252,11 +252,32 @@ void amg_build(const CsrHost& A0, const std::vector<double>& null0, bool singula
       if (C.ci[k] == i) dsum += C.v[k];
     }
   if (singular) {
-    double ww = 0.0;
-    for (int64_t i = 0; i < nc; ++i) ww += w[i] * w[i];
-    const double tau = dsum / static_cast<double>(nc) / std::max(ww, 1e-300);
+    // one null vector per connected component of the coarse graph (a disjoint union of
+    // meshes, e.g. an ensemble of independent samples, has one constant per sample): add
+    // tau w_c w_c^T for each component c
+    std::vector<int64_t> comp(nc, -1), stack;
+    int64_t ncomp = 0;
+    for (int64_t r = 0; r < nc; ++r) {
+      if (comp[r] >= 0) continue;
+      comp[r] = ncomp;
+      stack.assign(1, r);
+      while (!stack.empty()) {
+        const int64_t i = stack.back();
+        stack.pop_back();
+        for (int64_t k = C.rp[i]; k < C.rp[i + 1]; ++k)
+          if (C.v[k] != 0.0 && comp[C.ci[k]] < 0) {
+            comp[C.ci[k]] = ncomp;
+            stack.push_back(C.ci[k]);
+          }
+      }
+      ++ncomp;
+    }
+    std::vector<double> ww(ncomp, 0.0);
+    for (int64_t i = 0; i < nc; ++i) ww[comp[i]] += w[i] * w[i];
+    const double dmean = dsum / static_cast<double>(nc);
     for (int64_t i = 0; i < nc; ++i)
-      for (int64_t j = 0; j < nc; ++j) M[i * nc + j] += tau * w[i] * w[j];
+      for (int64_t j = 0; j < nc; ++j)
+        if (comp[i] == comp[j]) M[i * nc + j] += dmean / std::max(ww[comp[i]], 1e-300) * w[i] * w[j];
   }
   out.coarse_dense = std::move(M);
 }

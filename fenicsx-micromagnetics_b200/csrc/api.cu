@@ -674,8 +674,15 @@ int spx_hmat_destroy(spx_hmat hm) {
   API_END
 }
 
+struct EnsembleSpec {
+  int64_t nsamples;
+  const int64_t* offsets;
+  int64_t dense_max_nb;
+};
+
 static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
-                        const spx_demag_options* opt, HMatrix* preset, spx_demag* out) {
+                        const spx_demag_options* opt, HMatrix* preset, spx_demag* out,
+                        const EnsembleSpec* ens = nullptr) {
   API_BEGIN
   REQUIRE(out);
   *out = nullptr;
@@ -703,6 +710,13 @@ static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t
   if (preset) {
     SPX_CHECK(o.backend == 1, "an H-matrix can only be given to the hmatrix backend");
     o.preset = preset;
+  }
+  if (ens) {
+    SPX_CHECK(ens->nsamples >= 1 && ens->offsets, "an ensemble needs nsamples >= 1 and node offsets");
+    SPX_CHECK(ens->dense_max_nb >= 0, "dense_max_nb must be non-negative");
+    o.backend = 2;
+    o.sample_offsets.assign(ens->offsets, ens->offsets + ens->nsamples + 1);
+    o.dense_max_nb = ens->dense_max_nb;
   }
   auto d = std::make_unique<spx_demag_s>();
   switch (o.prec) {
@@ -732,6 +746,13 @@ static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t
 int spx_demag_create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                      const spx_demag_options* opt, spx_demag* out) {
   return demag_create(X, N, tets, E, Ms, opt, nullptr, out);
+}
+
+int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                              const spx_demag_options* opt, int64_t nsamples, const int64_t* node_offsets,
+                              int64_t dense_max_nb, spx_demag* out) {
+  const EnsembleSpec e{nsamples, node_offsets, dense_max_nb};
+  return demag_create(X, N, tets, E, Ms, opt, nullptr, out, &e);
 }
 
 int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,

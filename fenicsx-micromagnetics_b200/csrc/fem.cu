@@ -132,6 +132,50 @@ __global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const TV*
   }
 }
 
+// remove each component's mean from a projected solution (x = y sdinv when the FP64 state y
+// is kept; one CTA per component)
+template <class TV>
+__global__ void k_seg_center(const int64_t* __restrict__ off, TV* __restrict__ x, double* __restrict__ y,
+                             const double* __restrict__ sdinv) {
+  __shared__ double sh[32];
+  const int64_t a = off[blockIdx.x], b = off[blockIdx.x + 1];
+  double s = 0.0;
+  for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) s += y ? y[i] * sdinv[i] : static_cast<double>(x[i]);
+  const double mean = block_sum(s, sh) / static_cast<double>(b - a);
+  for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+    if (y) {
+      const double xv = y[i] * sdinv[i] - mean;
+      x[i] = static_cast<TV>(xv);
+      y[i] = xv / sdinv[i];
+    } else {
+      x[i] = static_cast<TV>(static_cast<double>(x[i]) - mean);
+    }
+  }
+}
+
+// bh = (b minus its mean over each component) * sdinv, in FP64 (one CTA per component)
+template <class TV>
+__global__ void k_seg_center_bh(const int64_t* __restrict__ off, const TV* __restrict__ b,
+                                const double* __restrict__ sdinv, double* __restrict__ bh) {
+  __shared__ double sh[32];
+  const int64_t a = off[blockIdx.x], e = off[blockIdx.x + 1];
+  double s = 0.0;
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) s += static_cast<double>(b[i]);
+  const double mean = block_sum(s, sh) / static_cast<double>(e - a);
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) bh[i] = (static_cast<double>(b[i]) - mean) * sdinv[i];
+}
+
+// out = b minus its mean over each component (one CTA per component)
+template <class TV>
+__global__ void k_seg_center_b(const int64_t* __restrict__ off, const TV* __restrict__ b, TV* __restrict__ out) {
+  __shared__ double sh[32];
+  const int64_t a = off[blockIdx.x], e = off[blockIdx.x + 1];
+  double s = 0.0;
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) s += static_cast<double>(b[i]);
+  const double mean = block_sum(s, sh) / static_cast<double>(e - a);
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) out[i] = static_cast<TV>(static_cast<double>(b[i]) - mean);
+}
+
 // starting guess: quadratic / linear / constant extrapolation of stored solutions
 __global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                            double* __restrict__ out, int mode) {  // mode 0: out = a - b; 1: out += a
@@ -353,6 +397,7 @@ struct CgIrParams {
   double* res_acc;  // [0] sum of initial relative residuals, [1] sum of final ones
   double rtol, atol, inner_rtol;
   int maxit, max_outer, inner_maxit, warm, project;
+  int bh_given;  // bh already holds the scaled, projected right-hand side (FP64)
 };
 
 template <class TV>
@@ -367,7 +412,7 @@ __global__ void __launch_bounds__(CG_BLOCK, 1) k_cg_ir(CgIrParams<TV> P) {
   const int64_t n = P.n;
   double tot[4];
   double meanb = 0.0;
-  if (P.project) {
+  if (P.project && !P.bh_given) {
     double part = 0.0;
     CG_ROWS_BEGIN part += static_cast<double>(P.b[row]);
     CG_ROWS_END
@@ -379,8 +424,13 @@ __global__ void __launch_bounds__(CG_BLOCK, 1) k_cg_ir(CgIrParams<TV> P) {
   {
     double bb = 0.0;
     CG_ROWS_BEGIN
-      const double bv = static_cast<double>(P.b[row]) - meanb;
-      P.bh[row] = bv * P.sdinv[row];
+      double bv;
+      if (P.bh_given) {
+        bv = P.bh[row] / P.sdinv[row];
+      } else {
+        bv = static_cast<double>(P.b[row]) - meanb;
+        P.bh[row] = bv * P.sdinv[row];
+      }
       if (!P.warm) P.y[row] = 0.0;
       bb += bv * bv;
     CG_ROWS_END
@@ -608,8 +658,21 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   }
   SPX_CUDA(cudaMemsetAsync(bar.p, 0, bar.bytes(), st));
   SPX_CUDA(cudaMemsetAsync(err.p, 0, err.bytes(), st));
+  // ensembles: every component's right-hand side projected on its own (FP64 for the solvers
+  // that keep an FP64 state, so that no FP32 rounding leaves a component inconsistent)
+  const bool seg = project && seg_off.n > 1;
+  if (seg && ir) {
+    k_seg_center_bh<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, b, sdinv64.p, bh64.p);
+    SPX_LAUNCH_CHECK();
+  } else if (seg) {
+    if (bseg.n < n * sizeof(TV)) bseg.alloc(n * sizeof(TV));
+    TV* bc = reinterpret_cast<TV*>(bseg.p);
+    k_seg_center_b<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, b, bc);
+    SPX_LAUNCH_CHECK();
+    b = bc;
+  }
   if (use_amg) {
-    launch_amg<TV>(b, x, rtol, atol, maxit, warm, project, st);
+    launch_amg<TV>(b, x, rtol, atol, maxit, warm, project, st, seg);
   } else if (sizeof(TM) == sizeof(float)) {
     CgIrParams<TV> q;
     q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
@@ -623,6 +686,7 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     q.res_acc = res_acc.p;
     q.rtol = rtol; q.atol = atol; q.inner_rtol = inner_rtol;
     q.maxit = maxit; q.max_outer = max_outer; q.inner_maxit = maxit; q.warm = warm ? 1 : 0;
+    q.bh_given = seg ? 1 : 0;
     q.project = project ? 1 : 0;
     void* a2[] = {&q};
     SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg_ir<TV>), dim3(grid), dim3(block), a2, 0, st));
@@ -639,6 +703,11 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     p.rtol = rtol; p.atol = atol; p.maxit = maxit; p.warm = warm ? 1 : 0; p.project = project ? 1 : 0;
     void* args[] = {&p};
     SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg), dim3(grid), dim3(block), args, 0, st));
+  }
+  if (project && seg_off.n > 1) {
+    k_seg_center<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, x, ir ? y64.p : nullptr,
+                                                                           sdinv64.p);
+    SPX_LAUNCH_CHECK();
   }
   if (slot == 0 && stage_correct && have_pred0) {  // stage 1's prediction error
     if (!delta.n) delta.alloc(n);
@@ -757,6 +826,9 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
     SPX_CHECK(Nb * Nb * 8 <= (int64_t)64 * 1024 * 1024 * 1024, "dense boundary operator too large");
     Bdense.alloc(static_cast<size_t>(Nb * Nb));
     bd.dense_B(Bdense.p, s);
+  } else if (opt.backend == 2) {
+    block_boundary_build<TM>(blk, bd, X, N, tets, E, opt, s);
+    cg1.seg_off.upload(opt.sample_offsets, s);
   } else {
     if (opt.preset) {
       SPX_CHECK(opt.preset->Nb == Nb && opt.preset->packed, "the given H-matrix does not belong to this boundary");
@@ -799,6 +871,8 @@ void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, i
     k_dense_gemv<TV><<<grid_for(Nb * 32, 256), 256, 0, s>>>(Nb, Bdense.p, xb.p, bverts.p, u1.p, phi.p, gB.p);
     SPX_LAUNCH_CHECK();
     prof.launches[PC_BND] += 2;
+  } else if (opt.backend == 2) {
+    prof.launches[PC_BND] += block_boundary_apply<TV, TM>(blk, Nb, bverts.p, u1.p, xb.p, phi.p, gB.p, s);
   } else {
     H.apply_gather<TV>(u1.p, bverts.p, phi.p, u1.p, gB.p, s);
     prof.launches[PC_BND] += H.n_far > 0 ? 3 : 2;
@@ -842,7 +916,7 @@ int64_t DemagCtx<TV, TM>::device_bytes() const {
   if (cg1.amg) tot += cg1.amg->device_bytes() + cg1.amg_a32.bytes() + cg1.amg_rsum.bytes();
   tot += cg2.vals.bytes() + cg2.vals64.bytes() + cg2.work.bytes() + cg2.P.col.bytes();
   tot += AIB.bytes() + PIB.col.bytes() + Bdense.bytes();
-  tot += H.device_bytes();
+  tot += H.device_bytes() + blk.device_bytes();
   return tot;
 }
 

@@ -104,6 +104,11 @@ struct CgSystem {
   // state (y64 or x) is taken only from a solve of the same kind, whose right-hand sides
   // have the same scale; otherwise the solve starts from zero
   int last_kind = 0;
+  // singular systems made of several independent components (ensembles): node offsets of
+  // the components; a projected solve removes every component's mean from the right-hand
+  // side (each component's system must be consistent on its own) and from the solution
+  DevBuf<int64_t> seg_off;
+  DevBuf<char> bseg;  // right-hand side with every component's mean removed (TV)
   DevBuf<double> pred0, delta;
   double inner_rtol = 1e-3;
   int max_outer = 10;
@@ -121,7 +126,8 @@ struct CgSystem {
   void enable_amg(const HostSell& hs, const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col, const std::vector<double>& a,
                   const std::vector<double>& d, bool singular, cudaStream_t s);
   template <class TV>
-  void launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, cudaStream_t st);
+  void launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, cudaStream_t st,
+                  bool bh_given = false);
   // kind: 0 forward, 1 adjoint, 2 tangent; -1 derives it from the slot (0-3, 4-7, 8-11)
   template <class TV>
   CgStats solve(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project, int slot,
@@ -132,8 +138,33 @@ struct CgSystem {
   }
 };
 
+// Block-diagonal boundary operator of an ensemble (a disjoint union of independent sample
+// meshes, ensemble.cu): each sample's Lindholm operator over its own boundary only.  Samples
+// with Nb <= dense_max_nb keep a dense block (TM precision, all blocks applied by one
+// batched launch); larger ones an H-matrix built on the sample's own boundary.
+struct BlockBoundary {
+  int64_t nsamples = 0;
+  std::vector<int64_t> b0, nb;        // per sample: first boundary row (union order), count
+  std::vector<int> dense;             // per sample: 1 dense block, 0 H-matrix
+  int64_t ndense = 0, dense_rows = 0, dense_entries = 0;
+  DevBuf<int64_t> d_row0;             // [ndense + 1] prefix of the dense samples' rows
+  DevBuf<int64_t> d_b0, d_nb, d_off;  // per dense sample: boundary offset, Nb, pool offset
+  DevBuf<char> pool;                  // dense blocks, row-major per sample (TM)
+  std::vector<std::unique_ptr<HMatrix>> H;  // per sample (null for dense samples)
+  int64_t device_bytes() const;
+};
+
+struct DemagOptions;
+template <class TM>
+void block_boundary_build(BlockBoundary& bb, const BoundaryDev& bd, const double* X, int64_t N, const int32_t* tets,
+                          int64_t E, const DemagOptions& o, cudaStream_t s);
+// g = B u1|bnd per sample, phi[bverts] = u1 + g; returns the number of launches
+template <class TV, class TM>
+int block_boundary_apply(BlockBoundary& bb, int64_t Nb, const int32_t* bverts, const TV* u1, TV* xb, TV* phi, TV* gB,
+                         cudaStream_t s);
+
 struct DemagOptions {
-  int backend = 0;          // 0 dense, 1 hmatrix
+  int backend = 0;          // 0 dense, 1 hmatrix, 2 block-diagonal ensemble (BlockBoundary)
   Prec prec = Prec::F64;    // vector / matrix precision of the pipeline
   Prec hprec = Prec::F64;   // storage precision of the H-matrix factors
   double rtol_u1 = 1e-6, rtol_u2 = 1e-6, atol = 1e-12;
@@ -143,6 +174,9 @@ struct DemagOptions {
   int u1_pc = 0;            // u1 preconditioner: 0 smoothed-aggregation AMG, 1 Jacobi
   HMatrix* preset = nullptr;  // hmatrix backend: adopt this H-matrix (moved in) instead of building
   HBuildConfig hcfg;
+  // ensemble backend: sample s owns nodes [sample_offsets[s], sample_offsets[s + 1])
+  std::vector<int64_t> sample_offsets;
+  int64_t dense_max_nb = 4096;
 };
 
 // Transposed operators of the demag map m -> H, built on first use of
@@ -179,6 +213,7 @@ struct DemagCtx {
   DevBuf<double> AIB;    // interior rows x boundary columns, FP64
   DevBuf<double> Bdense;
   HMatrix H;
+  BlockBoundary blk;
   DevBuf<TV> b, u1, phi, gB, bI, xI, xb;
   CgStats last1, last2;
   int64_t applies = 0;

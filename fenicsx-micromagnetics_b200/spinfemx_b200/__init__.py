@@ -24,6 +24,8 @@ _EXPORTS = {
     "fem_assemble": ".geometry",
     "cluster_tree_perm": ".geometry",
     "dense_b_apply": ".geometry",
+    "LLGEnsemble": ".ensemble",
+    "ensemble_mesh": ".ensemble",
     "llg_trajectory": ".adjoint",
     "trajectory_tangent": ".adjoint",
 }

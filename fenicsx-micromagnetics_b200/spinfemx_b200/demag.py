@@ -27,7 +27,8 @@ class DemagFieldLindholmGPU:
                  hmatrix_max_temporary_block_bytes=256 * 1024 ** 2, hmatrix_use_fp32=True, precision="f64",
                  hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False,
                  u1_preconditioner="amg", hmatrix_cache_path=None, hmatrix_cache_dir="./hmatrix_cache",
-                 cache_tag=None, hmatrix_force_rebuild=False, hmatrix_cache_compressed=False, **unused):
+                 cache_tag=None, hmatrix_force_rebuild=False, hmatrix_cache_compressed=False, sample_offsets=None,
+                 dense_max_nb=4096, **unused):
         """Options as in the reference, plus:
 
         precision          'f64' | 'f32' (plain FP32) | 'mixed' (FP64 vectors, FP32 matrices,
@@ -40,6 +41,10 @@ class DemagFieldLindholmGPU:
                            prediction error
         u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or
                            'jacobi'
+        boundary_backend   also 'ensemble': X / tets is a disjoint union of independent samples
+                           (``sample_offsets``: node ranges, see spinfemx_b200.ensemble); each
+                           sample gets its own boundary operator, dense when its Nb <=
+                           ``dense_max_nb``, an H-matrix otherwise
         hmatrix_cache_path / cache_tag
                            npz cache of the H-matrix in the reference's schema
                            (Demag_Lindholm_GPU.py:353-377 naming in hmatrix_cache_dir or
@@ -59,8 +64,10 @@ class DemagFieldLindholmGPU:
         self.volume_scale = float(volume_scale)
         self.precision = precision
         req = str(boundary_backend).strip().lower()
-        if req not in {"dense", "hmatrix", "auto"}:
-            raise ValueError("boundary_backend must be 'dense', 'hmatrix', or 'auto'.")
+        if req not in {"dense", "hmatrix", "auto", "ensemble"}:
+            raise ValueError("boundary_backend must be 'dense', 'hmatrix', 'auto' or 'ensemble'.")
+        if (req == "ensemble") != (sample_offsets is not None):
+            raise ValueError("boundary_backend='ensemble' and sample_offsets go together")
         if req == "auto":
             Nb = _lib.c_i64()
             call("spx_boundary_sizes", ptr(X), self.N, ptr(tets), tets.shape[0], C.byref(Nb), None)
@@ -117,6 +124,11 @@ class DemagFieldLindholmGPU:
             call("spx_demag_create_with_hmat", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o),
                  Hc.handle, C.byref(self._h))
             del Hc  # its data moved into the demag object
+        elif req == "ensemble":
+            offs = np.ascontiguousarray(np.asarray(sample_offsets, dtype=np.int64).reshape(-1))
+            self.sample_offsets = offs
+            call("spx_demag_create_ensemble", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o),
+                 offs.size - 1, ptr(offs), int(dense_max_nb), C.byref(self._h))
         else:
             call("spx_demag_create", ptr(X), self.N, ptr(tets), tets.shape[0], self.Ms, C.byref(o),
                  C.byref(self._h))

@@ -179,6 +179,17 @@ SPX_API int spx_demag_create(const double* X, int64_t N, const int32_t* tets, in
  * differs from its packing */
 SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                        const spx_demag_options* opt, spx_hmat h, spx_demag* out);
+/* Ensemble of independent samples (batched form; no counterpart in the reference, which runs
+ * one mesh per object): X / tets is the disjoint union of the samples' meshes, sample s owning
+ * nodes [node_offsets[s], node_offsets[s+1]) (node_offsets[0] = 0, node_offsets[nsamples] = N)
+ * and the tetrahedra that reference them.  FEM operators, both Poisson solves and
+ * spx_demag_apply run once for all samples; the boundary operator is block diagonal: the
+ * Lindholm operator of each sample's own boundary, dense (one batched launch for all dense
+ * samples) when the sample's Nb <= dense_max_nb, else an H-matrix with opt->hmat.
+ * opt->backend is ignored.  spx_demag_apply_transpose is not available for ensembles. */
+SPX_API int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
+                                      const spx_demag_options* opt, int64_t nsamples, const int64_t* node_offsets,
+                                      int64_t dense_max_nb, spx_demag* out);
 SPX_API int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s);
 /* out = D^T w for the linear demag map D: m -> H of spx_demag_apply (AoS FP64 device,
  * length 3N).  No counterpart in the reference.  Evaluated as
