@@ -513,7 +513,18 @@ def run_ensemble(a):
     torch.cuda.synchronize()
     ms = allmax(e0.elapsed_time(e1), ws)
     clocks = sampler.stop() if sampler else None
-    st = ens.hef.stats()
+    # per-phase breakdown on a separate (profiled) run of the same number of steps
+    from spinfemx_b200 import _lib
+    _lib.call("spx_demag_profile_begin", dm.handle)
+    ens.step(dt, a.steps)
+    ms_cat = np.zeros(8)
+    nl_cat = np.zeros(8, np.int64)
+    ng_cat = np.zeros(8, np.int64)
+    _lib.call("spx_demag_profile_end", dm.handle, _lib.ptr(ms_cat), _lib.ptr(nl_cat), _lib.ptr(ng_cat))
+    cats = ["div", "u1_solve", "boundary_apply", "u2_rhs", "u2_solve", "phi", "stage"]
+    phases = {c: {"ms_per_step": round(float(ms_cat[k]) / a.steps, 4), "launches_per_step":
+                  round(float(nl_cat[k]) / a.steps, 1)} for k, c in enumerate(cats) if ng_cat[k]}
+    launches = int(nl_cat[:7].sum())
     # the same samples one by one (separate field objects, same options), a few of them timed
     seq = None
     if a.ens_compare and rank == 0:
@@ -560,7 +571,8 @@ def run_ensemble(a):
                                f"Bz U[-0.5,0.5] T, RK4 dt 20 fs",
                    "nodes": nodes, "boundary_nodes": int(dm.Nb), "boundary_blocks": blk,
                    "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2, "parallelism": f"samples sharded, {ws} rank(s)"},
-        "launches_per_step": round(st["launches"] / max(st["steps"], 1), 1),
+        "phases": phases,
+        "gpu_launches_per_step": round(launches / a.steps, 1),
         "unbatched": seq,
         "setup_s": round(setup_s, 1),
         "clocks": clocks,

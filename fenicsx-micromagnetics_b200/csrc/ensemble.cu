@@ -9,8 +9,9 @@
 //   B = blockdiag(B_s),  B_s = Lindholm operator of sample s's own boundary triangles.
 // Samples with Nb_s <= dense_max_nb keep a dense block; a single launch applies all dense
 // blocks (a warp per boundary row over the concatenated rows, ragged row lengths).  Larger
-// samples get an H-matrix built on the sample's own boundary and are applied with the
-// boundary gather / scatter fused (HMatrix::apply_gather with the sample's slice of bverts).
+// samples get an H-matrix built on the sample's own boundary; these are concatenated into
+// one block-diagonal H-matrix (hmat_merge) applied by one k_hgather / k_far_z / k_rows
+// sequence for all of them, the boundary gather / scatter fused through an index map.
 #include <algorithm>
 
 #include "fem.cuh"
@@ -30,6 +31,13 @@ __global__ void k_gather_b(int64_t n, const int32_t* __restrict__ idx, const TV*
                            TV* __restrict__ dst) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) dst[i] = src[idx[i]];
+}
+
+template <class TV>
+__global__ void k_scatter_rows(int64_t n, const int32_t* __restrict__ idx, const TV* __restrict__ src,
+                               TV* __restrict__ dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[idx[i]] = src[i];
 }
 
 // warp per dense boundary row r (concatenated over the dense samples):
@@ -77,6 +85,7 @@ int64_t BlockBoundary::device_bytes() const {
   int64_t t = static_cast<int64_t>(pool.bytes() + d_row0.bytes() + d_b0.bytes() + d_nb.bytes() + d_off.bytes());
   for (const auto& h : H)
     if (h) t += h->device_bytes();
+  if (Hm) t += Hm->device_bytes() + static_cast<int64_t>(hidx.bytes() + hmap.bytes() + gbh.bytes());
   return t;
 }
 
@@ -160,6 +169,25 @@ void block_boundary_build(BlockBoundary& bb, const BoundaryDev& bd, const double
     bb.H[k]->build(bk, o.hcfg, s);
     bb.H[k]->pack(o.hprec, s);
   }
+  // one block-diagonal H-matrix for all H-matrix samples
+  std::vector<const HMatrix*> parts;
+  std::vector<int32_t> hidx, hmap;
+  for (int64_t k = 0; k < ns; ++k)
+    if (bb.H[k]) {
+      parts.push_back(bb.H[k].get());
+      for (int64_t i = 0; i < bb.nb[k]; ++i) {
+        hidx.push_back(bv[bb.b0[k] + i]);
+        hmap.push_back(static_cast<int32_t>(bb.b0[k] + i));
+      }
+    }
+  if (!parts.empty()) {
+    bb.Hm = std::make_unique<HMatrix>();
+    hmat_merge(parts, *bb.Hm, s);
+    bb.hidx.upload(hidx, s);
+    bb.hmap.upload(hmap, s);
+    bb.gbh.alloc(hidx.size() * sizeof(double));
+    for (auto& h : bb.H) h.reset();
+  }
   SPX_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -177,11 +205,14 @@ int block_boundary_apply(BlockBoundary& bb, int64_t Nb, const int32_t* bverts, c
     SPX_LAUNCH_CHECK();
     launches += 2;
   }
-  for (int64_t k = 0; k < bb.nsamples; ++k)
-    if (bb.H[k]) {
-      bb.H[k]->apply_gather<TV>(u1, bverts + bb.b0[k], phi, u1, gB + bb.b0[k], s);
-      launches += bb.H[k]->n_far > 0 ? 3 : 2;
-    }
+  if (bb.Hm) {
+    TV* yh = reinterpret_cast<TV*>(bb.gbh.p);
+    bb.Hm->apply_gather<TV>(u1, bb.hidx.p, phi, u1, yh, s);
+    const int64_t nh = bb.Hm->Nb;
+    k_scatter_rows<TV><<<grid_for(nh, 256), 256, 0, s>>>(nh, bb.hmap.p, yh, gB);
+    SPX_LAUNCH_CHECK();
+    launches += (bb.Hm->nunits > 0 ? 3 : 2) + 1;
+  }
   return launches;
 }
 

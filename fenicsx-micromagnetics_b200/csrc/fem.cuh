@@ -150,7 +150,12 @@ struct BlockBoundary {
   DevBuf<int64_t> d_row0;             // [ndense + 1] prefix of the dense samples' rows
   DevBuf<int64_t> d_b0, d_nb, d_off;  // per dense sample: boundary offset, Nb, pool offset
   DevBuf<char> pool;                  // dense blocks, row-major per sample (TM)
-  std::vector<std::unique_ptr<HMatrix>> H;  // per sample (null for dense samples)
+  std::vector<std::unique_ptr<HMatrix>> H;  // per sample while building (null for dense samples)
+  // all H-matrix samples merged into one block-diagonal H-matrix (one apply for all)
+  std::unique_ptr<HMatrix> Hm;
+  DevBuf<int32_t> hidx;               // merged boundary index -> ensemble vertex
+  DevBuf<int32_t> hmap;               // merged boundary index -> ensemble boundary row
+  DevBuf<char> gbh;                   // merged-order result (TV)
   int64_t device_bytes() const;
 };
 

@@ -199,6 +199,123 @@ void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec 
   H.pack(p, s);
 }
 
+namespace {
+template <class T>
+std::vector<T> download(const DevBuf<T>& b) {
+  std::vector<T> h(b.n);
+  if (b.n) SPX_CUDA(cudaMemcpy(h.data(), b.p, b.n * sizeof(T), cudaMemcpyDeviceToHost));
+  return h;
+}
+size_t factor_bytes(Prec p) { return p == Prec::F64 ? 8 : (p == Prec::F32 ? 4 : 2); }
+size_t tile_bytes(Prec p) { return p == Prec::F64 ? 8 : 4; }
+}  // namespace
+
+// Block-diagonal concatenation of packed H-matrices (ensembles): the boundary index space,
+// the permuted space, the factor and tile pools, the far-field z vectors and partial sums,
+// the groups, the k_far_z warps and the row segments of part k follow those of parts < k,
+// so one apply (k_hgather, k_far_z, k_rows) serves all parts.  Only the apply-side data is
+// merged (no tree, no FP64 pools: the result cannot be repacked or transposed).
+void hmat_merge(const std::vector<const HMatrix*>& parts, HMatrix& M, cudaStream_t s) {
+  SPX_CHECK(!parts.empty(), "nothing to merge");
+  const Prec p = parts[0]->prec;
+  const size_t fb = factor_bytes(p), nbt = tile_bytes(p);
+  std::vector<int32_t> perm, warp_first(1, 0), seg_start;
+  std::vector<double> diag;
+  std::vector<FarUnit> units;
+  std::vector<FarGroup> groups;
+  std::vector<int64_t> item_ptr(1, 0), near_begin;
+  std::vector<RowItem> items;
+  int64_t c0 = 0, z0 = 0, zp0 = 0, g0 = 0, u0 = 0, i0 = 0, fbytes = 0, nbytes = 0, nwarps = 0;
+  std::vector<int64_t> foff, noff;
+  for (const HMatrix* H : parts) {
+    SPX_CHECK(H->packed && H->prec == p, "merged H-matrices must be packed in the same precision");
+    foff.push_back(fbytes);
+    noff.push_back(nbytes);
+    fbytes += ((static_cast<int64_t>(H->far_f.n) + 255) / 256) * 256;
+    nbytes += ((static_cast<int64_t>(H->near_f.n) + 255) / 256) * 256;
+  }
+  M.far_f.alloc(std::max<int64_t>(fbytes, 1));
+  M.near_f.alloc(std::max<int64_t>(nbytes, 1));
+  for (size_t k = 0; k < parts.size(); ++k) {
+    const HMatrix& H = *parts[k];
+    const int64_t F = foff[k] / static_cast<int64_t>(fb), Nn = noff[k] / static_cast<int64_t>(nbt);
+    if (H.far_f.n)
+      SPX_CUDA(cudaMemcpyAsync(M.far_f.p + foff[k], H.far_f.p, H.far_f.n, cudaMemcpyDeviceToDevice, s));
+    if (H.near_f.n)
+      SPX_CUDA(cudaMemcpyAsync(M.near_f.p + noff[k], H.near_f.p, H.near_f.n, cudaMemcpyDeviceToDevice, s));
+    for (int32_t v : download(H.perm)) perm.push_back(static_cast<int32_t>(v + c0));
+    for (double v : download(H.diag_perm)) diag.push_back(v);
+    for (FarUnit U : download(H.units)) {
+      U.voff += F;
+      U.xc += static_cast<int32_t>(c0);
+      U.zout += static_cast<int32_t>((U.flags & 3) == 2 ? zp0 : z0);
+      if (U.grp >= 0) U.grp += static_cast<int32_t>(g0);
+      units.push_back(U);
+    }
+    for (FarGroup G : download(H.groups)) {
+      G.pbase += static_cast<int32_t>(zp0);
+      G.zdst += static_cast<int32_t>(z0);
+      groups.push_back(G);
+    }
+    const std::vector<int32_t> wf = download(H.warp_first);
+    for (int64_t w = 0; w < H.nwarps_z; ++w) warp_first.push_back(static_cast<int32_t>(wf[w + 1] + u0));
+    const std::vector<int32_t> ss = download(H.seg_start);
+    const std::vector<int64_t> ip = download(H.item_ptr), nb = download(H.near_begin);
+    const std::vector<RowItem> it = download(H.items);
+    for (int64_t g = 0; g < H.nseg; ++g) {
+      seg_start.push_back(static_cast<int32_t>(ss[g] + c0));
+      near_begin.push_back(nb[g] + i0);
+      for (int64_t q = ip[g]; q < ip[g + 1]; ++q) {
+        RowItem r = it[q];
+        if (q < nb[g]) {  // far: U tile, scaled by z
+          r.off += F;
+          r.src += static_cast<int32_t>(z0);
+        } else {  // near: tile, scaled by x~
+          r.off += Nn;
+          r.src += static_cast<int32_t>(c0);
+        }
+        items.push_back(r);
+      }
+      item_ptr.push_back(static_cast<int64_t>(items.size()));
+    }
+    c0 += H.Nb;
+    z0 += H.zlen;
+    zp0 += H.zpart_len;
+    g0 += static_cast<int64_t>(H.groups.n);
+    u0 += H.nunits;
+    i0 += static_cast<int64_t>(it.size());
+    nwarps += H.nwarps_z;
+    M.n_far += H.n_far;
+    M.n_near += H.n_near;
+    M.bytes_far += H.bytes_far;
+    M.bytes_near += H.bytes_near;
+  }
+  SPX_CHECK(z0 < (int64_t(1) << 31) && zp0 < (int64_t(1) << 31) && c0 < (int64_t(1) << 31),
+            "merged H-matrix too large for 32-bit indices");
+  seg_start.push_back(static_cast<int32_t>(c0));
+  M.device = parts[0]->device;
+  M.Nb = c0;
+  M.prec = p;
+  M.perm.upload(perm, s);
+  M.diag_perm.upload(diag, s);
+  M.units.upload(units, s);
+  M.warp_first.upload(warp_first, s);
+  M.groups.upload(groups, s);
+  M.gcnt.alloc(std::max<size_t>(groups.size(), 1));
+  M.gcnt.zero(s);
+  M.seg_start.upload(seg_start, s);
+  M.item_ptr.upload(item_ptr, s);
+  M.near_begin.upload(near_begin, s);
+  M.items.upload(items, s);
+  M.nseg = static_cast<int64_t>(seg_start.size()) - 1;
+  M.zlen = z0;
+  M.zpart_len = zp0;
+  M.nunits = u0;
+  M.nwarps_z = nwarps;
+  M.packed = true;
+  SPX_CUDA(cudaStreamSynchronize(s));
+}
+
 HMatrix& HMatrix::transposed(cudaStream_t s) {
   if (tr) return *tr;
   SPX_CHECK(packed, "H-matrix is not packed");

@@ -131,6 +131,10 @@ void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec 
                  const int32_t* indices, const double* data, const int32_t* perm_in, const double* diag_jump,
                  cudaStream_t s);
 
+// Block-diagonal concatenation of packed H-matrices (same packing precision) for one apply
+// over all of them (hio.cu); apply-side data only.
+void hmat_merge(const std::vector<const HMatrix*>& parts, HMatrix& M, cudaStream_t s);
+
 // y = H x (original boundary ordering, FP64) using the library's static device scratch
 // instead of allocated buffers (see spx_hmat_apply_noalloc in include/spx.h).
 void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s);

@@ -11,6 +11,7 @@ from oracle import llg as ollg
 from oracle import mesh as omesh
 
 BOXES = [(6, 5, 2), (9, 7, 3), (12, 10, 2)]  # Nb 106, 224, 330
+DENSE_MAX = 200  # sample 0 dense, samples 1 and 2 H-matrices (merged into one)
 MAT = dict(Ms=1.1e6, Aex=1.6e-11, Ku=8e5, D_int=3e-3, alpha=0.3)
 TIGHT = dict(ksp_rtol_u1=1e-12, ksp_rtol_u2=1e-12, ksp_atol=0.0, ksp_maxit_u1=20000, ksp_maxit_u2=20000)
 HM = dict(hmatrix_epsilon=1e-7, hmatrix_leaf_size=16)
@@ -61,13 +62,13 @@ def test_ensemble_demag_equals_per_sample(spx, precision):
     X, T, off = spx.ensemble_mesh(ms)
     kw = dict(precision=precision, **TIGHT, **HM)
     d = spx.DemagFieldLindholmGPU(X, T, MAT["Ms"], boundary_backend="ensemble", sample_offsets=off,
-                                  dense_max_nb=300, **kw)
+                                  dense_max_nb=DENSE_MAX, **kw)
     m = np.concatenate([_m0(Xs.shape[0], 10 + k) for k, (Xs, _) in enumerate(ms)])
     H = torch.empty(3 * X.shape[0], dtype=torch.float64, device="cuda")
     d.compute_vec(_t(m), H)
     H = H.cpu().numpy()
     for k, (Xs, Ts) in enumerate(ms):
-        ds = spx.DemagFieldLindholmGPU(Xs, Ts, MAT["Ms"], boundary_backend="dense" if k < 2 else "hmatrix", **kw)
+        ds = spx.DemagFieldLindholmGPU(Xs, Ts, MAT["Ms"], boundary_backend="dense" if k == 0 else "hmatrix", **kw)
         Hs = torch.empty(3 * Xs.shape[0], dtype=torch.float64, device="cuda")
         ds.compute_vec(_t(m[3 * off[k]:3 * off[k + 1]]), Hs)
         Hs = Hs.cpu().numpy()
@@ -85,7 +86,8 @@ def test_ensemble_trajectory_equals_per_sample(spx):
     mu0 = 4e-7 * np.pi
     dk = dict(precision="f64", **TIGHT, **HM)
     ens = spx.LLGEnsemble(ms, MAT["Ms"], Aex=MAT["Aex"], Ku=MAT["Ku"], D_int=MAT["D_int"], alpha=MAT["alpha"],
-                          H0=[[0.0, 0.0, b / mu0] for b in Bz], dense_max_nb=300, precision="f64", demag_kwargs=dk)
+                          H0=[[0.0, 0.0, b / mu0] for b in Bz], dense_max_nb=DENSE_MAX, precision="f64",
+                          demag_kwargs=dk)
     m0 = [_m0(Xs.shape[0], 20 + k) for k, (Xs, _) in enumerate(ms)]
     ens.set_state(m0)
     nsteps, dt = 10, 2e-14
@@ -93,7 +95,7 @@ def test_ensemble_trajectory_equals_per_sample(spx):
     mE = ens.split(ens.get_state().cpu().numpy())
     for k, (Xs, Ts) in enumerate(ms):
         N = Xs.shape[0]
-        kw = dict(dk, boundary_backend="dense" if k < 2 else "hmatrix")
+        kw = dict(dk, boundary_backend="dense" if k == 0 else "hmatrix")
         hef = spx.EffectiveField(Xs, Ts, MAT["Ms"], Aex=MAT["Aex"], Ku=MAT["Ku"], n_ani_vec=[0.0, 0.0, 1.0],
                                  D_int=MAT["D_int"], n0_int_vec=[0.0, 0.0, 1.0], alpha=MAT["alpha"],
                                  H0_static=[0.0, 0.0, Bz[k] / mu0], use_demag=True, demag_kwargs=kw)
