@@ -493,7 +493,7 @@ def run_ensemble(a):
                   a.warm_start])
     t0 = time.time()
     ens = spx.LLGEnsemble(meshes, 1.1e6, H0=[[0.0, 0.0, b / MU0] for b in Bz], dense_max_nb=4096,
-                          precision=a.precision, demag_kwargs=dk, **mat)
+                          precision=a.precision, demag_kwargs=dk, graph=bool(a.graph), **mat)
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     dm = ens.hef.demag_field
@@ -525,6 +525,16 @@ def run_ensemble(a):
     phases = {c: {"ms_per_step": round(float(ms_cat[k]) / a.steps, 4), "launches_per_step":
                   round(float(nl_cat[k]) / a.steps, 1)} for k, c in enumerate(cats) if ng_cat[k]}
     launches = int(nl_cat[:7].sum())
+    info = np.zeros(6, np.int64)
+    _lib.call("spx_demag_ensemble_info", dm.handle, _lib.ptr(info))
+    c_a = counters(dm)
+    wm = 8 if a.precision == "f64" else 4
+    wv = 4 if a.precision == "f32" else 8
+    bnd_bytes = float(info[2] * wm + info[4] + info[5] + 6 * dm.Nb * wv)
+    if "boundary_apply" in phases:
+        per_apply = phases["boundary_apply"]["ms_per_step"] / 4.0
+        phases["boundary_apply"]["algorithmic_bytes_per_apply"] = bnd_bytes
+        phases["boundary_apply"]["achieved_GBps"] = round(bnd_bytes / (per_apply * 1e-3) / 1e9, 1)
     # the same samples one by one (separate field objects, same options), a few of them timed
     seq = None
     if a.ens_compare and rank == 0:
@@ -572,6 +582,11 @@ def run_ensemble(a):
                    "nodes": nodes, "boundary_nodes": int(dm.Nb), "boundary_blocks": blk,
                    "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2, "parallelism": f"samples sharded, {ws} rank(s)"},
         "phases": phases,
+        "graph": ens.hef.graph_stats(),
+        "boundary": {"dense_samples": int(info[1]), "dense_entries": int(info[2]), "hmatrix_rows": int(info[3]),
+                     "hmatrix_far_bytes": int(info[4]), "hmatrix_near_bytes": int(info[5])},
+        "cg": {"u1_iters_per_solve": round(c_a[0][0] / max(c_a[0][2], 1), 1),
+               "u2_iters_per_solve": round(c_a[1][0] / max(c_a[1][2], 1), 1)},
         "gpu_launches_per_step": round(launches / a.steps, 1),
         "unbatched": seq,
         "setup_s": round(setup_s, 1),
@@ -752,6 +767,7 @@ def main():
     ap.add_argument("--traffic", type=json.loads, default=None,
                     help='per-group DRAM bytes per launch from an ncu capture, e.g. {"u1_solve": 1.2e9}')
     ap.add_argument("--samples", type=int, default=64)
+    ap.add_argument("--graph", type=int, default=1, help="ensemble: replay RK4 steps from CUDA graphs")
     ap.add_argument("--ens-compare", type=int, default=6, help="ensemble: samples also timed one by one")
     ap.add_argument("--workload", default="film", choices=["film", "adjoint", "ensemble"],
                     help="film: LLG steps/s on the 0.48M-node film (the headline); adjoint: trajectory gradient "

@@ -431,6 +431,7 @@ void DemagCtx<TV, TM>::apply_transpose(const TV* w, TV* out, bool accumulate, in
     SPX_CUDA(cudaStreamSynchronize(s));
     A.ready = true;
   }
+  ++epoch;
   // adjoint solves start from the extrapolation of earlier adjoint solutions of the same RK
   // stage (slots 4-7) when warm starts are on, from zero otherwise
   const int sl = (opt.warm_start != 0 && slot >= 0) ? slot : -1;

@@ -97,6 +97,7 @@ struct DemagBase {
   virtual int amg_levels(int64_t* out, int maxl) = 0;
   virtual void set_tolerances(double r1, double r2, double at, int m1, int m2) = 0;
   virtual void apply_transpose(const double* w, double* out, cudaStream_t s) = 0;
+  virtual void ensemble_info(int64_t* out6) const = 0;
 };
 
 template <class TV, class TM>
@@ -166,8 +167,18 @@ struct DemagImpl : DemagBase {
     return a->nlev;
   }
   void set_tolerances(double r1, double r2, double at, int m1, int m2) override {
+    ++d.epoch;  // captured step graphs hold the old tolerances
     d.opt.rtol_u1 = r1; d.opt.rtol_u2 = r2; d.opt.atol = at;
     d.opt.maxit_u1 = m1; d.opt.maxit_u2 = m2;
+  }
+  void ensemble_info(int64_t* o) const override {
+    const BlockBoundary& b = d.blk;
+    o[0] = b.nsamples;
+    o[1] = b.ndense;
+    o[2] = b.dense_entries;
+    o[3] = b.Hm ? b.Hm->Nb : 0;
+    o[4] = b.Hm ? b.Hm->bytes_far : 0;
+    o[5] = b.Hm ? b.Hm->bytes_near : 0;
   }
   void apply_transpose(const double* w, double* out, cudaStream_t s) override {
     if (sizeof(TV) == sizeof(double)) {
@@ -206,6 +217,9 @@ struct LLGBase {
   virtual void step_jvp(const double* mn, const double* dm, const double* dKu, const double* dH0, double dt,
                         double* mo, double* dmo, cudaStream_t s) = 0;
   virtual void set_ku_map(const double* ku) = 0;
+  virtual void set_graph(int on) = 0;
+  virtual void graph_stats(int64_t* replays, int32_t* active) const = 0;
+  virtual std::string graph_error() const = 0;
 };
 
 template <class TV, class TM>
@@ -265,6 +279,7 @@ struct LLGImpl : LLGBase {
     SPX_CUDA(cudaStreamSynchronize(s));
   }
   void set_uniform_field(double x, double y, double z) override {
+    l.graph_reset();
     l.H0.release();
     l.h0[0] = x; l.h0[1] = y; l.h0[2] = z;
   }
@@ -315,7 +330,20 @@ struct LLGImpl : LLGBase {
     back(mo, tb, s);
     back(dmo, td, s);
   }
-  void set_ku_map(const double* ku) override { l.set_ku_map(ku, 0); }
+  void set_ku_map(const double* ku) override {
+    l.graph_reset();
+    l.set_ku_map(ku, 0);
+  }
+  void set_graph(int on) override {
+    l.graph_reset();
+    l.graph_on = on != 0;
+    l.graph_error.clear();
+  }
+  void graph_stats(int64_t* replays, int32_t* active) const override {
+    if (replays) *replays = l.graph_replays;
+    if (active) *active = (l.graph_on && l.graph_ok) ? 1 : 0;
+  }
+  std::string graph_error() const override { return l.graph_error; }
 };
 
 struct spx_llg_s {
@@ -755,6 +783,13 @@ int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, i
   return demag_create(X, N, tets, E, Ms, opt, nullptr, out, &e);
 }
 
+int spx_demag_ensemble_info(spx_demag d, int64_t* out6) {
+  API_BEGIN
+  REQUIRE(d); REQUIRE(out6);
+  d->impl->ensemble_info(out6);
+  API_END
+}
+
 int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                const spx_demag_options* opt, spx_hmat hm, spx_demag* out) {
   if (!hm) {
@@ -1058,6 +1093,22 @@ int spx_llg_step_jvp(spx_llg l, const double* m_n, const double* dm, const doubl
   REQUIRE(l); REQUIRE(m_n); REQUIRE(dm); REQUIRE(m_out); REQUIRE(dm_out);
   SPX_CHECK(dt > 0.0, "dt must be positive");
   l->impl->step_jvp(m_n, dm, dKu, dH0, dt, m_out, dm_out, S(s));
+  API_END
+}
+
+int spx_llg_set_graph(spx_llg l, int32_t enable) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->set_graph(enable);
+  API_END
+}
+
+int spx_llg_graph_stats(spx_llg l, int64_t* replays, int32_t* active) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->graph_stats(replays, active);
+  const std::string e = l->impl->graph_error();
+  if (!e.empty()) spx::set_last_error(e);
   API_END
 }
 

@@ -899,6 +899,7 @@ void DemagCtx<TV, TM>::potential(const TV* m, cudaStream_t s, bool sync_stats, i
     prof.launches[PC_PHI] += 1;
   }
   ++applies;
+  ++epoch;
 }
 
 template <class TV, class TM>

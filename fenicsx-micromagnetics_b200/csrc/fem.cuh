@@ -222,6 +222,7 @@ struct DemagCtx {
   DevBuf<TV> b, u1, phi, gB, bI, xI, xb;
   CgStats last1, last2;
   int64_t applies = 0;
+  int64_t epoch = 0;   // solves issued outside a captured step (invalidates step graphs)
   Profiler prof;
   int64_t launches = 0;
   void create(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms, const DemagOptions& o,

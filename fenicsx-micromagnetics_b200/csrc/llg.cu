@@ -442,9 +442,87 @@ void LLGCtx<TV, TM>::rhs(const TV* min, TV* out, cudaStream_t s) {
 }
 
 template <class TV, class TM>
+LLGCtx<TV, TM>::~LLGCtx() {
+  graph_reset();
+  if (gstream) cudaStreamDestroy(gstream);
+}
+
+template <class TV, class TM>
+void LLGCtx<TV, TM>::graph_reset() {
+  for (auto& g : gexec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  graph_ok = false;
+}
+
+template <class TV, class TM>
 void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
-  const TV h = static_cast<TV>(dt);
+  const bool profiling = use_demag && demag->prof.on;
   for (int64_t it = 0; it < nsteps; ++it) {
+    if (!graph_on || profiling) {
+      step_once(dt, s);
+      continue;
+    }
+    const int64_t ep = use_demag ? demag->epoch : 0;
+    if (graph_ok && (dt != gdt || ep != gepoch)) graph_reset();
+    if (!graph_ok) {
+      if (gwarm < 3) {  // fill the extrapolation rings (and every lazily allocated buffer) first
+        step_once(dt, s);
+        ++gwarm;
+        continue;
+      }
+      if (!gstream) SPX_CUDA(cudaStreamCreateWithFlags(&gstream, cudaStreamNonBlocking));
+      const int64_t st0 = steps, re0 = rhs_evals, la0 = launches;
+      try {
+        for (int p = 0; p < 3; ++p) {
+          cudaGraph_t g = nullptr;
+          SPX_CUDA(cudaStreamBeginCapture(gstream, cudaStreamCaptureModeThreadLocal));
+          try {
+            step_once(dt, gstream);
+          } catch (...) {
+            cudaStreamEndCapture(gstream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+          }
+          SPX_CUDA(cudaStreamEndCapture(gstream, &g));
+          const cudaError_t e = cudaGraphInstantiate(&gexec[p], g, 0);
+          cudaGraphDestroy(g);
+          SPX_CUDA(e);
+        }
+      } catch (const Error& e) {
+        // capture not possible here: keep stepping without graphs
+        graph_reset();
+        graph_on = false;
+        graph_error = e.what();
+        cudaGetLastError();
+        steps = st0; rhs_evals = re0; launches = la0;
+        step_once(dt, s);
+        continue;
+      }
+      // the three captures advanced the rings by three steps: back to the same phase
+      launches = la0;
+      steps = st0;
+      rhs_evals = re0;
+      graph_ok = true;
+      gdt = dt;
+      gphase = 0;
+      gepoch = use_demag ? demag->epoch : 0;
+    }
+    SPX_CUDA(cudaGraphLaunch(gexec[gphase], s));
+    gphase = (gphase + 1) % 3;
+    ++graph_replays;
+    ++steps;
+    rhs_evals += 4;
+    launches += 4;
+  }
+}
+
+template <class TV, class TM>
+void LLGCtx<TV, TM>::step_once(double dt, cudaStream_t s) {
+  const TV h = static_cast<TV>(dt);
+  for (int64_t it = 0; it < 1; ++it) {
     const TV* in[4] = {m.p, ms0.p, ms1.p, ms0.p};
     TV* out[4] = {ms0.p, ms1.p, ms0.p, nullptr};
     const TV cnext[4] = {TV(0.5) * h, TV(0.5) * h, h, TV(0)};

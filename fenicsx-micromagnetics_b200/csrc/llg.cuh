@@ -74,6 +74,22 @@ struct LLGCtx {
   DevBuf<double> red;
   int64_t steps = 0, rhs_evals = 0;
   mutable int64_t launches = 0;
+  // CUDA graphs of one RK4 step (set_graph): three captures, one per phase of the Krylov
+  // extrapolation ring (each step advances every slot's ring by one, period 3), replayed in
+  // turn; dropped when dt, a field parameter or the solver state outside the graphs changes
+  bool graph_on = false, graph_ok = false;
+  cudaStream_t gstream = nullptr;
+  cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+  int gphase = 0, gwarm = 0;
+  double gdt = 0.0;
+  int64_t gepoch = -1, graph_replays = 0;
+  std::string graph_error;
+  void graph_reset();
+  void step_once(double dt, cudaStream_t s);
+  LLGCtx() = default;
+  LLGCtx(const LLGCtx&) = delete;
+  LLGCtx& operator=(const LLGCtx&) = delete;
+  ~LLGCtx();
   std::vector<double> diag_lin_host;        // [3N] diagonal of exchange + DMI (no anisotropy)
   std::vector<double> X_host, n_int_host;   // kept when DMI is on (adjoint set-up)
   std::vector<int32_t> tets_host;

@@ -68,6 +68,7 @@ SIGNATURES = {
     "spx_hmat_destroy": (C.c_int, [c_vp]),
     "spx_demag_create": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), C.POINTER(c_vp)]),
     "spx_demag_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_demag_ensemble_info": (C.c_int, [c_vp, c_vp]),
     "spx_demag_create_ensemble": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), c_i64, c_vp,
                                             c_i64, C.POINTER(c_vp)]),
     "spx_demag_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
@@ -100,6 +101,8 @@ SIGNATURES = {
     "spx_llg_set_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_get_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_step": (C.c_int, [c_vp, c_dbl, c_i64, c_vp]),
+    "spx_llg_set_graph": (C.c_int, [c_vp, c_i32]),
+    "spx_llg_graph_stats": (C.c_int, [c_vp, P_i64, P_i32]),
     "spx_llg_set_anisotropy_map": (C.c_int, [c_vp, c_vp]),
     "spx_llg_rhs_vjp": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_step_vjp": (C.c_int, [c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp, c_vp]),

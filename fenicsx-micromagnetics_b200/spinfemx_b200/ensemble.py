@@ -36,7 +36,7 @@ class LLGEnsemble:
 
     def __init__(self, meshes, Ms, *, Aex=0.0, Ku=0.0, n_ani=(0.0, 0.0, 1.0), D_int=0.0, n_int=(0.0, 0.0, 1.0),
                  alpha=0.5, gamma=2.211e5, H0=None, use_demag=True, dense_max_nb=4096, precision="mixed",
-                 demag_kwargs=None):
+                 demag_kwargs=None, graph=False):
         self.X, self.tets, self.offsets = ensemble_mesh(meshes)
         self.nsamples = len(self.offsets) - 1
         N = self.X.shape[0]
@@ -54,6 +54,8 @@ class LLGEnsemble:
                                   n_ani_vec=n_ani if Ku != 0.0 else None, D_int=D_int,
                                   n0_int_vec=n_int if D_int != 0.0 else None, alpha=alpha, gamma=gamma,
                                   use_demag=use_demag, demag_kwargs=dk, H0_static=H0n, precision=precision)
+        if graph:
+            self.hef.set_graph(True)
 
     def join(self, ms):
         """Union state (3N) from per-sample states [(3 N_s), ...]."""

@@ -180,6 +180,15 @@ class EffectiveField:
     def step(self, dt, nsteps=1):
         call("spx_llg_step", self._h, float(dt), int(nsteps), _lib.stream_ptr())
 
+    def set_graph(self, enable=True):
+        """Replay each RK4 step from captured CUDA graphs (same results as ordinary steps)."""
+        call("spx_llg_set_graph", self._h, 1 if enable else 0)
+
+    def graph_stats(self):
+        r, a = _lib.c_i64(), _lib.c_i32()
+        call("spx_llg_graph_stats", self._h, C.byref(r), C.byref(a))
+        return {"replayed_steps": r.value, "active": bool(a.value)}
+
     def run_host(self, m_host, dt, nsteps, out=None):
         """End-to-end call on host buffers (numpy or pinned torch CPU tensors)."""
         if out is None:

@@ -187,6 +187,9 @@ SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t
  * Lindholm operator of each sample's own boundary, dense (one batched launch for all dense
  * samples) when the sample's Nb <= dense_max_nb, else an H-matrix with opt->hmat.
  * opt->backend is ignored.  spx_demag_apply_transpose is not available for ensembles. */
+/* out6 = (samples, dense samples, dense block entries, boundary rows of the merged H-matrix of
+ * the other samples, its far-factor bytes, its near-tile bytes); zeros for a non-ensemble */
+SPX_API int spx_demag_ensemble_info(spx_demag d, int64_t* out6);
 SPX_API int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                       const spx_demag_options* opt, int64_t nsamples, const int64_t* node_offsets,
                                       int64_t dense_max_nb, spx_demag* out);
@@ -258,6 +261,15 @@ SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz
  *   spx_llg_step_jvp: one RK4 step of the state and of its tangent: m_out = step(m_n),
  *                     dm_out = d step . (dm, dKu, dH0); dKu: device N or NULL, dH0: host 3
  *                     or NULL. */
+/* CUDA graphs for spx_llg_step (no counterpart in the reference): with enable != 0, each RK4
+ * step is replayed from captured graphs (three captures, one per phase of the per-stage Krylov
+ * extrapolation history) after three ordinary steps; the graphs are recaptured when dt, the
+ * applied field, the Ku map or the solver tolerances change or when any other call used the
+ * demag solvers.  Results are those of ordinary steps.  spx_llg_graph_stats reports the steps
+ * replayed from graphs and whether graphs are active; if capture failed, stepping continues
+ * without graphs and spx_last_error holds the reason. */
+SPX_API int spx_llg_set_graph(spx_llg l, int32_t enable);
+SPX_API int spx_llg_graph_stats(spx_llg l, int64_t* replays, int32_t* active);
 SPX_API int spx_llg_set_anisotropy_map(spx_llg l, const double* Ku_nodes);
 SPX_API int spx_llg_rhs_vjp(spx_llg l, const double* m, const double* w, double* mbar, double* gKu, double* gH0,
                             spx_stream_t s);

@@ -112,3 +112,29 @@ def test_ensemble_trajectory_equals_per_sample(spx):
             for _ in range(nsteps):
                 mo = ollg.rk4_step(o.llg_rhs, mo, dt)
             assert np.abs(mE[k] - mo).max() < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_graph_replayed_steps_equal_ordinary_steps(spx, precision):
+    """RK4 steps replayed from CUDA graphs (with per-stage extrapolated Krylov starts) give the
+    ordinary steps' results exactly; a field change recaptures."""
+    ms = _meshes()
+    mu0 = 4e-7 * np.pi
+    dk = dict(precision=precision, ksp_rtol_u1=1e-10, ksp_rtol_u2=1e-10, warm_start="extrapolate_corrected", **HM)
+    runs = []
+    for graph in (False, True):
+        ens = spx.LLGEnsemble(ms, MAT["Ms"], Aex=MAT["Aex"], Ku=MAT["Ku"], D_int=MAT["D_int"], alpha=MAT["alpha"],
+                              H0=[[0.0, 0.0, b / mu0] for b in (0.3, -0.2, 0.45)], dense_max_nb=DENSE_MAX,
+                              precision=precision, demag_kwargs=dk)
+        ens.hef.set_graph(graph)
+        ens.set_state([_m0(Xs.shape[0], 30 + k) for k, (Xs, _) in enumerate(ms)])
+        ens.step(2e-14, 12)
+        a = ens.get_state().cpu().numpy()
+        ens.hef.set_uniform_field(0.0, 1e5, 0.0)
+        ens.step(2e-14, 7)
+        runs.append((a, ens.get_state().cpu().numpy(), ens.hef.graph_stats()))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert runs[1][2]["replayed_steps"] == 9 + 7 and runs[1][2]["active"]
+    assert runs[0][2]["replayed_steps"] == 0
