@@ -20,10 +20,13 @@ namespace spx {
 
 namespace {
 
+// n x n FP64 block -> rows of ld TM entries (zero padded)
 template <class TM>
-__global__ void k_to_tm(int64_t n, const double* __restrict__ src, TM* __restrict__ dst) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = static_cast<TM>(src[i]);
+__global__ void k_to_tm(int64_t n, int64_t ld, const double* __restrict__ src, TM* __restrict__ dst) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * ld) return;
+  const int64_t i = t / ld, j = t % ld;
+  dst[t] = j < n ? static_cast<TM>(src[i * n + j]) : TM(0);
 }
 
 template <class TV>
@@ -40,41 +43,70 @@ __global__ void k_scatter_rows(int64_t n, const int32_t* __restrict__ idx, const
   if (i < n) dst[idx[i]] = src[i];
 }
 
-// warp per dense boundary row r (concatenated over the dense samples):
-// g = B_s[i, :] . xb[b0_s : b0_s + nb_s],  gB[b0_s + i] = g,  phi[bverts[b0_s + i]] = u1 + g
+// row stride of a dense block: the row length rounded up to 16 bytes (zero padding)
+template <class TM>
+constexpr int64_t block_ld(int64_t n) {
+  return (n + (16 / sizeof(TM)) - 1) / (16 / sizeof(TM)) * (16 / sizeof(TM));
+}
+
+template <class TM> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int E = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int E = 2; };
+__device__ __forceinline__ void vec_elems(const float4& v, double e[4]) { e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w; }
+__device__ __forceinline__ void vec_elems(const double2& v, double e[2]) { e[0] = v.x; e[1] = v.y; }
+
+// CTA per tile of up to TILE_ROWS rows of one dense sample: the sample's boundary vector x
+// is staged in shared memory (FP64, nb_s <= dense_max_nb entries), then each warp streams
+// its rows of B_s as 16-byte vectors (rows padded to 16 bytes, four vectors in flight per
+// lane):  g = B_s[i, :] . x,  gB[b0_s + i] = g,  phi[bverts[b0_s + i]] = u1 + g.
+constexpr int TILE_ROWS = 64;
 template <class TV, class TM>
-__global__ void __launch_bounds__(256) k_block_gemv(int64_t nrows, int ndense, const int64_t* __restrict__ row0,
-                                                    const int64_t* __restrict__ b0, const int64_t* __restrict__ nbv,
-                                                    const int64_t* __restrict__ off, const TM* __restrict__ pool,
-                                                    const TV* __restrict__ xb, const int32_t* __restrict__ bverts,
-                                                    const TV* __restrict__ u1, TV* __restrict__ phi,
-                                                    TV* __restrict__ gB) {
-  const int lane = threadIdx.x & 31;
-  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
-  for (int64_t r = w; r < nrows; r += nw) {
-    int lo = 0, hi = ndense;  // row0[lo] <= r < row0[hi]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (row0[mid] <= r) lo = mid;
-      else hi = mid;
+__global__ void __launch_bounds__(256) k_block_gemv(const int32_t* __restrict__ tiles, const int64_t* __restrict__ b0,
+                                                    const int64_t* __restrict__ nbv, const int64_t* __restrict__ off,
+                                                    const TM* __restrict__ pool, const TV* __restrict__ xb,
+                                                    const int32_t* __restrict__ bverts, const TV* __restrict__ u1,
+                                                    TV* __restrict__ phi, TV* __restrict__ gB) {
+  extern __shared__ double xs[];
+  using VT = typename Vec16<TM>::T;
+  constexpr int E = Vec16<TM>::E;
+  const int q = tiles[2 * blockIdx.x], i0 = tiles[2 * blockIdx.x + 1];
+  const int64_t n = nbv[q], base = b0[q];
+  const int64_t nv = block_ld<TM>(n) / E;
+  for (int64_t j = threadIdx.x; j < nv * E; j += blockDim.x) xs[j] = j < n ? static_cast<double>(xb[base + j]) : 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int64_t i1 = std::min<int64_t>(n, i0 + TILE_ROWS);
+  for (int64_t i = i0 + wid; i < i1; i += nwarp) {
+    const VT* row = reinterpret_cast<const VT*>(pool + off[q] + i * nv * E);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    int64_t v = lane;
+    for (; v + 96 < nv; v += 128) {
+      VT w[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) w[t] = __ldcs(row + v + 32 * t);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        double e[E];
+        vec_elems(w[t], e);
+        const double* xv = xs + (v + 32 * t) * E;  // padding entries of B are zero
+#pragma unroll
+        for (int u = 0; u < E; ++u) acc[t] += e[u] * xv[u];
+      }
     }
-    const int64_t i = r - row0[lo], n = nbv[lo], base = b0[lo];
-    const TM* row = pool + off[lo] + i * n;
-    const TV* x = xb + base;
-    double acc0 = 0.0, acc1 = 0.0;
-    int64_t j = lane;
-    for (; j + 32 < n; j += 64) {
-      acc0 += static_cast<double>(row[j]) * static_cast<double>(x[j]);
-      acc1 += static_cast<double>(row[j + 32]) * static_cast<double>(x[j + 32]);
+    for (; v < nv; v += 32) {
+      double e[E];
+      vec_elems(__ldcs(row + v), e);
+      const int64_t c = v * E;
+#pragma unroll
+      for (int u = 0; u < E; ++u)
+        if (c + u < n) acc[0] += e[u] * xs[c + u];
     }
-    if (j < n) acc0 += static_cast<double>(row[j]) * static_cast<double>(x[j]);
-    const double g = warp_sum(acc0 + acc1);
+    const double g = warp_sum((acc[0] + acc[1]) + (acc[2] + acc[3]));
     if (lane == 0) {
       const TV y = static_cast<TV>(g);
       gB[base + i] = y;
-      const int32_t v = bverts[base + i];
-      phi[v] = u1[v] + y;
+      const int32_t vtx = bverts[base + i];
+      phi[vtx] = u1[vtx] + y;
     }
   }
 }
@@ -82,7 +114,7 @@ __global__ void __launch_bounds__(256) k_block_gemv(int64_t nrows, int ndense, c
 }  // namespace
 
 int64_t BlockBoundary::device_bytes() const {
-  int64_t t = static_cast<int64_t>(pool.bytes() + d_row0.bytes() + d_b0.bytes() + d_nb.bytes() + d_off.bytes());
+  int64_t t = static_cast<int64_t>(pool.bytes() + d_tiles.bytes() + d_b0.bytes() + d_nb.bytes() + d_off.bytes());
   for (const auto& h : H)
     if (h) t += h->device_bytes();
   if (Hm) t += Hm->device_bytes() + static_cast<int64_t>(hidx.bytes() + hmap.bytes() + gbh.bytes());
@@ -122,36 +154,47 @@ void block_boundary_build(BlockBoundary& bb, const BoundaryDev& bd, const double
       for (int q = 0; q < 4; ++q) stets[k].push_back(static_cast<int32_t>(tets[4 * e + q] - off[k]));
   }
   // dense blocks: B_s = fill(rows_s, rows_s) + diag(Omega/4pi - 1), stored in TM
-  std::vector<int64_t> row0(1, 0), db0, dnb, doff;
-  int64_t pos = 0;
+  SPX_CHECK(o.dense_max_nb <= 27000, "dense_max_nb above 27000 (the staged boundary vector must fit in 216 KB of "
+                                     "shared memory); larger samples use H-matrices");
+  std::vector<int64_t> db0, dnb, doff;
+  std::vector<int32_t> tiles;
+  int64_t pos = 0, entries = 0, rows = 0;
   for (int64_t k = 0; k < ns; ++k)
     if (bb.dense[k]) {
       db0.push_back(bb.b0[k]);
       dnb.push_back(bb.nb[k]);
       doff.push_back(pos);
-      pos += bb.nb[k] * bb.nb[k];
-      row0.push_back(row0.back() + bb.nb[k]);
+      pos += bb.nb[k] * block_ld<TM>(bb.nb[k]);
+      entries += bb.nb[k] * bb.nb[k];
+      rows += bb.nb[k];
+      for (int64_t i0 = 0; i0 < bb.nb[k]; i0 += TILE_ROWS) {
+        tiles.push_back(static_cast<int32_t>(db0.size() - 1));
+        tiles.push_back(static_cast<int32_t>(i0));
+      }
+      bb.max_ld = std::max<int64_t>(bb.max_ld, block_ld<TM>(bb.nb[k]));
     }
   bb.ndense = static_cast<int64_t>(db0.size());
-  bb.dense_rows = row0.back();
-  bb.dense_entries = pos;
+  bb.dense_rows = rows;
+  bb.ntiles = static_cast<int64_t>(tiles.size() / 2);
+  bb.dense_entries = entries;  // algorithmic (rows are stored padded to 16 bytes)
   bb.pool.alloc(std::max<int64_t>(pos, 1) * sizeof(TM));
   if (bb.ndense) {
     int64_t maxnb = 0;
     for (int64_t v : dnb) maxnb = std::max(maxnb, v);
     DevBuf<double> tmp(static_cast<size_t>(maxnb * maxnb));
-    DevBuf<int32_t> rows(static_cast<size_t>(maxnb));
+    DevBuf<int32_t> rows_d(static_cast<size_t>(maxnb));
     std::vector<int32_t> hr(maxnb);
     for (int64_t q = 0; q < bb.ndense; ++q) {
       const int64_t n = dnb[q];
       for (int64_t i = 0; i < n; ++i) hr[i] = static_cast<int32_t>(db0[q] + i);
-      SPX_CUDA(cudaMemcpyAsync(rows.p, hr.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-      bd.fill_block(rows.p, n, rows.p, n, tmp.p, s);
+      SPX_CUDA(cudaMemcpyAsync(rows_d.p, hr.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+      bd.fill_block(rows_d.p, n, rows_d.p, n, tmp.p, s);
       launch_add_diag(n, bd.omega_sum.p + db0[q], tmp.p, s);
-      k_to_tm<TM><<<grid_for(n * n, 256), 256, 0, s>>>(n * n, tmp.p, reinterpret_cast<TM*>(bb.pool.p) + doff[q]);
+      const int64_t ld = block_ld<TM>(n);
+      k_to_tm<TM><<<grid_for(n * ld, 256), 256, 0, s>>>(n, ld, tmp.p, reinterpret_cast<TM*>(bb.pool.p) + doff[q]);
       SPX_LAUNCH_CHECK();
     }
-    bb.d_row0.upload(row0, s);
+    bb.d_tiles.upload(tiles, s);
     bb.d_b0.upload(db0, s);
     bb.d_nb.upload(dnb, s);
     bb.d_off.upload(doff, s);
@@ -198,10 +241,13 @@ int block_boundary_apply(BlockBoundary& bb, int64_t Nb, const int32_t* bverts, c
   if (bb.ndense) {
     k_gather_b<TV><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, bverts, u1, xb);
     SPX_LAUNCH_CHECK();
-    const unsigned g = static_cast<unsigned>(std::min<int64_t>((bb.dense_rows + 7) / 8, 148 * 16));
-    k_block_gemv<TV, TM><<<g, 256, 0, s>>>(bb.dense_rows, static_cast<int>(bb.ndense), bb.d_row0.p, bb.d_b0.p,
-                                           bb.d_nb.p, bb.d_off.p, reinterpret_cast<const TM*>(bb.pool.p), xb, bverts,
-                                           u1, phi, gB);
+    const size_t smem = static_cast<size_t>(bb.max_ld) * sizeof(double);
+    if (smem > 48 * 1024)
+      SPX_CUDA(cudaFuncSetAttribute(k_block_gemv<TV, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+    k_block_gemv<TV, TM><<<static_cast<unsigned>(bb.ntiles), 256, smem, s>>>(
+        bb.d_tiles.p, bb.d_b0.p, bb.d_nb.p, bb.d_off.p, reinterpret_cast<const TM*>(bb.pool.p), xb, bverts, u1, phi,
+        gB);
     SPX_LAUNCH_CHECK();
     launches += 2;
   }

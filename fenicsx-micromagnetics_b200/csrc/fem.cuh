@@ -146,8 +146,8 @@ struct BlockBoundary {
   int64_t nsamples = 0;
   std::vector<int64_t> b0, nb;        // per sample: first boundary row (union order), count
   std::vector<int> dense;             // per sample: 1 dense block, 0 H-matrix
-  int64_t ndense = 0, dense_rows = 0, dense_entries = 0;
-  DevBuf<int64_t> d_row0;             // [ndense + 1] prefix of the dense samples' rows
+  int64_t ndense = 0, dense_rows = 0, dense_entries = 0, ntiles = 0, max_ld = 0;
+  DevBuf<int32_t> d_tiles;            // [ntiles][2]: dense sample, first row of a 64-row tile
   DevBuf<int64_t> d_b0, d_nb, d_off;  // per dense sample: boundary offset, Nb, pool offset
   DevBuf<char> pool;                  // dense blocks, row-major per sample (TM)
   std::vector<std::unique_ptr<HMatrix>> H;  // per sample while building (null for dense samples)
