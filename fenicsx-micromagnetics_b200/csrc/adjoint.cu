@@ -485,6 +485,7 @@ template <class TV, class TM>
 void LLGCtx<TV, TM>::adjoint_setup(cudaStream_t s) {
   LLGAdjoint<TV, TM>& A = adj;
   if (A.ready) return;
+  SPX_CHECK(!has_stt && !has_sot, "adjoint and tangent products do not include spin torques");
   const HostFem& fem = demag ? demag->fem : own_fem;
   const HostSell& hs = demag ? demag->hsell : own_sell;
   const int64_t nnz = fem.rowptr[N];

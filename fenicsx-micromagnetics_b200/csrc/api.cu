@@ -217,6 +217,8 @@ struct LLGBase {
   virtual void step_jvp(const double* mn, const double* dm, const double* dKu, const double* dH0, double dt,
                         double* mo, double* dmo, cudaStream_t s) = 0;
   virtual void set_ku_map(const double* ku) = 0;
+  virtual void zhang_li(const double* m, double* out, cudaStream_t s) = 0;
+  virtual void set_sot(double Hdl, double Hfl, const double* p) = 0;
   virtual void set_graph(int on) = 0;
   virtual void graph_stats(int64_t* replays, int32_t* active) const = 0;
   virtual std::string graph_error() const = 0;
@@ -333,6 +335,15 @@ struct LLGImpl : LLGBase {
   void set_ku_map(const double* ku) override {
     l.graph_reset();
     l.set_ku_map(ku, 0);
+  }
+  void zhang_li(const double* m, double* o, cudaStream_t s) override {
+    TV* q = outbuf(o);
+    l.zhang_li(in(m, s), q, s);
+    out(o, s);
+  }
+  void set_sot(double Hdl, double Hfl, const double* p) override {
+    l.graph_reset();
+    l.set_sot(Hdl, Hfl, p, 0);
   }
   void set_graph(int on) override {
     l.graph_reset();
@@ -939,6 +950,8 @@ static LLGParams to_params(const spx_llg_params* p) {
   q.D_int = p->D_int; q.n_int = p->n_int; q.H0_nodes = p->H0_nodes;
   for (int c = 0; c < 3; ++c) q.H0_uniform[c] = p->H0_uniform[c];
   q.use_demag = p->use_demag;
+  q.stt_J = p->stt_J; q.stt_P = p->stt_P; q.stt_beta = p->stt_beta; q.stt_dir = p->stt_dir;
+  q.sot_Hdl = p->sot_Hdl; q.sot_Hfl = p->sot_Hfl; q.sot_p = p->sot_p;
   SPX_CHECK(!((q.Ku != 0.0 || q.Ku_nodes) && !q.n_ani), "anisotropy needs easy axes (n_ani)");
   return q;
 }
@@ -1093,6 +1106,20 @@ int spx_llg_step_jvp(spx_llg l, const double* m_n, const double* dm, const doubl
   REQUIRE(l); REQUIRE(m_n); REQUIRE(dm); REQUIRE(m_out); REQUIRE(dm_out);
   SPX_CHECK(dt > 0.0, "dt must be positive");
   l->impl->step_jvp(m_n, dm, dKu, dH0, dt, m_out, dm_out, S(s));
+  API_END
+}
+
+int spx_llg_zhang_li(spx_llg l, const double* m, double* out, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m); REQUIRE(out);
+  l->impl->zhang_li(m, out, S(s));
+  API_END
+}
+
+int spx_llg_set_sot(spx_llg l, double H_dl, double H_fl, const double* polarization) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->set_sot(H_dl, H_fl, polarization);
   API_END
 }
 

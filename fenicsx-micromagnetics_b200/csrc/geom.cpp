@@ -246,6 +246,34 @@ void assemble_fem(const double* X, int64_t N, const int32_t* tets, int64_t E, Ho
   }
 }
 
+// Zhang-Li advection operator (gpu/solvers/llg_stt_module_GPU.py:402-429): the P1 form
+// int (J . grad u) v dx with the nodal (P1) current-direction field J, on the node pattern,
+// unscaled.  Per tetrahedron grad(phi_b) is constant and int phi_a phi_k = vol/20 (1 + d_ak).
+void assemble_zhang_li(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const double* J,
+                       std::vector<double>& K) {
+  const int64_t nnz = fem.rowptr[fem.N];
+  K.assign(nnz, 0.0);
+  auto find = [&](int32_t i, int32_t j) -> int64_t {
+    const int32_t* b = fem.col.data() + fem.rowptr[i];
+    const int32_t* e = fem.col.data() + fem.rowptr[i + 1];
+    return fem.rowptr[i] + (std::lower_bound(b, e, j) - b);
+  };
+  for (int64_t e = 0; e < E; ++e) {
+    const int32_t* t = tets + 4 * e;
+    double g[4][3], vol;
+    tet_grads(X, t, g, &vol);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        double sum = 0.0;
+        for (int k = 0; k < 4; ++k) {
+          const double* Jk = J + 3 * static_cast<int64_t>(t[k]);
+          sum += vol / 20.0 * (a == k ? 2.0 : 1.0) * (Jk[0] * g[b][0] + Jk[1] * g[b][1] + Jk[2] * g[b][2]);
+        }
+        K[find(t[a], t[b])] += sum;
+      }
+  }
+}
+
 void assemble_dmi_interfacial(const double* X, const int32_t* tets, int64_t E, const HostFem& fem,
                               const HostBoundary& bd, const double* nN, std::vector<double>& B9) {
   const int64_t nnz = fem.rowptr[fem.N];

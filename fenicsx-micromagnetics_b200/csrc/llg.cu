@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
     const TV mx = a.m[3 * i], my = a.m[3 * i + 1], mz = a.m[3 * i + 2];
     const TV pi = DEMAG ? a.phi[i] : TV(0);
     TV hx = 0, hy = 0, hz = 0;
+    TV zx = 0, zy = 0, zz = 0;  // Zhang-Li (J . grad) m / V_i
     for (int k = 0; k < width; ++k) {
       const int64_t idx = base + ((int64_t)k << 5) + lane;
       const int64_t j = a.col[idx];
@@ -43,6 +44,12 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
       hx += e * dx;
       hy += e * dy;
       hz += e * dz;
+      if (a.Kz) {
+        const TV kz = static_cast<TV>(a.Kz[idx]);
+        zx += kz * dx;
+        zy += kz * dy;
+        zz += kz * dz;
+      }
       if (DMI) {
         const TM* K = a.Kd + idx;
         const int64_t L = a.L;
@@ -84,14 +91,34 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
       a.out[3 * i] = hx;
       a.out[3 * i + 1] = hy;
       a.out[3 * i + 2] = hz;
+      if (a.zout) {
+        a.zout[3 * i] = zx;
+        a.zout[3 * i + 1] = zy;
+        a.zout[3 * i + 2] = zz;
+      }
       continue;
     }
     const TV cx = my * hz - mz * hy, cy = mz * hx - mx * hz, cz = mx * hy - my * hx;
     const TV ccx = my * cz - mz * cy, ccy = mz * cx - mx * cz, ccz = mx * cy - my * cx;
     const TV s = a.stab * (TV(1) - (mx * mx + my * my + mz * mz));
-    const TV rx = a.pref * (a.precess * cx + a.alpha * ccx) + s * mx;
-    const TV ry = a.pref * (a.precess * cy + a.alpha * ccy) + s * my;
-    const TV rz = a.pref * (a.precess * cz + a.alpha * ccz) + s * mz;
+    TV rx = a.pref * (a.precess * cx + a.alpha * ccx) + s * mx;
+    TV ry = a.pref * (a.precess * cy + a.alpha * ccy) + s * my;
+    TV rz = a.pref * (a.precess * cz + a.alpha * ccz) + s * mz;
+    if (a.Kz) {  // - prefZ (stt_a m x z + stt_b m x (m x z))   (llg_stt_module_GPU.py:101-139)
+      const TV qx = my * zz - mz * zy, qy = mz * zx - mx * zz, qz = mx * zy - my * zx;
+      const TV qqx = my * qz - mz * qy, qqy = mz * qx - mx * qz, qqz = mx * qy - my * qx;
+      rx -= a.prefZ * (a.stt_a * qx + a.stt_b * qqx);
+      ry -= a.prefZ * (a.stt_a * qy + a.stt_b * qqy);
+      rz -= a.prefZ * (a.stt_a * qz + a.stt_b * qqz);
+    }
+    if (a.sot_p) {  // + c_fl m x p + c_dl m x (m x p)   (llg_SOT_module_GPU.py:170-205)
+      const TV px = a.sot_p[3 * i], py = a.sot_p[3 * i + 1], pz = a.sot_p[3 * i + 2];
+      const TV qx = my * pz - mz * py, qy = mz * px - mx * pz, qz = mx * py - my * px;
+      const TV qqx = my * qz - mz * qy, qqy = mz * qx - mx * qz, qqz = mx * qy - my * qx;
+      rx += a.c_fl * qx + a.c_dl * qqx;
+      ry += a.c_fl * qy + a.c_dl * qqy;
+      rz += a.c_fl * qz + a.c_dl * qqz;
+    }
     if (a.mode == 1) {
       a.out[3 * i] = rx;
       a.out[3 * i + 1] = ry;
@@ -122,7 +149,7 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
 template <class TV, class TM, bool DMI, bool ANI>
 __global__ void __launch_bounds__(256) k_jv(StageArgs<TV, TM> a, const TV* __restrict__ Ms,
                                             const TV* __restrict__ Hm, const TV* __restrict__ v,
-                                            TV* __restrict__ out, TV gamma) {
+                                            TV* __restrict__ out, TV gamma, const TV* __restrict__ Zm) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
@@ -133,12 +160,17 @@ __global__ void __launch_bounds__(256) k_jv(StageArgs<TV, TM> a, const TV* __res
     const int width = static_cast<int>((a.sp[sl + 1] - base) >> 5);
     const TV vx = v[3 * i], vy = v[3 * i + 1], vz = v[3 * i + 2];
     TV hvx = 0, hvy = 0, hvz = 0;
+    TV jvx = 0, jvy = 0, jvz = 0;  // Z(v)
     for (int k = 0; k < width; ++k) {
       const int64_t idx = base + ((int64_t)k << 5) + lane;
       const int64_t j = a.col[idx];
       const TV x = v[3 * j] - vx, y = v[3 * j + 1] - vy, z = v[3 * j + 2] - vz;
       const TV e = static_cast<TV>(a.Kex[idx]);
       hvx += e * x; hvy += e * y; hvz += e * z;
+      if (a.Kz) {
+        const TV kz = static_cast<TV>(a.Kz[idx]);
+        jvx += kz * x; jvy += kz * y; jvz += kz * z;
+      }
       if (DMI) {
         const TM* K = a.Kd + idx;
         const int64_t L = a.L;
@@ -174,21 +206,114 @@ __global__ void __launch_bounds__(256) k_jv(StageArgs<TV, TM> a, const TV* __res
     const TV dampz = vz * mdHm - TV(2) * hz * mdv + mz * common - hvz * mdmm;
     const TV coef = -gamma / (TV(1) + a.alpha * a.alpha);
     const TV sc = a.stab * (TV(1) - mdmm);
-    out[3 * i] = coef * (a.precess * (cvx + cmx) + a.alpha * dampx) + sc * vx - TV(2) * a.stab * mx * mdv;
-    out[3 * i + 1] = coef * (a.precess * (cvy + cmy) + a.alpha * dampy) + sc * vy - TV(2) * a.stab * my * mdv;
-    out[3 * i + 2] = coef * (a.precess * (cvz + cmz) + a.alpha * dampz) + sc * vz - TV(2) * a.stab * mz * mdv;
+    TV ox = coef * (a.precess * (cvx + cmx) + a.alpha * dampx) + sc * vx - TV(2) * a.stab * mx * mdv;
+    TV oy = coef * (a.precess * (cvy + cmy) + a.alpha * dampy) + sc * vy - TV(2) * a.stab * my * mdv;
+    TV oz = coef * (a.precess * (cvz + cmz) + a.alpha * dampz) + sc * vz - TV(2) * a.stab * mz * mdv;
+    if (a.Kz) {  // _JAC_VEC_STT_KERNEL (llg_stt_module_GPU.py:142-215), jm = Z(m_state), jv = Z(v)
+      const TV jmx = Zm[3 * i], jmy = Zm[3 * i + 1], jmz = Zm[3 * i + 2];
+      const TV mjx = my * jvz - mz * jvy, mjy = mz * jvx - mx * jvz, mjz = mx * jvy - my * jvx;
+      const TV vjx = vy * jmz - vz * jmy, vjy = vz * jmx - vx * jmz, vjz = vx * jmy - vy * jmx;
+      const TV MjV = mx * jvx + my * jvy + mz * jvz, VjM = vx * jmx + vy * jmy + vz * jmz;
+      const TV MjM = mx * jmx + my * jmy + mz * jmz;
+      const TV pa = -a.stt_a * a.prefZ, pb = -a.stt_b * a.prefZ;
+      ox += pa * (mjx + vjx) + pb * (vx * MjM + mx * VjM + mx * MjV - jvx * mdmm - TV(2) * jmx * mdv);
+      oy += pa * (mjy + vjy) + pb * (vy * MjM + my * VjM + my * MjV - jvy * mdmm - TV(2) * jmy * mdv);
+      oz += pa * (mjz + vjz) + pb * (vz * MjM + mz * VjM + mz * MjV - jvz * mdmm - TV(2) * jmz * mdv);
+    }
+    if (a.sot_p) {  // _JAC_VEC_SOT_KERNEL (llg_SOT_module_GPU.py:208-275)
+      const TV px = a.sot_p[3 * i], py = a.sot_p[3 * i + 1], pz = a.sot_p[3 * i + 2];
+      const TV qx = my * pz - mz * py, qy = mz * px - mx * pz, qz = mx * py - my * px;
+      const TV dx = vy * pz - vz * py, dy = vz * px - vx * pz, dz = vx * py - vy * px;
+      ox += a.c_fl * dx + a.c_dl * ((vy * qz - vz * qy) + (my * dz - mz * dy));
+      oy += a.c_fl * dy + a.c_dl * ((vz * qx - vx * qz) + (mz * dx - mx * dz));
+      oz += a.c_fl * dz + a.c_dl * ((vx * qy - vy * qx) + (mx * dy - my * dx));
+    }
+    out[3 * i] = ox;
+    out[3 * i + 1] = oy;
+    out[3 * i + 2] = oz;
+  }
+}
+
+// spin torques of the 3x3 block preconditioner: STT (G = Z(m_state), c3, c4:
+// _PC_BUILD_INV3_STT_KERNEL, llg_stt_module_GPU.py:218-393) or SOT (column-wise local
+// Jacobian with per-component diagonal, _PC_BUILD_INV3_SOT_KERNEL, llg_SOT_module_GPU.py:278-437)
+struct PcTorque {
+  const void* G;  // TV [3n] or null
+  double c3, c4;
+  const void* P;  // TV [3n] (SOT polarisation) or null
+  double pref, alpha, precess, c_fl, c_dl;
+};
+
+// column c of the local SOT Jacobian: Jv_SOT with v = e_c and H_v = k e_c
+__device__ __forceinline__ void sot_column(const double m[3], const double h[3], const double p[3], int c, double k,
+                                           const PcTorque& t, double Stab, double out[3]) {
+  double v[3] = {0.0, 0.0, 0.0}, hv[3] = {0.0, 0.0, 0.0};
+  v[c] = 1.0;
+  hv[c] = k;
+  auto cross = [](const double a[3], const double b[3], double r[3]) {
+    r[0] = a[1] * b[2] - a[2] * b[1];
+    r[1] = a[2] * b[0] - a[0] * b[2];
+    r[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double cv[3], cm[3], q[3], dq[3], vq[3], mdq[3];
+  cross(v, h, cv);
+  cross(m, hv, cm);
+  const double mdH = m[0] * h[0] + m[1] * h[1] + m[2] * h[2];
+  const double mdHv = m[0] * hv[0] + m[1] * hv[1] + m[2] * hv[2];
+  const double vdH = v[0] * h[0] + v[1] * h[1] + v[2] * h[2];
+  const double mdv = m[0] * v[0] + m[1] * v[1] + m[2] * v[2];
+  const double mdm = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const double common = vdH + mdHv;
+  cross(m, p, q);
+  cross(v, p, dq);
+  cross(v, q, vq);
+  cross(m, dq, mdq);
+  const double sc = Stab * (1.0 - mdm);
+  for (int r = 0; r < 3; ++r) {
+    const double damp = v[r] * mdH - 2.0 * h[r] * mdv + m[r] * common - hv[r] * mdm;
+    out[r] = t.pref * (t.precess * (cv[r] + cm[r]) + t.alpha * damp) + t.c_fl * dq[r] + t.c_dl * (vq[r] + mdq[r]) +
+             sc * v[r] - 2.0 * Stab * m[r] * mdv;
   }
 }
 
 template <class TV>
 __global__ void k_pc_build(int64_t n, const TV* __restrict__ M, const TV* __restrict__ H, const TV* __restrict__ D,
                            int include_stab, int use_abs_kappa, double shift, double eps_reg, double det_eps,
-                           double c1, double c2, double Stab, TV* __restrict__ inv) {
+                           double c1, double c2, double Stab, PcTorque tq, TV* __restrict__ inv) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double mx = M[3 * i], my = M[3 * i + 1], mz = M[3 * i + 2];
   const double hx = H[3 * i], hy = H[3 * i + 1], hz = H[3 * i + 2];
   const double dex = D[3 * i], dey = D[3 * i + 1], dez = D[3 * i + 2];
+  if (tq.P) {  // SOT: columns of the local Jacobian, then the same inverse with its own det guard
+    const TV* Pp = static_cast<const TV*>(tq.P);
+    const double m3[3] = {mx, my, mz}, h3[3] = {hx, hy, hz};
+    const double p3[3] = {static_cast<double>(Pp[3 * i]), static_cast<double>(Pp[3 * i + 1]),
+                          static_cast<double>(Pp[3 * i + 2])};
+    const double kd[3] = {use_abs_kappa ? fabs(dex) : dex, use_abs_kappa ? fabs(dey) : dey,
+                          use_abs_kappa ? fabs(dez) : dez};
+    double Jc[3][3];
+    for (int c = 0; c < 3; ++c) sot_column(m3, h3, p3, c, kd[c], tq, Stab, Jc[c]);
+    const double s = shift + eps_reg;
+    double A[3][3];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) A[r][c] = (r == c ? s : 0.0) - Jc[c][r];
+    double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) - A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                 A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    if (fabs(det) < det_eps) det += (det >= 0.0 ? 1.0 : -1.0) * det_eps;
+    const double id = 1.0 / det;
+    TV* o = inv + 9 * i;
+    o[0] = static_cast<TV>((A[1][1] * A[2][2] - A[1][2] * A[2][1]) * id);
+    o[1] = static_cast<TV>(-(A[0][1] * A[2][2] - A[0][2] * A[2][1]) * id);
+    o[2] = static_cast<TV>((A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id);
+    o[3] = static_cast<TV>(-(A[1][0] * A[2][2] - A[1][2] * A[2][0]) * id);
+    o[4] = static_cast<TV>((A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id);
+    o[5] = static_cast<TV>(-(A[0][0] * A[1][2] - A[0][2] * A[1][0]) * id);
+    o[6] = static_cast<TV>((A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id);
+    o[7] = static_cast<TV>(-(A[0][0] * A[2][1] - A[0][1] * A[2][0]) * id);
+    o[8] = static_cast<TV>((A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id);
+    return;
+  }
   const double kappa = use_abs_kappa ? (fabs(dex) + fabs(dey) + fabs(dez)) / 3.0 : (dex + dey + dez) / 3.0;
   const double mdH = mx * hx + my * hy + mz * hz;
   const double mdm = mx * mx + my * my + mz * mz;
@@ -207,6 +332,26 @@ __global__ void k_pc_build(int64_t n, const TV* __restrict__ M, const TV* __rest
     const double m3[3] = {mx, my, mz};
     for (int r = 0; r < 3; ++r)
       for (int c = 0; c < 3; ++c) J[r][c] += Stab * ((r == c ? s0 : 0.0) - 2.0 * m3[r] * m3[c]);
+  }
+  if (tq.G) {  // STT: c3 [g]x-like terms and c4 B(g)
+    const TV* Gp = static_cast<const TV*>(tq.G);
+    const double gx = Gp[3 * i], gy = Gp[3 * i + 1], gz = Gp[3 * i + 2];
+    const double mdG = mx * gx + my * gy + mz * gz;
+    J[0][1] += tq.c3 * (-gz);
+    J[0][2] += tq.c3 * gy;
+    J[1][0] += tq.c3 * gz;
+    J[1][2] += tq.c3 * (-gx);
+    J[2][0] += tq.c3 * (-gy);
+    J[2][1] += tq.c3 * gx;
+    J[0][0] += tq.c4 * (mdG - gx * mx);
+    J[1][1] += tq.c4 * (mdG - gy * my);
+    J[2][2] += tq.c4 * (mdG - gz * mz);
+    J[0][1] += tq.c4 * (mx * gy - 2.0 * gx * my);
+    J[0][2] += tq.c4 * (mx * gz - 2.0 * gx * mz);
+    J[1][0] += tq.c4 * (my * gx - 2.0 * gy * mx);
+    J[1][2] += tq.c4 * (my * gz - 2.0 * gy * mz);
+    J[2][0] += tq.c4 * (mz * gx - 2.0 * gz * mx);
+    J[2][1] += tq.c4 * (mz * gy - 2.0 * gz * my);
   }
   const double s = shift + eps_reg;
   double A[3][3];
@@ -372,6 +517,27 @@ void LLGCtx<TV, TM>::create(DemagCtx<TV, TM>* dm, const double* X, int64_t N_, c
   h0[0] = p.H0_uniform[0];
   h0[1] = p.H0_uniform[1];
   h0[2] = p.H0_uniform[2];
+  has_stt = p.stt_dir != nullptr;
+  has_sot = p.sot_p != nullptr;
+  SPX_CHECK(!(has_stt && has_sot), "STT and SOT together are not supported (separate solvers in the reference)");
+  if (has_stt) {
+    // prefZhang = J P muB / (e Ms (1 + beta^2)) / (1 + alpha^2) / 1e-9 (llg_stt_module_GPU.py:571-578)
+    const double e = 1.6021766e-19, muB = 9.27400915e-24;
+    prefZ = p.stt_J * p.stt_P * muB / (e * p.Ms * (1.0 + p.stt_beta * p.stt_beta)) / (1.0 + p.alpha * p.alpha) / 1e-9;
+    stt_a = p.stt_beta - p.alpha;
+    stt_b = 1.0 + p.alpha * p.stt_beta;
+    c3 = (p.stt_beta - p.alpha) * prefZ;
+    c4 = -(1.0 + p.alpha * p.stt_beta) * prefZ;
+    std::vector<double> kz;
+    assemble_zhang_li(X, tets, E, *fem, p.stt_dir, kz);
+    for (int64_t i = 0; i < N; ++i)
+      for (int64_t k = fem->rowptr[i]; k < fem->rowptr[i + 1]; ++k) kz[k] /= fem->vol[i];
+    sell_values<TM>(*hs, kz.data(), 1, true, nnz, 1.0, v);
+    Kz.upload(v, s);
+    Zm.alloc(3 * N);
+    Zm.zero(s);
+  }
+  if (has_sot) set_sot(p.sot_Hdl, p.sot_Hfl, p.sot_p, s);
   use_demag = (dm != nullptr) && p.use_demag;
   m.alloc(3 * N); ms0.alloc(3 * N); ms1.alloc(3 * N); acc.alloc(3 * N);
   Mstate.alloc(3 * N); Hm.alloc(3 * N); pcinv.alloc(9 * N);
@@ -406,6 +572,14 @@ StageArgs<TV, TM> LLGCtx<TV, TM>::args(const TV* min, TV* out, int mode, bool wi
   a.precess = static_cast<TV>(prm.do_precess);
   a.stab = static_cast<TV>(stab);
   a.mode = mode;
+  a.Kz = has_stt ? Kz.p : nullptr;
+  a.zout = nullptr;
+  a.prefZ = static_cast<TV>(prefZ);
+  a.stt_a = static_cast<TV>(stt_a);
+  a.stt_b = static_cast<TV>(stt_b);
+  a.sot_p = has_sot ? sotp.p : nullptr;
+  a.c_fl = static_cast<TV>(c_fl);
+  a.c_dl = static_cast<TV>(c_dl);
   return a;
 }
 
@@ -552,7 +726,9 @@ void LLGCtx<TV, TM>::step_once(double dt, cudaStream_t s) {
 template <class TV, class TM>
 void LLGCtx<TV, TM>::update_jac_state(const TV* min, cudaStream_t s) {
   SPX_CUDA(cudaMemcpyAsync(Mstate.p, min, 3 * N * sizeof(TV), cudaMemcpyDeviceToDevice, s));
-  launch_stage(args(Mstate.p, Hm.p, 0, false), false, s);
+  StageArgs<TV, TM> a = args(Mstate.p, Hm.p, 0, false);
+  if (has_stt) a.zout = Zm.p;
+  launch_stage(a, false, s);
 }
 
 template <class TV, class TM>
@@ -560,19 +736,69 @@ void LLGCtx<TV, TM>::jv(const TV* v, TV* out, cudaStream_t s) {
   StageArgs<TV, TM> a = args(Mstate.p, out, 0, false);
   const unsigned g = grid_for(a.nslices * 32, 256);
   const TV gam = static_cast<TV>(prm.gamma);
-  if (has_dmi && has_ani) k_jv<TV, TM, true, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else if (has_dmi) k_jv<TV, TM, true, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else if (has_ani) k_jv<TV, TM, false, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
-  else k_jv<TV, TM, false, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam);
+  const TV* zm = has_stt ? Zm.p : nullptr;
+  if (has_dmi && has_ani) k_jv<TV, TM, true, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam, zm);
+  else if (has_dmi) k_jv<TV, TM, true, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam, zm);
+  else if (has_ani) k_jv<TV, TM, false, true><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam, zm);
+  else k_jv<TV, TM, false, false><<<g, 256, 0, s>>>(a, Mstate.p, Hm.p, v, out, gam, zm);
   SPX_LAUNCH_CHECK();
 }
 
 template <class TV, class TM>
 void LLGCtx<TV, TM>::pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s) {
+  PcTorque tq{};
+  if (has_stt) {
+    tq.G = Zm.p;
+    tq.c3 = c3;
+    tq.c4 = c4;
+  }
+  if (has_sot) {
+    tq.P = sotp.p;
+    tq.pref = pref;
+    tq.alpha = prm.alpha;
+    tq.precess = prm.do_precess;
+    tq.c_fl = c_fl;
+    tq.c_dl = c_dl;
+  }
   k_pc_build<TV><<<grid_for(N, 256), 256, 0, s>>>(N, Mstate.p, Hm.p, diagK.p, include_stab, use_abs_kappa, shift,
-                                                  1e-14, 1e-30, c1, c2, stab, pcinv.p);
+                                                  1e-14, 1e-30, c1, c2, stab, tq, pcinv.p);
   SPX_LAUNCH_CHECK();
   pc_ready = true;
+}
+
+template <class TV, class TM>
+void LLGCtx<TV, TM>::zhang_li(const TV* min, TV* out, cudaStream_t s) {
+  SPX_CHECK(has_stt, "no spin-transfer torque configured");
+  DevBuf<TV> tmp(3 * N);
+  StageArgs<TV, TM> a = args(min, tmp.p, 0, false);
+  a.zout = out;
+  launch_stage(a, false, s);
+  SPX_CUDA(cudaStreamSynchronize(s));
+}
+
+template <class TV, class TM>
+void LLGCtx<TV, TM>::set_sot(double Hdl, double Hfl, const double* p_nodes, cudaStream_t s) {
+  // c_fl = -gamma (H_fl - alpha H_dl) / (1 + alpha^2), c_dl = -gamma (H_dl + alpha H_fl) / (1 + alpha^2)
+  // (llg_SOT_module_GPU.py:814-817)
+  prm.sot_Hdl = Hdl;
+  prm.sot_Hfl = Hfl;
+  const double den = 1.0 + prm.alpha * prm.alpha;
+  c_fl = -prm.gamma * (Hfl - prm.alpha * Hdl) / den;
+  c_dl = -prm.gamma * (Hdl + prm.alpha * Hfl) / den;
+  if (p_nodes) {
+    std::vector<TV> pp(3 * N);
+    for (int64_t i = 0; i < N; ++i) {
+      const double a = p_nodes[3 * i], b = p_nodes[3 * i + 1], c = p_nodes[3 * i + 2];
+      const double r = std::sqrt(a * a + b * b + c * c);
+      const double sc = r > 0.0 ? 1.0 / r : 1.0;
+      pp[3 * i] = static_cast<TV>(a * sc);
+      pp[3 * i + 1] = static_cast<TV>(b * sc);
+      pp[3 * i + 2] = static_cast<TV>(c * sc);
+    }
+    sotp.upload(pp, s);
+    has_sot = true;
+  }
+  SPX_CHECK(has_sot, "SOT needs a polarisation field");
 }
 
 template <class TV, class TM>

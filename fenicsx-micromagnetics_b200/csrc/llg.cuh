@@ -16,6 +16,12 @@ struct LLGParams {
   const double* H0_nodes = nullptr;  // [3N] static field (A/m)
   double H0_uniform[3] = {0.0, 0.0, 0.0};
   int use_demag = 1;
+  // Zhang-Li spin-transfer torque (gpu/solvers/llg_stt_module_GPU.py)
+  double stt_J = 0.0, stt_P = 0.0, stt_beta = 0.0;
+  const double* stt_dir = nullptr;   // [3N] current direction (null: no STT)
+  // spin-orbit torque (gpu/solvers/llg_SOT_module_GPU.py)
+  double sot_Hdl = 0.0, sot_Hfl = 0.0;
+  const double* sot_p = nullptr;     // [3N] polarisation (null: no SOT)
 };
 
 // Arguments of the fused stage kernel k_stage (llg.cu)
@@ -42,6 +48,13 @@ struct StageArgs {
   TV pref, alpha, precess, stab;
   TV c_next, w_acc, dt6;
   int mode, stage;
+  // spin torques: Zhang-Li operator (row-scaled, rows sum to zero; null: no STT) and its
+  // output in mode 0 (zout, may be null); SOT polarisation (null: no SOT)
+  const TM* Kz;
+  TV* zout;
+  TV prefZ, stt_a, stt_b;
+  const TV* sot_p;
+  TV c_fl, c_dl;
 };
 
 // Work data of the adjoint and tangent products (adjoint.cu), built on first use.
@@ -71,6 +84,10 @@ struct LLGCtx {
   double pref = 0, stab = 0, c1 = 0, c2 = 0;
   bool has_dmi = false, has_ani = false, use_demag = false, pc_ready = false;
   DevBuf<TV> m, ms0, ms1, acc, Mstate, Hm, pcinv;
+  DevBuf<TM> Kz;              // Zhang-Li operator / V_i on the node pattern (STT)
+  DevBuf<TV> Zm, sotp;        // Z(M_state) (Jv / PC state), SOT polarisation
+  bool has_stt = false, has_sot = false;
+  double prefZ = 0.0, stt_a = 0.0, stt_b = 0.0, c_fl = 0.0, c_dl = 0.0, c3 = 0.0, c4 = 0.0;
   DevBuf<double> red;
   int64_t steps = 0, rhs_evals = 0;
   mutable int64_t launches = 0;
@@ -104,7 +121,12 @@ struct LLGCtx {
   void step_rk4(double dt, int64_t nsteps, cudaStream_t s);
   void update_jac_state(const TV* m, cudaStream_t s);
   void jv(const TV* v, TV* out, cudaStream_t s);
+  // mode 0: LLG (+ STT terms when STT is on, JvContextSTT); 2: SOT column-wise build
+  // (JvContextSOT.update_pc_full_fast_gpu(shift, use_abs_diag)), use_abs_kappa = use_abs_diag
   void pc_build(double shift, int include_stab, int use_abs_kappa, cudaStream_t s);
+  // Z(m) = (J . grad) m / V_i (ZhangLiGPU.compute_vec)
+  void zhang_li(const TV* m, TV* out, cudaStream_t s);
+  void set_sot(double Hdl, double Hfl, const double* p_nodes, cudaStream_t s);
   void pc_apply(const TV* x, TV* y, cudaStream_t s);
   // adjoint / tangent products (adjoint.cu).  gKu [N] and gH0 [3] are FP64 device
   // accumulators (+=), either may be null.

@@ -134,6 +134,10 @@ void assemble_dmi_interfacial(const double* X, const int32_t* tets, int64_t E, c
                               const HostBoundary& bd, const double* n_nodes,
                               std::vector<double>& blocks9);
 
+// Zhang-Li operator int (J . grad u) v dx on the node pattern (unscaled), J nodal [3N].
+void assemble_zhang_li(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const double* J,
+                       std::vector<double>& K);
+
 // Cluster tree of gpu/fields/lindholm_hmatrix_gpu/tree.py:41-96 (bit-exact permutation).
 struct TreeNode {
   int32_t start, stop;

@@ -14,6 +14,10 @@ _EXPORTS = {
     "DemagFieldLindholmGPU": ".demag",
     "EffectiveField": ".llg",
     "JvContext": ".llg",
+    "EffectiveFieldSTTGPU": ".llg",
+    "EffectiveFieldSOTGPU": ".llg",
+    "JvContextSTT": ".llg",
+    "JvContextSOT": ".llg",
     "LLG_GPU": ".llg",
     "HMatrixGPUPackedFused": ".hmatrix",
     "HMatrixBuildConfig": ".hmatrix",

@@ -34,7 +34,9 @@ class DemagOptions(C.Structure):
 class LLGParams(C.Structure):
     _fields_ = [("Ms", c_dbl), ("gamma", c_dbl), ("alpha", c_dbl), ("do_precess", c_dbl), ("Aex", c_dbl),
                 ("Ku", c_dbl), ("Ku_nodes", c_vp), ("n_ani", c_vp), ("D_int", c_dbl), ("n_int", c_vp),
-                ("H0_nodes", c_vp), ("H0_uniform", c_dbl * 3), ("use_demag", c_i32), ("precision", c_i32)]
+                ("H0_nodes", c_vp), ("H0_uniform", c_dbl * 3), ("use_demag", c_i32), ("precision", c_i32),
+                ("stt_J", c_dbl), ("stt_P", c_dbl), ("stt_beta", c_dbl), ("stt_dir", c_vp),
+                ("sot_Hdl", c_dbl), ("sot_Hfl", c_dbl), ("sot_p", c_vp)]
 
 
 # name -> (restype, argtypes)
@@ -101,6 +103,8 @@ SIGNATURES = {
     "spx_llg_set_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_get_state": (C.c_int, [c_vp, c_vp, c_vp]),
     "spx_llg_step": (C.c_int, [c_vp, c_dbl, c_i64, c_vp]),
+    "spx_llg_zhang_li": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_llg_set_sot": (C.c_int, [c_vp, c_dbl, c_dbl, c_vp]),
     "spx_llg_set_graph": (C.c_int, [c_vp, c_i32]),
     "spx_llg_graph_stats": (C.c_int, [c_vp, P_i64, P_i32]),
     "spx_llg_set_anisotropy_map": (C.c_int, [c_vp, c_vp]),

@@ -39,7 +39,7 @@ def _vec3(a, N, name):
 class EffectiveField:
     def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani_vec=None, D_bulk=0.0, D_int=0.0, n0_int_vec=None,
                  gamma=2.211e5, alpha=0.5, do_precess=1, use_demag=False, demag_method="lindholm",
-                 demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64"):
+                 demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64", _stt=None, _sot=None):
         if float(D_bulk) != 0.0:
             raise NotImplementedError("bulk DMI is not part of this build")
         if str(demag_method).lower() not in {"lindholm", "lindholm_gpu"}:
@@ -86,6 +86,14 @@ class EffectiveField:
         self._H0 = H0 if H0 is not None else np.zeros(3 * self.N)
         p.use_demag = 1 if use_demag else 0
         p.precision = _lib.PREC[precision]
+        if _stt is not None:  # (J, P, beta, direction [3N])
+            jd = _vec3(_stt[3], self.N, "Jdir_vec")
+            self._keep.append(jd)
+            p.stt_J, p.stt_P, p.stt_beta, p.stt_dir = float(_stt[0]), float(_stt[1]), float(_stt[2]), ptr(jd).value
+        if _sot is not None:  # (H_dl, H_fl, polarisation [3N])
+            pv = _vec3(_sot[2], self.N, "polarization_vec")
+            self._keep.append(pv)
+            p.sot_Hdl, p.sot_Hfl, p.sot_p = float(_sot[0]), float(_sot[1]), ptr(pv).value
         self._h = C.c_void_p()
         dh = self.demag_field.handle if self.demag_field is not None else None
         call("spx_llg_create", dh, ptr(X), self.N, ptr(tets), tets.shape[0], C.byref(p), C.byref(self._h))
@@ -280,6 +288,117 @@ class JvContext:
             y.copy_(x)
             return
         call("spx_llg_pc_apply", self.hef.handle, ptr(x), ptr(y), _lib.stream_ptr())
+
+
+class EffectiveFieldSTTGPU(EffectiveField):
+    """EffectiveField with the Zhang-Li spin-transfer torque (gpu/solvers/llg_stt_module_GPU.py:523-1163).
+
+    prefZhang = J P muB / (e Ms (1 + beta^2)) / (1 + alpha^2) / 1e-9; the RHS adds
+    -prefZhang ((beta - alpha) m x z + (1 + alpha beta) m x (m x z)) with z = (J . grad) m / V_i.
+    """
+
+    def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani_vec=None, D_bulk=0.0, D_int=0.0, n0_int_vec=None,
+                 H0_static=None, gamma=2.211e5, alpha=0.5, do_precess=1, Jmagnitude=0.0, Jdir_vec=None, P=0.0,
+                 beta=0.0, use_demag=False, demag_method="lindholm", demag_kwargs=None, H_time_func=None,
+                 precision="f64", Ku_nodes=None):
+        if H_time_func is not None:
+            raise NotImplementedError("time-dependent fields are not part of this build")
+        if Jdir_vec is None:
+            raise ValueError("Jdir_vec is required")
+        self.Jmagnitude, self.P, self.beta = float(Jmagnitude), float(P), float(beta)
+        super().__init__(X, tets, Ms, Aex=Aex, Ku=Ku, n_ani_vec=n_ani_vec, D_bulk=D_bulk, D_int=D_int,
+                         n0_int_vec=n0_int_vec, gamma=gamma, alpha=alpha, do_precess=do_precess,
+                         use_demag=use_demag, demag_method=demag_method, demag_kwargs=demag_kwargs,
+                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision,
+                         _stt=(self.Jmagnitude, self.P, self.beta, Jdir_vec))
+        e, muB = 1.6021766e-19, 9.27400915e-24
+        self.prefZhang = (self.Jmagnitude * self.P * muB / (e * self.Ms * (1.0 + self.beta ** 2))
+                          / (1.0 + self.alpha ** 2) / 1e-9)
+
+    def zhang_li_vec(self, m_vec, out_vec):
+        self._chk(m_vec, "m_vec")
+        self._chk(out_vec, "out_vec")
+        call("spx_llg_zhang_li", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
+        self._tail(out_vec)
+
+    def llg_rhs_STT_vec(self, m_vec, out_vec):
+        self.llg_rhs_vec(m_vec, out_vec)
+
+    def ifunction_STT(self, ts, t, y, ydot, f):
+        return self.ifunction(ts, t, y, ydot, f)
+
+    def update_jac_state_STT(self, m_vec):
+        self.update_jac_state(m_vec)
+
+    def jac_vec_times_STT_vec(self, v_vec, out_vec):
+        self.jac_vec_times_vec(v_vec, out_vec)
+
+
+class EffectiveFieldSOTGPU(EffectiveField):
+    """EffectiveField with spin-orbit torques (gpu/solvers/llg_SOT_module_GPU.py:544-1150): the RHS adds
+    c_fl m x p + c_dl m x (m x p), c_fl = -gamma (H_fl - alpha H_dl) / (1 + alpha^2),
+    c_dl = -gamma (H_dl + alpha H_fl) / (1 + alpha^2)."""
+
+    def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani_vec=None, D_bulk=0.0, D_int=0.0, n0_int_vec=None,
+                 H0_static=None, gamma=2.211e5, alpha=0.5, do_precess=1, H_dl=0.0, H_fl=0.0,
+                 polarization_vec=None, use_demag=False, demag_method="lindholm", demag_kwargs=None,
+                 H_time_func=None, precision="f64", Ku_nodes=None):
+        if H_time_func is not None:
+            raise NotImplementedError("time-dependent fields are not part of this build")
+        pol = (0.0, 1.0, 0.0) if polarization_vec is None else polarization_vec
+        super().__init__(X, tets, Ms, Aex=Aex, Ku=Ku, n_ani_vec=n_ani_vec, D_bulk=D_bulk, D_int=D_int,
+                         n0_int_vec=n0_int_vec, gamma=gamma, alpha=alpha, do_precess=do_precess,
+                         use_demag=use_demag, demag_method=demag_method, demag_kwargs=demag_kwargs,
+                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision,
+                         _sot=(float(H_dl), float(H_fl), pol))
+        self.H_dl, self.H_fl = float(H_dl), float(H_fl)
+        self._update_sot_coefficients()
+
+    def _update_sot_coefficients(self):
+        den = 1.0 + self.alpha * self.alpha
+        self.c_fl = -self.gamma * (self.H_fl - self.alpha * self.H_dl) / den
+        self.c_dl = -self.gamma * (self.H_dl + self.alpha * self.H_fl) / den
+
+    def set_sot(self, H_dl=None, H_fl=None, polarization_vec=None):
+        if H_dl is not None:
+            self.H_dl = float(H_dl)
+        if H_fl is not None:
+            self.H_fl = float(H_fl)
+        pv = None if polarization_vec is None else _vec3(polarization_vec, self.N, "polarization_vec")
+        if pv is not None:
+            self._keep.append(pv)
+        call("spx_llg_set_sot", self._h, self.H_dl, self.H_fl, ptr(pv))
+        self._update_sot_coefficients()
+
+    def llg_rhs_SOT_vec(self, m_vec, out_vec):
+        self.llg_rhs_vec(m_vec, out_vec)
+
+    def ifunction_SOT(self, ts, t, y, ydot, f):
+        return self.ifunction(ts, t, y, ydot, f)
+
+    def update_jac_state_SOT(self, m_vec):
+        self.update_jac_state(m_vec)
+
+    def jac_vec_times_SOT_vec(self, v_vec, out_vec):
+        self.jac_vec_times_vec(v_vec, out_vec)
+
+
+class JvContextSTT(JvContext):
+    """JvContextSTT (llg_stt_module_GPU.py:1210-1336): the 3x3 block preconditioner with the STT terms
+    c3 = (beta - alpha) prefZhang, c4 = -(1 + alpha beta) prefZhang."""
+
+    def __init__(self, hef: EffectiveFieldSTTGPU, eps_reg=1e-14, det_eps=1e-30):
+        super().__init__(hef, eps_reg, det_eps)
+        a, b = hef.alpha, hef.beta
+        self.c3 = (b - a) * hef.prefZhang
+        self.c4 = -(1.0 + a * b) * hef.prefZhang
+
+
+class JvContextSOT(JvContext):
+    """JvContextSOT (llg_SOT_module_GPU.py:1202-1290): column-wise local SOT Jacobian."""
+
+    def update_pc_full_fast_gpu(self, shift, use_abs_diag=False):
+        super().update_pc_full_fast_gpu(shift, include_stab=True, use_abs_kappa=use_abs_diag)
 
 
 class LLG_GPU:

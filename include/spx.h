@@ -226,6 +226,15 @@ typedef struct {
   double H0_uniform[3];                /* set_uniform_field */
   int32_t use_demag;
   int32_t precision;                   /* used when d == NULL; otherwise the demag's precision */
+  /* Zhang-Li spin-transfer torque (LLG_STT_GPU.add_current, llg_stt_module_GPU.py:1409-1414;
+   * EffectiveFieldSTTGPU, :523-590): current density J (A/m^2), polarisation P, non-adiabaticity
+   * beta, nodal current direction [N][3] (NULL: no STT) */
+  double stt_J, stt_P, stt_beta;
+  const double* stt_dir;
+  /* spin-orbit torque (EffectiveFieldSOTGPU.set_sot, llg_SOT_module_GPU.py:812-862): damping-like
+   * and field-like fields (A/m), nodal polarisation [N][3] (normalised per node; NULL: no SOT) */
+  double sot_Hdl, sot_Hfl;
+  const double* sot_p;
 } spx_llg_params;
 /* EffectiveField.__init__ (llg_module_GPU.py:388-724); d may be NULL (no demag) */
 SPX_API int spx_llg_create(spx_demag d, const double* X, int64_t N, const int32_t* tets, int64_t E,
@@ -261,6 +270,17 @@ SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz
  *   spx_llg_step_jvp: one RK4 step of the state and of its tangent: m_out = step(m_n),
  *                     dm_out = d step . (dm, dKu, dH0); dKu: device N or NULL, dH0: host 3
  *                     or NULL. */
+/* Spin torques.  With spx_llg_params.stt_dir set, spx_llg_rhs / spx_llg_step include the Zhang-Li
+ * torque (llg_rhs_STT_vec, llg_stt_module_GPU.py:1054-1085), spx_llg_jv the STT Jacobian
+ * (jac_vec_times_STT_vec, :1123-1163) and spx_llg_pc_build the STT block preconditioner
+ * (JvContextSTT, :1248-1296); with sot_p set, the SOT forms (llg_rhs_SOT_vec,
+ * llg_SOT_module_GPU.py:1069-1096; jac_vec_times_SOT_vec, :1114-1150; JvContextSOT, :1218-1251,
+ * use_abs_kappa standing for use_abs_diag).
+ *   spx_llg_zhang_li: out = (J . grad) m / V_i (ZhangLiGPU.compute_vec, :431-435).
+ *   spx_llg_set_sot:  EffectiveFieldSOTGPU.set_sot (:855-862); polarization host [N][3] or NULL
+ *                     (keep the current one), normalised per node. */
+SPX_API int spx_llg_zhang_li(spx_llg l, const double* m, double* out, spx_stream_t s);
+SPX_API int spx_llg_set_sot(spx_llg l, double H_dl, double H_fl, const double* polarization);
 /* CUDA graphs for spx_llg_step (no counterpart in the reference): with enable != 0, each RK4
  * step is replayed from captured graphs (three captures, one per phase of the per-stage Krylov
  * extrapolation history) after three ordinary steps; the graphs are recaptured when dt, the

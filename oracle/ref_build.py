@@ -3,7 +3,8 @@
 TEST INFRASTRUCTURE.  The reference keeps its per-node kernels as CUDA-C
 bodies inside ``cupy.ElementwiseKernel(...)`` calls
 (``gpu/solvers/llg_module_GPU.py:100-308``,
-``gpu/fields/Anisotropy_GPU.py:24-50``).  Those bodies are plain C
+``gpu/fields/Anisotropy_GPU.py:24-50``, ``gpu/solvers/llg_stt_module_GPU.py:101-393``,
+``gpu/solvers/llg_SOT_module_GPU.py:170-437``).  Those bodies are plain C
 arithmetic on doubles, so this recipe reads the reference sources where they
 lie, pulls each kernel's parameter lists and body out of the Python AST, wraps
 each body in a C loop over arrays and compiles the result with gcc into
@@ -37,6 +38,12 @@ KERNELS = {
     "_PC_APPLY_KERNEL": "gpu/solvers/llg_module_GPU.py",
     "_ANISOTROPY_NODAL_KERNEL": "gpu/fields/Anisotropy_GPU.py",
     "_ANISOTROPY_DIAG_KERNEL": "gpu/fields/Anisotropy_GPU.py",
+    "_LLG_RHS_STT_KERNEL": "gpu/solvers/llg_stt_module_GPU.py",
+    "_JAC_VEC_STT_KERNEL": "gpu/solvers/llg_stt_module_GPU.py",
+    "_PC_BUILD_INV3_STT_KERNEL": "gpu/solvers/llg_stt_module_GPU.py",
+    "_LLG_RHS_SOT_KERNEL": "gpu/solvers/llg_SOT_module_GPU.py",
+    "_JAC_VEC_SOT_KERNEL": "gpu/solvers/llg_SOT_module_GPU.py",
+    "_PC_BUILD_INV3_SOT_KERNEL": "gpu/solvers/llg_SOT_module_GPU.py",
 }
 
 _CTYPE = {"float64": "double", "int32": "int"}

@@ -16,6 +16,8 @@ Each fixture holds seeded inputs and the outputs of the REFERENCE's own code:
   (CPU, full-pivot ACA): block partition, ranks, near nnz, H @ x.
 * ``hcache_film14.npz``  the reference's own npz cache (``HMatrixCPUData.save``,
   storage.py:72-149) of a 14x14x2 film H-matrix (eps 1e-4, leaf 16), for the cache reader.
+* ``torque_kernels.npz``  the reference's STT / SOT per-node kernel bodies
+  (llg_stt_module_GPU.py, llg_SOT_module_GPU.py) compiled the same way.
 * ``llg_kernels.npz``  the reference's per-node CUDA-C kernel bodies compiled
   with gcc by ``oracle/ref_build.py`` plus the CPU numba Jv kernel.
 
@@ -221,6 +223,68 @@ def make_llg_kernels():
     np.savez_compressed(OUT / "llg_kernels.npz", **out)
 
 
+def make_torque_kernels():
+    """The reference's STT / SOT per-node kernels on seeded inputs (torque_kernels.npz)."""
+    from oracle import torques
+    ref = ref_build.RefElementwise(ref_build.build(force=True))
+    rng = np.random.default_rng(1006)
+    n = 211
+    m = rng.normal(size=(n, 3))
+    m[: n // 2] /= np.linalg.norm(m[: n // 2], axis=1)[:, None]
+    H = rng.normal(size=(n, 3)) * 1e5
+    z = rng.normal(size=(n, 3)) * 0.3
+    v = rng.normal(size=(n, 3))
+    Hv = rng.normal(size=(n, 3)) * 1e5
+    zv = rng.normal(size=(n, 3)) * 0.3
+    p = rng.normal(size=(n, 3))
+    p /= np.linalg.norm(p, axis=1)[:, None]
+    D = rng.normal(size=(n, 3)) * 1e4
+    gamma, alpha, Ms, beta = 2.211e5, 0.3, 8e5, 0.05
+    pref = -gamma / (1 + alpha ** 2)
+    stab = Ms * gamma / (1 + alpha ** 2) * 0.5
+    prefZ = torques.pref_zhang(1e12, 0.6, beta, Ms, alpha)
+    c_fl, c_dl = torques.sot_coefficients(gamma, alpha, 3e4, -1e4)
+    d3 = lambda a, pfx: {f"{pfx}x": a[:, 0], f"{pfx}y": a[:, 1], f"{pfx}z": a[:, 2]}  # noqa: E731
+    out = dict(m=m, H=H, z=z, v=v, Hv=Hv, zv=zv, p=p, D=D, gamma=gamma, alpha=alpha, Ms=Ms, beta=beta,
+               prefZ=prefZ, c_fl=c_fl, c_dl=c_dl)
+    r = ref.call("_LLG_RHS_STT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(z, "z"), prefactor=pref,
+                                                 alpha=alpha, do_precess=1.0, Stab=stab, prefZhang=prefZ,
+                                                 stt_a=beta - alpha, stt_b=1.0 + alpha * beta))
+    out["rhs_stt"] = np.stack([r["rx"], r["ry"], r["rz"]], 1)
+    j = ref.call("_JAC_VEC_STT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(z, "jm"), **d3(v, "v"),
+                                                 **d3(Hv, "hv"), **d3(zv, "jv"), prefactor=pref, alpha=alpha,
+                                                 do_precess=1.0, Stab=stab, prefZhang=prefZ, beta=beta))
+    out["jv_stt"] = np.stack([j["ox"], j["oy"], j["oz"]], 1)
+    c1 = gamma / (1 + alpha ** 2)
+    c2 = gamma * alpha / (1 + alpha ** 2)
+    c3 = (beta - alpha) * prefZ
+    c4 = -(1.0 + alpha * beta) * prefZ
+    keys = ("i00", "i01", "i02", "i10", "i11", "i12", "i20", "i21", "i22")
+    for tag, (shift, inc, absk) in {"a": (1e12, 1, 1), "b": (3e11, 0, 0)}.items():
+        pc = ref.call("_PC_BUILD_INV3_STT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(z, "g"),
+                                                            d0=D[:, 0], d1=D[:, 1], d2=D[:, 2], shift=shift,
+                                                            eps_reg=1e-14, det_eps=1e-30, c1=c1, c2=c2, c3=c3,
+                                                            c4=c4, Stab=stab, include_stab=inc, use_abs_kappa=absk))
+        out[f"pc_stt_{tag}"] = np.stack([pc[k] for k in keys], 1).reshape(n, 3, 3)
+        out[f"pc_stt_{tag}_params"] = np.array([shift, inc, absk], dtype=np.float64)
+    r = ref.call("_LLG_RHS_SOT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(p, "p"), prefactor=pref,
+                                                 alpha=alpha, do_precess=1.0, Stab=stab, c_fl=c_fl, c_dl=c_dl))
+    out["rhs_sot"] = np.stack([r["rx"], r["ry"], r["rz"]], 1)
+    j = ref.call("_JAC_VEC_SOT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(p, "p"), **d3(v, "v"),
+                                                 **d3(Hv, "hv"), prefactor=pref, alpha=alpha, do_precess=1.0,
+                                                 Stab=stab, c_fl=c_fl, c_dl=c_dl))
+    out["jv_sot"] = np.stack([j["ox"], j["oy"], j["oz"]], 1)
+    for tag, (shift, absd) in {"a": (1e12, 0), "b": (3e11, 1)}.items():
+        pc = ref.call("_PC_BUILD_INV3_SOT_KERNEL", n, dict(**d3(m, "m"), **d3(H, "h"), **d3(p, "p"),
+                                                            d0=D[:, 0], d1=D[:, 1], d2=D[:, 2], shift=shift,
+                                                            eps_reg=1e-14, det_eps=1e-30, prefactor=pref,
+                                                            alpha=alpha, do_precess=1.0, Stab=stab, c_fl=c_fl,
+                                                            c_dl=c_dl, use_abs_diag=absd))
+        out[f"pc_sot_{tag}"] = np.stack([pc[k] for k in keys], 1).reshape(n, 3, 3)
+        out[f"pc_sot_{tag}_params"] = np.array([shift, absd], dtype=np.float64)
+    np.savez_compressed(OUT / "torque_kernels.npz", **out)
+
+
 def main():
     mods = ref_build.import_reference_hmatrix()
     bds = {}
@@ -229,6 +293,7 @@ def main():
         bds[name] = lindholm.boundary_data(X, T)
         print(name, "N", X.shape[0], "E", T.shape[0], "Nb", bds[name]["Xb"].shape[0], flush=True)
     make_llg_kernels()
+    make_torque_kernels()
     make_lindholm_pairs(mods, bds["c1"])
     make_dense(mods, bds["c1"])
     make_trees(mods, bds)

@@ -182,3 +182,45 @@ def test_rk4_preserves_norm_with_exchange():
     for _ in range(20):
         m = llg.rk4_step(hef.llg_rhs, m, 1e-14)
     assert np.abs(np.linalg.norm(m.reshape(-1, 3), axis=1) - 1).max() < 1e-6
+
+
+def test_torque_kernels_vs_reference(golden):
+    """STT / SOT restatements against the reference's own kernel bodies (gcc-compiled)."""
+    from oracle import torques
+    g = golden("torque_kernels.npz")
+    gamma, alpha, Ms, beta = (float(g[k]) for k in ("gamma", "alpha", "Ms", "beta"))
+    prefZ, c_fl, c_dl = float(g["prefZ"]), float(g["c_fl"]), float(g["c_dl"])
+    pref, stab = llg.constants(Ms, gamma, alpha)
+
+    def close(a, b):
+        a = np.asarray(a).reshape(np.asarray(b).shape)
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    close(torques.rhs_stt(g["m"], g["H"], g["z"], pref, alpha, 1.0, stab, prefZ, beta), g["rhs_stt"])
+    close(torques.jv_stt(g["m"], g["H"], g["z"], g["v"], g["Hv"], g["zv"], pref, alpha, 1.0, stab, prefZ, beta),
+          g["jv_stt"])
+    c1, c2 = gamma / (1 + alpha ** 2), gamma * alpha / (1 + alpha ** 2)
+    c3, c4 = (beta - alpha) * prefZ, -(1.0 + alpha * beta) * prefZ
+    for tag in "ab":
+        shift, inc, absk = g[f"pc_stt_{tag}_params"]
+        close(torques.pc_build_stt(g["m"], g["H"], g["z"], g["D"], shift, c1, c2, c3, c4, stab,
+                                   include_stab=bool(inc), use_abs_kappa=bool(absk)), g[f"pc_stt_{tag}"])
+    close(torques.rhs_sot(g["m"], g["H"], g["p"], pref, alpha, 1.0, stab, c_fl, c_dl), g["rhs_sot"])
+    close(torques.jv_sot(g["m"], g["H"], g["p"], g["v"], g["Hv"], pref, alpha, 1.0, stab, c_fl, c_dl), g["jv_sot"])
+    for tag in "ab":
+        shift, absd = g[f"pc_sot_{tag}_params"]
+        close(torques.pc_build_sot(g["m"], g["H"], g["p"], g["D"], shift, pref, alpha, 1.0, stab, c_fl, c_dl,
+                                   use_abs_diag=bool(absd)), g[f"pc_sot_{tag}"])
+
+
+def test_zhang_li_known_answer():
+    """(J . grad) m of a linear field with constant J is exact at every node (lumped mass)."""
+    from oracle import torques
+    X, T = mesh.kuhn_box(6, 5, 3, 2.0)
+    N = X.shape[0]
+    Jd = np.array([0.6, -0.8, 0.0])
+    Z = torques.zhang_li_matrix(X, T, np.tile(Jd, N))
+    G = np.array([[0.1, -0.2, 0.05], [0.3, 0.0, -0.1], [-0.05, 0.2, 0.15]])  # m_c = G[c] . x + const
+    m = X @ G.T + np.array([0.2, -0.1, 0.4])
+    z = torques.apply3(Z, m.ravel()).reshape(-1, 3)
+    assert np.abs(z - (G @ Jd)[None, :]).max() < 1e-12
+    assert np.abs(Z @ np.ones(N)).max() < 1e-14
