@@ -219,6 +219,9 @@ struct LLGBase {
   virtual void set_ku_map(const double* ku) = 0;
   virtual void zhang_li(const double* m, double* out, cudaStream_t s) = 0;
   virtual void set_sot(double Hdl, double Hfl, const double* p) = 0;
+  virtual void min_eval(double* m, double* d, int normalize, double* out5, cudaStream_t s) = 0;
+  virtual void min_trial(const double* m_old, const double* d_old, double alpha, double* mt, double* dt,
+                         double* out5, cudaStream_t s) = 0;
   virtual void set_graph(int on) = 0;
   virtual void graph_stats(int64_t* replays, int32_t* active) const = 0;
   virtual std::string graph_error() const = 0;
@@ -344,6 +347,25 @@ struct LLGImpl : LLGBase {
   void set_sot(double Hdl, double Hfl, const double* p) override {
     l.graph_reset();
     l.set_sot(Hdl, Hfl, p, 0);
+  }
+  void min_eval(double* m, double* d, int normalize, double* out5, cudaStream_t s) override {
+    TV* mm = f64 ? reinterpret_cast<TV*>(m) : const_cast<TV*>(in_to(m, ta, s));
+    TV* dd = out_of(d, td);
+    l.min_eval(mm, nullptr, nullptr, dd, normalize != 0, out5, s);
+    if (!f64 && normalize) convert<TV, double>(3 * l.N, mm, m, s);
+    back(d, td, s);
+    if (!f64) SPX_CUDA(cudaStreamSynchronize(s));
+  }
+  void min_trial(const double* m_old, const double* d_old, double alpha, double* mt, double* dt, double* out5,
+                 cudaStream_t s) override {
+    const TV* mo = in_to(m_old, ta, s);
+    const TV* dold = in_to(d_old, tc, s);
+    TV* m1 = out_of(mt, tb);
+    TV* d1 = out_of(dt, td);
+    l.min_trial(mo, dold, alpha, m1, d1, out5, s);
+    back(mt, tb, s);
+    back(dt, td, s);
+    if (!f64) SPX_CUDA(cudaStreamSynchronize(s));
   }
   void set_graph(int on) override {
     l.graph_reset();
@@ -1120,6 +1142,21 @@ int spx_llg_set_sot(spx_llg l, double H_dl, double H_fl, const double* polarizat
   API_BEGIN
   REQUIRE(l);
   l->impl->set_sot(H_dl, H_fl, polarization);
+  API_END
+}
+
+int spx_llg_min_eval(spx_llg l, double* m, double* d, int32_t normalize, double* out5, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m); REQUIRE(d); REQUIRE(out5);
+  l->impl->min_eval(m, d, normalize, out5, S(s));
+  API_END
+}
+
+int spx_llg_min_trial(spx_llg l, const double* m_old, const double* d_old, double alpha, double* m_trial,
+                      double* d_trial, double* out5, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(m_old); REQUIRE(d_old); REQUIRE(m_trial); REQUIRE(d_trial); REQUIRE(out5);
+  l->impl->min_trial(m_old, d_old, alpha, m_trial, d_trial, out5, S(s));
   API_END
 }
 

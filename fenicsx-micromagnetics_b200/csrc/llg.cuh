@@ -139,6 +139,12 @@ struct LLGCtx {
   void step_jvp(const TV* mn, const TV* dm, const double* dKu, const double dH0[3], double dt, TV* m_out, TV* dm_out,
                 cudaStream_t s);
   void set_ku_map(const double* Ku_nodes, cudaStream_t s);
+  // energy minimiser (minimize.cu): d = projected field at m (m normalised first when asked),
+  // out5 = (E [J], max |d|, s.y, s.s, y.y) with s, y relative to (m_old, d_old) when given
+  DevBuf<double> minvol, minpart;
+  DevBuf<TV> minH;
+  void min_eval(TV* m, const TV* m_old, const TV* d_old, TV* d, bool normalize, double out5[5], cudaStream_t s);
+  void min_trial(const TV* m_old, const TV* d_old, double alpha, TV* m_t, TV* d_t, double out5[5], cudaStream_t s);
 };
 
 template <class A, class B>

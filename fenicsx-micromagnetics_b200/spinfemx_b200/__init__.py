@@ -29,6 +29,8 @@ _EXPORTS = {
     "cluster_tree_perm": ".geometry",
     "dense_b_apply": ".geometry",
     "LLGEnsemble": ".ensemble",
+    "EnergyMinimizerGPU": ".minimizer",
+    "LaBonteBBMinimizerGPU": ".minimizer",
     "ensemble_mesh": ".ensemble",
     "llg_trajectory": ".adjoint",
     "trajectory_tangent": ".adjoint",

@@ -105,6 +105,8 @@ SIGNATURES = {
     "spx_llg_step": (C.c_int, [c_vp, c_dbl, c_i64, c_vp]),
     "spx_llg_zhang_li": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_set_sot": (C.c_int, [c_vp, c_dbl, c_dbl, c_vp]),
+    "spx_llg_min_eval": (C.c_int, [c_vp, c_vp, c_vp, c_i32, c_vp, c_vp]),
+    "spx_llg_min_trial": (C.c_int, [c_vp, c_vp, c_vp, c_dbl, c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_set_graph": (C.c_int, [c_vp, c_i32]),
     "spx_llg_graph_stats": (C.c_int, [c_vp, P_i64, P_i32]),
     "spx_llg_set_anisotropy_map": (C.c_int, [c_vp, c_vp]),

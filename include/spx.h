@@ -281,6 +281,18 @@ SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz
  *                     (keep the current one), normalised per node. */
 SPX_API int spx_llg_zhang_li(spx_llg l, const double* m, double* out, spx_stream_t s);
 SPX_API int spx_llg_set_sot(spx_llg l, double H_dl, double H_fl, const double* polarization);
+/* LaBonte / Barzilai-Borwein energy minimiser, device part (LaBonteBBMinimizerGPU,
+ * Minimizer_GPU.py:171-845; the step-length and acceptance logic is host code, see
+ * spinfemx_b200/minimizer.py).  FP64 device AoS vectors; out5 (host) = (E [J, lumped, as
+ * compute_Energy_minimize_gpu, llg_module_GPU.py:1079-1229], max_i |d_i|, s.y, s.s, y.y).
+ *   spx_llg_min_eval:  (m normalised in place when normalize != 0) d = H_eff(m) - (m.H_eff) m;
+ *                      out5[2..4] = 0.
+ *   spx_llg_min_trial: m_trial = Cayley step of m_old along d_old with step alpha
+ *                      (_CAYLEY_KERNEL, :46-74), d_trial = projected field at m_trial,
+ *                      s = m_trial - m_old, y = d_old - d_trial. */
+SPX_API int spx_llg_min_eval(spx_llg l, double* m, double* d, int32_t normalize, double* out5, spx_stream_t s);
+SPX_API int spx_llg_min_trial(spx_llg l, const double* m_old, const double* d_old, double alpha, double* m_trial,
+                              double* d_trial, double* out5, spx_stream_t s);
 /* CUDA graphs for spx_llg_step (no counterpart in the reference): with enable != 0, each RK4
  * step is replayed from captured graphs (three captures, one per phase of the per-stage Krylov
  * extrapolation history) after three ordinary steps; the graphs are recaptured when dt, the
