@@ -32,6 +32,9 @@ _EXPORTS = {
     "EnergyMinimizerGPU": ".minimizer",
     "LaBonteBBMinimizerGPU": ".minimizer",
     "ensemble_mesh": ".ensemble",
+    "read_xdmf_mesh": ".io",
+    "read_hdf5": ".io",
+    "XDMFWriter": ".io",
     "llg_trajectory": ".adjoint",
     "trajectory_tangent": ".adjoint",
 }

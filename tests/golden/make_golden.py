@@ -16,6 +16,8 @@ Each fixture holds seeded inputs and the outputs of the REFERENCE's own code:
   (CPU, full-pivot ACA): block partition, ranks, near nnz, H @ x.
 * ``hcache_film14.npz``  the reference's own npz cache (``HMatrixCPUData.save``,
   storage.py:72-149) of a 14x14x2 film H-matrix (eps 1e-4, leaf 16), for the cache reader.
+* ``example_chain_mesh.npz``  the reference's octahedral-nanoparticle chain example mesh
+  (examples/cpu/hysteresis_octahedral_nanoparticles/chain.xdmf + .h5) read by spinfemx_b200.io.
 * ``torque_kernels.npz``  the reference's STT / SOT per-node kernel bodies
   (llg_stt_module_GPU.py, llg_SOT_module_GPU.py) compiled the same way.
 * ``llg_kernels.npz``  the reference's per-node CUDA-C kernel bodies compiled
@@ -39,6 +41,7 @@ sys.path.insert(0, str(ROOT))
 from oracle import lindholm, mesh, ref_build  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
+REF_EXAMPLES = Path("/root/reference/examples")
 
 CASES = {
     # name: (nx, ny, nz, h)
@@ -285,6 +288,16 @@ def make_torque_kernels():
     np.savez_compressed(OUT / "torque_kernels.npz", **out)
 
 
+def make_example_mesh():
+    """The reference's hysteresis_octahedral_nanoparticles/chain mesh (XDMF + gzip HDF5) read by
+    spinfemx_b200.io, stored as example_chain_mesh.npz: a small unstructured mesh for the GPU
+    tests (nothing on the GPU side reads the reference)."""
+    sys.path.insert(0, str(ROOT / "fenicsx-micromagnetics_b200"))
+    from spinfemx_b200 import io as sio
+    X, T, _ = sio.read_xdmf_mesh(REF_EXAMPLES / "cpu/hysteresis_octahedral_nanoparticles/chain.xdmf")
+    np.savez_compressed(OUT / "example_chain_mesh.npz", X=X, tets=T)
+
+
 def main():
     mods = ref_build.import_reference_hmatrix()
     bds = {}
@@ -294,6 +307,7 @@ def main():
         print(name, "N", X.shape[0], "E", T.shape[0], "Nb", bds[name]["Xb"].shape[0], flush=True)
     make_llg_kernels()
     make_torque_kernels()
+    make_example_mesh()
     make_lindholm_pairs(mods, bds["c1"])
     make_dense(mods, bds["c1"])
     make_trees(mods, bds)
