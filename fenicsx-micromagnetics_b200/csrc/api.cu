@@ -683,6 +683,18 @@ int spx_hmat_apply(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   API_END
 }
 
+int spx_hmat_apply_multi(spx_hmat hm, const double* X, double* Y, int32_t nrhs, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(hm);
+  REQUIRE(X);
+  REQUIRE(Y);
+  SPX_CHECK(nrhs >= 1, "nrhs must be at least 1");
+  std::vector<int64_t> off(nrhs);
+  for (int32_t r = 0; r < nrhs; ++r) off[r] = static_cast<int64_t>(r) * hm->h.Nb;
+  hm->h.apply_multi<double>(X, nullptr, off.data(), Y, nullptr, nullptr, nullptr, nrhs, S(s));
+  API_END
+}
+
 int spx_hmat_apply_transpose(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   API_BEGIN
   REQUIRE(hm);

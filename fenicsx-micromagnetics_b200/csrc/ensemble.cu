@@ -9,9 +9,12 @@
 //   B = blockdiag(B_s),  B_s = Lindholm operator of sample s's own boundary triangles.
 // Samples with Nb_s <= dense_max_nb keep a dense block; a single launch applies all dense
 // blocks (a warp per boundary row over the concatenated rows, ragged row lengths).  Larger
-// samples get an H-matrix built on the sample's own boundary; these are concatenated into
-// one block-diagonal H-matrix (hmat_merge) applied by one k_hgather / k_far_z / k_rows
-// sequence for all of them, the boundary gather / scatter fused through an index map.
+// samples get an H-matrix built on the sample's own boundary; samples of the same geometry
+// (coordinates equal up to a translation, same tetrahedra) share one H-matrix applied to all
+// of them at once (HMatrix::apply_multi, every factor read once per batch of states), and
+// the remaining ones are concatenated into one block-diagonal H-matrix (hmat_merge) applied
+// by one k_hgather / k_far_z / k_rows sequence, the boundary gather / scatter fused through
+// an index map.
 #include <algorithm>
 
 #include "fem.cuh"
@@ -118,6 +121,7 @@ int64_t BlockBoundary::device_bytes() const {
   for (const auto& h : H)
     if (h) t += h->device_bytes();
   if (Hm) t += Hm->device_bytes() + static_cast<int64_t>(hidx.bytes() + hmap.bytes() + gbh.bytes());
+  for (const auto& sh : shared) t += sh.H->device_bytes();
   return t;
 }
 
@@ -199,9 +203,33 @@ void block_boundary_build(BlockBoundary& bb, const BoundaryDev& bd, const double
     bb.d_nb.upload(dnb, s);
     bb.d_off.upload(doff, s);
   }
-  // H-matrix samples: built on the sample's own boundary
+  // H-matrix samples with the same geometry (node coordinates up to a translation, same
+  // tetrahedra) share one H-matrix applied to all of them at once (HMatrix::apply_multi)
+  std::vector<int64_t> group_of(ns, -1);
+  std::vector<int64_t> reps;
   for (int64_t k = 0; k < ns; ++k) {
     if (bb.dense[k]) continue;
+    const int64_t Nk = off[k + 1] - off[k];
+    for (size_t g = 0; g < reps.size() && group_of[k] < 0; ++g) {
+      const int64_t r = reps[g];
+      if (off[r + 1] - off[r] != Nk || stets[r] != stets[k]) continue;
+      bool same = true;
+      for (int64_t i = 0; i < Nk && same; ++i)
+        for (int c = 0; c < 3 && same; ++c)
+          same = (X[3 * (off[k] + i) + c] - X[3 * off[k] + c]) == (X[3 * (off[r] + i) + c] - X[3 * off[r] + c]);
+      if (same) group_of[k] = static_cast<int64_t>(g);
+    }
+    if (group_of[k] < 0) {
+      group_of[k] = static_cast<int64_t>(reps.size());
+      reps.push_back(k);
+    }
+  }
+  std::vector<std::vector<int64_t>> members(reps.size());
+  for (int64_t k = 0; k < ns; ++k)
+    if (group_of[k] >= 0) members[group_of[k]].push_back(k);
+  // H-matrix samples: built on the sample's own boundary (one per group)
+  for (int64_t k = 0; k < ns; ++k) {
+    if (bb.dense[k] || reps[group_of[k]] != k) continue;
     const int64_t Nk = off[k + 1] - off[k];
     BoundaryDev bk;
     bk.create(X + 3 * off[k], Nk, stets[k].data(), static_cast<int64_t>(stets[k].size() / 4));
@@ -212,7 +240,15 @@ void block_boundary_build(BlockBoundary& bb, const BoundaryDev& bd, const double
     bb.H[k]->build(bk, o.hcfg, s);
     bb.H[k]->pack(o.hprec, s);
   }
-  // one block-diagonal H-matrix for all H-matrix samples
+  // groups of several samples: one H-matrix, all members in one multi-state apply
+  for (size_t g = 0; g < reps.size(); ++g)
+    if (members[g].size() > 1) {
+      BlockBoundary::Shared sh;
+      sh.H = std::move(bb.H[reps[g]]);
+      for (int64_t k : members[g]) sh.b0.push_back(bb.b0[k]);
+      bb.shared.push_back(std::move(sh));
+    }
+  // one block-diagonal H-matrix for the remaining (single) H-matrix samples
   std::vector<const HMatrix*> parts;
   std::vector<int32_t> hidx, hmap;
   for (int64_t k = 0; k < ns; ++k)
@@ -250,6 +286,11 @@ int block_boundary_apply(BlockBoundary& bb, int64_t Nb, const int32_t* bverts, c
         gB);
     SPX_LAUNCH_CHECK();
     launches += 2;
+  }
+  for (auto& sh : bb.shared) {
+    const int R = static_cast<int>(sh.b0.size());
+    sh.H->apply_multi<TV>(u1, bverts, sh.b0.data(), phi, u1, gB, sh.b0.data(), R, s);
+    launches += ((R + 7) / 8) * (sh.H->nunits > 0 ? 3 : 2);
   }
   if (bb.Hm) {
     TV* yh = reinterpret_cast<TV*>(bb.gbh.p);

@@ -153,6 +153,12 @@ struct BlockBoundary {
   std::vector<std::unique_ptr<HMatrix>> H;  // per sample while building (null for dense samples)
   // all H-matrix samples merged into one block-diagonal H-matrix (one apply for all)
   std::unique_ptr<HMatrix> Hm;
+  // samples of one geometry: one H-matrix and the members' first boundary rows
+  struct Shared {
+    std::unique_ptr<HMatrix> H;
+    std::vector<int64_t> b0;
+  };
+  std::vector<Shared> shared;
   DevBuf<int32_t> hidx;               // merged boundary index -> ensemble vertex
   DevBuf<int32_t> hmap;               // merged boundary index -> ensemble boundary row
   DevBuf<char> gbh;                   // merged-order result (TV)

@@ -105,6 +105,7 @@ struct HMatrix {
   int64_t nseg = 0, zlen = 0, zpart_len = 0, n_far = 0, n_near = 0, nunits = 0, nwarps_z = 0;
   int64_t bytes_far = 0, bytes_near = 0;
   std::unique_ptr<HMatrix> tr;    // H^T (same tree; built on first use by transposed())
+  DevBuf<double> xmulti, zmulti, zpmulti;  // state-interleaved work vectors of apply_multi
 
   void build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s);
   void pack(Prec p, cudaStream_t s);
@@ -114,6 +115,12 @@ struct HMatrix {
   // as dst[gidx[i]] = y_i (+ add[gidx[i]] if add != nullptr).  T is the vector type.
   template <class T>
   void apply_gather(const T* src, const int32_t* gidx, T* dst, const T* add, T* yb, cudaStream_t s);
+  // R right-hand sides at once (hmat_multi.cu): for state r, x_r(b) = src[g_r(b)] and
+  // dst[g_r(b)] = y_r(b) (+ add[g_r(b)]), g_r(b) = gidx[goff[r] + b] with an index array, else
+  // goff[r] + b; yb[yoff[r] + b] = y_r(b) when yb is given.  goff / yoff: host arrays of R.
+  template <class T>
+  void apply_multi(const T* src, const int32_t* gidx, const int64_t* goff, T* dst, const T* add, T* yb,
+                   const int64_t* yoff, int R, cudaStream_t s);
   int64_t device_bytes() const;
   // H^T packed in the same precision: far blocks keep their factors with the roles of U^T and
   // V exchanged, near tiles are transposed (hio.cu).  Built once, kept in `tr`.

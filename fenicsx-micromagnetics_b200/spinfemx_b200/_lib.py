@@ -65,6 +65,7 @@ SIGNATURES = {
     "spx_hmat_repack": (C.c_int, [c_vp, c_i32]),
     "spx_hmat_apply_noalloc": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    "spx_hmat_apply_multi": (C.c_int, [c_vp, c_vp, c_vp, c_i32, c_vp]),
     "spx_hmat_far_factors": (C.c_int, [c_vp, c_i64, c_vp, c_vp]),
     "spx_hmat_memory": (C.c_int, [c_vp, P_i64, P_i64, P_i64]),
     "spx_hmat_destroy": (C.c_int, [c_vp]),

@@ -195,6 +195,17 @@ class HMatrixGPUPackedFused:
         call("spx_hmat_apply", self._h, ptr(x), ptr(out), _lib.stream_ptr())
         return out
 
+    def matmat(self, X_gpu, out=None):
+        """Y = H X for a CUDA float64 tensor of shape (R, Nb) (R vectors, one per row) in one pass."""
+        import torch
+        if X_gpu.dtype != torch.float64 or not X_gpu.is_cuda or X_gpu.dim() != 2 or X_gpu.shape[1] != self.size:
+            raise TypeError("matmat expects a CUDA float64 tensor of shape (R, Nb)")
+        X = X_gpu.contiguous()
+        if out is None:
+            out = torch.empty_like(X)
+        call("spx_hmat_apply_multi", self._h, ptr(X), ptr(out), int(X.shape[0]), _lib.stream_ptr())
+        return out
+
     def rmatvec(self, x_gpu, out=None):
         """y = H^T x (transposed apply; the transposed H-matrix is packed on the first call)."""
         import torch

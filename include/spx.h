@@ -128,6 +128,12 @@ SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
  * zero), so calls that overlap on the GPU (other streams, other threads) race; serialise
  * them.  x, y: FP64 device vectors of length Nb. */
 SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_stream_t s);
+/* Y = H X for nrhs vectors at once (no counterpart in the reference, whose fused apply takes one
+ * vector): X and Y hold nrhs FP64 device vectors of length Nb one after the other (vector r at
+ * X + r Nb).  Each packed factor vector read from memory serves all nrhs products (FP64
+ * accumulation), so the factor traffic of an apply is shared; batches above 8 are applied in
+ * chunks of at most 8.  Results equal nrhs calls of spx_hmat_apply up to rounding. */
+SPX_API int spx_hmat_apply_multi(spx_hmat h, const double* X, double* Y, int32_t nrhs, spx_stream_t s);
 /* y = H^T x (original boundary ordering, FP64 device vectors of length Nb).  No counterpart
  * in the reference (its H-matrix backends apply H only); the adjoint of the demag operator
  * needs it.  The transposed H-matrix (same cluster tree, transposed partition, far factors
