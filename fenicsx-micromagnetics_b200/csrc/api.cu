@@ -98,6 +98,7 @@ struct DemagBase {
   virtual void set_tolerances(double r1, double r2, double at, int m1, int m2) = 0;
   virtual void apply_transpose(const double* w, double* out, cudaStream_t s) = 0;
   virtual void ensemble_info(int64_t* out6) const = 0;
+  virtual HMatrix* shared_hmat(int idx) = 0;
 };
 
 template <class TV, class TM>
@@ -170,6 +171,10 @@ struct DemagImpl : DemagBase {
     ++d.epoch;  // captured step graphs hold the old tolerances
     d.opt.rtol_u1 = r1; d.opt.rtol_u2 = r2; d.opt.atol = at;
     d.opt.maxit_u1 = m1; d.opt.maxit_u2 = m2;
+  }
+  HMatrix* shared_hmat(int idx) override {
+    if (idx < 0 || idx >= static_cast<int>(d.blk.shared.size())) return nullptr;
+    return d.blk.shared[idx].H.get();
   }
   void ensemble_info(int64_t* o) const override {
     const BlockBoundary& b = d.blk;
@@ -637,7 +642,7 @@ int spx_hmat_stats(spx_hmat hm, int64_t* st, double* secs) {
     const int64_t v[16] = {s.dense_blocks, s.low_rank_blocks, s.rejected_low_rank_blocks,
                            s.forced_subdivisions_memory, s.compression_tolerance_subdivisions,
                            s.max_observed_rank, s.sum_observed_rank, s.block_entry_evaluations, s.near_entries,
-                           s.far_entries, s.n_far, s.n_near, s.aca_steps, s.waves, 0, 0};
+                           s.far_entries, s.n_far, s.n_near, s.aca_steps, s.waves, hm->h.Nb, 0};
     std::memcpy(st, v, sizeof(v));
   }
   if (secs) *secs = s.build_seconds;
@@ -901,6 +906,16 @@ int spx_demag_hmat(spx_demag d, spx_hmat* h) {
   REQUIRE(h);
   HMatrix* H = d->impl->hmat();
   SPX_CHECK(H != nullptr, "demag uses the dense boundary operator");
+  *h = reinterpret_cast<spx_hmat>(H);
+  API_END
+}
+
+int spx_demag_ensemble_hmat(spx_demag d, int32_t group, spx_hmat* h) {
+  API_BEGIN
+  REQUIRE(d);
+  REQUIRE(h);
+  HMatrix* H = d->impl->shared_hmat(group);
+  SPX_CHECK(H != nullptr, "no H-matrix shared by several samples with this index");
   *h = reinterpret_cast<spx_hmat>(H);
   API_END
 }

@@ -27,6 +27,9 @@ constexpr int MROWS_WARPS = 8;
 constexpr int MSEG = 64;  // rows per segment (the packing's segment bound)
 
 template <class TF> struct W16;
+// factor vectors kept in flight per lane: the E x R FP64 accumulators and UF 16-byte vectors
+// share the 128 registers a thread has at two CTAs of 256 threads per SM
+template <int E, int R> struct InFlight { static constexpr int UF = E * R >= 64 ? 1 : (E * R >= 32 ? 2 : 4); };
 template <> struct W16<double> { using T = double2; static constexpr int E = 2; };
 template <> struct W16<float> { using T = float4; static constexpr int E = 4; };
 template <> struct W16<__nv_bfloat16> { using T = uint4; static constexpr int E = 8; };
@@ -69,8 +72,9 @@ __global__ void k_hgather_multi(int64_t Nb, const TS* __restrict__ src, const in
   }
 }
 
+// two CTAs per SM (128 registers a thread) unless the accumulators alone take 128 registers
 template <class TF, int R>
-__global__ void __launch_bounds__(MZ_WARPS * 32, 2)
+__global__ void __launch_bounds__(MZ_WARPS * 32, W16<TF>::E * R >= 64 ? 1 : 2)
     k_far_z_multi(const FarUnit* __restrict__ units, const int32_t* __restrict__ warp_first, int nwarps,
                   const TF* __restrict__ F, const double* __restrict__ xm, double* __restrict__ z,
                   double* __restrict__ zpart, const FarGroup* __restrict__ groups, unsigned int* __restrict__ gcnt) {
@@ -100,16 +104,35 @@ __global__ void __launch_bounds__(MZ_WARPS * 32, 2)
     if (vl < nvq) {
       const VT* tile = reinterpret_cast<const VT*>(F + U.voff) + vl;
       const double* x = xm + static_cast<int64_t>(U.xc) * R;
-#pragma unroll 2
-      for (int c = ph; c < U.nc; c += P) {
-        double e[E], a[R];
+      int c = ph;
+      constexpr int UF = InFlight<E, R>::UF;
+      for (; c + (UF - 1) * P < U.nc; c += UF * P) {  // UF factor vectors in flight
+        VT w[UF];
+#pragma unroll
+        for (int u = 0; u < UF; ++u) w[u] = tile[static_cast<int64_t>(c + u * P) * nvq];
+#pragma unroll
+        for (int u = 0; u < UF; ++u) {
+          double e[E];
+          elems(w[u], e);
+          const double* xr = x + static_cast<int64_t>(c + u * P) * R;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const double a = xr[r];
+#pragma unroll
+            for (int t = 0; t < E; ++t) acc[t][r] += e[t] * a;
+          }
+        }
+      }
+      for (; c < U.nc; c += P) {
+        double e[E];
         elems(tile[static_cast<int64_t>(c) * nvq], e);
+        const double* xr = x + static_cast<int64_t>(c) * R;
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = x[static_cast<int64_t>(c) * R + r];
+        for (int r = 0; r < R; ++r) {
+          const double a = xr[r];
 #pragma unroll
-        for (int t = 0; t < E; ++t)
-#pragma unroll
-          for (int r = 0; r < R; ++r) acc[t][r] += e[t] * a[r];
+          for (int t = 0; t < E; ++t) acc[t][r] += e[t] * a;
+        }
       }
     }
     const int fl = U.flags & 3;
@@ -180,16 +203,35 @@ __device__ __forceinline__ void rows_items_multi(const RowItem* __restrict__ ite
     if (vl >= nvec) continue;
     const VT* tile = reinterpret_cast<const VT*>(base + I.off) + vl;
     const double* v = vs + static_cast<int64_t>(I.src) * R;
-#pragma unroll 2
-    for (int q = ph; q < I.len; q += P) {
-      double e[E], a[R];
+    int q = ph;
+    constexpr int UF = InFlight<E, R>::UF;
+    for (; q + (UF - 1) * P < I.len; q += UF * P) {  // UF tile vectors in flight
+      VT w[UF];
+#pragma unroll
+      for (int u = 0; u < UF; ++u) w[u] = tile[static_cast<int64_t>(q + u * P) * nvec];
+#pragma unroll
+      for (int u = 0; u < UF; ++u) {
+        double e[E];
+        elems(w[u], e);
+        const double* vr = v + static_cast<int64_t>(q + u * P) * R;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double a = vr[r];
+#pragma unroll
+          for (int t = 0; t < E; ++t) acc[t][r] += e[t] * a;
+        }
+      }
+    }
+    for (; q < I.len; q += P) {
+      double e[E];
       elems(tile[static_cast<int64_t>(q) * nvec], e);
+      const double* vr = v + static_cast<int64_t>(q) * R;
 #pragma unroll
-      for (int r = 0; r < R; ++r) a[r] = v[static_cast<int64_t>(q) * R + r];
+      for (int r = 0; r < R; ++r) {
+        const double a = vr[r];
 #pragma unroll
-      for (int t = 0; t < E; ++t)
-#pragma unroll
-        for (int r = 0; r < R; ++r) acc[t][r] += e[t] * a[r];
+        for (int t = 0; t < E; ++t) acc[t][r] += e[t] * a;
+      }
     }
   }
 #pragma unroll

@@ -139,6 +139,13 @@ class DemagFieldLindholmGPU:
         self.last_its_u2 = 0
         self.B_dense_gpu = None
         self.B_hmatrix_gpu = None
+        if req == "ensemble":
+            hh = C.c_void_p()
+            if _lib.lib().spx_demag_ensemble_hmat(self._h, 0, C.byref(hh)) == 0:  # samples sharing a mesh
+                st = np.zeros(16, np.int64)
+                call("spx_hmat_stats", hh, ptr(st), None)
+                self.B_hmatrix_gpu = HMatrixGPUPackedFused.from_handle(hh, self, {"bf16": "mixed"}.get(hprec, hprec),
+                                                                       int(st[14]))
         if req == "hmatrix":
             hh = C.c_void_p()
             call("spx_demag_hmat", self._h, C.byref(hh))

@@ -106,7 +106,7 @@ typedef struct {
 SPX_API int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out);
 /* stats[16]: dense_blocks, low_rank_blocks, rejected_low_rank_blocks, forced_subdivisions_memory,
  * compression_tolerance_subdivisions, max_observed_rank, sum_observed_rank, block_entry_evaluations,
- * near_entries, far_entries, n_far, n_near, aca_steps, waves, 0, 0 */
+ * near_entries, far_entries, n_far, n_near, aca_steps, waves, Nb, 0 */
 SPX_API int spx_hmat_stats(spx_hmat h, int64_t* stats16, double* build_seconds);
 SPX_API int spx_hmat_num_blocks(spx_hmat h, int64_t* n);
 /* blocks [n][6]: row_start, row_stop, col_start, col_stop, is_far, rank (permuted coordinates) */
@@ -196,6 +196,9 @@ SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t
 /* out6 = (samples, dense samples, dense block entries, boundary rows of the merged H-matrix of
  * the other samples, its far-factor bytes, its near-tile bytes); zeros for a non-ensemble */
 SPX_API int spx_demag_ensemble_info(spx_demag d, int64_t* out6);
+/* H-matrix shared by the samples of geometry group `group` of an ensemble (borrowed, valid while
+ * d lives; groups are numbered in order of their first sample) */
+SPX_API int spx_demag_ensemble_hmat(spx_demag d, int32_t group, spx_hmat* h);
 SPX_API int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                       const spx_demag_options* opt, int64_t nsamples, const int64_t* node_offsets,
                                       int64_t dense_max_nb, spx_demag* out);
