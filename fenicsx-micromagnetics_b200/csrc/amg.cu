@@ -194,9 +194,41 @@ struct RowRange {
   int lane;
 };
 
+// L2 residency hints.  The cycle's matrices (level 0: ~8 B per nonzero, read five times per
+// PCG iteration together with the PCG product) are loaded with an evict_last policy so that
+// they stay in L2 across the phases and iterations while vectors, transfer operators and the
+// FP64 true-residual values stream past them (those use evict_first where read once).
+__device__ __forceinline__ uint64_t l2_policy_keep() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_stream() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ld_hint(const float* a, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ int32_t ld_hint(const int32_t* a, uint64_t pol) {
+  int32_t v;
+  asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ double ld_hint(const double* a, uint64_t pol) {
+  double v;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+
+// row dot products of one SELL-32 slice (values and columns are read-only for the kernel's
+// lifetime; loaded with the L2 policy `pol`)
 __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
                                           const float* __restrict__ val, int64_t sl, int lane,
-                                          const float* __restrict__ v) {
+                                          const float* __restrict__ v, uint64_t pol) {
   const int64_t base = sp[sl];
   const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
   const float* vv = val + base + lane;
@@ -208,8 +240,8 @@ __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const 
     int32_t c[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      w[u] = vv[(k + u) * 32];
-      c[u] = cc[(k + u) * 32];
+      w[u] = ld_hint(vv + (k + u) * 32, pol);
+      c[u] = ld_hint(cc + (k + u) * 32, pol);
     }
 #pragma unroll
     for (int u = 0; u < 8; u += 2) {
@@ -218,12 +250,12 @@ __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const 
     }
   }
   for (; k + 2 <= width; k += 2) {
-    const float w0 = vv[k * 32], w1 = vv[(k + 1) * 32];
-    const int32_t c0 = cc[k * 32], c1 = cc[(k + 1) * 32];
+    const float w0 = ld_hint(vv + k * 32, pol), w1 = ld_hint(vv + (k + 1) * 32, pol);
+    const int32_t c0 = ld_hint(cc + k * 32, pol), c1 = ld_hint(cc + (k + 1) * 32, pol);
     a0 += w0 * v[c0];
     a1 += w1 * v[c1];
   }
-  if (k < width) a0 += vv[k * 32] * v[cc[k * 32]];
+  if (k < width) a0 += ld_hint(vv + k * 32, pol) * v[ld_hint(cc + k * 32, pol)];
   return a0 + a1;
 }
 
@@ -232,7 +264,7 @@ __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db);
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep());
     if (i < L.n) {
       const float di = L.dinv[i];
       const float d0 = L.db[i] / L.theta;
@@ -249,7 +281,7 @@ __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
 __device__ void pre_b(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d);
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
     if (i < L.n) {
       const float di = L.dinv[i];
       L.r[i] = (L.r[i] - di * t) / di;
@@ -288,7 +320,7 @@ __device__ void restrict_to(const AmgLevelDev& L, const AmgLevelDev& C, RowRange
 __device__ void prolong_from(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.p_nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x);
+    const float t = sell_dot(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, l2_policy_stream());
     if (i < L.n) L.x[i] += t;
   }
 }
@@ -297,7 +329,7 @@ __device__ void prolong_from(const AmgLevelDev& L, const AmgLevelDev& C, RowRang
 __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x);
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep());
     if (i < L.n) {
       const float r0 = L.db[i] - L.dinv[i] * t;
       const float d0 = r0 / L.theta;
@@ -314,7 +346,7 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d);
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
     if (i < L.n) {
       const float r1 = L.r[i] - L.dinv[i] * t;
       const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;
@@ -481,15 +513,16 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       double rh = 0.0;
       PCG_ROWS_BEGIN
         double acc = 0.0, acc2 = 0.0;
+        const uint64_t pst = l2_policy_stream(), pkeep = l2_policy_keep();
         int k = 0;
         for (; k + 2 <= width; k += 2) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += P.v64[idx] * P.y[P.col[idx]];
-          acc2 += P.v64[idx + 32] * P.y[P.col[idx + 32]];
+          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
+          acc2 += ld_hint(P.v64 + idx + 32, pst) * P.y[ld_hint(P.col + idx + 32, pkeep)];
         }
         if (k < width) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += P.v64[idx] * P.y[P.col[idx]];
+          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
         }
         const double r = P.bh[row] - (acc + acc2);
         P.r[row] = r;
@@ -516,12 +549,15 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       double pq = 0.0;
       PCG_ROWS_BEGIN
         const double ui = static_cast<double>(u0[row]);
+        const uint64_t pkeep = l2_policy_keep();
         double acc = 0.0, acc2 = 0.0;
         int k = 0;
         for (; k + 4 <= width; k += 4) {
           const int64_t i0 = base + ((int64_t)k << 5) + lane;
-          const float w0 = P.a32[i0], w1 = P.a32[i0 + 32], w2 = P.a32[i0 + 64], w3 = P.a32[i0 + 96];
-          const int32_t c0 = P.col[i0], c1 = P.col[i0 + 32], c2 = P.col[i0 + 64], c3 = P.col[i0 + 96];
+          const float w0 = ld_hint(P.a32 + i0, pkeep), w1 = ld_hint(P.a32 + i0 + 32, pkeep),
+                      w2 = ld_hint(P.a32 + i0 + 64, pkeep), w3 = ld_hint(P.a32 + i0 + 96, pkeep);
+          const int32_t c0 = ld_hint(P.col + i0, pkeep), c1 = ld_hint(P.col + i0 + 32, pkeep),
+                        c2 = ld_hint(P.col + i0 + 64, pkeep), c3 = ld_hint(P.col + i0 + 96, pkeep);
           acc += static_cast<double>(w0) * (static_cast<double>(u0[c0]) - ui);
           acc2 += static_cast<double>(w1) * (static_cast<double>(u0[c1]) - ui);
           acc += static_cast<double>(w2) * (static_cast<double>(u0[c2]) - ui);
@@ -529,7 +565,8 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
         }
         for (; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += static_cast<double>(P.a32[idx]) * (static_cast<double>(u0[P.col[idx]]) - ui);
+          acc += static_cast<double>(ld_hint(P.a32 + idx, pkeep)) *
+                 (static_cast<double>(u0[ld_hint(P.col + idx, pkeep)]) - ui);
         }
         acc = (acc + acc2 + P.rsum[row] * ui) * P.sdinv[row];
         const double z = ui / P.sdinv[row];
