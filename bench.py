@@ -105,7 +105,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_init(n_gpus):
+def dist_init(n_gpus, timeout_s=300):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL on GPUs, gloo on a
+    host without one (the CPU tests of the multi-rank logic)."""
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -113,9 +115,12 @@ def dist_init(n_gpus):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=timeout_s))
     elif torch.cuda.is_available():
         torch.cuda.set_device(0)
     return rank, ws, local
@@ -128,13 +133,20 @@ def barrier(ws):
 
 
 def allmax(x, ws):
+    """Max over ranks (device times are reported as the slowest rank's)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, ms_max, ws):
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return ws * units_per_rank / (ms_max * 1e-3)
 
 
 def amg_iter_bytes(levels, n0, nnz0):
@@ -237,7 +249,6 @@ def run_ours(a):
     st1 = hef.stats()
     c_after = counters(dm)
     ms_max = allmax(ms, ws)
-    sps = a.steps / (ms_max * 1e-3)
     # demag accuracy of the final state against an FP64 evaluation (same GPU operator)
     mfin = hef.get_state()
     err = None
@@ -259,7 +270,7 @@ def run_ours(a):
             hin, hout = hout, hin
         torch.cuda.synchronize()
         el = allmax(time.perf_counter() - t1, ws)
-        e2e = {"value": ws * ke / el, "unit": "steps/s", "h2d_bytes_per_step": 3 * N * 8,
+        e2e = {"value": job_rate(ke, el * 1e3, ws), "unit": "steps/s", "h2d_bytes_per_step": 3 * N * 8,
                "d2h_bytes_per_step": 3 * N * 8, "steps": ke}
     if rank != 0:
         finish(ws)
@@ -291,7 +302,7 @@ def run_ours(a):
             "traffic": a.traffic.get(dom) if a.traffic else None}
     launches = int(sum(int(x) for x in nl_cat[:7]))
     line = {
-        "metric": METRIC, "value": round(ws * sps, 4), "unit": "steps/s", "n_gpus": ws, "steps": a.steps,
+        "metric": METRIC, "value": round(job_rate(a.steps, ms_max, ws), 4), "unit": "steps/s", "n_gpus": ws, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp64 vectors / fp32 operators"}[a.precision],
         "data": "synthetic (seeded Kuhn-box film and magnetisation)",
@@ -531,7 +542,7 @@ def run_film_batch(a):
     Hmem = dm.B_hmatrix_gpu.memory_report() if dm.B_hmatrix_gpu is not None else {}
     line = {
         "metric": f"LLG film-steps/s at 0.48M nodes, batch of {R} films sharing one H-matrix",
-        "value": round(ws * R * a.steps / (ms * 1e-3), 4), "unit": "film-steps/s", "n_gpus": ws,
+        "value": round(job_rate(R * a.steps, ms, ws), 4), "unit": "film-steps/s", "n_gpus": ws,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp64 vectors / fp32 operators"}[a.precision],
@@ -665,7 +676,7 @@ def run_ensemble(a):
     blk["hmatrix"] = len(meshes) - blk["dense"]
     line = {
         "metric": "ensemble sample-steps/s: 64 independent boxes (BASELINE config 4 shapes), one launch per phase",
-        "value": round(ws * len(meshes) * a.steps / (ms * 1e-3), 2), "unit": "sample-steps/s", "n_gpus": ws,
+        "value": round(job_rate(len(meshes) * a.steps, ms, ws), 2), "unit": "sample-steps/s", "n_gpus": ws,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": {"f32": "fp32", "f64": "fp64", "mixed": "fp64 vectors / fp32 operators"}[a.precision],
