@@ -28,15 +28,15 @@ def golden():
 
 
 @pytest.fixture(scope="session")
-def c1_mesh():
+def box20_mesh():
     from oracle import mesh
     return mesh.kuhn_box(20, 20, 5, 2.0)
 
 
 @pytest.fixture(scope="session")
-def c1_bd(c1_mesh):
+def box20_bd(box20_mesh):
     from oracle import lindholm
-    return lindholm.boundary_data(*c1_mesh)
+    return lindholm.boundary_data(*box20_mesh)
 
 
 def has_gpu():

@@ -7,8 +7,8 @@ Run in a container that has the reference checkout and numba:
 Each fixture holds seeded inputs and the outputs of the REFERENCE's own code:
 
 * ``lindholm_pairs.npz``  gpu/fields/Lindholm_kernel.py (numba) weights and
-  solid angles for random (target, triangle) pairs of the config-1 box.
-* ``c1_dense.npz``  lindholm_hmatrix_gpu/entry_provider.py
+  solid angles for random (target, triangle) pairs of the 20x20x5 box (2 nm cubes).
+* ``box20_dense.npz``  lindholm_hmatrix_gpu/entry_provider.py
   ``LindholmEntryProviderCPU.fill_block(all, all)`` + diag jump: row sums,
   B @ x for seeded x, sample rows.
 * ``trees.npz``  lindholm_hmatrix_gpu/tree.py permutations.
@@ -45,7 +45,7 @@ REF_EXAMPLES = Path("/root/reference/examples")
 
 CASES = {
     # name: (nx, ny, nz, h)
-    "c1": (20, 20, 5, 2.0),
+    "box20": (20, 20, 5, 2.0),
     "film30": (30, 30, 2, 2.5),
     "film48": (48, 48, 2, 2.5),
 }
@@ -90,7 +90,7 @@ def make_dense(mods, bd):
     rng = np.random.default_rng(1002)
     X = rng.standard_normal((Nb, 3))
     sample = np.sort(rng.choice(Nb, 24, replace=False))
-    np.savez_compressed(OUT / "c1_dense.npz", rowsum=B.sum(axis=1), x=X, Bx=B @ X,
+    np.savez_compressed(OUT / "box20_dense.npz", rowsum=B.sum(axis=1), x=X, Bx=B @ X,
                         sample_rows=sample.astype(np.int32), B_rows=B[sample],
                         omega_sum=bd["omega_sum"])
 
@@ -308,8 +308,8 @@ def main():
     make_llg_kernels()
     make_torque_kernels()
     make_example_mesh()
-    make_lindholm_pairs(mods, bds["c1"])
-    make_dense(mods, bds["c1"])
+    make_lindholm_pairs(mods, bds["box20"])
+    make_dense(mods, bds["box20"])
     make_trees(mods, bds)
     make_aca(mods)
     for name in CASES:

@@ -7,7 +7,7 @@ Tolerances (relative unless stated):
   demag, dense FP64, tight CG          1e-9 ; reference CG tolerance (rtol 1e-6) 1e-5
   demag, H-matrix FP64                 1e-5
   LLG field / RHS / Jv / PC (FP64)     1e-11
-  RK4 trajectory (FP64, C1 box)        max|dm| 1e-8
+  RK4 trajectory (FP64, 20x20x5 box)   max|dm| 1e-8
 """
 import math
 
@@ -41,22 +41,22 @@ def spx():
 
 
 @pytest.fixture(scope="module")
-def c1(spx):
+def box20(spx):
     X, T = omesh.kuhn_box(20, 20, 5, 2.0)
     return X, T, spx.BoundaryGeometry(X, T)
 
 
-def test_lindholm_pairs_vs_reference(golden, c1, c1_bd):
+def test_lindholm_pairs_vs_reference(golden, box20, box20_bd):
     g = golden("lindholm_pairs.npz")
-    _, _, geom = c1
+    _, _, geom = box20
     w = geom.lindholm_pairs(torch.as_tensor(g["x0"], device=DEV),
                             torch.as_tensor(g["tri"], device=DEV)).cpu().numpy()
     assert np.abs(w - g["w"]).max() <= 1e-12 * np.abs(g["w"]).max()
 
 
-def test_dense_B_vs_reference(golden, c1):
-    g = golden("c1_dense.npz")
-    _, _, geom = c1
+def test_dense_B_vs_reference(golden, box20):
+    g = golden("box20_dense.npz")
+    _, _, geom = box20
     B = geom.dense_B()
     Bh = B.cpu().numpy()
     assert np.abs(Bh[g["sample_rows"]] - g["B_rows"]).max() < 1e-13
@@ -71,17 +71,17 @@ def geom_apply(B, x):
     return spx.dense_b_apply(B, xt).cpu().numpy()
 
 
-def test_fill_block_vs_oracle(c1, c1_bd):
-    _, _, geom = c1
+def test_fill_block_vs_oracle(box20, box20_bd):
+    _, _, geom = box20
     rng = np.random.default_rng(11)
     rows = np.sort(rng.choice(1202, 300, replace=False)).astype(np.int32)
     cols = rng.choice(1202, 777, replace=False).astype(np.int32)
     got = geom.fill_block(torch.as_tensor(rows, device=DEV), torch.as_tensor(cols, device=DEV)).cpu().numpy()
-    ref = olin.fill_block(c1_bd, rows, cols)
+    ref = olin.fill_block(box20_bd, rows, cols)
     assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
 
 
-CASES = {"c1": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
+CASES = {"box20": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -157,7 +157,7 @@ def test_hmatrix_reduced_precisions(spx, golden):
 
 
 @pytest.fixture(scope="module")
-def c1_oracle():
+def box20_oracle():
     X, T = omesh.kuhn_box(20, 20, 5, 2.0)
     return odemag.DemagOracle(X, T, 8e5)
 
@@ -169,8 +169,8 @@ def _m0(N, seed=1000):
     return m.ravel()
 
 
-def test_demag_dense_vs_oracle(spx, c1_oracle):
-    o = c1_oracle
+def test_demag_dense_vs_oracle(spx, box20_oracle):
+    o = box20_oracle
     m = _m0(o.N)
     Href, u1r, u2r, _ = o.compute(m, return_parts=True)
     mt = torch.as_tensor(m, device=DEV)
@@ -191,8 +191,8 @@ def test_demag_dense_vs_oracle(spx, c1_oracle):
     assert d6.last_its_u1 > 0 and d6.last_res_u1 <= 1e-6
 
 
-def test_demag_hmatrix_vs_oracle(spx, c1_oracle):
-    o = c1_oracle
+def test_demag_hmatrix_vs_oracle(spx, box20_oracle):
+    o = box20_oracle
     m = _m0(o.N)
     Href = o.compute(m)
     mt = torch.as_tensor(m, device=DEV)
@@ -204,8 +204,8 @@ def test_demag_hmatrix_vs_oracle(spx, c1_oracle):
     assert d.B_hmatrix_gpu.stats()["n_far"] > 0
 
 
-def test_demag_fp32_vs_oracle(spx, c1_oracle):
-    o = c1_oracle
+def test_demag_fp32_vs_oracle(spx, box20_oracle):
+    o = box20_oracle
     m = _m0(o.N)
     Href = o.compute(m)
     mt = torch.as_tensor(m, device=DEV)
@@ -268,9 +268,9 @@ def test_llg_field_rhs_jv_pc_vs_oracle(spx, with_demag):
     assert rel(y.cpu().numpy(), shift * v - ref) < 1e-11
 
 
-def test_rk4_trajectory_c1_vs_oracle(spx, c1_oracle):
-    # config-1 box: dense FP64 demag + exchange, alpha 0.5, dt 10 fs
-    o = c1_oracle
+def test_rk4_trajectory_box20_vs_oracle(spx, box20_oracle):
+    # 20x20x5 box (2 nm cubes): dense FP64 demag + exchange, alpha 0.5, dt 10 fs
+    o = box20_oracle
     m0 = _m0(o.N)
     ohef = ollg.EffectiveFieldOracle(o.X, o.tets, 8e5, Aex=1.3e-11, alpha=0.5, demag=o)
     nsteps = 20
@@ -288,8 +288,8 @@ def test_rk4_trajectory_c1_vs_oracle(spx, c1_oracle):
     assert np.abs(hm - mg).max() < 1e-12
 
 
-def test_cg_iteration_cap_reports_not_converged(spx, c1_oracle):
-    o = c1_oracle
+def test_cg_iteration_cap_reports_not_converged(spx, box20_oracle):
+    o = box20_oracle
     mt = torch.as_tensor(_m0(o.N), device=DEV)
     out = torch.empty_like(mt)
     d = spx.DemagFieldLindholmGPU(o.X, o.tets, 8e5, ksp_maxit_u1=3)
@@ -297,9 +297,9 @@ def test_cg_iteration_cap_reports_not_converged(spx, c1_oracle):
     assert d.last_its_u1 == 3 and d.last_res_u1 > 1e-6
 
 
-def test_demag_mixed_vs_oracle(spx, c1_oracle):
+def test_demag_mixed_vs_oracle(spx, box20_oracle):
     # FP64 vectors, FP32 matrices, FP32 CG inside FP64 refinement, difference-form operators
-    o = c1_oracle
+    o = box20_oracle
     m = _m0(o.N)
     Href = o.compute(m)
     mt = torch.as_tensor(m, device=DEV)
@@ -314,9 +314,9 @@ def test_demag_mixed_vs_oracle(spx, c1_oracle):
 
 
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
-def test_rk4_extrapolated_starts_vs_oracle(spx, c1_oracle, precision):
+def test_rk4_extrapolated_starts_vs_oracle(spx, box20_oracle, precision):
     # per-RK-stage extrapolated CG starts change iteration counts, not the trajectory
-    o = c1_oracle
+    o = box20_oracle
     m0 = _m0(o.N)
     ohef = ollg.EffectiveFieldOracle(o.X, o.tets, 8e5, Aex=1.3e-11, alpha=0.5, demag=o)
     nsteps = 12

@@ -12,9 +12,11 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 sys.path.insert(0, str(ROOT / "fenicsx-micromagnetics_b200"))
+sys.path.insert(0, str(ROOT))
+from oracle.ref_build import REF_ROOT  # noqa: E402
 from spinfemx_b200 import io as sio  # noqa: E402
 
-EXAMPLES = Path("/root/reference/examples")
+EXAMPLES = REF_ROOT.parents[1] / "examples"  # the reference checkout's examples, when present
 GOLD = ROOT / "tests" / "golden"
 
 

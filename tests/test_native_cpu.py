@@ -84,7 +84,7 @@ def test_fem_assembly_matches_oracle(spx):
 
 def test_cluster_tree_bit_exact_vs_reference(spx, golden):
     g = golden("trees.npz")
-    cases = {"c1": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
+    cases = {"box20": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
     for name, dims in cases.items():
         bd = spx.boundary_data(*omesh.kuhn_box(*dims))
         for leaf in (16, 32, 64):

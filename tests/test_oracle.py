@@ -7,16 +7,16 @@ import pytest
 from oracle import demag, fem, hmatrix, lindholm, llg, mesh
 
 
-def test_kuhn_box_counts(c1_mesh):
-    X, T = c1_mesh
+def test_kuhn_box_counts(box20_mesh):
+    X, T = box20_mesh
     assert (X.shape[0], T.shape[0]) == mesh.box_counts(20, 20, 5) == (2646, 12000)
     vol, _ = fem.tet_geometry(X, T)
     assert np.allclose(vol, 8.0 / 6.0)
     assert abs(vol.sum() - 40 * 40 * 10) < 1e-6
 
 
-def test_boundary_counts_and_solid_angles(c1_bd):
-    bd = c1_bd
+def test_boundary_counts_and_solid_angles(box20_bd):
+    bd = box20_bd
     assert bd["Xb"].shape[0] == 1202 and bd["tri_lid"].shape[0] == 2400
     frac = bd["omega_sum"] / (4 * math.pi)
     # face 1/2, edge 1/4, corner 1/8 on a box (known answer)
@@ -28,9 +28,9 @@ def test_boundary_counts_and_solid_angles(c1_bd):
     assert np.all(np.sum(c * bd["ntri"], axis=1) > 0)
 
 
-def test_lindholm_weights_vs_reference(golden, c1_bd):
+def test_lindholm_weights_vs_reference(golden, box20_bd):
     g = golden("lindholm_pairs.npz")
-    bd = c1_bd
+    bd = box20_bd
     t = g["tri"]
     w = lindholm.lindholm_weights(g["x0"], bd["tri_pts"][t, 0], bd["tri_pts"][t, 1], bd["tri_pts"][t, 2],
                                   bd["ntri"][t], bd["area"][t], bd["s_edge"][t], bd["eta"][t], bd["gamma"][t])
@@ -41,30 +41,30 @@ def test_lindholm_weights_vs_reference(golden, c1_bd):
     assert np.abs(om - g["omega"]).max() < 1e-13
 
 
-def test_dense_B_vs_reference(golden, c1_bd):
-    g = golden("c1_dense.npz")
-    assert np.allclose(c1_bd["omega_sum"], g["omega_sum"], rtol=0, atol=1e-13)
-    rows = lindholm.dense_rows(c1_bd, g["sample_rows"])
+def test_dense_B_vs_reference(golden, box20_bd):
+    g = golden("box20_dense.npz")
+    assert np.allclose(box20_bd["omega_sum"], g["omega_sum"], rtol=0, atol=1e-13)
+    rows = lindholm.dense_rows(box20_bd, g["sample_rows"])
     assert np.abs(rows - g["B_rows"]).max() < 1e-13
-    B = lindholm.dense_B(c1_bd)
+    B = lindholm.dense_B(box20_bd)
     assert np.abs(B @ g["x"] - g["Bx"]).max() < 1e-11 * np.abs(g["Bx"]).max()
     assert np.abs(B.sum(1) - g["rowsum"]).max() < 1e-12
     # B . 1 = -1 on every row (known answer of the double layer + jump)
     assert np.abs(g["rowsum"] + 1.0).max() < 5e-3
 
 
-def test_fill_block_matches_dense(c1_bd):
+def test_fill_block_matches_dense(box20_bd):
     rng = np.random.default_rng(7)
     rows = np.sort(rng.choice(1202, 50, replace=False))
     cols = np.sort(rng.choice(1202, 70, replace=False))
-    blk = lindholm.fill_block(c1_bd, rows, cols)
-    full = lindholm.dense_rows(c1_bd, rows, with_diag=False)
+    blk = lindholm.fill_block(box20_bd, rows, cols)
+    full = lindholm.dense_rows(box20_bd, rows, with_diag=False)
     assert np.abs(blk - full[:, cols]).max() < 1e-14
 
 
 def test_cluster_tree_vs_reference(golden):
     g = golden("trees.npz")
-    cases = {"c1": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
+    cases = {"box20": (20, 20, 5, 2.0), "film30": (30, 30, 2, 2.5), "film48": (48, 48, 2, 2.5)}
     for name, dims in cases.items():
         bd = lindholm.boundary_data(*mesh.kuhn_box(*dims))
         for leaf in (16, 32, 64):
@@ -82,7 +82,7 @@ def test_fullaca_vs_reference(golden):
         assert abs(rel - float(g[f"rel{k}"])) < 1e-12
 
 
-@pytest.mark.parametrize("name,dims", [("c1", (20, 20, 5, 2.0)), ("film30", (30, 30, 2, 2.5))])
+@pytest.mark.parametrize("name,dims", [("box20", (20, 20, 5, 2.0)), ("film30", (30, 30, 2, 2.5))])
 def test_hmatrix_build_vs_reference(golden, name, dims):
     g = golden(f"hmat_{name}.npz")
     bd = lindholm.boundary_data(*mesh.kuhn_box(*dims))
@@ -129,8 +129,8 @@ def test_llg_kernels_vs_reference(golden):
     assert np.abs(d - g["ani_diag"]).max() <= 1e-12 * np.abs(g["ani_diag"]).max()
 
 
-def test_fem_known_answers(c1_mesh):
-    X, T = c1_mesh
+def test_fem_known_answers(box20_mesh):
+    X, T = box20_mesh
     A = fem.stiffness(X, T)
     assert np.abs(A @ np.ones(X.shape[0])).max() < 1e-12
     Ms = 8e5
