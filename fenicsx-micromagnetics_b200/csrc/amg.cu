@@ -82,7 +82,8 @@ __global__ void k_to_float_rows(const double* __restrict__ a, float* __restrict_
 }  // namespace
 
 void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, const int32_t* col0, const float* val0,
-                       int64_t nslices0) {
+                       int64_t nslices0, int nrep) {
+  reps = nrep;
   nlev = static_cast<int>(h.lv.size());
   n0 = h.lv[0].A.n;
   nc = h.lv.back().A.n;
@@ -107,14 +108,15 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, con
     std::vector<float> di(L.dinv.begin(), L.dinv.end());
     dinv[l].upload(di, s);
     D.dinv = dinv[l].p;
-    vec[l].alloc(6 * static_cast<size_t>(L.A.n));
+    const int64_t nv = L.A.n * reps;  // every level vector holds the reps blocks one after the other
+    vec[l].alloc(6 * static_cast<size_t>(nv));
     vec[l].zero(s);
     D.b = vec[l].p;
-    D.db = vec[l].p + L.A.n;
-    D.x = vec[l].p + 2 * L.A.n;
-    D.x2 = vec[l].p + 3 * L.A.n;
-    D.d = vec[l].p + 4 * L.A.n;
-    D.r = vec[l].p + 5 * L.A.n;
+    D.db = vec[l].p + nv;
+    D.x = vec[l].p + 2 * nv;
+    D.x2 = vec[l].p + 3 * nv;
+    D.d = vec[l].p + 4 * nv;
+    D.r = vec[l].p + 5 * nv;
     if (l + 1 == nlev) break;  // dense coarsest: vectors only
     HostSell hs, hp;
     std::vector<float> v, vp;
@@ -380,6 +382,216 @@ __device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cin
   }
 }
 
+// ---- R identical blocks (a batch of samples of one mesh): the matrix of one block and its
+// hierarchy are stored once, every vector holds R blocks one after the other ([R][n] per level).
+// Each phase reads a matrix slice once and gathers the R blocks' entries of every column, so a
+// warp keeps KB x R gathers in flight; each block's sums are formed column by column in order.
+
+template <int R>
+__device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                           const float* __restrict__ val, int64_t sl, int lane,
+                                           const float* __restrict__ v, int64_t nv, uint64_t pol, float (&t)[R]) {
+  constexpr int KB = R >= 8 ? 1 : 8 / R;
+  const int64_t base = sp[sl];
+  const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
+  const float* vv = val + base + lane;
+  const int32_t* cc = col + base + lane;
+#pragma unroll
+  for (int r = 0; r < R; ++r) t[r] = 0.0f;
+  int k = 0;
+  for (; k + KB <= width; k += KB) {
+    float w[KB];
+    int32_t c[KB];
+#pragma unroll
+    for (int u = 0; u < KB; ++u) {
+      w[u] = ld_hint(vv + (k + u) * 32, pol);
+      c[u] = ld_hint(cc + (k + u) * 32, pol);
+    }
+    float g[KB][R];
+#pragma unroll
+    for (int u = 0; u < KB; ++u)
+#pragma unroll
+      for (int r = 0; r < R; ++r) g[u][r] = v[r * nv + c[u]];
+#pragma unroll
+    for (int u = 0; u < KB; ++u)
+#pragma unroll
+      for (int r = 0; r < R; ++r) t[r] += w[u] * g[u][r];
+  }
+  for (; k < width; ++k) {
+    const float w = ld_hint(vv + k * 32, pol);
+    const int32_t c = ld_hint(cc + k * 32, pol);
+#pragma unroll
+    for (int r = 0; r < R; ++r) t[r] += w * v[r * nv + c];
+  }
+}
+
+template <int R>
+__device__ void pre_a_r(const AmgLevelDev& L, RowRange rr) {
+  const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
+  for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    const int64_t i = sl * 32 + rr.lane;
+    float t[R];
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.db, L.n, l2_policy_keep(), t);
+    if (i < L.n) {
+      const float di = L.dinv[i];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t j = r * L.n + i;
+        const float d0 = L.db[j] / L.theta;
+        const float r1 = L.db[j] - di * t[r] / L.theta;
+        const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
+        L.x[j] = d0 + d1;
+        L.d[j] = d1;
+        L.r[j] = r1;
+      }
+    }
+  }
+}
+
+template <int R>
+__device__ void pre_b_r(const AmgLevelDev& L, RowRange rr) {
+  for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    const int64_t i = sl * 32 + rr.lane;
+    float t[R];
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, L.n, l2_policy_keep(), t);
+    if (i < L.n) {
+      const float di = L.dinv[i];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t j = r * L.n + i;
+        L.r[j] = (L.r[j] - di * t[r]) / di;
+      }
+    }
+  }
+}
+
+template <int R>
+__device__ void restrict_to_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
+  const int G = L.r_lanes;
+  const int gl = rr.lane & (G - 1);
+  const int64_t rows_per_warp = 32 / G;
+  const int64_t first = rr.gw * rows_per_warp + rr.lane / G, stride = rr.nw * rows_per_warp;
+  const int64_t nrows_pad = (C.n + rows_per_warp - 1) / rows_per_warp * rows_per_warp;
+  for (int64_t a = first - rr.lane / G; a < nrows_pad; a += stride) {  // uniform per warp
+    const int64_t row = a + rr.lane / G;
+    float t[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) t[r] = 0.0f;
+    if (row < C.n) {
+      const int64_t k1 = L.r_rp[row + 1];
+      for (int64_t k = L.r_rp[row] + gl; k < k1; k += G) {
+        const float w = L.r_val[k];
+        const int32_t c = L.r_col[k];
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[r] += w * L.r[r * L.n + c];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      for (int o = G >> 1; o > 0; o >>= 1) t[r] += __shfl_xor_sync(0xffffffffu, t[r], o);
+    if (row < C.n && gl == 0) {
+      const float dc = C.dinv[row];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        C.b[r * C.n + row] = t[r];
+        C.db[r * C.n + row] = dc * t[r];
+      }
+    }
+  }
+}
+
+template <int R>
+__device__ void prolong_from_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
+  for (int64_t sl = rr.gw; sl < L.p_nslices; sl += rr.nw) {
+    const int64_t i = sl * 32 + rr.lane;
+    float t[R];
+    sell_dot_r<R>(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, C.n, l2_policy_stream(), t);
+    if (i < L.n) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) L.x[r * L.n + i] += t[r];
+    }
+  }
+}
+
+template <int R>
+__device__ void post_c_r(const AmgLevelDev& L, RowRange rr) {
+  for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    const int64_t i = sl * 32 + rr.lane;
+    float t[R];
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.x, L.n, l2_policy_keep(), t);
+    if (i < L.n) {
+      const float di = L.dinv[i];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t j = r * L.n + i;
+        const float r0 = L.db[j] - di * t[r];
+        const float d0 = r0 / L.theta;
+        L.x2[j] = L.x[j] + d0;
+        L.d[j] = d0;
+        L.r[j] = r0;
+      }
+    }
+  }
+}
+
+// on the top level also the partial dots (r64, z^), (w, z^) over all R blocks
+template <int R>
+__device__ void post_d_r(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
+                         const double* __restrict__ sdinv, double& rz, double& wz, bool top) {
+  const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
+  for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    const int64_t i = sl * 32 + rr.lane;
+    float t[R];
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, L.n, l2_policy_keep(), t);
+    if (i < L.n) {
+      const float di = L.dinv[i];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t j = r * L.n + i;
+        const float r1 = L.r[j] - di * t[r];
+        const float d1 = rho1 * rho0 * L.d[j] + (2.0f * rho1 / L.delta) * r1;
+        const float z = L.x2[j] + d1;
+        L.x[j] = z;
+        if (top) {  // sdinv and r64 are per block row j (sdinv replicated over the blocks)
+          const double zh = static_cast<double>(z) / sdinv[j];
+          rz += r64[j] * zh;
+          wz += zh / sdinv[j];
+        }
+      }
+    }
+  }
+}
+
+// dense coarsest level for R blocks: b entries past nc (the row padding) are taken as 0
+template <int R>
+__device__ void coarse_solve_r(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, int64_t ldc,
+                               RowRange rr) {
+  const int64_t nv = ldc / 4;
+  for (int64_t i = rr.gw; i < nc; i += rr.nw) {
+    const float4* row = reinterpret_cast<const float4*>(cinv + i * ldc);
+    float s[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[r] = 0.0f;
+    for (int64_t j = rr.lane; j < nv; j += 32) {
+      const float4 c = row[j];
+      const float cq[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int64_t jj = 4 * j + q;
+        if (jj < nc) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) s[r] += cq[q] * L.b[r * nc + jj];
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
+      if (rr.lane == 0) L.x[r * nc + i] = s[r];
+    }
+  }
+}
+
 template <class TV>
 struct PcgParams {
   int64_t n, nslices;
@@ -407,6 +619,7 @@ struct PcgParams {
   int nlev;
   const float* cinv;
   int64_t nc, ldc;
+  int reps;  // identical blocks: vectors hold reps x n entries, the matrix n rows
 };
 
 #define PCG_ROWS_BEGIN                                              \
@@ -631,6 +844,242 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
   }
 }
 
+// the V-cycle of k_pcg_amg for R identical blocks (same phases and barriers)
+template <class TV, int R>
+__device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
+  const unsigned nb = gridDim.x;
+  unsigned int* cnt = P.bar;
+  unsigned int* gen = P.bar + 1;
+  const RowRange rr{static_cast<int64_t>((blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5),
+                    static_cast<int64_t>((gridDim.x * static_cast<int64_t>(blockDim.x)) >> 5),
+                    static_cast<int>(threadIdx.x & 31)};
+  const int NL = P.nlev;
+  for (int l = 0; l + 1 < NL; ++l) {
+    const AmgLevelDev& L = P.lv[l];
+    pre_a_r<R>(L, rr);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pre_b_r<R>(L, rr);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    restrict_to_r<R>(L, P.lv[l + 1], rr);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+  }
+  coarse_solve_r<R>(P.lv[NL - 1], P.cinv, P.nc, P.ldc, rr);
+  if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+  for (int l = NL - 2; l >= 0; --l) {
+    const AmgLevelDev& L = P.lv[l];
+    prolong_from_r<R>(L, P.lv[l + 1], rr);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    post_c_r<R>(L, rr);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    double rz = 0.0, wz = 0.0;
+    post_d_r<R>(L, rr, P.r, P.sdinv, rz, wz, l == 0);
+    if (l == 0) cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+  }
+  return true;
+}
+
+// k_pcg_amg on R identical blocks: one CG on the block-diagonal system (the scalars are those of
+// the whole system, as for a disjoint union), with the block's matrix and hierarchy stored once.
+// Per-row data of the matrix (rsum, level dinv) are indexed by the block row i, the vectors and
+// the replicated sdinv / diag by j = r n + i.
+template <class TV, int R>
+__global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
+  __shared__ double sh[160];
+  const unsigned nb = gridDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  unsigned int* cnt = P.bar;
+  unsigned int* gen = P.bar + 1;
+  const int64_t n = P.n;
+  float* b0 = P.lv[0].b;
+  float* db0 = P.lv[0].db;
+  const float* dinv0 = P.lv[0].dinv;
+  double tot[4];
+  double meanb = 0.0;
+  if (P.project && !P.bh_given) {
+    double part = 0.0;
+    PCG_ROWS_BEGIN
+#pragma unroll
+      for (int r = 0; r < R; ++r) part += static_cast<double>(P.b[r * n + row]);
+    PCG_ROWS_END
+    cta_partial(P.part, 0, part, 0.0, 0.0, 0.0, sh);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    cta_total(P.part, 0, tot, sh);
+    meanb = tot[0] / static_cast<double>(R * n);
+  }
+  {
+    double bb = 0.0;
+    PCG_ROWS_BEGIN
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int64_t j = r * n + row;
+        double bv;
+        if (P.bh_given) {
+          bv = P.bh[j] / P.sdinv[j];
+        } else {
+          bv = static_cast<double>(P.b[j]) - meanb;
+          P.bh[j] = bv * P.sdinv[j];
+        }
+        if (!P.warm) P.y[j] = 0.0;
+        bb += bv * bv;
+      }
+    PCG_ROWS_END
+    cta_partial(P.part, 1, bb, 0.0, 0.0, 0.0, sh);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
+  cta_total(P.part, 1, tot, sh);
+  const double bb = tot[0];
+  if (P.warm && !(bb > 0.0)) {  // b = 0: the solution is 0
+    PCG_ROWS_BEGIN
+#pragma unroll
+      for (int r = 0; r < R; ++r) P.y[r * n + row] = 0.0;
+    PCG_ROWS_END
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+  }
+  const double tol2 = fmax(P.rtol * P.rtol * bb, P.atol * P.atol);
+  int total = 0, outers = 0;
+  double rr = 0.0, rr0 = -1.0;
+  for (int outer = 0; outer < P.max_outer; ++outer) {
+    ++outers;
+    // true residual r = bh - A^ y (FP64) of every block, its unscaled norm, r -> level-0 rhs
+    {
+      double rh = 0.0;
+      const uint64_t pst = l2_policy_stream(), pkeep = l2_policy_keep();
+      PCG_ROWS_BEGIN
+        double acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[r] = 0.0;
+        for (int k = 0; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          const double v = ld_hint(P.v64 + idx, pst);
+          const int32_t c = ld_hint(P.col + idx, pkeep);
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += v * P.y[r * n + c];
+        }
+        const float di0 = dinv0[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int64_t j = r * n + row;
+          const double rv = P.bh[j] - acc[r];
+          P.r[j] = rv;
+          const float rf = static_cast<float>(rv / P.sdinv[j]);
+          b0[j] = rf;
+          db0[j] = di0 * rf;
+          rh += P.diag[j] * rv * rv;
+        }
+      PCG_ROWS_END
+      cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    }
+    cta_total(P.part, 0, tot, sh);
+    rr = tot[0];
+    if (rr0 < 0.0) rr0 = rr;
+    if (rr <= tol2 || total >= P.maxit) break;
+    double rz_old = 1.0;
+    for (int it = 0;; ++it) {
+      if (!vcycle_r<TV, R>(P, 2, sh)) return;
+      cta_total(P.part, 2, tot, sh);
+      const double rz = tot[0];
+      const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
+      const double beta = it == 0 ? 0.0 : rz / rz_old;
+      const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ of every block
+      double pq = 0.0;
+      const uint64_t pkeep = l2_policy_keep();
+      PCG_ROWS_BEGIN
+        double ui[R], acc[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          ui[r] = static_cast<double>(u0[r * n + row]);
+          acc[r] = 0.0;
+        }
+        for (int k = 0; k < width; ++k) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          const double w = static_cast<double>(ld_hint(P.a32 + idx, pkeep));
+          const int32_t cc = ld_hint(P.col + idx, pkeep);
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += w * (static_cast<double>(u0[r * n + cc]) - ui[r]);
+        }
+        const double rs = P.rsum[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int64_t j = r * n + row;
+          const double sd = P.sdinv[j];
+          const double av = (acc[r] + rs * ui[r]) * sd;
+          const double z = ui[r] / sd;
+          const double w = 1.0 / sd;
+          const double pv = (z - c * w) + (it == 0 ? 0.0 : beta * P.p[j]);
+          const double qv = av + (it == 0 ? 0.0 : beta * P.q[j]);
+          P.p[j] = pv;
+          P.q[j] = qv;
+          pq += pv * qv;
+        }
+      PCG_ROWS_END
+      cta_partial(P.part, 3, pq, 0.0, 0.0, 0.0, sh);
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      cta_total(P.part, 3, tot, sh);
+      const double pqt = tot[0];
+      if (!(pqt > 0.0) || !(rz > 0.0)) break;
+      const double alpha = rz / pqt;
+      double rh = 0.0;
+      PCG_ROWS_BEGIN
+        const float di0 = dinv0[row];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int64_t j = r * n + row;
+          P.y[j] += alpha * P.p[j];
+          const double rv = P.r[j] - alpha * P.q[j];
+          P.r[j] = rv;
+          const float rf = static_cast<float>(rv / P.sdinv[j]);
+          b0[j] = rf;
+          db0[j] = di0 * rf;
+          rh += P.diag[j] * rv * rv;
+        }
+      PCG_ROWS_END
+      cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
+      if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      cta_total(P.part, 0, tot, sh);
+      rr = tot[0];
+      ++total;
+      rz_old = rz;
+      if (rr <= 0.25 * tol2 || total >= P.maxit) break;
+    }
+  }
+  double mx = 0.0;
+  if (P.project) {
+    double sx = 0.0;
+    PCG_ROWS_BEGIN
+#pragma unroll
+      for (int r = 0; r < R; ++r) sx += P.y[r * n + row] * P.sdinv[r * n + row];
+    PCG_ROWS_END
+    cta_partial(P.part, 1, sx, 0.0, 0.0, 0.0, sh);
+    if (!grid_barrier(cnt, gen, nb, P.err)) return;
+    cta_total(P.part, 1, tot, sh);
+    mx = tot[0] / static_cast<double>(R * n);
+  }
+  PCG_ROWS_BEGIN
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t j = r * n + row;
+      const double xv = P.y[j] * P.sdinv[j] - mx;
+      P.x[j] = static_cast<TV>(xv);
+      P.y[j] = xv / P.sdinv[j];
+    }
+  PCG_ROWS_END
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *P.iters = total;
+    *P.resid = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+    atomicAdd(P.iters_acc, (unsigned long long)total);
+    atomicAdd(P.iters_acc + 1, (unsigned long long)outers);
+    atomicAdd(P.iters_acc + 2, 1ull);
+    if (bb > 0.0) {
+      atomicAdd(P.res_acc, sqrt(fmax(rr0, 0.0) / bb));
+      atomicAdd(P.res_acc + 1, sqrt(rr / bb));
+    }
+  }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host entry
@@ -638,6 +1087,7 @@ template <class TM>
 void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col,
                               const std::vector<double>& a, const std::vector<double>& d, bool singular,
                               cudaStream_t s) {
+  const int64_t n = n1;  // the stored block (reps copies of it form the system)
   CsrHost Ah;
   Ah.n = n;
   Ah.ncols = n;
@@ -652,6 +1102,7 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
     w[i] = std::sqrt(d[i]);
     ww += d[i];
   }
+  ww *= reps;  // the null vector of the whole system repeats w in every block
   AmgHost h;
   amg_build(Ah, w, singular, AmgOptions{}, h);
   if (h.lv.size() < 2) {  // no coarsening possible: keep the Jacobi solver
@@ -680,24 +1131,32 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
     for (int64_t k = 0; k < static_cast<int64_t>(L0.R.v.size()); ++k) L0.R.v[k] /= std::sqrt(d[L0.R.ci[k]]);
   }
   amg = std::make_unique<AmgDevice>();
-  amg->upload(h, s, P.slice_ptr.p, P.col.p, amg_a32.p, P.nslices);
+  amg->upload(h, s, P.slice_ptr.p, P.col.p, amg_a32.p, P.nslices, reps);
   amg_ww = ww;
   amg_singular = singular;
   if (!y64.n) {
-    y64.alloc(n);
+    y64.alloc(this->n);
     y64.zero(s);
   }
-  if (!bh64.n) bh64.alloc(n);
-  amg_work.alloc(3 * static_cast<size_t>(n));
+  if (!bh64.n) bh64.alloc(this->n);
+  amg_work.alloc(3 * static_cast<size_t>(this->n));
   amg_work.zero(s);
   if (!vals64.n) {  // FP64 scaled values (the FP64 CG keeps them in vals)
     std::vector<double> v(P.len);
     SPX_CUDA(cudaMemcpy(v.data(), vals.p, P.len * sizeof(double), cudaMemcpyDeviceToHost));
     vals64.upload(v, s);
   }
+  SPX_CHECK(reps == 1 || reps == 2 || reps == 4 || reps == 8, "repeated blocks: 1, 2, 4 or 8");
   int per_sm = 0;
   SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_amg<double>, PCG_BLOCK, 0));
   SPX_CHECK(per_sm > 0, "AMG PCG kernel cannot be resident");
+  if (reps > 1) {
+    const void* kr = reps == 2 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 2>)
+                     : reps == 4 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 4>)
+                                 : reinterpret_cast<const void*>(k_pcg_amg_r<double, 8>);
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK, 0));
+    SPX_CHECK(per_sm > 0, "AMG PCG kernel (repeated blocks) cannot be resident");
+  }
   int dev;
   SPX_CUDA(cudaGetDevice(&dev));
   amg_grid = num_sms(dev);
@@ -710,7 +1169,7 @@ template <class TV>
 void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int maxit, bool warm, bool project,
                               cudaStream_t st, bool bh_given) {
   PcgParams<TV> q;
-  q.n = n; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p;
+  q.n = n1; q.nslices = P.nslices; q.sp = P.slice_ptr.p; q.col = P.col.p; q.reps = reps;
   q.v64 = vals64.p; q.a32 = amg_a32.p; q.rsum = amg_rsum.p; q.sdinv = sdinv64.p; q.diag = diag64.p;
   q.b = b; q.x = x;
   q.bh = bh64.p; q.y = y64.p;
@@ -722,8 +1181,11 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   q.bh_given = bh_given ? 1 : 0;
   q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc; q.ldc = amg->ldc;
   void* args[] = {&q};
-  SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_pcg_amg<TV>), dim3(amg_grid), dim3(PCG_BLOCK),
-                                       args, 0, st));
+  void* k = reinterpret_cast<void*>(k_pcg_amg<TV>);
+  if (reps == 2) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 2>);
+  if (reps == 4) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 4>);
+  if (reps == 8) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 8>);
+  SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(PCG_BLOCK), args, 0, st));
 }
 
 template void CgSystem<double>::enable_amg(const HostSell&, const std::vector<int64_t>&, const std::vector<int32_t>&,

@@ -75,6 +75,7 @@ struct AmgLevelDev {
 struct AmgDevice {
   int nlev = 0;            // levels 0..nlev-2 are cycled, level nlev-1 is the dense coarsest
   int64_t n0 = 0, nc = 0, ldc = 0;  // ldc: row stride of the coarsest inverse (cinv)
+  int reps = 1;
   std::vector<DevSell<float>> A, P;
   std::vector<DevBuf<int64_t>> rrp;
   std::vector<DevBuf<int32_t>> rcol;
@@ -84,8 +85,9 @@ struct AmgDevice {
   std::vector<int64_t> sizes, nnz, pnnz, rnnz;  // per level: rows, nonzeros of A, P, R
   // top0: when set, level 0's matrix is this SELL-32 (slice pointers, columns, FP32 values of
   // nslices0 slices) owned by the caller instead of a copy of lv[0].A
+  // nrep: the cycle runs on nrep identical blocks at once (level vectors of nrep x rows)
   void upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0 = nullptr, const int32_t* col0 = nullptr,
-              const float* val0 = nullptr, int64_t nslices0 = 0);
+              const float* val0 = nullptr, int64_t nslices0 = 0, int nrep = 1);
   int64_t device_bytes() const;
 };
 

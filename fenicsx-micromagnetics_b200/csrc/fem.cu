@@ -569,13 +569,39 @@ __global__ void __launch_bounds__(CG_BLOCK, 1) k_cg_ir(CgIrParams<TV> P) {
   }
 }
 
+// number of identical diagonal blocks of the FEM system when every sample of an ensemble has
+// the same matrix bit for bit (equal node counts, tets and stiffness values; columns shifted by
+// the sample's offset): 2, 4 or 8 such blocks, else 1
+int repeated_blocks(const HostFem& fem, const std::vector<int64_t>& off) {
+  const int64_t ns = static_cast<int64_t>(off.size()) - 1;
+  if (ns != 2 && ns != 4 && ns != 8) return 1;
+  const int64_t n1 = off[1] - off[0];
+  if (off[0] != 0 || n1 <= AmgOptions{}.coarse_max) return 1;  // the block must have an AMG hierarchy
+  for (int64_t s = 1; s <= ns; ++s)
+    if (off[s] != s * n1) return 1;
+  const int64_t nnz1 = fem.rowptr[n1];
+  for (int64_t s = 1; s < ns; ++s) {
+    const int64_t r0 = s * n1, k0 = fem.rowptr[r0];
+    if (fem.rowptr[r0 + n1] - k0 != nnz1) return 1;
+    for (int64_t i = 0; i <= n1; ++i)
+      if (fem.rowptr[r0 + i] - k0 != fem.rowptr[i]) return 1;
+    for (int64_t k = 0; k < nnz1; ++k)
+      if (fem.col[k0 + k] != fem.col[k] + r0 || fem.A[k0 + k] != fem.A[k]) return 1;
+  }
+  return static_cast<int>(ns);
+}
+
 // ------------------------------------------------------------------ CgSystem
 template <class TM>
-void CgSystem<TM>::setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d) {
-  n = s.nrows;
+void CgSystem<TM>::setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d,
+                         int nrep) {
+  SPX_CHECK(nrep >= 1, "at least one block");
+  reps = nrep;
+  n1 = s.nrows;
+  n = n1 * reps;
   P.upload(s);
-  std::vector<double> v64(vals_sell.size(), 0.0), sd(n);
-  for (int64_t i = 0; i < n; ++i) {
+  std::vector<double> v64(vals_sell.size(), 0.0), sd(n1);
+  for (int64_t i = 0; i < n1; ++i) {
     SPX_CHECK(d[i] > 0.0, "CG system has a non-positive diagonal");
     sd[i] = 1.0 / std::sqrt(d[i]);
   }
@@ -585,13 +611,21 @@ void CgSystem<TM>::setup(const HostSell& s, const std::vector<double>& vals_sell
       for (int l = 0; l < SELL_C; ++l) {
         const int64_t idx = s.slice_ptr[sl] + k * SELL_C + l;
         const int64_t row = sl * SELL_C + l;
-        v64[idx] = (row < n) ? vals_sell[idx] * sd[row] * sd[s.col[idx]] : 0.0;
+        v64[idx] = (row < n1) ? vals_sell[idx] * sd[row] * sd[s.col[idx]] : 0.0;
       }
   }
   std::vector<TM> vt(v64.begin(), v64.end());
   vals.upload(vt);
-  sdinv64.upload(sd);
-  diag64.upload(d.data(), static_cast<size_t>(n));
+  {  // per-row FP64 data, repeated for every block
+    std::vector<double> sdr(n), dr(n);
+    for (int r = 0; r < reps; ++r)
+      for (int64_t i = 0; i < n1; ++i) {
+        sdr[r * n1 + i] = sd[i];
+        dr[r * n1 + i] = d[i];
+      }
+    sdinv64.upload(sdr);
+    diag64.upload(dr);
+  }
   if (sizeof(TM) == sizeof(float)) {
     vals64.upload(v64);
     y64.alloc(n);
@@ -631,6 +665,7 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   if (kind != last_kind) warm = false;
   last_kind = kind;
   const bool use_amg = static_cast<bool>(amg);
+  SPX_CHECK(reps == 1 || use_amg, "a system of repeated blocks is solved by the AMG PCG only");
   const bool ir = sizeof(TM) == sizeof(float) || use_amg;  // solution state kept in y64
   SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
   if (slot >= 0) {
@@ -784,15 +819,38 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
   }
   vol.upload(fem.vol, s);
   {
-    std::vector<double> a;
-    sell_values<double>(hsell, fem.A.data(), 1, true, nnz, 1.0, a);
-    std::vector<double> d(N);
-    for (int64_t i = 0; i < N; ++i)
-      for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
-        if (fem.col[k] == i) d[i] = fem.A[k];
-    cg1.setup(hsell, a, d);
+    // an ensemble whose samples all have the same stiffness matrix (a batch of one mesh): the
+    // u1 system is that block repeated on the diagonal; its matrix and AMG hierarchy are stored
+    // once and the PCG runs on all blocks together (2, 4 or 8 of them)
+    const int reps = (opt.backend == 2 && opt.u1_pc == 0) ? repeated_blocks(fem, opt.sample_offsets) : 1;
+    if (reps > 1) {
+      const int64_t n1 = N / reps, nnz1 = fem.rowptr[n1];
+      std::vector<int64_t> rp1(fem.rowptr.begin(), fem.rowptr.begin() + n1 + 1);
+      std::vector<int32_t> col1(fem.col.begin(), fem.col.begin() + nnz1);
+      std::vector<double> A1(fem.A.begin(), fem.A.begin() + nnz1);
+      std::vector<int32_t> rows1(n1);
+      for (int64_t i = 0; i < n1; ++i) rows1[i] = static_cast<int32_t>(i);
+      HostSell hs1;
+      build_sell(rp1, col1, rows1, nullptr, hs1);
+      std::vector<double> a1, d1(n1);
+      sell_values<double>(hs1, A1.data(), 1, true, nnz1, 1.0, a1);
+      for (int64_t i = 0; i < n1; ++i)
+        for (int64_t k = rp1[i]; k < rp1[i + 1]; ++k)
+          if (col1[k] == i) d1[i] = A1[k];
+      cg1.setup(hs1, a1, d1, reps);
+      cg1.enable_amg(hs1, rp1, col1, A1, d1, true, s);
+      SPX_CHECK(static_cast<bool>(cg1.amg), "no AMG hierarchy for the repeated block");
+    } else {
+      std::vector<double> a;
+      sell_values<double>(hsell, fem.A.data(), 1, true, nnz, 1.0, a);
+      std::vector<double> d(N);
+      for (int64_t i = 0; i < N; ++i)
+        for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
+          if (fem.col[k] == i) d[i] = fem.A[k];
+      cg1.setup(hsell, a, d);
+      if (opt.u1_pc == 0) cg1.enable_amg(hsell, fem.rowptr, fem.col, fem.A, d, true, s);
+    }
     cg1.stage_correct = opt.warm_start == 3;
-    if (opt.u1_pc == 0) cg1.enable_amg(hsell, fem.rowptr, fem.col, fem.A, d, true, s);
   }
   std::vector<int32_t> bmap(N, -1), imap(N, -1), inter;
   for (int64_t k = 0; k < Nb; ++k) bmap[bd.host.bverts[k]] = static_cast<int32_t>(k);

@@ -81,7 +81,9 @@ constexpr int CG_SLOTS = 12;
 
 template <class TM>
 struct CgSystem {
-  int64_t n = 0;
+  int64_t n = 0;       // unknowns: reps blocks of n1 rows
+  int64_t n1 = 0;      // rows of the stored matrix
+  int reps = 1;        // identical diagonal blocks sharing the stored matrix (AMG path only)
   DevSell<TM> P;
   DevBuf<TM> vals;     // scaled values
   DevBuf<double> vals64, sdinv64, diag64, y64, bh64;  // FP64 data of the refinement solve
@@ -121,7 +123,8 @@ struct CgSystem {
   double amg_ww = 0.0;
   bool amg_singular = false;
   int amg_grid = 0;
-  void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d);
+  // nrep > 1: the system is nrep copies of this block on the diagonal (vectors of nrep x rows)
+  void setup(const HostSell& s, const std::vector<double>& vals_sell, const std::vector<double>& d, int nrep = 1);
   // build the AMG hierarchy of D^-1/2 A D^-1/2 from the CSR of A (same rows as setup)
   void enable_amg(const HostSell& hs, const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col, const std::vector<double>& a,
                   const std::vector<double>& d, bool singular, cudaStream_t s);

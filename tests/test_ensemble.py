@@ -138,3 +138,29 @@ def test_graph_replayed_steps_equal_ordinary_steps(spx, precision):
     assert np.array_equal(runs[0][1], runs[1][1])
     assert runs[1][2]["replayed_steps"] == 9 + 7 and runs[1][2]["active"]
     assert runs[0][2]["replayed_steps"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,R", [("f64", 2), ("mixed", 4)])
+def test_batch_of_one_mesh_shares_the_u1_hierarchy(spx, precision, R):
+    """R films of one mesh: the u1 system is one block repeated on the diagonal, solved with the
+    block's matrix and AMG hierarchy stored once; every film's field equals the film run alone."""
+    Xs, Ts = omesh.kuhn_box(40, 40, 2, 2.5)  # 5,043 nodes per film
+    X, T, off = spx.ensemble_mesh([(Xs, Ts)] * R)
+    kw = dict(precision=precision, ksp_rtol_u1=1e-12, ksp_rtol_u2=1e-12, ksp_atol=0.0, ksp_maxit_u1=20000,
+              ksp_maxit_u2=20000, hmatrix_epsilon=1e-7, hmatrix_leaf_size=32)
+    d = spx.DemagFieldLindholmGPU(X, T, MAT["Ms"], boundary_backend="ensemble", sample_offsets=off, dense_max_nb=0,
+                                  **kw)
+    assert d.amg_levels()[0]["rows"] == Xs.shape[0]  # the hierarchy of one film
+    m = np.concatenate([_m0(Xs.shape[0], 40 + k) for k in range(R)])
+    H = torch.empty(3 * X.shape[0], dtype=torch.float64, device="cuda")
+    d.compute_vec(_t(m), H)
+    d.compute_vec(_t(m), H)  # a second (warm) solve
+    H = H.cpu().numpy()
+    ds = spx.DemagFieldLindholmGPU(Xs, Ts, MAT["Ms"], boundary_backend="hmatrix", **kw)
+    Hs = torch.empty(3 * Xs.shape[0], dtype=torch.float64, device="cuda")
+    for k in range(R):
+        ds.compute_vec(_t(m[3 * off[k]:3 * off[k + 1]]), Hs)
+        ref = Hs.cpu().numpy()
+        err = np.linalg.norm(H[3 * off[k]:3 * off[k + 1]] - ref) / np.linalg.norm(ref)
+        assert err < (1e-9 if precision == "f64" else 2e-6), (k, err)
