@@ -75,7 +75,9 @@ struct spx_boundary_s {
   BoundaryDev bd;
 };
 struct spx_hmat_s {
-  HMatrix h;
+  HMatrix own;             // the matrix of a handle made by spx_hmat_build / spx_hmat_import
+  HMatrix* ext = nullptr;  // a borrowed view: the matrix of a demag object (which owns this handle)
+  HMatrix& h() { return ext ? *ext : own; }
   // near field as CSR, computed by spx_hmat_export_sizes for spx_hmat_export
   std::vector<int32_t> near_indptr, near_indices;
   std::vector<double> near_data;
@@ -83,6 +85,16 @@ struct spx_hmat_s {
 // ---- type-erased demag / LLG handles (precision chosen at create)
 struct DemagBase {
   virtual ~DemagBase() = default;
+  // handles lent out by spx_demag_hmat / spx_demag_ensemble_hmat (views of matrices this object
+  // owns; they live as long as it does)
+  std::vector<std::unique_ptr<spx_hmat_s>> views;
+  spx_hmat view_of(HMatrix* H) {
+    for (auto& v : views)
+      if (v->ext == H) return v.get();
+    views.push_back(std::make_unique<spx_hmat_s>());
+    views.back()->ext = H;
+    return views.back().get();
+  }
   virtual int64_t N() const = 0;
   virtual void apply(const double* m, double* H, cudaStream_t s) = 0;
   virtual void potentials(double* u1, double* phi, cudaStream_t s) = 0;
@@ -573,8 +585,8 @@ int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out) {
   REQUIRE(out);
   *out = nullptr;
   auto h = std::make_unique<spx_hmat_s>();
-  h->h.build(b->bd, to_hcfg(cfg), 0);
-  h->h.pack(to_prec(cfg ? cfg->precision : 0), 0);
+  h->own.build(b->bd, to_hcfg(cfg), 0);
+  h->own.pack(to_prec(cfg ? cfg->precision : 0), 0);
   *out = h.release();
   API_END
 }
@@ -583,8 +595,8 @@ int spx_hmat_export_sizes(spx_hmat hm, int64_t* nfar, int64_t* u_entries, int64_
   API_BEGIN
   REQUIRE(hm);
   int64_t f = 0, u = 0, v = 0;
-  hmat_far_sizes(hm->h, f, u, v);
-  hmat_near_csr(hm->h, hm->near_indptr, hm->near_indices, hm->near_data);
+  hmat_far_sizes(hm->h(), f, u, v);
+  hmat_near_csr(hm->h(), hm->near_indptr, hm->near_indices, hm->near_data);
   if (nfar) *nfar = f;
   if (u_entries) *u_entries = u;
   if (v_entries) *v_entries = v;
@@ -596,7 +608,7 @@ int spx_hmat_export(spx_hmat hm, int32_t* perm, double* diag_jump, int64_t* far_
                     double* V, int32_t* near_indptr, int32_t* near_indices, double* near_data) {
   API_BEGIN
   REQUIRE(hm);
-  const HMatrix& H = hm->h;
+  const HMatrix& H = hm->h();
   SPX_CHECK(hm->near_indptr.size() == static_cast<size_t>(H.Nb + 1),
             "call spx_hmat_export_sizes before spx_hmat_export");
   if (perm) std::memcpy(perm, H.tree.perm.data(), H.Nb * sizeof(int32_t));
@@ -628,7 +640,7 @@ int spx_hmat_import(spx_boundary b, const spx_hmat_config* cfg, const int32_t* p
   SPX_CHECK(near_indptr[0] == 0 && (near_indptr[b->bd.host.Nb] == 0 || (near_indices && near_data)),
             "near CSR needs indices and data");
   auto h = std::make_unique<spx_hmat_s>();
-  hmat_import(h->h, b->bd, to_hcfg(cfg), to_prec(cfg ? cfg->precision : 0), nfar, far_meta5, relres, U, V,
+  hmat_import(h->own, b->bd, to_hcfg(cfg), to_prec(cfg ? cfg->precision : 0), nfar, far_meta5, relres, U, V,
               near_indptr, near_indices, near_data, perm, diag_jump, 0);
   *out = h.release();
   API_END
@@ -637,12 +649,12 @@ int spx_hmat_import(spx_boundary b, const spx_hmat_config* cfg, const int32_t* p
 int spx_hmat_stats(spx_hmat hm, int64_t* st, double* secs) {
   API_BEGIN
   REQUIRE(hm);
-  const HStats& s = hm->h.stats;
+  const HStats& s = hm->h().stats;
   if (st) {
     const int64_t v[16] = {s.dense_blocks, s.low_rank_blocks, s.rejected_low_rank_blocks,
                            s.forced_subdivisions_memory, s.compression_tolerance_subdivisions,
                            s.max_observed_rank, s.sum_observed_rank, s.block_entry_evaluations, s.near_entries,
-                           s.far_entries, s.n_far, s.n_near, s.aca_steps, s.waves, hm->h.Nb, 0};
+                           s.far_entries, s.n_far, s.n_near, s.aca_steps, s.waves, hm->h().Nb, 0};
     std::memcpy(st, v, sizeof(v));
   }
   if (secs) *secs = s.build_seconds;
@@ -653,7 +665,7 @@ int spx_hmat_num_blocks(spx_hmat hm, int64_t* n) {
   API_BEGIN
   REQUIRE(hm);
   REQUIRE(n);
-  *n = static_cast<int64_t>(hm->h.blocks.size());
+  *n = static_cast<int64_t>(hm->h().blocks.size());
   API_END
 }
 
@@ -661,9 +673,9 @@ int spx_hmat_blocks(spx_hmat hm, int64_t* out6, int64_t cap) {
   API_BEGIN
   REQUIRE(hm);
   REQUIRE(out6);
-  SPX_CHECK(cap >= static_cast<int64_t>(hm->h.blocks.size()), "capacity smaller than the number of blocks");
+  SPX_CHECK(cap >= static_cast<int64_t>(hm->h().blocks.size()), "capacity smaller than the number of blocks");
   int64_t k = 0;
-  for (const HBlock& b : hm->h.blocks) {
+  for (const HBlock& b : hm->h().blocks) {
     out6[6 * k] = b.rs; out6[6 * k + 1] = b.re; out6[6 * k + 2] = b.cs; out6[6 * k + 3] = b.ce;
     out6[6 * k + 4] = b.type; out6[6 * k + 5] = b.rank;
     ++k;
@@ -675,7 +687,7 @@ int spx_hmat_perm(spx_hmat hm, int32_t* perm) {
   API_BEGIN
   REQUIRE(hm);
   REQUIRE(perm);
-  std::memcpy(perm, hm->h.tree.perm.data(), hm->h.tree.perm.size() * sizeof(int32_t));
+  std::memcpy(perm, hm->h().tree.perm.data(), hm->h().tree.perm.size() * sizeof(int32_t));
   API_END
 }
 
@@ -684,7 +696,7 @@ int spx_hmat_apply(spx_hmat hm, const double* x, double* y, spx_stream_t s) {
   REQUIRE(hm);
   REQUIRE(x);
   REQUIRE(y);
-  hm->h.apply_f64(x, y, S(s));
+  hm->h().apply_f64(x, y, S(s));
   API_END
 }
 
@@ -695,8 +707,8 @@ int spx_hmat_apply_multi(spx_hmat hm, const double* X, double* Y, int32_t nrhs, 
   REQUIRE(Y);
   SPX_CHECK(nrhs >= 1, "nrhs must be at least 1");
   std::vector<int64_t> off(nrhs);
-  for (int32_t r = 0; r < nrhs; ++r) off[r] = static_cast<int64_t>(r) * hm->h.Nb;
-  hm->h.apply_multi<double>(X, nullptr, off.data(), Y, nullptr, nullptr, nullptr, nrhs, S(s));
+  for (int32_t r = 0; r < nrhs; ++r) off[r] = static_cast<int64_t>(r) * hm->h().Nb;
+  hm->h().apply_multi<double>(X, nullptr, off.data(), Y, nullptr, nullptr, nullptr, nrhs, S(s));
   API_END
 }
 
@@ -705,7 +717,7 @@ int spx_hmat_apply_transpose(spx_hmat hm, const double* x, double* y, spx_stream
   REQUIRE(hm);
   REQUIRE(x);
   REQUIRE(y);
-  hm->h.transposed(S(s)).apply_f64(x, y, S(s));
+  hm->h().transposed(S(s)).apply_f64(x, y, S(s));
   API_END
 }
 
@@ -714,40 +726,41 @@ int spx_hmat_apply_noalloc(spx_hmat hm, const double* x, double* y, spx_stream_t
   REQUIRE(hm);
   REQUIRE(x);
   REQUIRE(y);
-  hmat_apply_noalloc(hm->h, x, y, S(s));
+  hmat_apply_noalloc(hm->h(), x, y, S(s));
   API_END
 }
 
 int spx_hmat_repack(spx_hmat hm, int32_t precision) {
   API_BEGIN
   REQUIRE(hm);
-  hm->h.pack(to_prec(precision), 0);
+  hm->h().pack(to_prec(precision), 0);
   API_END
 }
 
 int spx_hmat_far_factors(spx_hmat hm, int64_t index, double* Ut, double* V) {
   API_BEGIN
   REQUIRE(hm);
-  SPX_CHECK(index >= 0 && index < static_cast<int64_t>(hm->h.blocks.size()), "block index out of range");
-  const HBlock& b = hm->h.blocks[index];
+  SPX_CHECK(index >= 0 && index < static_cast<int64_t>(hm->h().blocks.size()), "block index out of range");
+  const HBlock& b = hm->h().blocks[index];
   SPX_CHECK(b.type == 1, "block is not a far (low-rank) block");
   const int64_t m = b.re - b.rs, n = b.ce - b.cs, k = b.rank;
-  if (Ut) SPX_CUDA(cudaMemcpy(Ut, hm->h.far_pool64.p + b.off_u, k * m * sizeof(double), cudaMemcpyDeviceToHost));
-  if (V) SPX_CUDA(cudaMemcpy(V, hm->h.far_pool64.p + b.off_v, k * n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Ut) SPX_CUDA(cudaMemcpy(Ut, hm->h().far_pool64.p + b.off_u, k * m * sizeof(double), cudaMemcpyDeviceToHost));
+  if (V) SPX_CUDA(cudaMemcpy(V, hm->h().far_pool64.p + b.off_v, k * n * sizeof(double), cudaMemcpyDeviceToHost));
   API_END
 }
 
 int spx_hmat_memory(spx_hmat hm, int64_t* far_bytes, int64_t* near_bytes, int64_t* total) {
   API_BEGIN
   REQUIRE(hm);
-  if (far_bytes) *far_bytes = hm->h.bytes_far;
-  if (near_bytes) *near_bytes = hm->h.bytes_near;
-  if (total) *total = hm->h.device_bytes();
+  if (far_bytes) *far_bytes = hm->h().bytes_far;
+  if (near_bytes) *near_bytes = hm->h().bytes_near;
+  if (total) *total = hm->h().device_bytes();
   API_END
 }
 
 int spx_hmat_destroy(spx_hmat hm) {
   API_BEGIN
+  SPX_CHECK(!hm || !hm->ext, "this H-matrix handle belongs to a demag object (destroy the demag object instead)");
   delete hm;
   API_END
 }
@@ -846,7 +859,11 @@ int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t* tets, 
     spx::set_last_error("null H-matrix handle");
     return SPX_ERR_INVALID;
   }
-  return demag_create(X, N, tets, E, Ms, opt, &hm->h, out);
+  if (hm->ext) {
+    spx::set_last_error("the H-matrix handle belongs to a demag object");
+    return SPX_ERR_INVALID;
+  }
+  return demag_create(X, N, tets, E, Ms, opt, &hm->own, out);
 }
 
 int spx_demag_apply(spx_demag d, const double* m, double* H, spx_stream_t s) {
@@ -906,7 +923,7 @@ int spx_demag_hmat(spx_demag d, spx_hmat* h) {
   REQUIRE(h);
   HMatrix* H = d->impl->hmat();
   SPX_CHECK(H != nullptr, "demag uses the dense boundary operator");
-  *h = reinterpret_cast<spx_hmat>(H);
+  *h = d->impl->view_of(H);
   API_END
 }
 
@@ -916,7 +933,7 @@ int spx_demag_ensemble_hmat(spx_demag d, int32_t group, spx_hmat* h) {
   REQUIRE(h);
   HMatrix* H = d->impl->shared_hmat(group);
   SPX_CHECK(H != nullptr, "no H-matrix shared by several samples with this index");
-  *h = reinterpret_cast<spx_hmat>(H);
+  *h = d->impl->view_of(H);
   API_END
 }
 

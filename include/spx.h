@@ -143,6 +143,8 @@ SPX_API int spx_hmat_apply_transpose(spx_hmat h, const double* x, double* y, spx
 /* low-rank factors U^T (k x m) and V (k x n) of far block `index` (as listed by spx_hmat_blocks), FP64 host */
 SPX_API int spx_hmat_far_factors(spx_hmat h, int64_t index, double* Ut, double* V);
 SPX_API int spx_hmat_memory(spx_hmat h, int64_t* far_bytes, int64_t* near_bytes, int64_t* total_bytes);
+/* frees a handle made by spx_hmat_build / spx_hmat_import; handles lent by a demag object
+ * (spx_demag_hmat, spx_demag_ensemble_hmat) are refused: they go with the demag object */
 SPX_API int spx_hmat_destroy(spx_hmat h);
 /* The reference's cache contents (HMatrixCPUData, lindholm_hmatrix_gpu/storage.py:29-325; the
  * npz file itself is read and written by numpy in the Python layer):
@@ -217,7 +219,8 @@ SPX_API int spx_demag_energy(spx_demag d, const double* m, const double* H, doub
 /* last_its_u1 / last_its_u2 and the relative residuals of the last apply */
 SPX_API int spx_demag_stats(spx_demag d, int64_t* its_u1, int64_t* its_u2, double* res_u1, double* res_u2);
 SPX_API int spx_demag_info(spx_demag d, int64_t* N, int64_t* Nb, int64_t* NI, int64_t* device_bytes);
-/* H-matrix of an hmatrix-backend demag (borrowed; valid while d lives) */
+/* H-matrix of an hmatrix-backend demag (borrowed, valid while d lives; every spx_hmat call
+ * accepts it, spx_hmat_destroy and spx_demag_create_with_hmat refuse it) */
 SPX_API int spx_demag_hmat(spx_demag d, spx_hmat* h);
 SPX_API int spx_demag_destroy(spx_demag d);
 

@@ -137,3 +137,31 @@ def test_demag_uses_the_cache(spx, tmp_path):
         H = torch.empty_like(m)
         d.compute_vec(m, H)
         assert float(torch.linalg.norm(H - H0) / torch.linalg.norm(H0)) < 1e-9
+
+
+def test_borrowed_handle_of_a_demag_object(spx, tmp_path):
+    """The H-matrix a demag object lends out (spx_demag_hmat) is a full handle: it saves in the
+    cache schema and reloads to the same operator, the demag object keeps working, and
+    destroying it through the ABI is refused (it goes with the demag object)."""
+    import ctypes as C
+
+    import torch
+    from spinfemx_b200 import _lib
+    X, T = omesh.kuhn_box(*FILM14)
+    d = spx.DemagFieldLindholmGPU(X, T, 8e5, boundary_backend="hmatrix", hmatrix_epsilon=1e-4,
+                                  hmatrix_leaf_size=16, precision="f64")
+    m = np.tile([0.6, 0.8, 0.0], X.shape[0])
+    Hf = torch.empty(3 * X.shape[0], dtype=torch.float64, device="cuda")
+    d.compute_vec(torch.as_tensor(m, device="cuda"), Hf)
+    before = Hf.cpu().numpy().copy()
+    B = d.B_hmatrix_gpu
+    path = tmp_path / "borrowed.npz"
+    B.save(path, compressed=False)  # export through the borrowed handle
+    geom = spx.BoundaryGeometry(X, T)
+    cfg = spx.HMatrixBuildConfig(epsilon=1e-4, eta=2.0, leaf_size=16)
+    H2, _ = spx.HMatrixGPUPackedFused.load(path, geom, cfg, precision="f64")
+    x = torch.as_tensor(_x(geom.Nb, 7), device="cuda")
+    assert _rel(H2.matvec(x).cpu().numpy(), B.matvec(x).cpu().numpy()) < 1e-13
+    assert _lib.lib().spx_hmat_destroy(B.handle) != 0  # refused, nothing freed
+    d.compute_vec(torch.as_tensor(m, device="cuda"), Hf)
+    assert np.array_equal(Hf.cpu().numpy(), before)
