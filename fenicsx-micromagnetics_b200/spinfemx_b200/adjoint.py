@@ -17,9 +17,14 @@ from __future__ import annotations
 import numpy as np
 
 
-def _dev_f64(x, n, name):
+def _device(hef):
+    """Device of the field object's state (the GPU for the library's field objects)."""
+    return getattr(hef, "device", "cuda")
+
+
+def _dev_f64(x, n, name, device="cuda"):
     import torch
-    t = torch.as_tensor(x, dtype=torch.float64, device="cuda").contiguous().reshape(-1)
+    t = torch.as_tensor(x, dtype=torch.float64, device=device).contiguous().reshape(-1)
     if t.numel() != n:
         raise ValueError(f"{name} must have {n} entries")
     return t
@@ -34,7 +39,7 @@ def _make_function():
             if nsteps < 0 or every < 1 or dt <= 0.0:
                 raise ValueError("nsteps >= 0, checkpoint_every >= 1 and dt > 0 are required")
             _apply_params(hef, Ku, H0)
-            m = _dev_f64(m0.detach(), hef.local_size, "m0")
+            m = _dev_f64(m0.detach(), hef.local_size, "m0", _device(hef))
             hef.set_state(m)
             ckpts = []
             n = 0
@@ -57,8 +62,9 @@ def _make_function():
             Ku, H0 = ctx.params
             _apply_params(hef, Ku, H0)
             lam = gT.detach().to(torch.float64).contiguous().clone()
-            gKu = torch.zeros(hef.N, dtype=torch.float64, device="cuda") if ctx.want[0] else None
-            gH0 = torch.zeros(3, dtype=torch.float64, device="cuda") if ctx.want[1] else None
+            dev = _device(hef)
+            gKu = torch.zeros(hef.N, dtype=torch.float64, device=dev) if ctx.want[0] else None
+            gH0 = torch.zeros(3, dtype=torch.float64, device=dev) if ctx.want[1] else None
             for seg in range(len(ctx.ckpts) - 1, -1, -1):
                 n0 = seg * every
                 k = min(every, ctx.nsteps - n0)
