@@ -115,3 +115,20 @@ def test_invalid_arguments_raise_value_error(spx):
         spx.HMatrixBuildConfig(epsilon=-1.0)
     with pytest.raises(ValueError):
         spx.HMatrixBuildConfig(compressor="svd")
+
+
+def test_geometry_hash_matches_the_reference_cache(spx):
+    """The cache key's geometry hash (sha256 of the boundary points and triangles,
+    builder.py:98-103) equals the one the reference wrote into its own cache of the
+    14x14x2 film (tests/golden/hcache_film14.npz)."""
+    import json
+    from spinfemx_b200.hmatrix import geometry_hash
+    a = np.load(Path(__file__).resolve().parent / "golden" / "hcache_film14.npz", allow_pickle=False)
+    meta = json.loads(str(np.asarray(a["metadata_json"]).item()))
+    X, T = omesh.kuhn_box(14, 14, 2, 2.5)
+    bd = spx.boundary_data(X, T)
+    assert bd["Xb"].shape[0] == meta["Nb"]
+    assert geometry_hash(bd["Xb"], bd["tri_lid"]) == meta["geometry_hash"]
+    X2 = X.copy()
+    X2[:, 2] *= 1.01  # another geometry, another key
+    assert geometry_hash(spx.boundary_data(X2, T)["Xb"], bd["tri_lid"]) != meta["geometry_hash"]
