@@ -432,6 +432,10 @@ static std::unique_ptr<LLGBase> make_llg(spx_demag d, const double* X, int64_t N
 }
 
 
+namespace spx {
+int barrier_timeout_probe(int nblocks, long long limit, int* timed_out_ctas);  // failure_probe.cu
+}
+
 extern "C" {
 
 const char* spx_last_error(void) { return spx::g_last_error.c_str(); }
@@ -755,6 +759,16 @@ int spx_hmat_memory(spx_hmat hm, int64_t* far_bytes, int64_t* near_bytes, int64_
   if (far_bytes) *far_bytes = hm->h().bytes_far;
   if (near_bytes) *near_bytes = hm->h().bytes_near;
   if (total) *total = hm->h().device_bytes();
+  API_END
+}
+
+int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int32_t* timed_out_ctas) {
+  API_BEGIN
+  REQUIRE(status);
+  REQUIRE(timed_out_ctas);
+  int t = 0;
+  *status = spx::barrier_timeout_probe(nblocks, static_cast<long long>(limit), &t);
+  *timed_out_ctas = t;
   API_END
 }
 

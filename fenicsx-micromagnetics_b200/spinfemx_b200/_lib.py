@@ -73,6 +73,7 @@ SIGNATURES = {
     "spx_demag_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_demag_ensemble_info": (C.c_int, [c_vp, c_vp]),
     "spx_demag_ensemble_hmat": (C.c_int, [c_vp, c_i32, C.POINTER(c_vp)]),
+    "spx_debug_barrier_probe": (C.c_int, [c_i32, c_i64, C.POINTER(c_i32), C.POINTER(c_i32)]),
     "spx_demag_create_ensemble": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), c_i64, c_vp,
                                             c_i64, C.POINTER(c_vp)]),
     "spx_demag_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),

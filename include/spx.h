@@ -50,6 +50,12 @@ SPX_API const char* spx_last_error(void);
 SPX_API int spx_version(void);
 /* number of visible CUDA devices (0 without a GPU; never fails) */
 SPX_API int spx_device_count(int32_t* n);
+/* Failure-detection probe (no counterpart in the reference, which has no bounded waits): runs
+ * a grid barrier on nblocks CTAs (2 .. number of SMs) that one CTA never reaches.  The others'
+ * bounded waits run out after `limit` polls (1 .. 2^24) and return; *status receives the error
+ * code the device recorded (SPX_ERR_TIMEOUT) and *timed_out_ctas how many CTAs gave up.  The
+ * context stays usable.  Returns SPX_OK when the probe ran. */
+SPX_API int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int32_t* timed_out_ctas);
 
 /* ------------------------------------------------------------------ host geometry
  * Boundary data of build_boundary_data_serial (gpu/fields/Demag_Lindholm.py:177-285):

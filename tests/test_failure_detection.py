@@ -1,0 +1,41 @@
+"""Failure detection without a GPU fault: a grid barrier that one CTA never reaches makes the
+other CTAs' bounded waits run out.  The kernel records SPX_ERR_TIMEOUT and returns, the host
+reads the status, and the context keeps working (the same bounded wait guards the barriers
+of the persistent CG and AMG-PCG kernels)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import mesh as omesh
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.mark.parametrize("nblocks", [2, 16])
+def test_barrier_wait_runs_out_and_reports(nblocks):
+    import spinfemx_b200 as spx
+    from spinfemx_b200 import _lib
+    status, gave_up = C.c_int32(-1), C.c_int32(-1)
+    _lib.call("spx_debug_barrier_probe", nblocks, 1 << 14, C.byref(status), C.byref(gave_up))
+    assert status.value == 5  # SPX_ERR_TIMEOUT
+    assert gave_up.value == nblocks - 1
+    # the context is still usable: a demag evaluation runs and matches a second one
+    X, T = omesh.kuhn_box(4, 4, 2, 2.0)
+    d = spx.DemagFieldLindholmGPU(X, T, 8e5, boundary_backend="dense", precision="f64")
+    m = torch.as_tensor(np.tile([0.0, 0.6, 0.8], X.shape[0]), device="cuda")
+    H1, H2 = torch.empty_like(m), torch.empty_like(m)
+    d.compute_vec(m, H1)
+    d.compute_vec(m, H2)
+    torch.cuda.synchronize()
+    assert torch.isfinite(H1).all() and torch.allclose(H1, H2, rtol=1e-10, atol=0.0)
+
+
+def test_probe_rejects_bad_arguments():
+    from spinfemx_b200 import _lib
+    status, gave_up = C.c_int32(), C.c_int32()
+    assert _lib.lib().spx_debug_barrier_probe(1, 100, C.byref(status), C.byref(gave_up)) == 1
+    assert _lib.lib().spx_debug_barrier_probe(4, 0, C.byref(status), C.byref(gave_up)) == 1
