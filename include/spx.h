@@ -199,13 +199,16 @@ SPX_API int spx_demag_create_with_hmat(const double* X, int64_t N, const int32_t
  * and the tetrahedra that reference them.  FEM operators, both Poisson solves and
  * spx_demag_apply run once for all samples; the boundary operator is block diagonal: the
  * Lindholm operator of each sample's own boundary, dense (one batched launch for all dense
- * samples) when the sample's Nb <= dense_max_nb, else an H-matrix with opt->hmat.
- * opt->backend is ignored.  spx_demag_apply_transpose is not available for ensembles. */
+ * samples) when the sample's Nb <= dense_max_nb, else an H-matrix with opt->hmat; samples
+ * of one geometry (equal up to a translation) share one H-matrix applied to all of them at
+ * once, and 2, 4 or 8 samples whose stiffness matrices are identical share the u1 matrix and
+ * AMG hierarchy.  opt->backend is ignored.  spx_demag_apply_transpose is not available for
+ * ensembles. */
 /* out6 = (samples, dense samples, dense block entries, boundary rows of the merged H-matrix of
  * the other samples, its far-factor bytes, its near-tile bytes); zeros for a non-ensemble */
 SPX_API int spx_demag_ensemble_info(spx_demag d, int64_t* out6);
-/* H-matrix shared by the samples of geometry group `group` of an ensemble (borrowed, valid while
- * d lives; groups are numbered in order of their first sample) */
+/* H-matrix shared by the samples of geometry group `group` of an ensemble (lent like
+ * spx_demag_hmat, valid while d lives; groups are numbered in order of their first sample) */
 SPX_API int spx_demag_ensemble_hmat(spx_demag d, int32_t group, spx_hmat* h);
 SPX_API int spx_demag_create_ensemble(const double* X, int64_t N, const int32_t* tets, int64_t E, double Ms,
                                       const spx_demag_options* opt, int64_t nsamples, const int64_t* node_offsets,
