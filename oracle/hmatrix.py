@@ -11,6 +11,10 @@ Restates:
   larger-diameter node subdivided first :260-275)
 * ``HMatrixStorageBuilder.finalize`` and ``HMatrixCPUData.matvec_cpu``
   storage.py:175-190, :333-390
+* ``PackedCPU``: the same matvec (x~ = x[perm]; diag jump + near CSR + sum_b U_b (V_b x~))
+  over the arrays of the reference's npz cache schema (``HMatrixCPUData.save``,
+  storage.py:77-149), row- and block-parallel on all host threads (numba); per-thread
+  partial sums of the far field are added at the end.  Used as the timed CPU baseline.
 """
 from __future__ import annotations
 
@@ -211,3 +215,81 @@ def build(bd, epsilon=1e-5, eta=2.0, leaf_size=64, max_rank=None,
         near = sp.csr_matrix((Nb, Nb))
     return HOracle(perm=perm, diag_jump=lindholm.diag_jump(bd), near=near, far=far,
                    dense_blocks=dense, stats=stats)
+
+
+def _packed_kernels():
+    from numba import njit, prange
+
+    @njit(parallel=True, cache=False)
+    def near_part(indptr, indices, data, diag, xp, y):
+        for i in prange(indptr.size - 1):
+            acc = diag[i] * xp[i]
+            for k in range(indptr[i], indptr[i + 1]):
+                acc += data[k] * xp[indices[k]]
+            y[i] = acc
+
+    @njit(parallel=True, cache=False)
+    def far_part(meta, U, V, xp, ybuf, chunk_start):
+        nth = ybuf.shape[0]
+        for t in prange(nth):
+            zt = np.empty(256)
+            for b in range(chunk_start[t], chunk_start[t + 1]):
+                rs, re, cs, ce, k = meta[b, 0], meta[b, 1], meta[b, 2], meta[b, 3], meta[b, 4]
+                uo, vo = meta[b, 5], meta[b, 6]
+                n = ce - cs
+                if k > zt.size:
+                    zt = np.empty(k)
+                for q in range(k):                    # z = V x~[cs:ce], V is k x n row-major
+                    acc = 0.0
+                    base = vo + q * n
+                    for c in range(n):
+                        acc += V[base + c] * xp[cs + c]
+                    zt[q] = acc
+                for r in range(re - rs):              # y += U z, U is m x k row-major
+                    acc = 0.0
+                    base = uo + r * k
+                    for q in range(k):
+                        acc += U[base + q] * zt[q]
+                    ybuf[t, rs + r] += acc
+
+    return near_part, far_part
+
+
+class PackedCPU:
+    """H-matrix apply over the reference's cache arrays on all host threads (see header)."""
+
+    def __init__(self, arrays, threads=None):
+        import os
+        import numba
+        self.perm = np.asarray(arrays["perm"], np.int64)
+        self.diag = np.asarray(arrays["diag_jump"], np.float64)[self.perm]
+        self.indptr = np.asarray(arrays["near_indptr"], np.int64)
+        self.indices = np.asarray(arrays["near_indices"], np.int32)
+        self.data = np.asarray(arrays["near_data"], np.float64)
+        fm = arrays["far_meta"]
+        self.meta = np.stack([fm["row_start"], fm["row_stop"], fm["col_start"], fm["col_stop"], fm["rank"],
+                              fm["u_offset"], fm["v_offset"]], axis=1).astype(np.int64) if len(fm) else \
+            np.zeros((0, 7), np.int64)
+        self.U = np.asarray(arrays["far_U_flat"], np.float64)
+        self.V = np.asarray(arrays["far_V_flat"], np.float64)
+        self.threads = int(threads or numba.get_num_threads() or os.cpu_count() or 1)
+        # blocks dealt to threads in contiguous runs of about equal factor entries
+        w = (self.meta[:, 1] - self.meta[:, 0] + self.meta[:, 3] - self.meta[:, 2]) * self.meta[:, 4]
+        cw = np.concatenate([[0], np.cumsum(w)])
+        targets = cw[-1] * np.arange(self.threads + 1) / self.threads
+        self.chunk = np.searchsorted(cw, targets).astype(np.int64)
+        self.chunk[0], self.chunk[-1] = 0, self.meta.shape[0]
+        self.near_k, self.far_k = _packed_kernels()
+        self.ybuf = np.zeros((self.threads, self.perm.size))
+
+    def matvec(self, x):
+        x = np.asarray(x, dtype=np.float64)
+        xp = x[self.perm]
+        yp = np.empty_like(xp)
+        self.near_k(self.indptr, self.indices, self.data, self.diag, xp, yp)
+        self.ybuf[:] = 0.0
+        self.far_k(self.meta, self.U, self.V, xp, self.ybuf, self.chunk)
+        yp += self.ybuf.sum(axis=0)
+        y = np.empty_like(x)
+        y[self.perm] = yp
+        return y

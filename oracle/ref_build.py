@@ -27,7 +27,9 @@ from pathlib import Path
 
 import numpy as np
 
-REF_ROOT = Path("/root/reference/src/spinfemx")
+# The reference checkout this recipe reads: $SPX_REFERENCE_PATH, by default the
+# read-only checkout beside the build container's repository.
+REF_ROOT = Path(os.environ.get("SPX_REFERENCE_PATH", "/root/reference")) / "src" / "spinfemx"
 HERE = Path(__file__).resolve().parent
 REF_OUT = HERE / "_ref"
 

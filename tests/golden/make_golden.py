@@ -16,6 +16,11 @@ Each fixture holds seeded inputs and the outputs of the REFERENCE's own code:
   (CPU, full-pivot ACA): block partition, ranks, near nnz, H @ x.
 * ``hcache_film14.npz``  the reference's own npz cache (``HMatrixCPUData.save``,
   storage.py:72-149) of a 14x14x2 film H-matrix (eps 1e-4, leaf 16), for the cache reader.
+* ``c2_rows.npz``  4,096 seeded boundary rows of the dense operator of the 400x400x2 film
+  (2.5 nm cubes, Nb = 323,202): ``LindholmEntryProviderCPU.fill_block(rows, all)`` plus the
+  diagonal jump, applied to three vectors defined by ``c2_row_vectors`` (random, smooth
+  in-plane, linear through the thickness); stores the row sums and B[rows] @ x.  About two
+  minutes on 8 cores (``python tests/golden/make_golden.py c2_rows``).
 * ``example_chain_mesh.npz``  the reference's octahedral-nanoparticle chain example mesh
   (examples/cpu/hysteresis_octahedral_nanoparticles/chain.xdmf + .h5) read by spinfemx_b200.io.
 * ``torque_kernels.npz``  the reference's STT / SOT per-node kernel bodies
@@ -41,7 +46,7 @@ sys.path.insert(0, str(ROOT))
 from oracle import lindholm, mesh, ref_build  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
-REF_EXAMPLES = Path("/root/reference/examples")
+REF_EXAMPLES = ref_build.REF_ROOT.parents[1] / "examples"
 
 CASES = {
     # name: (nx, ny, nz, h)
@@ -288,6 +293,50 @@ def make_torque_kernels():
     np.savez_compressed(OUT / "torque_kernels.npz", **out)
 
 
+C2_CASE = (400, 400, 2, 2.5)
+C2_ROWS_SEED = 3100
+
+
+def c2_row_vectors(Xb):
+    """The three vectors the c2_rows fixture applies B to (boundary order, Nb x 3):
+    seeded standard normal; cos(2 pi x / 1000) cos(2 pi y / 1000) (smooth at the film's
+    scale); z - mean(z) plus 0.1 x seeded noise (linear through the thickness)."""
+    Nb = Xb.shape[0]
+    rng = np.random.default_rng(C2_ROWS_SEED + 1)
+    x = np.empty((Nb, 3))
+    x[:, 0] = rng.standard_normal(Nb)
+    x[:, 1] = np.cos(2 * math.pi * Xb[:, 0] / 1000.0) * np.cos(2 * math.pi * Xb[:, 1] / 1000.0)
+    x[:, 2] = (Xb[:, 2] - Xb[:, 2].mean()) + 0.1 * rng.standard_normal(Nb)
+    return x
+
+
+def make_c2_rows(mods, nrows=4096, chunk=256):
+    """Rows of the reference's dense Lindholm operator on the 400x400x2 film (the
+    H-matrix headline mesh), with the diagonal jump Omega/4pi - 1 added, applied to
+    c2_row_vectors: the reference answer for the H-matrix apply at full size."""
+    X, T = mesh.kuhn_box(*C2_CASE)
+    bd = lindholm.boundary_data(X, T)
+    Nb = bd["Xb"].shape[0]
+    prov = provider_for(mods, bd)
+    rng = np.random.default_rng(C2_ROWS_SEED)
+    rows = np.sort(rng.choice(Nb, nrows, replace=False)).astype(np.int32)
+    x = c2_row_vectors(bd["Xb"])
+    cols = np.arange(Nb, dtype=np.int32)
+    y = np.empty((nrows, 3))
+    rowsum = np.empty(nrows)
+    jump = bd["omega_sum"] / (4.0 * math.pi) - 1.0
+    for s in range(0, nrows, chunk):
+        r = rows[s:s + chunk]
+        B = prov.fill_block(r, cols)
+        B[np.arange(r.size), r] += jump[r]
+        y[s:s + chunk] = B @ x
+        rowsum[s:s + chunk] = B.sum(axis=1)
+        print(f"c2_rows {s + r.size}/{nrows}", flush=True)
+    np.savez_compressed(OUT / "c2_rows.npz", rows=rows, y=y, rowsum=rowsum, nb=np.int64(Nb),
+                        x_sum=x.sum(axis=0), x_sqsum=(x * x).sum(axis=0), seed=np.int64(C2_ROWS_SEED),
+                        case=np.array(C2_CASE, dtype=np.float64))
+
+
 def make_example_mesh():
     """The reference's hysteresis_octahedral_nanoparticles/chain mesh (XDMF + gzip HDF5) read by
     spinfemx_b200.io, stored as example_chain_mesh.npz: a small unstructured mesh for the GPU
@@ -300,6 +349,9 @@ def make_example_mesh():
 
 def main():
     mods = ref_build.import_reference_hmatrix()
+    if sys.argv[1:] == ["c2_rows"]:
+        make_c2_rows(mods)
+        return
     bds = {}
     for name, (nx, ny, nz, h) in CASES.items():
         X, T = mesh.kuhn_box(nx, ny, nz, h)
@@ -316,6 +368,7 @@ def main():
         d = make_hmatrix(mods, name, bds[name])
         print(name, "far", len(d.far_blocks), "near nnz", d.near_csr.nnz, flush=True)
     make_cache(mods)
+    make_c2_rows(mods)
 
 
 if __name__ == "__main__":

@@ -7,7 +7,7 @@ Tolerances (relative unless stated):
   demag, dense FP64, tight CG          1e-9 ; reference CG tolerance (rtol 1e-6) 1e-5
   demag, H-matrix FP64                 1e-5
   LLG field / RHS / Jv / PC (FP64)     1e-11
-  RK4 trajectory (FP64, 20x20x5 box)   max|dm| 1e-8
+  RK4 trajectory (FP64, 20x20x5 box, 200 steps of 10 fs)   max|dm| 1e-8
 """
 import math
 
@@ -269,11 +269,12 @@ def test_llg_field_rhs_jv_pc_vs_oracle(spx, with_demag):
 
 
 def test_rk4_trajectory_box20_vs_oracle(spx, box20_oracle):
-    # 20x20x5 box (2 nm cubes): dense FP64 demag + exchange, alpha 0.5, dt 10 fs
+    # the small-box workload: 20x20x5 box (2 nm cubes), dense FP64 demag + exchange,
+    # alpha 0.5, 200 fixed steps of 10 fs from the seeded (1,1,1)/sqrt(3) + N(0, 0.1^2) state
     o = box20_oracle
     m0 = _m0(o.N)
     ohef = ollg.EffectiveFieldOracle(o.X, o.tets, 8e5, Aex=1.3e-11, alpha=0.5, demag=o)
-    nsteps = 20
+    nsteps = 200
     m = m0.copy()
     for _ in range(nsteps):
         m = ollg.rk4_step(ohef.llg_rhs, m, 1e-14)

@@ -224,3 +224,22 @@ def test_zhang_li_known_answer():
     z = torques.apply3(Z, m.ravel()).reshape(-1, 3)
     assert np.abs(z - (G @ Jd)[None, :]).max() < 1e-12
     assert np.abs(Z @ np.ones(N)).max() < 1e-14
+
+
+def test_packed_cpu_apply_equals_matvec():
+    """The thread-parallel CPU apply over the cache arrays (the timed CPU baseline) equals
+    the oracle's HMatrixCPUData.matvec_cpu restatement."""
+    import bench
+    from oracle import hmatrix as ohm
+    from oracle import lindholm as olin
+    from oracle import mesh as omesh
+
+    class A:
+        nx, ny, nz, h, hmatrix_epsilon, hmatrix_leaf = 24, 24, 2, 2.5, 1e-5, 32
+    arrays = bench.film_hmatrix_arrays(A)
+    assert len(arrays["far_meta"]) > 0
+    P = ohm.PackedCPU(arrays, threads=4)
+    X, T = omesh.kuhn_box(24, 24, 2, 2.5)
+    h = ohm.build(olin.boundary_data(X, T), epsilon=1e-5, eta=2.0, leaf_size=32)
+    x = np.random.default_rng(3).standard_normal(P.perm.size)
+    assert np.abs(P.matvec(x) - h.matvec(x)).max() <= 1e-13 * np.abs(h.matvec(x)).max()
