@@ -10,6 +10,8 @@ namespace {
 thread_local std::string g_last_error;
 }
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+std::atomic<int64_t> g_fail_alloc_min_bytes{0};
+std::atomic<int32_t> g_fail_alloc_count{0};
 }  // namespace spx
 
 using namespace spx;
@@ -242,6 +244,11 @@ struct LLGBase {
   virtual void set_graph(int on) = 0;
   virtual void graph_stats(int64_t* replays, int32_t* active) const = 0;
   virtual std::string graph_error() const = 0;
+  virtual void set_time_field(const double* h3, const double* hn, cudaStream_t s) = 0;
+  virtual void step_time_field(double dt, const double* htu, const double* htn, cudaStream_t s) = 0;
+  virtual double rk_attempt(double dt, double rtol, double atol, const double* htu, const double* htn, bool reuse,
+                            cudaStream_t s) = 0;
+  virtual void rk_accept(cudaStream_t s) = 0;
 };
 
 template <class TV, class TM>
@@ -286,9 +293,37 @@ struct LLGImpl : LLGBase {
     l.pc_apply(in(x, s), q, s);
     out(y, s);
   }
-  void set_state(const double* m, cudaStream_t s) override { convert<double, TV>(3 * l.N, m, l.m.p, s); }
+  void set_state(const double* m, cudaStream_t s) override {
+    l.rk_fsal = false;
+    convert<double, TV>(3 * l.N, m, l.m.p, s);
+  }
   void get_state(double* m, cudaStream_t s) override { convert<TV, double>(3 * l.N, l.m.p, m, s); }
-  void step(double dt, int64_t n, cudaStream_t s) override { l.step_rk4(dt, n, s); }
+  void step(double dt, int64_t n, cudaStream_t s) override {
+    l.rk_fsal = false;
+    l.step_rk4(dt, n, s);
+  }
+  DevBuf<TV> tstage;
+  // nodal stage fields [nst][3N] in the pipeline's vector type (FP64 pipelines use the caller's)
+  const TV* stage_fields(const double* hn, int nst, cudaStream_t s) {
+    if (!hn) return nullptr;
+    if (f64) return reinterpret_cast<const TV*>(hn);
+    if (tstage.n < static_cast<size_t>(nst * 3 * l.N)) tstage.alloc(static_cast<size_t>(nst) * 3 * l.N);
+    convert<double, TV>(nst * 3 * l.N, hn, tstage.p, s);
+    return tstage.p;
+  }
+  void set_time_field(const double* h3, const double* hn, cudaStream_t s) override {
+    l.set_time_field(h3, stage_fields(hn, 1, s), s);
+  }
+  void step_time_field(double dt, const double* htu, const double* htn, cudaStream_t s) override {
+    l.graph_reset();
+    l.rk_fsal = false;
+    l.step_once(dt, s, htu, stage_fields(htn, 4, s));
+  }
+  double rk_attempt(double dt, double rtol, double atol, const double* htu, const double* htn, bool reuse,
+                    cudaStream_t s) override {
+    return l.rk_attempt(dt, rtol, atol, htu, stage_fields(htn, 7, s), reuse, s);
+  }
+  void rk_accept(cudaStream_t s) override { l.rk_accept(s); }
   void run_host(const double* hin, double* hout, double dt, int64_t n) override {
     const int64_t n3 = 3 * l.N;
     cudaStream_t s = 0;
@@ -302,6 +337,7 @@ struct LLGImpl : LLGBase {
   }
   void set_uniform_field(double x, double y, double z) override {
     l.graph_reset();
+    l.rk_fsal = false;
     l.H0.release();
     l.h0[0] = x; l.h0[1] = y; l.h0[2] = z;
   }
@@ -354,6 +390,7 @@ struct LLGImpl : LLGBase {
   }
   void set_ku_map(const double* ku) override {
     l.graph_reset();
+    l.rk_fsal = false;
     l.set_ku_map(ku, 0);
   }
   void zhang_li(const double* m, double* o, cudaStream_t s) override {
@@ -363,6 +400,7 @@ struct LLGImpl : LLGBase {
   }
   void set_sot(double Hdl, double Hfl, const double* p) override {
     l.graph_reset();
+    l.rk_fsal = false;
     l.set_sot(Hdl, Hfl, p, 0);
   }
   void min_eval(double* m, double* d, int normalize, double* out5, cudaStream_t s) override {
@@ -772,6 +810,14 @@ int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int
   API_END
 }
 
+int spx_debug_fail_alloc(int64_t min_bytes, int32_t count) {
+  API_BEGIN
+  SPX_CHECK(min_bytes >= 0 && count >= 0, "min_bytes and count must be non-negative");
+  spx::g_fail_alloc_min_bytes.store(min_bytes);
+  spx::g_fail_alloc_count.store(count);
+  API_END
+}
+
 int spx_hmat_destroy(spx_hmat hm) {
   API_BEGIN
   SPX_CHECK(!hm || !hm->ext, "this H-matrix handle belongs to a demag object (destroy the demag object instead)");
@@ -1139,6 +1185,48 @@ int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, in
   REQUIRE(l); REQUIRE(m_in); REQUIRE(m_out);
   SPX_CHECK(dt > 0.0 && nsteps >= 0, "dt must be positive and nsteps non-negative");
   l->impl->run_host(m_in, m_out, dt, nsteps);
+  API_END
+}
+
+int spx_llg_set_time_field(spx_llg l, const double* h_uniform3, const double* h_nodes, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->set_time_field(h_uniform3, h_nodes, S(s));
+  API_END
+}
+
+int spx_llg_step_time_field(spx_llg l, double dt, const double* h_uniform4x3, const double* h_nodes4,
+                            spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l);
+  SPX_CHECK(dt > 0.0, "dt must be positive");
+  l->impl->step_time_field(dt, h_uniform4x3, h_nodes4, S(s));
+  API_END
+}
+
+int spx_llg_rk_attempt(spx_llg l, int32_t scheme, double dt, double rtol, double atol, const double* h_uniform7x3,
+                       const double* h_nodes7, int32_t reuse_fsal, double* err_norm, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(err_norm);
+  SPX_CHECK(scheme == 0, "scheme must be 0 (Dormand-Prince 5(4))");
+  SPX_CHECK(dt > 0.0, "dt must be positive");
+  SPX_CHECK(rtol >= 0.0 && atol >= 0.0 && rtol + atol > 0.0, "rtol and atol must be non-negative, not both zero");
+  *err_norm = l->impl->rk_attempt(dt, rtol, atol, h_uniform7x3, h_nodes7, reuse_fsal != 0, S(s));
+  API_END
+}
+
+int spx_llg_rk_accept(spx_llg l, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->rk_accept(S(s));
+  API_END
+}
+
+int spx_vec_node_diff_max(const double* a, const double* b, int64_t N, double* out, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(a); REQUIRE(b); REQUIRE(out);
+  SPX_CHECK(N >= 0, "N must be non-negative");
+  *out = N ? spx::node_diff_max(N, a, b, S(s)) : 0.0;
   API_END
 }
 

@@ -87,6 +87,14 @@ __global__ void __launch_bounds__(256) k_stage(StageArgs<TV, TM> a) {
       hy += a.h0y;
       hz += a.h0z;
     }
+    if (a.Ht) {
+      hx += a.Ht[3 * i];
+      hy += a.Ht[3 * i + 1];
+      hz += a.Ht[3 * i + 2];
+    }
+    hx += a.htx;
+    hy += a.hty;
+    hz += a.htz;
     if (a.mode == 0) {
       a.out[3 * i] = hx;
       a.out[3 * i + 1] = hy;
@@ -394,7 +402,16 @@ __global__ void k_mdoth(int64_t n, const double* __restrict__ w, const TV* __res
     s += w[i] * (static_cast<double>(m[3 * i]) * H[3 * i] + static_cast<double>(m[3 * i + 1]) * H[3 * i + 1] +
                  static_cast<double>(m[3 * i + 2]) * H[3 * i + 2]);
   s = block_sum(s, sh);
-  if (threadIdx.x == 0) atomicAdd(out, s);
+  if (threadIdx.x == 0) out[blockIdx.x] = s;  // one partial per CTA, summed in a fixed order
+}
+
+// out[0] = sum of part[0..n) in a fixed order (one CTA), so the energy is run-to-run exact
+__global__ void k_sum_parts(int n, const double* __restrict__ part, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) out[0] = s;
 }
 
 template <class A, class B>
@@ -565,6 +582,10 @@ StageArgs<TV, TM> LLGCtx<TV, TM>::args(const TV* min, TV* out, int mode, bool wi
   a.h0x = static_cast<TV>(h0[0]);
   a.h0y = static_cast<TV>(h0[1]);
   a.h0z = static_cast<TV>(h0[2]);
+  a.Ht = ht_nodes.n ? ht_nodes.p : nullptr;
+  a.htx = static_cast<TV>(ht[0]);
+  a.hty = static_cast<TV>(ht[1]);
+  a.htz = static_cast<TV>(ht[2]);
   a.m = min;
   a.out = out;
   a.pref = static_cast<TV>(pref);
@@ -694,7 +715,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
 }
 
 template <class TV, class TM>
-void LLGCtx<TV, TM>::step_once(double dt, cudaStream_t s) {
+void LLGCtx<TV, TM>::step_once(double dt, cudaStream_t s, const double* htu, const TV* htn) {
   const TV h = static_cast<TV>(dt);
   for (int64_t it = 0; it < 1; ++it) {
     const TV* in[4] = {m.p, ms0.p, ms1.p, ms0.p};
@@ -710,6 +731,12 @@ void LLGCtx<TV, TM>::step_once(double dt, cudaStream_t s) {
       a.c_next = cnext[st];
       a.w_acc = wacc[st];
       a.dt6 = h / TV(6);
+      if (htu || htn) {  // per-stage time field replaces the current-time one
+        a.htx = htu ? static_cast<TV>(htu[3 * st]) : TV(0);
+        a.hty = htu ? static_cast<TV>(htu[3 * st + 1]) : TV(0);
+        a.htz = htu ? static_cast<TV>(htu[3 * st + 2]) : TV(0);
+        a.Ht = htn ? htn + 3 * N * st : nullptr;
+      }
       Profiler* pf = use_demag ? &demag->prof : nullptr;
       if (pf) pf->mark(PC_STAGE, s);
       launch_stage(a, use_demag, s);
@@ -817,12 +844,14 @@ template struct LLGCtx<double, float>;
 
 template <class TV, class TM>
 double demag_energy(DemagCtx<TV, TM>& d, const TV* m, const TV* H, cudaStream_t s) {
-  DevBuf<double> r(1);
-  r.zero(s);
-  k_mdoth<TV><<<std::min<unsigned>(grid_for(d.N, 256), 1184), 256, 0, s>>>(d.N, d.vol.p, m, H, r.p);
+  const unsigned grid = std::max(1u, std::min<unsigned>(grid_for(d.N, 256), 1184));
+  DevBuf<double> r(grid + 1);
+  k_mdoth<TV><<<grid, 256, 0, s>>>(d.N, d.vol.p, m, H, r.p);
+  SPX_LAUNCH_CHECK();
+  k_sum_parts<<<1, 256, 0, s>>>(static_cast<int>(grid), r.p, r.p + grid);
   SPX_LAUNCH_CHECK();
   double h = 0.0;
-  SPX_CUDA(cudaMemcpyAsync(&h, r.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  SPX_CUDA(cudaMemcpyAsync(&h, r.p + grid, sizeof(double), cudaMemcpyDeviceToHost, s));
   SPX_CUDA(cudaStreamSynchronize(s));
   return -0.5 * d.mu0 * d.Ms * h / 1e27;
 }

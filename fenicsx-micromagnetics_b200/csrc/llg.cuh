@@ -41,6 +41,8 @@ struct StageArgs {
   TV ani_p0;         // scalar prefactor when ani_p == null
   const TV* H0;      // [3n] (or null)
   TV h0x, h0y, h0z;
+  const TV* Ht;      // [3n] time-dependent applied field at this evaluation's time (or null)
+  TV htx, hty, htz;  // its uniform part
   const TV* m;       // stage input (AoS)
   TV* out;           // mode 0: H ; mode 1: rhs ; mode 2: next stage m
   TV* mn;            // RK state (mode 2)
@@ -102,7 +104,25 @@ struct LLGCtx {
   int64_t gepoch = -1, graph_replays = 0;
   std::string graph_error;
   void graph_reset();
-  void step_once(double dt, cudaStream_t s);
+  // one classic RK4 step; htu (host [4][3]) / htn (device [4][3N]) optional per-stage
+  // time-dependent fields (stage times t, t + dt/2, t + dt/2, t + dt)
+  void step_once(double dt, cudaStream_t s, const double* htu = nullptr, const TV* htn = nullptr);
+  // time-dependent applied field (EffectiveField.H_time_func, llg_module_GPU.py:909-956,
+  // 998-1000): the value at the current time, added by heff / rhs / the Jacobian state
+  double ht[3] = {0.0, 0.0, 0.0};
+  DevBuf<TV> ht_nodes;  // [3N] nodal part (empty: none)
+  void set_time_field(const double* h3, const TV* h_nodes, cudaStream_t s);
+  // embedded explicit Runge-Kutta (drivers.cu): Dormand-Prince 5(4) with first-same-as-last,
+  // the scheme of the reference's PETSc TS rk/5dp (llg_module_GPU.py:1724-1787)
+  DevBuf<TV> rk_k[7], rk_y, rk_ynew;
+  DevBuf<double> rk_part;
+  bool rk_fsal = false;
+  // one attempt of size dt from the state m: rk_ynew = 5th-order solution, returns the
+  // weighted RMS norm of the embedded error (tol_i = atol + rtol max(|y5_i|, |y4_i|)).
+  // htu (host [7][3]) / htn (device [7][3N]): per-stage time fields at t + c_i dt, or null.
+  double rk_attempt(double dt, double rtol, double atol, const double* htu, const TV* htn, bool reuse_fsal,
+                    cudaStream_t s);
+  void rk_accept(cudaStream_t s);  // m = rk_ynew; k1 of the next attempt = k7 (FSAL)
   LLGCtx() = default;
   LLGCtx(const LLGCtx&) = delete;
   LLGCtx& operator=(const LLGCtx&) = delete;
@@ -149,6 +169,9 @@ struct LLGCtx {
 
 template <class A, class B>
 void convert(int64_t n, const A* src, B* dst, cudaStream_t s);
+
+// max over nodes of |a_i - b_i| for AoS FP64 device vectors [n][3] (drivers.cu)
+double node_diff_max(int64_t n, const double* a, const double* b, cudaStream_t s);
 
 template <class TV, class TM>
 double demag_energy(DemagCtx<TV, TM>& d, const TV* m, const TV* H, cudaStream_t s);

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -56,6 +57,19 @@ void set_last_error(const std::string& msg);
 #define SPX_LAUNCH_CHECK() SPX_CUDA(cudaGetLastError())
 
 // ---------------------------------------------------------------- buffers
+// Allocation-failure injection for tests of the out-of-memory paths (spx_debug_fail_alloc):
+// the next g_fail_alloc_count device allocations of at least g_fail_alloc_min_bytes bytes
+// fail with ERR_OOM before cudaMalloc is called.  Host-side only; no device fault.
+extern std::atomic<int64_t> g_fail_alloc_min_bytes;
+extern std::atomic<int32_t> g_fail_alloc_count;
+inline void injected_alloc_failure(size_t bytes) {
+  if (g_fail_alloc_count.load(std::memory_order_relaxed) <= 0) return;
+  if (static_cast<int64_t>(bytes) < g_fail_alloc_min_bytes.load(std::memory_order_relaxed)) return;
+  if (g_fail_alloc_count.fetch_sub(1) > 0)
+    throw Error(ERR_OOM, "cudaMalloc: out of memory (injected by spx_debug_fail_alloc, " + std::to_string(bytes) +
+                             " bytes)");
+}
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -73,7 +87,10 @@ struct DevBuf {
   void alloc(size_t count) {
     release();
     n = count;
-    if (count) SPX_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)));
+    if (count) {
+      injected_alloc_failure(count * sizeof(T));
+      SPX_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T)));
+    }
   }
   void release() {
     if (p) cudaFree(p);

@@ -52,6 +52,21 @@ STAT_NAMES = ("dense_blocks", "low_rank_blocks", "rejected_low_rank_blocks", "fo
 
 @dataclass
 class HMatrixBuildConfig:
+    """The reference's build configuration (builder.py:24-95): same fields, defaults and
+    validation messages, except that this library builds on the GPU only.
+
+    * ``build_backend``: "gpu" (the default here) and "auto" build on the current CUDA device;
+      "cpu" (the reference's default, its numba builder) is refused with ValueError.
+    * ``gpu_device_id`` must name the current CUDA device: the H-matrix is built and applied
+      where the caller's tensors live.
+    * ``gpu_memory_fraction`` bounds the build's device workspace to that fraction of the
+      free device memory (at most 6 GiB); ``batch_bytes`` > 0 sets it directly.
+    * ``gpu_fallback_to_cpu``: there is no CPU builder to fall back to.  On an allocation
+      failure the build retries with half the workspace (down to 64 MiB) and raises
+      MemoryError only when that fails too.
+    * the randomized-SVD and progress fields are accepted and validated; the compressor is
+      full-pivot ACA.
+    """
     epsilon: float = 1e-6
     eta: float = 2.0
     leaf_size: int = 64
@@ -60,6 +75,14 @@ class HMatrixBuildConfig:
     max_temporary_block_bytes: int = 256 * 1024 * 1024
     low_rank_storage_factor: float = 0.95
     build_backend: str = "gpu"
+    gpu_device_id: int | None = None
+    gpu_memory_fraction: float = 0.75
+    gpu_fallback_to_cpu: bool = True
+    gpu_aca_residual_check_interval: int = 1
+    gpu_rsvd_initial_rank: int = 16
+    gpu_rsvd_oversampling: int = 8
+    gpu_rsvd_power_iterations: int = 1
+    gpu_progress_interval_seconds: float = 5.0
     batch_bytes: int = 0
 
     def __post_init__(self):
@@ -84,13 +107,76 @@ class HMatrixBuildConfig:
         b = str(self.build_backend).strip().lower()
         if b not in {"gpu", "auto", "cpu"}:
             raise ValueError("build_backend must be 'cpu', 'gpu', or 'auto'.")
-        self.build_backend = "gpu"
+        if b == "cpu":
+            raise ValueError("build_backend='cpu' (the reference's numba builder) is not part of this library; "
+                             "use 'gpu' or 'auto'")
+        self.build_backend = b
+        if self.gpu_device_id is not None:
+            self.gpu_device_id = int(self.gpu_device_id)
+            if self.gpu_device_id < 0:
+                raise ValueError("gpu_device_id must be non-negative.")
+        if not (0.0 < float(self.gpu_memory_fraction) <= 1.0):
+            raise ValueError("gpu_memory_fraction must be in (0, 1].")
+        if self.gpu_aca_residual_check_interval < 1:
+            raise ValueError("gpu_aca_residual_check_interval must be positive.")
+        if self.gpu_rsvd_initial_rank < 1:
+            raise ValueError("gpu_rsvd_initial_rank must be positive.")
+        if self.gpu_rsvd_oversampling < 0:
+            raise ValueError("gpu_rsvd_oversampling must be non-negative.")
+        if self.gpu_rsvd_power_iterations < 0:
+            raise ValueError("gpu_rsvd_power_iterations must be non-negative.")
+        if self.gpu_progress_interval_seconds < 0.0:
+            raise ValueError("gpu_progress_interval_seconds must be non-negative.")
 
-    def to_c(self, precision="f64"):
+    def workspace_bytes(self):
+        """Device workspace of one fill/ACA batch: batch_bytes if set, else gpu_memory_fraction
+        of the free device memory, at most 6 GiB."""
+        if self.batch_bytes > 0:
+            return int(self.batch_bytes)
+        try:
+            import torch
+            free = torch.cuda.mem_get_info()[0] if torch.cuda.is_available() else 0
+        except Exception:
+            free = 0
+        cap = 6 * 1024 ** 3
+        return int(min(cap, self.gpu_memory_fraction * free)) if free else 0
+
+    def check_device(self):
+        if self.gpu_device_id is None:
+            return
+        import torch
+        cur = torch.cuda.current_device()
+        if self.gpu_device_id != cur:
+            raise ValueError(f"gpu_device_id={self.gpu_device_id} differs from the current CUDA device {cur}; "
+                             "the H-matrix is built and applied on the current device")
+
+    def to_c(self, precision="f64", batch_bytes=None):
+        bb = self.batch_bytes if batch_bytes is None else batch_bytes
         return _lib.HmatConfig(epsilon=self.epsilon, eta=self.eta, leaf_size=int(self.leaf_size),
                                max_rank=int(self.max_rank or 0),
                                max_temporary_block_bytes=int(self.max_temporary_block_bytes),
-                               precision=_lib.PREC[precision], reserved=0, batch_bytes=int(self.batch_bytes))
+                               precision=_lib.PREC[precision], reserved=0, batch_bytes=int(bb))
+
+
+MIN_WORKSPACE = 64 * 1024 ** 2
+
+
+def build_with_retry(geometry, cfg, precision):
+    """spx_hmat_build with the workspace of cfg; on an allocation failure the build is
+    repeated with half the workspace, down to 64 MiB (the reference instead subdivides the
+    block or falls back to its CPU builder, builder.py:597-662, 880-901)."""
+    ws = cfg.workspace_bytes()
+    while True:
+        h = C.c_void_p()
+        c = cfg.to_c(precision, batch_bytes=ws)
+        try:
+            call("spx_hmat_build", geometry.handle, C.byref(c), C.byref(h))
+            return h
+        except MemoryError:
+            cur = ws if ws > 0 else 6 * 1024 ** 3
+            if cur // 2 < MIN_WORKSPACE:
+                raise
+            ws = cur // 2
 
 
 def _precision_name(use_fp32=True, precision=None):
@@ -127,9 +213,8 @@ class HMatrixGPUPackedFused:
                 raise ValueError("a BoundaryGeometry is required")
             self._geometry = geometry
             cfg = config or HMatrixBuildConfig()
-            self._h = C.c_void_p()
-            c = cfg.to_c(self.precision)
-            call("spx_hmat_build", geometry.handle, C.byref(c), C.byref(self._h))
+            cfg.check_device()
+            self._h = build_with_retry(geometry, cfg, self.precision)
             self._owned = True
         n = _lib.c_i64()
         call("spx_hmat_num_blocks", self._h, C.byref(n))

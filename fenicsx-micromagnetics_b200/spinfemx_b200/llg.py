@@ -36,10 +36,16 @@ def _vec3(a, N, name):
     return a
 
 
+# Dormand-Prince 5(4) stage times (fractions of the step), see csrc/drivers.cu
+DP5_C = (0.0, 0.2, 0.3, 0.8, 8.0 / 9.0, 1.0, 1.0)
+RK4_C = (0.0, 0.5, 0.5, 1.0)
+
+
 class EffectiveField:
     def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani_vec=None, D_bulk=0.0, D_int=0.0, n0_int_vec=None,
                  gamma=2.211e5, alpha=0.5, do_precess=1, use_demag=False, demag_method="lindholm",
-                 demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64", _stt=None, _sot=None):
+                 demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64", H_time_func=None,
+                 _stt=None, _sot=None):
         if float(D_bulk) != 0.0:
             raise NotImplementedError("bulk DMI is not part of this build")
         if str(demag_method).lower() not in {"lindholm", "lindholm_gpu"}:
@@ -57,6 +63,8 @@ class EffectiveField:
         self.LLGSteps = 0
         self.JacSteps = 0
         self.current_time = 0.0
+        self.H_time_func = H_time_func
+        self._ht_time = None  # time of the field last handed to the library
         self.demag_field = None
         if use_demag:
             kw = dict(demag_kwargs or {})
@@ -121,15 +129,75 @@ class EffectiveField:
         self._H0 = np.tile([float(Hx), float(Hy), float(Hz)], self.N)
         self._H0_dev = None
 
+    # -------------------------------------------------------------- time-dependent field
+    def _eval_H_time(self, t):
+        """H_time_func at time t as (uniform [3] numpy or None, nodal [3N] CUDA float64 or None):
+        the callback is tried as f(t, x) with the mesh coordinates, then as f(t); it may return
+        (3,), (3N,) or (N, 3), as numpy or torch (llg_module_GPU.py:909-956)."""
+        import torch
+        try:
+            out = self.H_time_func(float(t), self.X)
+        except TypeError:
+            out = self.H_time_func(float(t))
+        if isinstance(out, torch.Tensor):
+            arr = out.detach().to(dtype=torch.float64)
+            if arr.numel() == 3:
+                return arr.cpu().numpy().reshape(3).copy(), None
+            if arr.numel() == 3 * self.N and (arr.dim() == 1 or tuple(arr.shape) == (self.N, 3)):
+                return None, arr.reshape(-1).to("cuda").contiguous()
+            raise ValueError(f"Unsupported torch H_time_func shape {tuple(arr.shape)}")
+        arr = np.asarray(out, dtype=np.float64)
+        if arr.ndim == 1 and arr.size == 3:
+            return arr.copy(), None
+        if (arr.ndim == 1 and arr.size == 3 * self.N) or arr.shape == (self.N, 3):
+            return None, torch.as_tensor(np.ascontiguousarray(arr.reshape(-1)), device="cuda")
+        raise ValueError("H_time_func must return (3,), (local_size,), or (local_dofs, 3) values.")
+
+    def _sync_time_field(self):
+        """Hand H_time_func(current_time) to the library before an evaluation."""
+        if self.H_time_func is None:
+            if self._ht_time is not None:  # a callback was removed: clear its field
+                call("spx_llg_set_time_field", self._h, None, None, _lib.stream_ptr())
+                self._ht_time = None
+            return
+        if self._ht_time == self.current_time:
+            return
+        u, n = self._eval_H_time(self.current_time)
+        call("spx_llg_set_time_field", self._h, ptr(u), ptr(n), _lib.stream_ptr())
+        self._ht_time = self.current_time
+
+    def _stage_fields(self, t, dt, cs):
+        """Per-stage values of H_time_func at t + c dt: (uniform [len(cs)][3] host, nodal
+        [len(cs)][3N] CUDA) with None where the callback gives no such part."""
+        import torch
+        vals = {}
+        for c in cs:
+            if c not in vals:
+                vals[c] = self._eval_H_time(t + c * dt)
+        if any(v[1] is not None for v in vals.values()):
+            nod = torch.zeros((len(cs), self.local_size), dtype=torch.float64, device="cuda")
+            for i, c in enumerate(cs):
+                if vals[c][1] is not None:
+                    nod[i] = vals[c][1]
+        else:
+            nod = None
+        uni = np.zeros((len(cs), 3))
+        for i, c in enumerate(cs):
+            if vals[c][0] is not None:
+                uni[i] = vals[c][0]
+        return np.ascontiguousarray(uni), nod
+
     def compute_H_eff_vec(self, m_vec, out_vec):
         self._chk(m_vec, "m_vec")
         self._chk(out_vec, "out_vec")
+        self._sync_time_field()
         call("spx_llg_heff", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
         self._tail(out_vec)
 
     def compute_H_jac_vec(self, m_vec, out_vec):
         self._chk(m_vec, "m_vec")
         self._chk(out_vec, "out_vec")
+        self._sync_time_field()
         call("spx_llg_hjac", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
         self._tail(out_vec)
 
@@ -145,11 +213,13 @@ class EffectiveField:
         self.LLGSteps += 1
         self._chk(m_vec, "m_vec")
         self._chk(out_vec, "out_vec")
+        self._sync_time_field()
         call("spx_llg_rhs", self._h, ptr(m_vec), ptr(out_vec), _lib.stream_ptr())
         self._tail(out_vec)
 
     def update_jac_state(self, m_vec):
         self._chk(m_vec, "m_vec")
+        self._sync_time_field()
         call("spx_llg_update_jac_state", self._h, ptr(m_vec), _lib.stream_ptr())
 
     def jac_vec_times_vec(self, v_vec, out_vec):
@@ -186,7 +256,30 @@ class EffectiveField:
         return out_vec
 
     def step(self, dt, nsteps=1):
-        call("spx_llg_step", self._h, float(dt), int(nsteps), _lib.stream_ptr())
+        """nsteps classic RK4 steps of size dt from the state; with H_time_func the field is
+        evaluated at each stage time (t, t + dt/2, t + dt) and current_time advances."""
+        if self.H_time_func is None:
+            call("spx_llg_step", self._h, float(dt), int(nsteps), _lib.stream_ptr())
+            return
+        for _ in range(int(nsteps)):
+            u, n = self._stage_fields(self.current_time, float(dt), RK4_C)
+            call("spx_llg_step_time_field", self._h, float(dt), ptr(u), ptr(n), _lib.stream_ptr())
+            self.current_time += float(dt)
+
+    def rk_attempt(self, dt, rtol, atol, reuse_fsal=True):
+        """One Dormand-Prince 5(4) attempt of size dt at current_time (not committed); returns
+        the weighted RMS norm of the embedded error (<= 1: acceptable)."""
+        u = n = None
+        if self.H_time_func is not None:
+            u, n = self._stage_fields(self.current_time, float(dt), DP5_C)
+        e = _lib.c_dbl()
+        call("spx_llg_rk_attempt", self._h, 0, float(dt), float(rtol), float(atol), ptr(u), ptr(n),
+             1 if reuse_fsal else 0, C.byref(e), _lib.stream_ptr())
+        return e.value
+
+    def rk_accept(self, dt):
+        call("spx_llg_rk_accept", self._h, _lib.stream_ptr())
+        self.current_time += float(dt)
 
     def set_graph(self, enable=True):
         """Replay each RK4 step from captured CUDA graphs (same results as ordinary steps)."""
@@ -301,15 +394,13 @@ class EffectiveFieldSTTGPU(EffectiveField):
                  H0_static=None, gamma=2.211e5, alpha=0.5, do_precess=1, Jmagnitude=0.0, Jdir_vec=None, P=0.0,
                  beta=0.0, use_demag=False, demag_method="lindholm", demag_kwargs=None, H_time_func=None,
                  precision="f64", Ku_nodes=None):
-        if H_time_func is not None:
-            raise NotImplementedError("time-dependent fields are not part of this build")
         if Jdir_vec is None:
             raise ValueError("Jdir_vec is required")
         self.Jmagnitude, self.P, self.beta = float(Jmagnitude), float(P), float(beta)
         super().__init__(X, tets, Ms, Aex=Aex, Ku=Ku, n_ani_vec=n_ani_vec, D_bulk=D_bulk, D_int=D_int,
                          n0_int_vec=n0_int_vec, gamma=gamma, alpha=alpha, do_precess=do_precess,
                          use_demag=use_demag, demag_method=demag_method, demag_kwargs=demag_kwargs,
-                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision,
+                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision, H_time_func=H_time_func,
                          _stt=(self.Jmagnitude, self.P, self.beta, Jdir_vec))
         e, muB = 1.6021766e-19, 9.27400915e-24
         self.prefZhang = (self.Jmagnitude * self.P * muB / (e * self.Ms * (1.0 + self.beta ** 2))
@@ -343,13 +434,11 @@ class EffectiveFieldSOTGPU(EffectiveField):
                  H0_static=None, gamma=2.211e5, alpha=0.5, do_precess=1, H_dl=0.0, H_fl=0.0,
                  polarization_vec=None, use_demag=False, demag_method="lindholm", demag_kwargs=None,
                  H_time_func=None, precision="f64", Ku_nodes=None):
-        if H_time_func is not None:
-            raise NotImplementedError("time-dependent fields are not part of this build")
         pol = (0.0, 1.0, 0.0) if polarization_vec is None else polarization_vec
         super().__init__(X, tets, Ms, Aex=Aex, Ku=Ku, n_ani_vec=n_ani_vec, D_bulk=D_bulk, D_int=D_int,
                          n0_int_vec=n0_int_vec, gamma=gamma, alpha=alpha, do_precess=do_precess,
                          use_demag=use_demag, demag_method=demag_method, demag_kwargs=demag_kwargs,
-                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision,
+                         H0_static=H0_static, Ku_nodes=Ku_nodes, precision=precision, H_time_func=H_time_func,
                          _sot=(float(H_dl), float(H_fl), pol))
         self.H_dl, self.H_fl = float(H_dl), float(H_fl)
         self._update_sot_coefficients()
@@ -429,9 +518,8 @@ class LLG_GPU:
         raise NotImplementedError("bulk DMI is not part of this build")
 
     def add_external_field(self, H0_vec=None, H_time_func=None):
-        if H_time_func is not None:
-            raise NotImplementedError("time-dependent fields are not part of this build")
         self._kw["H0_static"] = H0_vec
+        self._kw["H_time_func"] = H_time_func
 
     def _build(self):
         if self.hef is None:
@@ -439,6 +527,75 @@ class LLG_GPU:
                                       do_precess=self.do_precess, use_demag=self._demag is not None,
                                       demag_kwargs=self._demag, precision=self.precision, **self._kw)
         return self.hef
+
+    def relax_explicit(self, m0_array, t0, t_final, dt_init, rk_type="5dp", dt_save=None, dt_snap=None,
+                       output_dir="output_explicit", ts_rtol=1e-6, ts_atol=1e-6, stopping_dmdt=0.0,
+                       monitor_fn=None, save_final_state=False, check_every_stop=5, stop_print=False,
+                       return_stats=False, max_steps=50_000_000):
+        """Adaptive explicit relaxation (LLG_GPU.relax_explicit, llg_module_GPU.py:1790-1970).
+
+        Dormand-Prince 5(4) steps on the device (spx_llg_rk_attempt) from t0 until t_final is
+        reached or passed (PETSc ExactFinalTime STEPOVER), with the step adaptor of
+        _ensure_solver_explicit (:1765-1772, PETSc TSAdapt "basic"): weighted RMS error norm
+        with tol_i = atol + rtol max(|y5_i|, |y4_i|); accept when <= 1; next step
+        dt * clip(safety * err^(-1/5), 0.1, 3.0), safety 0.9, times the reject safety 0.1 after
+        a second rejection in a row; dt kept in [1e-18, 1e-10].  The dm/dt stopper
+        (StopByMaxDmdtFDGPU, :314-382) ends the run when max_i |m_i - m_prev_i| / (t - t_prev)
+        falls below stopping_dmdt deg/ns, tested every check_every_stop steps.  monitor_fn(step,
+        t, m) is called after every accepted step when given; with save_final_state the final
+        state is written as <output_dir>/Relax_explicit.xdmf (the reference also writes ADIOS2).
+        Returns (m, elapsed) or (m, elapsed, stats)."""
+        import time
+        import torch
+        if rk_type != "5dp":
+            raise ValueError("rk_type must be '5dp' (Dormand-Prince 5(4))")
+        hef = self._build()
+        if m0_array is not None:
+            m0 = m0_array if isinstance(m0_array, torch.Tensor) else torch.as_tensor(
+                np.asarray(m0_array, dtype=np.float64))
+            hef.set_state(m0.to(device="cuda", dtype=torch.float64).contiguous())
+        hef.current_time = float(t0)
+        ad = TSAdaptBasic()
+        stopper = DmdtStopper(hef, stopping_dmdt, check_every_stop, stop_print)
+        dt = min(max(float(dt_init), ad.dt_min), ad.dt_max)
+        step, reason, reuse = 0, 0, False
+        t_start = time.perf_counter()
+        while step < max_steps:
+            if hef.current_time >= float(t_final):
+                reason = 1          # TS_CONVERGED_TIME
+                break
+            accept_prev = True
+            while True:
+                enorm = hef.rk_attempt(dt, ts_rtol, ts_atol, reuse_fsal=reuse)
+                accept, dt_next = ad.choose(dt, enorm, accept_prev)
+                if accept:
+                    break
+                reuse = True        # k1 of the state is still valid
+                accept_prev = False
+                dt = dt_next
+            hef.rk_accept(dt)
+            reuse = True
+            step += 1
+            if monitor_fn is not None:
+                monitor_fn(step, hef.current_time, hef.get_state())
+            if stopper(step, hef.current_time):
+                reason = 2          # TS_CONVERGED_USER
+                dt = dt_next
+                break
+            dt = dt_next
+        elapsed = time.perf_counter() - t_start
+        m = hef.get_state()
+        if save_final_state:
+            from pathlib import Path
+            from .io import XDMFWriter
+            Path(output_dir).mkdir(parents=True, exist_ok=True)
+            XDMFWriter(Path(output_dir) / "Relax_explicit.xdmf", self.X, self.tets).write_function(
+                m, time=hef.current_time, name="m")
+        stats = {"t_end": float(hef.current_time), "dt_last": float(dt), "nsteps": int(step), "reason": int(reason),
+                 "rejected": int(ad.rejected), "maxdmdt_deg_ns": float(stopper.last_max_dmdt_deg_ns)}
+        if return_stats:
+            return m, elapsed, stats
+        return m, elapsed
 
     def run_fixed(self, m0, dt, nsteps):
         """Integrate nsteps of RK4 at step dt from m0 (3N numpy or CUDA tensor); returns m (CUDA tensor)."""
@@ -449,3 +606,63 @@ class LLG_GPU:
         hef.set_state(m)
         hef.step(dt, nsteps)
         return hef.get_state()
+
+
+class TSAdaptBasic:
+    """Step-size choice of PETSc's TSAdapt "basic" with the options the reference sets in
+    _ensure_solver_explicit (llg_module_GPU.py:1765-1772): clip (0.1, 3.0), safety 0.9,
+    reject safety 0.1, dt_min 1e-18, dt_max 1e-10; the error exponent is -1/5 (the
+    Dormand-Prince pair's order)."""
+
+    def __init__(self, clip=(0.1, 3.0), safety=0.9, reject_safety=0.1, dt_min=1e-18, dt_max=1e-10, order=5):
+        self.clip, self.safety, self.reject_safety = clip, safety, reject_safety
+        self.dt_min, self.dt_max, self.order = dt_min, dt_max, order
+        self.rejected = 0
+
+    def choose(self, h, enorm, accept_prev=True):
+        """(accept, next h) for an attempt of size h with error norm enorm."""
+        safety = self.safety
+        if enorm > 1.0:
+            if not accept_prev:
+                safety *= self.reject_safety
+            accept = h < (1.0 + 1.4901161193847656e-08) * self.dt_min
+        else:
+            accept = True
+        if not accept:
+            self.rejected += 1
+        hfac = safety * enorm ** (-1.0 / self.order) if enorm > 0.0 else float("inf")
+        hfac = min(max(hfac, self.clip[0]), self.clip[1])
+        return accept, min(max(h * hfac, self.dt_min), self.dt_max)
+
+
+class DmdtStopper:
+    """StopByMaxDmdtFDGPU (llg_module_GPU.py:314-382): every check_every steps, max over nodes
+    of |m - m_prev| / (t - t_prev), in deg/ns; stops below the threshold (<= 0: never)."""
+
+    def __init__(self, hef, stopping_dm_dt_deg_ns, check_every=10, print_every_hit=True):
+        self.hef = hef
+        self.thresh_deg_ns = float(stopping_dm_dt_deg_ns)
+        self.check_every = int(check_every)
+        self.print_every_hit = bool(print_every_hit)
+        self.u_prev = None
+        self.t_prev = None
+        self.last_max_dmdt_deg_ns = float("nan")
+
+    def __call__(self, step, t):
+        if self.thresh_deg_ns <= 0.0:
+            return False
+        if self.check_every > 1 and step % self.check_every != 0:
+            return False
+        u = self.hef.get_state()
+        if self.t_prev is None or t - self.t_prev <= 0.0:
+            self.u_prev, self.t_prev = u, t
+            return False
+        out = _lib.c_dbl()
+        call("spx_vec_node_diff_max", ptr(u), ptr(self.u_prev), self.hef.N, C.byref(out), _lib.stream_ptr())
+        mx = out.value / (t - self.t_prev)
+        self.last_max_dmdt_deg_ns = mx * (180.0 / np.pi) * 1e-9
+        if self.print_every_hit:
+            print(f"[dmdt] step={step} t={t * 1e9:.6f} ns  max|dm/dt|={self.last_max_dmdt_deg_ns:.6e} deg/ns",
+                  flush=True)
+        self.u_prev, self.t_prev = u, t
+        return self.last_max_dmdt_deg_ns < self.thresh_deg_ns

@@ -217,9 +217,13 @@ class EnergyMinimizerGPU:
         raise NotImplementedError("cubic anisotropy is not part of this build")
 
     def add_external_field(self, H0_vec=None, H_time_func=None):
-        if H_time_func is not None:
-            raise NotImplementedError("time-dependent fields are not part of this build")
+        """Static field and, optionally, H_time_func evaluated at the field object's
+        current_time, which the minimiser keeps fixed (llg_module_GPU.py:1185-1194)."""
         self._kw["H0_static"] = H0_vec
+        self._kw["H_time_func"] = H_time_func
+        if self.hef is not None:
+            self.hef.H_time_func = H_time_func
+            self.hef._ht_time = None
         if self.hef is not None and H0_vec is not None:
             self.hef.set_uniform_field(*np.asarray(H0_vec, dtype=np.float64).reshape(3))
 
@@ -245,6 +249,7 @@ class EnergyMinimizerGPU:
         hef = self._build()
         if m0_array is not None:
             hef.set_state(torch.as_tensor(np.asarray(m0_array, dtype=np.float64).ravel(), device="cuda"))
+        hef._sync_time_field()
         t0 = time.perf_counter()
         alg = LaBonteBBMinimizerGPU(hef)
         stats = alg.minimize(max_iter=max_iter, tol=tol, print_every=print_every, verbose=verbose, **kwargs)

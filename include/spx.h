@@ -41,9 +41,23 @@ typedef struct CUstream_st* spx_stream_t; /* same type as cudaStream_t */
 #define SPX_ERR_INTERNAL 6
 #define SPX_ERR_NO_DEVICE 7
 
-#define SPX_PREC_F64 0   /* every vector, factor and tile in FP64                        */
-#define SPX_PREC_F32 1   /* FP32 vectors/solvers, FP32 H-matrix factors and near tiles    */
-#define SPX_PREC_MIXED 2 /* FP32 vectors, BF16 far factors, FP32 near tiles, compensated */
+/* Precision codes.  They mean different things in the two places that take them:
+ *
+ *   code            spx_hmat_config.precision /        spx_demag_options.precision /
+ *                   spx_hmat_repack (packed storage    spx_llg_params.precision (the whole
+ *                   of the H-matrix apply)             demag + LLG pipeline)
+ *   SPX_PREC_F64    FP64 far factors, FP64 near tiles  FP64 vectors, operators, solvers
+ *   SPX_PREC_F32    FP32 far factors, FP32 near tiles  FP32 vectors, operators, CG
+ *   SPX_PREC_MIXED  BF16 far factors, FP32 near tiles  FP64 vectors with FP32 operators: FP32
+ *                   (compensated sums)                 AMG cycle / CG inside FP64 refinement
+ *
+ * An H-matrix apply always accumulates in the type of the vectors it is given (FP64 for
+ * spx_hmat_apply).  With a pipeline precision of SPX_PREC_MIXED the H-matrix packing is
+ * spx_hmat_config.precision (SPX_PREC_F32 by default in the Python layer); BF16 factors
+ * (packing SPX_PREC_MIXED) do not meet a 1e-5 demag tolerance on thin films. */
+#define SPX_PREC_F64 0
+#define SPX_PREC_F32 1
+#define SPX_PREC_MIXED 2
 
 /* ------------------------------------------------------------------ library */
 SPX_API const char* spx_last_error(void);
@@ -56,6 +70,11 @@ SPX_API int spx_device_count(int32_t* n);
  * code the device recorded (SPX_ERR_TIMEOUT) and *timed_out_ctas how many CTAs gave up.  The
  * context stays usable.  Returns SPX_OK when the probe ran. */
 SPX_API int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int32_t* timed_out_ctas);
+/* Out-of-memory injection for tests of the recovery paths (no counterpart in the reference,
+ * whose builder catches CuPy's OutOfMemoryError, lindholm_hmatrix_gpu/builder.py:597-662):
+ * the next `count` device allocations of the library of at least `min_bytes` bytes fail with
+ * SPX_ERR_OOM on the host, before cudaMalloc is called (count 0 switches it off). */
+SPX_API int spx_debug_fail_alloc(int64_t min_bytes, int32_t count);
 
 /* ------------------------------------------------------------------ host geometry
  * Boundary data of build_boundary_data_serial (gpu/fields/Demag_Lindholm.py:177-285):
@@ -125,14 +144,17 @@ SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
  * run: a solver callback whose device memory is owned by another allocator (a PETSc or
  * framework memory pool that must not be bypassed), or a loop that may not stall on
  * cudaMalloc.  No counterpart in the reference.  This entry point allocates nothing: its
- * scratch (x in permuted order plus the far-field z vectors, Nb + sum of ranks elements in
- * the packed precision, 256-byte aligned) lives in one fixed 32 MiB device array that every
- * GPU loading libspx holds until exit; larger H-matrices are rejected with SPX_ERR_INVALID.
- * The first call on a device looks up that array's device address with
- * cudaGetSymbolAddress, so make the first call on each device before any stream capture.
- * All calls share the array and overwrite it completely (nothing in it has to start at
- * zero), so calls that overlap on the GPU (other streams, other threads) race; serialise
- * them.  x, y: FP64 device vectors of length Nb. */
+ * scratch lives in one fixed 32 MiB device array that every GPU loading libspx holds until
+ * exit.  The scratch is FP64 whatever the packing: x in permuted order (Nb), the far-field
+ * z vectors (sum of ranks) and the partial sums of far blocks split between warps (zpart),
+ * (Nb + zlen + zpart_len) x 8 bytes with each part rounded up to 256 bytes, i.e. about 4.19M
+ * elements for every packing; larger H-matrices are rejected with SPX_ERR_INVALID.  The
+ * first call on a device looks up that array's device address with cudaGetSymbolAddress
+ * and keeps it for the life of the process, so make the first call on each device before
+ * any stream capture, and do not reset the device (cudaDeviceReset) afterwards.  All calls
+ * share the array and overwrite it completely (nothing in it has to start at zero), so
+ * calls that overlap on the GPU (other streams, other threads) race; serialise them.
+ * x, y: FP64 device vectors of length Nb. */
 SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_stream_t s);
 /* Y = H X for nrhs vectors at once (no counterpart in the reference, whose fused apply takes one
  * vector): X and Y hold nrhs FP64 device vectors of length Nb one after the other (vector r at
@@ -276,6 +298,35 @@ SPX_API int spx_llg_step(spx_llg l, double dt, int64_t nsteps, spx_stream_t s);
 /* end-to-end call with HOST buffers: copy m_in to the device, run nsteps, copy the
  * result back (pinned host memory gives full PCIe/C2C bandwidth) */
 SPX_API int spx_llg_run_host(spx_llg l, const double* m_in, double* m_out, double dt, int64_t nsteps);
+/* Time-dependent applied field (EffectiveField H_time_func, llg_module_GPU.py:909-956; added
+ * to H_eff at the current time, :998-1000).  The callback lives on the host side; these
+ * calls take its values.
+ *   spx_llg_set_time_field:  the field at the current time, used by spx_llg_heff / _hjac /
+ *                            _rhs / _update_jac_state until changed: h_uniform3 host [3] or
+ *                            NULL (zero) plus h_nodes device [N][3] or NULL; both add up.
+ *   spx_llg_step_time_field: one classic RK4 step of size dt whose stage s (times t, t+dt/2,
+ *                            t+dt/2, t+dt) adds h_uniform4x3[3s..3s+2] (host, or NULL) and
+ *                            h_nodes4 + 3N s (device [4][N][3], or NULL). */
+SPX_API int spx_llg_set_time_field(spx_llg l, const double* h_uniform3, const double* h_nodes, spx_stream_t s);
+SPX_API int spx_llg_step_time_field(spx_llg l, double dt, const double* h_uniform4x3, const double* h_nodes4,
+                                    spx_stream_t s);
+/* Embedded explicit Runge-Kutta attempt (the reference's PETSc TS rk/5dp, llg_module_GPU.py:
+ * 1724-1787; the step-size adaptor is the caller's, as PETSc's TSAdapt is outside the RHS).
+ * scheme 0 = Dormand-Prince 5(4).  From the state, computes the 5th-order candidate of one
+ * step of size dt (not committed) and *err_norm = sqrt(mean_i (e_i / tol_i)^2) over the 3N
+ * entries, e the difference to the embedded 4th-order solution, tol_i = atol + rtol
+ * max(|y5_i|, |y4_i|) (PETSc's weighted 2-norm).  Stage i (time t + c_i dt, c = 0, 1/5,
+ * 3/10, 4/5, 8/9, 1, 1) adds h_uniform7x3[3i..] (host) and h_nodes7 + 3N i (device) when
+ * given.  reuse_fsal != 0 takes stage 1 from the last accepted attempt's stage 7 (first same
+ * as last) when that is still valid.  Reads one scalar back (synchronises the stream).
+ * spx_llg_rk_accept makes the candidate the state. */
+SPX_API int spx_llg_rk_attempt(spx_llg l, int32_t scheme, double dt, double rtol, double atol,
+                               const double* h_uniform7x3, const double* h_nodes7, int32_t reuse_fsal,
+                               double* err_norm, spx_stream_t s);
+SPX_API int spx_llg_rk_accept(spx_llg l, spx_stream_t s);
+/* max over nodes of |a_i - b_i| for FP64 device AoS vectors [N][3] (StopByMaxDmdtFDGPU's
+ * max |du|, llg_module_GPU.py:355-359) */
+SPX_API int spx_vec_node_diff_max(const double* a, const double* b, int64_t N, double* out, spx_stream_t s);
 /* EffectiveField.set_uniform_field (llg_module_GPU.py:897-904): replace the static field by a uniform one */
 SPX_API int spx_llg_set_uniform_field(spx_llg l, double hx, double hy, double hz);
 /* Adjoint and tangent products (no counterpart in the reference, which has no gradients).

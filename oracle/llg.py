@@ -12,6 +12,14 @@ Restates, FP64 numpy, AoS vectors (node-major, 3 components):
                (llg_module_GPU.py:430-431)
 * ``EffectiveFieldOracle``  EffectiveField.compute_H_eff_vec (:972-1006),
                compute_H_jac_vec (:1232-1257), diagK (:674-691)
+* ``EffectiveFieldOracle(H_time=...)`` adds the time-dependent field H_time(t) (the
+  reference's H_time_func, llg_module_GPU.py:909-956, 998-1000) at the evaluation time.
+* ``dp5_attempt`` / ``relax_explicit``: the reference's explicit relaxation
+  (llg_module_GPU.py:1724-1970): PETSc TS rk/5dp (Dormand-Prince 5(4), coefficients of
+  Dormand & Prince 1980) with the TSAdapt "basic" options it sets (clip 0.1-3, safety 0.9,
+  reject safety 0.1, dt in [1e-18, 1e-10], weighted RMS error norm, exponent -1/5), and the
+  dm/dt stopper StopByMaxDmdtFDGPU (:314-382).  PETSc itself is not in this image, so the
+  step sequence is pinned by this restatement, not by PETSc output.
 * ``rk4_step`` the fixed-step scheme used for every trajectory comparison.
   The reference integrates with PETSc TS rk/5dp (adaptive) or BDF; neither
   exposes a fixed step (llg_module_GPU.py:1746-1772), so the oracle and the
@@ -121,7 +129,7 @@ class EffectiveFieldOracle:
     """H_eff = K_lin m + H_ani(m) + H_demag(m) + H0 (+ H(t))."""
 
     def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani=None, D_int=0.0, n_int=None,
-                 H0=None, demag=None, gamma=2.211e5, alpha=0.5, do_precess=1.0, bd=None):
+                 H0=None, demag=None, gamma=2.211e5, alpha=0.5, do_precess=1.0, bd=None, H_time=None):
         import scipy.sparse as sp
         from . import lindholm
         self.X = np.asarray(X, dtype=np.float64)
@@ -148,6 +156,7 @@ class EffectiveFieldOracle:
             self.n_ani = n / np.maximum(np.linalg.norm(n, axis=1), 1e-300)[:, None]
         self.H0 = np.zeros(3 * N) if H0 is None else np.asarray(H0, dtype=np.float64).ravel()
         self.demag = demag
+        self.H_time = H_time
         self.diagK = self.K_lin.diagonal()
         if self.has_ani:
             self.diagK = self.diagK + fem.anisotropy_diag(self.n_ani, self.Ku, self.Ms)
@@ -158,17 +167,23 @@ class EffectiveFieldOracle:
             H = H + fem.anisotropy_field(m, self.n_ani, self.Ku, self.Ms)
         return H
 
-    def h_eff(self, m):
+    def h_time(self, t):
+        if self.H_time is None:
+            return 0.0
+        v = np.asarray(self.H_time(float(t)), dtype=np.float64)
+        return np.tile(v, self.N) if v.size == 3 else v.reshape(-1)
+
+    def h_eff(self, m, t=0.0):
         H = self.linear(m)
         if self.demag is not None:
             H = H + self.demag.compute(m)
-        return H + self.H0
+        return H + self.H0 + self.h_time(t)
 
-    def h_jac(self, m):
-        return self.linear(m) + self.H0
+    def h_jac(self, m, t=0.0):
+        return self.linear(m) + self.H0 + self.h_time(t)
 
-    def llg_rhs(self, m):
-        return rhs(m, self.h_eff(m), self.prefactor, self.alpha, self.do_precess, self.stab)
+    def llg_rhs(self, m, t=0.0):
+        return rhs(m, self.h_eff(m, t), self.prefactor, self.alpha, self.do_precess, self.stab)
 
 
 def rk4_step(f, m, dt):
@@ -177,3 +192,89 @@ def rk4_step(f, m, dt):
     k3 = f(m + 0.5 * dt * k2)
     k4 = f(m + dt * k3)
     return m + (dt / 6.0) * (k1 + 2.0 * k2 + 2.0 * k3 + k4)
+
+
+def rk4_step_t(f, t, m, dt):
+    """Classic RK4 for a time-dependent right-hand side f(m, t)."""
+    k1 = f(m, t)
+    k2 = f(m + 0.5 * dt * k1, t + 0.5 * dt)
+    k3 = f(m + 0.5 * dt * k2, t + 0.5 * dt)
+    k4 = f(m + dt * k3, t + dt)
+    return m + (dt / 6.0) * (k1 + 2.0 * k2 + 2.0 * k3 + k4)
+
+
+DP_C = [0.0, 1 / 5, 3 / 10, 4 / 5, 8 / 9, 1.0, 1.0]
+DP_A = [[],
+        [1 / 5],
+        [3 / 40, 9 / 40],
+        [44 / 45, -56 / 15, 32 / 9],
+        [19372 / 6561, -25360 / 2187, 64448 / 6561, -212 / 729],
+        [9017 / 3168, -355 / 33, 46732 / 5247, 49 / 176, -5103 / 18656],
+        [35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84]]
+DP_B4 = [5179 / 57600, 0.0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40]
+
+
+def dp5_attempt(f, t, m, dt, rtol, atol, k1=None):
+    """One Dormand-Prince 5(4) attempt: (y5, weighted RMS error norm, k7)."""
+    k = [f(m, t) if k1 is None else k1]
+    y = None
+    for i in range(1, 7):
+        y = m + dt * sum(a * kj for a, kj in zip(DP_A[i], k))
+        k.append(f(y, t + DP_C[i] * dt))
+    y5 = y
+    e = dt * sum((b5 - b4) * kj for b5, b4, kj in zip(DP_A[6] + [0.0], DP_B4, k))
+    y4 = y5 - e
+    tol = atol + rtol * np.maximum(np.abs(y5), np.abs(y4))
+    return y5, float(np.sqrt(np.mean((e / tol) ** 2))), k[6]
+
+
+def relax_explicit(f, m0, t0, t_final, dt_init, rtol=1e-6, atol=1e-6, stopping_dmdt=0.0, check_every=5,
+                   max_steps=10 ** 7):
+    """The explicit adaptive relaxation loop: returns (m, stats) with stats t_end, dt_last,
+    nsteps, reason (1 final time reached, 2 dm/dt below the threshold), rejected, dts."""
+    clip, safety0, rsafety, dt_min, dt_max = (0.1, 3.0), 0.9, 0.1, 1e-18, 1e-10
+    t, m, dt = float(t0), np.asarray(m0, dtype=np.float64).copy(), min(max(dt_init, dt_min), dt_max)
+    k1 = None
+    steps, rejected, reason, dts = 0, 0, 0, []
+    u_prev, t_prev, last = None, None, float("nan")
+    nxt = dt
+    while steps < max_steps:
+        if t >= t_final:
+            reason = 1
+            break
+        accept_prev = True
+        while True:
+            y5, en, k7 = dp5_attempt(f, t, m, dt, rtol, atol, k1)
+            safety = safety0
+            if en > 1.0:
+                if not accept_prev:
+                    safety *= rsafety
+                accept = dt < (1.0 + 1.4901161193847656e-08) * dt_min
+            else:
+                accept = True
+            hfac = safety * en ** (-1.0 / 5.0) if en > 0.0 else float("inf")
+            nxt = min(max(dt * min(max(hfac, clip[0]), clip[1]), dt_min), dt_max)
+            if accept:
+                break
+            rejected += 1
+            accept_prev = False
+            k1 = f(m, t) if k1 is None else k1
+            dt = nxt
+        m, t, k1 = y5, t + dt, k7
+        dts.append(dt)
+        steps += 1
+        stop = False
+        if stopping_dmdt > 0.0 and (check_every <= 1 or steps % check_every == 0):
+            if t_prev is None or t - t_prev <= 0.0:
+                u_prev, t_prev = m.copy(), t
+            else:
+                du = (m - u_prev).reshape(-1, 3)
+                last = float(np.sqrt((du * du).sum(axis=1)).max()) / (t - t_prev) * (180.0 / np.pi) * 1e-9
+                u_prev, t_prev = m.copy(), t
+                stop = last < stopping_dmdt
+        dt = nxt
+        if stop:
+            reason = 2
+            break
+    return m, {"t_end": t, "dt_last": dt, "nsteps": steps, "reason": reason, "rejected": rejected, "dts": dts,
+               "maxdmdt_deg_ns": last}

@@ -39,3 +39,28 @@ def test_probe_rejects_bad_arguments():
     status, gave_up = C.c_int32(), C.c_int32()
     assert _lib.lib().spx_debug_barrier_probe(1, 100, C.byref(status), C.byref(gave_up)) == 1
     assert _lib.lib().spx_debug_barrier_probe(4, 0, C.byref(status), C.byref(gave_up)) == 1
+
+
+def test_hmatrix_build_recovers_from_out_of_memory():
+    """An allocation failure during the H-matrix build (injected on the host, no device fault)
+    makes the build retry with half the workspace; the result equals a normal build.  With
+    every large allocation failing, the build raises MemoryError and the context stays usable."""
+    import spinfemx_b200 as spx
+    from spinfemx_b200 import _lib
+    X, T = omesh.kuhn_box(30, 30, 2, 2.5)
+    geom = spx.BoundaryGeometry(X, T)
+    cfg = spx.HMatrixBuildConfig(epsilon=1e-5, eta=2.0, leaf_size=64, batch_bytes=1 << 30)
+    H0 = spx.HMatrixGPUPackedFused(geom, cfg, precision="f64")
+    x = torch.as_tensor(np.random.default_rng(8).standard_normal(H0.size), device="cuda")
+    y0 = H0.matvec(x).clone()
+    try:
+        _lib.call("spx_debug_fail_alloc", 1 << 20, 1)   # the first fill/ACA workspace fails
+        H1 = spx.HMatrixGPUPackedFused(geom, cfg, precision="f64")
+        assert torch.equal(H1.matvec(x), y0)
+        assert H1.stats()["n_far"] == H0.stats()["n_far"]
+        _lib.call("spx_debug_fail_alloc", 1 << 20, 1 << 20)   # every large allocation fails
+        with pytest.raises(MemoryError):
+            spx.HMatrixGPUPackedFused(geom, cfg, precision="f64")
+    finally:
+        _lib.call("spx_debug_fail_alloc", 0, 0)
+    assert torch.equal(H0.matvec(x), y0)

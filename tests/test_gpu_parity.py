@@ -184,6 +184,7 @@ def test_demag_dense_vs_oracle(spx, box20_oracle):
     assert rel(u2.cpu().numpy(), u2r) < 1e-9
     E = d.Energy_lumped_gpu(mt, out)
     assert abs(E / o.energy(m, Href) - 1.0) < 1e-9
+    assert all(d.Energy_lumped_gpu(mt, out) == E for _ in range(3))  # fixed-order reduction
     # the reference's own CG tolerance (rtol 1e-6)
     d6 = spx.DemagFieldLindholmGPU(o.X, o.tets, 8e5, boundary_backend="dense")
     d6.compute_vec(mt, out)

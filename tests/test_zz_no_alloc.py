@@ -27,18 +27,27 @@ def test_hmat_apply_noalloc_matches_apply(precision):
                                   precision=precision)
     stream = _lib.stream_ptr()
     rng = np.random.default_rng(4321)
-    for call_no in range(2):
-        x = torch.as_tensor(rng.standard_normal(H.size), device="cuda")
-        y_ref = torch.empty_like(x)
+    # a fresh handle: the no-allocation calls come first and must not create the apply
+    # buffers that spx_hmat_apply allocates on its first call
+    before = H.memory_report()["accounted_gpu_bytes"]
+    xs = [torch.as_tensor(rng.standard_normal(H.size), device="cuda") for _ in range(2)]
+    outs = []
+    for call_no, x in enumerate(xs):
         y_na = torch.full_like(x, float("nan"))
-        _lib.check(_lib.lib().spx_hmat_apply(H._h, _lib.ptr(x), _lib.ptr(y_ref), stream))
         _lib.check(_lib.lib().spx_hmat_apply_noalloc(H._h, _lib.ptr(x), _lib.ptr(y_na), stream))
         torch.cuda.synchronize()
-        a, b = y_na.cpu().numpy(), y_ref.cpu().numpy()
+        outs.append(y_na.cpu().numpy())
+        assert H.memory_report()["accounted_gpu_bytes"] == before, call_no
+    for call_no, x in enumerate(xs):
+        y_ref = torch.empty_like(x)
+        _lib.check(_lib.lib().spx_hmat_apply(H._h, _lib.ptr(x), _lib.ptr(y_ref), stream))
+        torch.cuda.synchronize()
+        a, b = outs[call_no], y_ref.cpu().numpy()
         assert np.all(np.isfinite(a)), call_no
         assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b), call_no
+    assert H.memory_report()["accounted_gpu_bytes"] > before  # spx_hmat_apply did allocate
     # the Python wrapper reaches the same entry point
-    out = torch.empty_like(x)
-    H.matvec_noalloc(x, out)
+    out = torch.empty_like(xs[1])
+    H.matvec_noalloc(xs[1], out)
     torch.cuda.synchronize()
-    assert np.linalg.norm(out.cpu().numpy() - y_ref.cpu().numpy()) <= 1e-12 * np.linalg.norm(y_ref.cpu().numpy())
+    assert np.linalg.norm(out.cpu().numpy() - outs[1]) <= 1e-12 * np.linalg.norm(outs[1])
