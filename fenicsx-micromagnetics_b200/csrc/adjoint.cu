@@ -511,17 +511,15 @@ void LLGCtx<TV, TM>::adjoint_setup(cudaStream_t s) {
     if (demag) bh = &demag->bd.host;
     else { build_boundary(X_host.data(), N, tets_host.data(), static_cast<int64_t>(tets_host.size() / 4), bhost); bh = &bhost; }
     std::vector<double> b9;
-    assemble_dmi_interfacial(X_host.data(), tets_host.data(), static_cast<int64_t>(tets_host.size() / 4), fem, *bh,
-                             n_int_host.data(), b9);
+    dmi_blocks_scaled(X_host.data(), tets_host.data(), static_cast<int64_t>(tets_host.size() / 4), fem, *bh,
+                      prm.Ms, prm.D_int, n_int_host.empty() ? nullptr : n_int_host.data(), prm.D_bulk, b9);
     std::vector<double> bt(9 * nnz), ks(9 * N, 0.0);
     for (int64_t j = 0; j < N; ++j)
       for (int64_t k = fem.rowptr[j]; k < fem.rowptr[j + 1]; ++k) {
         const int64_t kt = tp[k];
-        const int32_t i = fem.col[k];
-        const double sc = -2.0 * prm.D_int / (mu0 * prm.Ms) / 1e-9 / fem.vol[i];
         for (int r = 0; r < 3; ++r)
           for (int c = 0; c < 3; ++c) {
-            const double v = sc * b9[9 * kt + 3 * r + c];  // block (i, j)[r][c] -> (j, i)[c][r]
+            const double v = b9[9 * kt + 3 * r + c];  // block (i, j)[r][c] -> (j, i)[c][r]
             bt[9 * k + 3 * c + r] = v;
             ks[(3 * c + r) * N + j] += v;
           }

@@ -1073,7 +1073,7 @@ static LLGParams to_params(const spx_llg_params* p) {
   SPX_CHECK(p->Ms > 0.0, "Ms must be positive");
   q.Ms = p->Ms; q.gamma = p->gamma; q.alpha = p->alpha; q.do_precess = p->do_precess;
   q.Aex = p->Aex; q.Ku = p->Ku; q.Ku_nodes = p->Ku_nodes; q.n_ani = p->n_ani;
-  q.D_int = p->D_int; q.n_int = p->n_int; q.H0_nodes = p->H0_nodes;
+  q.D_int = p->D_int; q.n_int = p->n_int; q.H0_nodes = p->H0_nodes; q.D_bulk = p->D_bulk;
   for (int c = 0; c < 3; ++c) q.H0_uniform[c] = p->H0_uniform[c];
   q.use_demag = p->use_demag;
   q.stt_J = p->stt_J; q.stt_P = p->stt_P; q.stt_beta = p->stt_beta; q.stt_dir = p->stt_dir;

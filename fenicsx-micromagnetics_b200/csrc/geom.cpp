@@ -330,6 +330,82 @@ void assemble_dmi_interfacial(const double* X, const int32_t* tets, int64_t E, c
   }
 }
 
+// Bulk DMI operator restating gpu/fields/DMI_Bulk_GPU.py:52-66 (unscaled):
+//   K u . v = - int curl(u) . v dx + 0.5 int_ds (nu x u) . v,
+// as 3x3 blocks [c][d] (row component c of phi_a, column component d of phi_b) on the scalar
+// pattern: volume part - sum_k eps_{c k d} int phi_a d_k phi_b, boundary part
+// 0.5 sum_k eps_{c k d} nu_k int_F phi_a phi_b.
+void assemble_dmi_bulk(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const HostBoundary& bd,
+                       std::vector<double>& B9) {
+  const int64_t nnz = fem.rowptr[fem.N];
+  B9.assign(9 * nnz, 0.0);
+  auto find = [&](int32_t i, int32_t j) -> int64_t {
+    const int32_t* b = fem.col.data() + fem.rowptr[i];
+    const int32_t* e = fem.col.data() + fem.rowptr[i + 1];
+    const int32_t* p = std::lower_bound(b, e, j);
+    if (p == e || *p != j) throw Error(ERR_INTERNAL, "DMI entry outside the P1 pattern");
+    return fem.rowptr[i] + (p - b);
+  };
+  // eps_{c k d} w_k as a 3x3 matrix [c][d] (the cross product e_c . (w x e_d))
+  auto cross_mat = [](const double w[3], double C[3][3]) {
+    C[0][0] = 0.0;   C[0][1] = -w[2]; C[0][2] = w[1];
+    C[1][0] = w[2];  C[1][1] = 0.0;   C[1][2] = -w[0];
+    C[2][0] = -w[1]; C[2][1] = w[0];  C[2][2] = 0.0;
+  };
+  for (int64_t e = 0; e < E; ++e) {
+    const int32_t* t = tets + 4 * e;
+    double g[4][3], vol;
+    tet_grads(X, t, g, &vol);
+    for (int b = 0; b < 4; ++b) {
+      double C[3][3];
+      cross_mat(g[b], C);  // (curl(phi_b e_d))_c = eps_{c k d} d_k phi_b
+      for (int a = 0; a < 4; ++a) {
+        const int64_t k = find(t[a], t[b]);
+        for (int c = 0; c < 3; ++c)
+          for (int d = 0; d < 3; ++d) B9[9 * k + 3 * c + d] -= (vol / 4.0) * C[c][d];
+      }
+    }
+  }
+  for (int64_t f = 0; f < bd.Nt; ++f) {
+    const int32_t* tv = bd.tris.data() + 3 * f;
+    double C[3][3];
+    cross_mat(bd.ntri.data() + 3 * f, C);  // (nu x e_d)_c
+    const double A = bd.area[f];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        const double mab = A / 12.0 * (a == b ? 2.0 : 1.0);  // int_F phi_a phi_b
+        const int64_t k = find(tv[a], tv[b]);
+        for (int c = 0; c < 3; ++c)
+          for (int d = 0; d < 3; ++d) B9[9 * k + 3 * c + d] += 0.5 * mab * C[c][d];
+      }
+  }
+}
+
+void dmi_blocks_scaled(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const HostBoundary& bd,
+                       double Ms, double D_int, const double* n_int, double D_bulk, std::vector<double>& B9) {
+  constexpr double mu0 = 4e-7 * 3.14159265358979323846;
+  const int64_t nnz = fem.rowptr[fem.N];
+  B9.assign(9 * nnz, 0.0);
+  std::vector<double> part;
+  if (D_int != 0.0) {
+    SPX_CHECK(n_int != nullptr, "interfacial DMI needs the interface normal field");
+    assemble_dmi_interfacial(X, tets, E, fem, bd, n_int, part);
+    for (int64_t i = 0; i < fem.N; ++i) {
+      const double sc = -2.0 * D_int / (mu0 * Ms) / 1e-9 / fem.vol[i];
+      for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
+        for (int q = 0; q < 9; ++q) B9[9 * k + q] += sc * part[9 * k + q];
+    }
+  }
+  if (D_bulk != 0.0) {
+    assemble_dmi_bulk(X, tets, E, fem, bd, part);
+    for (int64_t i = 0; i < fem.N; ++i) {
+      const double sc = 2.0 * D_bulk / (mu0 * Ms) * 1e9 / fem.vol[i];
+      for (int64_t k = fem.rowptr[i]; k < fem.rowptr[i + 1]; ++k)
+        for (int q = 0; q < 9; ++q) B9[9 * k + q] += sc * part[9 * k + q];
+    }
+  }
+}
+
 // ------------------------------------------------------------------ SELL-32
 void build_sell(const std::vector<int64_t>& rowptr, const std::vector<int32_t>& col,
                 const std::vector<int32_t>& rows, const std::vector<int32_t>* col_map, HostSell& out) {

@@ -472,23 +472,19 @@ void LLGCtx<TV, TM>::create(DemagCtx<TV, TM>* dm, const double* X, int64_t N_, c
   std::vector<TM> v;
   sell_values<TM>(*hs, kex.data(), 1, true, nnz, 1.0, v);
   Kex.upload(v, s);
-  has_dmi = (p.D_int != 0.0);
+  has_dmi = (p.D_int != 0.0) || (p.D_bulk != 0.0);
   if (has_dmi) {
-    SPX_CHECK(p.n_int != nullptr, "interfacial DMI needs the interface normal field");
+    SPX_CHECK(p.D_int == 0.0 || p.n_int != nullptr, "interfacial DMI needs the interface normal field");
     HostBoundary bhost;
     const HostBoundary* bh = nullptr;
     if (dm) bh = &dm->bd.host;
     else { build_boundary(X, N, tets, E, bhost); bh = &bhost; }
     std::vector<double> b9;
-    assemble_dmi_interfacial(X, tets, E, *fem, *bh, p.n_int, b9);
+    dmi_blocks_scaled(X, tets, E, *fem, *bh, p.Ms, p.D_int, p.n_int, p.D_bulk, b9);
     std::vector<double> ks(9 * N, 0.0);
     for (int64_t i = 0; i < N; ++i) {
-      const double sc = -2.0 * p.D_int / (mu0 * p.Ms) / 1e-9 / fem->vol[i];
       for (int64_t k = fem->rowptr[i]; k < fem->rowptr[i + 1]; ++k) {
-        for (int q = 0; q < 9; ++q) {
-          b9[9 * k + q] *= sc;
-          ks[q * N + i] += b9[9 * k + q];
-        }
+        for (int q = 0; q < 9; ++q) ks[q * N + i] += b9[9 * k + q];
         if (fem->col[k] == i)
           for (int c = 0; c < 3; ++c) diag[3 * i + c] += b9[9 * k + 4 * c];
       }
@@ -501,7 +497,7 @@ void LLGCtx<TV, TM>::create(DemagCtx<TV, TM>* dm, const double* X, int64_t N_, c
   if (has_dmi) {
     X_host.assign(X, X + 3 * N);
     tets_host.assign(tets, tets + 4 * E);
-    n_int_host.assign(p.n_int, p.n_int + 3 * N);
+    if (p.n_int) n_int_host.assign(p.n_int, p.n_int + 3 * N);
   }
   has_ani = false;
   if (p.n_ani && (p.Ku != 0.0 || p.Ku_nodes)) {

@@ -13,6 +13,7 @@ struct LLGParams {
   const double* n_ani = nullptr;     // [3N]
   double D_int = 0.0;
   const double* n_int = nullptr;     // [3N] interface normal
+  double D_bulk = 0.0;               // bulk DMI constant (J/m^2)
   const double* H0_nodes = nullptr;  // [3N] static field (A/m)
   double H0_uniform[3] = {0.0, 0.0, 0.0};
   int use_demag = 1;

@@ -151,6 +151,15 @@ void assemble_dmi_interfacial(const double* X, const int32_t* tets, int64_t E, c
                               const HostBoundary& bd, const double* n_nodes,
                               std::vector<double>& blocks9);
 
+// Bulk-DMI operator restating gpu/fields/DMI_Bulk_GPU.py:52-66 as 3x3 blocks (unscaled).
+void assemble_dmi_bulk(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const HostBoundary& bd,
+                       std::vector<double>& blocks9);
+// Both DMI operators with their row prefactors (interfacial -2 D_int / (mu0 Ms) / 1e-9 / V_i,
+// DMI_Interfacial_GPU.py:160-165; bulk 2 D_bulk / (mu0 Ms) * 1e9 / V_i, DMI_Bulk_GPU.py:63-66),
+// summed; a term with a zero constant is left out.
+void dmi_blocks_scaled(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const HostBoundary& bd,
+                       double Ms, double D_int, const double* n_int, double D_bulk, std::vector<double>& blocks9);
+
 // Zhang-Li operator int (J . grad u) v dx on the node pattern (unscaled), J nodal [3N].
 void assemble_zhang_li(const double* X, const int32_t* tets, int64_t E, const HostFem& fem, const double* J,
                        std::vector<double>& K);

@@ -36,7 +36,7 @@ class LLGParams(C.Structure):
                 ("Ku", c_dbl), ("Ku_nodes", c_vp), ("n_ani", c_vp), ("D_int", c_dbl), ("n_int", c_vp),
                 ("H0_nodes", c_vp), ("H0_uniform", c_dbl * 3), ("use_demag", c_i32), ("precision", c_i32),
                 ("stt_J", c_dbl), ("stt_P", c_dbl), ("stt_beta", c_dbl), ("stt_dir", c_vp),
-                ("sot_Hdl", c_dbl), ("sot_Hfl", c_dbl), ("sot_p", c_vp)]
+                ("sot_Hdl", c_dbl), ("sot_Hfl", c_dbl), ("sot_p", c_vp), ("D_bulk", c_dbl)]
 
 
 # name -> (restype, argtypes)

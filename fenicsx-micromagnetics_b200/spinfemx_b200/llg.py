@@ -46,8 +46,6 @@ class EffectiveField:
                  gamma=2.211e5, alpha=0.5, do_precess=1, use_demag=False, demag_method="lindholm",
                  demag_kwargs=None, H0_static=None, Ku_nodes=None, precision="f64", H_time_func=None,
                  _stt=None, _sot=None):
-        if float(D_bulk) != 0.0:
-            raise NotImplementedError("bulk DMI is not part of this build")
         if str(demag_method).lower() not in {"lindholm", "lindholm_gpu"}:
             raise NotImplementedError("only the Lindholm FEM/BEM demag method is implemented")
         X, tets = as_mesh(X, tets)
@@ -57,7 +55,7 @@ class EffectiveField:
         self.local_size = 3 * self.N
         self.Ms, self.gamma, self.alpha = float(Ms), float(gamma), float(alpha)
         self.do_precess = float(do_precess)
-        self.A, self.Ku, self.D_int = float(Aex), float(Ku), float(D_int)
+        self.A, self.Ku, self.D_int, self.D_bulk = float(Aex), float(Ku), float(D_int), float(D_bulk)
         self.prefactorEQ = -self.gamma / (1.0 + self.alpha ** 2)
         self.Stab = self.Ms * self.gamma / (1.0 + self.alpha ** 2) * 0.5
         self.LLGSteps = 0
@@ -75,7 +73,7 @@ class EffectiveField:
         self._keep = []
         p = _lib.LLGParams()
         p.Ms, p.gamma, p.alpha, p.do_precess = self.Ms, self.gamma, self.alpha, self.do_precess
-        p.Aex, p.Ku, p.D_int = self.A, self.Ku, self.D_int
+        p.Aex, p.Ku, p.D_int, p.D_bulk = self.A, self.Ku, self.D_int, self.D_bulk
         n_ani = _vec3(n_ani_vec, self.N, "n_ani_vec")
         n_int = _vec3(n0_int_vec, self.N, "n0_int_vec")
         H0 = _vec3(H0_static, self.N, "H0_static")
@@ -515,7 +513,7 @@ class LLG_GPU:
         self._kw.update(D_int=float(D_int), n0_int_vec=n0_vec)
 
     def add_dmi_bulk(self, D_bulk):
-        raise NotImplementedError("bulk DMI is not part of this build")
+        self._kw["D_bulk"] = float(D_bulk)
 
     def add_external_field(self, H0_vec=None, H_time_func=None):
         self._kw["H0_static"] = H0_vec

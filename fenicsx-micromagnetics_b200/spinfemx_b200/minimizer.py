@@ -211,7 +211,7 @@ class EnergyMinimizerGPU:
         self._kw.update(D_int=float(D_int), n0_int_vec=n0_vec)
 
     def add_dmi_bulk(self, D_bulk):
-        raise NotImplementedError("bulk DMI is not part of this build")
+        self._kw["D_bulk"] = float(D_bulk)
 
     def add_cubic_anisotropy(self, Kc1, u1_vec, u2_vec):
         raise NotImplementedError("cubic anisotropy is not part of this build")

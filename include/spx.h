@@ -278,6 +278,9 @@ typedef struct {
    * and field-like fields (A/m), nodal polarisation [N][3] (normalised per node; NULL: no SOT) */
   double sot_Hdl, sot_Hfl;
   const double* sot_p;
+  /* bulk DMI (LLG_GPU.add_dmi_bulk, DMIBULK in gpu/fields/DMI_Bulk_GPU.py:43-77): D (J/m^2) of
+   * H = 2D/(mu0 Ms) M_lump^-1 K m, K = -curl + boundary term; 0 = none */
+  double D_bulk;
 } spx_llg_params;
 /* EffectiveField.__init__ (llg_module_GPU.py:388-724); d may be NULL (no demag) */
 SPX_API int spx_llg_create(spx_demag d, const double* X, int64_t N, const int32_t* tets, int64_t E,

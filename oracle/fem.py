@@ -151,6 +151,45 @@ def dmi_interfacial_matrix(X, tets, D, Ms, n_nodes, bd_tris, bd_normals, vol=Non
     return (sp.diags(np.repeat(pref, 3)) @ K).tocsr()
 
 
+def dmi_bulk_matrix(X, tets, D, Ms, bd_tris, bd_normals, vol=None):
+    """Bulk DMI operator, restating DMI_Bulk_GPU.py:52-66: the form
+    -int curl(u) . v dx + 0.5 int_ds (nu x u) . v (nu outward normal), row-scaled by
+    2D/(mu0 Ms) * 1e9 / V_i (mesh in nm)."""
+    tets = np.asarray(tets, dtype=np.int64)
+    N = X.shape[0]
+    if vol is None:
+        vol = lumped_volume(X, tets)
+    tv, g = tet_geometry(X, tets)
+    E = tets.shape[0]
+    eps = np.zeros((3, 3, 3))
+    eps[0, 1, 2] = eps[1, 2, 0] = eps[2, 0, 1] = 1.0
+    eps[0, 2, 1] = eps[2, 1, 0] = eps[1, 0, 2] = -1.0
+    # curl(phi_b e_d)_c = eps_{c k d} d_k phi_b ; int phi_a = vol / 4
+    C = np.einsum("ckd,ebk->ebcd", eps, g)                         # [E, b, c, d]
+    Kl = -(tv / 4.0)[:, None, None, None, None] * np.broadcast_to(C[:, None], (E, 4, 4, 3, 3))
+    Kl = np.transpose(Kl, (0, 1, 3, 2, 4))                           # [E, a, c, b, d]
+    rows = (3 * np.broadcast_to(tets[:, :, None, None, None], (E, 4, 3, 4, 3))
+            + np.arange(3)[None, None, :, None, None])
+    cols = (3 * np.broadcast_to(tets[:, None, None, :, None], (E, 4, 3, 4, 3))
+            + np.arange(3)[None, None, None, None, :])
+    K = sp.csr_matrix((Kl.ravel(), (rows.ravel(), cols.ravel())), shape=(3 * N, 3 * N))
+    tris = np.asarray(bd_tris, dtype=np.int64)
+    nu = np.asarray(bd_normals, dtype=np.float64)
+    P = X[tris]
+    area = 0.5 * np.linalg.norm(np.cross(P[:, 1] - P[:, 0], P[:, 2] - P[:, 0]), axis=1)
+    F = tris.shape[0]
+    Cn = np.einsum("ckd,fk->fcd", eps, nu)                           # (nu x e_d)_c
+    mab = (np.ones((3, 3)) + np.eye(3)) / 12.0                       # int_F phi_a phi_b / area
+    Bl = 0.5 * area[:, None, None, None, None] * mab[None, :, None, :, None] * Cn[:, None, :, None, :]
+    rows = (3 * np.broadcast_to(tris[:, :, None, None, None], (F, 3, 3, 3, 3))
+            + np.arange(3)[None, None, :, None, None])
+    cols = (3 * np.broadcast_to(tris[:, None, None, :, None], (F, 3, 3, 3, 3))
+            + np.arange(3)[None, None, None, None, :])
+    K = K + sp.csr_matrix((Bl.ravel(), (rows.ravel(), cols.ravel())), shape=(3 * N, 3 * N))
+    pref = 2.0 * D / (MU0 * Ms) * 1e9 / vol
+    return (sp.diags(np.repeat(pref, 3)) @ K).tocsr()
+
+
 def anisotropy_field(m, n_axis, Ku, Ms):
     """Nodal uniaxial field H = 2Ku/(mu0 Ms) (m.n) n (Anisotropy_GPU.py:317-330).
 

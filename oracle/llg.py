@@ -129,7 +129,8 @@ class EffectiveFieldOracle:
     """H_eff = K_lin m + H_ani(m) + H_demag(m) + H0 (+ H(t))."""
 
     def __init__(self, X, tets, Ms, Aex=0.0, Ku=0.0, n_ani=None, D_int=0.0, n_int=None,
-                 H0=None, demag=None, gamma=2.211e5, alpha=0.5, do_precess=1.0, bd=None, H_time=None):
+                 H0=None, demag=None, gamma=2.211e5, alpha=0.5, do_precess=1.0, bd=None, H_time=None,
+                 D_bulk=0.0):
         import scipy.sparse as sp
         from . import lindholm
         self.X = np.asarray(X, dtype=np.float64)
@@ -148,6 +149,9 @@ class EffectiveFieldOracle:
             nvec = np.asarray(n_int, dtype=np.float64).reshape(N, 3)
             K = K + fem.dmi_interfacial_matrix(self.X, self.tets, D_int, self.Ms, nvec,
                                                bd["tris"], bd["ntri"], self.vol)
+        if D_bulk != 0.0:
+            bd = lindholm.boundary_data(self.X, self.tets) if bd is None else bd
+            K = K + fem.dmi_bulk_matrix(self.X, self.tets, D_bulk, self.Ms, bd["tris"], bd["ntri"], self.vol)
         self.K_lin = K.tocsr()
         self.Ku = Ku
         self.has_ani = np.any(np.asarray(Ku) != 0.0)
