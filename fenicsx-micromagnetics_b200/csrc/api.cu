@@ -37,6 +37,12 @@ using namespace spx;
 
 static cudaStream_t S(spx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// H-matrix packing precision (SPX_PREC_F32_F16 included)
+static Prec to_hprec(int32_t p) {
+  SPX_CHECK(p >= 0 && p <= 3, "H-matrix precision must be SPX_PREC_F64, _F32, _MIXED or _F32_F16");
+  return static_cast<Prec>(p);
+}
+
 static Prec to_prec(int32_t p) {
   SPX_CHECK(p >= 0 && p <= 2, "precision must be SPX_PREC_F64, SPX_PREC_F32 or SPX_PREC_MIXED");
   return static_cast<Prec>(p);
@@ -62,6 +68,8 @@ static HBuildConfig to_hcfg(const spx_hmat_config* c) {
   h.max_rank = c->max_rank > 0 ? c->max_rank : -1;
   h.max_temporary_block_bytes = c->max_temporary_block_bytes;
   if (c->batch_bytes > 0) h.batch_bytes = c->batch_bytes;
+  SPX_CHECK((c->flags & ~SPX_HMAT_RECOMPRESS) == 0, "unknown spx_hmat_config.flags bits");
+  h.recompress = (c->flags & SPX_HMAT_RECOMPRESS) != 0;
   return h;
 }
 
@@ -628,7 +636,7 @@ int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out) {
   *out = nullptr;
   auto h = std::make_unique<spx_hmat_s>();
   h->own.build(b->bd, to_hcfg(cfg), 0);
-  h->own.pack(to_prec(cfg ? cfg->precision : 0), 0);
+  h->own.pack(to_hprec(cfg ? cfg->precision : 0), 0);
   *out = h.release();
   API_END
 }
@@ -682,7 +690,7 @@ int spx_hmat_import(spx_boundary b, const spx_hmat_config* cfg, const int32_t* p
   SPX_CHECK(near_indptr[0] == 0 && (near_indptr[b->bd.host.Nb] == 0 || (near_indices && near_data)),
             "near CSR needs indices and data");
   auto h = std::make_unique<spx_hmat_s>();
-  hmat_import(h->own, b->bd, to_hcfg(cfg), to_prec(cfg ? cfg->precision : 0), nfar, far_meta5, relres, U, V,
+  hmat_import(h->own, b->bd, to_hcfg(cfg), to_hprec(cfg ? cfg->precision : 0), nfar, far_meta5, relres, U, V,
               near_indptr, near_indices, near_data, perm, diag_jump, 0);
   *out = h.release();
   API_END
@@ -775,7 +783,7 @@ int spx_hmat_apply_noalloc(spx_hmat hm, const double* x, double* y, spx_stream_t
 int spx_hmat_repack(spx_hmat hm, int32_t precision) {
   API_BEGIN
   REQUIRE(hm);
-  hm->h().pack(to_prec(precision), 0);
+  hm->h().pack(to_hprec(precision), 0);
   API_END
 }
 
@@ -807,6 +815,23 @@ int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int
   int t = 0;
   *status = spx::barrier_timeout_probe(nblocks, static_cast<long long>(limit), &t);
   *timed_out_ctas = t;
+  API_END
+}
+
+int spx_hmat_recompress(spx_hmat hm, int64_t* out3, double* max_rel_err) {
+  API_BEGIN
+  REQUIRE(hm);
+  HMatrix& H = hm->h();
+  SPX_CHECK(H.far_pool64.n > 0 || H.stats.n_far == 0, "this H-matrix has no FP64 factors (merged)");
+  const Prec p = H.prec;
+  const RecompressStats st = H.recompress(0);
+  H.pack(p, 0);
+  if (out3) {
+    out3[0] = st.entries_before;
+    out3[1] = st.entries_after;
+    out3[2] = st.rewritten;
+  }
+  if (max_rel_err) *max_rel_err = st.truncation_error_max;
   API_END
 }
 
@@ -846,7 +871,7 @@ static int demag_create(const double* X, int64_t N, const int32_t* tets, int64_t
     SPX_CHECK(opt->warm_start >= 0 && opt->warm_start <= 3, "warm_start must be 0, 1, 2 or 3");
     o.backend = opt->backend;
     o.prec = to_prec(opt->precision);
-    o.hprec = to_prec(opt->hmat.precision);
+    o.hprec = to_hprec(opt->hmat.precision);
     if (opt->rtol_u1 > 0) o.rtol_u1 = opt->rtol_u1;
     if (opt->rtol_u2 > 0) o.rtol_u2 = opt->rtol_u2;
     if (opt->atol >= 0) o.atol = opt->atol;

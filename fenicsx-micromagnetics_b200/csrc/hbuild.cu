@@ -556,8 +556,11 @@ void HMatrix::build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s
     else stats.near_entries += (int64_t)(b.re - b.rs) * (b.ce - b.cs);
   }
   SPX_CUDA(cudaStreamSynchronize(s));
-  stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   packed = false;
+  recompressed = false;
+  sigma.clear();
+  if (c.recompress) recompress(s);
+  stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
 }
 
 }  // namespace spx

@@ -196,6 +196,9 @@ void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec 
   H.stats.n_far = H.stats.low_rank_blocks;
   H.stats.n_near = H.stats.dense_blocks;
   SPX_CUDA(cudaStreamSynchronize(s));
+  H.recompressed = false;
+  H.sigma.clear();
+  if (c.recompress) H.recompress(s);
   H.pack(p, s);
 }
 
@@ -229,6 +232,7 @@ void hmat_merge(const std::vector<const HMatrix*>& parts, HMatrix& M, cudaStream
   std::vector<int64_t> foff, noff;
   for (const HMatrix* H : parts) {
     SPX_CHECK(H->packed && H->prec == p, "merged H-matrices must be packed in the same precision");
+    SPX_CHECK(p != Prec::SPLIT, "the f32/f16 split packing is not available for merged (ensemble) H-matrices");
     foff.push_back(fbytes);
     noff.push_back(nbytes);
     fbytes += ((static_cast<int64_t>(H->far_f.n) + 255) / 256) * 256;
@@ -353,7 +357,9 @@ HMatrix& HMatrix::transposed(cudaStream_t s) {
   }
   T->near_pool64.upload(neart, s);
   SPX_CUDA(cudaStreamSynchronize(s));
-  T->pack(prec, s);
+  // the split packing scales the columns of U by their singular values, which the transpose
+  // moves to V: the transpose of a split-packed matrix is packed in FP32
+  T->pack(prec == Prec::SPLIT ? Prec::F32 : prec, s);
   tr = std::move(T);
   return *tr;
 }

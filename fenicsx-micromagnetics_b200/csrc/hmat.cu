@@ -34,6 +34,8 @@
 #include <mutex>
 #include <string>
 
+#include <cuda_fp16.h>
+
 #include "hmat.cuh"
 
 namespace spx {
@@ -62,20 +64,27 @@ constexpr int ROWS_WARPS = 8;   // warps per k_rows CTA
 inline int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
 }  // namespace
 
-// dst[q * ld + r] = pool[src + q * sq + r * sr] for r < nr, 0 for nr <= r < ld, q < nq
+// dst[q * ld + r] = pool[src + q * sq + r * sr] * (scaled by qscale[qs + q] when qs >= 0, or
+// by rscale[qs + r] when rs != 0) for r < nr, 0 for nr <= r < ld, q < nq
 struct PackJob {
   int64_t src, dst;
   int32_t nq, nr, ld, sq, sr;
+  int64_t qs = -1;  // first scale factor of this job (-1: none)
+  int32_t rs = 0;   // 1: the scale runs along r instead of q
 };
+template <class T> __device__ __forceinline__ T from_d_s(double v) { return from_d<T>(v); }
+template <> __device__ __forceinline__ __half from_d_s<__half>(double v) { return __double2half(v); }
 template <class T>
 __global__ void k_pack(const PackJob* __restrict__ jobs, int64_t njobs, const double* __restrict__ pool,
-                       T* __restrict__ out) {
+                       const double* __restrict__ scale, T* __restrict__ out) {
   for (int64_t jb = blockIdx.x; jb < njobs; jb += gridDim.x) {
     const PackJob j = jobs[jb];
     const int64_t L = static_cast<int64_t>(j.nq) * j.ld;
     for (int64_t e = threadIdx.x; e < L; e += blockDim.x) {
       const int64_t q = e / j.ld, r = e - q * j.ld;
-      out[j.dst + e] = r < j.nr ? from_d<T>(pool[j.src + q * j.sq + r * j.sr]) : from_d<T>(0.0);
+      double v = r < j.nr ? pool[j.src + q * j.sq + r * j.sr] : 0.0;
+      if (j.qs >= 0 && r < j.nr) v *= scale[j.qs + (j.rs ? r : q)];
+      out[j.dst + e] = from_d_s<T>(v);
     }
   }
 }
@@ -96,6 +105,7 @@ template <class TF> struct V16;
 template <> struct V16<double> { using T = double2; static constexpr int E = 2; };
 template <> struct V16<float> { using T = float4; static constexpr int E = 4; };
 template <> struct V16<__nv_bfloat16> { using T = uint4; static constexpr int E = 8; };
+template <> struct V16<__half> { using T = uint4; static constexpr int E = 8; };
 
 template <class TA, class TF>
 __device__ __forceinline__ void v16_elems(const typename V16<TF>::T& v, TA out[V16<TF>::E]);
@@ -122,6 +132,20 @@ __device__ __forceinline__ void bf16x8(const uint4& v, TA out[8]) {
     out[2 * q + 1] = static_cast<TA>(__uint_as_float(w[q] & 0xffff0000u));
   }
 }
+template <class TA>
+__device__ __forceinline__ void h16x8(const uint4& v, TA out[8]) {
+  const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[q]));
+    out[2 * q] = static_cast<TA>(f.x);
+    out[2 * q + 1] = static_cast<TA>(f.y);
+  }
+}
+template <>
+__device__ __forceinline__ void v16_elems<double, __half>(const uint4& v, double out[8]) { h16x8<double>(v, out); }
+template <>
+__device__ __forceinline__ void v16_elems<float, __half>(const uint4& v, float out[8]) { h16x8<float>(v, out); }
 template <>
 __device__ __forceinline__ void v16_elems<double, __nv_bfloat16>(const uint4& v, double out[8]) { bf16x8<double>(v, out); }
 template <>
@@ -253,7 +277,8 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
 template <class T, class TA, class TV>
 __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, int64_t first, int64_t end,
                                            const T* __restrict__ base, const TV* __restrict__ vs, int nr,
-                                           TA* __restrict__ part, int lane, bool kahan) {
+                                           TA* __restrict__ part, int lane, bool kahan,
+                                           const double* __restrict__ vscale = nullptr) {
   constexpr int E = V16<T>::E;
   using VT = typename V16<T>::T;
   const int nvec = (nr + E - 1) / E;
@@ -285,6 +310,7 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
     if (!active) continue;
     const VT* tile = reinterpret_cast<const VT*>(base + I.off) + vl;
     const TV* v = vs + I.src;
+    const double* sc = vscale ? vscale + I.src : nullptr;
     int q = ph;
     for (; q + 3 * P < I.len; q += 4 * P) {
       VT w[4];
@@ -293,6 +319,7 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
       for (int u = 0; u < 4; ++u) {
         w[u] = tile[static_cast<int64_t>(q + u * P) * nvec];
         a[u] = static_cast<TA>(v[q + u * P]);
+        if (sc) a[u] *= static_cast<TA>(sc[q + u * P]);
       }
       if (kahan) {
 #pragma unroll
@@ -325,7 +352,7 @@ __device__ __forceinline__ void rows_items(const RowItem* __restrict__ items, in
     }
     for (; q < I.len; q += P) {
       const VT w = tile[static_cast<int64_t>(q) * nvec];
-      const TA a = static_cast<TA>(v[q]);
+      const TA a = static_cast<TA>(v[q]) * (sc ? static_cast<TA>(sc[q]) : TA(1));
       TA e[E];
       v16_elems<TA, T>(w, e);
       if (kahan) {
@@ -364,7 +391,8 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const int64_t* __restrict__ near_begin, const RowItem* __restrict__ items, const TF* __restrict__ F,
     const TN* __restrict__ Nt, const TA* __restrict__ z, const TX* __restrict__ xp,
     const double* __restrict__ diag, const int32_t* __restrict__ perm, const int32_t* __restrict__ gidx,
-    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, int kahan) {
+    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, int kahan,
+    const int64_t* __restrict__ half_begin, const __half* __restrict__ Fh, const double* __restrict__ zscale) {
   __shared__ TA part[ROWS_WARPS][SEG_MAX];
   const int sgm = blockIdx.x;
   const int r0 = seg_start[sgm], nr = seg_start[sgm + 1] - r0;
@@ -372,7 +400,9 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
   for (int r = lane; r < SEG_MAX; r += 32) part[warp][r] = TA(0);
   __syncwarp();
   const int64_t i0 = item_ptr[sgm], im = near_begin[sgm], i1 = item_ptr[sgm + 1];
-  rows_items<TF, TA, TA>(items, i0 + warp, im, F, z, nr, part[warp], lane, false);
+  const int64_t ih = half_begin ? half_begin[sgm] : im;
+  rows_items<TF, TA, TA>(items, i0 + warp, ih, F, z, nr, part[warp], lane, false);
+  if (ih < im) rows_items<__half, TA, TA>(items, ih + warp, im, Fh, z, nr, part[warp], lane, false, zscale);
   rows_items<TN, TA, TX>(items, im + warp, i1, Nt, xp, nr, part[warp], lane, kahan != 0);
   __syncthreads();
   for (int r = threadIdx.x; r < nr; r += blockDim.x) {
@@ -391,8 +421,9 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
 // ------------------------------------------------------------------ host side
 namespace {
 
-void run_pack_jobs_f(const std::vector<PackJob>& jobs, const double* pool, char* out, Prec p, bool near,
-                     cudaStream_t s) {
+template <class T>
+void run_pack_jobs(const std::vector<PackJob>& jobs, const double* pool, const double* scale, char* out,
+                   cudaStream_t s) {
   if (jobs.empty()) return;
   constexpr size_t CH = size_t(1) << 20;
   for (size_t k0 = 0; k0 < jobs.size(); k0 += CH) {
@@ -400,22 +431,90 @@ void run_pack_jobs_f(const std::vector<PackJob>& jobs, const double* pool, char*
     DevBuf<PackJob> d;
     d.upload(jobs.data() + k0, c, s);
     const unsigned grid = static_cast<unsigned>(std::min<size_t>(c, 65535));
-    if (p == Prec::F64)
-      k_pack<double><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool, reinterpret_cast<double*>(out));
-    else if (p == Prec::F32 || near)
-      k_pack<float><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool, reinterpret_cast<float*>(out));
-    else
-      k_pack<__nv_bfloat16><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool,
-                                                 reinterpret_cast<__nv_bfloat16*>(out));
+    k_pack<T><<<grid, 128, 0, s>>>(d.p, static_cast<int64_t>(c), pool, scale, reinterpret_cast<T*>(out));
     SPX_LAUNCH_CHECK();
     SPX_CUDA(cudaStreamSynchronize(s));
   }
 }
 
+// far_z units dealt to warps in contiguous ranges of about equal cost; the last unit of a
+// block in each warp writes the block (flags 1), or contributes partials to a group (flags 2)
+// whose slots start at *ppos.  Returns the warp ranges.
+std::vector<int32_t> plan_units(std::vector<FarUnit>& units, size_t elem_bytes, int nsm, int64_t& nw_out,
+                                std::vector<FarGroup>& groups, int64_t& ppos) {
+  const int64_t nw = std::max<int64_t>(1, std::min<int64_t>(static_cast<int64_t>(nsm) * Z_CTAS_PER_SM * Z_WARPS,
+                                                            static_cast<int64_t>(units.size())));
+  std::vector<double> cost(units.size() + 1, 0.0);
+  for (size_t u = 0; u < units.size(); ++u) {
+    const FarUnit& U = units[u];
+    cost[u + 1] = cost[u] + static_cast<double>(U.nc) * U.ldk * elem_bytes + 8.0 * U.nc + 512.0;
+  }
+  std::vector<int32_t> wf(nw + 1, 0);
+  {
+    size_t u = 0;
+    for (int64_t w = 0; w <= nw; ++w) {
+      const double target = cost.back() * static_cast<double>(w) / static_cast<double>(nw);
+      while (u < units.size() && cost[u] < target) ++u;
+      wf[w] = static_cast<int32_t>(u);
+    }
+    wf[nw] = static_cast<int32_t>(units.size());
+  }
+  std::vector<int32_t> warp_of(units.size());
+  for (int64_t w = 0; w < nw; ++w)
+    for (int32_t u = wf[w]; u < wf[w + 1]; ++u) warp_of[u] = static_cast<int32_t>(w);
+  size_t u = 0;
+  while (u < units.size()) {
+    size_t e = u;
+    while (e < units.size() && units[e].zout == units[u].zout) ++e;  // block = units [u, e)
+    std::vector<size_t> lasts;
+    for (size_t v = u; v < e; ++v)
+      if (v + 1 == e || warp_of[v + 1] != warp_of[v]) lasts.push_back(v);
+    if (lasts.size() == 1) {
+      units[lasts[0]].flags = 1;
+    } else {
+      const int32_t g = static_cast<int32_t>(groups.size());
+      groups.push_back(FarGroup{static_cast<int32_t>(ppos), static_cast<int32_t>(lasts.size()), units[u].zout,
+                                units[u].k});
+      for (size_t c = 0; c < lasts.size(); ++c) {
+        FarUnit& L = units[lasts[c]];
+        L.flags = 2;
+        L.grp = g;
+        L.zout = static_cast<int32_t>(ppos + static_cast<int64_t>(c) * L.ldk);
+      }
+      ppos += static_cast<int64_t>(lasts.size()) * units[u].ldk;
+    }
+    u = e;
+  }
+  nw_out = units.empty() ? 0 : nw;
+  return wf;
+}
+
+// FP32 columns kept by a recompressed block under the split packing: the trailing columns go
+// to FP16 when their rounding (relative 2^-11 in U and in V) stays within a tenth of the
+// block's error budget, sqrt(sum_{j>=c} 2 (sigma_j 2^-11)^2) <= 0.1 eps ||A||; rounded up to
+// a multiple of 4 (the FP32 vector width); k (all FP32) without singular values.
+int split_head(const std::vector<double>& sig, int k, double eps) {
+  if (static_cast<int>(sig.size()) != k || k == 0) return k;
+  double n2 = 0.0;
+  for (double v : sig) n2 += v * v;
+  const double bud = 0.1 * eps * std::sqrt(n2);
+  const double u16 = std::ldexp(1.0, -11);
+  double acc = 0.0;
+  int c = k;
+  for (int j = k - 1; j >= 0; --j) {
+    acc += 2.0 * (sig[j] * u16) * (sig[j] * u16);
+    if (std::sqrt(acc) > bud) break;
+    c = j;
+  }
+  const int c4 = static_cast<int>(round_up(c, 4));
+  return c4 >= k ? k : c4;
+}
+
 template <class TF, class TN>
-void do_pack(HMatrix& H, cudaStream_t s) {
+void do_pack(HMatrix& H, cudaStream_t s, bool split = false) {
   constexpr int EF = 16 / static_cast<int>(sizeof(TF));
   constexpr int EN = 16 / static_cast<int>(sizeof(TN));
+  constexpr int EH = 8;  // FP16 elements per 16 bytes
   // row segments: leaf clusters in permutation order, cut into pieces of <= SEG_MAX rows
   std::vector<int32_t> ls;
   for (const TreeNode& nd : H.tree.nodes)
@@ -431,33 +530,66 @@ void do_pack(HMatrix& H, cudaStream_t s) {
   seg.push_back(static_cast<int32_t>(H.Nb));
   const int64_t nseg = static_cast<int64_t>(seg.size()) - 1;
 
-  std::vector<PackJob> jf, jn;
-  std::vector<FarUnit> units;
-  std::vector<std::vector<RowItem>> far_items(nseg), near_items(nseg);
-  int64_t fpos = 0, npos = 0, zpos = 0, nf = 0, nn = 0;
-  for (const HBlock& b : H.blocks) {
+  std::vector<PackJob> jf, jn, jh;
+  std::vector<FarUnit> units, units_h;
+  std::vector<std::vector<RowItem>> far_items(nseg), half_items(nseg), near_items(nseg);
+  std::vector<double> scale;  // 1 / sigma of the FP16 columns of U (pack), sigma per z entry (apply)
+  std::vector<double> zsc;
+  int64_t fpos = 0, hpos = 0, npos = 0, zpos = 0, nf = 0, nn = 0;
+  for (size_t bi = 0; bi < H.blocks.size(); ++bi) {
+    const HBlock& b = H.blocks[bi];
     const int32_t m = b.re - b.rs, n = b.ce - b.cs;
     int64_t sg = std::upper_bound(seg.begin(), seg.end(), b.rs) - seg.begin() - 1;
     SPX_CHECK(sg >= 0 && seg[sg] == b.rs, "block rows do not start at a segment boundary");
     if (b.type == 1) {
       const int32_t k = b.rank;
-      const int32_t ldk = static_cast<int32_t>(round_up(std::max(k, 1), EF));
+      const int32_t kh = split ? split_head(H.sigma.empty() ? std::vector<double>() : H.sigma[bi], k,
+                                            H.cfg.epsilon) : k;  // FP32 columns
+      const int32_t kt = k - kh;                                 // FP16 columns
+      const int32_t ldk = static_cast<int32_t>(round_up(std::max(kh, 1), EF));
       const int64_t pv = fpos;
-      // V^T: n rows of ldk (row c = V[0..k-1, c]); units of at most ~16 KB of rows
-      jf.push_back(PackJob{b.off_v, pv, n, k, ldk, 1, n});
+      // V^T head: n rows of ldk (row c = V[0..kh-1, c]); units of at most ~16 KB of rows
+      jf.push_back(PackJob{b.off_v, pv, n, kh, ldk, 1, n});
       fpos = pv + static_cast<int64_t>(n) * ldk;
-      if (k > 0) {
+      if (kh > 0) {
         const int32_t uc = std::max<int32_t>(8, static_cast<int32_t>(16384 / (static_cast<int64_t>(ldk) * sizeof(TF))));
         for (int32_t c0 = 0; c0 < n; c0 += uc)
-          units.push_back(FarUnit{pv + static_cast<int64_t>(c0) * ldk, ldk, std::min(uc, n - c0), b.cs + c0, k,
+          units.push_back(FarUnit{pv + static_cast<int64_t>(c0) * ldk, ldk, std::min(uc, n - c0), b.cs + c0, kh,
                                   static_cast<int32_t>(zpos), -1, 0, 0});
       }
-      for (; sg < nseg && seg[sg] < b.re; ++sg) {
-        const int32_t a = seg[sg], nr = seg[sg + 1] - seg[sg];
+      int64_t sgu = sg;
+      for (; sgu < nseg && seg[sgu] < b.re; ++sgu) {
+        const int32_t a = seg[sgu], nr = seg[sgu + 1] - seg[sgu];
         const int32_t ld = static_cast<int32_t>(round_up(nr, EF));
-        jf.push_back(PackJob{b.off_u + (a - b.rs), fpos, k, nr, ld, m, 1});
-        far_items[sg].push_back(RowItem{fpos, k, static_cast<int32_t>(zpos)});
-        fpos = round_up(fpos + (int64_t)k * ld, EF);
+        jf.push_back(PackJob{b.off_u + (a - b.rs), fpos, kh, nr, ld, m, 1});
+        far_items[sgu].push_back(RowItem{fpos, kh, static_cast<int32_t>(zpos)});
+        fpos = round_up(fpos + (int64_t)kh * ld, EF);
+      }
+      for (int32_t q = 0; q < kh; ++q) zsc.push_back(1.0);
+      if (kt > 0) {
+        // tail: unit columns of U (scaled by 1 / sigma) and unit rows of V in FP16; z of the
+        // tail is scaled back by sigma in the row kernel
+        const std::vector<double>& sig = H.sigma[bi];
+        const int64_t s0 = static_cast<int64_t>(scale.size());
+        for (int32_t q = 0; q < kt; ++q) scale.push_back(1.0 / sig[kh + q]);
+        const int32_t ldh = static_cast<int32_t>(round_up(kt, EH));
+        const int64_t ph = hpos;
+        jh.push_back(PackJob{b.off_v + static_cast<int64_t>(kh) * n, ph, n, kt, ldh, 1, n});
+        hpos = ph + static_cast<int64_t>(n) * ldh;
+        const int32_t uc = std::max<int32_t>(8, static_cast<int32_t>(16384 / (static_cast<int64_t>(ldh) * 2)));
+        for (int32_t c0 = 0; c0 < n; c0 += uc)
+          units_h.push_back(FarUnit{ph + static_cast<int64_t>(c0) * ldh, ldh, std::min(uc, n - c0), b.cs + c0, kt,
+                                    static_cast<int32_t>(zpos + kh), -1, 0, 0});
+        for (sgu = sg; sgu < nseg && seg[sgu] < b.re; ++sgu) {
+          const int32_t a = seg[sgu], nr = seg[sgu + 1] - seg[sgu];
+          const int32_t ld = static_cast<int32_t>(round_up(nr, EH));
+          PackJob J{b.off_u + static_cast<int64_t>(kh) * m + (a - b.rs), hpos, kt, nr, ld, m, 1};
+          J.qs = s0;
+          jh.push_back(J);
+          half_items[sgu].push_back(RowItem{hpos, kt, static_cast<int32_t>(zpos + kh)});
+          hpos = round_up(hpos + (int64_t)kt * ld, EH);
+        }
+        for (int32_t q = 0; q < kt; ++q) zsc.push_back(sig[kh + q]);
       }
       zpos += k;
       ++nf;
@@ -478,83 +610,59 @@ void do_pack(HMatrix& H, cudaStream_t s) {
   H.zlen = zpos;
   H.far_f.alloc(std::max<int64_t>(fpos, 1) * sizeof(TF));
   H.near_f.alloc(std::max<int64_t>(npos, 1) * sizeof(TN));
-  H.bytes_far = fpos * (int64_t)sizeof(TF);
+  H.far_h.alloc(hpos > 0 ? hpos * 2 : 0);
+  H.bytes_far = fpos * (int64_t)sizeof(TF) + hpos * 2;
   H.bytes_near = npos * (int64_t)sizeof(TN);
-  run_pack_jobs_f(jf, H.far_pool64.p, H.far_f.p, H.prec, false, s);
-  run_pack_jobs_f(jn, H.near_pool64.p, H.near_f.p, H.prec, true, s);
+  const bool bf = (H.prec == Prec::MIXED);
+  if (sizeof(TF) == 8) run_pack_jobs<double>(jf, H.far_pool64.p, nullptr, H.far_f.p, s);
+  else if (bf) run_pack_jobs<__nv_bfloat16>(jf, H.far_pool64.p, nullptr, H.far_f.p, s);
+  else run_pack_jobs<float>(jf, H.far_pool64.p, nullptr, H.far_f.p, s);
+  if (sizeof(TN) == 8) run_pack_jobs<double>(jn, H.near_pool64.p, nullptr, H.near_f.p, s);
+  else run_pack_jobs<float>(jn, H.near_pool64.p, nullptr, H.near_f.p, s);
+  if (!jh.empty()) {
+    DevBuf<double> dsc;
+    dsc.upload(scale, s);
+    run_pack_jobs<__half>(jh, H.far_pool64.p, dsc.p, H.far_h.p, s);
+  }
 
-  // far_z units dealt to warps in contiguous ranges of about equal cost
   const int nsm = num_sms(H.device);
-  const int64_t nw = std::max<int64_t>(1, std::min<int64_t>(static_cast<int64_t>(nsm) * Z_CTAS_PER_SM * Z_WARPS,
-                                                            static_cast<int64_t>(units.size())));
-  std::vector<double> cost(units.size() + 1, 0.0);
-  for (size_t u = 0; u < units.size(); ++u) {
-    const FarUnit& U = units[u];
-    cost[u + 1] = cost[u] + static_cast<double>(U.nc) * U.ldk * sizeof(TF) + 8.0 * U.nc + 512.0;
-  }
-  std::vector<int32_t> wf(nw + 1, 0);
-  {
-    size_t u = 0;
-    for (int64_t w = 0; w <= nw; ++w) {
-      const double target = cost.back() * static_cast<double>(w) / static_cast<double>(nw);
-      while (u < units.size() && cost[u] < target) ++u;
-      wf[w] = static_cast<int32_t>(u);
-    }
-    wf[nw] = static_cast<int32_t>(units.size());
-  }
-  // the last unit of a block in each warp writes the block: directly when one warp holds
-  // the whole block, else as contributor c of a group
   std::vector<FarGroup> groups;
-  int64_t ppos = 0;
-  {
-    std::vector<int32_t> warp_of(units.size());
-    for (int64_t w = 0; w < nw; ++w)
-      for (int32_t u = wf[w]; u < wf[w + 1]; ++u) warp_of[u] = static_cast<int32_t>(w);
-    size_t u = 0;
-    while (u < units.size()) {
-      size_t e = u;
-      while (e < units.size() && units[e].zout == units[u].zout) ++e;  // block = units [u, e)
-      std::vector<size_t> lasts;
-      for (size_t v = u; v < e; ++v)
-        if (v + 1 == e || warp_of[v + 1] != warp_of[v]) lasts.push_back(v);
-      if (lasts.size() == 1) {
-        units[lasts[0]].flags = 1;
-      } else {
-        const int32_t g = static_cast<int32_t>(groups.size());
-        groups.push_back(FarGroup{static_cast<int32_t>(ppos), static_cast<int32_t>(lasts.size()), units[u].zout,
-                                  units[u].k});
-        for (size_t c = 0; c < lasts.size(); ++c) {
-          FarUnit& L = units[lasts[c]];
-          L.flags = 2;
-          L.grp = g;
-          L.zout = static_cast<int32_t>(ppos + static_cast<int64_t>(c) * L.ldk);
-        }
-        ppos += static_cast<int64_t>(lasts.size()) * units[u].ldk;
-      }
-      u = e;
-    }
-  }
+  int64_t ppos = 0, nw = 0, nwh = 0;
+  std::vector<int32_t> wf = plan_units(units, sizeof(TF), nsm, nw, groups, ppos);
+  const int32_t g_h0 = static_cast<int32_t>(groups.size());
+  std::vector<int32_t> wfh = plan_units(units_h, 2, nsm, nwh, groups, ppos);
+  (void)g_h0;
   SPX_CHECK(ppos < (int64_t(1) << 31), "far-field partial slots exceed 2^31");
-  for (const FarUnit& U : units)
-    SPX_CHECK(U.voff % EF == 0 && U.nc >= 1 && U.k >= 1 && U.ldk % EF == 0 && U.ldk >= U.k &&
-                  U.voff + static_cast<int64_t>(U.nc) * U.ldk <= fpos && U.xc >= 0 &&
-                  U.xc + static_cast<int64_t>(U.nc) <= H.Nb &&
-                  ((U.flags & 3) != 2 || (U.grp >= 0 && U.grp < static_cast<int64_t>(groups.size()) &&
-                                          U.zout + static_cast<int64_t>(U.k) <= ppos)),
-              "far_z plan: unit out of range");
+  auto check_units = [&](const std::vector<FarUnit>& us, int64_t cap, int E) {
+    for (const FarUnit& U : us)
+      SPX_CHECK(U.voff % E == 0 && U.nc >= 1 && U.k >= 1 && U.ldk % E == 0 && U.ldk >= U.k &&
+                    U.voff + static_cast<int64_t>(U.nc) * U.ldk <= cap && U.xc >= 0 &&
+                    U.xc + static_cast<int64_t>(U.nc) <= H.Nb &&
+                    ((U.flags & 3) != 2 || (U.grp >= 0 && U.grp < static_cast<int64_t>(groups.size()) &&
+                                            U.zout + static_cast<int64_t>(U.k) <= ppos)),
+                "far_z plan: unit out of range");
+  };
+  check_units(units, fpos, EF);
+  check_units(units_h, hpos, EH);
   H.zpart_len = ppos;
   H.nunits = static_cast<int64_t>(units.size());
-  H.nwarps_z = units.empty() ? 0 : nw;
+  H.nwarps_z = nw;
+  H.nunits_h = static_cast<int64_t>(units_h.size());
+  H.nwarps_z_h = nwh;
   H.units.upload(units, s);
   H.warp_first.upload(wf, s);
+  H.units_h.upload(units_h, s);
+  H.warp_first_h.upload(wfh, s);
   H.groups.upload(groups, s);
   H.gcnt.alloc(std::max<size_t>(groups.size(), 1));
   H.gcnt.zero(s);
 
-  std::vector<int64_t> ip(nseg + 1, 0), nb(nseg, 0);
+  std::vector<int64_t> ip(nseg + 1, 0), nb(nseg, 0), hb(nseg, 0);
   std::vector<RowItem> items;
   for (int64_t g = 0; g < nseg; ++g) {
     items.insert(items.end(), far_items[g].begin(), far_items[g].end());
+    hb[g] = static_cast<int64_t>(items.size());
+    items.insert(items.end(), half_items[g].begin(), half_items[g].end());
     nb[g] = static_cast<int64_t>(items.size());
     items.insert(items.end(), near_items[g].begin(), near_items[g].end());
     ip[g + 1] = static_cast<int64_t>(items.size());
@@ -564,6 +672,13 @@ void do_pack(HMatrix& H, cudaStream_t s) {
   H.item_ptr.upload(ip, s);
   H.near_begin.upload(nb, s);
   H.items.upload(items, s);
+  if (H.nunits_h > 0) {
+    H.half_begin.upload(hb, s);
+    H.zscale.upload(zsc, s);
+  } else {
+    H.half_begin.release();
+    H.zscale.release();
+  }
   SPX_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -580,10 +695,19 @@ void launch_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const
                                                        H.groups.p, H.gcnt.p);
     SPX_LAUNCH_CHECK();
   }
+  if (H.nunits_h > 0) {  // FP16 trailing columns of the split packing
+    const unsigned ctas = static_cast<unsigned>((H.nwarps_z_h + Z_WARPS - 1) / Z_WARPS);
+    k_far_z<__half, TA, TX><<<ctas, Z_WARPS * 32, 0, s>>>(
+        H.units_h.p, H.warp_first_h.p, static_cast<int>(H.nwarps_z_h), reinterpret_cast<const __half*>(H.far_h.p),
+        xp, z, zpart, H.groups.p, H.gcnt.p);
+    SPX_LAUNCH_CHECK();
+  }
+  const bool half = H.nunits_h > 0;
   k_rows<TF, TN, TA, TX, TS><<<static_cast<unsigned>(H.nseg), ROWS_WARPS * 32, 0, s>>>(
       H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TF*>(H.far_f.p),
       reinterpret_cast<const TN*>(H.near_f.p), z, xp, H.diag_perm.p, H.perm.p, gidx, dst, add, yb,
-      (H.prec != Prec::F64 && sizeof(TA) == sizeof(float)) ? 1 : 0);
+      (H.prec != Prec::F64 && sizeof(TA) == sizeof(float)) ? 1 : 0, half ? H.half_begin.p : nullptr,
+      half ? reinterpret_cast<const __half*>(H.far_h.p) : nullptr, half ? H.zscale.p : nullptr);
   SPX_LAUNCH_CHECK();
 }
 
@@ -600,12 +724,14 @@ void do_apply(HMatrix& H, const TS* src, const int32_t* gidx, TS* dst, const TS*
 }  // namespace
 
 void HMatrix::pack(Prec p, cudaStream_t s) {
+  if (p == Prec::SPLIT && !recompressed) recompress(s);  // the split needs SVD-ordered columns
   tr.reset();
   prec = p;
   switch (p) {
     case Prec::F64: do_pack<double, double>(*this, s); break;
     case Prec::F32: do_pack<float, float>(*this, s); break;
     case Prec::MIXED: do_pack<__nv_bfloat16, float>(*this, s); break;
+    case Prec::SPLIT: do_pack<float, float>(*this, s, true); break;
   }
   packed = true;
 }
@@ -617,13 +743,15 @@ void HMatrix::apply_gather(const T* src, const int32_t* gidx, T* dst, const T* a
   if (sizeof(T) == sizeof(double)) {
     switch (prec) {
       case Prec::F64: do_apply<double, double, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
-      case Prec::F32: do_apply<float, float, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::F32:
+      case Prec::SPLIT: do_apply<float, float, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
       case Prec::MIXED: do_apply<__nv_bfloat16, float, double, double, T>(*this, src, gidx, dst, add, yb, s); break;
     }
   } else {
     switch (prec) {
       case Prec::F64: do_apply<double, double, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
-      case Prec::F32: do_apply<float, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
+      case Prec::F32:
+      case Prec::SPLIT: do_apply<float, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
       case Prec::MIXED: do_apply<__nv_bfloat16, float, float, float, T>(*this, src, gidx, dst, add, yb, s); break;
     }
   }
@@ -639,7 +767,8 @@ int64_t HMatrix::device_bytes() const {
   return static_cast<int64_t>(far_f.bytes() + near_f.bytes() + units.bytes() + warp_first.bytes() + groups.bytes() +
                               gcnt.bytes() + seg_start.bytes() + item_ptr.bytes() + near_begin.bytes() +
                               items.bytes() + z.bytes() + zpart.bytes() + xperm.bytes() + diag_perm.bytes() +
-                              perm.bytes());
+                              perm.bytes() + far_h.bytes() + units_h.bytes() + warp_first_h.bytes() +
+                              half_begin.bytes() + zscale.bytes());
 }
 
 }  // namespace spx
@@ -694,7 +823,8 @@ void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s) 
   SPX_CHECK(H.packed, "H-matrix is not packed");
   switch (H.prec) {
     case Prec::F64: apply_noalloc_impl<double, double, double, double>(H, x, y, s); break;
-    case Prec::F32: apply_noalloc_impl<float, float, double, double>(H, x, y, s); break;
+    case Prec::F32:
+    case Prec::SPLIT: apply_noalloc_impl<float, float, double, double>(H, x, y, s); break;
     case Prec::MIXED: apply_noalloc_impl<__nv_bfloat16, float, double, double>(H, x, y, s); break;
   }
 }

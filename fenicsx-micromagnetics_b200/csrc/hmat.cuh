@@ -31,7 +31,10 @@ struct BoundaryDev {
   void dense_B(double* B, cudaStream_t s) const;
 };
 
-enum class Prec : int { F64 = 0, F32 = 1, MIXED = 2 };
+// packing of the H-matrix apply data: F64 / F32 factors and tiles; MIXED = BF16 factors with
+// FP32 tiles; SPLIT = recompressed factors with FP32 leading and FP16 trailing columns, FP32
+// tiles (pipelines use F64, F32 and MIXED only)
+enum class Prec : int { F64 = 0, F32 = 1, MIXED = 2, SPLIT = 3 };
 
 struct HBuildConfig {
   double epsilon = 1e-5;
@@ -41,6 +44,7 @@ struct HBuildConfig {
   int64_t max_temporary_block_bytes = 256ll * 1024 * 1024;
   double low_rank_storage_factor = 0.95;
   int64_t batch_bytes = 6ll * 1024 * 1024 * 1024;  // device workspace per fill/ACA batch
+  bool recompress = false;  // SVD recompression of the far factors after the build
 };
 
 struct HStats {
@@ -77,6 +81,11 @@ struct RowItem {
   int32_t len, src;
 };
 
+struct RecompressStats {
+  int64_t entries_before = 0, entries_after = 0, rewritten = 0;
+  double truncation_error_max = 0.0;  // largest truncation error of a block, relative to its norm
+};
+
 struct HMatrix {
   int device = 0;
   int64_t Nb = 0;
@@ -100,6 +109,12 @@ struct HMatrix {
   DevBuf<int64_t> item_ptr;       // [nseg + 1] items of each segment: far ones, then near ones
   DevBuf<int64_t> near_begin;     // [nseg] first near item of each segment
   DevBuf<RowItem> items;
+  DevBuf<char> far_h;             // SPLIT: FP16 trailing columns (V^T rows and U tiles)
+  DevBuf<FarUnit> units_h;        // SPLIT: k_far_z units of the FP16 columns
+  DevBuf<int32_t> warp_first_h;
+  DevBuf<int64_t> half_begin;     // SPLIT: [nseg] first FP16 far item of each segment
+  DevBuf<double> zscale;          // SPLIT: [zlen] sigma of each FP16 column (1 elsewhere)
+  int64_t nunits_h = 0, nwarps_z_h = 0;
   DevBuf<char> z, zpart;          // far z vectors and partial sums (accumulation type)
   DevBuf<char> xperm;             // x in perm order (vector type)
   int64_t nseg = 0, zlen = 0, zpart_len = 0, n_far = 0, n_near = 0, nunits = 0, nwarps_z = 0;
@@ -107,6 +122,11 @@ struct HMatrix {
   std::unique_ptr<HMatrix> tr;    // H^T (same tree; built on first use by transposed())
   DevBuf<double> xmulti, zmulti, zpmulti;  // state-interleaved work vectors of apply_multi
 
+  // SVD recompression of the far factors (hrecompress.cu); columns ordered by decreasing
+  // singular value, sigma[block] holds them for rewritten blocks (empty otherwise)
+  bool recompressed = false;
+  std::vector<std::vector<double>> sigma;
+  RecompressStats recompress(cudaStream_t s);
   void build(const BoundaryDev& bd, const HBuildConfig& c, cudaStream_t s);
   void pack(Prec p, cudaStream_t s);
   // y = H x in the original boundary ordering, FP64 vectors

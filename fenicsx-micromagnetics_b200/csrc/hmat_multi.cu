@@ -341,6 +341,14 @@ void HMatrix::apply_multi(const T* src, const int32_t* gidx, const int64_t* goff
     case Prec::F64: apply_chunks<double, double, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
     case Prec::F32: apply_chunks<float, float, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
     case Prec::MIXED: apply_chunks<__nv_bfloat16, float, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
+    case Prec::SPLIT:  // one state at a time through the single-vector kernels
+      SPX_CHECK(yb == nullptr || yoff != nullptr, "state outputs need offsets");
+      for (int r = 0; r < R; ++r) {
+        T* y = yb ? yb + yoff[r] : nullptr;
+        if (gidx) apply_gather<T>(src, gidx + goff[r], dst, add, y, s);
+        else apply_gather<T>(src + goff[r], nullptr, dst + goff[r], add ? add + goff[r] : nullptr, y, s);
+      }
+      break;
   }
 }
 template void HMatrix::apply_multi<double>(const double*, const int32_t*, const int64_t*, double*, const double*,

@@ -13,7 +13,7 @@ LIB_PATH = _HERE / "libspx.so"
 
 SPX_OK, SPX_ERR_INVALID, SPX_ERR_CUDA, SPX_ERR_OOM = 0, 1, 2, 3
 SPX_ERR_NOT_CONVERGED, SPX_ERR_TIMEOUT, SPX_ERR_INTERNAL, SPX_ERR_NO_DEVICE = 4, 5, 6, 7
-PREC = {"f64": 0, "fp64": 0, "float64": 0, "f32": 1, "fp32": 1, "float32": 1, "mixed": 2, "bf16": 2}
+PREC = {"f64": 0, "fp64": 0, "float64": 0, "f32": 1, "fp32": 1, "float32": 1, "mixed": 2, "bf16": 2, "f32_f16": 3}
 
 c_i32, c_i64, c_dbl, c_vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 P_i32, P_i64, P_dbl = C.POINTER(c_i32), C.POINTER(c_i64), C.POINTER(c_dbl)
@@ -21,7 +21,7 @@ P_i32, P_i64, P_dbl = C.POINTER(c_i32), C.POINTER(c_i64), C.POINTER(c_dbl)
 
 class HmatConfig(C.Structure):
     _fields_ = [("epsilon", c_dbl), ("eta", c_dbl), ("leaf_size", c_i32), ("max_rank", c_i32),
-                ("max_temporary_block_bytes", c_i64), ("precision", c_i32), ("reserved", c_i32),
+                ("max_temporary_block_bytes", c_i64), ("precision", c_i32), ("flags", c_i32),
                 ("batch_bytes", c_i64)]
 
 
@@ -63,6 +63,7 @@ SIGNATURES = {
     "spx_hmat_perm": (C.c_int, [c_vp, c_vp]),
     "spx_hmat_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_repack": (C.c_int, [c_vp, c_i32]),
+    "spx_hmat_recompress": (C.c_int, [c_vp, c_vp, P_dbl]),
     "spx_hmat_apply_noalloc": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_apply_multi": (C.c_int, [c_vp, c_vp, c_vp, c_i32, c_vp]),

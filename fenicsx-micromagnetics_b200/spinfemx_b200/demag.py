@@ -28,7 +28,7 @@ class DemagFieldLindholmGPU:
                  hmatrix_precision=None, warm_start=False, hmatrix_batch_bytes=0, hmatrix_verbose=False,
                  u1_preconditioner="amg", hmatrix_cache_path=None, hmatrix_cache_dir="./hmatrix_cache",
                  cache_tag=None, hmatrix_force_rebuild=False, hmatrix_cache_compressed=False, sample_offsets=None,
-                 dense_max_nb=4096, **unused):
+                 dense_max_nb=4096, hmatrix_recompress=False, **unused):
         """Options as in the reference, plus:
 
         precision          'f64' | 'f32' (plain FP32) | 'mixed' (FP64 vectors, FP32 matrices,
@@ -41,6 +41,8 @@ class DemagFieldLindholmGPU:
                            prediction error
         u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or
                            'jacobi'
+        hmatrix_recompress SVD-recompress the ACA factors after the build (same tolerance;
+                           needed by hmatrix_precision 'f32_f16')
         boundary_backend   also 'ensemble': X / tets is a disjoint union of independent samples
                            (``sample_offsets``: node ranges, see spinfemx_b200.ensemble); each
                            sample gets its own boundary operator, dense when its Nb <=
@@ -76,8 +78,10 @@ class DemagFieldLindholmGPU:
         if precision not in ("f64", "f32", "mixed"):
             raise ValueError("precision must be 'f64', 'f32' or 'mixed'")
         hprec = hmatrix_precision or ("f64" if precision == "f64" else "f32")
-        if hprec not in ("f64", "f32", "bf16"):
-            raise ValueError("hmatrix_precision must be 'f64', 'f32' or 'bf16'")
+        if hprec not in ("f64", "f32", "bf16", "f32_f16"):
+            raise ValueError("hmatrix_precision must be 'f64', 'f32', 'bf16' or 'f32_f16'")
+        if hprec == "f32_f16":
+            hmatrix_recompress = True
         self.hmatrix_precision = hprec
         ws = {False: 0, True: 1, 0: 0, 1: 1, 2: 2, 3: 3, "extrapolate": 2, "extrapolate_corrected": 3}.get(warm_start)
         if ws is None:
@@ -98,7 +102,8 @@ class DemagFieldLindholmGPU:
         o.hmat = _lib.HmatConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
                                  leaf_size=int(hmatrix_leaf_size), max_rank=int(hmatrix_max_rank or 0),
                                  max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
-                                 precision=_lib.PREC[hprec], reserved=0, batch_bytes=int(hmatrix_batch_bytes))
+                                 precision=_lib.PREC[hprec], flags=1 if hmatrix_recompress else 0,
+                                 batch_bytes=int(hmatrix_batch_bytes))
         self._h = C.c_void_p()
         self.hmatrix_cache_path = None
         if req == "hmatrix" and (hmatrix_cache_path is not None or cache_tag is not None):
@@ -116,7 +121,7 @@ class DemagFieldLindholmGPU:
             cfg = HMatrixBuildConfig(epsilon=float(hmatrix_epsilon), eta=float(hmatrix_eta),
                                      leaf_size=int(hmatrix_leaf_size), max_rank=hmatrix_max_rank,
                                      max_temporary_block_bytes=int(hmatrix_max_temporary_block_bytes),
-                                     batch_bytes=int(hmatrix_batch_bytes))
+                                     batch_bytes=int(hmatrix_batch_bytes), recompress=bool(hmatrix_recompress))
             Hc = build_or_load_hmatrix(self.hmatrix_cache_path, X, tets, cfg, precision=hprec,
                                        force_rebuild=bool(hmatrix_force_rebuild), verbose=bool(hmatrix_verbose),
                                        cache_compressed=bool(hmatrix_cache_compressed))

@@ -66,6 +66,8 @@ class HMatrixBuildConfig:
       MemoryError only when that fails too.
     * the randomized-SVD and progress fields are accepted and validated; the compressor is
       full-pivot ACA.
+    * ``recompress`` (this library's): SVD-recompress the ACA factors after the build to the
+      smallest ranks that keep every block within epsilon; required by the 'f32_f16' packing.
     """
     epsilon: float = 1e-6
     eta: float = 2.0
@@ -84,6 +86,7 @@ class HMatrixBuildConfig:
     gpu_rsvd_power_iterations: int = 1
     gpu_progress_interval_seconds: float = 5.0
     batch_bytes: int = 0
+    recompress: bool = False
 
     def __post_init__(self):
         if self.epsilon <= 0.0:
@@ -155,7 +158,8 @@ class HMatrixBuildConfig:
         return _lib.HmatConfig(epsilon=self.epsilon, eta=self.eta, leaf_size=int(self.leaf_size),
                                max_rank=int(self.max_rank or 0),
                                max_temporary_block_bytes=int(self.max_temporary_block_bytes),
-                               precision=_lib.PREC[precision], reserved=0, batch_bytes=int(bb))
+                               precision=_lib.PREC[precision],
+                               flags=1 if (self.recompress or precision == "f32_f16") else 0, batch_bytes=int(bb))
 
 
 MIN_WORKSPACE = 64 * 1024 ** 2
@@ -264,6 +268,15 @@ class HMatrixGPUPackedFused:
         p = np.empty(self.size, np.int32)
         call("spx_hmat_perm", self._h, ptr(p))
         return p
+
+    def recompress(self):
+        """SVD recompression of the far factors (same tolerance); returns entries before /
+        after, blocks rewritten and the largest block truncation error (relative)."""
+        out = np.zeros(3, np.int64)
+        e = _lib.c_dbl()
+        call("spx_hmat_recompress", self._h, ptr(out), C.byref(e))
+        return {"entries_before": int(out[0]), "entries_after": int(out[1]), "rewritten": int(out[2]),
+                "max_rel_truncation": e.value}
 
     def repack(self, precision):
         call("spx_hmat_repack", self._h, _lib.PREC[precision])

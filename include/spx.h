@@ -58,6 +58,12 @@ typedef struct CUstream_st* spx_stream_t; /* same type as cudaStream_t */
 #define SPX_PREC_F64 0
 #define SPX_PREC_F32 1
 #define SPX_PREC_MIXED 2
+/* H-matrix packing only (spx_hmat_config.precision, spx_hmat_repack): factors recompressed
+ * (SPX_HMAT_RECOMPRESS, implied) with the leading columns of each far block in FP32 and the
+ * trailing ones, whose FP16 rounding stays within a tenth of the block's epsilon budget, as
+ * FP16 unit vectors scaled by their singular values; FP32 near tiles.  A transposed apply
+ * packs its transpose in FP32; ensembles (merged H-matrices) do not take it. */
+#define SPX_PREC_F32_F16 3
 
 /* ------------------------------------------------------------------ library */
 SPX_API const char* spx_last_error(void);
@@ -123,9 +129,16 @@ typedef struct {
   int32_t max_rank;                  /* <= 0: no limit */
   int64_t max_temporary_block_bytes; /* forced subdivision above this dense size */
   int32_t precision;                 /* SPX_PREC_* of the packed apply data */
-  int32_t reserved;
+  int32_t flags;                     /* SPX_HMAT_RECOMPRESS: SVD-recompress the ACA factors after the build */
   int64_t batch_bytes;               /* device workspace per fill/ACA batch (0: default) */
 } spx_hmat_config;
+/* flags: after the ACA build, rewrite every far block (rank <= 64) from the SVD of its core,
+ * truncated to the smallest rank that keeps ||A - U V||_F <= epsilon ||A||_F given its ACA
+ * residual (checked a posteriori per block; no counterpart in the reference, whose builder
+ * stores the ACA factors; its truncated_svd compressor, compressors.py:102-235, is the same
+ * family applied to dense blocks).  Columns come out in decreasing singular value, which the
+ * SPX_PREC_F32_F16 packing needs. */
+#define SPX_HMAT_RECOMPRESS 1
 /* build: cluster tree, block partition, GPU fill and full-pivot ACA
  * (HMatrixBuilder.build / build_or_load_hmatrix, builder.py:186-419, 814-927) */
 SPX_API int spx_hmat_build(spx_boundary b, const spx_hmat_config* cfg, spx_hmat* out);
@@ -140,6 +153,11 @@ SPX_API int spx_hmat_perm(spx_hmat h, int32_t* perm);
 /* y = H x in the original boundary ordering (HMatrixGPUPackedFused.matvec, backend_fused.py:496-512) */
 SPX_API int spx_hmat_apply(spx_hmat h, const double* x, double* y, spx_stream_t s);
 SPX_API int spx_hmat_repack(spx_hmat h, int32_t precision);
+/* SVD recompression of the far factors (see SPX_HMAT_RECOMPRESS) of a built or imported
+ * H-matrix, repacked in its current precision; out3 = (far factor entries before, after,
+ * blocks rewritten), *max_rel_err = the largest truncation error of a block relative to its
+ * norm.  No counterpart in the reference. */
+SPX_API int spx_hmat_recompress(spx_hmat h, int64_t* out3, double* max_rel_err);
 /* y = H x like spx_hmat_apply, for callers that cannot allocate device memory while they
  * run: a solver callback whose device memory is owned by another allocator (a PETSc or
  * framework memory pool that must not be bypassed), or a loop that may not stall on

@@ -10,6 +10,7 @@ and the rows' sums.  It was made by ``tests/golden/make_golden.py c2_rows``.
 Tolerances (relative L2 over the 4,096 rows, per vector):
   H-matrix (ACA 1e-5, leaf 64, eta 2), FP64 factors   1e-5 (the ACA tolerance)
   the same H-matrix packed with FP32 factors          1e-5
+  recompressed, FP32 + FP16 split columns             1e-5
   row sums of H (H 1 = -1 on every row)               1e-5 absolute
 """
 import numpy as np
@@ -66,9 +67,13 @@ def test_c2_hmatrix_vs_reference_rows(golden):
     H = spx.HMatrixGPUPackedFused(geom, spx.HMatrixBuildConfig(epsilon=1e-5, eta=2.0, leaf_size=64),
                                   precision="f64")
     ones = torch.ones(H.size, dtype=torch.float64, device="cuda")
-    for prec in ("f64", "f32"):
-        if prec != "f64":
-            H.repack(prec)
+    for prec in ("f64", "f32", "recompressed f32_f16"):
+        if prec == "f32":
+            H.repack("f32")
+        elif prec.startswith("recompressed"):
+            st = H.recompress()
+            assert st["entries_after"] < st["entries_before"]
+            H.repack("f32_f16")
         y = np.stack([H.matvec(torch.as_tensor(x[:, k].copy(), device="cuda")).cpu().numpy()[rows]
                       for k in range(3)], 1)
         errs = rows_rel_err(y, g["y"])
