@@ -76,7 +76,9 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", action="store_true")
     ap.add_argument("--ptxas-v", action="store_true", help="print register/spill usage")
+    ap.add_argument("-D", action="append", default=[], help="extra preprocessor definition (tuning builds)")
     a = ap.parse_args()
     ex = ["-Xptxas", "-v"] if a.ptxas_v else []
-    print(build(force=a.force or a.ptxas_v, verbose=a.v or a.ptxas_v, extra=ex))
+    ex += [f"-D{d}" for d in a.D]
+    print(build(force=a.force or a.ptxas_v or bool(a.D), verbose=a.v or a.ptxas_v, extra=ex))
     sys.exit(0)

@@ -189,7 +189,10 @@ int64_t AmgDevice::device_bytes() const {
 // ------------------------------------------------------------------ device phases
 namespace {
 
-constexpr int PCG_BLOCK = 1024;
+#ifndef SPX_PCG_BLOCK
+#define SPX_PCG_BLOCK 1024
+#endif
+constexpr int PCG_BLOCK = SPX_PCG_BLOCK;  // one CTA per SM (threads per CTA)
 
 struct RowRange {
   int64_t gw, nw;  // first warp, warp stride
@@ -383,15 +386,37 @@ __device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cin
 }
 
 // ---- R identical blocks (a batch of samples of one mesh): the matrix of one block and its
-// hierarchy are stored once, every vector holds R blocks one after the other ([R][n] per level).
-// Each phase reads a matrix slice once and gathers the R blocks' entries of every column, so a
-// warp keeps KB x R gathers in flight; each block's sums are formed column by column in order.
+// hierarchy are stored once.  The cycle's level vectors and the PCG work vectors r, p, q hold
+// the R blocks interleaved ([row][R]), so the R entries of a column are one vector load (8, 16
+// or 32 bytes); the PCG's right-hand side, solution and iterate (b, x, y, bh) keep the
+// ensemble's block order ([R][n]).  Each phase reads a matrix slice once.
+
+template <int R> struct VecR;
+template <> struct VecR<2> { using T = float2; };
+template <> struct VecR<4> { using T = float4; };
+template <int R>
+__device__ __forceinline__ void load_r(const float* __restrict__ v, int64_t c, float (&g)[R]) {
+  if constexpr (R == 8) {
+    const float4 a = reinterpret_cast<const float4*>(v + c * 8)[0];
+    const float4 b = reinterpret_cast<const float4*>(v + c * 8)[1];
+    g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y; g[6] = b.z; g[7] = b.w;
+  } else if constexpr (R == 4) {
+    const float4 a = reinterpret_cast<const float4*>(v)[c];
+    g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w;
+  } else if constexpr (R == 2) {
+    const float2 a = reinterpret_cast<const float2*>(v)[c];
+    g[0] = a.x; g[1] = a.y;
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) g[r] = v[c * R + r];
+  }
+}
 
 template <int R>
 __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
                                            const float* __restrict__ val, int64_t sl, int lane,
-                                           const float* __restrict__ v, int64_t nv, uint64_t pol, float (&t)[R]) {
-  constexpr int KB = R >= 8 ? 1 : 8 / R;
+                                           const float* __restrict__ v, uint64_t pol, float (&t)[R]) {
+  constexpr int KB = R >= 8 ? 4 : 8;  // columns in flight per thread
   const int64_t base = sp[sl];
   const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
   const float* vv = val + base + lane;
@@ -409,9 +434,7 @@ __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const
     }
     float g[KB][R];
 #pragma unroll
-    for (int u = 0; u < KB; ++u)
-#pragma unroll
-      for (int r = 0; r < R; ++r) g[u][r] = v[r * nv + c[u]];
+    for (int u = 0; u < KB; ++u) load_r<R>(v, c[u], g[u]);
 #pragma unroll
     for (int u = 0; u < KB; ++u)
 #pragma unroll
@@ -420,8 +443,10 @@ __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const
   for (; k < width; ++k) {
     const float w = ld_hint(vv + k * 32, pol);
     const int32_t c = ld_hint(cc + k * 32, pol);
+    float g[R];
+    load_r<R>(v, c, g);
 #pragma unroll
-    for (int r = 0; r < R; ++r) t[r] += w * v[r * nv + c];
+    for (int r = 0; r < R; ++r) t[r] += w * g[r];
   }
 }
 
@@ -431,12 +456,12 @@ __device__ void pre_a_r(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
     float t[R];
-    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.db, L.n, l2_policy_keep(), t);
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = r * L.n + i;
+        const int64_t j = i * R + r;
         const float d0 = L.db[j] / L.theta;
         const float r1 = L.db[j] - di * t[r] / L.theta;
         const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
@@ -453,12 +478,12 @@ __device__ void pre_b_r(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
     float t[R];
-    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, L.n, l2_policy_keep(), t);
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = r * L.n + i;
+        const int64_t j = i * R + r;
         L.r[j] = (L.r[j] - di * t[r]) / di;
       }
     }
@@ -479,11 +504,22 @@ __device__ void restrict_to_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRan
     for (int r = 0; r < R; ++r) t[r] = 0.0f;
     if (row < C.n) {
       const int64_t k1 = L.r_rp[row + 1];
-      for (int64_t k = L.r_rp[row] + gl; k < k1; k += G) {
-        const float w = L.r_val[k];
-        const int32_t c = L.r_col[k];
+      int64_t k = L.r_rp[row] + gl;
+      for (; k + G < k1; k += 2 * G) {  // two gathers in flight per lane
+        const float w0 = L.r_val[k], w1 = L.r_val[k + G];
+        const int32_t c0 = L.r_col[k], c1 = L.r_col[k + G];
+        float g0[R], g1[R];
+        load_r<R>(L.r, c0, g0);
+        load_r<R>(L.r, c1, g1);
 #pragma unroll
-        for (int r = 0; r < R; ++r) t[r] += w * L.r[r * L.n + c];
+        for (int r = 0; r < R; ++r) t[r] += w0 * g0[r] + w1 * g1[r];
+      }
+      for (; k < k1; k += G) {
+        const float w = L.r_val[k];
+        float g[R];
+        load_r<R>(L.r, L.r_col[k], g);
+#pragma unroll
+        for (int r = 0; r < R; ++r) t[r] += w * g[r];
       }
     }
 #pragma unroll
@@ -493,8 +529,8 @@ __device__ void restrict_to_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRan
       const float dc = C.dinv[row];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        C.b[r * C.n + row] = t[r];
-        C.db[r * C.n + row] = dc * t[r];
+        C.b[row * R + r] = t[r];
+        C.db[row * R + r] = dc * t[r];
       }
     }
   }
@@ -505,10 +541,10 @@ __device__ void prolong_from_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRa
   for (int64_t sl = rr.gw; sl < L.p_nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
     float t[R];
-    sell_dot_r<R>(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, C.n, l2_policy_stream(), t);
+    sell_dot_r<R>(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, l2_policy_stream(), t);
     if (i < L.n) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) L.x[r * L.n + i] += t[r];
+      for (int r = 0; r < R; ++r) L.x[i * R + r] += t[r];
     }
   }
 }
@@ -518,12 +554,12 @@ __device__ void post_c_r(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
     float t[R];
-    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.x, L.n, l2_policy_keep(), t);
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = r * L.n + i;
+        const int64_t j = i * R + r;
         const float r0 = L.db[j] - di * t[r];
         const float d0 = r0 / L.theta;
         L.x2[j] = L.x[j] + d0;
@@ -534,7 +570,8 @@ __device__ void post_c_r(const AmgLevelDev& L, RowRange rr) {
   }
 }
 
-// on the top level also the partial dots (r64, z^), (w, z^) over all R blocks
+// on the top level also the partial dots (r64, z^), (w, z^) over all R blocks; r64 is the
+// interleaved PCG residual, sdinv the block-ordered (replicated) scaling
 template <int R>
 __device__ void post_d_r(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
                          const double* __restrict__ sdinv, double& rz, double& wz, bool top) {
@@ -542,27 +579,28 @@ __device__ void post_d_r(const AmgLevelDev& L, RowRange rr, const double* __rest
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
     float t[R];
-    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, L.n, l2_policy_keep(), t);
+    sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
+      const double sd = top ? sdinv[i] : 1.0;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = r * L.n + i;
+        const int64_t j = i * R + r;
         const float r1 = L.r[j] - di * t[r];
         const float d1 = rho1 * rho0 * L.d[j] + (2.0f * rho1 / L.delta) * r1;
         const float z = L.x2[j] + d1;
         L.x[j] = z;
-        if (top) {  // sdinv and r64 are per block row j (sdinv replicated over the blocks)
-          const double zh = static_cast<double>(z) / sdinv[j];
+        if (top) {
+          const double zh = static_cast<double>(z) / sd;
           rz += r64[j] * zh;
-          wz += zh / sdinv[j];
+          wz += zh / sd;
         }
       }
     }
   }
 }
 
-// dense coarsest level for R blocks: b entries past nc (the row padding) are taken as 0
+// dense coarsest level for R blocks (interleaved vectors; b entries past nc are taken as 0)
 template <int R>
 __device__ void coarse_solve_r(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, int64_t ldc,
                                RowRange rr) {
@@ -579,15 +617,17 @@ __device__ void coarse_solve_r(const AmgLevelDev& L, const float* __restrict__ c
       for (int q = 0; q < 4; ++q) {
         const int64_t jj = 4 * j + q;
         if (jj < nc) {
+          float g[R];
+          load_r<R>(L.b, jj, g);
 #pragma unroll
-          for (int r = 0; r < R; ++r) s[r] += cq[q] * L.b[r * nc + jj];
+          for (int r = 0; r < R; ++r) s[r] += cq[q] * g[r];
         }
       }
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       for (int o = 16; o > 0; o >>= 1) s[r] += __shfl_xor_sync(0xffffffffu, s[r], o);
-      if (rr.lane == 0) L.x[r * nc + i] = s[r];
+      if (rr.lane == 0) L.x[i * R + r] = s[r];
     }
   }
 }
@@ -881,8 +921,9 @@ __device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
 
 // k_pcg_amg on R identical blocks: one CG on the block-diagonal system (the scalars are those of
 // the whole system, as for a disjoint union), with the block's matrix and hierarchy stored once.
-// Per-row data of the matrix (rsum, level dinv) are indexed by the block row i, the vectors and
-// the replicated sdinv / diag by j = r n + i.
+// Per-row data (rsum, sdinv, diag, level dinv) are those of block row i (identical blocks); b, x,
+// y, bh are indexed in block order (r n + i), the work vectors r, p, q and the level vectors
+// interleaved (i R + r).
 template <class TV, int R>
 __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
   __shared__ double sh[160];
@@ -912,15 +953,16 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
   {
     double bb = 0.0;
     PCG_ROWS_BEGIN
+      const double sd = P.sdinv[row];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int64_t j = r * n + row;
         double bv;
         if (P.bh_given) {
-          bv = P.bh[j] / P.sdinv[j];
+          bv = P.bh[j] / sd;
         } else {
           bv = static_cast<double>(P.b[j]) - meanb;
-          P.bh[j] = bv * P.sdinv[j];
+          P.bh[j] = bv * sd;
         }
         if (!P.warm) P.y[j] = 0.0;
         bb += bv * bv;
@@ -951,7 +993,15 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
         double acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = 0.0;
-        for (int k = 0; k < width; ++k) {
+        int k = 0;
+        for (; k + 2 <= width; k += 2) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          const double v0 = ld_hint(P.v64 + idx, pst), v1 = ld_hint(P.v64 + idx + 32, pst);
+          const int32_t c0 = ld_hint(P.col + idx, pkeep), c1 = ld_hint(P.col + idx + 32, pkeep);
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] += v0 * P.y[r * n + c0] + v1 * P.y[r * n + c1];
+        }
+        if (k < width) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
           const double v = ld_hint(P.v64 + idx, pst);
           const int32_t c = ld_hint(P.col + idx, pkeep);
@@ -959,15 +1009,16 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
           for (int r = 0; r < R; ++r) acc[r] += v * P.y[r * n + c];
         }
         const float di0 = dinv0[row];
+        const double sd = P.sdinv[row], dg = P.diag[row];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int64_t j = r * n + row;
-          const double rv = P.bh[j] - acc[r];
+          const double rv = P.bh[r * n + row] - acc[r];
+          const int64_t j = row * R + r;
           P.r[j] = rv;
-          const float rf = static_cast<float>(rv / P.sdinv[j]);
+          const float rf = static_cast<float>(rv / sd);
           b0[j] = rf;
           db0[j] = di0 * rf;
-          rh += P.diag[j] * rv * rv;
+          rh += dg * rv * rv;
         }
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
@@ -984,28 +1035,50 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
       const double rz = tot[0];
       const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
       const double beta = it == 0 ? 0.0 : rz / rz_old;
-      const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ of every block
+      const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ of every block (interleaved)
       double pq = 0.0;
       const uint64_t pkeep = l2_policy_keep();
       PCG_ROWS_BEGIN
+        float uf[R];
+        load_r<R>(u0, row, uf);
         double ui[R], acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          ui[r] = static_cast<double>(u0[r * n + row]);
+          ui[r] = static_cast<double>(uf[r]);
           acc[r] = 0.0;
         }
-        for (int k = 0; k < width; ++k) {
+        int k = 0;
+        for (; k + 4 <= width; k += 4) {
+          const int64_t i0 = base + ((int64_t)k << 5) + lane;
+          float w[4];
+          int32_t cc[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            w[u] = ld_hint(P.a32 + i0 + 32 * u, pkeep);
+            cc[u] = ld_hint(P.col + i0 + 32 * u, pkeep);
+          }
+          float g[4][R];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) load_r<R>(u0, cc[u], g[u]);
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+              acc[r] += static_cast<double>(w[u]) * (static_cast<double>(g[u][r]) - ui[r]);
+        }
+        for (; k < width; ++k) {
           const int64_t idx = base + ((int64_t)k << 5) + lane;
           const double w = static_cast<double>(ld_hint(P.a32 + idx, pkeep));
-          const int32_t cc = ld_hint(P.col + idx, pkeep);
+          float g[R];
+          load_r<R>(u0, ld_hint(P.col + idx, pkeep), g);
 #pragma unroll
-          for (int r = 0; r < R; ++r) acc[r] += w * (static_cast<double>(u0[r * n + cc]) - ui[r]);
+          for (int r = 0; r < R; ++r) acc[r] += w * (static_cast<double>(g[r]) - ui[r]);
         }
         const double rs = P.rsum[row];
+        const double sd = P.sdinv[row];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int64_t j = r * n + row;
-          const double sd = P.sdinv[j];
+          const int64_t j = row * R + r;
           const double av = (acc[r] + rs * ui[r]) * sd;
           const double z = ui[r] / sd;
           const double w = 1.0 / sd;
@@ -1025,16 +1098,17 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
       double rh = 0.0;
       PCG_ROWS_BEGIN
         const float di0 = dinv0[row];
+        const double sd = P.sdinv[row], dg = P.diag[row];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int64_t j = r * n + row;
-          P.y[j] += alpha * P.p[j];
+          const int64_t j = row * R + r;
+          P.y[r * n + row] += alpha * P.p[j];
           const double rv = P.r[j] - alpha * P.q[j];
           P.r[j] = rv;
-          const float rf = static_cast<float>(rv / P.sdinv[j]);
+          const float rf = static_cast<float>(rv / sd);
           b0[j] = rf;
           db0[j] = di0 * rf;
-          rh += P.diag[j] * rv * rv;
+          rh += dg * rv * rv;
         }
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
@@ -1050,8 +1124,9 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
   if (P.project) {
     double sx = 0.0;
     PCG_ROWS_BEGIN
+      const double sd = P.sdinv[row];
 #pragma unroll
-      for (int r = 0; r < R; ++r) sx += P.y[r * n + row] * P.sdinv[r * n + row];
+      for (int r = 0; r < R; ++r) sx += P.y[r * n + row] * sd;
     PCG_ROWS_END
     cta_partial(P.part, 1, sx, 0.0, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return;
@@ -1059,12 +1134,13 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
     mx = tot[0] / static_cast<double>(R * n);
   }
   PCG_ROWS_BEGIN
+    const double sd = P.sdinv[row];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int64_t j = r * n + row;
-      const double xv = P.y[j] * P.sdinv[j] - mx;
+      const double xv = P.y[j] * sd - mx;
       P.x[j] = static_cast<TV>(xv);
-      P.y[j] = xv / P.sdinv[j];
+      P.y[j] = xv / sd;
     }
   PCG_ROWS_END
   if (blockIdx.x == 0 && threadIdx.x == 0) {
