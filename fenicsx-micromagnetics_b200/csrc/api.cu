@@ -835,6 +835,29 @@ int spx_hmat_recompress(spx_hmat hm, int64_t* out3, double* max_rel_err) {
   API_END
 }
 
+int spx_hmat_tensor_cores(spx_hmat hm, int32_t enable, int64_t* plan_bytes) {
+  API_BEGIN
+  REQUIRE(hm);
+  HMatrix& H = hm->h();
+  if (enable) {
+    SPX_CHECK(H.packed && (H.prec == Prec::F32 || H.prec == Prec::F64 || H.prec == Prec::SPLIT),
+              "the tensor-core multi-state apply needs an F64, F32 or F32_F16 packing");
+    if (!H.tc) tc_build(H, 0);
+  } else {
+    H.tc.reset();
+  }
+  if (plan_bytes) *plan_bytes = tc_bytes(H);
+  API_END
+}
+
+int spx_hmat_tc_status(spx_hmat hm, int32_t* status) {
+  API_BEGIN
+  REQUIRE(hm); REQUIRE(status);
+  HMatrix& H = hm->h();
+  *status = tc_error(H, 0);
+  API_END
+}
+
 int spx_debug_fail_alloc(int64_t min_bytes, int32_t count) {
   API_BEGIN
   SPX_CHECK(min_bytes >= 0 && count >= 0, "min_bytes and count must be non-negative");

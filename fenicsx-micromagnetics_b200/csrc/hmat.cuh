@@ -81,6 +81,8 @@ struct RowItem {
   int32_t len, src;
 };
 
+struct TcPlan;  // hmat_tc.cu
+
 struct RecompressStats {
   int64_t entries_before = 0, entries_after = 0, rewritten = 0;
   double truncation_error_max = 0.0;  // largest truncation error of a block, relative to its norm
@@ -121,6 +123,8 @@ struct HMatrix {
   int64_t bytes_far = 0, bytes_near = 0;
   std::unique_ptr<HMatrix> tr;    // H^T (same tree; built on first use by transposed())
   DevBuf<double> xmulti, zmulti, zpmulti;  // state-interleaved work vectors of apply_multi
+  // far-field GEMMs of apply_multi on the tensor cores for batches of 8 (hmat_tc.cu); null: off
+  std::shared_ptr<TcPlan> tc;
 
   // SVD recompression of the far factors (hrecompress.cu); columns ordered by decreasing
   // singular value, sigma[block] holds them for rewritten blocks (empty otherwise)
@@ -161,6 +165,14 @@ void hmat_import(HMatrix& H, const BoundaryDev& bd, const HBuildConfig& c, Prec 
 // Block-diagonal concatenation of packed H-matrices (same packing precision) for one apply
 // over all of them (hio.cu); apply-side data only.
 void hmat_merge(const std::vector<const HMatrix*>& parts, HMatrix& M, cudaStream_t s);
+
+// tensor-core far field of the multi-state apply (hmat_tc.cu): tc_build packs the factors
+// (needs the FP64 pools), tc_far_apply returns the far part of Y (perm order, [Nb][8] FP64)
+// for the gathered X~ ([Nb][8]); tc_error reads the kernels' timeout flag
+void tc_build(HMatrix& H, cudaStream_t s);
+const double* tc_far_apply(HMatrix& H, const double* xm, cudaStream_t s);
+int tc_error(HMatrix& H, cudaStream_t s);
+int64_t tc_bytes(const HMatrix& H);
 
 // y = H x (original boundary ordering, FP64) using the library's static device scratch
 // instead of allocated buffers (see spx_hmat_apply_noalloc in include/spx.h).

@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(MROWS_WARPS * 32) k_rows_multi(
     const int64_t* __restrict__ near_begin, const RowItem* __restrict__ items, const TF* __restrict__ F,
     const TN* __restrict__ Nt, const double* __restrict__ z, const double* __restrict__ xm,
     const double* __restrict__ diag, const int32_t* __restrict__ perm, const int32_t* __restrict__ gidx, Offs goff,
-    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, Offs yoff) {
+    TD* __restrict__ dst, const TD* __restrict__ add, TD* __restrict__ yb, Offs yoff,
+    const double* __restrict__ yinit, int near_only) {
   __shared__ double part[MROWS_WARPS][MSEG * R];
   const int sgm = blockIdx.x;
   const int r0 = seg_start[sgm], nr = seg_start[sgm + 1] - r0;
@@ -265,13 +266,14 @@ __global__ void __launch_bounds__(MROWS_WARPS * 32) k_rows_multi(
   for (int q = lane; q < MSEG * R; q += 32) part[warp][q] = 0.0;
   __syncwarp();
   const int64_t i0 = item_ptr[sgm], im = near_begin[sgm], i1 = item_ptr[sgm + 1];
-  rows_items_multi<TF, R>(items, i0 + warp, im, F, z, nr, part[warp], lane);
+  if (!near_only) rows_items_multi<TF, R>(items, i0 + warp, im, F, z, nr, part[warp], lane);
   rows_items_multi<TN, R>(items, im + warp, i1, Nt, xm, nr, part[warp], lane);
   __syncthreads();
   for (int q = threadIdx.x; q < nr * R; q += blockDim.x) {
     const int row = q / R, r = q - row * R;
     const int64_t i = r0 + row;
     double y = diag[i] * xm[i * R + r];
+    if (yinit) y += yinit[i * R + r];  // the far field from the tensor-core path
 #pragma unroll
     for (int w = 0; w < MROWS_WARPS; ++w) y += part[w][row * R + r];
     const int32_t b = perm[i];
@@ -297,6 +299,15 @@ void launch_multi(HMatrix& H, const TS* src, const int32_t* gidx, const int64_t*
     H.zpmulti.alloc(std::max<int64_t>(H.zpart_len, 1) * R);
   k_hgather_multi<TS, R><<<grid_for(Nb, 256), 256, 0, s>>>(Nb, src, gidx, g, H.perm.p, H.xmulti.p);
   SPX_LAUNCH_CHECK();
+  if (R == 8 && H.tc) {  // far field on the tensor cores, then near field + diagonal + scatter
+    const double* yfar = tc_far_apply(H, H.xmulti.p, s);
+    k_rows_multi<TF, TN, TS, R><<<static_cast<unsigned>(H.nseg), MROWS_WARPS * 32, 0, s>>>(
+        H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TF*>(H.far_f.p),
+        reinterpret_cast<const TN*>(H.near_f.p), H.zmulti.p, H.xmulti.p, H.diag_perm.p, H.perm.p, gidx, g, dst, add,
+        yb, y, yfar, 1);
+    SPX_LAUNCH_CHECK();
+    return;
+  }
   if (H.nunits > 0) {
     const unsigned ctas = static_cast<unsigned>((H.nwarps_z + MZ_WARPS - 1) / MZ_WARPS);
     k_far_z_multi<TF, R><<<ctas, MZ_WARPS * 32, 0, s>>>(H.units.p, H.warp_first.p, static_cast<int>(H.nwarps_z),
@@ -307,7 +318,7 @@ void launch_multi(HMatrix& H, const TS* src, const int32_t* gidx, const int64_t*
   k_rows_multi<TF, TN, TS, R><<<static_cast<unsigned>(H.nseg), MROWS_WARPS * 32, 0, s>>>(
       H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TF*>(H.far_f.p),
       reinterpret_cast<const TN*>(H.near_f.p), H.zmulti.p, H.xmulti.p, H.diag_perm.p, H.perm.p, gidx, g, dst, add,
-      yb, y);
+      yb, y, nullptr, 0);
   SPX_LAUNCH_CHECK();
 }
 
@@ -341,14 +352,19 @@ void HMatrix::apply_multi(const T* src, const int32_t* gidx, const int64_t* goff
     case Prec::F64: apply_chunks<double, double, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
     case Prec::F32: apply_chunks<float, float, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
     case Prec::MIXED: apply_chunks<__nv_bfloat16, float, T>(*this, src, gidx, goff, dst, add, yb, yoff, R, s); break;
-    case Prec::SPLIT:  // one state at a time through the single-vector kernels
+    case Prec::SPLIT: {  // batches of 8 on the tensor cores when enabled, the rest one at a time
       SPX_CHECK(yb == nullptr || yoff != nullptr, "state outputs need offsets");
-      for (int r = 0; r < R; ++r) {
+      int r = 0;
+      if (tc)
+        for (; r + 8 <= R; r += 8)
+          launch_multi<float, float, T, 8>(*this, src, gidx, goff + r, dst, add, yb, yoff ? yoff + r : nullptr, s);
+      for (; r < R; ++r) {
         T* y = yb ? yb + yoff[r] : nullptr;
         if (gidx) apply_gather<T>(src, gidx + goff[r], dst, add, y, s);
         else apply_gather<T>(src + goff[r], nullptr, dst + goff[r], add ? add + goff[r] : nullptr, y, s);
       }
       break;
+    }
   }
 }
 template void HMatrix::apply_multi<double>(const double*, const int32_t*, const int64_t*, double*, const double*,

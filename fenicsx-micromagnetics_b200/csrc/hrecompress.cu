@@ -434,6 +434,7 @@ RecompressStats HMatrix::recompress(cudaStream_t s) {
   recompressed = true;
   packed = false;
   tr.reset();
+  tc.reset();  // the tensor-core plan packs the old factors
   return st;
 }
 

@@ -64,6 +64,8 @@ SIGNATURES = {
     "spx_hmat_apply": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_repack": (C.c_int, [c_vp, c_i32]),
     "spx_hmat_recompress": (C.c_int, [c_vp, c_vp, P_dbl]),
+    "spx_hmat_tensor_cores": (C.c_int, [c_vp, c_i32, P_i64]),
+    "spx_hmat_tc_status": (C.c_int, [c_vp, P_i32]),
     "spx_hmat_apply_noalloc": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_apply_transpose": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_hmat_apply_multi": (C.c_int, [c_vp, c_vp, c_vp, c_i32, c_vp]),

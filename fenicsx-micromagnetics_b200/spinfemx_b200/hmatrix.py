@@ -269,6 +269,19 @@ class HMatrixGPUPackedFused:
         call("spx_hmat_perm", self._h, ptr(p))
         return p
 
+    def enable_tensor_cores(self, enable=True):
+        """Run the far field of matmat on the tensor cores for batches of 8 states (builds the
+        packed factors once); returns the plan's device bytes."""
+        b = _lib.c_i64()
+        call("spx_hmat_tensor_cores", self._h, 1 if enable else 0, C.byref(b))
+        return b.value
+
+    def tensor_core_status(self):
+        """0, or the timeout code of a tensor-core kernel since the last call."""
+        st = _lib.c_i32()
+        call("spx_hmat_tc_status", self._h, C.byref(st))
+        return st.value
+
     def recompress(self):
         """SVD recompression of the far factors (same tolerance); returns entries before /
         after, blocks rewritten and the largest block truncation error (relative)."""

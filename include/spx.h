@@ -180,6 +180,16 @@ SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_s
  * accumulation), so the factor traffic of an apply is shared; batches above 8 are applied in
  * chunks of at most 8.  Results equal nrhs calls of spx_hmat_apply up to rounding. */
 SPX_API int spx_hmat_apply_multi(spx_hmat h, const double* X, double* Y, int32_t nrhs, spx_stream_t s);
+/* Tensor cores for spx_hmat_apply_multi (no counterpart in the reference): with enable != 0,
+ * batches of 8 states run their far field as two block-sparse GEMMs on tcgen05 (column
+ * clusters: Z = V X; row clusters: Y += U Z; kind::tf32 with a three-term hi/lo split, FP32
+ * accumulation per tile of at most 2048 K elements, FP64 sums of the tiles), the near field
+ * and diagonal on the CUDA cores.  Builds the packed factors (about the FP32 factor bytes
+ * again; *plan_bytes = device bytes of the plan); enable = 0 drops them.  Needs the H-matrix's
+ * FP64 factors (built or imported, not merged).  spx_hmat_tc_status returns (and clears) the
+ * timeout flag of its kernels (SPX_ERR_TIMEOUT if a bounded wait ran out, else SPX_OK). */
+SPX_API int spx_hmat_tensor_cores(spx_hmat h, int32_t enable, int64_t* plan_bytes);
+SPX_API int spx_hmat_tc_status(spx_hmat h, int32_t* status);
 /* y = H^T x (original boundary ordering, FP64 device vectors of length Nb).  No counterpart
  * in the reference (its H-matrix backends apply H only); the adjoint of the demag operator
  * needs it.  The transposed H-matrix (same cluster tree, transposed partition, far factors

@@ -1,0 +1,47 @@
+"""The multi-state apply with the far field on the tensor cores (tcgen05, kind::tf32 with a
+three-term split) against the CUDA-core paths.
+
+Tolerances (relative L2 per state): tensor-core batch vs single applies of the same packing
+1e-6 (TF32 three-term products, FP32 accumulation per tile of <= 2048 K elements, FP64 sums);
+vs the dense operator 1e-5 (the ACA tolerance).  Batches of 8 use the tensor cores; other
+sizes fall back to the CUDA-core kernels for the remainder."""
+import numpy as np
+import pytest
+
+from oracle import mesh as omesh
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+
+def rel_rows(A, B):
+    return [float(torch.linalg.norm(A[r] - B[r]) / torch.linalg.norm(B[r])) for r in range(A.shape[0])]
+
+
+@pytest.mark.parametrize("nx,prec", [(48, "f32"), (100, "f32"), (100, "f32_f16")])
+def test_tensor_core_matmat_vs_single(nx, prec):
+    import spinfemx_b200 as spx
+    X, T = omesh.kuhn_box(nx, nx, 2, 2.5)
+    geom = spx.BoundaryGeometry(X, T)
+    H = spx.HMatrixGPUPackedFused(geom, spx.HMatrixBuildConfig(epsilon=1e-5), precision=prec)
+    g = torch.Generator(device=DEV).manual_seed(5)
+    Xs = torch.randn(8, H.size, dtype=torch.float64, device=DEV, generator=g)
+    Ys = torch.stack([H.matvec(Xs[r].contiguous()) for r in range(8)])
+    assert H.enable_tensor_cores() > 0
+    Yt = H.matmat(Xs)
+    torch.cuda.synchronize()
+    assert H.tensor_core_status() == 0
+    assert max(rel_rows(Yt, Ys)) < 1e-6
+    if nx == 48:
+        B = geom.dense_B()
+        assert max(rel_rows(Yt, (B @ Xs.T).T)) < 1e-5
+    # 11 states: one batch of 8 on the tensor cores, the rest on the CUDA cores
+    X11 = torch.randn(11, H.size, dtype=torch.float64, device=DEV, generator=g)
+    Y11 = H.matmat(X11)
+    Y11s = torch.stack([H.matvec(X11[r].contiguous()) for r in range(11)])
+    assert max(rel_rows(Y11, Y11s)) < 1e-6
+    # repeatable and switchable
+    assert torch.equal(H.matmat(Xs), Yt)
+    H.enable_tensor_cores(False)
+    assert max(rel_rows(H.matmat(Xs), Ys)) < 1e-9 if prec == "f32" else True
