@@ -538,6 +538,14 @@ def run_film_batch(a):
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     dm = ens.hef.demag_field
+    tc_bytes = None
+    if a.tensor_cores:  # far field of the shared H-matrix on the tensor cores (batches of 8)
+        import ctypes as C_
+        hh = C_.c_void_p()
+        _lib.call("spx_demag_ensemble_hmat", dm.handle, 0, C_.byref(hh))
+        nb = C_.c_int64()
+        _lib.call("spx_hmat_tensor_cores", hh, 1, C_.byref(nb))
+        tc_bytes = nb.value
     ens.set_state(m0s)
     ens.step(a.dt, a.warmup)
     torch.cuda.synchronize()
@@ -594,6 +602,7 @@ def run_film_batch(a):
                                f"each, one H-matrix ACA 1e-5 leaf 64 eta 2 (factors {dm.hmatrix_precision}) "
                                f"applied to all films, RK4 dt {a.dt:g}s",
                    "batch": R, "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2,
+                   "tensor_cores": bool(a.tensor_cores), "tensor_core_plan_bytes": tc_bytes,
                    "hmatrix_factor_gb": round((Hmem.get("far_bytes", 0) + Hmem.get("near_bytes", 0)) / 1e9, 2),
                    "demag_rel_err_vs_fp64_film0": err},
         "phases_ms_per_step": phases,
@@ -1049,6 +1058,7 @@ def main():
     ap.add_argument("--graph", type=int, default=1, help="ensemble: replay RK4 steps from CUDA graphs")
     ap.add_argument("--ens-compare", type=int, default=6, help="ensemble: samples also timed one by one")
     ap.add_argument("--batch", type=int, default=1, help="film: films of the same mesh integrated together")
+    ap.add_argument("--tensor-cores", type=int, default=0, help="batch: far field of the shared H-matrix on tcgen05")
     ap.add_argument("--workload", default="film", choices=["film", "adjoint", "ensemble"],
                     help="film: LLG steps/s on the 0.48M-node film (the headline); adjoint: trajectory gradient "
                          "on the 100x100x2 film")

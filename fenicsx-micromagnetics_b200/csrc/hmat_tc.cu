@@ -21,7 +21,8 @@
 // Warp roles of k_tc_gemm (384 threads, one CTA per SM, persistent over a tile list):
 //   warp 0   : cp.async.bulk of A stages into a 4-stage ring (mbarrier transaction counts);
 //   warp 1   : one thread issues tcgen05.mma (3 per K-step) and tcgen05.commit;
-//   warp 2   : allocates / frees 32 tensor-memory columns (two 128 x 8 FP32 accumulators);
+//   warp 2   : allocates / frees 32 tensor-memory columns (two 128 x 16 FP32 accumulators, of
+//              which the first 8 columns are the states; B's rows 8-15 are zero);
 //   warps 4-7: epilogue, tcgen05.ld of the accumulator (lanes 32 (w % 4) .. + 31) to partials;
 //   warps 8-11: split A into hi / lo in place, gather and split B, fence.proxy.async.
 // Every mbarrier wait is bounded; on a timeout the kernel records SPX_ERR_TIMEOUT, the roles
@@ -72,7 +73,9 @@ constexpr int STEP_BYTES = TM * 8 * 4;  // 4096: 128 rows x 8 TF32
 constexpr int STAGE_STEPS = 4;
 constexpr int NSTAGE = 4;
 constexpr int STAGE_BYTES = STAGE_STEPS * STEP_BYTES;
-constexpr int BSTEP_BYTES = R * 8 * 4;  // 256: 8 states x 8 TF32
+constexpr int NB = 16;                  // MMA N: M = 128 takes N in multiples of 16, so the
+                                        // 8 states are padded with 8 zero rows of B
+constexpr int BSTEP_BYTES = NB * 8 * 4;  // 512: 16 rows x 8 TF32
 constexpr int KSTEP_MAX = 256;          // K-steps per tile (2048 elements)
 constexpr int THREADS = 384;
 constexpr int SMEM_BYTES = 2 * NSTAGE * STAGE_BYTES + 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES + 1024 + 256;
@@ -124,8 +127,9 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   d |= static_cast<uint64_t>(1) << 46;  // descriptor version of sm_100
   return d;                             // base offset 0, no swizzle
 }
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 8, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((8u >> 3) << 17) | ((128u >> 4) << 24);
+// instruction descriptor: D F32, A and B TF32, both K-major, N = 16, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((static_cast<uint32_t>(NB) >> 3) << 17) |
+                           ((128u >> 4) << 24);
 
 __device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
   asm volatile(
@@ -148,9 +152,9 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 
 __device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
-// B (8 states x 8 K) of one K-step, K-major core-matrix layout: K chunk c = k / 4 at
-// c * 128 bytes, state n at n * 16, element k % 4 at 4 bytes
-__device__ __forceinline__ int boff(int n, int k) { return (k >> 2) * 128 + n * 16 + (k & 3) * 4; }
+// B (16 rows x 8 K; rows 8-15 stay zero) of one K-step, K-major core-matrix layout: K chunk
+// c = k / 4 at c * 256 bytes, row group n / 8 at 128, row n % 8 at 16, element k % 4 at 4
+__device__ __forceinline__ int boff(int n, int k) { return (k >> 2) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (k & 3) * 4; }
 
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const TcTile* __restrict__ tiles, int ntiles, const char* __restrict__ A,
@@ -185,6 +189,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
+  for (int e = tid; e < 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES / 16; e += THREADS)
+    reinterpret_cast<float4*>(sBhi)[e] = make_float4(0.f, 0.f, 0.f, 0.f);  // B hi and lo (contiguous)
+  fence_proxy_async();
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)), "r"(32)
                  : "memory");
@@ -226,7 +233,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int buf = tc & 1, use = tc >> 1;
         if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
         tc_after();
-        const uint32_t d = tbase + static_cast<uint32_t>(buf * R);
+        const uint32_t d = tbase + static_cast<uint32_t>(buf * NB);
         uint32_t acc = 0;
         bool ok = true;
         for (int s0 = 0; s0 < T.nsteps; s0 += STAGE_STEPS, ++item) {
@@ -240,7 +247,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t bh = su32(sBhi + (st * STAGE_STEPS + k) * BSTEP_BYTES);
             const uint32_t bl = su32(sBlo + (st * STAGE_STEPS + k) * BSTEP_BYTES);
             const uint64_t da = sdesc(a, 2048, 128), dal = sdesc(al, 2048, 128);
-            const uint64_t dbh = sdesc(bh, 128, 256), dbl = sdesc(bl, 128, 256);
+            const uint64_t dbh = sdesc(bh, 256, 128), dbl = sdesc(bl, 256, 128);
             mma_tf32(d, da, dbh, acc);
             acc = 1;
             mma_tf32(d, da, dbl, 1);
@@ -266,7 +273,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (!mbar_wait(&accf[buf], use & 1)) { fail(); break; }
       tc_after();
       uint32_t v[8];
-      tmem_ld8(tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * R), v);
+      tmem_ld8(tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * NB), v);
       tc_before();
       mbar_arrive(&acce[buf]);
       const int row = 32 * sp + lane;
