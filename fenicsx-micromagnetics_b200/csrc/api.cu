@@ -1,4 +1,5 @@
 // extern "C" entry points of libspx (declared in include/spx.h).
+#include <algorithm>
 #include <cstring>
 #include <memory>
 
@@ -835,14 +836,59 @@ int spx_hmat_recompress(spx_hmat hm, int64_t* out3, double* max_rel_err) {
   API_END
 }
 
+// time of one 8-state apply (ms, median of 3 after a warm-up) with the current setting
+static float time_multi8(HMatrix& H) {
+  const int64_t Nb = H.Nb;
+  DevBuf<double> X(8 * Nb), Y(8 * Nb);
+  X.zero(0);
+  std::vector<int64_t> off(8);
+  for (int r = 0; r < 8; ++r) off[r] = r * Nb;
+  cudaEvent_t a, b;
+  SPX_CUDA(cudaEventCreate(&a));
+  SPX_CUDA(cudaEventCreate(&b));
+  H.apply_multi<double>(X.p, nullptr, off.data(), Y.p, nullptr, nullptr, nullptr, 8, 0);
+  std::vector<float> t;
+  for (int k = 0; k < 3; ++k) {
+    SPX_CUDA(cudaEventRecord(a, 0));
+    H.apply_multi<double>(X.p, nullptr, off.data(), Y.p, nullptr, nullptr, nullptr, 8, 0);
+    SPX_CUDA(cudaEventRecord(b, 0));
+    SPX_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    SPX_CUDA(cudaEventElapsedTime(&ms, a, b));
+    t.push_back(ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::sort(t.begin(), t.end());
+  return t[1];
+}
+
 int spx_hmat_tensor_cores(spx_hmat hm, int32_t enable, int64_t* plan_bytes) {
   API_BEGIN
   REQUIRE(hm);
   HMatrix& H = hm->h();
+  SPX_CHECK(enable >= 0 && enable <= 2, "enable must be 0, 1 or 2 (autotune)");
   if (enable) {
     SPX_CHECK(H.packed && (H.prec == Prec::F32 || H.prec == Prec::F64 || H.prec == Prec::SPLIT),
               "the tensor-core multi-state apply needs an F64, F32 or F32_F16 packing");
-    if (!H.tc) tc_build(H, 0);
+    if (enable == 1) {
+      if (!H.tc) tc_build(H, 0);
+    } else {  // autotune: CUDA-core kernels vs tensor-core tiles of 512 / 2048 K elements
+      H.tc.reset();
+      float best = H.prec == Prec::SPLIT ? 1e30f : time_multi8(H);
+      int best_k = 0;
+      for (int ks : {64, 256}) {
+        tc_build(H, 0, ks);
+        const float t = time_multi8(H);
+        SPX_CHECK(tc_error(H, 0) == 0, "tensor-core apply timed out during autotuning");
+        if (t < best) {
+          best = t;
+          best_k = ks;
+        }
+        H.tc.reset();
+      }
+      if (best_k > 0) tc_build(H, 0, best_k);
+    }
   } else {
     H.tc.reset();
   }

@@ -169,7 +169,7 @@ void hmat_merge(const std::vector<const HMatrix*>& parts, HMatrix& M, cudaStream
 // tensor-core far field of the multi-state apply (hmat_tc.cu): tc_build packs the factors
 // (needs the FP64 pools), tc_far_apply returns the far part of Y (perm order, [Nb][8] FP64)
 // for the gathered X~ ([Nb][8]); tc_error reads the kernels' timeout flag
-void tc_build(HMatrix& H, cudaStream_t s);
+void tc_build(HMatrix& H, cudaStream_t s, int kstep_max = 0);
 const double* tc_far_apply(HMatrix& H, const double* xm, cudaStream_t s);
 int tc_error(HMatrix& H, cudaStream_t s);
 int64_t tc_bytes(const HMatrix& H);

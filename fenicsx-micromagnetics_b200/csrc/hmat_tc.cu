@@ -55,6 +55,7 @@ struct TcPack {
 
 struct TcPlan {
   int64_t zlen = 0, nslots1 = 0, nslots2 = 0, a_bytes = 0;
+  int kstep_max = 0;
   DevBuf<char> A1, A2;                 // packed A of the two phases
   DevBuf<TcTile> t1, t2;
   int32_t nt1 = 0, nt2 = 0;
@@ -76,7 +77,7 @@ constexpr int STAGE_BYTES = STAGE_STEPS * STEP_BYTES;
 constexpr int NB = 16;                  // MMA N: M = 128 takes N in multiples of 16, so the
                                         // 8 states are padded with 8 zero rows of B
 constexpr int BSTEP_BYTES = NB * 8 * 4;  // 512: 16 rows x 8 TF32
-constexpr int KSTEP_MAX = 256;          // K-steps per tile (2048 elements)
+constexpr int KSTEP_MAX_DEFAULT = 256;  // K-steps per tile (2048 elements); the autotuner also tries 64
 constexpr int THREADS = 384;
 constexpr int SMEM_BYTES = 2 * NSTAGE * STAGE_BYTES + 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES + 1024 + 256;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
@@ -383,8 +384,9 @@ Csr make_csr(int64_t nrows, const std::vector<std::pair<int64_t, int32_t>>& pair
 
 }  // namespace
 
-void tc_build(HMatrix& H, cudaStream_t s) {
+void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   using namespace tc;
+  const int KSTEP_MAX = kstep_max > 0 ? kstep_max : KSTEP_MAX_DEFAULT;
   SPX_CHECK(H.far_pool64.n > 0 || H.stats.n_far == 0, "the tensor-core apply needs the FP64 factors");
   auto P = std::make_shared<TcPlan>();
   std::vector<int> far;
@@ -492,6 +494,7 @@ void tc_build(HMatrix& H, cudaStream_t s) {
   P->nslots1 = slot1;
   P->nslots2 = slot2;
   P->a_bytes = a1 + a2;
+  P->kstep_max = KSTEP_MAX;
   P->A1.alloc(std::max<int64_t>(a1, 16));
   P->A2.alloc(std::max<int64_t>(a2, 16));
   P->t1.upload(t1, s);

@@ -271,9 +271,11 @@ class HMatrixGPUPackedFused:
 
     def enable_tensor_cores(self, enable=True):
         """Run the far field of matmat on the tensor cores for batches of 8 states (builds the
-        packed factors once); returns the plan's device bytes."""
+        packed factors once); enable="auto" times the CUDA-core path and two tensor-core tile
+        lengths and keeps the fastest.  Returns the plan's device bytes (0: CUDA cores)."""
         b = _lib.c_i64()
-        call("spx_hmat_tensor_cores", self._h, 1 if enable else 0, C.byref(b))
+        mode = 2 if enable == "auto" else (1 if enable else 0)
+        call("spx_hmat_tensor_cores", self._h, mode, C.byref(b))
         return b.value
 
     def tensor_core_status(self):

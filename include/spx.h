@@ -188,6 +188,9 @@ SPX_API int spx_hmat_apply_multi(spx_hmat h, const double* X, double* Y, int32_t
  * again; *plan_bytes = device bytes of the plan); enable = 0 drops them.  Needs the H-matrix's
  * FP64 factors (built or imported, not merged).  spx_hmat_tc_status returns (and clears) the
  * timeout flag of its kernels (SPX_ERR_TIMEOUT if a bounded wait ran out, else SPX_OK). */
+/* enable = 2 autotunes: one 8-state apply is timed on the CUDA-core kernels and on tensor-core
+ * tiles of 512 and of 2048 K elements, and the fastest is kept (*plan_bytes = 0 when the
+ * CUDA cores win). */
 SPX_API int spx_hmat_tensor_cores(spx_hmat h, int32_t enable, int64_t* plan_bytes);
 SPX_API int spx_hmat_tc_status(spx_hmat h, int32_t* status);
 /* y = H^T x (original boundary ordering, FP64 device vectors of length Nb).  No counterpart

@@ -45,3 +45,16 @@ def test_tensor_core_matmat_vs_single(nx, prec):
     assert torch.equal(H.matmat(Xs), Yt)
     H.enable_tensor_cores(False)
     assert max(rel_rows(H.matmat(Xs), Ys)) < 1e-9 if prec == "f32" else True
+
+
+def test_tensor_core_autotune_keeps_results():
+    import spinfemx_b200 as spx
+    X, T = omesh.kuhn_box(60, 60, 2, 2.5)
+    geom = spx.BoundaryGeometry(X, T)
+    H = spx.HMatrixGPUPackedFused(geom, spx.HMatrixBuildConfig(epsilon=1e-5), precision="f32")
+    g = torch.Generator(device=DEV).manual_seed(9)
+    Xs = torch.randn(8, H.size, dtype=torch.float64, device=DEV, generator=g)
+    Ys = torch.stack([H.matvec(Xs[r].contiguous()) for r in range(8)])
+    H.enable_tensor_cores("auto")          # keeps the fastest of three paths
+    assert H.tensor_core_status() == 0
+    assert max(rel_rows(H.matmat(Xs), Ys)) < 1e-6
