@@ -79,7 +79,9 @@ constexpr int NB = 16;                  // MMA N: M = 128 takes N in multiples o
 constexpr int BSTEP_BYTES = NB * 8 * 4;  // 512: 16 rows x 8 TF32
 constexpr int KSTEP_MAX_DEFAULT = 256;  // K-steps per tile (2048 elements); the autotuner also tries 64
 constexpr int THREADS = 384;
-constexpr int SMEM_BYTES = 2 * NSTAGE * STAGE_BYTES + 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES + 1024 + 256;
+// + a 32 KB guard after the buffers, so that no descriptor-addressed read can leave the
+// allocation even past the last stage
+constexpr int SMEM_BYTES = 2 * NSTAGE * STAGE_BYTES + 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES + 1024 + 256 + 32768;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
