@@ -258,6 +258,10 @@ struct LLGBase {
   virtual double rk_attempt(double dt, double rtol, double atol, const double* htu, const double* htn, bool reuse,
                             cudaStream_t s) = 0;
   virtual void rk_accept(cudaStream_t s) = 0;
+  virtual ImplicitResult bdf_attempt(double t, double dt, const ImplicitOpts& o, const double* htu,
+                                     const double* htn, cudaStream_t s) = 0;
+  virtual void bdf_accept(cudaStream_t s) = 0;
+  virtual void bdf_reset() = 0;
 };
 
 template <class TV, class TM>
@@ -304,11 +308,13 @@ struct LLGImpl : LLGBase {
   }
   void set_state(const double* m, cudaStream_t s) override {
     l.rk_fsal = false;
+    l.bdf_reset();
     convert<double, TV>(3 * l.N, m, l.m.p, s);
   }
   void get_state(double* m, cudaStream_t s) override { convert<TV, double>(3 * l.N, l.m.p, m, s); }
   void step(double dt, int64_t n, cudaStream_t s) override {
     l.rk_fsal = false;
+    l.bdf_reset();
     l.step_rk4(dt, n, s);
   }
   DevBuf<TV> tstage;
@@ -326,19 +332,30 @@ struct LLGImpl : LLGBase {
   void step_time_field(double dt, const double* htu, const double* htn, cudaStream_t s) override {
     l.graph_reset();
     l.rk_fsal = false;
+    l.bdf_reset();
     l.step_once(dt, s, htu, stage_fields(htn, 4, s));
   }
   double rk_attempt(double dt, double rtol, double atol, const double* htu, const double* htn, bool reuse,
                     cudaStream_t s) override {
     return l.rk_attempt(dt, rtol, atol, htu, stage_fields(htn, 7, s), reuse, s);
   }
-  void rk_accept(cudaStream_t s) override { l.rk_accept(s); }
+  void rk_accept(cudaStream_t s) override {
+    l.rk_accept(s);
+    l.bdf_reset();
+  }
+  ImplicitResult bdf_attempt(double t, double dt, const ImplicitOpts& o, const double* htu, const double* htn,
+                             cudaStream_t s) override {
+    return l.bdf_attempt(t, dt, o, htu, stage_fields(htn, 2, s), s);
+  }
+  void bdf_accept(cudaStream_t s) override { l.bdf_accept(s); }
+  void bdf_reset() override { l.bdf_reset(); }
   void run_host(const double* hin, double* hout, double dt, int64_t n) override {
     const int64_t n3 = 3 * l.N;
     cudaStream_t s = 0;
     if (!hstage.n) hstage.alloc(n3);
     SPX_CUDA(cudaMemcpyAsync(hstage.p, hin, n3 * sizeof(double), cudaMemcpyHostToDevice, s));
     convert<double, TV>(n3, hstage.p, l.m.p, s);
+    l.bdf_reset();
     l.step_rk4(dt, n, s);
     convert<TV, double>(n3, l.m.p, hstage.p, s);
     SPX_CUDA(cudaMemcpyAsync(hout, hstage.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1313,6 +1330,66 @@ int spx_llg_rk_accept(spx_llg l, spx_stream_t s) {
   API_BEGIN
   REQUIRE(l);
   l->impl->rk_accept(S(s));
+  API_END
+}
+
+static ImplicitOpts implicit_opts(const spx_bdf_opts* p) {
+  ImplicitOpts o;
+  if (!p) return o;
+  o.rtol = p->rtol; o.atol = p->atol;
+  o.snes_rtol = p->snes_rtol; o.snes_atol = p->snes_atol; o.snes_stol = p->snes_stol; o.snes_divtol = p->snes_divtol;
+  o.ksp_rtol = p->ksp_rtol; o.ksp_atol = p->ksp_atol; o.ksp_dtol = p->ksp_dtol;
+  o.ls_alpha = p->ls_alpha; o.ls_minlambda = p->ls_minlambda; o.ls_maxstep = p->ls_maxstep;
+  o.snes_max_it = p->snes_max_it; o.ksp_max_it = p->ksp_max_it; o.ksp_restart = p->ksp_restart;
+  o.ls_max_it = p->ls_max_it; o.use_pc = p->use_pc;
+  SPX_CHECK(o.rtol >= 0.0 && o.atol >= 0.0 && o.rtol + o.atol > 0.0,
+            "rtol and atol must be non-negative, not both zero");
+  SPX_CHECK(o.snes_max_it >= 1 && o.ksp_max_it >= 1 && o.ls_max_it >= 0, "iteration limits must be positive");
+  SPX_CHECK(o.ksp_restart >= 1 && o.ksp_restart <= 100, "ksp_restart must be in [1, 100]");
+  SPX_CHECK(o.ls_maxstep > 0.0 && o.ksp_dtol > 0.0, "ls_maxstep and ksp_dtol must be positive");
+  return o;
+}
+
+int spx_bdf_default_opts(spx_bdf_opts* o) {
+  API_BEGIN
+  REQUIRE(o);
+  const ImplicitOpts d;
+  o->rtol = d.rtol; o->atol = d.atol;
+  o->snes_rtol = d.snes_rtol; o->snes_atol = d.snes_atol; o->snes_stol = d.snes_stol; o->snes_divtol = d.snes_divtol;
+  o->ksp_rtol = d.ksp_rtol; o->ksp_atol = d.ksp_atol; o->ksp_dtol = d.ksp_dtol;
+  o->ls_alpha = d.ls_alpha; o->ls_minlambda = d.ls_minlambda; o->ls_maxstep = d.ls_maxstep;
+  o->snes_max_it = d.snes_max_it; o->ksp_max_it = d.ksp_max_it; o->ksp_restart = d.ksp_restart;
+  o->ls_max_it = d.ls_max_it; o->use_pc = d.use_pc; o->reserved = 0;
+  API_END
+}
+
+int spx_llg_bdf_attempt(spx_llg l, double t, double dt, const spx_bdf_opts* o, const double* h_uniform2x3,
+                        const double* h_nodes2, spx_bdf_result* r, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l); REQUIRE(r);
+  SPX_CHECK(dt > 0.0 && std::isfinite(t) && std::isfinite(dt), "dt must be positive and t finite");
+  const ImplicitResult x = l->impl->bdf_attempt(t, dt, implicit_opts(o), h_uniform2x3, h_nodes2, S(s));
+  r->wlte = x.wlte;
+  r->snes_reason = x.snes_reason;
+  r->order = x.order;
+  r->restarted = x.restarted;
+  r->newton_its = x.newton_its;
+  r->linear_its = x.linear_its;
+  r->fevals = x.fevals;
+  API_END
+}
+
+int spx_llg_bdf_accept(spx_llg l, spx_stream_t s) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->bdf_accept(S(s));
+  API_END
+}
+
+int spx_llg_bdf_reset(spx_llg l) {
+  API_BEGIN
+  REQUIRE(l);
+  l->impl->bdf_reset();
   API_END
 }
 

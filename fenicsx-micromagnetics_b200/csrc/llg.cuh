@@ -70,6 +70,38 @@ struct LLGAdjoint {
   DevBuf<double> part;
 };
 
+// Options and outcome of one implicit BDF attempt (implicit.cu); the fields mirror
+// spx_bdf_opts / spx_bdf_result of the C ABI.
+struct ImplicitOpts {
+  double rtol = 1e-6, atol = 1e-6;                                          // TS error tolerances
+  double snes_rtol = 1e-2, snes_atol = 1e-4, snes_stol = 1e-8, snes_divtol = 1e4;
+  double ksp_rtol = 1e-4, ksp_atol = 1e-50, ksp_dtol = 1e5;
+  double ls_alpha = 1e-4, ls_minlambda = 1e-12, ls_maxstep = 1e8;
+  int snes_max_it = 8, ksp_max_it = 200, ksp_restart = 30, ls_max_it = 40;
+  int use_pc = 1;
+};
+
+struct ImplicitResult {
+  double wlte = -1.0;   // weighted RMS local error estimate (< 0: none)
+  int snes_reason = 0;  // > 0 converged, < 0 diverged (PETSc's SNESConvergedReason values)
+  int order = 0;        // order of the error estimate for the step adaptor
+  int restarted = 0;    // 1: no history, a backward-Euler half step came first
+  int newton_its = 0, linear_its = 0, fevals = 0;
+};
+
+// History and work vectors of the implicit driver
+template <class TV>
+struct ImplicitWork {
+  DevBuf<TV> hist[2];  // y_{n-1}, y_{n-2} (newest first)
+  double t[2] = {0.0, 0.0};
+  int n = 0;           // past points held (0: the next attempt restarts)
+  DevBuf<TV> half, cand, pred, base, f, F, G, W, Y, t1, t2, V;
+  DevBuf<double> part, mpart, dev;
+  bool has_cand = false, cand_restart = false;
+  double cand_t = 0.0, cand_th = 0.0, cand_t0 = 0.0;
+  int64_t fevals = 0;
+};
+
 // TV: nodal vector type, TM: operator value type (see DemagCtx)
 template <class TV, class TM>
 struct LLGCtx {
@@ -124,6 +156,22 @@ struct LLGCtx {
   double rk_attempt(double dt, double rtol, double atol, const double* htu, const TV* htn, bool reuse_fsal,
                     cudaStream_t s);
   void rk_accept(cudaStream_t s);  // m = rk_ynew; k1 of the next attempt = k7 (FSAL)
+  // implicit BDF(2) driver (implicit.cu): one attempt of size dt from (t, m), Newton-Krylov
+  // stage solves; htu (host [2][3]) / htn (device [2][3N]) the time field at t + dt/2 and
+  // t + dt, or null.  bdf_accept makes the candidate the state and shifts the history.
+  ImplicitWork<TV> im;
+  ImplicitResult bdf_attempt(double t, double dt, const ImplicitOpts& o, const double* htu, const TV* htn,
+                             cudaStream_t s);
+  void bdf_accept(cudaStream_t s);
+  void bdf_reset() { im.n = 0; im.has_cand = false; }
+  void im_alloc();
+  void im_lin(int nv, const TV* const* v, const double* c, TV* out, cudaStream_t s);
+  double im_dot(const TV* a, const TV* b, cudaStream_t s);
+  void im_apply_A(double shift, const TV* v, TV* out, cudaStream_t s);
+  void im_apply_P(const TV* x, TV* y, bool use_pc, cudaStream_t s);
+  double im_residual(double shift, const TV* y, TV* F, cudaStream_t s);
+  int im_gmres(double shift, const TV* b, TV* x, const ImplicitOpts& o, int* its, cudaStream_t s);
+  int im_newton(double shift, TV* y, const ImplicitOpts& o, int* nits, int* lits, cudaStream_t s);
   LLGCtx() = default;
   LLGCtx(const LLGCtx&) = delete;
   LLGCtx& operator=(const LLGCtx&) = delete;

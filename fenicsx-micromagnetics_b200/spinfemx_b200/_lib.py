@@ -39,6 +39,19 @@ class LLGParams(C.Structure):
                 ("sot_Hdl", c_dbl), ("sot_Hfl", c_dbl), ("sot_p", c_vp), ("D_bulk", c_dbl)]
 
 
+class BdfOpts(C.Structure):
+    _fields_ = [("rtol", c_dbl), ("atol", c_dbl), ("snes_rtol", c_dbl), ("snes_atol", c_dbl),
+                ("snes_stol", c_dbl), ("snes_divtol", c_dbl), ("ksp_rtol", c_dbl), ("ksp_atol", c_dbl),
+                ("ksp_dtol", c_dbl), ("ls_alpha", c_dbl), ("ls_minlambda", c_dbl), ("ls_maxstep", c_dbl),
+                ("snes_max_it", c_i32), ("ksp_max_it", c_i32), ("ksp_restart", c_i32), ("ls_max_it", c_i32),
+                ("use_pc", c_i32), ("reserved", c_i32)]
+
+
+class BdfResult(C.Structure):
+    _fields_ = [("wlte", c_dbl), ("snes_reason", c_i32), ("order", c_i32), ("restarted", c_i32),
+                ("newton_its", c_i32), ("linear_its", c_i32), ("fevals", c_i32)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "spx_last_error": (C.c_char_p, []),
@@ -82,6 +95,11 @@ SIGNATURES = {
     "spx_llg_step_time_field": (C.c_int, [c_vp, c_dbl, c_vp, c_vp, c_vp]),
     "spx_llg_rk_attempt": (C.c_int, [c_vp, c_i32, c_dbl, c_dbl, c_dbl, c_vp, c_vp, c_i32, P_dbl, c_vp]),
     "spx_llg_rk_accept": (C.c_int, [c_vp, c_vp]),
+    "spx_bdf_default_opts": (C.c_int, [C.POINTER(BdfOpts)]),
+    "spx_llg_bdf_attempt": (C.c_int, [c_vp, c_dbl, c_dbl, C.POINTER(BdfOpts), c_vp, c_vp, C.POINTER(BdfResult),
+                                      c_vp]),
+    "spx_llg_bdf_accept": (C.c_int, [c_vp, c_vp]),
+    "spx_llg_bdf_reset": (C.c_int, [c_vp]),
     "spx_vec_node_diff_max": (C.c_int, [c_vp, c_vp, c_i64, P_dbl, c_vp]),
     "spx_demag_create_ensemble": (C.c_int, [c_vp, c_i64, c_vp, c_i64, c_dbl, C.POINTER(DemagOptions), c_i64, c_vp,
                                             c_i64, C.POINTER(c_vp)]),

@@ -279,6 +279,27 @@ class EffectiveField:
         call("spx_llg_rk_accept", self._h, _lib.stream_ptr())
         self.current_time += float(dt)
 
+    def bdf_attempt(self, dt, opts):
+        """One implicit BDF(2) attempt of size dt at current_time (spx_llg_bdf_attempt, not
+        committed).  opts: a _lib.BdfOpts.  Returns a dict with snes_reason (< 0: the stage
+        solve failed), wlte (weighted RMS local error estimate, < 0: none), order, restarted,
+        newton_its, linear_its, fevals."""
+        u = n = None
+        if self.H_time_func is not None:
+            u, n = self._stage_fields(self.current_time, float(dt), (0.5, 1.0))
+        r = _lib.BdfResult()
+        call("spx_llg_bdf_attempt", self._h, float(self.current_time), float(dt), C.byref(opts), ptr(u), ptr(n),
+             C.byref(r), _lib.stream_ptr())
+        return {k: getattr(r, k) for k, _ in _lib.BdfResult._fields_}
+
+    def bdf_accept(self, dt):
+        call("spx_llg_bdf_accept", self._h, _lib.stream_ptr())
+        self.current_time += float(dt)
+        self._ht_time = None   # the library holds the field of the last stage time
+
+    def bdf_reset(self):
+        call("spx_llg_bdf_reset", self._h)
+
     def set_graph(self, enable=True):
         """Replay each RK4 step from captured CUDA graphs (same results as ordinary steps)."""
         call("spx_llg_set_graph", self._h, 1 if enable else 0)
@@ -595,6 +616,98 @@ class LLG_GPU:
             return m, elapsed, stats
         return m, elapsed
 
+    def relax(self, m0_array, t0, t_final, dt_init, dt_save=None, dt_snap=None, output_dir="output", ts_rtol=1e-6,
+              ts_atol=1e-6, snes_rtol=1e-2, snes_atol=1e-4, ksp_rtol=1e-4, stopping_dmdt=0.0, monitor_fn=None,
+              save_final_state=True, check_every_stop=5, stop_print=False, return_stats=False, use_pc_python=True,
+              max_steps=50_000_000, max_reject=10):
+        """Implicit relaxation (LLG_GPU.relax, llg_module_GPU.py:2183-2381, with the solver of
+        _ensure_solver, :2052-2181).
+
+        Variable-step BDF(2) attempts on the device (spx_llg_bdf_attempt: Newton with the
+        quadratic backtracking line search, left-preconditioned GMRES(30) on shift I - J with
+        the 3x3 block preconditioner when use_pc_python, else none) from t0 until t_final is
+        reached or passed, with the TSAdapt "basic" options of _ensure_solver (:2074-2081):
+        clip (0.1, 3.0), safety 0.9, reject safety 0.1, dt in [1e-17, 1e-10], exponent
+        -1/order of the error estimate; a failed stage solve rejects the attempt and scales dt
+        by 0.25.  More than max_reject rejections in one step end the run (reason -2, PETSc's
+        TS_DIVERGED_STEP_REJECTED).  The dm/dt stopper (StopByMaxDmdtFDGPU, :314-382) ends the
+        run below stopping_dmdt deg/ns, tested every check_every_stop steps.  monitor_fn(step,
+        t, m) runs after every accepted step.  With save_final_state the final state is
+        written as <output_dir>/Relax.xdmf (the reference also writes ADIOS2).  Returns
+        (m, ctx, elapsed) or (m, ctx, elapsed, stats), ctx an ImplicitContext."""
+        import time
+        import torch
+        hef = self._build()
+        if m0_array is not None:
+            m0 = m0_array if isinstance(m0_array, torch.Tensor) else torch.as_tensor(
+                np.asarray(m0_array, dtype=np.float64))
+            hef.set_state(m0.to(device="cuda", dtype=torch.float64).contiguous())
+        hef.current_time = float(t0)
+        hef.bdf_reset()
+        o = _lib.BdfOpts()
+        call("spx_bdf_default_opts", C.byref(o))
+        o.rtol, o.atol = float(ts_rtol), float(ts_atol)
+        o.snes_rtol, o.snes_atol, o.ksp_rtol = float(snes_rtol), float(snes_atol), float(ksp_rtol)
+        o.use_pc = 1 if use_pc_python else 0
+        ad = TSAdaptBasic(dt_min=1e-17, dt_max=1e-10)
+        ctx = ImplicitContext()
+        stopper = DmdtStopper(hef, stopping_dmdt, check_every_stop, stop_print)
+        dt = min(max(float(dt_init), ad.dt_min), ad.dt_max)
+        step, reason, failures = 0, 0, 0
+        t_start = time.perf_counter()
+        while step < max_steps:
+            if hef.current_time >= float(t_final):
+                reason = 1          # TS_CONVERGED_TIME
+                break
+            accept_prev, nrej = True, 0
+            while True:
+                r = hef.bdf_attempt(dt, o)
+                ctx.newton_its += r["newton_its"]
+                ctx.linear_its += r["linear_its"]
+                ctx.fevals += r["fevals"]
+                if r["snes_reason"] < 0:
+                    failures += 1
+                    ad.rejected += 1
+                    accept, dt_next = False, dt * 0.25
+                else:
+                    ad.order = r["order"]
+                    accept, dt_next = ad.choose(dt, r["wlte"], accept_prev)
+                if accept:
+                    break
+                nrej += 1
+                accept_prev = False
+                dt = dt_next
+                if nrej > max_reject:
+                    reason = -2     # TS_DIVERGED_STEP_REJECTED
+                    break
+            if reason == -2:
+                break
+            hef.bdf_accept(dt)
+            step += 1
+            if monitor_fn is not None:
+                monitor_fn(step, hef.current_time, hef.get_state())
+            if stopper(step, hef.current_time):
+                reason = 2          # TS_CONVERGED_USER
+                dt = dt_next
+                break
+            dt = dt_next
+        elapsed = time.perf_counter() - t_start
+        ctx.calls = ctx.callsPre = ctx.linear_its
+        m = hef.get_state()
+        if save_final_state:
+            from pathlib import Path
+            from .io import XDMFWriter
+            Path(output_dir).mkdir(parents=True, exist_ok=True)
+            XDMFWriter(Path(output_dir) / "Relax.xdmf", self.X, self.tets).write_function(
+                m, time=hef.current_time, name="m")
+        stats = {"t_end": float(hef.current_time), "dt_last": float(dt), "nsteps": int(step), "reason": int(reason),
+                 "rejected": int(ad.rejected), "snes_failures": int(failures), "newton_its": ctx.newton_its,
+                 "linear_its": ctx.linear_its, "fevals": ctx.fevals,
+                 "maxdmdt_deg_ns": float(stopper.last_max_dmdt_deg_ns)}
+        if return_stats:
+            return m, ctx, elapsed, stats
+        return m, ctx, elapsed
+
     def run_fixed(self, m0, dt, nsteps):
         """Integrate nsteps of RK4 at step dt from m0 (3N numpy or CUDA tensor); returns m (CUDA tensor)."""
         import torch
@@ -606,11 +719,23 @@ class LLG_GPU:
         return hef.get_state()
 
 
+class ImplicitContext:
+    """What relax() returns in place of the reference's JvContext (llg_module_GPU.py:1412-1547):
+    the last shift and the counters of the run (calls = operator products in GMRES, callsPre
+    = preconditioner applications, both one per GMRES iteration)."""
+
+    def __init__(self):
+        self.shift = 0.0
+        self.calls = self.callsPre = 0
+        self.newton_its = self.linear_its = self.fevals = 0
+
+
 class TSAdaptBasic:
     """Step-size choice of PETSc's TSAdapt "basic" with the options the reference sets in
     _ensure_solver_explicit (llg_module_GPU.py:1765-1772): clip (0.1, 3.0), safety 0.9,
     reject safety 0.1, dt_min 1e-18, dt_max 1e-10; the error exponent is -1/5 (the
-    Dormand-Prince pair's order)."""
+    Dormand-Prince pair's order).  The implicit driver (_ensure_solver, :2074-2081) uses
+    dt_min 1e-17 and the order of each attempt's error estimate."""
 
     def __init__(self, clip=(0.1, 3.0), safety=0.9, reject_safety=0.1, dt_min=1e-18, dt_max=1e-10, order=5):
         self.clip, self.safety, self.reject_safety = clip, safety, reject_safety
@@ -618,7 +743,10 @@ class TSAdaptBasic:
         self.rejected = 0
 
     def choose(self, h, enorm, accept_prev=True):
-        """(accept, next h) for an attempt of size h with error norm enorm."""
+        """(accept, next h) for an attempt of size h with error norm enorm (< 0: no estimate,
+        accepted with h kept)."""
+        if enorm < 0.0:
+            return True, min(max(h, self.dt_min), self.dt_max)
         safety = self.safety
         if enorm > 1.0:
             if not accept_prev:

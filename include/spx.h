@@ -358,6 +358,40 @@ SPX_API int spx_llg_rk_attempt(spx_llg l, int32_t scheme, double dt, double rtol
                                const double* h_uniform7x3, const double* h_nodes7, int32_t reuse_fsal,
                                double* err_norm, spx_stream_t s);
 SPX_API int spx_llg_rk_accept(spx_llg l, spx_stream_t s);
+/* Implicit BDF(2) attempt: the stage solves of the reference's implicit driver
+ * (LLG_GPU._ensure_solver / relax, llg_module_GPU.py:2052-2381: PETSc TS bdf, SNES newtonls
+ * with the bt line search of order 2, KSP gmres left-preconditioned by JvContext's 3x3 block
+ * inverse, operator shift I - J, residual ydot - f).  The step-size adaptor is the caller's.
+ *   spx_bdf_default_opts: the reference's options (ts rtol/atol 1e-6, snes rtol 1e-2, atol
+ *       1e-4, stol 1e-8, divtol 1e4, max 8 its; ksp rtol 1e-4, atol 1e-50, dtol 1e5, max 200
+ *       its, restart 30; line search alpha 1e-4, min lambda 1e-12, max step 1e8, max 40 its;
+ *       use_pc 1 = the block preconditioner, 0 = none).
+ *   spx_llg_bdf_attempt: from the state at time t, one step of size dt (not committed).  With
+ *       no history (after create, set_state, any other stepping call or bdf_reset) a
+ *       backward-Euler half step to t + dt/2 comes first.  h_uniform2x3 (host [2][3]) and
+ *       h_nodes2 (device [2][N][3]) are the time-dependent field at t + dt/2 and t + dt, or
+ *       NULL.  Fills *r: snes_reason (> 0 converged: 2 |F| < atol, 3 |F| <= rtol |F_0|,
+ *       4 small step; < 0 the attempt failed), wlte (weighted RMS local error estimate,
+ *       tol_i = atol + rtol max(|y_i|, |m_i|)), order (of the estimate, for the adaptor's
+ *       exponent -1/order), restarted, and the Newton / GMRES iterations and RHS evaluations.
+ *   spx_llg_bdf_accept: makes a converged attempt the state and shifts the history. */
+typedef struct {
+  double rtol, atol;
+  double snes_rtol, snes_atol, snes_stol, snes_divtol;
+  double ksp_rtol, ksp_atol, ksp_dtol;
+  double ls_alpha, ls_minlambda, ls_maxstep;
+  int32_t snes_max_it, ksp_max_it, ksp_restart, ls_max_it;
+  int32_t use_pc, reserved;
+} spx_bdf_opts;
+typedef struct {
+  double wlte;
+  int32_t snes_reason, order, restarted, newton_its, linear_its, fevals;
+} spx_bdf_result;
+SPX_API int spx_bdf_default_opts(spx_bdf_opts* o);
+SPX_API int spx_llg_bdf_attempt(spx_llg l, double t, double dt, const spx_bdf_opts* o, const double* h_uniform2x3,
+                                const double* h_nodes2, spx_bdf_result* r, spx_stream_t s);
+SPX_API int spx_llg_bdf_accept(spx_llg l, spx_stream_t s);
+SPX_API int spx_llg_bdf_reset(spx_llg l);
 /* max over nodes of |a_i - b_i| for FP64 device AoS vectors [N][3] (StopByMaxDmdtFDGPU's
  * max |du|, llg_module_GPU.py:355-359) */
 SPX_API int spx_vec_node_diff_max(const double* a, const double* b, int64_t N, double* out, spx_stream_t s);

@@ -6,6 +6,9 @@
   options of the reference, from a random state on the same box: the same number of accepted
   and rejected steps as the oracle, step sizes within 1e-6 relative, final state within 1e-8;
   with the dm/dt stopper (StopByMaxDmdtFDGPU, :314-382) both stop at the same step.
+* relax (llg_module_GPU.py:2052-2381): BDF(2) with Newton-GMRES stage solves (block
+  preconditioner on and off, with and without a time-dependent field) against
+  oracle/implicit.py, with the same bars plus Newton / GMRES iteration totals within 2 %.
 """
 import math
 
@@ -99,4 +102,56 @@ def test_relax_explicit_dp5_vs_oracle(box, stop, t_final):
     assert st["rejected"] == so["rejected"]
     assert np.allclose(np.diff([0.0] + dts), so["dts"], rtol=1e-6, atol=0.0)
     assert abs(st["t_end"] - so["t_end"]) <= 1e-6 * so["t_end"]
+    assert np.abs(m.cpu().numpy() - mo).max() < 1e-8
+
+
+# ---------------------------------------------------------------- implicit driver (relax)
+# LLG_GPU.relax (llg_module_GPU.py:2052-2381) against oracle/implicit.py: the same BDF(2)
+# step sequence (accepted and rejected attempts), step sizes within 1e-6 relative, Newton and
+# GMRES iteration totals within 2 %, final state within 1e-8.
+
+@pytest.mark.parametrize("stop,t_final,use_pc", [(0.0, 2e-12, True), (1e3, 1e-9, True), (0.0, 1e-12, False)])
+def test_relax_implicit_bdf_vs_oracle(box, stop, t_final, use_pc):
+    import spinfemx_b200 as spx
+    from oracle import implicit as oimp
+    X, T, od = box
+    N = X.shape[0]
+    ohef = ollg.EffectiveFieldOracle(X, T, MS, Aex=AEX, alpha=ALPHA, demag=od, H0=np.tile([0.0, 0.0, 3e4], N))
+    m0 = _m0(N, 7)
+    dt0, tol = 1e-13, 1e-6
+    mo, so = oimp.relax_implicit(ohef, m0, 0.0, t_final, dt0, tol, tol, stopping_dmdt=stop, check_every=5,
+                                 use_pc=use_pc)
+    llg = spx.LLG_GPU(X, T, MS, alpha=ALPHA)
+    llg.add_exchange(AEX)
+    llg.add_demag(**TIGHT)
+    llg.add_external_field(H0_vec=[0.0, 0.0, 3e4])
+    ts = []
+    m, ctx, _, st = llg.relax(m0, 0.0, t_final, dt0, ts_rtol=tol, ts_atol=tol, stopping_dmdt=stop,
+                              check_every_stop=5, return_stats=True, save_final_state=False, use_pc_python=use_pc,
+                              monitor_fn=lambda step, t, u: ts.append(t))
+    assert so["nsteps"] > 50 and so["rejected"] >= 1
+    assert st["nsteps"] == so["nsteps"] and st["rejected"] == so["rejected"]
+    assert st["reason"] == so["reason"] == (2 if stop else 1)
+    assert st["snes_failures"] == so["snes_failures"]
+    assert np.allclose(np.diff([0.0] + ts), so["dts"], rtol=1e-6, atol=0.0)
+    assert abs(st["newton_its"] - so["newton_its"]) <= 0.02 * so["newton_its"]
+    assert abs(st["linear_its"] - so["linear_its"]) <= 0.02 * so["linear_its"]
+    assert ctx.linear_its == st["linear_its"]
+    assert np.abs(m.cpu().numpy() - mo).max() < 1e-8
+
+
+def test_relax_implicit_time_field_vs_oracle(box):
+    import spinfemx_b200 as spx
+    from oracle import implicit as oimp
+    X, T, od = box
+    N = X.shape[0]
+    ohef = ollg.EffectiveFieldOracle(X, T, MS, Aex=AEX, alpha=ALPHA, demag=od, H_time=_pulse)
+    m0 = _m0(N, 8)
+    mo, so = oimp.relax_implicit(ohef, m0, 0.0, 1e-12, 1e-13, 1e-6, 1e-6)
+    llg = spx.LLG_GPU(X, T, MS, alpha=ALPHA)
+    llg.add_exchange(AEX)
+    llg.add_demag(**TIGHT)
+    llg.add_external_field(H_time_func=lambda t: _pulse(t))
+    m, _, _, st = llg.relax(m0, 0.0, 1e-12, 1e-13, return_stats=True, save_final_state=False)
+    assert st["nsteps"] == so["nsteps"] and st["rejected"] == so["rejected"]
     assert np.abs(m.cpu().numpy() - mo).max() < 1e-8
