@@ -929,6 +929,13 @@ int spx_debug_fail_alloc(int64_t min_bytes, int32_t count) {
   API_END
 }
 
+int spx_debug_noalloc_cap(int64_t bytes) {
+  API_BEGIN
+  SPX_CHECK(bytes >= 0, "bytes must be non-negative");
+  spx::g_noalloc_cap.store(bytes);
+  API_END
+}
+
 int spx_hmat_destroy(spx_hmat hm) {
   API_BEGIN
   SPX_CHECK(!hm || !hm->ext, "this H-matrix handle belongs to a demag object (destroy the demag object instead)");

@@ -784,6 +784,7 @@ namespace spx {
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+std::atomic<int64_t> g_noalloc_cap{0};  // test cap on the accepted scratch size (0: none)
 
 namespace {
 
@@ -808,9 +809,12 @@ void apply_noalloc_impl(HMatrix& H, const double* x, double* y, cudaStream_t s) 
   const size_t xbytes = ((static_cast<size_t>(Nb) * sizeof(TX) + 255) / 256) * 256;
   const size_t zbytes = ((static_cast<size_t>(std::max<int64_t>(H.zlen, 1)) * sizeof(TA) + 255) / 256) * 256;
   const size_t pbytes = static_cast<size_t>(std::max<int64_t>(H.zpart_len, 1)) * sizeof(TA);
-  if (xbytes + zbytes + pbytes > kNoAllocScratchBytes)
-    throw Error(ERR_INVALID, "H-matrix too large for the 32 MiB static scratch of spx_hmat_apply_noalloc "
-                             "(needs " + std::to_string(xbytes + zbytes + pbytes) + " bytes); use spx_hmat_apply");
+  const int64_t cap = g_noalloc_cap.load();
+  const size_t limit = cap > 0 ? std::min(kNoAllocScratchBytes, static_cast<size_t>(cap)) : kNoAllocScratchBytes;
+  if (xbytes + zbytes + pbytes > limit)
+    throw Error(ERR_INVALID, "H-matrix too large for the " + std::to_string(limit) +
+                             "-byte static scratch of spx_hmat_apply_noalloc (needs " +
+                             std::to_string(xbytes + zbytes + pbytes) + " bytes); use spx_hmat_apply");
   unsigned char* base = static_cast<unsigned char*>(noalloc_scratch_address());
   launch_apply<TF, TN, TA, TX, double>(H, x, nullptr, y, nullptr, nullptr, reinterpret_cast<TX*>(base),
                                        reinterpret_cast<TA*>(base + xbytes),

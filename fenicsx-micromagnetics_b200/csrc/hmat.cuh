@@ -177,5 +177,6 @@ int64_t tc_bytes(const HMatrix& H);
 // y = H x (original boundary ordering, FP64) using the library's static device scratch
 // instead of allocated buffers (see spx_hmat_apply_noalloc in include/spx.h).
 void hmat_apply_noalloc(HMatrix& H, const double* x, double* y, cudaStream_t s);
+extern std::atomic<int64_t> g_noalloc_cap;  // test cap on its accepted scratch (0: none)
 
 }  // namespace spx

@@ -81,6 +81,9 @@ SPX_API int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* sta
  * the next `count` device allocations of the library of at least `min_bytes` bytes fail with
  * SPX_ERR_OOM on the host, before cudaMalloc is called (count 0 switches it off). */
 SPX_API int spx_debug_fail_alloc(int64_t min_bytes, int32_t count);
+/* Lowers the scratch size that spx_hmat_apply_noalloc accepts to `bytes` (0: back to its
+ * 32 MiB), so that its refusal of a too-large H-matrix can be tested on a small one. */
+SPX_API int spx_debug_noalloc_cap(int64_t bytes);
 
 /* ------------------------------------------------------------------ host geometry
  * Boundary data of build_boundary_data_serial (gpu/fields/Demag_Lindholm.py:177-285):

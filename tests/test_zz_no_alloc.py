@@ -51,3 +51,34 @@ def test_hmat_apply_noalloc_matches_apply(precision):
     H.matvec_noalloc(xs[1], out)
     torch.cuda.synchronize()
     assert np.linalg.norm(out.cpu().numpy() - outs[1]) <= 1e-12 * np.linalg.norm(outs[1])
+
+
+def test_hmat_apply_noalloc_refuses_too_large():
+    """An H-matrix whose scratch does not fit the static array is refused before any launch:
+    SPX_ERR_INVALID with a message that names the needed bytes, the output left untouched,
+    the handle still usable.  The 32 MiB array is lowered to 4 KiB for the test
+    (spx_debug_noalloc_cap) so that a small film needs more than it holds."""
+    import spinfemx_b200 as spx
+    from spinfemx_b200 import _lib
+    from oracle import mesh
+
+    X, T = mesh.kuhn_box(20, 20, 2, 2.5)
+    H = spx.HMatrixGPUPackedFused(spx.BoundaryGeometry(X, T),
+                                  spx.HMatrixBuildConfig(epsilon=1e-5, eta=2.0, leaf_size=64), precision="f32")
+    stream = _lib.stream_ptr()
+    x = torch.ones(H.size, dtype=torch.float64, device="cuda")
+    y = torch.full_like(x, float("nan"))
+    lib = _lib.lib()
+    try:
+        _lib.check(lib.spx_debug_noalloc_cap(4096))
+        rc = lib.spx_hmat_apply_noalloc(H._h, _lib.ptr(x), _lib.ptr(y), stream)
+        msg = lib.spx_last_error().decode()
+    finally:
+        _lib.check(lib.spx_debug_noalloc_cap(0))
+    torch.cuda.synchronize()
+    assert rc == _lib.SPX_ERR_INVALID
+    assert "too large" in msg and "needs" in msg
+    assert torch.isnan(y).all()
+    _lib.check(lib.spx_hmat_apply_noalloc(H._h, _lib.ptr(x), _lib.ptr(y), stream))
+    torch.cuda.synchronize()
+    assert np.abs(y.cpu().numpy() + 1.0).max() < 1e-5   # H 1 = -1
