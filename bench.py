@@ -250,7 +250,7 @@ def run_ours(a):
         demag_kwargs=dict(boundary_backend="hmatrix", hmatrix_epsilon=a.hmatrix_epsilon, hmatrix_eta=2.0,
                           hmatrix_leaf_size=a.hmatrix_leaf, ksp_rtol_u1=a.rtol_u1, ksp_rtol_u2=a.rtol_u2,
                           precision=a.precision,
-                          hmatrix_precision=a.hmatrix_precision,
+                          hmatrix_precision=a.hmatrix_precision, hmatrix_recompress=bool(a.hmatrix_recompress),
                           warm_start={0: False, 1: True, 2: "extrapolate", 3: "extrapolate_corrected"}[a.warm_start]))
     torch.cuda.synchronize()
     setup_s = time.time() - t0
@@ -348,7 +348,8 @@ def run_ours(a):
         "data": "synthetic (seeded Kuhn-box film and magnetisation)",
         "config": {"workload": f"film {a.nx}x{a.ny}x{a.nz} cubes @{a.h}nm, N={N}, Nb={dm.Nb}, H-matrix ACA "
                                f"{a.hmatrix_epsilon:g} leaf {a.hmatrix_leaf} eta 2, RK4 dt {a.dt:g}s, {a.precision} "
-                               f"(H factors {dm.hmatrix_precision})",
+                               f"(H factors {dm.hmatrix_precision}"
+                               f"{', SVD-recompressed' if a.hmatrix_recompress else ''})",
                    "nodes": N, "boundary_nodes": dm.Nb, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (H-matrix factors %.1f GB per apply)" % (
                        (Hmem["far_bytes"] + Hmem["near_bytes"]) / 1e9),
@@ -532,6 +533,7 @@ def run_film_batch(a):
     t0 = time.time()
     dk = dict(hmatrix_epsilon=1e-5, hmatrix_eta=2.0, hmatrix_leaf_size=64, ksp_rtol_u1=a.rtol_u1,
               ksp_rtol_u2=a.rtol_u2, hmatrix_precision=a.hmatrix_precision,
+              hmatrix_recompress=bool(a.hmatrix_recompress),
               warm_start={0: False, 1: True, 2: "extrapolate", 3: "extrapolate_corrected"}[a.warm_start])
     ens = spx.LLGEnsemble([(X, T)] * R, 8e5, Aex=1.3e-11, alpha=0.02, H0=[H0] * R, dense_max_nb=0,
                           precision=a.precision, demag_kwargs=dk)
@@ -587,6 +589,25 @@ def run_film_batch(a):
         ref.compute_vec(m_0, Hr)
         err = float(torch.linalg.norm(Hall[: 3 * N] - Hr) / torch.linalg.norm(Hr))
         del ref
+    single = None
+    if rank == 0 and a.compare_single:
+        # the same film alone (same precision, H-matrix settings and solver tolerances), timed
+        # over the same number of steps: the batched form's gain over one film at a time
+        hef1 = spx.EffectiveField(X, T, 8e5, Aex=1.3e-11, alpha=0.02, H0_static=H0, use_demag=True,
+                                  precision=a.precision, demag_kwargs=dict(dk, precision=a.precision))
+        hef1.set_state(torch.as_tensor(m0s[0], device="cuda"))
+        hef1.step(a.dt, a.warmup)
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        hef1.step(a.dt, a.steps)
+        f1.record()
+        torch.cuda.synchronize()
+        rate1 = 1000.0 * a.steps / f0.elapsed_time(f1)
+        single = {"steps_per_s": round(rate1, 4), "precision": a.precision,
+                  "h_factors": hef1.demag_field.hmatrix_precision}
+        del hef1
+        torch.cuda.empty_cache()
     if rank != 0:
         finish(ws)
         return
@@ -606,6 +627,8 @@ def run_film_batch(a):
                    "hmatrix_factor_gb": round((Hmem.get("far_bytes", 0) + Hmem.get("near_bytes", 0)) / 1e9, 2),
                    "demag_rel_err_vs_fp64_film0": err},
         "phases_ms_per_step": phases,
+        "single_film": single,
+        "vs_single_film": (round(job_rate(R * a.steps, ms, ws) / single["steps_per_s"], 3) if single else None),
         "cg": {"u1_iters_per_solve": round(dc[0][0] / max(dc[0][2], 1), 1),
                "u1_refinements_per_solve": round(dc[0][1] / max(dc[0][2], 1), 2),
                "u2_iters_per_solve": round(dc[1][0] / max(dc[1][2], 1), 1),
@@ -1033,7 +1056,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["f32", "f64", "mixed"])
-    ap.add_argument("--hmatrix-precision", default=None, choices=["f64", "f32", "bf16"])
+    ap.add_argument("--hmatrix-precision", default=None, choices=["f64", "f32", "bf16", "f32_f16"])
+    ap.add_argument("--hmatrix-recompress", type=int, default=1,
+                    help="SVD-recompress the ACA factors after the build (same tolerance)")
     ap.add_argument("--hmatrix-epsilon", type=float, default=1e-5,
                     help="film: ACA tolerance (the metric is quoted at 1e-5; larger values only for small "
                          "profiling captures of the solver kernels)")
@@ -1059,6 +1084,7 @@ def main():
     ap.add_argument("--ens-compare", type=int, default=6, help="ensemble: samples also timed one by one")
     ap.add_argument("--batch", type=int, default=1, help="film: films of the same mesh integrated together")
     ap.add_argument("--tensor-cores", type=int, default=0, help="batch: far field of the shared H-matrix on tcgen05")
+    ap.add_argument("--compare-single", type=int, default=1, help="batch: also time the film alone")
     ap.add_argument("--workload", default="film", choices=["film", "adjoint", "ensemble"],
                     help="film: LLG steps/s on the 0.48M-node film (the headline); adjoint: trajectory gradient "
                          "on the 100x100x2 film")

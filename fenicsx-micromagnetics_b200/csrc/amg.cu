@@ -26,6 +26,8 @@
 
 namespace spx {
 
+std::atomic<int> g_pcg_timing{0};  // phase timing marks of the AMG-PCG kernel (spx_debug_pcg_timing)
+
 namespace {
 
 void csr_to_sell(const CsrHost& A, HostSell& s, std::vector<float>& val) {
@@ -660,6 +662,7 @@ struct PcgParams {
   const float* cinv;
   int64_t nc, ldc;
   int reps;  // identical blocks: vectors hold reps x n entries, the matrix n rows
+  int timing;  // phase timing marks on (spx_debug_pcg_timing)
 };
 
 #define PCG_ROWS_BEGIN                                              \
@@ -673,10 +676,29 @@ struct PcgParams {
   }                  \
   }
 
+// Phase timing (switched on by spx_debug_pcg_timing): CTA 0 adds the globaltimer interval
+// since its previous mark to the slot of the phase that just ended (the phase's slowest CTA
+// plus the barrier); read and cleared by pcg_phase_times.  Slots: V-cycle phases in order
+// (3 per level down, the coarse solve, 3 per level up), 28 the PCG product, 29 the update,
+// 30 the true residual.
+__device__ unsigned long long g_pcg_phase_ns[32];
+__device__ unsigned long long g_pcg_phase_n[32];
+__device__ __forceinline__ void pcg_mark(unsigned long long& t_prev, int slot, int on) {
+  if (on && blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t_prev != 0ull && slot >= 0 && slot < 32) {
+      g_pcg_phase_ns[slot] += t - t_prev;
+      g_pcg_phase_n[slot] += 1ull;
+    }
+    t_prev = t;
+  }
+}
+
 // z^ = V(r^): lv[0].b / lv[0].db hold the unscaled residual D^1/2 r^ (FP32) on entry, lv[0].x
 // holds u = D^-1/2 z^ on exit, and slot `slot` of the partials holds (r^, z^), (w, z^).  nlev >= 2.
 template <class TV>
-__device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
+__device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh, unsigned long long& tm) {
   const unsigned nb = gridDim.x;
   unsigned int* cnt = P.bar;
   unsigned int* gen = P.bar + 1;
@@ -684,33 +706,42 @@ __device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh) {
                     static_cast<int64_t>((gridDim.x * static_cast<int64_t>(blockDim.x)) >> 5),
                     static_cast<int>(threadIdx.x & 31)};
   const int NL = P.nlev;
+  int ph = 0;
   for (int l = 0; l + 1 < NL; ++l) {
     const AmgLevelDev& L = P.lv[l];
     pre_a(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     pre_b(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     restrict_to(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
   }
   coarse_solve(P.lv[NL - 1], P.cinv, P.nc, P.ldc, rr);
   if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+  pcg_mark(tm, ph++, P.timing);
   for (int l = NL - 2; l >= 0; --l) {
     const AmgLevelDev& L = P.lv[l];
     prolong_from(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     post_c(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     double rz = 0.0, wz = 0.0;
     post_d(L, rr, P.r, P.sdinv, rz, wz, l == 0);
     if (l == 0) cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
   }
   return true;
 }
 
 template <class TV>
 __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
+  unsigned long long tm = 0ull;
   __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
@@ -786,6 +817,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 30, P.timing);
     }
     cta_total(P.part, 0, tot, sh);
     rr = tot[0];
@@ -793,7 +825,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
     if (rr <= tol2 || total >= P.maxit) break;
     double rz_old = 1.0;
     for (int it = 0;; ++it) {
-      if (!vcycle(P, 2, sh)) return;
+      if (!vcycle(P, 2, sh, tm)) return;
       cta_total(P.part, 2, tot, sh);
       const double rz = tot[0];
       const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
@@ -832,6 +864,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       PCG_ROWS_END
       cta_partial(P.part, 3, pq, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 28, P.timing);
       cta_total(P.part, 3, tot, sh);
       const double pqt = tot[0];
       if (!(pqt > 0.0) || !(rz > 0.0)) break;
@@ -848,6 +881,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 29, P.timing);
       cta_total(P.part, 0, tot, sh);
       rr = tot[0];
       ++total;
@@ -1256,12 +1290,27 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   q.maxit = maxit; q.max_outer = max_outer; q.warm = warm ? 1 : 0; q.project = project ? 1 : 0;
   q.bh_given = bh_given ? 1 : 0;
   q.lv = amg->lv.p; q.nlev = amg->nlev; q.cinv = amg->cinv.p; q.nc = amg->nc; q.ldc = amg->ldc;
+  q.timing = g_pcg_timing.load(std::memory_order_relaxed);
   void* args[] = {&q};
   void* k = reinterpret_cast<void*>(k_pcg_amg<TV>);
   if (reps == 2) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 2>);
   if (reps == 4) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 4>);
   if (reps == 8) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 8>);
   SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(PCG_BLOCK), args, 0, st));
+}
+
+// per-slot sums (ns) and counts of the phase timing marks since the last call
+void pcg_phase_times(double* ns32, int64_t* n32) {
+  unsigned long long a[32], b[32], z[32] = {};
+  SPX_CUDA(cudaDeviceSynchronize());
+  SPX_CUDA(cudaMemcpyFromSymbol(a, g_pcg_phase_ns, sizeof(a)));
+  SPX_CUDA(cudaMemcpyFromSymbol(b, g_pcg_phase_n, sizeof(b)));
+  SPX_CUDA(cudaMemcpyToSymbol(g_pcg_phase_ns, z, sizeof(z)));
+  SPX_CUDA(cudaMemcpyToSymbol(g_pcg_phase_n, z, sizeof(z)));
+  for (int i = 0; i < 32; ++i) {
+    ns32[i] = static_cast<double>(a[i]);
+    n32[i] = static_cast<int64_t>(b[i]);
+  }
 }
 
 template void CgSystem<double>::enable_amg(const HostSell&, const std::vector<int64_t>&, const std::vector<int32_t>&,

@@ -498,6 +498,9 @@ static std::unique_ptr<LLGBase> make_llg(spx_demag d, const double* X, int64_t N
 
 namespace spx {
 int barrier_timeout_probe(int nblocks, long long limit, int* timed_out_ctas);  // failure_probe.cu
+double barrier_time_us(int nblocks, int threads, int nbar);                  // failure_probe.cu
+void pcg_phase_times(double* ns32, int64_t* n32);                           // amg.cu
+extern std::atomic<int> g_pcg_timing;                                       // amg.cu
 }
 
 extern "C" {
@@ -833,6 +836,26 @@ int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int
   int t = 0;
   *status = spx::barrier_timeout_probe(nblocks, static_cast<long long>(limit), &t);
   *timed_out_ctas = t;
+  API_END
+}
+
+int spx_debug_barrier_time(int32_t nblocks, int32_t threads, int32_t nbarriers, double* us_per_barrier) {
+  API_BEGIN
+  REQUIRE(us_per_barrier);
+  *us_per_barrier = spx::barrier_time_us(nblocks, threads, nbarriers);
+  API_END
+}
+
+int spx_debug_pcg_timing(int32_t enable) {
+  API_BEGIN
+  spx::g_pcg_timing.store(enable != 0 ? 1 : 0);
+  API_END
+}
+
+int spx_debug_pcg_phase_times(double* ns32, int64_t* counts32) {
+  API_BEGIN
+  REQUIRE(ns32); REQUIRE(counts32);
+  spx::pcg_phase_times(ns32, counts32);
   API_END
 }
 

@@ -253,28 +253,36 @@ __device__ __forceinline__ double block_sum(double v, double* smem) {
 __device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int* gen,
                                              unsigned int nblocks, int* err,
                                              long long limit = (1ll << 26)) {
-  // One monotonic arrival counter (zeroed before the launch): a CTA adds 1 and waits until
-  // the counter reaches the next multiple of nblocks.  `gen` is not used.
+  // One monotonic arrival counter (zeroed before the launch): after the CTA's own barrier,
+  // thread 0 adds 1 with release semantics at GPU scope (covering every write the CTA made
+  // before bar.sync) and polls with acquire loads until the counter reaches the next multiple
+  // of nblocks; the closing bar.sync hands the acquired view to the CTA.  The error word is
+  // read every 1024 polls only (a CTA that gave up never arrives, so the others stop by it or
+  // by their own poll limit).  `gen` is not used.
   (void)gen;
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vc = count;
-    volatile int* verr = err;
-    __threadfence();
-    const unsigned int old = atomicAdd(count, 1u);
+    unsigned int old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(count) : "memory");
     const unsigned int target = (old / nblocks + 1u) * nblocks;
-    long long it = 0;
-    while (static_cast<int>(*vc - target) < 0) {
-      if (*verr != 0) break;
-      if (++it > limit) {
+    int ok = 1;
+    for (long long it = 1;; ++it) {
+      unsigned int v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+      if (static_cast<int>(v - target) >= 0) break;
+      if ((it & 1023) == 0 && *reinterpret_cast<volatile int*>(err) != 0) {
+        ok = 0;
+        break;
+      }
+      if (it > limit) {
         atomicCAS(err, 0, ERR_TIMEOUT);
+        ok = 0;
         break;
       }
       if (it > 4096) __nanosleep(32);
     }
-    __threadfence();
-    s_ok = (*verr == 0);
+    s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;

@@ -76,6 +76,18 @@ SPX_API int spx_device_count(int32_t* n);
  * code the device recorded (SPX_ERR_TIMEOUT) and *timed_out_ctas how many CTAs gave up.  The
  * context stays usable.  Returns SPX_OK when the probe ran. */
 SPX_API int spx_debug_barrier_probe(int32_t nblocks, int64_t limit, int32_t* status, int32_t* timed_out_ctas);
+/* Cost of the grid barrier that separates the phases of the persistent solvers: nbarriers
+ * barriers in a row on nblocks CTAs (1 .. number of SMs) of `threads` threads, timed with CUDA
+ * events on a cooperative launch; *us_per_barrier = microseconds per barrier. */
+SPX_API int spx_debug_barrier_time(int32_t nblocks, int32_t threads, int32_t nbarriers, double* us_per_barrier);
+/* Per-phase time of the AMG-PCG kernel: spx_debug_pcg_timing(1) makes later launches record,
+ * for 32 phase slots (V-cycle phases in order: pre-smoothing, residual and restriction per
+ * level down, the coarse solve, prolongation and two post-smoothing sweeps per level up; 28
+ * the PCG product, 29 the update, 30 the true residual), the nanoseconds from the previous
+ * phase end to this one's as CTA 0 saw them (the slowest CTA's work plus the barrier).
+ * spx_debug_pcg_phase_times returns the summed times and sample counts and clears them. */
+SPX_API int spx_debug_pcg_timing(int32_t enable);
+SPX_API int spx_debug_pcg_phase_times(double* ns32, int64_t* counts32);
 /* Out-of-memory injection for tests of the recovery paths (no counterpart in the reference,
  * whose builder catches CuPy's OutOfMemoryError, lindholm_hmatrix_gpu/builder.py:597-662):
  * the next `count` device allocations of the library of at least `min_bytes` bytes fail with

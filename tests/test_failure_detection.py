@@ -34,11 +34,26 @@ def test_barrier_wait_runs_out_and_reports(nblocks):
     assert torch.isfinite(H1).all() and torch.allclose(H1, H2, rtol=1e-10, atol=0.0)
 
 
+def test_barrier_cost_is_measured():
+    """The phase boundary of the persistent solvers, timed alone: finite, a few microseconds,
+    and no wait ran out (the call checks the error word)."""
+    import spinfemx_b200  # noqa: F401  (loads the library)
+    from spinfemx_b200 import _lib
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    for threads in (1024, 256):
+        us = C.c_double()
+        _lib.call("spx_debug_barrier_time", nsm, threads, 2000, C.byref(us))
+        assert 0.0 < us.value < 50.0, (threads, us.value)
+
+
 def test_probe_rejects_bad_arguments():
     from spinfemx_b200 import _lib
     status, gave_up = C.c_int32(), C.c_int32()
     assert _lib.lib().spx_debug_barrier_probe(1, 100, C.byref(status), C.byref(gave_up)) == 1
     assert _lib.lib().spx_debug_barrier_probe(4, 0, C.byref(status), C.byref(gave_up)) == 1
+    us = C.c_double()
+    assert _lib.lib().spx_debug_barrier_time(0, 1024, 10, C.byref(us)) == 1
+    assert _lib.lib().spx_debug_barrier_time(4, 1000, 10, C.byref(us)) == 1
 
 
 def test_hmatrix_build_recovers_from_out_of_memory():
