@@ -415,6 +415,21 @@ __device__ __forceinline__ void load_r(const float* __restrict__ v, int64_t c, f
 }
 
 template <int R>
+__device__ __forceinline__ void store_r(float* __restrict__ v, int64_t c, const float (&g)[R]) {
+  if constexpr (R == 8) {
+    reinterpret_cast<float4*>(v + c * 8)[0] = make_float4(g[0], g[1], g[2], g[3]);
+    reinterpret_cast<float4*>(v + c * 8)[1] = make_float4(g[4], g[5], g[6], g[7]);
+  } else if constexpr (R == 4) {
+    reinterpret_cast<float4*>(v)[c] = make_float4(g[0], g[1], g[2], g[3]);
+  } else if constexpr (R == 2) {
+    reinterpret_cast<float2*>(v)[c] = make_float2(g[0], g[1]);
+  } else {
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[c * R + r] = g[r];
+  }
+}
+
+template <int R>
 __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
                                            const float* __restrict__ val, int64_t sl, int lane,
                                            const float* __restrict__ v, uint64_t pol, float (&t)[R]) {
@@ -461,16 +476,20 @@ __device__ void pre_a_r(const AmgLevelDev& L, RowRange rr) {
     sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
+      float db[R], xo[R], dd[R], ro[R];
+      load_r<R>(L.db, i, db);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = i * R + r;
-        const float d0 = L.db[j] / L.theta;
-        const float r1 = L.db[j] - di * t[r] / L.theta;
+        const float d0 = db[r] / L.theta;
+        const float r1 = db[r] - di * t[r] / L.theta;
         const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
-        L.x[j] = d0 + d1;
-        L.d[j] = d1;
-        L.r[j] = r1;
+        xo[r] = d0 + d1;
+        dd[r] = d1;
+        ro[r] = r1;
       }
+      store_r<R>(L.x, i, xo);
+      store_r<R>(L.d, i, dd);
+      store_r<R>(L.r, i, ro);
     }
   }
 }
@@ -483,11 +502,11 @@ __device__ void pre_b_r(const AmgLevelDev& L, RowRange rr) {
     sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
+      float rv[R];
+      load_r<R>(L.r, i, rv);
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int64_t j = i * R + r;
-        L.r[j] = (L.r[j] - di * t[r]) / di;
-      }
+      for (int r = 0; r < R; ++r) rv[r] = (rv[r] - di * t[r]) / di;
+      store_r<R>(L.r, i, rv);
     }
   }
 }
@@ -529,11 +548,11 @@ __device__ void restrict_to_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRan
       for (int o = G >> 1; o > 0; o >>= 1) t[r] += __shfl_xor_sync(0xffffffffu, t[r], o);
     if (row < C.n && gl == 0) {
       const float dc = C.dinv[row];
+      float dbv[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        C.b[row * R + r] = t[r];
-        C.db[row * R + r] = dc * t[r];
-      }
+      for (int r = 0; r < R; ++r) dbv[r] = dc * t[r];
+      store_r<R>(C.b, row, t);
+      store_r<R>(C.db, row, dbv);
     }
   }
 }
@@ -545,8 +564,11 @@ __device__ void prolong_from_r(const AmgLevelDev& L, const AmgLevelDev& C, RowRa
     float t[R];
     sell_dot_r<R>(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, l2_policy_stream(), t);
     if (i < L.n) {
+      float xv[R];
+      load_r<R>(L.x, i, xv);
 #pragma unroll
-      for (int r = 0; r < R; ++r) L.x[i * R + r] += t[r];
+      for (int r = 0; r < R; ++r) xv[r] += t[r];
+      store_r<R>(L.x, i, xv);
     }
   }
 }
@@ -559,15 +581,20 @@ __device__ void post_c_r(const AmgLevelDev& L, RowRange rr) {
     sell_dot_r<R>(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep(), t);
     if (i < L.n) {
       const float di = L.dinv[i];
+      float db[R], xv[R], x2[R], dd[R], ro[R];
+      load_r<R>(L.db, i, db);
+      load_r<R>(L.x, i, xv);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = i * R + r;
-        const float r0 = L.db[j] - di * t[r];
+        const float r0 = db[r] - di * t[r];
         const float d0 = r0 / L.theta;
-        L.x2[j] = L.x[j] + d0;
-        L.d[j] = d0;
-        L.r[j] = r0;
+        x2[r] = xv[r] + d0;
+        dd[r] = d0;
+        ro[r] = r0;
       }
+      store_r<R>(L.x2, i, x2);
+      store_r<R>(L.d, i, dd);
+      store_r<R>(L.r, i, ro);
     }
   }
 }
@@ -585,19 +612,23 @@ __device__ void post_d_r(const AmgLevelDev& L, RowRange rr, const double* __rest
     if (i < L.n) {
       const float di = L.dinv[i];
       const double sd = top ? sdinv[i] : 1.0;
+      float rv[R], dv[R], x2[R], zo[R];
+      load_r<R>(L.r, i, rv);
+      load_r<R>(L.d, i, dv);
+      load_r<R>(L.x2, i, x2);
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int64_t j = i * R + r;
-        const float r1 = L.r[j] - di * t[r];
-        const float d1 = rho1 * rho0 * L.d[j] + (2.0f * rho1 / L.delta) * r1;
-        const float z = L.x2[j] + d1;
-        L.x[j] = z;
+        const float r1 = rv[r] - di * t[r];
+        const float d1 = rho1 * rho0 * dv[r] + (2.0f * rho1 / L.delta) * r1;
+        const float z = x2[r] + d1;
+        zo[r] = z;
         if (top) {
           const double zh = static_cast<double>(z) / sd;
-          rz += r64[j] * zh;
+          rz += r64[i * R + r] * zh;
           wz += zh / sd;
         }
       }
+      store_r<R>(L.x, i, zo);
     }
   }
 }

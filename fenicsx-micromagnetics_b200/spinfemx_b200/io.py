@@ -16,7 +16,10 @@ available here, so this module reads the files itself:
   DataItems are ``Format="HDF"`` (file.h5:/path), ``"XML"`` (inline) or ``"Binary"`` (raw).
 * ``XDMFWriter``: a mesh plus a time series of nodal vector fields as XDMF with raw binary
   heavy data (one little-endian file per array), readable by ParaView and by
-  ``read_xdmf_mesh`` / ``read_xdmf_series``.  ADIOS2 ``.bp`` output is not part of this build.
+  ``read_xdmf_mesh`` / ``read_xdmf_series``.
+* ``write_mesh`` / ``write_function`` / ``read_mesh`` / ``read_function``: checkpoints for a
+  restart, with adios4dolfinx's call names, in this module's own directory format (ADIOS2 BP
+  itself is not part of this build).
 """
 from __future__ import annotations
 
@@ -377,4 +380,80 @@ class XDMFWriter:
         self.path.write_text(xml)
 
 
-__all__ = ["read_hdf5", "read_xdmf_mesh", "read_xdmf_series", "XDMFWriter"]
+# ------------------------------------------------------------------ checkpoints
+# The reference saves a relaxed state with adios4dolfinx (write_mesh + write_function into
+# "Relax.bp", llg_module_GPU.py:2035-2042, 2373-2376) and restarts from it with read_mesh +
+# read_function (examples/gpu/Current_driven_skyrmion_Torus/Dynamics.py:33-43).  The same four
+# calls are offered here.  ADIOS2 is not in this image, so the checkpoint is this module's own
+# format, not ADIOS2 BP: a directory (as a BP file is) with index.json and raw little-endian
+# FP64 / int32 arrays; values round-trip exactly.
+
+def _ckpt_index(d: Path):
+    import json
+    f = d / "index.json"
+    return json.loads(f.read_text()) if f.exists() else {"format": "spinfemx_b200 checkpoint", "version": 1,
+                                                          "mesh": None, "functions": {}}
+
+
+def _ckpt_save(d: Path, idx):
+    import json
+    (d / "index.json").write_text(json.dumps(idx, indent=1))
+
+
+def write_mesh(filename, X, tets):
+    """Start a checkpoint at ``filename`` (a directory) with the mesh (X [N][3] nm, tets [E][4])."""
+    d = Path(filename)
+    d.mkdir(parents=True, exist_ok=True)
+    X = np.ascontiguousarray(X, dtype="<f8").reshape(-1, 3)
+    T = np.ascontiguousarray(tets, dtype="<i4").reshape(-1, 4)
+    X.tofile(d / "mesh_X.f64")
+    T.tofile(d / "mesh_tets.i32")
+    idx = {"format": "spinfemx_b200 checkpoint", "version": 1, "functions": {},
+           "mesh": {"nodes": int(X.shape[0]), "cells": int(T.shape[0])}}
+    _ckpt_save(d, idx)
+
+
+def write_function(filename, values, time=0.0, name="m"):
+    """Add nodal vectors (3N values, numpy or torch) named ``name`` at ``time`` (replacing an
+    entry of the same name and time)."""
+    d = Path(filename)
+    idx = _ckpt_index(d)
+    if idx.get("mesh") is None:
+        raise ValueError(f"{d}: write_mesh first")
+    if hasattr(values, "detach"):
+        values = values.detach().cpu().numpy()
+    v = np.ascontiguousarray(np.asarray(values, dtype="<f8").reshape(-1))
+    if v.size != 3 * idx["mesh"]["nodes"]:
+        raise ValueError(f"expected {3 * idx['mesh']['nodes']} values, got {v.size}")
+    entries = [e for e in idx["functions"].get(name, []) if e["time"] != float(time)]
+    serial = int(idx.get("arrays_written", 0))
+    fname = f"{name}_{serial:05d}.f64"
+    idx["arrays_written"] = serial + 1
+    v.tofile(d / fname)
+    entries.append({"time": float(time), "file": fname})
+    idx["functions"][name] = entries
+    _ckpt_save(d, idx)
+
+
+def read_mesh(filename):
+    """(X [N][3], tets [E][4]) of a checkpoint."""
+    d = Path(filename)
+    idx = _ckpt_index(d)
+    if idx.get("mesh") is None:
+        raise FileNotFoundError(f"{d}: no checkpoint mesh")
+    X = np.fromfile(d / "mesh_X.f64", dtype="<f8").reshape(-1, 3)
+    T = np.fromfile(d / "mesh_tets.i32", dtype="<i4").reshape(-1, 4)
+    return X, T
+
+
+def read_function(filename, time=0.0, name="m"):
+    """The 3N values of ``name`` stored at exactly ``time`` (KeyError otherwise)."""
+    d = Path(filename)
+    for e in _ckpt_index(d)["functions"].get(name, []):
+        if e["time"] == float(time):
+            return np.fromfile(d / e["file"], dtype="<f8")
+    raise KeyError(f"{d}: no function {name!r} at time {time!r}")
+
+
+__all__ = ["read_hdf5", "read_xdmf_mesh", "read_xdmf_series", "XDMFWriter", "write_mesh", "write_function",
+           "read_mesh", "read_function"]

@@ -547,6 +547,20 @@ class LLG_GPU:
                                       demag_kwargs=self._demag, precision=self.precision, **self._kw)
         return self.hef
 
+    def _save_final(self, m, output_dir, stem, t, checkpoint):
+        """The final state as <output_dir>/<stem>.xdmf (always, as the reference) and, with
+        checkpoint, as the restart checkpoint <output_dir>/<stem>.bp (io.write_mesh +
+        io.write_function at time 0, name "m": the reference's adios4dolfinx calls, in this
+        package's own checkpoint format)."""
+        from pathlib import Path
+        from . import io as sio
+        out = Path(output_dir)
+        out.mkdir(parents=True, exist_ok=True)
+        sio.XDMFWriter(out / f"{stem}.xdmf", self.X, self.tets).write_function(m, time=t, name="m")
+        if checkpoint:
+            sio.write_mesh(out / f"{stem}.bp", self.X, self.tets)
+            sio.write_function(out / f"{stem}.bp", m, time=0.0, name="m")
+
     def relax_explicit(self, m0_array, t0, t_final, dt_init, rk_type="5dp", dt_save=None, dt_snap=None,
                        output_dir="output_explicit", ts_rtol=1e-6, ts_atol=1e-6, stopping_dmdt=0.0,
                        monitor_fn=None, save_final_state=False, check_every_stop=5, stop_print=False,
@@ -561,8 +575,9 @@ class LLG_GPU:
         a second rejection in a row; dt kept in [1e-18, 1e-10].  The dm/dt stopper
         (StopByMaxDmdtFDGPU, :314-382) ends the run when max_i |m_i - m_prev_i| / (t - t_prev)
         falls below stopping_dmdt deg/ns, tested every check_every_stop steps.  monitor_fn(step,
-        t, m) is called after every accepted step when given; with save_final_state the final
-        state is written as <output_dir>/Relax_explicit.xdmf (the reference also writes ADIOS2).
+        t, m) is called after every accepted step when given.  The final state is written as
+        <output_dir>/Relax_explicit.xdmf and, with save_final_state, as the restart checkpoint
+        <output_dir>/Relax_explicit.bp (spinfemx_b200.io.read_mesh / read_function).
         Returns (m, elapsed) or (m, elapsed, stats)."""
         import time
         import torch
@@ -604,12 +619,7 @@ class LLG_GPU:
             dt = dt_next
         elapsed = time.perf_counter() - t_start
         m = hef.get_state()
-        if save_final_state:
-            from pathlib import Path
-            from .io import XDMFWriter
-            Path(output_dir).mkdir(parents=True, exist_ok=True)
-            XDMFWriter(Path(output_dir) / "Relax_explicit.xdmf", self.X, self.tets).write_function(
-                m, time=hef.current_time, name="m")
+        self._save_final(m, output_dir, "Relax_explicit", hef.current_time, save_final_state)
         stats = {"t_end": float(hef.current_time), "dt_last": float(dt), "nsteps": int(step), "reason": int(reason),
                  "rejected": int(ad.rejected), "maxdmdt_deg_ns": float(stopper.last_max_dmdt_deg_ns)}
         if return_stats:
@@ -632,8 +642,9 @@ class LLG_GPU:
         by 0.25.  More than max_reject rejections in one step end the run (reason -2, PETSc's
         TS_DIVERGED_STEP_REJECTED).  The dm/dt stopper (StopByMaxDmdtFDGPU, :314-382) ends the
         run below stopping_dmdt deg/ns, tested every check_every_stop steps.  monitor_fn(step,
-        t, m) runs after every accepted step.  With save_final_state the final state is
-        written as <output_dir>/Relax.xdmf (the reference also writes ADIOS2).  Returns
+        t, m) runs after every accepted step.  The final state is written as
+        <output_dir>/Relax.xdmf and, with save_final_state, as the restart checkpoint
+        <output_dir>/Relax.bp (spinfemx_b200.io.read_mesh / read_function).  Returns
         (m, ctx, elapsed) or (m, ctx, elapsed, stats), ctx an ImplicitContext."""
         import time
         import torch
@@ -694,12 +705,7 @@ class LLG_GPU:
         elapsed = time.perf_counter() - t_start
         ctx.calls = ctx.callsPre = ctx.linear_its
         m = hef.get_state()
-        if save_final_state:
-            from pathlib import Path
-            from .io import XDMFWriter
-            Path(output_dir).mkdir(parents=True, exist_ok=True)
-            XDMFWriter(Path(output_dir) / "Relax.xdmf", self.X, self.tets).write_function(
-                m, time=hef.current_time, name="m")
+        self._save_final(m, output_dir, "Relax", hef.current_time, save_final_state)
         stats = {"t_end": float(hef.current_time), "dt_last": float(dt), "nsteps": int(step), "reason": int(reason),
                  "rejected": int(ad.rejected), "snes_failures": int(failures), "newton_its": ctx.newton_its,
                  "linear_its": ctx.linear_its, "fevals": ctx.fevals,

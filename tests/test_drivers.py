@@ -81,7 +81,7 @@ def test_time_field_rk4_vs_oracle(box, kind):
 
 
 @pytest.mark.parametrize("stop,t_final", [(0.0, 2e-11), (1e4, 1e-10)])
-def test_relax_explicit_dp5_vs_oracle(box, stop, t_final):
+def test_relax_explicit_dp5_vs_oracle(box, stop, t_final, tmp_path):
     import spinfemx_b200 as spx
     X, T, od = box
     N = X.shape[0]
@@ -95,7 +95,7 @@ def test_relax_explicit_dp5_vs_oracle(box, stop, t_final):
     llg.add_external_field(H0_vec=[0.0, 0.0, 3e4])
     dts = []
     m, _, st = llg.relax_explicit(m0, 0.0, t_final, dt0, ts_rtol=tol, ts_atol=tol, stopping_dmdt=stop,
-                                  check_every_stop=5, return_stats=True,
+                                  check_every_stop=5, return_stats=True, output_dir=str(tmp_path),
                                   monitor_fn=lambda step, t, u: dts.append(t))
     assert so["nsteps"] > 100 and so["rejected"] > 5 and st["nsteps"] == so["nsteps"]
     assert st["reason"] == so["reason"] == (2 if stop else 1)
@@ -111,7 +111,7 @@ def test_relax_explicit_dp5_vs_oracle(box, stop, t_final):
 # GMRES iteration totals within 2 %, final state within 1e-8.
 
 @pytest.mark.parametrize("stop,t_final,use_pc", [(0.0, 2e-12, True), (1e3, 1e-9, True), (0.0, 1e-12, False)])
-def test_relax_implicit_bdf_vs_oracle(box, stop, t_final, use_pc):
+def test_relax_implicit_bdf_vs_oracle(box, stop, t_final, use_pc, tmp_path):
     import spinfemx_b200 as spx
     from oracle import implicit as oimp
     X, T, od = box
@@ -128,6 +128,7 @@ def test_relax_implicit_bdf_vs_oracle(box, stop, t_final, use_pc):
     ts = []
     m, ctx, _, st = llg.relax(m0, 0.0, t_final, dt0, ts_rtol=tol, ts_atol=tol, stopping_dmdt=stop,
                               check_every_stop=5, return_stats=True, save_final_state=False, use_pc_python=use_pc,
+                              output_dir=str(tmp_path),
                               monitor_fn=lambda step, t, u: ts.append(t))
     assert so["nsteps"] > 50 and so["rejected"] >= 1
     assert st["nsteps"] == so["nsteps"] and st["rejected"] == so["rejected"]
@@ -140,7 +141,7 @@ def test_relax_implicit_bdf_vs_oracle(box, stop, t_final, use_pc):
     assert np.abs(m.cpu().numpy() - mo).max() < 1e-8
 
 
-def test_relax_implicit_time_field_vs_oracle(box):
+def test_relax_implicit_time_field_vs_oracle(box, tmp_path):
     import spinfemx_b200 as spx
     from oracle import implicit as oimp
     X, T, od = box
@@ -152,6 +153,10 @@ def test_relax_implicit_time_field_vs_oracle(box):
     llg.add_exchange(AEX)
     llg.add_demag(**TIGHT)
     llg.add_external_field(H_time_func=lambda t: _pulse(t))
-    m, _, _, st = llg.relax(m0, 0.0, 1e-12, 1e-13, return_stats=True, save_final_state=False)
+    m, _, _, st = llg.relax(m0, 0.0, 1e-12, 1e-13, return_stats=True, save_final_state=True,
+                            output_dir=str(tmp_path))
     assert st["nsteps"] == so["nsteps"] and st["rejected"] == so["rejected"]
     assert np.abs(m.cpu().numpy() - mo).max() < 1e-8
+    # restart from the checkpoint: the state read back is the final state bit for bit
+    from spinfemx_b200 import io as sio
+    assert np.array_equal(sio.read_function(tmp_path / "Relax.bp", time=0.0, name="m"), m.cpu().numpy())

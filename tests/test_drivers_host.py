@@ -29,7 +29,7 @@ class OracleStepper:
         return self.m
 
 
-def test_relax_explicit_host_loop_matches_oracle():
+def test_relax_explicit_host_loop_matches_oracle(tmp_path):
     import sys
     from pathlib import Path
     sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "fenicsx-micromagnetics_b200"))
@@ -45,7 +45,7 @@ def test_relax_explicit_host_loop_matches_oracle():
     llg.hef = OracleStepper(ohef.llg_rhs, m0)
     ts = []
     m, _, st = llg.relax_explicit(None, 0.0, 1e-11, 1e-12, ts_rtol=1e-6, ts_atol=1e-6, return_stats=True,
-                                  monitor_fn=lambda step, t, u: ts.append(t))
+                                  output_dir=str(tmp_path), monitor_fn=lambda step, t, u: ts.append(t))
     assert so["rejected"] > 0 and st["rejected"] == so["rejected"]
     assert st["nsteps"] == so["nsteps"] and st["reason"] == so["reason"] == 1
     assert np.allclose(np.diff([0.0] + ts), so["dts"], rtol=1e-12, atol=0.0)
@@ -77,7 +77,7 @@ class OracleBDF:
         return self.b.m
 
 
-def test_relax_implicit_host_loop_matches_oracle():
+def test_relax_implicit_host_loop_matches_oracle(tmp_path):
     """LLG_GPU.relax's step-size loop (TSAdapt basic with the implicit options, failed-solve
     scaling, reject limit) with its device calls answered by the oracle's BDF attempts retraces
     oracle.implicit.relax_implicit step for step."""
@@ -97,8 +97,16 @@ def test_relax_implicit_host_loop_matches_oracle():
     llg.hef = OracleBDF(ohef, m0)
     ts = []
     m, ctx, _, st = llg.relax(None, 0.0, 1e-12, 1e-13, ts_rtol=1e-6, ts_atol=1e-6, return_stats=True,
-                              save_final_state=False, monitor_fn=lambda step, t, u: ts.append(t))
+                              save_final_state=True, output_dir=str(tmp_path),
+                              monitor_fn=lambda step, t, u: ts.append(t))
     assert so["rejected"] > 0 and st["rejected"] == so["rejected"]
     assert st["nsteps"] == so["nsteps"] and st["reason"] == so["reason"] == 1
     assert np.allclose(np.diff([0.0] + ts), so["dts"], rtol=1e-12, atol=0.0)
     assert np.array_equal(m, mo)
+    # the restart checkpoint and the XDMF of the final state
+    from spinfemx_b200 import io as sio
+    Xr, Tr = sio.read_mesh(tmp_path / "Relax.bp")
+    assert np.array_equal(Xr, X) and np.array_equal(Tr, T)
+    assert np.array_equal(sio.read_function(tmp_path / "Relax.bp", time=0.0, name="m"), m)
+    (t_last, mx), = sio.read_xdmf_series(tmp_path / "Relax.xdmf", "m")
+    assert t_last == st["t_end"] and np.array_equal(mx.ravel(), m)

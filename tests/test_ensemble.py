@@ -141,7 +141,7 @@ def test_graph_replayed_steps_equal_ordinary_steps(spx, precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,R", [("f64", 2), ("mixed", 4)])
+@pytest.mark.parametrize("precision,R", [("f64", 2), ("mixed", 4), ("mixed", 8)])
 def test_batch_of_one_mesh_shares_the_u1_hierarchy(spx, precision, R):
     """R films of one mesh: the u1 system is one block repeated on the diagonal, solved with the
     block's matrix and AMG hierarchy stored once; every film's field equals the film run alone."""
