@@ -98,3 +98,33 @@ def test_chain_mesh_demag_and_llg_vs_oracle():
     hef.set_state(torch.as_tensor(m, device="cuda"))
     hef.step(1e-14, 5)
     assert np.abs(hef.get_state().cpu().numpy() - mo).max() < 1e-9
+
+
+def test_checkpoint_round_trip(tmp_path):
+    """write_mesh / write_function / read_mesh / read_function (the adios4dolfinx calls of the
+    reference's save and restart) round-trip the mesh and several states exactly; a missing
+    time or name raises KeyError; values of the wrong length are refused."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "fenicsx-micromagnetics_b200"))
+    from spinfemx_b200 import io as sio
+    from oracle import mesh as omesh
+    X, T = omesh.kuhn_box(3, 2, 2, 2.0)
+    rng = np.random.default_rng(0)
+    f = tmp_path / "Relax.bp"
+    sio.write_mesh(f, X, T)
+    m0, m1 = rng.normal(size=3 * X.shape[0]), rng.normal(size=3 * X.shape[0])
+    sio.write_function(f, m0, time=0.0, name="m")
+    sio.write_function(f, m1, time=1e-12, name="m")
+    sio.write_function(f, m1 * 2, time=0.0, name="H")
+    Xr, Tr = sio.read_mesh(f)
+    assert np.array_equal(Xr, X) and np.array_equal(Tr, T)
+    assert np.array_equal(sio.read_function(f, 0.0, "m"), m0)
+    assert np.array_equal(sio.read_function(f, 1e-12, "m"), m1)
+    assert np.array_equal(sio.read_function(f, 0.0, "H"), m1 * 2)
+    sio.write_function(f, m1, time=0.0, name="m")          # replaces the entry at t = 0
+    assert np.array_equal(sio.read_function(f, 0.0, "m"), m1)
+    with pytest.raises(KeyError):
+        sio.read_function(f, 2e-12, "m")
+    with pytest.raises(ValueError):
+        sio.write_function(f, m0[:-3], time=3.0)
