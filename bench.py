@@ -594,7 +594,8 @@ def run_film_batch(a):
         # the same film alone (same precision, H-matrix settings and solver tolerances), timed
         # over the same number of steps: the batched form's gain over one film at a time
         hef1 = spx.EffectiveField(X, T, 8e5, Aex=1.3e-11, alpha=0.02, H0_static=H0, use_demag=True,
-                                  precision=a.precision, demag_kwargs=dict(dk, precision=a.precision))
+                                  precision=a.precision,
+                                  demag_kwargs=dict(dk, precision=a.precision, boundary_backend="hmatrix"))
         hef1.set_state(torch.as_tensor(m0s[0], device="cuda"))
         hef1.step(a.dt, a.warmup)
         torch.cuda.synchronize()

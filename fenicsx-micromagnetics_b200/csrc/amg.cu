@@ -194,7 +194,11 @@ namespace {
 #ifndef SPX_PCG_BLOCK
 #define SPX_PCG_BLOCK 1024
 #endif
-constexpr int PCG_BLOCK = SPX_PCG_BLOCK;  // one CTA per SM (threads per CTA)
+#ifndef SPX_PCG_CTAS_PER_SM
+#define SPX_PCG_CTAS_PER_SM 1
+#endif
+constexpr int PCG_BLOCK = SPX_PCG_BLOCK;          // threads per CTA
+constexpr int PCG_CTAS_PER_SM = SPX_PCG_CTAS_PER_SM;  // resident CTAs per SM (all SMs filled)
 
 struct RowRange {
   int64_t gw, nw;  // first warp, warp stride
@@ -771,7 +775,7 @@ __device__ bool vcycle(const PcgParams<TV>& P, int slot, double* sh, unsigned lo
 }
 
 template <class TV>
-__global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg(PcgParams<TV> P) {
+__global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParams<TV> P) {
   unsigned long long tm = 0ull;
   __shared__ double sh[160];
   const unsigned nb = gridDim.x;
@@ -990,7 +994,7 @@ __device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
 // y, bh are indexed in block order (r n + i), the work vectors r, p, q and the level vectors
 // interleaved (i R + r).
 template <class TV, int R>
-__global__ void __launch_bounds__(PCG_BLOCK, 1) k_pcg_amg_r(PcgParams<TV> P) {
+__global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgParams<TV> P) {
   __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
@@ -1290,17 +1294,17 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
   SPX_CHECK(reps == 1 || reps == 2 || reps == 4 || reps == 8, "repeated blocks: 1, 2, 4 or 8");
   int per_sm = 0;
   SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_amg<double>, PCG_BLOCK, 0));
-  SPX_CHECK(per_sm > 0, "AMG PCG kernel cannot be resident");
+  SPX_CHECK(per_sm >= PCG_CTAS_PER_SM, "AMG PCG kernel cannot be resident");
   if (reps > 1) {
     const void* kr = reps == 2 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 2>)
                      : reps == 4 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 4>)
                                  : reinterpret_cast<const void*>(k_pcg_amg_r<double, 8>);
     SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK, 0));
-    SPX_CHECK(per_sm > 0, "AMG PCG kernel (repeated blocks) cannot be resident");
+    SPX_CHECK(per_sm >= PCG_CTAS_PER_SM, "AMG PCG kernel (repeated blocks) cannot be resident");
   }
   int dev;
   SPX_CUDA(cudaGetDevice(&dev));
-  amg_grid = num_sms(dev);
+  amg_grid = num_sms(dev) * PCG_CTAS_PER_SM;
   if (part.n < 4 * 4 * static_cast<size_t>(amg_grid)) part.alloc(4 * 4 * static_cast<size_t>(amg_grid));
   SPX_CUDA(cudaStreamSynchronize(s));
 }
