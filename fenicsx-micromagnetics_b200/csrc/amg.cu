@@ -197,7 +197,12 @@ namespace {
 #ifndef SPX_PCG_CTAS_PER_SM
 #define SPX_PCG_CTAS_PER_SM 1
 #endif
+#ifndef SPX_PCG_BLOCK_R
+#define SPX_PCG_BLOCK_R 512
+#endif
 constexpr int PCG_BLOCK = SPX_PCG_BLOCK;          // threads per CTA
+// the R-block kernels keep R values per row in registers: fewer threads, more registers each
+constexpr int PCG_BLOCK_R = SPX_PCG_BLOCK_R;
 constexpr int PCG_CTAS_PER_SM = SPX_PCG_CTAS_PER_SM;  // resident CTAs per SM (all SMs filled)
 
 struct RowRange {
@@ -235,24 +240,37 @@ __device__ __forceinline__ double ld_hint(const double* a, uint64_t pol) {
   return v;
 }
 
-// row dot products of one SELL-32 slice (values and columns are read-only for the kernel's
-// lifetime; loaded with the L2 policy `pol`)
-__device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
-                                          const float* __restrict__ val, int64_t sl, int lane,
-                                          const float* __restrict__ v, uint64_t pol) {
-  const int64_t base = sp[sl];
-  const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
+// Slice bounds of SELL-32 slice sl (zero width past the last slice).  The phases load the
+// bounds of a warp's next slice while they work on the current one.
+__device__ __forceinline__ void slice_bounds(const int64_t* __restrict__ sp, int64_t sl, int64_t ns, int64_t& base,
+                                             int& width) {
+  if (sl < ns) {
+    base = sp[sl];
+    width = static_cast<int>((sp[sl + 1] - base) >> 5);
+  } else {
+    base = 0;
+    width = 0;
+  }
+}
+
+// row dot products of one SELL-32 slice at `base` of `width` columns (values and columns are
+// read-only for the kernel's lifetime; loaded with the L2 policy `pol`).  Columns go in rounds
+// of eight gathers per thread; the last round is predicated, so a slice costs ceil(width / 8)
+// dependent load rounds.
+__device__ __forceinline__ float sell_dot_bw(const int32_t* __restrict__ col, const float* __restrict__ val,
+                                             int64_t base, int width, int lane, const float* __restrict__ v,
+                                             uint64_t pol) {
   const float* vv = val + base + lane;
   const int32_t* cc = col + base + lane;
   float a0 = 0.0f, a1 = 0.0f;
-  int k = 0;
-  for (; k + 8 <= width; k += 8) {  // eight gathers in flight per thread
+  for (int k = 0; k < width; k += 8) {
     float w[8];
     int32_t c[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      w[u] = ld_hint(vv + (k + u) * 32, pol);
-      c[u] = ld_hint(cc + (k + u) * 32, pol);
+      const bool in = k + u < width;
+      w[u] = in ? ld_hint(vv + (k + u) * 32, pol) : 0.0f;
+      c[u] = in ? ld_hint(cc + (k + u) * 32, pol) : 0;
     }
 #pragma unroll
     for (int u = 0; u < 8; u += 2) {
@@ -260,43 +278,49 @@ __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const 
       a1 += w[u + 1] * v[c[u + 1]];
     }
   }
-  for (; k + 2 <= width; k += 2) {
-    const float w0 = ld_hint(vv + k * 32, pol), w1 = ld_hint(vv + (k + 1) * 32, pol);
-    const int32_t c0 = ld_hint(cc + k * 32, pol), c1 = ld_hint(cc + (k + 1) * 32, pol);
-    a0 += w0 * v[c0];
-    a1 += w1 * v[c1];
-  }
-  if (k < width) a0 += ld_hint(vv + k * 32, pol) * v[ld_hint(cc + k * 32, pol)];
   return a0 + a1;
 }
+
 
 // pre-smoothing from x = 0, Chebyshev steps 1 and 2 (one SpMV: A d0, d0 = D^-1 b / theta)
 __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
+  int64_t b, nbs;
+  int w, nwd;
+  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep());
-    if (i < L.n) {
-      const float di = L.dinv[i];
-      const float d0 = L.db[i] / L.theta;
-      const float r1 = L.db[i] - di * t / L.theta;
+    const bool live = i < L.n;
+    const float di = live ? L.dinv[i] : 0.0f, dbi = live ? L.db[i] : 0.0f;
+    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.db, l2_policy_keep());
+    if (live) {
+      const float d0 = dbi / L.theta;
+      const float r1 = dbi - di * t / L.theta;
       const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
       L.x[i] = d0 + d1;
       L.d[i] = d1;
       L.r[i] = r1;
     }
+    b = nbs;
+    w = nwd;
   }
 }
 
 // residual b - A x after pre-smoothing (A d1), stored in r
 __device__ void pre_b(const AmgLevelDev& L, RowRange rr) {
+  int64_t b, nbs;
+  int w, nwd;
+  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
-    if (i < L.n) {
-      const float di = L.dinv[i];
-      L.r[i] = (L.r[i] - di * t) / di;
-    }
+    const bool live = i < L.n;
+    const float di = live ? L.dinv[i] : 1.0f, ri = live ? L.r[i] : 0.0f;
+    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.d, l2_policy_keep());
+    if (live) L.r[i] = (ri - di * t) / di;
+    b = nbs;
+    w = nwd;
   }
 }
 
@@ -329,25 +353,41 @@ __device__ void restrict_to(const AmgLevelDev& L, const AmgLevelDev& C, RowRange
 }
 
 __device__ void prolong_from(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
+  int64_t b, nbs;
+  int w, nwd;
+  slice_bounds(L.p_sp, rr.gw, L.p_nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.p_nslices; sl += rr.nw) {
+    slice_bounds(L.p_sp, sl + rr.nw, L.p_nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, l2_policy_stream());
-    if (i < L.n) L.x[i] += t;
+    const bool live = i < L.n;
+    const float xi = live ? L.x[i] : 0.0f;
+    const float t = sell_dot_bw(L.p_col, L.p_val, b, w, rr.lane, C.x, l2_policy_stream());
+    if (live) L.x[i] = xi + t;
+    b = nbs;
+    w = nwd;
   }
 }
 
 // post-smoothing from x, Chebyshev step 1 (r0 = D^-1 (b - A x), x2 = x + r0 / theta)
 __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
+  int64_t b, nbs;
+  int w, nwd;
+  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep());
-    if (i < L.n) {
-      const float r0 = L.db[i] - L.dinv[i] * t;
+    const bool live = i < L.n;
+    const float dbi = live ? L.db[i] : 0.0f, di = live ? L.dinv[i] : 0.0f, xi = live ? L.x[i] : 0.0f;
+    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.x, l2_policy_keep());
+    if (live) {
+      const float r0 = dbi - di * t;
       const float d0 = r0 / L.theta;
-      L.x2[i] = L.x[i] + d0;
+      L.x2[i] = xi + d0;
       L.d[i] = d0;
       L.r[i] = r0;
     }
+    b = nbs;
+    w = nwd;
   }
 }
 
@@ -355,20 +395,30 @@ __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
 __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
                        const double* __restrict__ sdinv, double& rz, double& wz, bool top) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
+  int64_t b, nbs;
+  int w, nwd;
+  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
+    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
-    if (i < L.n) {
-      const float r1 = L.r[i] - L.dinv[i] * t;
-      const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;
-      const float z = L.x2[i] + d1;
+    const bool live = i < L.n;
+    const float ri = live ? L.r[i] : 0.0f, di = live ? L.dinv[i] : 0.0f, dd = live ? L.d[i] : 0.0f,
+                x2 = live ? L.x2[i] : 0.0f;
+    const double sd = (live && top) ? sdinv[i] : 1.0, r6 = (live && top) ? r64[i] : 0.0;
+    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.d, l2_policy_keep());
+    if (live) {
+      const float r1 = ri - di * t;
+      const float d1 = rho1 * rho0 * dd + (2.0f * rho1 / L.delta) * r1;
+      const float z = x2 + d1;
       L.x[i] = z;
       if (top) {  // level 0 runs unscaled: z is u = D^-1/2 z^, z^ = u / sdinv
-        const double zh = static_cast<double>(z) / sdinv[i];
-        rz += r64[i] * zh;
-        wz += zh / sdinv[i];
+        const double zh = static_cast<double>(z) / sd;
+        rz += r6 * zh;
+        wz += zh / sd;
       }
     }
+    b = nbs;
+    w = nwd;
   }
 }
 
@@ -444,14 +494,14 @@ __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const
   const int32_t* cc = col + base + lane;
 #pragma unroll
   for (int r = 0; r < R; ++r) t[r] = 0.0f;
-  int k = 0;
-  for (; k + KB <= width; k += KB) {
+  for (int k = 0; k < width; k += KB) {  // the last round predicated
     float w[KB];
     int32_t c[KB];
 #pragma unroll
     for (int u = 0; u < KB; ++u) {
-      w[u] = ld_hint(vv + (k + u) * 32, pol);
-      c[u] = ld_hint(cc + (k + u) * 32, pol);
+      const bool in = k + u < width;
+      w[u] = in ? ld_hint(vv + (k + u) * 32, pol) : 0.0f;
+      c[u] = in ? ld_hint(cc + (k + u) * 32, pol) : 0;
     }
     float g[KB][R];
 #pragma unroll
@@ -460,14 +510,6 @@ __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const
     for (int u = 0; u < KB; ++u)
 #pragma unroll
       for (int r = 0; r < R; ++r) t[r] += w[u] * g[u][r];
-  }
-  for (; k < width; ++k) {
-    const float w = ld_hint(vv + k * 32, pol);
-    const int32_t c = ld_hint(cc + k * 32, pol);
-    float g[R];
-    load_r<R>(v, c, g);
-#pragma unroll
-    for (int r = 0; r < R; ++r) t[r] += w * g[r];
   }
 }
 
@@ -710,6 +752,22 @@ struct PcgParams {
 #define PCG_ROWS_END \
   }                  \
   }
+// SpMV phases: the bounds of the warp's next slice are loaded while it works on this one
+#define PCG_SLICES_BEGIN                                     \
+  {                                                          \
+    int64_t base, nbase_;                                    \
+    int width, nwidth_;                                      \
+    slice_bounds(P.sp, gw, P.nslices, base, width);          \
+    for (int64_t sl = gw; sl < P.nslices; sl += nw) {        \
+      slice_bounds(P.sp, sl + nw, P.nslices, nbase_, nwidth_); \
+      const int64_t row = sl * 32 + lane;                    \
+      if (row < n) {
+#define PCG_SLICES_END \
+  }                    \
+  base = nbase_;       \
+  width = nwidth_;     \
+  }                    \
+  }
 
 // Phase timing (switched on by spx_debug_pcg_timing): CTA 0 adds the globaltimer interval
 // since its previous mark to the slot of the phase that just ended (the phase's slowest CTA
@@ -830,26 +888,32 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
     // true residual r = bh - A^ y (FP64), its unscaled norm, r -> level-0 right-hand side
     {
       double rh = 0.0;
-      PCG_ROWS_BEGIN
+      PCG_SLICES_BEGIN
         double acc = 0.0, acc2 = 0.0;
         const uint64_t pst = l2_policy_stream(), pkeep = l2_policy_keep();
-        int k = 0;
-        for (; k + 2 <= width; k += 2) {
-          const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
-          acc2 += ld_hint(P.v64 + idx + 32, pst) * P.y[ld_hint(P.col + idx + 32, pkeep)];
+        const double bhi = P.bh[row], sdi = P.sdinv[row], dgi = P.diag[row];
+        const float di0 = dinv0[row];
+        for (int k = 0; k < width; k += 4) {  // rounds of four columns, the last predicated
+          double v[4], g[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int64_t idx = base + ((int64_t)(k + u) << 5) + lane;
+            const bool in = k + u < width;
+            v[u] = in ? ld_hint(P.v64 + idx, pst) : 0.0;
+            g[u] = in ? P.y[ld_hint(P.col + idx, pkeep)] : 0.0;
+          }
+          acc += v[0] * g[0];
+          acc2 += v[1] * g[1];
+          acc += v[2] * g[2];
+          acc2 += v[3] * g[3];
         }
-        if (k < width) {
-          const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
-        }
-        const double r = P.bh[row] - (acc + acc2);
+        const double r = bhi - (acc + acc2);
         P.r[row] = r;
-        const float rf = static_cast<float>(r / P.sdinv[row]);
+        const float rf = static_cast<float>(r / sdi);
         b0[row] = rf;
-        db0[row] = dinv0[row] * rf;
-        rh += P.diag[row] * r * r;
-      PCG_ROWS_END
+        db0[row] = di0 * rf;
+        rh += dgi * r * r;
+      PCG_SLICES_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
       pcg_mark(tm, 30, P.timing);
@@ -867,9 +931,11 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
       const double beta = it == 0 ? 0.0 : rz / rz_old;
       const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ from the unscaled level-0 cycle
       double pq = 0.0;
-      PCG_ROWS_BEGIN
+      PCG_SLICES_BEGIN
         const double ui = static_cast<double>(u0[row]);
         const uint64_t pkeep = l2_policy_keep();
+        const double rsi = P.rsum[row], sdi = P.sdinv[row];
+        const double pold = it == 0 ? 0.0 : P.p[row], qold = it == 0 ? 0.0 : P.q[row];
         double acc = 0.0, acc2 = 0.0;
         int k = 0;
         for (; k + 4 <= width; k += 4) {
@@ -883,20 +949,29 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
           acc += static_cast<double>(w2) * (static_cast<double>(u0[c2]) - ui);
           acc2 += static_cast<double>(w3) * (static_cast<double>(u0[c3]) - ui);
         }
-        for (; k < width; ++k) {
-          const int64_t idx = base + ((int64_t)k << 5) + lane;
-          acc += static_cast<double>(ld_hint(P.a32 + idx, pkeep)) *
-                 (static_cast<double>(u0[ld_hint(P.col + idx, pkeep)]) - ui);
+        if (k < width) {  // up to three remaining columns, loaded together, summed in order
+          float wt[3];
+          int32_t ct[3];
+#pragma unroll
+          for (int u = 0; u < 3; ++u) {
+            const int64_t idx = base + ((int64_t)(k + u) << 5) + lane;
+            const bool in = k + u < width;
+            wt[u] = in ? ld_hint(P.a32 + idx, pkeep) : 0.0f;
+            ct[u] = in ? ld_hint(P.col + idx, pkeep) : 0;
+          }
+#pragma unroll
+          for (int u = 0; u < 3; ++u)
+            if (k + u < width) acc += static_cast<double>(wt[u]) * (static_cast<double>(u0[ct[u]]) - ui);
         }
-        acc = (acc + acc2 + P.rsum[row] * ui) * P.sdinv[row];
-        const double z = ui / P.sdinv[row];
-        const double w = 1.0 / P.sdinv[row];
-        const double pv = (z - c * w) + (it == 0 ? 0.0 : beta * P.p[row]);
-        const double qv = acc + (it == 0 ? 0.0 : beta * P.q[row]);
+        acc = (acc + acc2 + rsi * ui) * sdi;
+        const double z = ui / sdi;
+        const double w = 1.0 / sdi;
+        const double pv = (z - c * w) + (it == 0 ? 0.0 : beta * pold);
+        const double qv = acc + (it == 0 ? 0.0 : beta * qold);
         P.p[row] = pv;
         P.q[row] = qv;
         pq += pv * qv;
-      PCG_ROWS_END
+      PCG_SLICES_END
       cta_partial(P.part, 3, pq, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
       pcg_mark(tm, 28, P.timing);
@@ -994,7 +1069,7 @@ __device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
 // y, bh are indexed in block order (r n + i), the work vectors r, p, q and the level vectors
 // interleaved (i R + r).
 template <class TV, int R>
-__global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgParams<TV> P) {
+__global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgParams<TV> P) {
   __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
@@ -1058,7 +1133,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgPar
     {
       double rh = 0.0;
       const uint64_t pst = l2_policy_stream(), pkeep = l2_policy_keep();
-      PCG_ROWS_BEGIN
+      PCG_SLICES_BEGIN
         double acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) acc[r] = 0.0;
@@ -1089,7 +1164,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgPar
           db0[j] = di0 * rf;
           rh += dg * rv * rv;
         }
-      PCG_ROWS_END
+      PCG_SLICES_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
     }
@@ -1107,44 +1182,38 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgPar
       const float* u0 = P.lv[0].x;  // u = D^-1/2 z^ of every block (interleaved)
       double pq = 0.0;
       const uint64_t pkeep = l2_policy_keep();
-      PCG_ROWS_BEGIN
+      PCG_SLICES_BEGIN
         float uf[R];
         load_r<R>(u0, row, uf);
+        const double rs = P.rsum[row];
+        const double sd = P.sdinv[row];
         double ui[R], acc[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           ui[r] = static_cast<double>(uf[r]);
           acc[r] = 0.0;
         }
-        int k = 0;
-        for (; k + 4 <= width; k += 4) {
+        for (int k = 0; k < width; k += 4) {  // rounds of four columns, the last predicated
           const int64_t i0 = base + ((int64_t)k << 5) + lane;
           float w[4];
           int32_t cc[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
-            w[u] = ld_hint(P.a32 + i0 + 32 * u, pkeep);
-            cc[u] = ld_hint(P.col + i0 + 32 * u, pkeep);
+            const bool in = k + u < width;
+            w[u] = in ? ld_hint(P.a32 + i0 + 32 * u, pkeep) : 0.0f;
+            cc[u] = in ? ld_hint(P.col + i0 + 32 * u, pkeep) : 0;
           }
           float g[4][R];
 #pragma unroll
           for (int u = 0; u < 4; ++u) load_r<R>(u0, cc[u], g[u]);
 #pragma unroll
           for (int u = 0; u < 4; ++u)
+            if (k + u < width) {
 #pragma unroll
-            for (int r = 0; r < R; ++r)
-              acc[r] += static_cast<double>(w[u]) * (static_cast<double>(g[u][r]) - ui[r]);
+              for (int r = 0; r < R; ++r)
+                acc[r] += static_cast<double>(w[u]) * (static_cast<double>(g[u][r]) - ui[r]);
+            }
         }
-        for (; k < width; ++k) {
-          const int64_t idx = base + ((int64_t)k << 5) + lane;
-          const double w = static_cast<double>(ld_hint(P.a32 + idx, pkeep));
-          float g[R];
-          load_r<R>(u0, ld_hint(P.col + idx, pkeep), g);
-#pragma unroll
-          for (int r = 0; r < R; ++r) acc[r] += w * (static_cast<double>(g[r]) - ui[r]);
-        }
-        const double rs = P.rsum[row];
-        const double sd = P.sdinv[row];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int64_t j = row * R + r;
@@ -1157,7 +1226,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgPar
           P.q[j] = qv;
           pq += pv * qv;
         }
-      PCG_ROWS_END
+      PCG_SLICES_END
       cta_partial(P.part, 3, pq, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
       cta_total(P.part, 3, tot, sh);
@@ -1299,7 +1368,7 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
     const void* kr = reps == 2 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 2>)
                      : reps == 4 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 4>)
                                  : reinterpret_cast<const void*>(k_pcg_amg_r<double, 8>);
-    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK, 0));
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK_R, 0));
     SPX_CHECK(per_sm >= PCG_CTAS_PER_SM, "AMG PCG kernel (repeated blocks) cannot be resident");
   }
   int dev;
@@ -1331,7 +1400,7 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   if (reps == 2) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 2>);
   if (reps == 4) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 4>);
   if (reps == 8) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 8>);
-  SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(PCG_BLOCK), args, 0, st));
+  SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(reps > 1 ? PCG_BLOCK_R : PCG_BLOCK), args, 0, st));
 }
 
 // per-slot sums (ns) and counts of the phase timing marks since the last call
