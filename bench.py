@@ -46,6 +46,15 @@ MU0 = 4e-7 * math.pi
 TRAFFIC_PER_ALGORITHMIC_BYTE = {"boundary_apply": 635.9 / 610.4}
 
 
+def l2_persisting():
+    """(set-aside bytes, device maximum) of the L2 persisting carve-out of this context."""
+    import ctypes as C_
+    from spinfemx_b200 import _lib
+    cur, mx = C_.c_int64(), C_.c_int64()
+    _lib.call("spx_device_l2_persisting", C_.byref(cur), C_.byref(mx))
+    return {"set_aside_bytes": cur.value, "max_bytes": mx.value}
+
+
 def workload(nx, ny, nz, h, seed):
     from spinfemx_b200.geometry import kuhn_box
     X, T = kuhn_box(nx, ny, nz, h)
@@ -366,6 +375,7 @@ def run_ours(a):
                    "nodes": N, "boundary_nodes": dm.Nb, "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (H-matrix factors %.1f GB per apply)" % (
                        (Hmem["far_bytes"] + Hmem["near_bytes"]) / 1e9),
+                   "l2_persisting": l2_persisting(),
                    "cg_start": {0: "zero", 1: "previous", 2: "extrapolated per RK stage",
                                 3: "extrapolated per RK stage, corrected by stage 1"}[a.warm_start],
                    "rtol_u1": a.rtol_u1, "rtol_u2": a.rtol_u2,
@@ -648,6 +658,7 @@ def run_film_batch(a):
                "u2_iters_per_solve": round(dc[1][0] / max(dc[1][2], 1), 1),
                "u2_refinements_per_solve": round(dc[1][1] / max(dc[1][2], 1), 2)},
         "amg_levels": [[lv["rows"], lv["nnz_A"]] for lv in dm.amg_levels()],
+        "l2_persisting": l2_persisting(),
         "setup_s": round(setup_s, 1),
         "gpu_launches": int(sum(int(x) for x in nl_cat[:7])) * a.steps // max(nprof, 1),
         "clocks": clocks,

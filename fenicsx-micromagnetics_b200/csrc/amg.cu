@@ -19,6 +19,7 @@
 // returning; stopping rule ||b - A x|| <= max(rtol ||b||, atol) in the unscaled norm.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "amg.cuh"
@@ -27,6 +28,24 @@
 namespace spx {
 
 std::atomic<int> g_pcg_timing{0};  // phase timing marks of the AMG-PCG kernel (spx_debug_pcg_timing)
+
+// The cycle loads the matrices of its cycled levels with an L2 evict_last policy so that they
+// stay in L2 across phases and PCG iterations while the vectors stream past.  Lines of that
+// priority live in the L2 set-aside for persisting accesses, which is empty unless the context
+// asks for one, so the set-aside is raised (never lowered) to the hinted bytes, capped by the
+// device's maximum.  It is a limit of this process's context, not a GPU setting.
+// SPX_L2_PERSIST_MB overrides the size (0: leave the set-aside as it is).
+void reserve_persisting_l2(int64_t bytes, int dev) {
+  if (const char* e = std::getenv("SPX_L2_PERSIST_MB")) bytes = std::atoll(e) << 20;
+  if (bytes <= 0) return;
+  int mx = 0;
+  SPX_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxPersistingL2CacheSize, dev));
+  if (mx <= 0) return;
+  size_t cur = 0;
+  SPX_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+  const size_t want = std::min<size_t>(static_cast<size_t>(mx), static_cast<size_t>(bytes));
+  if (want > cur) SPX_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+}
 
 namespace {
 
@@ -934,8 +953,6 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
       PCG_SLICES_BEGIN
         const double ui = static_cast<double>(u0[row]);
         const uint64_t pkeep = l2_policy_keep();
-        const double rsi = P.rsum[row], sdi = P.sdinv[row];
-        const double pold = it == 0 ? 0.0 : P.p[row], qold = it == 0 ? 0.0 : P.q[row];
         double acc = 0.0, acc2 = 0.0;
         int k = 0;
         for (; k + 4 <= width; k += 4) {
@@ -963,6 +980,8 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
           for (int u = 0; u < 3; ++u)
             if (k + u < width) acc += static_cast<double>(wt[u]) * (static_cast<double>(u0[ct[u]]) - ui);
         }
+        const double rsi = P.rsum[row], sdi = P.sdinv[row];
+        const double pold = it == 0 ? 0.0 : P.p[row], qold = it == 0 ? 0.0 : P.q[row];
         acc = (acc + acc2 + rsi * ui) * sdi;
         const double z = ui / sdi;
         const double w = 1.0 / sdi;
@@ -1374,6 +1393,11 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
   int dev;
   SPX_CUDA(cudaGetDevice(&dev));
   amg_grid = num_sms(dev) * PCG_CTAS_PER_SM;
+  {
+    int64_t keep = P.len * static_cast<int64_t>(sizeof(float) + sizeof(int32_t));  // level 0 (shared pattern)
+    for (int l = 1; l + 1 < amg->nlev; ++l) keep += amg->A[l].len * static_cast<int64_t>(sizeof(float) + sizeof(int32_t));
+    reserve_persisting_l2(keep + keep / 8, dev);
+  }
   if (part.n < 4 * 4 * static_cast<size_t>(amg_grid)) part.alloc(4 * 4 * static_cast<size_t>(amg_grid));
   SPX_CUDA(cudaStreamSynchronize(s));
 }

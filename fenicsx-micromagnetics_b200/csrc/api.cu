@@ -846,6 +846,19 @@ int spx_debug_barrier_time(int32_t nblocks, int32_t threads, int32_t nbarriers, 
   API_END
 }
 
+int spx_device_l2_persisting(int64_t* current_bytes, int64_t* max_bytes) {
+  API_BEGIN
+  REQUIRE(current_bytes); REQUIRE(max_bytes);
+  int dev = 0, mx = 0;
+  SPX_CUDA(cudaGetDevice(&dev));
+  SPX_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxPersistingL2CacheSize, dev));
+  size_t cur = 0;
+  SPX_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+  *current_bytes = static_cast<int64_t>(cur);
+  *max_bytes = mx;
+  API_END
+}
+
 int spx_debug_pcg_timing(int32_t enable) {
   API_BEGIN
   spx::g_pcg_timing.store(enable != 0 ? 1 : 0);

@@ -95,6 +95,7 @@ SIGNATURES = {
     "spx_debug_barrier_time": (C.c_int, [c_i32, c_i32, c_i32, P_dbl]),
     "spx_debug_pcg_phase_times": (C.c_int, [c_vp, c_vp]),
     "spx_debug_pcg_timing": (C.c_int, [c_i32]),
+    "spx_device_l2_persisting": (C.c_int, [P_i64, P_i64]),
     "spx_llg_set_time_field": (C.c_int, [c_vp, c_vp, c_vp, c_vp]),
     "spx_llg_step_time_field": (C.c_int, [c_vp, c_dbl, c_vp, c_vp, c_vp]),
     "spx_llg_rk_attempt": (C.c_int, [c_vp, c_i32, c_dbl, c_dbl, c_dbl, c_vp, c_vp, c_i32, P_dbl, c_vp]),

@@ -88,6 +88,10 @@ SPX_API int spx_debug_barrier_time(int32_t nblocks, int32_t threads, int32_t nba
  * spx_debug_pcg_phase_times returns the summed times and sample counts and clears them. */
 SPX_API int spx_debug_pcg_timing(int32_t enable);
 SPX_API int spx_debug_pcg_phase_times(double* ns32, int64_t* counts32);
+/* The L2 set-aside for persisting accesses of this process's context (raised by the AMG setup
+ * to hold the cycle's matrices, which it loads with an evict_last policy) and the device's
+ * maximum, in bytes. */
+SPX_API int spx_device_l2_persisting(int64_t* current_bytes, int64_t* max_bytes);
 /* Out-of-memory injection for tests of the recovery paths (no counterpart in the reference,
  * whose builder catches CuPy's OutOfMemoryError, lindholm_hmatrix_gpu/builder.py:597-662):
  * the next `count` device allocations of the library of at least `min_bytes` bytes fail with
