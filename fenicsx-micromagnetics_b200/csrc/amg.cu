@@ -258,6 +258,13 @@ __device__ __forceinline__ double ld_hint(const double* a, uint64_t pol) {
   asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
   return v;
 }
+__device__ __forceinline__ float4 ld_hint4(const float4* a, uint64_t pol) {
+  float4 v;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+      : "l"(a), "l"(pol));
+  return v;
+}
 
 // Slice bounds of SELL-32 slice sl (zero width past the last slice).  The phases load the
 // bounds of a warp's next slice while they work on the current one.
@@ -446,14 +453,16 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
 __device__ void coarse_solve(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, int64_t ldc,
                              RowRange rr) {
   const int64_t nv = ldc / 4;
+  const uint64_t pol = l2_policy_keep();  // the inverse stays in L2 across iterations
+  const float4* b4 = reinterpret_cast<const float4*>(L.b);
   for (int64_t i = rr.gw; i < nc; i += rr.nw) {
     const float4* row = reinterpret_cast<const float4*>(cinv + i * ldc);
     float s = 0.0f;
 #pragma unroll 4
     for (int64_t j = rr.lane; j < nv; j += 32) {
-      const float4 c = row[j];
-      const float* b = L.b + 4 * j;
-      s += c.x * b[0] + c.y * b[1] + c.z * b[2] + c.w * b[3];
+      const float4 c = ld_hint4(row + j, pol);
+      const float4 b = b4[j];
+      s += c.x * b.x + c.y * b.y + c.z * b.z + c.w * b.w;
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (rr.lane == 0) L.x[i] = s;
@@ -1396,6 +1405,7 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
   {
     int64_t keep = P.len * static_cast<int64_t>(sizeof(float) + sizeof(int32_t));  // level 0 (shared pattern)
     for (int l = 1; l + 1 < amg->nlev; ++l) keep += amg->A[l].len * static_cast<int64_t>(sizeof(float) + sizeof(int32_t));
+    keep += amg->cinv.bytes();  // the dense coarsest inverse
     reserve_persisting_l2(keep + keep / 8, dev);
   }
   if (part.n < 4 * 4 * static_cast<size_t>(amg_grid)) part.alloc(4 * 4 * static_cast<size_t>(amg_grid));
