@@ -29,14 +29,15 @@ namespace spx {
 
 std::atomic<int> g_pcg_timing{0};  // phase timing marks of the AMG-PCG kernel (spx_debug_pcg_timing)
 
-// The cycle loads the matrices of its cycled levels with an L2 evict_last policy so that they
-// stay in L2 across phases and PCG iterations while the vectors stream past.  Lines of that
-// priority live in the L2 set-aside for persisting accesses, which is empty unless the context
-// asks for one, so the set-aside is raised (never lowered) to the hinted bytes, capped by the
-// device's maximum.  It is a limit of this process's context, not a GPU setting.
-// SPX_L2_PERSIST_MB overrides the size (0: leave the set-aside as it is).
+// The cycle loads the matrices of its cycled levels with an L2 evict_last policy.  A larger L2
+// set-aside for persisting lines (a limit of this process's context, not a GPU setting) can be
+// requested with SPX_L2_PERSIST_MB (MiB, raised only, capped by the device's maximum).  It is
+// off by default: measured on the 400 x 400 x 2 film, raising it from the context's 24 MB to
+// 75 MB left the u1 solve unchanged and slowed the streaming boundary apply by 7 %.
 void reserve_persisting_l2(int64_t bytes, int dev) {
-  if (const char* e = std::getenv("SPX_L2_PERSIST_MB")) bytes = std::atoll(e) << 20;
+  const char* e = std::getenv("SPX_L2_PERSIST_MB");
+  if (!e) return;
+  bytes = std::atoll(e) << 20;
   if (bytes <= 0) return;
   int mx = 0;
   SPX_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxPersistingL2CacheSize, dev));
@@ -266,8 +267,43 @@ __device__ __forceinline__ float4 ld_hint4(const float4* a, uint64_t pol) {
   return v;
 }
 
-// Slice bounds of SELL-32 slice sl (zero width past the last slice).  The phases load the
-// bounds of a warp's next slice while they work on the current one.
+// row dot products of one SELL-32 slice (values and columns are read-only for the kernel's
+// lifetime; loaded with the L2 policy `pol`)
+__device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
+                                          const float* __restrict__ val, int64_t sl, int lane,
+                                          const float* __restrict__ v, uint64_t pol) {
+  const int64_t base = sp[sl];
+  const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
+  const float* vv = val + base + lane;
+  const int32_t* cc = col + base + lane;
+  float a0 = 0.0f, a1 = 0.0f;
+  int k = 0;
+  for (; k + 8 <= width; k += 8) {  // eight gathers in flight per thread
+    float w[8];
+    int32_t c[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      w[u] = ld_hint(vv + (k + u) * 32, pol);
+      c[u] = ld_hint(cc + (k + u) * 32, pol);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+      a0 += w[u] * v[c[u]];
+      a1 += w[u + 1] * v[c[u + 1]];
+    }
+  }
+  for (; k + 2 <= width; k += 2) {
+    const float w0 = ld_hint(vv + k * 32, pol), w1 = ld_hint(vv + (k + 1) * 32, pol);
+    const int32_t c0 = ld_hint(cc + k * 32, pol), c1 = ld_hint(cc + (k + 1) * 32, pol);
+    a0 += w0 * v[c0];
+    a1 += w1 * v[c1];
+  }
+  if (k < width) a0 += ld_hint(vv + k * 32, pol) * v[ld_hint(cc + k * 32, pol)];
+  return a0 + a1;
+}
+
+// Slice bounds of SELL-32 slice sl (zero width past the last slice); the PCG product phase
+// loads the bounds of a warp's next slice while it works on the current one.
 __device__ __forceinline__ void slice_bounds(const int64_t* __restrict__ sp, int64_t sl, int64_t ns, int64_t& base,
                                              int& width) {
   if (sl < ns) {
@@ -279,74 +315,33 @@ __device__ __forceinline__ void slice_bounds(const int64_t* __restrict__ sp, int
   }
 }
 
-// row dot products of one SELL-32 slice at `base` of `width` columns (values and columns are
-// read-only for the kernel's lifetime; loaded with the L2 policy `pol`).  Columns go in rounds
-// of eight gathers per thread; the last round is predicated, so a slice costs ceil(width / 8)
-// dependent load rounds.
-__device__ __forceinline__ float sell_dot_bw(const int32_t* __restrict__ col, const float* __restrict__ val,
-                                             int64_t base, int width, int lane, const float* __restrict__ v,
-                                             uint64_t pol) {
-  const float* vv = val + base + lane;
-  const int32_t* cc = col + base + lane;
-  float a0 = 0.0f, a1 = 0.0f;
-  for (int k = 0; k < width; k += 8) {
-    float w[8];
-    int32_t c[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const bool in = k + u < width;
-      w[u] = in ? ld_hint(vv + (k + u) * 32, pol) : 0.0f;
-      c[u] = in ? ld_hint(cc + (k + u) * 32, pol) : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u += 2) {
-      a0 += w[u] * v[c[u]];
-      a1 += w[u + 1] * v[c[u + 1]];
-    }
-  }
-  return a0 + a1;
-}
-
-
 // pre-smoothing from x = 0, Chebyshev steps 1 and 2 (one SpMV: A d0, d0 = D^-1 b / theta)
 __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
-  int64_t b, nbs;
-  int w, nwd;
-  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
-    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const bool live = i < L.n;
-    const float di = live ? L.dinv[i] : 0.0f, dbi = live ? L.db[i] : 0.0f;
-    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.db, l2_policy_keep());
-    if (live) {
-      const float d0 = dbi / L.theta;
-      const float r1 = dbi - di * t / L.theta;
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep());
+    if (i < L.n) {
+      const float di = L.dinv[i];
+      const float d0 = L.db[i] / L.theta;
+      const float r1 = L.db[i] - di * t / L.theta;
       const float d1 = rho1 * rho0 * d0 + (2.0f * rho1 / L.delta) * r1;
       L.x[i] = d0 + d1;
       L.d[i] = d1;
       L.r[i] = r1;
     }
-    b = nbs;
-    w = nwd;
   }
 }
 
 // residual b - A x after pre-smoothing (A d1), stored in r
 __device__ void pre_b(const AmgLevelDev& L, RowRange rr) {
-  int64_t b, nbs;
-  int w, nwd;
-  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
-    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const bool live = i < L.n;
-    const float di = live ? L.dinv[i] : 1.0f, ri = live ? L.r[i] : 0.0f;
-    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.d, l2_policy_keep());
-    if (live) L.r[i] = (ri - di * t) / di;
-    b = nbs;
-    w = nwd;
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
+    if (i < L.n) {
+      const float di = L.dinv[i];
+      L.r[i] = (L.r[i] - di * t) / di;
+    }
   }
 }
 
@@ -379,41 +374,25 @@ __device__ void restrict_to(const AmgLevelDev& L, const AmgLevelDev& C, RowRange
 }
 
 __device__ void prolong_from(const AmgLevelDev& L, const AmgLevelDev& C, RowRange rr) {
-  int64_t b, nbs;
-  int w, nwd;
-  slice_bounds(L.p_sp, rr.gw, L.p_nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.p_nslices; sl += rr.nw) {
-    slice_bounds(L.p_sp, sl + rr.nw, L.p_nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const bool live = i < L.n;
-    const float xi = live ? L.x[i] : 0.0f;
-    const float t = sell_dot_bw(L.p_col, L.p_val, b, w, rr.lane, C.x, l2_policy_stream());
-    if (live) L.x[i] = xi + t;
-    b = nbs;
-    w = nwd;
+    const float t = sell_dot(L.p_sp, L.p_col, L.p_val, sl, rr.lane, C.x, l2_policy_stream());
+    if (i < L.n) L.x[i] += t;
   }
 }
 
 // post-smoothing from x, Chebyshev step 1 (r0 = D^-1 (b - A x), x2 = x + r0 / theta)
 __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
-  int64_t b, nbs;
-  int w, nwd;
-  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
-    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const bool live = i < L.n;
-    const float dbi = live ? L.db[i] : 0.0f, di = live ? L.dinv[i] : 0.0f, xi = live ? L.x[i] : 0.0f;
-    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.x, l2_policy_keep());
-    if (live) {
-      const float r0 = dbi - di * t;
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep());
+    if (i < L.n) {
+      const float r0 = L.db[i] - L.dinv[i] * t;
       const float d0 = r0 / L.theta;
-      L.x2[i] = xi + d0;
+      L.x2[i] = L.x[i] + d0;
       L.d[i] = d0;
       L.r[i] = r0;
     }
-    b = nbs;
-    w = nwd;
   }
 }
 
@@ -421,30 +400,20 @@ __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
 __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restrict__ r64,
                        const double* __restrict__ sdinv, double& rz, double& wz, bool top) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
-  int64_t b, nbs;
-  int w, nwd;
-  slice_bounds(L.sp, rr.gw, L.nslices, b, w);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
-    slice_bounds(L.sp, sl + rr.nw, L.nslices, nbs, nwd);
     const int64_t i = sl * 32 + rr.lane;
-    const bool live = i < L.n;
-    const float ri = live ? L.r[i] : 0.0f, di = live ? L.dinv[i] : 0.0f, dd = live ? L.d[i] : 0.0f,
-                x2 = live ? L.x2[i] : 0.0f;
-    const double sd = (live && top) ? sdinv[i] : 1.0, r6 = (live && top) ? r64[i] : 0.0;
-    const float t = sell_dot_bw(L.col, L.val, b, w, rr.lane, L.d, l2_policy_keep());
-    if (live) {
-      const float r1 = ri - di * t;
-      const float d1 = rho1 * rho0 * dd + (2.0f * rho1 / L.delta) * r1;
-      const float z = x2 + d1;
+    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
+    if (i < L.n) {
+      const float r1 = L.r[i] - L.dinv[i] * t;
+      const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;
+      const float z = L.x2[i] + d1;
       L.x[i] = z;
       if (top) {  // level 0 runs unscaled: z is u = D^-1/2 z^, z^ = u / sdinv
-        const double zh = static_cast<double>(z) / sd;
-        rz += r6 * zh;
-        wz += zh / sd;
+        const double zh = static_cast<double>(z) / sdinv[i];
+        rz += r64[i] * zh;
+        wz += zh / sdinv[i];
       }
     }
-    b = nbs;
-    w = nwd;
   }
 }
 
@@ -916,32 +885,26 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
     // true residual r = bh - A^ y (FP64), its unscaled norm, r -> level-0 right-hand side
     {
       double rh = 0.0;
-      PCG_SLICES_BEGIN
+      PCG_ROWS_BEGIN
         double acc = 0.0, acc2 = 0.0;
         const uint64_t pst = l2_policy_stream(), pkeep = l2_policy_keep();
-        const double bhi = P.bh[row], sdi = P.sdinv[row], dgi = P.diag[row];
-        const float di0 = dinv0[row];
-        for (int k = 0; k < width; k += 4) {  // rounds of four columns, the last predicated
-          double v[4], g[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int64_t idx = base + ((int64_t)(k + u) << 5) + lane;
-            const bool in = k + u < width;
-            v[u] = in ? ld_hint(P.v64 + idx, pst) : 0.0;
-            g[u] = in ? P.y[ld_hint(P.col + idx, pkeep)] : 0.0;
-          }
-          acc += v[0] * g[0];
-          acc2 += v[1] * g[1];
-          acc += v[2] * g[2];
-          acc2 += v[3] * g[3];
+        int k = 0;
+        for (; k + 2 <= width; k += 2) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
+          acc2 += ld_hint(P.v64 + idx + 32, pst) * P.y[ld_hint(P.col + idx + 32, pkeep)];
         }
-        const double r = bhi - (acc + acc2);
+        if (k < width) {
+          const int64_t idx = base + ((int64_t)k << 5) + lane;
+          acc += ld_hint(P.v64 + idx, pst) * P.y[ld_hint(P.col + idx, pkeep)];
+        }
+        const double r = P.bh[row] - (acc + acc2);
         P.r[row] = r;
-        const float rf = static_cast<float>(r / sdi);
+        const float rf = static_cast<float>(r / P.sdinv[row]);
         b0[row] = rf;
-        db0[row] = di0 * rf;
-        rh += dgi * r * r;
-      PCG_SLICES_END
+        db0[row] = dinv0[row] * rf;
+        rh += P.diag[row] * r * r;
+      PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
       pcg_mark(tm, 30, P.timing);

@@ -32,6 +32,7 @@
 // GPU's own memory.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "hmat.cuh"
@@ -388,7 +389,11 @@ Csr make_csr(int64_t nrows, const std::vector<std::pair<int64_t, int32_t>>& pair
 
 void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   using namespace tc;
-  const int KSTEP_MAX = kstep_max > 0 ? kstep_max : KSTEP_MAX_DEFAULT;
+  // K-steps of 8 per tile (FP32 accumulation in tensor memory runs over at most 8 x this many
+  // products; the tiles' partials are summed in FP64).  SPX_TC_KSTEP sets it for tuning.
+  int KSTEP_MAX = kstep_max > 0 ? kstep_max : KSTEP_MAX_DEFAULT;
+  if (kstep_max <= 0)
+    if (const char* e = std::getenv("SPX_TC_KSTEP")) KSTEP_MAX = std::max(1, std::atoi(e));
   SPX_CHECK(H.far_pool64.n > 0 || H.stats.n_far == 0, "the tensor-core apply needs the FP64 factors");
   auto P = std::make_shared<TcPlan>();
   std::vector<int> far;
