@@ -930,7 +930,7 @@ int spx_hmat_tensor_cores(spx_hmat hm, int32_t enable, int64_t* plan_bytes) {
       H.tc.reset();
       float best = H.prec == Prec::SPLIT ? 1e30f : time_multi8(H);
       int best_k = 0;
-      for (int ks : {64, 256}) {
+      for (int ks : {16, 64}) {  // stages of 32 K elements
         tc_build(H, 0, ks);
         const float t = time_multi8(H);
         SPX_CHECK(tc_error(H, 0) == 0, "tensor-core apply timed out during autotuning");

@@ -1,4 +1,5 @@
-// Far-field products of the multi-state H-matrix apply on the 5th-generation tensor cores.
+// Far-field products of the multi-state H-matrix apply on the 5th-generation tensor cores,
+// with exact integer products (the Ozaki scheme on tcgen05 kind::i8).
 //
 // For R = 8 states of one boundary, the far field of Y = H X is two block-sparse GEMMs:
 //   phase 1 (column clusters): for every column cluster tau, the V factors of all far blocks
@@ -6,25 +7,36 @@
 //     the z vectors of those blocks;
 //   phase 2 (row clusters): for every row cluster sigma, [U_b1 U_b2 ...] (M = |sigma|, K = sum of
 //     the blocks' ranks) times the stacked z (N = 8): their share of Y[sigma].
-// Both run through one kernel, k_tc_gemm, over a list of tiles of 128 rows: A (the factor
-// rows of the tile) is packed once in the canonical K-major no-swizzle shared-memory layout of
-// tcgen05 (8 x 16-byte core matrices; per K-step of 8 elements 4 KB), so each stage of 4
-// K-steps is one 16 KB cp.async.bulk copy; B (X~ or z for the tile's K range) is gathered by
-// CUDA cores.  The products use kind::tf32 with a three-term split (A_hi B_hi + A_hi B_lo +
-// A_lo B_hi, hi = the TF32 truncation, lo = the FP32 remainder): about 22 bits of A and B,
-// close to the FP32 factors' own precision.  Accumulation is FP32 in tensor memory over at most
-// 2048 K elements per tile; the tiles' FP32 partials are summed in FP64 (k_tc_reduce) into z
-// (phase 1, per z entry over its column chunks) and into the far part of Y (phase 2, per row
-// over the row clusters that contain it).  The near field, the diagonal and the scatter stay
-// on k_rows_multi (hmat_multi.cu), which adds this far part.
+// Both run through one kernel, k_tc_gemm, over a list of tiles of 128 rows and at most 2048 K
+// elements.
 //
-// Warp roles of k_tc_gemm (384 threads, one CTA per SM, persistent over a tile list):
-//   warp 0   : cp.async.bulk of A stages into a 4-stage ring (mbarrier transaction counts);
-//   warp 1   : one thread issues tcgen05.mma (3 per K-step) and tcgen05.commit;
-//   warp 2   : allocates / frees 32 tensor-memory columns (two 128 x 16 FP32 accumulators, of
-//              which the first 8 columns are the states; B's rows 8-15 are zero);
-//   warps 4-7: epilogue, tcgen05.ld of the accumulator (lanes 32 (w % 4) .. + 31) to partials;
-//   warps 8-11: split A into hi / lo in place, gather and split B, fence.proxy.async.
+// Arithmetic.  The thin film's double-layer potential is a small difference of large surface
+// contributions, so the far field needs FP64-class products: TF32 operands with FP32 tile sums
+// are 100x too coarse for a 1e-5 demag error.  Instead every operand is written as six signed
+// 7-bit slices of a 42-bit fixed-point value: an A element a = 2^e_r sum_t d_t 2^-7t with e_r
+// the exponent of its tile row's largest element, a B element b = 2^f_n sum_u c_u 2^-7u with
+// f_n the exponent of the largest element of its state over the B rows of the cluster (or row
+// group).  sum_k a_k b_k = 2^(e_r + f_n) sum_g 2^-7g A_g, where A_g = sum_{t+u=g} sum_k d_t c_u
+// is an exact int32 sum (|d c| <= 127^2, at most six slice pairs per g, K <= 2048).  The 21
+// slice pairs with t + u <= 7 go to six int32 accumulators in tensor memory (g = 2 .. 7); the
+// dropped pairs and the 42-bit truncation weigh 2^-42 of the row / state maxima.  The epilogue
+// forms the FP64 value of each tile row; tile partials are summed in FP64 (k_tc_reduce) into z
+// (phase 1) and into the far part of Y (phase 2).  The near field, the diagonal and the scatter
+// stay on k_rows_multi (hmat_multi.cu), which adds this far part.
+//
+// Data path of k_tc_gemm (512 threads, one CTA per SM, persistent over a tile list): A is packed
+// once as FP32 (4 bytes per factor element, the same bytes as the FP32 packing) in stages of 32
+// K elements, row-major [128][32]; each stage is one 16 KB cp.async.bulk copy into a 4-stage ring
+// (mbarrier transaction counts).  Converter warps cut the stage into its six int8 slices in the
+// canonical K-major no-swizzle layout of tcgen05 (8 x 16-byte core matrices, 4 KB per slice) and
+// the B rows (X~ or z, FP64) of the stage into six slices of 16 x 32 (rows 8-15 zero), then
+// fence.proxy.async.  One thread issues the 21 MMAs (M = 128, N = 16, K = 32) per stage and
+// tcgen05.commit; the epilogue warps read the six accumulators with tcgen05.ld.
+//   warp 0    : cp.async.bulk of A stages;
+//   warp 1    : MMA issuer;
+//   warp 2    : allocates / frees 256 tensor-memory columns (two buffers of 6 x 16 int32);
+//   warps 4-7 : epilogue (TMEM lanes 32 (w % 4) .. + 31) to FP64 partials;
+//   warps 8-15: converters.
 // Every mbarrier wait is bounded; on a timeout the kernel records SPX_ERR_TIMEOUT, the roles
 // stop, the MMA issuer waits (bounded) for its last commit, and tensor memory is freed.
 //
@@ -40,11 +52,13 @@
 namespace spx {
 
 struct TcTile {
-  int64_t a_off;   // bytes: packed A of nsteps K-steps
-  int32_t nsteps;  // K-steps of 8
-  int32_t b_row0;  // first row of the B source vector for K index 0
+  int64_t a_off;   // bytes: packed FP32 A of nsteps stages
+  int32_t nsteps;  // stages of 32 K elements
+  int32_t b_row0;  // first row of the B source for K index 0
   int32_t b_rows;  // valid K rows (B is zero past them)
   int32_t slot;    // output partial: rows slot * 128 .. + 127
+  int32_t bsc;     // row of the B exponent table (column cluster or row group)
+  int32_t pad;
 };
 
 struct TcPack {
@@ -52,17 +66,22 @@ struct TcPack {
   int64_t tab;     // phase 1: rowbase index of row 0; phase 2: colbase index of k = 0
   int64_t roff;    // phase 1: column offset added to rowbase; phase 2: row offset in the cluster
   int32_t nsteps, kvalid, rvalid, mode;
+  int32_t slot, pad;
 };
 
 struct TcPlan {
   int64_t zlen = 0, nslots1 = 0, nslots2 = 0, a_bytes = 0;
   int kstep_max = 0;
-  DevBuf<char> A1, A2;                 // packed A of the two phases
+  DevBuf<char> A1, A2;                 // packed FP32 A of the two phases
+  DevBuf<int32_t> ea1, ea2;            // A row exponents per slot [slots][128]
   DevBuf<TcTile> t1, t2;
   int32_t nt1 = 0, nt2 = 0;
   DevBuf<int64_t> rp1, rp2;            // CSR: z entry / perm row -> partial rows
   DevBuf<int32_t> ix1, ix2;
-  DevBuf<float> part1, part2;          // [slots * 128][8]
+  DevBuf<int64_t> br1, br2;            // B row ranges per exponent row [n][2]
+  int32_t nb1 = 0, nb2 = 0;
+  DevBuf<int32_t> eb1, eb2;            // B exponents [n][8]
+  DevBuf<double> part1, part2;         // [slots * 128][8]
   DevBuf<double> z, yfar;              // [zlen][8], [Nb][8]
   DevBuf<int> err;
 };
@@ -71,18 +90,23 @@ namespace tc {
 
 constexpr int R = 8;
 constexpr int TM = 128;
-constexpr int STEP_BYTES = TM * 8 * 4;  // 4096: 128 rows x 8 TF32
-constexpr int STAGE_STEPS = 4;
+constexpr int KS = 32;                        // K elements per stage (one kind::i8 MMA)
+constexpr int NSL = 6;                        // 7-bit slices per operand (42 bits)
+constexpr int NG = 6;                         // accumulator groups: slice pairs t + u = 2 .. 7
+constexpr int FIX = 7 * NSL;                  // fixed-point bits
 constexpr int NSTAGE = 4;
-constexpr int STAGE_BYTES = STAGE_STEPS * STEP_BYTES;
-constexpr int NB = 16;                  // MMA N: M = 128 takes N in multiples of 16, so the
-                                        // 8 states are padded with 8 zero rows of B
-constexpr int BSTEP_BYTES = NB * 8 * 4;  // 512: 16 rows x 8 TF32
-constexpr int KSTEP_MAX_DEFAULT = 256;  // K-steps per tile (2048 elements); the autotuner also tries 64
-constexpr int THREADS = 384;
+constexpr int AF_BYTES = TM * KS * 4;         // FP32 A of a stage: 16 KB
+constexpr int AS_BYTES = TM * KS;             // one int8 slice of A: 4 KB
+constexpr int NB = 16;                        // MMA N: 8 states + 8 zero rows of B
+constexpr int BS_BYTES = NB * KS;             // one int8 slice of B: 512 B
+constexpr int GCOLS = NG * NB;                // TMEM columns of one accumulator buffer
+constexpr int TCOLS = 256;                    // allocated TMEM columns (2 buffers)
+constexpr int KSTEP_MAX_DEFAULT = 64;         // stages per tile (2048 K elements)
+constexpr int THREADS = 512;
+constexpr int CONV_THREADS = 256;
 // + a 32 KB guard after the buffers, so that no descriptor-addressed read can leave the
 // allocation even past the last stage
-constexpr int SMEM_BYTES = 2 * NSTAGE * STAGE_BYTES + 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES + 1024 + 256 + 32768;
+constexpr int SMEM_BYTES = NSTAGE * AF_BYTES + NSTAGE * NSL * AS_BYTES + NSTAGE * NSL * BS_BYTES + 1024 + 32768;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -131,13 +155,13 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   d |= static_cast<uint64_t>(1) << 46;  // descriptor version of sm_100
   return d;                             // base offset 0, no swizzle
 }
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 16, M = 128
-constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((static_cast<uint32_t>(NB) >> 3) << 17) |
+// instruction descriptor: D S32, A and B signed int8, both K-major, N = 16, M = 128
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((static_cast<uint32_t>(NB) >> 3) << 17) |
                            ((128u >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(
           d),
       "l"(a), "l"(b), "r"(IDESC), "r"(acc)
       : "memory");
@@ -151,28 +175,40 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                : "r"(taddr)
                : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 42-bit fixed-point value of v 2^-e (|v| < 2^e) cut into six signed 7-bit slices, most
+// significant first, packed one per byte of the returned words (slice t in byte t of s[t / 4]).
+__device__ __forceinline__ void slices6(double v, int e, int8_t (&d)[NSL]) {
+  const long long m = llrint(ldexp(v, FIX - e));  // |m| < 2^42
+  const long long a = m < 0 ? -m : m;
+#pragma unroll
+  for (int t = 0; t < NSL; ++t) {
+    const int q = static_cast<int>((a >> (FIX - 7 * (t + 1))) & 127);
+    d[t] = static_cast<int8_t>(m < 0 ? -q : q);
+  }
 }
 
-__device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
-
-// B (16 rows x 8 K; rows 8-15 stay zero) of one K-step, K-major core-matrix layout: K chunk
-// c = k / 4 at c * 256 bytes, row group n / 8 at 128, row n % 8 at 16, element k % 4 at 4
-__device__ __forceinline__ int boff(int n, int k) { return (k >> 2) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (k & 3) * 4; }
+// byte offset of element (row, k) of a K-major no-swizzle int8 tile of 32 K columns:
+// 16-byte core-matrix rows, row groups of 8 at 128 bytes, the two K halves `half` bytes apart
+__device__ __forceinline__ int i8off(int row, int k, int half) {
+  return (k >> 4) * half + (row >> 3) * 128 + (row & 7) * 16 + (k & 15);
+}
 
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const TcTile* __restrict__ tiles, int ntiles, const char* __restrict__ A,
-              const double* __restrict__ bsrc, float* __restrict__ part, int* __restrict__ err) {
+              const int32_t* __restrict__ ea, const int32_t* __restrict__ eb, const double* __restrict__ bsrc,
+              double* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(1024) char smem[];
-  char* sA = smem;                                         // [NSTAGE][STAGE_BYTES]
-  char* sAlo = sA + NSTAGE * STAGE_BYTES;                  // [NSTAGE][STAGE_BYTES]
-  char* sBhi = sAlo + NSTAGE * STAGE_BYTES;                // [NSTAGE][STAGE_STEPS][256]
-  char* sBlo = sBhi + NSTAGE * STAGE_STEPS * BSTEP_BYTES;  // [NSTAGE][STAGE_STEPS][256]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sBlo + NSTAGE * STAGE_STEPS * BSTEP_BYTES);
-  uint64_t* full = bars;              // [NSTAGE] A copied
-  uint64_t* ready = bars + NSTAGE;    // [NSTAGE] A split, B staged
-  uint64_t* empty = bars + 2 * NSTAGE;  // [NSTAGE] MMAs done with the stage
-  uint64_t* accf = bars + 3 * NSTAGE;   // [2] accumulator complete
+  char* sAF = smem;                                  // [NSTAGE][AF_BYTES]   FP32 A, row-major [128][32]
+  char* sAS = sAF + NSTAGE * AF_BYTES;               // [NSTAGE][NSL][AS_BYTES] int8 slices of A
+  char* sBS = sAS + NSTAGE * NSL * AS_BYTES;         // [NSTAGE][NSL][BS_BYTES] int8 slices of B
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sBS + NSTAGE * NSL * BS_BYTES);
+  uint64_t* full = bars;                 // [NSTAGE] A copied
+  uint64_t* ready = bars + NSTAGE;       // [NSTAGE] slices written
+  uint64_t* empty = bars + 2 * NSTAGE;   // [NSTAGE] MMAs done with the stage
+  uint64_t* accf = bars + 3 * NSTAGE;    // [2] accumulator complete
   uint64_t* acce = bars + 3 * NSTAGE + 2;  // [2] accumulator read
   uint64_t* fin = bars + 3 * NSTAGE + 4;   // last MMAs done
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3 * NSTAGE + 6);
@@ -182,7 +218,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (tid == 0) {
     for (int s = 0; s < NSTAGE; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&ready[s], 128);
+      mbar_init(&ready[s], CONV_THREADS);
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -193,11 +229,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
-  for (int e = tid; e < 2 * NSTAGE * STAGE_STEPS * BSTEP_BYTES / 16; e += THREADS)
-    reinterpret_cast<float4*>(sBhi)[e] = make_float4(0.f, 0.f, 0.f, 0.f);  // B hi and lo (contiguous)
+  for (int e = tid; e < NSTAGE * NSL * BS_BYTES / 16; e += THREADS)
+    reinterpret_cast<int4*>(sBS)[e] = make_int4(0, 0, 0, 0);  // B rows 8-15 stay zero
   fence_proxy_async();
   if (warp == 2) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)), "r"(32)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)),
+                 "r"(TCOLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -216,13 +253,11 @@ __global__ void __launch_bounds__(THREADS, 1)
       int item = 0;
       for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
         const TcTile T = tiles[t];
-        for (int s0 = 0; s0 < T.nsteps; s0 += STAGE_STEPS, ++item) {
+        for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
           if (!mbar_wait(&empty[st], (rnd & 1) ^ 1)) { fail(); break; }
-          const int ns = min(STAGE_STEPS, T.nsteps - s0);
-          const uint32_t bytes = static_cast<uint32_t>(ns * STEP_BYTES);
-          mbar_expect_tx(&full[st], bytes);
-          bulk_g2s(sA + st * STAGE_BYTES, A + T.a_off + static_cast<int64_t>(s0) * STEP_BYTES, bytes, &full[st]);
+          mbar_expect_tx(&full[st], AF_BYTES);
+          bulk_g2s(sAF + st * AF_BYTES, A + T.a_off + static_cast<int64_t>(s0) * AF_BYTES, AF_BYTES, &full[st]);
         }
       }
       // leave no copy in flight: the last stages' copies have landed (bounded)
@@ -237,26 +272,21 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int buf = tc & 1, use = tc >> 1;
         if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
         tc_after();
-        const uint32_t d = tbase + static_cast<uint32_t>(buf * NB);
-        uint32_t acc = 0;
+        const uint32_t d0 = tbase + static_cast<uint32_t>(buf * GCOLS);
+        uint32_t started = 0;  // bit g: accumulator g holds this tile's sum already
         bool ok = true;
-        for (int s0 = 0; s0 < T.nsteps; s0 += STAGE_STEPS, ++item) {
+        for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
           if (!mbar_wait(&ready[st], rnd & 1)) { fail(); ok = false; break; }
           tc_after();
-          const int ns = min(STAGE_STEPS, T.nsteps - s0);
-          for (int k = 0; k < ns; ++k) {
-            const uint32_t a = su32(sA + st * STAGE_BYTES + k * STEP_BYTES);
-            const uint32_t al = su32(sAlo + st * STAGE_BYTES + k * STEP_BYTES);
-            const uint32_t bh = su32(sBhi + (st * STAGE_STEPS + k) * BSTEP_BYTES);
-            const uint32_t bl = su32(sBlo + (st * STAGE_STEPS + k) * BSTEP_BYTES);
-            const uint64_t da = sdesc(a, 2048, 128), dal = sdesc(al, 2048, 128);
-            const uint64_t dbh = sdesc(bh, 256, 128), dbl = sdesc(bl, 256, 128);
-            mma_tf32(d, da, dbh, acc);
-            acc = 1;
-            mma_tf32(d, da, dbl, 1);
-            mma_tf32(d, dal, dbh, 1);
-          }
+          for (int ta = 0; ta < NSL; ++ta)
+            for (int ub = 0; ub + ta < NG; ++ub) {
+              const int g = ta + ub;
+              const uint64_t da = sdesc(su32(sAS + (st * NSL + ta) * AS_BYTES), 2048, 128);
+              const uint64_t db = sdesc(su32(sBS + (st * NSL + ub) * BS_BYTES), 256, 128);
+              mma_i8(d0 + static_cast<uint32_t>(g * NB), da, db, (started >> g) & 1u);
+              started |= 1u << g;
+            }
           mma_commit(&empty[st]);
           issued = true;
         }
@@ -276,43 +306,67 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int buf = tc & 1, use = tc >> 1;
       if (!mbar_wait(&accf[buf], use & 1)) { fail(); break; }
       tc_after();
-      uint32_t v[8];
-      tmem_ld8(tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * NB), v);
+      uint32_t v[NG][8];
+      const uint32_t ta = tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * GCOLS);
+#pragma unroll
+      for (int g = 0; g < NG; ++g) tmem_ld8(ta + static_cast<uint32_t>(g * NB), v[g]);
+      tmem_wait_ld();
       tc_before();
       mbar_arrive(&acce[buf]);
       const int row = 32 * sp + lane;
-      float4* o = reinterpret_cast<float4*>(part + (static_cast<int64_t>(T.slot) * TM + row) * R);
-      o[0] = make_float4(__uint_as_float(v[0]), __uint_as_float(v[1]), __uint_as_float(v[2]), __uint_as_float(v[3]));
-      o[1] = make_float4(__uint_as_float(v[4]), __uint_as_float(v[5]), __uint_as_float(v[6]), __uint_as_float(v[7]));
+      const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
+      double* o = part + (static_cast<int64_t>(T.slot) * TM + row) * R;
+#pragma unroll
+      for (int n = 0; n < R; ++n) {
+        double y = 0.0;
+#pragma unroll
+        for (int g = NG - 1; g >= 0; --g) y += ldexp(static_cast<double>(static_cast<int32_t>(v[g][n])), -7 * (g + 2));
+        o[n] = ldexp(y, er + eb[static_cast<int64_t>(T.bsc) * R + n]);
+      }
     }
-  } else if (warp >= 8) {  // converter: A split in place, B gathered and split
-    const int ct = tid - 256;
+  } else if (warp >= 8) {  // converters: slices of A and of B
+    const int ct = tid - (THREADS - CONV_THREADS);
     int item = 0;
     for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
       const TcTile T = tiles[t];
       bool ok = true;
-      for (int s0 = 0; s0 < T.nsteps; s0 += STAGE_STEPS, ++item) {
+      for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
         const int st = item % NSTAGE, rnd = item / NSTAGE;
-        const int ns = min(STAGE_STEPS, T.nsteps - s0);
-        // the stage's copy has landed, so its previous MMAs are done and B / A_lo are free
+        // the stage's copy has landed, so its previous MMAs are done and the slices are free
         if (!mbar_wait(&full[st], rnd & 1)) { fail(); ok = false; break; }
-        for (int e = ct; e < ns * 64; e += 128) {
-          const int k8 = e >> 6, idx = e & 63, n = idx >> 3, j = idx & 7;
-          const int kk = (s0 + k8) * 8 + j;
-          const double x = kk < T.b_rows ? bsrc[(static_cast<int64_t>(T.b_row0) + kk) * R + n] : 0.0;
-          const float hi = tf32_trunc(static_cast<float>(x));
-          const float lo = static_cast<float>(x - static_cast<double>(hi));
-          const int o = (st * STAGE_STEPS + k8) * BSTEP_BYTES + boff(n, j);
-          *reinterpret_cast<float*>(sBhi + o) = hi;
-          *reinterpret_cast<float*>(sBlo + o) = lo;
+        // A: thread -> (row, 4 consecutive k); FP32 values, exponent of the tile row
+        const float4* af = reinterpret_cast<const float4*>(sAF + st * AF_BYTES);
+        char* as = sAS + st * NSL * AS_BYTES;
+        for (int e = ct; e < TM * KS / 4; e += CONV_THREADS) {
+          const int row = e >> 3, k = (e & 7) * 4;
+          const float4 a = af[e];
+          const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
+          int8_t d0[NSL], d1[NSL], d2[NSL], d3[NSL];
+          slices6(a.x, er, d0);
+          slices6(a.y, er, d1);
+          slices6(a.z, er, d2);
+          slices6(a.w, er, d3);
+          const int off = i8off(row, k, 2048);
+#pragma unroll
+          for (int q = 0; q < NSL; ++q) {
+            const uint32_t w = static_cast<uint32_t>(static_cast<uint8_t>(d0[q])) |
+                               (static_cast<uint32_t>(static_cast<uint8_t>(d1[q])) << 8) |
+                               (static_cast<uint32_t>(static_cast<uint8_t>(d2[q])) << 16) |
+                               (static_cast<uint32_t>(static_cast<uint8_t>(d3[q])) << 24);
+            *reinterpret_cast<uint32_t*>(as + q * AS_BYTES + off) = w;
+          }
         }
-        float4* a4 = reinterpret_cast<float4*>(sA + st * STAGE_BYTES);
-        float4* l4 = reinterpret_cast<float4*>(sAlo + st * STAGE_BYTES);
-        for (int e = ct; e < ns * (STEP_BYTES / 16); e += 128) {
-          const float4 v = a4[e];
-          const float4 h = make_float4(tf32_trunc(v.x), tf32_trunc(v.y), tf32_trunc(v.z), tf32_trunc(v.w));
-          a4[e] = h;
-          l4[e] = make_float4(v.x - h.x, v.y - h.y, v.z - h.z, v.w - h.w);
+        // B: thread -> (state n < 8, k); rows 8-15 stay zero
+        char* bs = sBS + st * NSL * BS_BYTES;
+        {
+          const int n = ct >> 5, k = ct & 31;  // 256 threads = 8 states x 32 k
+          const int kk = s0 * KS + k;
+          const double x = kk < T.b_rows ? bsrc[(static_cast<int64_t>(T.b_row0) + kk) * R + n] : 0.0;
+          int8_t c[NSL];
+          slices6(x, eb[static_cast<int64_t>(T.bsc) * R + n], c);
+          const int off = i8off(n, k, 256);
+#pragma unroll
+          for (int q = 0; q < NSL; ++q) bs[q * BS_BYTES + off] = static_cast<char>(c[q]);
         }
         fence_proxy_async();
         mbar_arrive(&ready[st]);
@@ -323,45 +377,72 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_before();
   __syncthreads();
   tc_after();
-  if (warp == 2) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(32) : "memory");
+  if (warp == 2) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TCOLS) : "memory");
 }
 
 // out[i][n] = sum over p in [rp[i], rp[i+1]) of part[ix[p]][n]  (FP64, fixed order)
 __global__ void k_tc_reduce(int64_t nrows, const int64_t* __restrict__ rp, const int32_t* __restrict__ ix,
-                            const float* __restrict__ part, double* __restrict__ out) {
+                            const double* __restrict__ part, double* __restrict__ out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t i = t >> 3;
   const int n = static_cast<int>(t & 7);
   if (i >= nrows) return;
   double s = 0.0;
-  for (int64_t p = rp[i]; p < rp[i + 1]; ++p) s += static_cast<double>(part[static_cast<int64_t>(ix[p]) * R + n]);
+  for (int64_t p = rp[i]; p < rp[i + 1]; ++p) s += part[static_cast<int64_t>(ix[p]) * R + n];
   out[i * R + n] = s;
 }
 
-// packed A of one (tile, K-step): 128 rows x 8 TF32 in the core-matrix layout
-// (row r, k): (k / 4) * 2048 + (r / 8) * 128 + (r % 8) * 16 + (k % 4) * 4 bytes
+// exponent e with max |v| < 2^(e - 1) (one bit of headroom for the rounding of the 42-bit
+// value), 0 for zero
+__device__ __forceinline__ int headroom_exp(double mx) { return mx > 0.0 ? ilogb(mx) + 2 : 0; }
+
+// B exponents: for every range [rng[2j], rng[2j+1]) of rows of src ([rows][8] FP64) and every
+// state n, out[j][n] = the exponent of the range's largest |value| (one CTA per range)
+__global__ void k_tc_bexp(int nr, const int64_t* __restrict__ rng, const double* __restrict__ src,
+                          int32_t* __restrict__ out) {
+  __shared__ double sh[8][32];
+  const int j = blockIdx.x;
+  if (j >= nr) return;
+  const int n = threadIdx.x & 7, w = threadIdx.x >> 3;  // 256 threads: 32 row lanes x 8 states
+  double mx = 0.0;
+  for (int64_t i = rng[2 * j] + w; i < rng[2 * j + 1]; i += 32) mx = fmax(mx, fabs(src[i * R + n]));
+  sh[n][w] = mx;
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double m = 0.0;
+    for (int q = 0; q < 32; ++q) m = fmax(m, sh[threadIdx.x][q]);
+    out[static_cast<int64_t>(j) * R + threadIdx.x] = headroom_exp(m);
+  }
+}
+
+// packed A of one tile: FP32, stage s holds rows 0..127 x K elements 32 s .. 32 s + 31 row-major;
+// ea[slot][r] = the exponent of row r's largest |value| over the tile (one CTA per tile, a thread
+// per row)
 __global__ void k_tc_pack(const TcPack* __restrict__ jobs, int njobs, const double* __restrict__ pool,
                           const int64_t* __restrict__ rowbase, const int64_t* __restrict__ colbase,
-                          char* __restrict__ A) {
-  const TcPack J = jobs[blockIdx.y];
-  for (int s = blockIdx.x; s < J.nsteps; s += gridDim.x) {
-    float* dst = reinterpret_cast<float*>(A + J.a_off + static_cast<int64_t>(s) * STEP_BYTES);
-    for (int e = threadIdx.x; e < TM * 8; e += blockDim.x) {
-      const int r = e >> 3, j = e & 7;
-      const int k = s * 8 + j;
-      double v = 0.0;
-      if (r < J.rvalid && k < J.kvalid) {
-        if (J.mode == 1) {
-          const int64_t b = rowbase[J.tab + r];
-          if (b >= 0) v = pool[b + J.roff + k];
-        } else {
-          const int64_t b = colbase[J.tab + k];
-          if (b >= 0) v = pool[b + J.roff + r];
-        }
+                          char* __restrict__ A, int32_t* __restrict__ ea) {
+  const TcPack J = jobs[blockIdx.x];
+  const int r = threadIdx.x;  // 128 threads
+  float* dst = reinterpret_cast<float*>(A + J.a_off);
+  const int K = J.nsteps * KS;
+  double mx = 0.0;
+  int64_t b = -1;
+  if (r < J.rvalid && J.mode == 1) b = rowbase[J.tab + r];
+  for (int k = 0; k < K; ++k) {
+    double v = 0.0;
+    if (r < J.rvalid && k < J.kvalid) {
+      if (J.mode == 1) {
+        if (b >= 0) v = pool[b + J.roff + k];
+      } else {
+        const int64_t c = colbase[J.tab + k];
+        if (c >= 0) v = pool[c + J.roff + r];
       }
-      dst[((j >> 2) * 2048 + (r >> 3) * 128 + (r & 7) * 16 + (j & 3) * 4) >> 2] = static_cast<float>(v);
     }
+    const float f = static_cast<float>(v);
+    mx = fmax(mx, fabs(static_cast<double>(f)));
+    dst[static_cast<int64_t>(k >> 5) * (TM * KS) + r * KS + (k & 31)] = f;
   }
+  ea[static_cast<int64_t>(J.slot) * TM + r] = headroom_exp(mx);
 }
 
 }  // namespace tc
@@ -389,11 +470,12 @@ Csr make_csr(int64_t nrows, const std::vector<std::pair<int64_t, int32_t>>& pair
 
 void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   using namespace tc;
-  // K-steps of 8 per tile (FP32 accumulation in tensor memory runs over at most 8 x this many
-  // products; the tiles' partials are summed in FP64).  SPX_TC_KSTEP sets it for tuning.
+  // stages of 32 K elements per tile (the int32 group sums stay exact far beyond the largest
+  // tile); SPX_TC_KSTEP sets it for tuning
   int KSTEP_MAX = kstep_max > 0 ? kstep_max : KSTEP_MAX_DEFAULT;
   if (kstep_max <= 0)
     if (const char* e = std::getenv("SPX_TC_KSTEP")) KSTEP_MAX = std::max(1, std::atoi(e));
+  KSTEP_MAX = std::min(KSTEP_MAX, 256);
   SPX_CHECK(H.far_pool64.n > 0 || H.stats.n_far == 0, "the tensor-core apply needs the FP64 factors");
   auto P = std::make_shared<TcPlan>();
   std::vector<int> far;
@@ -424,7 +506,7 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   P->zlen = zlen;
   std::vector<TcTile> t1, t2;
   std::vector<TcPack> p1, p2;
-  std::vector<int64_t> rowbase, colbase;
+  std::vector<int64_t> rowbase, colbase, br1, br2;
   std::vector<std::pair<int64_t, int32_t>> m1, m2;
   int64_t a1 = 0, a2 = 0;
   int32_t slot1 = 0, slot2 = 0;
@@ -438,24 +520,27 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
       size_t e = u;
       while (e < tmp.size() && tmp[e].first == tmp[u].first) ++e;
       const int64_t cs = tmp[u].first.first, K = tmp[u].first.second - cs;
+      const int32_t bsc = static_cast<int32_t>(br1.size() / 2);
+      br1.push_back(cs);
+      br1.push_back(cs + K);
       std::vector<std::pair<int64_t, int64_t>> rows;  // (pool base of V row q, z entry)
       for (size_t v = u; v < e; ++v) {
         const HBlock& B = H.blocks[tmp[v].second];
         const int64_t n = B.ce - B.cs;
         for (int q = 0; q < B.rank; ++q) rows.push_back({B.off_v + q * n, zoff[tmp[v].second] + q});
       }
-      const int64_t ksteps = (K + 7) / 8;
+      const int64_t ksteps = (K + KS - 1) / KS;
       for (int64_t m0 = 0; m0 < static_cast<int64_t>(rows.size()); m0 += TM) {
         const int64_t tab = static_cast<int64_t>(rowbase.size());
         const int rv = static_cast<int>(std::min<int64_t>(TM, rows.size() - m0));
         for (int r = 0; r < TM; ++r) rowbase.push_back(r < rv ? rows[m0 + r].first : -1);
         for (int64_t k0 = 0; k0 < ksteps; k0 += KSTEP_MAX) {
           const int ns = static_cast<int>(std::min<int64_t>(KSTEP_MAX, ksteps - k0));
-          const int kv = static_cast<int>(std::min<int64_t>(8 * ns, K - 8 * k0));
-          t1.push_back(TcTile{a1, ns, static_cast<int32_t>(cs + 8 * k0), kv, slot1});
-          p1.push_back(TcPack{a1, tab, 8 * k0, ns, kv, rv, 1});
+          const int kv = static_cast<int>(std::min<int64_t>(KS * ns, K - KS * k0));
+          t1.push_back(TcTile{a1, ns, static_cast<int32_t>(cs + KS * k0), kv, slot1, bsc, 0});
+          p1.push_back(TcPack{a1, tab, KS * k0, ns, kv, rv, 1, slot1, 0});
           for (int r = 0; r < rv; ++r) m1.push_back({rows[m0 + r].second, slot1 * TM + r});
-          a1 += static_cast<int64_t>(ns) * STEP_BYTES;
+          a1 += static_cast<int64_t>(ns) * AF_BYTES;
           ++slot1;
         }
       }
@@ -475,21 +560,26 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
       K += k8;
     }
     const int64_t z0 = zoff[rgroups[g][0]];
-    const int64_t ksteps = K / 8;
+    const int32_t bsc = static_cast<int32_t>(br2.size() / 2);
+    br2.push_back(z0);
+    br2.push_back(z0 + K);
+    const int64_t ksteps = (K + KS - 1) / KS;
     for (int64_t m0 = 0; m0 < rows; m0 += TM) {
       const int rv = static_cast<int>(std::min<int64_t>(TM, rows - m0));
       for (int64_t k0 = 0; k0 < ksteps; k0 += KSTEP_MAX) {
         const int ns = static_cast<int>(std::min<int64_t>(KSTEP_MAX, ksteps - k0));
-        const int kv = 8 * ns;
-        t2.push_back(TcTile{a2, ns, static_cast<int32_t>(z0 + 8 * k0), kv, slot2});
-        p2.push_back(TcPack{a2, kb + 8 * k0, m0, ns, kv, rv, 2});
+        const int kv = static_cast<int>(std::min<int64_t>(KS * ns, K - KS * k0));
+        t2.push_back(TcTile{a2, ns, static_cast<int32_t>(z0 + KS * k0), kv, slot2, bsc, 0});
+        p2.push_back(TcPack{a2, kb + KS * k0, m0, ns, kv, rv, 2, slot2, 0});
         for (int r = 0; r < rv; ++r) m2.push_back({rs + m0 + r, slot2 * TM + r});
-        a2 += static_cast<int64_t>(ns) * STEP_BYTES;
+        a2 += static_cast<int64_t>(ns) * AF_BYTES;
         ++slot2;
       }
     }
   }
-  SPX_CHECK(zlen < (int64_t(1) << 31) && slot1 < (1 << 24) && slot2 < (1 << 24), "tensor-core plan too large");
+  SPX_CHECK(zlen < (int64_t(1) << 31) && slot1 < (1 << 24) && slot2 < (1 << 24) &&
+                H.Nb + 2 * KS * KSTEP_MAX < (int64_t(1) << 31),
+            "tensor-core plan too large");
   // larger tiles first, dealt round-robin to the CTAs
   auto sort_tiles = [](std::vector<TcTile>& t) {
     std::stable_sort(t.begin(), t.end(), [](const TcTile& a, const TcTile& b) { return a.nsteps > b.nsteps; });
@@ -504,31 +594,37 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   P->kstep_max = KSTEP_MAX;
   P->A1.alloc(std::max<int64_t>(a1, 16));
   P->A2.alloc(std::max<int64_t>(a2, 16));
+  P->ea1.alloc(std::max<int64_t>(slot1, 1) * TM);
+  P->ea2.alloc(std::max<int64_t>(slot2, 1) * TM);
   P->t1.upload(t1, s);
   P->t2.upload(t2, s);
   {
     DevBuf<int64_t> drb, dcb;
     drb.upload(rowbase.empty() ? std::vector<int64_t>{-1} : rowbase, s);
     dcb.upload(colbase.empty() ? std::vector<int64_t>{-1} : colbase, s);
-    auto run = [&](const std::vector<TcPack>& jobs, char* dst) {
-      for (size_t j0 = 0; j0 < jobs.size(); j0 += 65535) {
-        const size_t c = std::min<size_t>(65535, jobs.size() - j0);
-        DevBuf<TcPack> dj;
-        dj.upload(jobs.data() + j0, c, s);
-        k_tc_pack<<<dim3(32, static_cast<unsigned>(c)), 256, 0, s>>>(dj.p, static_cast<int>(c), H.far_pool64.p,
-                                                                     drb.p, dcb.p, dst);
-        SPX_LAUNCH_CHECK();
-        SPX_CUDA(cudaStreamSynchronize(s));
-      }
+    auto run = [&](const std::vector<TcPack>& jobs, char* dst, int32_t* ea) {
+      if (jobs.empty()) return;
+      DevBuf<TcPack> dj;
+      dj.upload(jobs, s);
+      k_tc_pack<<<static_cast<unsigned>(jobs.size()), TM, 0, s>>>(dj.p, static_cast<int>(jobs.size()),
+                                                                 H.far_pool64.p, drb.p, dcb.p, dst, ea);
+      SPX_LAUNCH_CHECK();
+      SPX_CUDA(cudaStreamSynchronize(s));
     };
-    run(p1, P->A1.p);
-    run(p2, P->A2.p);
+    run(p1, P->A1.p, P->ea1.p);
+    run(p2, P->A2.p, P->ea2.p);
   }
   Csr c1 = make_csr(zlen, m1), c2 = make_csr(H.Nb, m2);
   P->rp1.upload(c1.rp, s);
   P->ix1.upload(c1.ix.empty() ? std::vector<int32_t>{0} : c1.ix, s);
   P->rp2.upload(c2.rp, s);
   P->ix2.upload(c2.ix.empty() ? std::vector<int32_t>{0} : c2.ix, s);
+  P->nb1 = static_cast<int32_t>(br1.size() / 2);
+  P->nb2 = static_cast<int32_t>(br2.size() / 2);
+  P->br1.upload(br1.empty() ? std::vector<int64_t>{0, 0} : br1, s);
+  P->br2.upload(br2.empty() ? std::vector<int64_t>{0, 0} : br2, s);
+  P->eb1.alloc(std::max<int64_t>(P->nb1, 1) * R);
+  P->eb2.alloc(std::max<int64_t>(P->nb2, 1) * R);
   P->part1.alloc(std::max<int64_t>(slot1, 1) * TM * R);
   P->part2.alloc(std::max<int64_t>(slot2, 1) * TM * R);
   P->z.alloc(std::max<int64_t>(zlen, 1) * R);
@@ -546,7 +642,9 @@ const double* tc_far_apply(HMatrix& H, const double* xm, cudaStream_t s) {
   TcPlan& P = *H.tc;
   const int grid = num_sms(H.device);
   if (P.nt1 > 0) {
-    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t1.p, P.nt1, P.A1.p, xm, P.part1.p, P.err.p);
+    k_tc_bexp<<<P.nb1, 256, 0, s>>>(P.nb1, P.br1.p, xm, P.eb1.p);
+    SPX_LAUNCH_CHECK();
+    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t1.p, P.nt1, P.A1.p, P.ea1.p, P.eb1.p, xm, P.part1.p, P.err.p);
     SPX_LAUNCH_CHECK();
   }
   if (P.zlen > 0) {
@@ -554,7 +652,9 @@ const double* tc_far_apply(HMatrix& H, const double* xm, cudaStream_t s) {
     SPX_LAUNCH_CHECK();
   }
   if (P.nt2 > 0) {
-    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t2.p, P.nt2, P.A2.p, P.z.p, P.part2.p, P.err.p);
+    k_tc_bexp<<<P.nb2, 256, 0, s>>>(P.nb2, P.br2.p, P.z.p, P.eb2.p);
+    SPX_LAUNCH_CHECK();
+    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t2.p, P.nt2, P.A2.p, P.ea2.p, P.eb2.p, P.z.p, P.part2.p, P.err.p);
     SPX_LAUNCH_CHECK();
   }
   k_tc_reduce<<<grid_for(H.Nb * R, 256), 256, 0, s>>>(H.Nb, P.rp2.p, P.ix2.p, P.part2.p, P.yfar.p);
@@ -573,8 +673,10 @@ int tc_error(HMatrix& H, cudaStream_t s) {
 int64_t tc_bytes(const HMatrix& H) {
   if (!H.tc) return 0;
   const TcPlan& P = *H.tc;
-  return static_cast<int64_t>(P.A1.bytes() + P.A2.bytes() + P.part1.bytes() + P.part2.bytes() + P.z.bytes() +
-                              P.yfar.bytes() + P.rp1.bytes() + P.rp2.bytes() + P.ix1.bytes() + P.ix2.bytes());
+  return static_cast<int64_t>(P.A1.bytes() + P.A2.bytes() + P.ea1.bytes() + P.ea2.bytes() + P.part1.bytes() +
+                              P.part2.bytes() + P.z.bytes() + P.yfar.bytes() + P.rp1.bytes() + P.rp2.bytes() +
+                              P.ix1.bytes() + P.ix2.bytes() + P.br1.bytes() + P.br2.bytes() + P.eb1.bytes() +
+                              P.eb2.bytes());
 }
 
 }  // namespace spx
