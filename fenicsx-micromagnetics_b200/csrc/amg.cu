@@ -101,6 +101,11 @@ __global__ void k_to_float_rows(const double* __restrict__ a, float* __restrict_
   b[e] = j < n ? static_cast<float>(a[i * n + j]) : 0.0f;
 }
 
+__global__ void k_f32_to_f16(int64_t n, const float* __restrict__ a, __half* __restrict__ b) {
+  const int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (e < n) b[e] = __float2half_rn(a[e]);
+}
+
 }  // namespace
 
 void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, const int32_t* col0, const float* val0,
@@ -110,9 +115,13 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, con
   n0 = h.lv[0].A.n;
   nc = h.lv.back().A.n;
   A.clear(); P.clear(); rrp.clear(); rcol.clear();
-  val.clear(); pval.clear(); rval.clear(); dinv.clear(); vec.clear();
+  val.clear(); pval.clear(); rval.clear(); dinv.clear(); vec.clear(); val16.clear();
   A.resize(nlev); P.resize(nlev); rrp.resize(nlev); rcol.resize(nlev);
-  val.resize(nlev); pval.resize(nlev); rval.resize(nlev); dinv.resize(nlev); vec.resize(nlev);
+  val.resize(nlev); pval.resize(nlev); rval.resize(nlev); dinv.resize(nlev); vec.resize(nlev); val16.resize(nlev);
+  // FP16 values for the cycle's sweeps (tuning option: half the value bytes of every sweep;
+  // the PCG product keeps the FP32 values)
+  const char* e16 = std::getenv("SPX_AMG_FP16");
+  const bool fp16 = e16 && std::atoi(e16) != 0;
   sizes.assign(nlev, 0);
   nnz.assign(nlev, 0);
   pnnz.assign(nlev, 0);
@@ -142,11 +151,14 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, con
     if (l + 1 == nlev) break;  // dense coarsest: vectors only
     HostSell hs, hp;
     std::vector<float> v, vp;
+    int64_t vlen = 0;
     if (l == 0 && sp0) {
       D.nslices = nslices0;
       D.sp = sp0;
       D.col = col0;
       D.val = val0;
+      SPX_CUDA(cudaMemcpyAsync(&vlen, sp0 + nslices0, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      SPX_CUDA(cudaStreamSynchronize(s));
     } else {
       csr_to_sell(L.A, hs, v);
       A[l].upload(hs, s);
@@ -155,6 +167,14 @@ void AmgDevice::upload(const AmgHost& h, cudaStream_t s, const int64_t* sp0, con
       D.sp = A[l].slice_ptr.p;
       D.col = A[l].col.p;
       D.val = val[l].p;
+      vlen = static_cast<int64_t>(v.size());
+    }
+    D.val16 = nullptr;
+    if (fp16 && vlen > 0) {
+      val16[l].alloc(vlen);
+      k_f32_to_f16<<<grid_for(vlen, 256), 256, 0, s>>>(vlen, D.val, val16[l].p);
+      SPX_LAUNCH_CHECK();
+      D.val16 = val16[l].p;
     }
     csr_to_sell(L.P, hp, vp);
     P[l].upload(hp, s);
@@ -267,14 +287,21 @@ __device__ __forceinline__ float4 ld_hint4(const float4* a, uint64_t pol) {
   return v;
 }
 
+__device__ __forceinline__ float ld_hint(const __half* a, uint64_t pol) {
+  unsigned short v;
+  asm("ld.global.nc.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+  return __half2float(__ushort_as_half(v));
+}
+
 // row dot products of one SELL-32 slice (values and columns are read-only for the kernel's
-// lifetime; loaded with the L2 policy `pol`)
+// lifetime; loaded with the L2 policy `pol`); VT = float or __half values
+template <class VT>
 __device__ __forceinline__ float sell_dot(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
-                                          const float* __restrict__ val, int64_t sl, int lane,
+                                          const VT* __restrict__ val, int64_t sl, int lane,
                                           const float* __restrict__ v, uint64_t pol) {
   const int64_t base = sp[sl];
   const int width = static_cast<int>((sp[sl + 1] - base) >> 5);
-  const float* vv = val + base + lane;
+  const VT* vv = val + base + lane;
   const int32_t* cc = col + base + lane;
   float a0 = 0.0f, a1 = 0.0f;
   int k = 0;
@@ -315,12 +342,18 @@ __device__ __forceinline__ void slice_bounds(const int64_t* __restrict__ sp, int
   }
 }
 
+// level matrix times a level vector for one slice, with the FP16 sweep values when present
+__device__ __forceinline__ float lvl_dot(const AmgLevelDev& L, int64_t sl, int lane, const float* __restrict__ v) {
+  return L.val16 ? sell_dot(L.sp, L.col, L.val16, sl, lane, v, l2_policy_keep())
+                 : sell_dot(L.sp, L.col, L.val, sl, lane, v, l2_policy_keep());
+}
+
 // pre-smoothing from x = 0, Chebyshev steps 1 and 2 (one SpMV: A d0, d0 = D^-1 b / theta)
 __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.db, l2_policy_keep());
+    const float t = lvl_dot(L, sl, rr.lane, L.db);
     if (i < L.n) {
       const float di = L.dinv[i];
       const float d0 = L.db[i] / L.theta;
@@ -337,7 +370,7 @@ __device__ void pre_a(const AmgLevelDev& L, RowRange rr) {
 __device__ void pre_b(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
+    const float t = lvl_dot(L, sl, rr.lane, L.d);
     if (i < L.n) {
       const float di = L.dinv[i];
       L.r[i] = (L.r[i] - di * t) / di;
@@ -385,7 +418,7 @@ __device__ void prolong_from(const AmgLevelDev& L, const AmgLevelDev& C, RowRang
 __device__ void post_c(const AmgLevelDev& L, RowRange rr) {
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.x, l2_policy_keep());
+    const float t = lvl_dot(L, sl, rr.lane, L.x);
     if (i < L.n) {
       const float r0 = L.db[i] - L.dinv[i] * t;
       const float d0 = r0 / L.theta;
@@ -402,7 +435,7 @@ __device__ void post_d(const AmgLevelDev& L, RowRange rr, const double* __restri
   const float rho0 = 1.0f / L.sigma, rho1 = 1.0f / (2.0f * L.sigma - rho0);
   for (int64_t sl = rr.gw; sl < L.nslices; sl += rr.nw) {
     const int64_t i = sl * 32 + rr.lane;
-    const float t = sell_dot(L.sp, L.col, L.val, sl, rr.lane, L.d, l2_policy_keep());
+    const float t = lvl_dot(L, sl, rr.lane, L.d);
     if (i < L.n) {
       const float r1 = L.r[i] - L.dinv[i] * t;
       const float d1 = rho1 * rho0 * L.d[i] + (2.0f * rho1 / L.delta) * r1;

@@ -19,6 +19,8 @@
 // of the level-0 matrix.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include "spx_internal.cuh"
 
 namespace spx {
@@ -59,6 +61,7 @@ struct AmgLevelDev {
   const int64_t* sp;       // A: SELL-32
   const int32_t* col;
   const float* val;
+  const __half* val16;     // FP16 copy of val for the cycle's sweeps (null: val)
   const float* dinv;
   int64_t p_nslices;       // P: SELL-32, n rows
   const int64_t* p_sp;
@@ -80,6 +83,7 @@ struct AmgDevice {
   std::vector<DevBuf<int64_t>> rrp;
   std::vector<DevBuf<int32_t>> rcol;
   std::vector<DevBuf<float>> val, pval, rval, dinv, vec;
+  std::vector<DevBuf<__half>> val16;  // FP16 sweep values (SPX_AMG_FP16)
   DevBuf<AmgLevelDev> lv;
   DevBuf<float> cinv;
   std::vector<int64_t> sizes, nnz, pnnz, rnnz;  // per level: rows, nonzeros of A, P, R
