@@ -187,10 +187,9 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
   const int u1 = warp_first[wg + 1];
   int u = warp_first[wg];
   FarUnit nxt;
-  if (u < u1) nxt = units[u];
-  if (lane < Z_PF && u + lane < u1) {  // the first units' V^T rows into L2
-    const FarUnit Pf = units[u + lane];
-    prefetch_l2(F + Pf.voff, static_cast<uint32_t>(Pf.nc) * Pf.ldk * sizeof(TF));
+  if (u < u1) {
+    nxt = units[u];
+    if (lane == 0) prefetch_l2(F + nxt.voff, static_cast<uint32_t>(nxt.nc) * nxt.ldk * sizeof(TF));
   }
   TA acc[E];
 #pragma unroll
@@ -198,10 +197,6 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
   for (; u < u1; ++u) {
     const FarUnit U = nxt;
     if (u + 1 < u1) nxt = units[u + 1];  // descriptor of the next unit in flight
-    if (lane == 0 && u + Z_PF < u1) {     // V^T rows Z_PF units ahead into L2
-      const FarUnit Pf = units[u + Z_PF];
-      prefetch_l2(F + Pf.voff, static_cast<uint32_t>(Pf.nc) * Pf.ldk * sizeof(TF));
-    }
     const int nvq = U.ldk / E;
     const int lg = log2_ceil_le5(nvq);
     const int G = 1 << lg, P = 32 >> lg;
@@ -239,6 +234,8 @@ __global__ void __launch_bounds__(Z_WARPS * 32, Z_CTAS_PER_SM)
         for (int t = 0; t < E; ++t) acc[t] += static_cast<TA>(e[t] * a);
       }
     }
+    if (lane == 0 && u + 1 < u1)  // the next unit's V^T rows into L2
+      prefetch_l2(F + nxt.voff, static_cast<uint32_t>(nxt.nc) * nxt.ldk * sizeof(TF));
     const int fl = U.flags & 3;
     if (fl == 0) continue;
     // the block ends in this warp: sum over the phases, write its k rows
