@@ -12,31 +12,32 @@
 //
 // Arithmetic.  The thin film's double-layer potential is a small difference of large surface
 // contributions, so the far field needs FP64-class products: TF32 operands with FP32 tile sums
-// are 100x too coarse for a 1e-5 demag error.  Instead every operand is written as six signed
-// 7-bit slices of a 42-bit fixed-point value: an A element a = 2^e_r sum_t d_t 2^-7t with e_r
-// the exponent of its tile row's largest element, a B element b = 2^f_n sum_u c_u 2^-7u with
-// f_n the exponent of the largest element of its state over the B rows of the cluster (or row
-// group).  sum_k a_k b_k = 2^(e_r + f_n) sum_g 2^-7g A_g, where A_g = sum_{t+u=g} sum_k d_t c_u
-// is an exact int32 sum (|d c| <= 127^2, at most six slice pairs per g, K <= 2048).  The 21
-// slice pairs with t + u <= 7 go to six int32 accumulators in tensor memory (g = 2 .. 7); the
-// dropped pairs and the 42-bit truncation weigh 2^-42 of the row / state maxima.  The epilogue
-// forms the FP64 value of each tile row; tile partials are summed in FP64 (k_tc_reduce) into z
+// are 100x too coarse for a 1e-5 demag error.  Instead every operand is a fixed-point integer
+// cut into balanced base-256 digits (int8 in [-128, 127]):
+//   A element  a = 2^(e_r - 31) sum_{t<4} d_t 256^(3 - t),  e_r from the largest |a| of the tile
+//              row (|a| < 2^(e_r - 1)); a is the FP32 factor, exact whenever |a| >= 2^(e_r - 8);
+//   B element  b = 2^(f_n - 47) sum_{u<6} c_u 256^(5 - u),  f_n from the largest |b| of state n
+//              over the B rows of the cluster (or row group).
+// sum_k a_k b_k = 2^(e_r + f_n - 78) sum_{t,u} 256^(8 - t - u) D_tu with D_tu = sum_k d_tk c_uk an
+// exact int32 sum (|d c| <= 2^14, K <= 8192 per tile: |D| <= 2^27).  No digit pair is dropped.
+// The six digits of every B element sit side by side in the MMA's N dimension (column
+// 8 u + n), so ONE MMA of N = 48 per A digit computes all 24 digit pairs of a K step: four
+// MMAs (M = 128, N = 48, K = 32) per stage into four int32 accumulators D_t in tensor memory.
+// The A digits are cut once, when the plan is built, into the MMA's shared-memory layout: a
+// stage is 16 KB in HBM (4 digits x 128 rows x 32 K), the same 4 bytes per factor element as
+// the FP32 packing, and goes to shared memory by one bulk copy with no conversion.  Only the
+// B rows (X~ or z, FP64) of a stage (8 states x 32 K) are cut at run time.  The epilogue forms
+// the FP64 value of each tile row; tile partials are summed in FP64 (k_tc_reduce) into z
 // (phase 1) and into the far part of Y (phase 2).  The near field, the diagonal and the scatter
 // stay on k_rows_multi (hmat_multi.cu), which adds this far part.
 //
-// Data path of k_tc_gemm (512 threads, one CTA per SM, persistent over a tile list): A is packed
-// once as FP32 (4 bytes per factor element, the same bytes as the FP32 packing) in stages of 32
-// K elements, row-major [128][32]; each stage is one 16 KB cp.async.bulk copy into a 4-stage ring
-// (mbarrier transaction counts).  Converter warps cut the stage into its six int8 slices in the
-// canonical K-major no-swizzle layout of tcgen05 (8 x 16-byte core matrices, 4 KB per slice) and
-// the B rows (X~ or z, FP64) of the stage into six slices of 16 x 32 (rows 8-15 zero), then
-// fence.proxy.async.  One thread issues the 21 MMAs (M = 128, N = 16, K = 32) per stage and
-// tcgen05.commit; the epilogue warps read the six accumulators with tcgen05.ld.
-//   warp 0    : cp.async.bulk of A stages;
-//   warp 1    : MMA issuer;
-//   warp 2    : allocates / frees 256 tensor-memory columns (two buffers of 6 x 16 int32);
-//   warps 4-7 : epilogue (TMEM lanes 32 (w % 4) .. + 31) to FP64 partials;
-//   warps 8-15: converters.
+// Data path of k_tc_gemm (384 threads, one CTA per SM, persistent over a tile list): an
+// 8-stage ring of A stages (cp.async.bulk, mbarrier transaction counts) and of B digit tiles.
+//   warp 0     : cp.async.bulk of A stages;
+//   warp 1     : MMA issuer (4 MMAs per stage, tcgen05.commit);
+//   warp 2     : allocates / frees 512 tensor-memory columns (two buffers of 4 x 48 int32);
+//   warps 4-7  : epilogue (TMEM lanes 32 (w % 4) .. + 31) to FP64 partials;
+//   warps 8-11 : cut the B rows of each stage into digits (canonical K-major layout).
 // Every mbarrier wait is bounded; on a timeout the kernel records SPX_ERR_TIMEOUT, the roles
 // stop, the MMA issuer waits (bounded) for its last commit, and tensor memory is freed.
 //
@@ -52,7 +53,7 @@
 namespace spx {
 
 struct TcTile {
-  int64_t a_off;   // bytes: packed FP32 A of nsteps stages
+  int64_t a_off;   // bytes: A digits of nsteps stages
   int32_t nsteps;  // stages of 32 K elements
   int32_t b_row0;  // first row of the B source for K index 0
   int32_t b_rows;  // valid K rows (B is zero past them)
@@ -72,7 +73,7 @@ struct TcPack {
 struct TcPlan {
   int64_t zlen = 0, nslots1 = 0, nslots2 = 0, a_bytes = 0;
   int kstep_max = 0;
-  DevBuf<char> A1, A2;                 // packed FP32 A of the two phases
+  DevBuf<char> A1, A2;                 // A digits of the two phases, stage by stage
   DevBuf<int32_t> ea1, ea2;            // A row exponents per slot [slots][128]
   DevBuf<TcTile> t1, t2;
   int32_t nt1 = 0, nt2 = 0;
@@ -91,24 +92,25 @@ namespace tc {
 constexpr int R = 8;
 constexpr int TM = 128;
 constexpr int KS = 32;                        // K elements per stage (one kind::i8 MMA)
-constexpr int NSL = 6;                        // 7-bit slices per operand (42 bits)
-constexpr int NG = 6;                         // accumulator groups: slice pairs t + u = 2 .. 7
-constexpr int FIX = 7 * NSL;                  // fixed-point bits
-constexpr int NSTAGE = 4;
-constexpr int AF_BYTES = TM * KS * 4;         // FP32 A of a stage: 16 KB
-constexpr int AS_BYTES = TM * KS;             // one int8 slice of A: 4 KB
-constexpr int NB = 16;                        // MMA N: 8 states + 8 zero rows of B
-constexpr int BS_BYTES = NB * KS;             // one int8 slice of B: 512 B
-constexpr int GCOLS = NG * NB;                // TMEM columns of one accumulator buffer
-constexpr int TCOLS = 256;                    // allocated TMEM columns (2 buffers)
+constexpr int NDA = 4;                        // base-256 digits of an A element (31-bit fixed point)
+constexpr int NDB = 6;                        // base-256 digits of a B element (47-bit fixed point)
+constexpr int FIXA = 8 * NDA - 1;             // fixed-point bits below 2^e
+constexpr int FIXB = 8 * NDB - 1;
+constexpr int NSTAGE = 8;
+constexpr int AD_BYTES = TM * KS;             // one digit plane of an A stage: 4 KB
+constexpr int AST_BYTES = NDA * AD_BYTES;     // an A stage: 16 KB (4 bytes per element)
+constexpr int NB = NDB * R;                   // MMA N = 48: column 8 u + n = digit u of state n
+constexpr int BST_BYTES = NB * KS;            // the B digits of a stage: 1.5 KB
+constexpr int ACOLS = NDA * NB;               // TMEM columns of one accumulator buffer (4 x 48)
+constexpr int TCOLS = 512;                    // allocated TMEM columns (2 buffers of 192)
 constexpr int KSTEP_MAX_DEFAULT = 64;         // stages per tile (2048 K elements)
-constexpr int THREADS = 512;
-constexpr int CONV_THREADS = 256;
+constexpr int THREADS = 384;
+constexpr int CONV_THREADS = 128;             // warps 8-11
 // + a 32 KB guard after the buffers, so that no descriptor-addressed read can leave the
 // allocation even past the last stage
-constexpr int SMEM_BYTES = NSTAGE * AF_BYTES + NSTAGE * NSL * AS_BYTES + NSTAGE * NSL * BS_BYTES + 1024 + 32768;
+constexpr int SMEM_BYTES = NSTAGE * AST_BYTES + NSTAGE * BST_BYTES + 1024 + 32768;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
-
+static_assert((TM / 8) * 128 * (KS / 16) == AD_BYTES && (NB / 8) * 128 * (KS / 16) == BST_BYTES, "digit tile layouts");
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
@@ -155,7 +157,7 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   d |= static_cast<uint64_t>(1) << 46;  // descriptor version of sm_100
   return d;                             // base offset 0, no swizzle
 }
-// instruction descriptor: D S32, A and B signed int8, both K-major, N = 16, M = 128
+// instruction descriptor: D S32, A and B signed int8, both K-major, N = 32, M = 128
 constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((static_cast<uint32_t>(NB) >> 3) << 17) |
                            ((128u >> 4) << 24);
 
@@ -178,15 +180,18 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// 42-bit fixed-point value of v 2^-e (|v| < 2^e) cut into six signed 7-bit slices, most
-// significant first, packed one per byte of the returned words (slice t in byte t of s[t / 4]).
-__device__ __forceinline__ void slices6(double v, int e, int8_t (&d)[NSL]) {
-  const long long m = llrint(ldexp(v, FIX - e));  // |m| < 2^42
-  const long long a = m < 0 ? -m : m;
+// ND balanced base-256 digits (most significant first) of the (8 ND - 1)-bit fixed-point
+// value llrint(v 2^(8 ND - 1 - e)), |v| < 2^(e - 1): sum_t d[t] 256^(ND - 1 - t) equals that
+// integer exactly.
+template <int ND>
+__device__ __forceinline__ void digits(double v, int e, int8_t (&d)[ND]) {
+  long long m = llrint(ldexp(v, 8 * ND - 1 - e));  // |m| <= 2^(8 ND - 2)
 #pragma unroll
-  for (int t = 0; t < NSL; ++t) {
-    const int q = static_cast<int>((a >> (FIX - 7 * (t + 1))) & 127);
-    d[t] = static_cast<int8_t>(m < 0 ? -q : q);
+  for (int t = ND - 1; t >= 0; --t) {
+    const int lo = static_cast<int>(m & 255);
+    const int s = lo >= 128 ? lo - 256 : lo;  // balanced digit in [-128, 127]
+    d[t] = static_cast<int8_t>(s);
+    m = (m - s) >> 8;
   }
 }
 
@@ -201,12 +206,11 @@ __global__ void __launch_bounds__(THREADS, 1)
               const int32_t* __restrict__ ea, const int32_t* __restrict__ eb, const double* __restrict__ bsrc,
               double* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(1024) char smem[];
-  char* sAF = smem;                                  // [NSTAGE][AF_BYTES]   FP32 A, row-major [128][32]
-  char* sAS = sAF + NSTAGE * AF_BYTES;               // [NSTAGE][NSL][AS_BYTES] int8 slices of A
-  char* sBS = sAS + NSTAGE * NSL * AS_BYTES;         // [NSTAGE][NSL][BS_BYTES] int8 slices of B
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sBS + NSTAGE * NSL * BS_BYTES);
+  char* sA = smem;                                   // [NSTAGE][NDA][AD_BYTES] A digits (as in HBM)
+  char* sB = sA + NSTAGE * AST_BYTES;                // [NSTAGE][BST_BYTES]    B digits, N = 48 rows
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + NSTAGE * BST_BYTES);
   uint64_t* full = bars;                 // [NSTAGE] A copied
-  uint64_t* ready = bars + NSTAGE;       // [NSTAGE] slices written
+  uint64_t* ready = bars + NSTAGE;       // [NSTAGE] B digits written
   uint64_t* empty = bars + 2 * NSTAGE;   // [NSTAGE] MMAs done with the stage
   uint64_t* accf = bars + 3 * NSTAGE;    // [2] accumulator complete
   uint64_t* acce = bars + 3 * NSTAGE + 2;  // [2] accumulator read
@@ -229,9 +233,6 @@ __global__ void __launch_bounds__(THREADS, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
-  for (int e = tid; e < NSTAGE * NSL * BS_BYTES / 16; e += THREADS)
-    reinterpret_cast<int4*>(sBS)[e] = make_int4(0, 0, 0, 0);  // B rows 8-15 stay zero
-  fence_proxy_async();
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)),
                  "r"(TCOLS)
@@ -256,8 +257,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
           if (!mbar_wait(&empty[st], (rnd & 1) ^ 1)) { fail(); break; }
-          mbar_expect_tx(&full[st], AF_BYTES);
-          bulk_g2s(sAF + st * AF_BYTES, A + T.a_off + static_cast<int64_t>(s0) * AF_BYTES, AF_BYTES, &full[st]);
+          mbar_expect_tx(&full[st], AST_BYTES);
+          bulk_g2s(sA + st * AST_BYTES, A + T.a_off + static_cast<int64_t>(s0) * AST_BYTES, AST_BYTES, &full[st]);
         }
       }
       // leave no copy in flight: the last stages' copies have landed (bounded)
@@ -272,21 +273,18 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int buf = tc & 1, use = tc >> 1;
         if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
         tc_after();
-        const uint32_t d0 = tbase + static_cast<uint32_t>(buf * GCOLS);
-        uint32_t started = 0;  // bit g: accumulator g holds this tile's sum already
+        const uint32_t d0 = tbase + static_cast<uint32_t>(buf * ACOLS);
         bool ok = true;
         for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
-          if (!mbar_wait(&ready[st], rnd & 1)) { fail(); ok = false; break; }
+          if (!mbar_wait(&full[st], rnd & 1) || !mbar_wait(&ready[st], rnd & 1)) { fail(); ok = false; break; }
           tc_after();
-          for (int ta = 0; ta < NSL; ++ta)
-            for (int ub = 0; ub + ta < NG; ++ub) {
-              const int g = ta + ub;
-              const uint64_t da = sdesc(su32(sAS + (st * NSL + ta) * AS_BYTES), 2048, 128);
-              const uint64_t db = sdesc(su32(sBS + (st * NSL + ub) * BS_BYTES), 256, 128);
-              mma_i8(d0 + static_cast<uint32_t>(g * NB), da, db, (started >> g) & 1u);
-              started |= 1u << g;
-            }
+          const uint64_t db = sdesc(su32(sB + st * BST_BYTES), (NB / 8) * 128, 128);
+#pragma unroll
+          for (int ta = 0; ta < NDA; ++ta) {
+            const uint64_t da = sdesc(su32(sA + st * AST_BYTES + ta * AD_BYTES), (TM / 8) * 128, 128);
+            mma_i8(d0 + static_cast<uint32_t>(ta * NB), da, db, s0 > 0 ? 1u : 0u);
+          }
           mma_commit(&empty[st]);
           issued = true;
         }
@@ -300,73 +298,59 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
   } else if (warp >= 4 && warp < 8) {  // epilogue: TMEM lanes 32 (warp % 4) .. + 31
     const int sp = warp & 3;
+    // 256^(8 - g) for the digit-pair weight g = t + u (exact powers of two)
+    const double wgt[NDA + NDB - 1] = {0x1p64, 0x1p56, 0x1p48, 0x1p40, 0x1p32, 0x1p24, 0x1p16, 0x1p8, 1.0};
     int tc = 0;
     for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tc) {
       const TcTile T = tiles[t];
       const int buf = tc & 1, use = tc >> 1;
       if (!mbar_wait(&accf[buf], use & 1)) { fail(); break; }
       tc_after();
-      uint32_t v[NG][8];
-      const uint32_t ta = tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * GCOLS);
+      const uint32_t ta0 = tbase + (static_cast<uint32_t>(32 * sp) << 16) + static_cast<uint32_t>(buf * ACOLS);
+      double y[R];
 #pragma unroll
-      for (int g = 0; g < NG; ++g) tmem_ld8(ta + static_cast<uint32_t>(g * NB), v[g]);
-      tmem_wait_ld();
+      for (int n = 0; n < R; ++n) y[n] = 0.0;
+#pragma unroll
+      for (int ta = 0; ta < NDA; ++ta) {
+        uint32_t v[NDB][8];  // v[u][n] = D_{ta,u}[row][n]
+#pragma unroll
+        for (int u = 0; u < NDB; ++u) tmem_ld8(ta0 + static_cast<uint32_t>(ta * NB + u * 8), v[u]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int n = 0; n < R; ++n)
+#pragma unroll
+          for (int u = 0; u < NDB; ++u) y[n] += static_cast<double>(static_cast<int32_t>(v[u][n])) * wgt[ta + u];
+      }
       tc_before();
       mbar_arrive(&acce[buf]);
       const int row = 32 * sp + lane;
       const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
       double* o = part + (static_cast<int64_t>(T.slot) * TM + row) * R;
 #pragma unroll
-      for (int n = 0; n < R; ++n) {
-        double y = 0.0;
-#pragma unroll
-        for (int g = NG - 1; g >= 0; --g) y += ldexp(static_cast<double>(static_cast<int32_t>(v[g][n])), -7 * (g + 2));
-        o[n] = ldexp(y, er + eb[static_cast<int64_t>(T.bsc) * R + n]);
-      }
+      for (int n = 0; n < R; ++n) o[n] = ldexp(y[n], er + eb[static_cast<int64_t>(T.bsc) * R + n] - FIXA - FIXB);
     }
-  } else if (warp >= 8) {  // converters: slices of A and of B
+  } else if (warp >= 8) {  // B digits: thread -> (state n, two k); rows 8 u + n of the N = 32 tile
     const int ct = tid - (THREADS - CONV_THREADS);
+    const int n = ct >> 4, k0 = (ct & 15) * 2;
     int item = 0;
     for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
       const TcTile T = tiles[t];
+      const int e = eb[static_cast<int64_t>(T.bsc) * R + n];
       bool ok = true;
       for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
         const int st = item % NSTAGE, rnd = item / NSTAGE;
-        // the stage's copy has landed, so its previous MMAs are done and the slices are free
-        if (!mbar_wait(&full[st], rnd & 1)) { fail(); ok = false; break; }
-        // A: thread -> (row, 4 consecutive k); FP32 values, exponent of the tile row
-        const float4* af = reinterpret_cast<const float4*>(sAF + st * AF_BYTES);
-        char* as = sAS + st * NSL * AS_BYTES;
-        for (int e = ct; e < TM * KS / 4; e += CONV_THREADS) {
-          const int row = e >> 3, k = (e & 7) * 4;
-          const float4 a = af[e];
-          const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
-          int8_t d0[NSL], d1[NSL], d2[NSL], d3[NSL];
-          slices6(a.x, er, d0);
-          slices6(a.y, er, d1);
-          slices6(a.z, er, d2);
-          slices6(a.w, er, d3);
-          const int off = i8off(row, k, 2048);
+        // the stage's previous MMAs are done, so its B digits may be overwritten
+        if (!mbar_wait(&empty[st], (rnd & 1) ^ 1)) { fail(); ok = false; break; }
+        char* bs = sB + st * BST_BYTES;
 #pragma unroll
-          for (int q = 0; q < NSL; ++q) {
-            const uint32_t w = static_cast<uint32_t>(static_cast<uint8_t>(d0[q])) |
-                               (static_cast<uint32_t>(static_cast<uint8_t>(d1[q])) << 8) |
-                               (static_cast<uint32_t>(static_cast<uint8_t>(d2[q])) << 16) |
-                               (static_cast<uint32_t>(static_cast<uint8_t>(d3[q])) << 24);
-            *reinterpret_cast<uint32_t*>(as + q * AS_BYTES + off) = w;
-          }
-        }
-        // B: thread -> (state n < 8, k); rows 8-15 stay zero
-        char* bs = sBS + st * NSL * BS_BYTES;
-        {
-          const int n = ct >> 5, k = ct & 31;  // 256 threads = 8 states x 32 k
+        for (int j = 0; j < 2; ++j) {
+          const int k = k0 + j;
           const int kk = s0 * KS + k;
           const double x = kk < T.b_rows ? bsrc[(static_cast<int64_t>(T.b_row0) + kk) * R + n] : 0.0;
-          int8_t c[NSL];
-          slices6(x, eb[static_cast<int64_t>(T.bsc) * R + n], c);
-          const int off = i8off(n, k, 256);
+          int8_t c[NDB];
+          digits<NDB>(x, e, c);
 #pragma unroll
-          for (int q = 0; q < NSL; ++q) bs[q * BS_BYTES + off] = static_cast<char>(c[q]);
+          for (int u = 0; u < NDB; ++u) bs[i8off(8 * u + n, k, (NB / 8) * 128)] = static_cast<char>(c[u]);
         }
         fence_proxy_async();
         mbar_arrive(&ready[st]);
@@ -415,20 +399,19 @@ __global__ void k_tc_bexp(int nr, const int64_t* __restrict__ rng, const double*
   }
 }
 
-// packed A of one tile: FP32, stage s holds rows 0..127 x K elements 32 s .. 32 s + 31 row-major;
-// ea[slot][r] = the exponent of row r's largest |value| over the tile (one CTA per tile, a thread
-// per row)
+// A digits of one tile: stage s holds digit planes t = 0..3, each the rows 0..127 x K elements
+// 32 s .. 32 s + 31 in the K-major no-swizzle layout of the MMA; ea[slot][r] = the exponent of row
+// r's largest |value| over the tile.  The values are the FP32 factors (the FP32 packing's
+// rounding).  One CTA per tile, a thread per row.
 __global__ void k_tc_pack(const TcPack* __restrict__ jobs, int njobs, const double* __restrict__ pool,
                           const int64_t* __restrict__ rowbase, const int64_t* __restrict__ colbase,
                           char* __restrict__ A, int32_t* __restrict__ ea) {
   const TcPack J = jobs[blockIdx.x];
   const int r = threadIdx.x;  // 128 threads
-  float* dst = reinterpret_cast<float*>(A + J.a_off);
   const int K = J.nsteps * KS;
-  double mx = 0.0;
   int64_t b = -1;
   if (r < J.rvalid && J.mode == 1) b = rowbase[J.tab + r];
-  for (int k = 0; k < K; ++k) {
+  auto value = [&](int k) -> float {
     double v = 0.0;
     if (r < J.rvalid && k < J.kvalid) {
       if (J.mode == 1) {
@@ -438,14 +421,30 @@ __global__ void k_tc_pack(const TcPack* __restrict__ jobs, int njobs, const doub
         if (c >= 0) v = pool[c + J.roff + r];
       }
     }
-    const float f = static_cast<float>(v);
-    mx = fmax(mx, fabs(static_cast<double>(f)));
-    dst[static_cast<int64_t>(k >> 5) * (TM * KS) + r * KS + (k & 31)] = f;
+    return static_cast<float>(v);
+  };
+  double mx = 0.0;
+  for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(static_cast<double>(value(k))));
+  const int e = headroom_exp(mx);
+  char* dst = A + J.a_off;
+  for (int k = 0; k < K; k += 4) {  // four K elements -> one 32-bit word per digit plane
+    uint32_t w[NDA] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int8_t d[NDA];
+      digits<NDA>(static_cast<double>(value(k + j)), e, d);
+#pragma unroll
+      for (int t = 0; t < NDA; ++t) w[t] |= static_cast<uint32_t>(static_cast<uint8_t>(d[t])) << (8 * j);
+    }
+    char* st = dst + static_cast<int64_t>(k >> 5) * AST_BYTES + i8off(r, k & 31, (TM / 8) * 128);
+#pragma unroll
+    for (int t = 0; t < NDA; ++t) *reinterpret_cast<uint32_t*>(st + t * AD_BYTES) = w[t];
   }
-  ea[static_cast<int64_t>(J.slot) * TM + r] = headroom_exp(mx);
+  ea[static_cast<int64_t>(J.slot) * TM + r] = e;
 }
 
 }  // namespace tc
+
 
 // ------------------------------------------------------------------ host: plan and apply
 namespace {
@@ -540,7 +539,7 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
           t1.push_back(TcTile{a1, ns, static_cast<int32_t>(cs + KS * k0), kv, slot1, bsc, 0});
           p1.push_back(TcPack{a1, tab, KS * k0, ns, kv, rv, 1, slot1, 0});
           for (int r = 0; r < rv; ++r) m1.push_back({rows[m0 + r].second, slot1 * TM + r});
-          a1 += static_cast<int64_t>(ns) * AF_BYTES;
+          a1 += static_cast<int64_t>(ns) * AST_BYTES;
           ++slot1;
         }
       }
@@ -572,7 +571,7 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
         t2.push_back(TcTile{a2, ns, static_cast<int32_t>(z0 + KS * k0), kv, slot2, bsc, 0});
         p2.push_back(TcPack{a2, kb + KS * k0, m0, ns, kv, rv, 2, slot2, 0});
         for (int r = 0; r < rv; ++r) m2.push_back({rs + m0 + r, slot2 * TM + r});
-        a2 += static_cast<int64_t>(ns) * AF_BYTES;
+        a2 += static_cast<int64_t>(ns) * AST_BYTES;
         ++slot2;
       }
     }

@@ -1,10 +1,11 @@
-"""The multi-state apply with the far field on the tensor cores (tcgen05 kind::i8: operands
-cut into six 7-bit slices of 42-bit fixed-point values, exact int32 slice-pair sums, FP64
-epilogue) against the CUDA-core paths.
+"""The multi-state apply with the far field on the tensor cores (tcgen05 kind::i8: FP32
+factors as 31-bit and FP64 states as 47-bit fixed-point values cut into base-256 digits, exact
+int32 digit-pair sums, FP64 epilogue) against the CUDA-core paths.
 
 Tolerances (relative L2 per state): tensor-core batch vs single applies of the FP32 packing
-1e-10 (the same FP32 factors; the 41-bit fixed point of each operand and the dropped slice
-pairs weigh about 1e-12 of the row / state maxima); of the FP32/FP16 split packing 1e-6 (the
+1e-9 (the same FP32 factors; factor elements below 2^-7 of their tile row's maximum are rounded
+at 2^-32 of that maximum, about 1/100 of the FP32 rounding that the FP32 packing already
+carries); of the FP32/FP16 split packing 1e-6 (the
 tensor-core plan holds every column in FP32, the split packing its trailing ones in FP16);
 vs the dense operator 1e-5 (the ACA tolerance).  Smooth inputs (the thin film's cancelling
 far field) are checked as well as random ones.  Batches of 8 use the tensor cores; other sizes
@@ -36,7 +37,7 @@ def test_tensor_core_matmat_vs_single(nx, prec):
     Yt = H.matmat(Xs)
     torch.cuda.synchronize()
     assert H.tensor_core_status() == 0
-    tol = 1e-10 if prec == "f32" else 1e-6
+    tol = 1e-9 if prec == "f32" else 1e-6
     assert max(rel_rows(Yt, Ys)) < tol
     # smooth states: constants and long waves over the film
     xb = torch.linspace(0.0, 1.0, H.size, dtype=torch.float64, device=DEV)
@@ -68,4 +69,4 @@ def test_tensor_core_autotune_keeps_results():
     Ys = torch.stack([H.matvec(Xs[r].contiguous()) for r in range(8)])
     H.enable_tensor_cores("auto")          # keeps the fastest of three paths
     assert H.tensor_core_status() == 0
-    assert max(rel_rows(H.matmat(Xs), Ys)) < 1e-10
+    assert max(rel_rows(H.matmat(Xs), Ys)) < 1e-9

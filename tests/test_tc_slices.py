@@ -1,63 +1,82 @@
-"""The integer-slice arithmetic of the tensor-core far field (csrc/hmat_tc.cu), restated in
-numpy on the CPU: operands cut into six signed 7-bit slices of 42-bit fixed-point values
-(exponent with one bit of headroom), the 21 slice pairs with t + u <= 5 (0-based) summed per
-group g = t + u in exact integers, and the FP64 epilogue sum_g 2^-7(g+2) A_g scaled by
-2^(e_r + f_n).
+"""The integer-digit arithmetic of the tensor-core far field (csrc/hmat_tc.cu), restated in
+numpy on the CPU: an operand is the fixed-point integer llrint(v 2^(8 nd - 1 - e)) (e with one
+bit of headroom over the largest |v| of the tile row / state range) cut into nd balanced
+base-256 digits in [-128, 127] (nd = 4 for the FP32 factors, 6 for the FP64 states); all 24
+digit pairs are summed in exact integers (D_tu = sum_k d_tk c_uk, what one kind::i8 MMA of
+N = 48 accumulates per A digit t), and the FP64 epilogue is sum_{t,u} 256^(8 - t - u) D_tu
+scaled by 2^(e_r + f_n - 78).
 
-* the slices reproduce each operand to 2^-41 of its row / state maximum;
-* a tile row's dot product over K = 2048 matches the exact (rational) value to 1e-12 of
-  sum |a_k b_k|, for FP32 factors and FP64 states, with and without cancellation;
-* every group sum stays inside int32 at the largest tile (K = 2048 in the plan; 8192 is the
+* the digits reproduce each operand's fixed-point value exactly, so an operand is exact to
+  2^(e - 8 nd) (FP32 factors within 2^7 of their row maximum are exact);
+* a tile row's dot product over K = 2048 matches the exact (rational) value within the
+  rounding bound of the two fixed points (half a unit of the last digit of each operand) and
+  to 1e-10 of sum |a_k b_k|, for FP32 factors and FP64 states, with and without cancellation.
+  The FP32 rounding of the factors themselves (2^-24 relative per element) weighs about 100x
+  more than this;
+* every pair sum stays inside int32 at the largest tile (K = 2048 in the plan; 8192 is the
   cap of SPX_TC_KSTEP x 32).
 """
 from fractions import Fraction
 
 import numpy as np
 
-FIX, NSL, NG = 42, 6, 6
+NDA, NDB = 4, 6
 
 
 def headroom_exp(mx):
     return int(np.floor(np.log2(mx))) + 2 if mx > 0 else 0
 
 
-def slices6(v, e):
-    """int slices d[0..5] of v (|v| < 2^(e-1)), most significant first."""
-    m = int(np.rint(np.ldexp(float(v), FIX - e)))
-    a = abs(m)
-    q = [(a >> (FIX - 7 * (t + 1))) & 127 for t in range(NSL)]
-    return [-x if m < 0 else x for x in q]
+def digits(v, e, nd):
+    """balanced base-256 digits d[0..nd-1] of llrint(v 2^(8 nd - 1 - e)), most significant first."""
+    m = int(np.rint(np.ldexp(float(v), 8 * nd - 1 - e)))
+    d = [0] * nd
+    for t in range(nd - 1, -1, -1):
+        lo = m & 255
+        s = lo - 256 if lo >= 128 else lo
+        d[t] = s
+        m = (m - s) >> 8
+    assert m == 0
+    return d
 
 
 def tile_dot(a, b):
     """The kernel's value of sum_k a_k b_k for one tile row and one state."""
     er = headroom_exp(np.abs(a).max())
     fn = headroom_exp(np.abs(b).max())
-    da = np.array([slices6(x, er) for x in a], dtype=np.int64)   # [K][6]
-    cb = np.array([slices6(x, fn) for x in b], dtype=np.int64)
-    groups = np.zeros(NG, dtype=np.int64)
-    for t in range(NSL):
-        for u in range(NG - t):
-            groups[t + u] += int(np.dot(da[:, t], cb[:, u]))
+    da = np.array([digits(x, er, NDA) for x in a], dtype=np.int64)   # [K][4]
+    cb = np.array([digits(x, fn, NDB) for x in b], dtype=np.int64)   # [K][6]
+    D = da.T @ cb                                                    # [t][u], exact
     y = 0.0
-    for g in range(NG - 1, -1, -1):
-        y += np.ldexp(float(groups[g]), -7 * (g + 2))
-    return np.ldexp(y, er + fn), groups
+    for t in range(NDA):
+        for u in range(NDB):
+            y += float(D[t, u]) * 2.0 ** (8 * (8 - t - u))
+    return np.ldexp(y, er + fn - (8 * NDA - 1) - (8 * NDB - 1)), D
 
 
 def exact_dot(a, b):
     return float(sum(Fraction(float(x)) * Fraction(float(y)) for x, y in zip(a, b)))
 
 
-def test_slices_reproduce_operands():
+def test_digits_reproduce_operands():
     rng = np.random.default_rng(1)
     v = rng.standard_normal(64) * 10.0 ** rng.uniform(-3, 3, 64)
     e = headroom_exp(np.abs(v).max())
-    for x in v:
-        d = slices6(x, e)
-        assert all(-127 <= q <= 127 for q in d)
-        back = sum(q * 2.0 ** (-7 * (t + 1)) for t, q in enumerate(d)) * 2.0 ** e
-        assert abs(back - x) <= 2.0 ** (e - FIX)
+    for nd in (NDA, NDB):
+        fix = 8 * nd - 1
+        for x in v:
+            d = digits(x, e, nd)
+            assert all(-128 <= q <= 127 for q in d)
+            m = sum(q * 256 ** (nd - 1 - t) for t, q in enumerate(d))
+            assert m == int(np.rint(np.ldexp(x, fix - e)))
+            assert abs(np.ldexp(float(m), e - fix) - x) <= 2.0 ** (e - fix - 1)
+    # FP32 values within 2^7 of the maximum are exact
+    f = (rng.standard_normal(256)).astype(np.float32)
+    e = headroom_exp(float(np.abs(f).max()))
+    for x in f:
+        if abs(float(x)) >= 2.0 ** (e - 8):
+            m = sum(q * 256 ** (3 - t) for t, q in enumerate(digits(float(x), e, NDA)))
+            assert np.ldexp(float(m), e - (8 * NDA - 1)) == float(x)
 
 
 def test_tile_dot_matches_exact_value():
@@ -72,13 +91,18 @@ def test_tile_dot_matches_exact_value():
         else:
             b = np.cos(np.linspace(0, 60.0, K)) * 1e-3 + 5.0              # cancellation
             a = (a - a.mean()).astype(np.float32)
-        y, groups = tile_dot(a.astype(np.float64), b)
+        y, D = tile_dot(a.astype(np.float64), b)
         ex = exact_dot(a, b)
-        scale = float(np.sum(np.abs(a.astype(np.float64) * b)))
-        assert abs(y - ex) <= 1e-12 * scale, (case, y, ex, scale)
-        assert np.abs(groups).max() < 2 ** 31
+        a64 = a.astype(np.float64)
+        scale = float(np.sum(np.abs(a64 * b)))
+        # rounding of the two fixed points: half a unit of each operand's last digit
+        er, fn = headroom_exp(np.abs(a64).max()), headroom_exp(np.abs(b).max())
+        bound = float(np.sum(np.abs(b)) * 2.0 ** (er - 8 * NDA) + np.sum(np.abs(a64)) * 2.0 ** (fn - 8 * NDB))
+        assert abs(y - ex) <= bound + 1e-15 * scale, (case, y, ex, bound)
+        assert abs(y - ex) <= 1e-10 * scale, (case, y, ex, scale)
+        assert np.abs(D).max() < 2 ** 31
 
 
-def test_group_sums_fit_int32_at_the_cap():
-    # the extreme: every slice at +-127, six pairs in one group, K = 8192
-    assert 6 * 8192 * 127 * 127 < 2 ** 31
+def test_pair_sums_fit_int32_at_the_cap():
+    # the extreme: every digit at -128, K = 8192 (one pair per accumulator column)
+    assert 8192 * 128 * 128 < 2 ** 31
