@@ -799,7 +799,7 @@ struct PcgParams {
   }                    \
   }
 
-// Phase timing (switched on by spx_debug_pcg_timing): CTA 0 adds the globaltimer interval
+// Phase timing of k_pcg_amg and k_pcg_amg_r (switched on by spx_debug_pcg_timing): CTA 0 adds the globaltimer interval
 // since its previous mark to the slot of the phase that just ended (the phase's slowest CTA
 // plus the barrier); read and cleared by pcg_phase_times.  Slots: V-cycle phases in order
 // (3 per level down, the coarse solve, 3 per level up), 28 the PCG product, 29 the update,
@@ -1054,7 +1054,7 @@ __global__ void __launch_bounds__(PCG_BLOCK, PCG_CTAS_PER_SM) k_pcg_amg(PcgParam
 
 // the V-cycle of k_pcg_amg for R identical blocks (same phases and barriers)
 template <class TV, int R>
-__device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
+__device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh, unsigned long long& tm) {
   const unsigned nb = gridDim.x;
   unsigned int* cnt = P.bar;
   unsigned int* gen = P.bar + 1;
@@ -1062,27 +1062,35 @@ __device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
                     static_cast<int64_t>((gridDim.x * static_cast<int64_t>(blockDim.x)) >> 5),
                     static_cast<int>(threadIdx.x & 31)};
   const int NL = P.nlev;
+  int ph = 0;
   for (int l = 0; l + 1 < NL; ++l) {
     const AmgLevelDev& L = P.lv[l];
     pre_a_r<R>(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     pre_b_r<R>(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     restrict_to_r<R>(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
   }
   coarse_solve_r<R>(P.lv[NL - 1], P.cinv, P.nc, P.ldc, rr);
   if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+  pcg_mark(tm, ph++, P.timing);
   for (int l = NL - 2; l >= 0; --l) {
     const AmgLevelDev& L = P.lv[l];
     prolong_from_r<R>(L, P.lv[l + 1], rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     post_c_r<R>(L, rr);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
     double rz = 0.0, wz = 0.0;
     post_d_r<R>(L, rr, P.r, P.sdinv, rz, wz, l == 0);
     if (l == 0) cta_partial(P.part, slot, rz, wz, 0.0, 0.0, sh);
     if (!grid_barrier(cnt, gen, nb, P.err)) return false;
+    pcg_mark(tm, ph++, P.timing);
   }
   return true;
 }
@@ -1094,6 +1102,7 @@ __device__ bool vcycle_r(const PcgParams<TV>& P, int slot, double* sh) {
 // interleaved (i R + r).
 template <class TV, int R>
 __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgParams<TV> P) {
+  unsigned long long tm = 0ull;
   __shared__ double sh[160];
   const unsigned nb = gridDim.x;
   const int lane = threadIdx.x & 31;
@@ -1191,6 +1200,7 @@ __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgP
       PCG_SLICES_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 30, P.timing);
     }
     cta_total(P.part, 0, tot, sh);
     rr = tot[0];
@@ -1198,7 +1208,7 @@ __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgP
     if (rr <= tol2 || total >= P.maxit) break;
     double rz_old = 1.0;
     for (int it = 0;; ++it) {
-      if (!vcycle_r<TV, R>(P, 2, sh)) return;
+      if (!vcycle_r<TV, R>(P, 2, sh, tm)) return;
       cta_total(P.part, 2, tot, sh);
       const double rz = tot[0];
       const double c = P.project && P.ww > 0.0 ? tot[1] / P.ww : 0.0;
@@ -1253,6 +1263,7 @@ __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgP
       PCG_SLICES_END
       cta_partial(P.part, 3, pq, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 28, P.timing);
       cta_total(P.part, 3, tot, sh);
       const double pqt = tot[0];
       if (!(pqt > 0.0) || !(rz > 0.0)) break;
@@ -1275,6 +1286,7 @@ __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgP
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;
+      pcg_mark(tm, 29, P.timing);
       cta_total(P.part, 0, tot, sh);
       rr = tot[0];
       ++total;

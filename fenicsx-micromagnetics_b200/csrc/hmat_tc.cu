@@ -32,12 +32,15 @@
 // stay on k_rows_multi (hmat_multi.cu), which adds this far part.
 //
 // Data path of k_tc_gemm (384 threads, one CTA per SM, persistent over a tile list): an
-// 8-stage ring of A stages (cp.async.bulk, mbarrier transaction counts) and of B digit tiles.
-//   warp 0     : cp.async.bulk of A stages;
+// 8-stage ring; a stage is the A digits (16 KB) and the stage's B rows (FP64, up to 2 KB), both
+// brought by cp.async.bulk onto one mbarrier (transaction counts), and the B digit tile.  Every
+// role loads the next tile's descriptor (and exponents) while it works on the current one.
+//   warp 0     : cp.async.bulk of the A digits and the B rows;
 //   warp 1     : MMA issuer (4 MMAs per stage, tcgen05.commit);
 //   warp 2     : allocates / frees 512 tensor-memory columns (two buffers of 4 x 48 int32);
 //   warps 4-7  : epilogue (TMEM lanes 32 (w % 4) .. + 31) to FP64 partials;
-//   warps 8-11 : cut the B rows of each stage into digits (canonical K-major layout).
+//   warps 8-11 : cut the B rows of each stage (from shared memory) into digits (canonical
+//                K-major layout).
 // Every mbarrier wait is bounded; on a timeout the kernel records SPX_ERR_TIMEOUT, the roles
 // stop, the MMA issuer waits (bounded) for its last commit, and tensor memory is freed.
 //
@@ -101,6 +104,7 @@ constexpr int AD_BYTES = TM * KS;             // one digit plane of an A stage: 
 constexpr int AST_BYTES = NDA * AD_BYTES;     // an A stage: 16 KB (4 bytes per element)
 constexpr int NB = NDB * R;                   // MMA N = 48: column 8 u + n = digit u of state n
 constexpr int BST_BYTES = NB * KS;            // the B digits of a stage: 1.5 KB
+constexpr int BX_BYTES = KS * R * 8;          // the B rows of a stage as copied (FP64): 2 KB
 constexpr int ACOLS = NDA * NB;               // TMEM columns of one accumulator buffer (4 x 48)
 constexpr int TCOLS = 512;                    // allocated TMEM columns (2 buffers of 192)
 constexpr int KSTEP_MAX_DEFAULT = 64;         // stages per tile (2048 K elements)
@@ -108,7 +112,7 @@ constexpr int THREADS = 384;
 constexpr int CONV_THREADS = 128;             // warps 8-11
 // + a 32 KB guard after the buffers, so that no descriptor-addressed read can leave the
 // allocation even past the last stage
-constexpr int SMEM_BYTES = NSTAGE * AST_BYTES + NSTAGE * BST_BYTES + 1024 + 32768;
+constexpr int SMEM_BYTES = NSTAGE * (AST_BYTES + BST_BYTES + BX_BYTES) + 1024 + 32768;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
 static_assert((TM / 8) * 128 * (KS / 16) == AD_BYTES && (NB / 8) * 128 * (KS / 16) == BST_BYTES, "digit tile layouts");
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -208,7 +212,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   extern __shared__ __align__(1024) char smem[];
   char* sA = smem;                                   // [NSTAGE][NDA][AD_BYTES] A digits (as in HBM)
   char* sB = sA + NSTAGE * AST_BYTES;                // [NSTAGE][BST_BYTES]    B digits, N = 48 rows
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + NSTAGE * BST_BYTES);
+  char* sX = sB + NSTAGE * BST_BYTES;                // [NSTAGE][BX_BYTES]     B rows as copied (FP64 [32][8])
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sX + NSTAGE * BX_BYTES);
   uint64_t* full = bars;                 // [NSTAGE] A copied
   uint64_t* ready = bars + NSTAGE;       // [NSTAGE] B digits written
   uint64_t* empty = bars + 2 * NSTAGE;   // [NSTAGE] MMAs done with the stage
@@ -250,16 +255,25 @@ __global__ void __launch_bounds__(THREADS, 1)
   };
 
   if (warp == 0) {
-    if (lane == 0) {  // producer
+    if (lane == 0) {  // producer: A digits and the stage's B rows (FP64) on one mbarrier
       int item = 0;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-        const TcTile T = tiles[t];
+      int t = blockIdx.x;
+      TcTile T;
+      if (t < ntiles) T = tiles[t];
+      for (; t < ntiles && !*abort_flag; t += gridDim.x) {
+        TcTile Tn;
+        if (t + static_cast<int>(gridDim.x) < ntiles) Tn = tiles[t + gridDim.x];  // next tile in flight
         for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
+          const int nb = min(KS, T.b_rows - s0 * KS);  // valid B rows of the stage
           if (!mbar_wait(&empty[st], (rnd & 1) ^ 1)) { fail(); break; }
-          mbar_expect_tx(&full[st], AST_BYTES);
+          mbar_expect_tx(&full[st], AST_BYTES + (nb > 0 ? nb * R * 8 : 0));
           bulk_g2s(sA + st * AST_BYTES, A + T.a_off + static_cast<int64_t>(s0) * AST_BYTES, AST_BYTES, &full[st]);
+          if (nb > 0)
+            bulk_g2s(sX + st * BX_BYTES, bsrc + (static_cast<int64_t>(T.b_row0) + s0 * KS) * R, nb * R * 8,
+                     &full[st]);
         }
+        T = Tn;
       }
       // leave no copy in flight: the last stages' copies have landed (bounded)
       for (int q = max(0, item - NSTAGE); q < item; ++q) mbar_wait(&full[q % NSTAGE], (q / NSTAGE) & 1);
@@ -268,14 +282,16 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (lane == 0) {  // MMA issuer
       int item = 0, tc = 0;
       bool issued = false;
-      for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tc) {
-        const TcTile T = tiles[t];
+      int t = blockIdx.x;
+      int ns = t < ntiles ? tiles[t].nsteps : 0;
+      for (; t < ntiles && !*abort_flag; t += gridDim.x, ++tc) {
+        const int nsn = t + static_cast<int>(gridDim.x) < ntiles ? tiles[t + gridDim.x].nsteps : 0;
         const int buf = tc & 1, use = tc >> 1;
         if (!mbar_wait(&acce[buf], (use & 1) ^ 1)) { fail(); break; }
         tc_after();
         const uint32_t d0 = tbase + static_cast<uint32_t>(buf * ACOLS);
         bool ok = true;
-        for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
+        for (int s0 = 0; s0 < ns; ++s0, ++item) {
           const int st = item % NSTAGE, rnd = item / NSTAGE;
           if (!mbar_wait(&full[st], rnd & 1) || !mbar_wait(&ready[st], rnd & 1)) { fail(); ok = false; break; }
           tc_after();
@@ -290,6 +306,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         if (!ok) break;
         mma_commit(&accf[buf]);
+        ns = nsn;
       }
       if (issued) {  // every MMA of this CTA has completed before tensor memory is freed
         mma_commit(fin);
@@ -298,11 +315,17 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
   } else if (warp >= 4 && warp < 8) {  // epilogue: TMEM lanes 32 (warp % 4) .. + 31
     const int sp = warp & 3;
+    const int row = 32 * sp + lane;
     // 256^(8 - g) for the digit-pair weight g = t + u (exact powers of two)
     const double wgt[NDA + NDB - 1] = {0x1p64, 0x1p56, 0x1p48, 0x1p40, 0x1p32, 0x1p24, 0x1p16, 0x1p8, 1.0};
     int tc = 0;
     for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tc) {
+      // the tile's exponents are loaded while its accumulators are being computed
       const TcTile T = tiles[t];
+      const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
+      int en[R];
+#pragma unroll
+      for (int n = 0; n < R; ++n) en[n] = eb[static_cast<int64_t>(T.bsc) * R + n];
       const int buf = tc & 1, use = tc >> 1;
       if (!mbar_wait(&accf[buf], use & 1)) { fail(); break; }
       tc_after();
@@ -323,30 +346,40 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       tc_before();
       mbar_arrive(&acce[buf]);
-      const int row = 32 * sp + lane;
-      const int er = ea[static_cast<int64_t>(T.slot) * TM + row];
       double* o = part + (static_cast<int64_t>(T.slot) * TM + row) * R;
 #pragma unroll
-      for (int n = 0; n < R; ++n) o[n] = ldexp(y[n], er + eb[static_cast<int64_t>(T.bsc) * R + n] - FIXA - FIXB);
+      for (int n = 0; n < R; ++n) o[n] = ldexp(y[n], er + en[n] - FIXA - FIXB);
     }
-  } else if (warp >= 8) {  // B digits: thread -> (state n, two k); rows 8 u + n of the N = 32 tile
+  } else if (warp >= 8) {  // B digits: thread -> (state n, two k); rows 8 u + n of the N = 48 tile
     const int ct = tid - (THREADS - CONV_THREADS);
     const int n = ct >> 4, k0 = (ct & 15) * 2;
     int item = 0;
-    for (int t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-      const TcTile T = tiles[t];
-      const int e = eb[static_cast<int64_t>(T.bsc) * R + n];
+    int t = blockIdx.x;
+    TcTile T;
+    int e = 0;
+    if (t < ntiles) {
+      T = tiles[t];
+      e = eb[static_cast<int64_t>(T.bsc) * R + n];
+    }
+    for (; t < ntiles && !*abort_flag; t += gridDim.x) {
+      TcTile Tn;
+      int en = 0;
+      if (t + static_cast<int>(gridDim.x) < ntiles) {  // next tile and its exponent in flight
+        Tn = tiles[t + gridDim.x];
+        en = eb[static_cast<int64_t>(Tn.bsc) * R + n];
+      }
       bool ok = true;
       for (int s0 = 0; s0 < T.nsteps; ++s0, ++item) {
         const int st = item % NSTAGE, rnd = item / NSTAGE;
-        // the stage's previous MMAs are done, so its B digits may be overwritten
-        if (!mbar_wait(&empty[st], (rnd & 1) ^ 1)) { fail(); ok = false; break; }
+        // the stage's copies have landed, so its previous MMAs are done and the digits are free
+        if (!mbar_wait(&full[st], rnd & 1)) { fail(); ok = false; break; }
+        const double* xs = reinterpret_cast<const double*>(sX + st * BX_BYTES);
         char* bs = sB + st * BST_BYTES;
+        const int nb = T.b_rows - s0 * KS;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int k = k0 + j;
-          const int kk = s0 * KS + k;
-          const double x = kk < T.b_rows ? bsrc[(static_cast<int64_t>(T.b_row0) + kk) * R + n] : 0.0;
+          const double x = k < nb ? xs[k * R + n] : 0.0;
           int8_t c[NDB];
           digits<NDB>(x, e, c);
 #pragma unroll
@@ -356,6 +389,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         mbar_arrive(&ready[st]);
       }
       if (!ok) break;
+      T = Tn;
+      e = en;
     }
   }
   tc_before();
@@ -399,48 +434,64 @@ __global__ void k_tc_bexp(int nr, const int64_t* __restrict__ rng, const double*
   }
 }
 
-// A digits of one tile: stage s holds digit planes t = 0..3, each the rows 0..127 x K elements
+// The FP32 value of element (row r, K index k) of pack job J (0 past the valid rows / K).
+__device__ __forceinline__ float tc_value(const TcPack& J, int r, int k, const double* __restrict__ pool,
+                                          const int64_t* __restrict__ rowbase, const int64_t* __restrict__ colbase) {
+  double v = 0.0;
+  if (r < J.rvalid && k < J.kvalid) {
+    if (J.mode == 1) {
+      const int64_t b = rowbase[J.tab + r];
+      if (b >= 0) v = pool[b + J.roff + k];
+    } else {
+      const int64_t c = colbase[J.tab + k];
+      if (c >= 0) v = pool[c + J.roff + r];
+    }
+  }
+  return static_cast<float>(v);
+}
+
+// Row maxima of the pack jobs: one CTA per (job, stage) of the flat stage list js, a thread per
+// row; amax[slot][r] holds the bits of the largest |FP32 value| (non-negative floats order like
+// their bit patterns), zeroed before.
+__global__ void k_tc_rowmax(const TcPack* __restrict__ jobs, const int2* __restrict__ js,
+                            const double* __restrict__ pool, const int64_t* __restrict__ rowbase,
+                            const int64_t* __restrict__ colbase, unsigned int* __restrict__ amax) {
+  const int2 q = js[blockIdx.x];
+  const TcPack J = jobs[q.x];
+  const int r = threadIdx.x;  // 128 threads
+  float mx = 0.0f;
+#pragma unroll 4
+  for (int j = 0; j < KS; ++j) mx = fmaxf(mx, fabsf(tc_value(J, r, q.y * KS + j, pool, rowbase, colbase)));
+  if (mx > 0.0f) atomicMax(amax + static_cast<int64_t>(J.slot) * TM + r, __float_as_uint(mx));
+}
+
+// A digits of one stage of a pack job: digit planes t = 0..3, each the rows 0..127 x K elements
 // 32 s .. 32 s + 31 in the K-major no-swizzle layout of the MMA; ea[slot][r] = the exponent of row
 // r's largest |value| over the tile.  The values are the FP32 factors (the FP32 packing's
-// rounding).  One CTA per tile, a thread per row.
-__global__ void k_tc_pack(const TcPack* __restrict__ jobs, int njobs, const double* __restrict__ pool,
-                          const int64_t* __restrict__ rowbase, const int64_t* __restrict__ colbase,
+// rounding).  One CTA per (job, stage), a thread per row.
+__global__ void k_tc_pack(const TcPack* __restrict__ jobs, const int2* __restrict__ js,
+                          const double* __restrict__ pool, const int64_t* __restrict__ rowbase,
+                          const int64_t* __restrict__ colbase, const unsigned int* __restrict__ amax,
                           char* __restrict__ A, int32_t* __restrict__ ea) {
-  const TcPack J = jobs[blockIdx.x];
+  const int2 q = js[blockIdx.x];
+  const TcPack J = jobs[q.x];
   const int r = threadIdx.x;  // 128 threads
-  const int K = J.nsteps * KS;
-  int64_t b = -1;
-  if (r < J.rvalid && J.mode == 1) b = rowbase[J.tab + r];
-  auto value = [&](int k) -> float {
-    double v = 0.0;
-    if (r < J.rvalid && k < J.kvalid) {
-      if (J.mode == 1) {
-        if (b >= 0) v = pool[b + J.roff + k];
-      } else {
-        const int64_t c = colbase[J.tab + k];
-        if (c >= 0) v = pool[c + J.roff + r];
-      }
-    }
-    return static_cast<float>(v);
-  };
-  double mx = 0.0;
-  for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(static_cast<double>(value(k))));
-  const int e = headroom_exp(mx);
-  char* dst = A + J.a_off;
-  for (int k = 0; k < K; k += 4) {  // four K elements -> one 32-bit word per digit plane
+  const int e = headroom_exp(static_cast<double>(__uint_as_float(amax[static_cast<int64_t>(J.slot) * TM + r])));
+  char* st = A + J.a_off + static_cast<int64_t>(q.y) * AST_BYTES;
+  for (int k = 0; k < KS; k += 4) {  // four K elements -> one 32-bit word per digit plane
     uint32_t w[NDA] = {0u, 0u, 0u, 0u};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       int8_t d[NDA];
-      digits<NDA>(static_cast<double>(value(k + j)), e, d);
+      digits<NDA>(static_cast<double>(tc_value(J, r, q.y * KS + k + j, pool, rowbase, colbase)), e, d);
 #pragma unroll
       for (int t = 0; t < NDA; ++t) w[t] |= static_cast<uint32_t>(static_cast<uint8_t>(d[t])) << (8 * j);
     }
-    char* st = dst + static_cast<int64_t>(k >> 5) * AST_BYTES + i8off(r, k & 31, (TM / 8) * 128);
+    char* o = st + i8off(r, k, (TM / 8) * 128);
 #pragma unroll
-    for (int t = 0; t < NDA; ++t) *reinterpret_cast<uint32_t*>(st + t * AD_BYTES) = w[t];
+    for (int t = 0; t < NDA; ++t) *reinterpret_cast<uint32_t*>(o + t * AD_BYTES) = w[t];
   }
-  ea[static_cast<int64_t>(J.slot) * TM + r] = e;
+  if (q.y == 0) ea[static_cast<int64_t>(J.slot) * TM + r] = e;
 }
 
 }  // namespace tc
@@ -601,17 +652,27 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
     DevBuf<int64_t> drb, dcb;
     drb.upload(rowbase.empty() ? std::vector<int64_t>{-1} : rowbase, s);
     dcb.upload(colbase.empty() ? std::vector<int64_t>{-1} : colbase, s);
-    auto run = [&](const std::vector<TcPack>& jobs, char* dst, int32_t* ea) {
+    auto run = [&](const std::vector<TcPack>& jobs, char* dst, int32_t* ea, int64_t nslots) {
       if (jobs.empty()) return;
+      std::vector<int2> js;
+      for (size_t j = 0; j < jobs.size(); ++j)
+        for (int st = 0; st < jobs[j].nsteps; ++st) js.push_back(make_int2(static_cast<int>(j), st));
       DevBuf<TcPack> dj;
       dj.upload(jobs, s);
-      k_tc_pack<<<static_cast<unsigned>(jobs.size()), TM, 0, s>>>(dj.p, static_cast<int>(jobs.size()),
-                                                                 H.far_pool64.p, drb.p, dcb.p, dst, ea);
+      DevBuf<int2> djs;
+      djs.upload(js, s);
+      DevBuf<unsigned int> amax;
+      amax.alloc(nslots * TM);
+      amax.zero(s);
+      const unsigned g = static_cast<unsigned>(js.size());
+      k_tc_rowmax<<<g, TM, 0, s>>>(dj.p, djs.p, H.far_pool64.p, drb.p, dcb.p, amax.p);
+      SPX_LAUNCH_CHECK();
+      k_tc_pack<<<g, TM, 0, s>>>(dj.p, djs.p, H.far_pool64.p, drb.p, dcb.p, amax.p, dst, ea);
       SPX_LAUNCH_CHECK();
       SPX_CUDA(cudaStreamSynchronize(s));
     };
-    run(p1, P->A1.p, P->ea1.p);
-    run(p2, P->A2.p, P->ea2.p);
+    run(p1, P->A1.p, P->ea1.p, slot1);
+    run(p2, P->A2.p, P->ea2.p, slot2);
   }
   Csr c1 = make_csr(zlen, m1), c2 = make_csr(H.Nb, m2);
   P->rp1.upload(c1.rp, s);
