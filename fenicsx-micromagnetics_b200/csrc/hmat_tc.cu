@@ -114,6 +114,7 @@ constexpr int CONV_THREADS = 128;             // warps 8-11
 // allocation even past the last stage
 constexpr int SMEM_BYTES = NSTAGE * (AST_BYTES + BST_BYTES + BX_BYTES) + 1024 + 32768;
 constexpr long long WAIT_LIMIT = 1ll << 22;  // polls of try_wait before a wait gives up
+static_assert(NDB == 6, "digits6 cuts the B rows");
 static_assert((TM / 8) * 128 * (KS / 16) == AD_BYTES && (NB / 8) * 128 * (KS / 16) == BST_BYTES, "digit tile layouts");
 __device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -197,6 +198,34 @@ __device__ __forceinline__ void digits(double v, int e, int8_t (&d)[ND]) {
     d[t] = static_cast<int8_t>(s);
     m = (m - s) >> 8;
   }
+}
+
+// 2^k as a double, -1022 <= k <= 1023 (exponent bits)
+__device__ __forceinline__ double pow2i(int k) { return __longlong_as_double(static_cast<long long>(k + 1023) << 52); }
+
+// digits<6>(v, e, d) for the B rows of every stage, in 32-bit integer steps: the 47-bit value
+// m = hi 2^24 + lo (lo in [0, 2^24)) gives three balanced digits of lo, whose carry (0 or 1)
+// goes into hi, and three of hi.  The digits are those of digits<6>.
+__device__ __forceinline__ void digits6(double v, int e, int8_t (&d)[6]) {
+  const int k = FIXB - e;
+  const double sv = (k >= -1022 && k <= 1023) ? v * pow2i(k) : ldexp(v, k);
+  const long long m = __double2ll_rn(sv);  // |m| <= 2^46
+  int lo = static_cast<int>(m & 0xFFFFFF);
+  int hi = static_cast<int>(m >> 24);      // |hi| <= 2^22
+#pragma unroll
+  for (int t = 5; t >= 3; --t) {
+    const int q = static_cast<int>(static_cast<int8_t>(lo & 255));
+    d[t] = static_cast<int8_t>(q);
+    lo = (lo - q) >> 8;
+  }
+  hi += lo;
+#pragma unroll
+  for (int t = 2; t >= 1; --t) {
+    const int q = static_cast<int>(static_cast<int8_t>(hi & 255));
+    d[t] = static_cast<int8_t>(q);
+    hi = (hi - q) >> 8;
+  }
+  d[0] = static_cast<int8_t>(hi);
 }
 
 // byte offset of element (row, k) of a K-major no-swizzle int8 tile of 32 K columns:
@@ -381,7 +410,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           const int k = k0 + j;
           const double x = k < nb ? xs[k * R + n] : 0.0;
           int8_t c[NDB];
-          digits<NDB>(x, e, c);
+          digits6(x, e, c);
 #pragma unroll
           for (int u = 0; u < NDB; ++u) bs[i8off(8 * u + n, k, (NB / 8) * 128)] = static_cast<char>(c[u]);
         }

@@ -106,3 +106,37 @@ def test_tile_dot_matches_exact_value():
 def test_pair_sums_fit_int32_at_the_cap():
     # the extreme: every digit at -128, K = 8192 (one pair per accumulator column)
     assert 8192 * 128 * 128 < 2 ** 31
+
+
+def digits6_split(v, e):
+    """The kernel's 32-bit form of digits(v, e, 6): m = hi 2^24 + lo, three balanced digits of
+    lo, the carry into hi, three digits of hi."""
+    m = int(np.rint(np.ldexp(float(v), 8 * NDB - 1 - e)))
+    lo, hi = m & 0xFFFFFF, m >> 24
+    d = [0] * 6
+    for t in (5, 4, 3):
+        q = ((lo & 255) ^ 128) - 128
+        d[t] = q
+        lo = (lo - q) >> 8
+    assert lo in (0, 1)
+    hi += lo
+    for t in (2, 1):
+        q = ((hi & 255) ^ 128) - 128
+        d[t] = q
+        hi = (hi - q) >> 8
+    d[0] = hi
+    return d
+
+
+def test_split_digits_equal_the_generic_ones():
+    rng = np.random.default_rng(3)
+    v = np.concatenate([rng.standard_normal(2000) * 10.0 ** rng.uniform(-6, 0, 2000), [0.0, 1.0, -1.0]])
+    e = headroom_exp(np.abs(v).max())
+    for x in v:
+        d = digits6_split(x, e)
+        assert d == digits(x, e, NDB)
+        assert all(-128 <= q <= 127 for q in d)
+    # the extremes of the 47-bit range
+    for m in (2 ** 46, -2 ** 46, 2 ** 46 - 1, -(2 ** 46 - 1), 2 ** 24 - 1, -(2 ** 24)):
+        x = np.ldexp(float(m), 1 - (8 * NDB - 1))  # e = 1
+        assert digits6_split(x, 1) == digits(x, 1, NDB)
