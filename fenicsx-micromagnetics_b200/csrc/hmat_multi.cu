@@ -284,6 +284,123 @@ __global__ void __launch_bounds__(MROWS_WARPS * 32) k_rows_multi(
   }
 }
 
+// Near field of 8 states for the tensor-core path (whose far part arrives in yinit): one CTA
+// per row segment (<= 64 rows, leaf near blocks of <= 64 columns per item), 256 threads.  Each
+// near tile (len x ld elements, column q of the block = ld consecutive entries) and its 8 x len
+// states are staged in shared memory by coalesced 16-byte loads; the next item's loads are in
+// flight (registers) while the current one is summed from shared memory.  Thread t sums row
+// t / 4 for states t % 4 and t % 4 + 4 (FP64), then adds the diagonal and the far part and
+// scatters like k_rows_multi.
+constexpr int NEAR_THREADS = 256;
+constexpr int NEAR_COLS = 64;                      // columns staged per round
+template <class TN>
+struct NearStage {
+  static constexpr int TILE = NEAR_COLS * MSEG;    // elements of a staged tile
+  static constexpr int BYTES = TILE * sizeof(TN) + NEAR_COLS * 8 * sizeof(double);
+  static constexpr int V16N = TILE * sizeof(TN) / 16;  // 16-byte vectors of a full tile
+  static constexpr int PER = (V16N + NEAR_THREADS - 1) / NEAR_THREADS;
+  static_assert(NEAR_COLS * 4 == NEAR_THREADS, "one double2 of the staged states per thread");
+};
+
+template <class TN, class TD>
+__global__ void __launch_bounds__(NEAR_THREADS) k_near_multi(
+    const int32_t* __restrict__ seg_start, const int64_t* __restrict__ item_ptr,
+    const int64_t* __restrict__ near_begin, const RowItem* __restrict__ items, const TN* __restrict__ Nt,
+    const double* __restrict__ xm, const double* __restrict__ diag, const int32_t* __restrict__ perm,
+    const int32_t* __restrict__ gidx, Offs goff, TD* __restrict__ dst, const TD* __restrict__ add,
+    TD* __restrict__ yb, Offs yoff, const double* __restrict__ yinit) {
+  constexpr int R = 8;
+  constexpr int E = W16<TN>::E;
+  using S = NearStage<TN>;
+  extern __shared__ __align__(16) char near_smem[];
+  const int sgm = blockIdx.x;
+  const int r0 = seg_start[sgm], nr = seg_start[sgm + 1] - r0;
+  const int nvec = (nr + E - 1) / E, ld = nvec * E;
+  const int tid = threadIdx.x, row = tid >> 2, rq = tid & 3;
+  const int64_t ib = near_begin[sgm], ie = item_ptr[sgm + 1];
+  // work units: (item, column chunk of NEAR_COLS)
+  auto chunks = [&](int64_t it) { return (items[it].len + NEAR_COLS - 1) / NEAR_COLS; };
+  int4 rv[S::PER];
+  double2 rx;
+  auto fetch = [&](int64_t it, int ch) {  // registers <- the chunk's tile vectors and states
+    const RowItem I = items[it];
+    const int c0 = ch * NEAR_COLS, nc = min(NEAR_COLS, I.len - c0);
+    const int nv = nc * ld * static_cast<int>(sizeof(TN)) / 16;
+    const int4* src = reinterpret_cast<const int4*>(Nt + I.off + static_cast<int64_t>(c0) * ld);
+#pragma unroll
+    for (int p = 0; p < S::PER; ++p) {
+      const int v = tid + p * NEAR_THREADS;
+      rv[p] = v < nv ? src[v] : make_int4(0, 0, 0, 0);
+    }
+    const double2* xs = reinterpret_cast<const double2*>(xm + (static_cast<int64_t>(I.src) + c0) * R);
+    rx = tid < nc * 4 ? xs[tid] : make_double2(0.0, 0.0);  // nc x 8 doubles = nc x 4 double2
+    return nc;
+  };
+  auto stash = [&](int buf) {
+    char* b = near_smem + buf * S::BYTES;
+    int4* tv = reinterpret_cast<int4*>(b);
+#pragma unroll
+    for (int p = 0; p < S::PER; ++p) {
+      const int v = tid + p * NEAR_THREADS;
+      if (v < S::V16N) tv[v] = rv[p];
+    }
+    reinterpret_cast<double2*>(b + S::TILE * sizeof(TN))[tid] = rx;
+  };
+  double a0 = 0.0, a1 = 0.0;
+  int64_t it = ib;
+  int ch = 0, nch = it < ie ? chunks(it) : 0;
+  int ncur = 0, buf = 0;
+  if (it < ie) {
+    ncur = fetch(it, ch);
+    stash(0);
+  }
+  __syncthreads();
+  while (it < ie) {
+    // the next unit's loads in flight while this one is summed
+    int64_t itn = it;
+    int chn = ch + 1, nchn = nch;
+    if (chn >= nch) {
+      ++itn;
+      chn = 0;
+      nchn = itn < ie ? chunks(itn) : 0;
+    }
+    int nnext = 0;
+    if (itn < ie) nnext = fetch(itn, chn);
+    const char* b = near_smem + buf * S::BYTES;
+    const TN* tl = reinterpret_cast<const TN*>(b);
+    const double* xs = reinterpret_cast<const double*>(b + S::TILE * sizeof(TN));
+    if (row < nr) {
+#pragma unroll 4
+      for (int q = 0; q < ncur; ++q) {
+        const double a = static_cast<double>(tl[q * ld + row]);
+        a0 += a * xs[q * R + rq];
+        a1 += a * xs[q * R + rq + 4];
+      }
+    }
+    if (itn < ie) stash(buf ^ 1);
+    __syncthreads();
+    buf ^= 1;
+    it = itn;
+    ch = chn;
+    nch = nchn;
+    ncur = nnext;
+  }
+  if (row < nr) {
+    const int64_t i = r0 + row;
+    const int32_t b = perm[i];
+    const double dg = diag[i];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = rq + 4 * h;
+      const double y = dg * xm[i * R + r] + yinit[i * R + r] + (h ? a1 : a0);
+      const int64_t o = gidx ? static_cast<int64_t>(gidx[goff.v[r] + b]) : goff.v[r] + b;
+      const TD yv = static_cast<TD>(y);
+      dst[o] = add ? static_cast<TD>(add[o] + yv) : yv;
+      if (yb) yb[yoff.v[r] + b] = yv;
+    }
+  }
+}
+
 template <class TF, class TN, class TS, int R>
 void launch_multi(HMatrix& H, const TS* src, const int32_t* gidx, const int64_t* goff, TS* dst, const TS* add,
                   TS* yb, const int64_t* yoff, cudaStream_t s) {
@@ -301,10 +418,12 @@ void launch_multi(HMatrix& H, const TS* src, const int32_t* gidx, const int64_t*
   SPX_LAUNCH_CHECK();
   if (R == 8 && H.tc) {  // far field on the tensor cores, then near field + diagonal + scatter
     const double* yfar = tc_far_apply(H, H.xmulti.p, s);
-    k_rows_multi<TF, TN, TS, R><<<static_cast<unsigned>(H.nseg), MROWS_WARPS * 32, 0, s>>>(
-        H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TF*>(H.far_f.p),
-        reinterpret_cast<const TN*>(H.near_f.p), H.zmulti.p, H.xmulti.p, H.diag_perm.p, H.perm.p, gidx, g, dst, add,
-        yb, y, yfar, 1);
+    constexpr int smem = 2 * NearStage<TN>::BYTES;
+    static_assert(smem <= 160 * 1024, "near-field staging");
+    SPX_CUDA(cudaFuncSetAttribute(k_near_multi<TN, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_near_multi<TN, TS><<<static_cast<unsigned>(H.nseg), NEAR_THREADS, smem, s>>>(
+        H.seg_start.p, H.item_ptr.p, H.near_begin.p, H.items.p, reinterpret_cast<const TN*>(H.near_f.p),
+        H.xmulti.p, H.diag_perm.p, H.perm.p, gidx, g, dst, add, yb, y, yfar);
     SPX_LAUNCH_CHECK();
     return;
   }
