@@ -710,28 +710,33 @@ __device__ void post_d_r(const AmgLevelDev& L, RowRange rr, const double* __rest
 }
 
 // dense coarsest level for R blocks (interleaved vectors; b entries past nc are taken as 0)
+// the right-hand sides of the dense coarsest level, transposed to [R][nc], for k_pcg_amg_r's
+// coarse phase (dynamic shared memory of nc x R floats)
+extern __shared__ float pcg_coarse_smem[];
+
+// dense coarsest level for R blocks (interleaved vectors): the CTA stages the R right-hand
+// sides in shared memory ([R][nc], one coalesced pass), then a warp per row of the inverse
+// reads the row once (L2 evict_last policy, coalesced) against all R of them
 template <int R>
 __device__ void coarse_solve_r(const AmgLevelDev& L, const float* __restrict__ cinv, int64_t nc, int64_t ldc,
                                RowRange rr) {
-  const int64_t nv = ldc / 4;
+  float* sb = pcg_coarse_smem;
+  for (int64_t e = threadIdx.x; e < nc * R; e += blockDim.x) {
+    const int64_t j = e / R;
+    sb[(e - j * R) * nc + j] = L.b[e];
+  }
+  __syncthreads();
+  const uint64_t pol = l2_policy_keep();  // the inverse stays in L2 across iterations
   for (int64_t i = rr.gw; i < nc; i += rr.nw) {
-    const float4* row = reinterpret_cast<const float4*>(cinv + i * ldc);
+    const float* row = cinv + i * ldc;
     float s[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) s[r] = 0.0f;
-    for (int64_t j = rr.lane; j < nv; j += 32) {
-      const float4 c = row[j];
-      const float cq[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll 4
+    for (int64_t j = rr.lane; j < nc; j += 32) {
+      const float c = ld_hint(row + j, pol);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t jj = 4 * j + q;
-        if (jj < nc) {
-          float g[R];
-          load_r<R>(L.b, jj, g);
-#pragma unroll
-          for (int r = 0; r < R; ++r) s[r] += cq[q] * g[r];
-        }
-      }
+      for (int r = 0; r < R; ++r) s[r] += c * sb[r * nc + j];
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -1404,7 +1409,18 @@ void CgSystem<TM>::enable_amg(const HostSell& hs, const std::vector<int64_t>& ro
     const void* kr = reps == 2 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 2>)
                      : reps == 4 ? reinterpret_cast<const void*>(k_pcg_amg_r<double, 4>)
                                  : reinterpret_cast<const void*>(k_pcg_amg_r<double, 8>);
-    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK_R, 0));
+    // the coarse phase stages the R right-hand sides in dynamic shared memory
+    const size_t dyn = static_cast<size_t>(amg->nc) * reps * sizeof(float);
+    SPX_CHECK(dyn <= 200 * 1024, "AMG coarsest level too large for the repeated-block kernel");
+    const void* kall[] = {reinterpret_cast<const void*>(k_pcg_amg_r<double, 2>),
+                          reinterpret_cast<const void*>(k_pcg_amg_r<double, 4>),
+                          reinterpret_cast<const void*>(k_pcg_amg_r<double, 8>),
+                          reinterpret_cast<const void*>(k_pcg_amg_r<float, 2>),
+                          reinterpret_cast<const void*>(k_pcg_amg_r<float, 4>),
+                          reinterpret_cast<const void*>(k_pcg_amg_r<float, 8>)};
+    for (const void* kk : kall)
+      SPX_CUDA(cudaFuncSetAttribute(kk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(dyn)));
+    SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr, PCG_BLOCK_R, dyn));
     SPX_CHECK(per_sm >= PCG_CTAS_PER_SM, "AMG PCG kernel (repeated blocks) cannot be resident");
   }
   int dev;
@@ -1442,7 +1458,8 @@ void CgSystem<TM>::launch_amg(const TV* b, TV* x, double rtol, double atol, int 
   if (reps == 2) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 2>);
   if (reps == 4) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 4>);
   if (reps == 8) k = reinterpret_cast<void*>(k_pcg_amg_r<TV, 8>);
-  SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(reps > 1 ? PCG_BLOCK_R : PCG_BLOCK), args, 0, st));
+  const size_t dyn = reps > 1 ? static_cast<size_t>(amg->nc) * reps * sizeof(float) : 0;
+  SPX_CUDA(cudaLaunchCooperativeKernel(k, dim3(amg_grid), dim3(reps > 1 ? PCG_BLOCK_R : PCG_BLOCK), args, dyn, st));
 }
 
 // per-slot sums (ns) and counts of the phase timing marks since the last call

@@ -285,22 +285,44 @@ __global__ void __launch_bounds__(MROWS_WARPS * 32) k_rows_multi(
 }
 
 // Near field of 8 states for the tensor-core path (whose far part arrives in yinit): one CTA
-// per row segment (<= 64 rows, leaf near blocks of <= 64 columns per item), 256 threads.  Each
-// near tile (len x ld elements, column q of the block = ld consecutive entries) and its 8 x len
-// states are staged in shared memory by coalesced 16-byte loads; the next item's loads are in
-// flight (registers) while the current one is summed from shared memory.  Thread t sums row
-// t / 4 for states t % 4 and t % 4 + 4 (FP64), then adds the diagonal and the far part and
+// of 64 threads per row segment (<= 64 rows; leaf near blocks, staged 64 columns at a time).
+// Each near tile (nc x ld elements: column q of the block is ld consecutive entries) and its
+// nc x 8 states go to shared memory by cp.async (16-byte copies), double-buffered so that the
+// next item's copies are in flight while the current one is summed.  Thread t sums rows
+// 2 (t / 2), 2 (t / 2) + 1 for states 4 (t % 2) .. + 3 (eight FP64 accumulators, one float2 and
+// two double2 shared-memory loads per column), then adds the diagonal and the far part and
 // scatters like k_rows_multi.
-constexpr int NEAR_THREADS = 256;
+constexpr int NEAR_THREADS = 64;
 constexpr int NEAR_COLS = 64;                      // columns staged per round
 template <class TN>
 struct NearStage {
   static constexpr int TILE = NEAR_COLS * MSEG;    // elements of a staged tile
-  static constexpr int BYTES = TILE * sizeof(TN) + NEAR_COLS * 8 * sizeof(double);
-  static constexpr int V16N = TILE * sizeof(TN) / 16;  // 16-byte vectors of a full tile
-  static constexpr int PER = (V16N + NEAR_THREADS - 1) / NEAR_THREADS;
-  static_assert(NEAR_COLS * 4 == NEAR_THREADS, "one double2 of the staged states per thread");
+  static constexpr int XOFF = TILE * sizeof(TN);   // byte offset of the staged states
+  static constexpr int BYTES = XOFF + NEAR_COLS * 8 * sizeof(double);
 };
+
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <class TN>
+__device__ __forceinline__ void near_pair(const TN* t, double& a0, double& a1);
+template <>
+__device__ __forceinline__ void near_pair<float>(const float* t, double& a0, double& a1) {
+  const float2 v = *reinterpret_cast<const float2*>(t);
+  a0 = v.x;
+  a1 = v.y;
+}
+template <>
+__device__ __forceinline__ void near_pair<double>(const double* t, double& a0, double& a1) {
+  const double2 v = *reinterpret_cast<const double2*>(t);
+  a0 = v.x;
+  a1 = v.y;
+}
 
 template <class TN, class TD>
 __global__ void __launch_bounds__(NEAR_THREADS) k_near_multi(
@@ -315,84 +337,71 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_multi(
   extern __shared__ __align__(16) char near_smem[];
   const int sgm = blockIdx.x;
   const int r0 = seg_start[sgm], nr = seg_start[sgm + 1] - r0;
-  const int nvec = (nr + E - 1) / E, ld = nvec * E;
-  const int tid = threadIdx.x, row = tid >> 2, rq = tid & 3;
+  const int ld = (nr + E - 1) / E * E;
+  const int tid = threadIdx.x, rp = 2 * (tid >> 1), sq = 4 * (tid & 1);
   const int64_t ib = near_begin[sgm], ie = item_ptr[sgm + 1];
-  // work units: (item, column chunk of NEAR_COLS)
-  auto chunks = [&](int64_t it) { return (items[it].len + NEAR_COLS - 1) / NEAR_COLS; };
-  int4 rv[S::PER];
-  double2 rx;
-  auto fetch = [&](int64_t it, int ch) {  // registers <- the chunk's tile vectors and states
+  // issue the copies of (item it, column chunk ch) into buffer buf; returns its column count
+  auto issue = [&](int64_t it, int ch, int buf) {
     const RowItem I = items[it];
     const int c0 = ch * NEAR_COLS, nc = min(NEAR_COLS, I.len - c0);
+    char* b = near_smem + buf * S::BYTES;
     const int nv = nc * ld * static_cast<int>(sizeof(TN)) / 16;
-    const int4* src = reinterpret_cast<const int4*>(Nt + I.off + static_cast<int64_t>(c0) * ld);
-#pragma unroll
-    for (int p = 0; p < S::PER; ++p) {
-      const int v = tid + p * NEAR_THREADS;
-      rv[p] = v < nv ? src[v] : make_int4(0, 0, 0, 0);
-    }
-    const double2* xs = reinterpret_cast<const double2*>(xm + (static_cast<int64_t>(I.src) + c0) * R);
-    rx = tid < nc * 4 ? xs[tid] : make_double2(0.0, 0.0);  // nc x 8 doubles = nc x 4 double2
+    const char* src = reinterpret_cast<const char*>(Nt + I.off + static_cast<int64_t>(c0) * ld);
+    for (int v = tid; v < nv; v += NEAR_THREADS) cp16(b + 16 * v, src + 16 * static_cast<int64_t>(v));
+    const char* xs = reinterpret_cast<const char*>(xm + (static_cast<int64_t>(I.src) + c0) * R);
+    for (int v = tid; v < nc * 4; v += NEAR_THREADS) cp16(b + S::XOFF + 16 * v, xs + 16 * static_cast<int64_t>(v));
+    cp_commit();
     return nc;
   };
-  auto stash = [&](int buf) {
-    char* b = near_smem + buf * S::BYTES;
-    int4* tv = reinterpret_cast<int4*>(b);
+  double acc[2][4];
 #pragma unroll
-    for (int p = 0; p < S::PER; ++p) {
-      const int v = tid + p * NEAR_THREADS;
-      if (v < S::V16N) tv[v] = rv[p];
-    }
-    reinterpret_cast<double2*>(b + S::TILE * sizeof(TN))[tid] = rx;
-  };
-  double a0 = 0.0, a1 = 0.0;
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) acc[h][s] = 0.0;
   int64_t it = ib;
-  int ch = 0, nch = it < ie ? chunks(it) : 0;
-  int ncur = 0, buf = 0;
-  if (it < ie) {
-    ncur = fetch(it, ch);
-    stash(0);
-  }
-  __syncthreads();
+  int ch = 0, buf = 0, ncur = 0;
+  if (it < ie) ncur = issue(it, 0, 0);
   while (it < ie) {
-    // the next unit's loads in flight while this one is summed
+    // the next unit: the next column chunk of this item, or the next item
     int64_t itn = it;
-    int chn = ch + 1, nchn = nch;
-    if (chn >= nch) {
+    int chn = ch + 1;
+    if (chn * NEAR_COLS >= items[it].len) {
       ++itn;
       chn = 0;
-      nchn = itn < ie ? chunks(itn) : 0;
     }
+    cp_wait_all();     // this unit's copies have landed (the only group in flight)
+    __syncthreads();   // ... for every thread; and the other buffer is no longer read
     int nnext = 0;
-    if (itn < ie) nnext = fetch(itn, chn);
+    if (itn < ie) nnext = issue(itn, chn, buf ^ 1);
     const char* b = near_smem + buf * S::BYTES;
     const TN* tl = reinterpret_cast<const TN*>(b);
-    const double* xs = reinterpret_cast<const double*>(b + S::TILE * sizeof(TN));
-    if (row < nr) {
+    const double2* xs = reinterpret_cast<const double2*>(b + S::XOFF);
+    if (rp < nr) {
 #pragma unroll 4
       for (int q = 0; q < ncur; ++q) {
-        const double a = static_cast<double>(tl[q * ld + row]);
-        a0 += a * xs[q * R + rq];
-        a1 += a * xs[q * R + rq + 4];
+        double a0, a1;
+        near_pair<TN>(tl + q * ld + rp, a0, a1);
+        const double2 x01 = xs[q * 4 + sq / 2], x23 = xs[q * 4 + sq / 2 + 1];
+        acc[0][0] += a0 * x01.x; acc[0][1] += a0 * x01.y; acc[0][2] += a0 * x23.x; acc[0][3] += a0 * x23.y;
+        acc[1][0] += a1 * x01.x; acc[1][1] += a1 * x01.y; acc[1][2] += a1 * x23.x; acc[1][3] += a1 * x23.y;
       }
     }
-    if (itn < ie) stash(buf ^ 1);
-    __syncthreads();
     buf ^= 1;
     it = itn;
     ch = chn;
-    nch = nchn;
     ncur = nnext;
   }
-  if (row < nr) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int row = rp + h;
+    if (row >= nr) continue;
     const int64_t i = r0 + row;
     const int32_t b = perm[i];
     const double dg = diag[i];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = rq + 4 * h;
-      const double y = dg * xm[i * R + r] + yinit[i * R + r] + (h ? a1 : a0);
+    for (int s = 0; s < 4; ++s) {
+      const int r = sq + s;
+      const double y = dg * xm[i * R + r] + yinit[i * R + r] + acc[h][s];
       const int64_t o = gidx ? static_cast<int64_t>(gidx[goff.v[r] + b]) : goff.v[r] + b;
       const TD yv = static_cast<TD>(y);
       dst[o] = add ? static_cast<TD>(add[o] + yv) : yv;

@@ -62,7 +62,8 @@ struct TcTile {
   int32_t b_rows;  // valid K rows (B is zero past them)
   int32_t slot;    // output partial: rows slot * 128 .. + 127
   int32_t bsc;     // row of the B exponent table (column cluster or row group)
-  int32_t pad;
+  int32_t direct;  // 1: the tile covers its rows' whole K range; the epilogue writes the
+                   // result rows straight to `zout` (rows mapped by zmap), not to partials
 };
 
 struct TcPack {
@@ -82,6 +83,9 @@ struct TcPlan {
   int32_t nt1 = 0, nt2 = 0;
   DevBuf<int64_t> rp1, rp2;            // CSR: z entry / perm row -> partial rows
   DevBuf<int32_t> ix1, ix2;
+  DevBuf<int64_t> zrows1;              // z entries summed from partials (tiles split in K)
+  int64_t nz1 = 0;
+  DevBuf<int32_t> zmap1;               // phase 1: slot row -> z entry (-1: padding) [slots][128]
   DevBuf<int64_t> br1, br2;            // B row ranges per exponent row [n][2]
   int32_t nb1 = 0, nb2 = 0;
   DevBuf<int32_t> eb1, eb2;            // B exponents [n][8]
@@ -237,7 +241,8 @@ __device__ __forceinline__ int i8off(int row, int k, int half) {
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const TcTile* __restrict__ tiles, int ntiles, const char* __restrict__ A,
               const int32_t* __restrict__ ea, const int32_t* __restrict__ eb, const double* __restrict__ bsrc,
-              double* __restrict__ part, int* __restrict__ err) {
+              double* __restrict__ part, double* __restrict__ zout, const int32_t* __restrict__ zmap,
+              int* __restrict__ err) {
   extern __shared__ __align__(1024) char smem[];
   char* sA = smem;                                   // [NSTAGE][NDA][AD_BYTES] A digits (as in HBM)
   char* sB = sA + NSTAGE * AST_BYTES;                // [NSTAGE][BST_BYTES]    B digits, N = 48 rows
@@ -376,8 +381,14 @@ __global__ void __launch_bounds__(THREADS, 1)
       tc_before();
       mbar_arrive(&acce[buf]);
       double* o = part + (static_cast<int64_t>(T.slot) * TM + row) * R;
+      if (T.direct) {  // the only partial of this row: straight to its z entry (padding rows dropped)
+        const int32_t zi = zmap[static_cast<int64_t>(T.slot) * TM + row];
+        o = zi >= 0 ? zout + static_cast<int64_t>(zi) * R : nullptr;
+      }
+      if (o) {
 #pragma unroll
-      for (int n = 0; n < R; ++n) o[n] = ldexp(y[n], er + en[n] - FIXA - FIXB);
+        for (int n = 0; n < R; ++n) o[n] = ldexp(y[n], er + en[n] - FIXA - FIXB);
+      }
     }
   } else if (warp >= 8) {  // B digits: thread -> (state n, two k); rows 8 u + n of the N = 48 tile
     const int ct = tid - (THREADS - CONV_THREADS);
@@ -429,7 +440,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // out[i][n] = sum over p in [rp[i], rp[i+1]) of part[ix[p]][n]  (FP64, fixed order)
-__global__ void k_tc_reduce(int64_t nrows, const int64_t* __restrict__ rp, const int32_t* __restrict__ ix,
+__global__ void k_tc_reduce(int64_t nrows, const int64_t* __restrict__ rows, const int64_t* __restrict__ rp,
+                            const int32_t* __restrict__ ix,
                             const double* __restrict__ part, double* __restrict__ out) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int64_t i = t >> 3;
@@ -437,7 +449,7 @@ __global__ void k_tc_reduce(int64_t nrows, const int64_t* __restrict__ rp, const
   if (i >= nrows) return;
   double s = 0.0;
   for (int64_t p = rp[i]; p < rp[i + 1]; ++p) s += part[static_cast<int64_t>(ix[p]) * R + n];
-  out[i * R + n] = s;
+  out[(rows ? rows[i] : i) * R + n] = s;
 }
 
 // exponent e with max |v| < 2^(e - 1) (one bit of headroom for the rounding of the 42-bit
@@ -587,6 +599,7 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   std::vector<TcPack> p1, p2;
   std::vector<int64_t> rowbase, colbase, br1, br2;
   std::vector<std::pair<int64_t, int32_t>> m1, m2;
+  std::vector<int32_t> zmap1;
   int64_t a1 = 0, a2 = 0;
   int32_t slot1 = 0, slot2 = 0;
   // phase 1: column clusters
@@ -616,9 +629,12 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
         for (int64_t k0 = 0; k0 < ksteps; k0 += KSTEP_MAX) {
           const int ns = static_cast<int>(std::min<int64_t>(KSTEP_MAX, ksteps - k0));
           const int kv = static_cast<int>(std::min<int64_t>(KS * ns, K - KS * k0));
-          t1.push_back(TcTile{a1, ns, static_cast<int32_t>(cs + KS * k0), kv, slot1, bsc, 0});
+          const int direct = ksteps <= KSTEP_MAX ? 1 : 0;
+          t1.push_back(TcTile{a1, ns, static_cast<int32_t>(cs + KS * k0), kv, slot1, bsc, direct});
           p1.push_back(TcPack{a1, tab, KS * k0, ns, kv, rv, 1, slot1, 0});
-          for (int r = 0; r < rv; ++r) m1.push_back({rows[m0 + r].second, slot1 * TM + r});
+          for (int r = 0; r < TM; ++r) zmap1.push_back(direct && r < rv ? static_cast<int32_t>(rows[m0 + r].second) : -1);
+          if (!direct)
+            for (int r = 0; r < rv; ++r) m1.push_back({rows[m0 + r].second, slot1 * TM + r});
           a1 += static_cast<int64_t>(ns) * AST_BYTES;
           ++slot1;
         }
@@ -703,7 +719,18 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
     run(p1, P->A1.p, P->ea1.p, slot1);
     run(p2, P->A2.p, P->ea2.p, slot2);
   }
-  Csr c1 = make_csr(zlen, m1), c2 = make_csr(H.Nb, m2);
+  // phase 1: partial sums only for the z entries of tiles split in K (compacted row list)
+  std::sort(m1.begin(), m1.end());
+  std::vector<int64_t> zr1;
+  std::vector<std::pair<int64_t, int32_t>> m1c;
+  for (auto& pr : m1) {
+    if (zr1.empty() || zr1.back() != pr.first) zr1.push_back(pr.first);
+    m1c.push_back({static_cast<int64_t>(zr1.size()) - 1, pr.second});
+  }
+  Csr c1 = make_csr(static_cast<int64_t>(zr1.size()), m1c), c2 = make_csr(H.Nb, m2);
+  P->nz1 = static_cast<int64_t>(zr1.size());
+  P->zrows1.upload(zr1.empty() ? std::vector<int64_t>{0} : zr1, s);
+  P->zmap1.upload(zmap1.empty() ? std::vector<int32_t>{-1} : zmap1, s);
   P->rp1.upload(c1.rp, s);
   P->ix1.upload(c1.ix.empty() ? std::vector<int32_t>{0} : c1.ix, s);
   P->rp2.upload(c2.rp, s);
@@ -717,6 +744,7 @@ void tc_build(HMatrix& H, cudaStream_t s, int kstep_max) {
   P->part1.alloc(std::max<int64_t>(slot1, 1) * TM * R);
   P->part2.alloc(std::max<int64_t>(slot2, 1) * TM * R);
   P->z.alloc(std::max<int64_t>(zlen, 1) * R);
+  P->z.zero(s);  // rank-padding entries stay zero (no tile writes them)
   P->yfar.alloc(H.Nb * R);
   P->err.alloc(1);
   P->err.zero(s);
@@ -733,20 +761,22 @@ const double* tc_far_apply(HMatrix& H, const double* xm, cudaStream_t s) {
   if (P.nt1 > 0) {
     k_tc_bexp<<<P.nb1, 256, 0, s>>>(P.nb1, P.br1.p, xm, P.eb1.p);
     SPX_LAUNCH_CHECK();
-    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t1.p, P.nt1, P.A1.p, P.ea1.p, P.eb1.p, xm, P.part1.p, P.err.p);
+    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t1.p, P.nt1, P.A1.p, P.ea1.p, P.eb1.p, xm, P.part1.p, P.z.p,
+                                               P.zmap1.p, P.err.p);
     SPX_LAUNCH_CHECK();
   }
-  if (P.zlen > 0) {
-    k_tc_reduce<<<grid_for(P.zlen * R, 256), 256, 0, s>>>(P.zlen, P.rp1.p, P.ix1.p, P.part1.p, P.z.p);
+  if (P.nz1 > 0) {
+    k_tc_reduce<<<grid_for(P.nz1 * R, 256), 256, 0, s>>>(P.nz1, P.zrows1.p, P.rp1.p, P.ix1.p, P.part1.p, P.z.p);
     SPX_LAUNCH_CHECK();
   }
   if (P.nt2 > 0) {
     k_tc_bexp<<<P.nb2, 256, 0, s>>>(P.nb2, P.br2.p, P.z.p, P.eb2.p);
     SPX_LAUNCH_CHECK();
-    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t2.p, P.nt2, P.A2.p, P.ea2.p, P.eb2.p, P.z.p, P.part2.p, P.err.p);
+    k_tc_gemm<<<grid, THREADS, SMEM_BYTES, s>>>(P.t2.p, P.nt2, P.A2.p, P.ea2.p, P.eb2.p, P.z.p, P.part2.p, nullptr,
+                                               nullptr, P.err.p);
     SPX_LAUNCH_CHECK();
   }
-  k_tc_reduce<<<grid_for(H.Nb * R, 256), 256, 0, s>>>(H.Nb, P.rp2.p, P.ix2.p, P.part2.p, P.yfar.p);
+  k_tc_reduce<<<grid_for(H.Nb * R, 256), 256, 0, s>>>(H.Nb, nullptr, P.rp2.p, P.ix2.p, P.part2.p, P.yfar.p);
   SPX_LAUNCH_CHECK();
   return P.yfar.p;
 }
@@ -765,7 +795,7 @@ int64_t tc_bytes(const HMatrix& H) {
   return static_cast<int64_t>(P.A1.bytes() + P.A2.bytes() + P.ea1.bytes() + P.ea2.bytes() + P.part1.bytes() +
                               P.part2.bytes() + P.z.bytes() + P.yfar.bytes() + P.rp1.bytes() + P.rp2.bytes() +
                               P.ix1.bytes() + P.ix2.bytes() + P.br1.bytes() + P.br2.bytes() + P.eb1.bytes() +
-                              P.eb2.bytes());
+                              P.eb2.bytes() + P.zrows1.bytes() + P.zmap1.bytes());
 }
 
 }  // namespace spx
