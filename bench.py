@@ -13,6 +13,11 @@ Workload (one "step" = one fixed-dt RK4 step = 4 effective-field/RHS evaluations
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
+At N = 1 the line also carries "batched": the same mesh as 8 films (seeded m0 each)
+integrated together in the mixed + batched form (one H-matrix applied to all films with the
+far field on the tensor cores, the u1 hierarchy shared), its film-steps/s, its ratio to the
+single film of the same run, and film 0's demag error against FP64 (--batched 0 turns it off).
+
 Multi-GPU: the film does not shard (one boundary operator couples every boundary
 node), so N GPUs run N independent replicas ("replicas only"); value = N x steps/s.
 """
@@ -303,12 +308,20 @@ def run_ours(a):
     # accuracy: the final state's demag field against an FP64 evaluation, the H-matrix
     # against the reference's dense rows, and the trajectory against an FP64 trajectory
     mfin = hef.get_state().clone()
-    err = rows_err = drift = hmat_arrays = None
+    err = rows_err = drift = hmat_arrays = hef64 = None
+    want_batch = rank == 0 and ws == 1 and a.batched > 1
     if rank == 0 and a.check_error:
         rows_err = rows_err_vs_reference(spx, X, T, dm.B_hmatrix_gpu)
-        err, drift, hmat_arrays = accuracy_vs_f64(spx, X, T, H0, m0, mfin, hef, a,
-                                                  export=bool(a.cpu_baseline and ws == 1))
+        err, drift, hmat_arrays, hef64 = accuracy_vs_f64(spx, X, T, H0, m0, mfin, hef, a,
+                                                         export=bool(a.cpu_baseline and ws == 1), keep=want_batch)
         hef.set_state(mfin)
+    # the mixed + batched form: films of this mesh integrated together (one GPU)
+    batched = None
+    if want_batch:
+        batched = batched_film_steps(spx, a, X, T, H0, a.batched,
+                                     hef64.demag_field if hef64 is not None else None)
+        del hef64
+        torch.cuda.empty_cache()
     # end-to-end through the host-buffer entry point (pinned), one step per call
     e2e = None
     if not a.no_e2e:
@@ -401,11 +414,68 @@ def run_ours(a):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+    if batched is not None:
+        batched["vs_single_film"] = round(batched["value"] / line["value"], 3)
+        line["batched"] = batched
     if a.cpu_baseline and ws == 1:
         line["cpu_baseline"] = cpu_baseline(a, hmat_arrays if hmat_arrays is not None else film_hmatrix_arrays(a))
         del hmat_arrays
     print(json.dumps(line), flush=True)
     finish(ws)
+
+
+def batched_film_steps(spx, a, X, T, H0, R, ref_demag=None):
+    """The mixed + batched form on one GPU: R films of this mesh (one seeded m0 each, the
+    seeds of `--batch R`) integrated together as one ensemble: ONE H-matrix applied to all
+    films per stage (far field on the tensor cores for batches of 8), the u1 hierarchy shared
+    by the identical diagonal blocks.  Film-steps/s over a.batched_steps RK4 steps, and film
+    0's demag field at the final state against the FP64 field `ref_demag`."""
+    import ctypes as C_
+    import torch
+    from spinfemx_b200 import _lib
+    N = X.shape[0]
+    m0s = [workload(a.nx, a.ny, a.nz, a.h, 2000 + j)[2] for j in range(R)]
+    dk = dict(hmatrix_epsilon=a.hmatrix_epsilon, hmatrix_eta=2.0, hmatrix_leaf_size=a.hmatrix_leaf,
+              ksp_rtol_u1=a.rtol_u1, ksp_rtol_u2=a.rtol_u2, hmatrix_precision=a.hmatrix_precision,
+              hmatrix_recompress=bool(a.hmatrix_recompress),
+              warm_start={0: False, 1: True, 2: "extrapolate", 3: "extrapolate_corrected"}[a.warm_start])
+    t0 = time.time()
+    ens = spx.LLGEnsemble([(X, T)] * R, 8e5, Aex=1.3e-11, alpha=0.02, H0=[H0] * R, dense_max_nb=0,
+                          precision=a.precision, demag_kwargs=dk)
+    dm = ens.hef.demag_field
+    tc_bytes = None
+    if R == 8:
+        hh = C_.c_void_p()
+        _lib.call("spx_demag_ensemble_hmat", dm.handle, 0, C_.byref(hh))
+        nb = C_.c_int64()
+        _lib.call("spx_hmat_tensor_cores", hh, 1, C_.byref(nb))
+        tc_bytes = nb.value
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+    ens.set_state(m0s)
+    ens.step(a.dt, max(a.warmup, 3))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.step(a.dt, a.batched_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    err = None
+    if ref_demag is not None:
+        mall = ens.get_state()
+        Hall = torch.empty_like(mall)
+        dm.compute_vec(mall, Hall)
+        m_0 = mall[: 3 * N].contiguous()
+        Hr = torch.empty_like(m_0)
+        ref_demag.compute_vec(m_0, Hr)
+        err = float(torch.linalg.norm(Hall[: 3 * N] - Hr) / torch.linalg.norm(Hr))
+    del ens
+    torch.cuda.empty_cache()
+    return {"films": R, "value": round(1000.0 * R * a.batched_steps / ms, 4), "unit": "film-steps/s",
+            "ms_per_step": round(ms / a.batched_steps, 4), "steps": a.batched_steps,
+            "tensor_cores": tc_bytes is not None, "tensor_core_plan_bytes": tc_bytes,
+            "demag_rel_err_vs_fp64_film0": err, "setup_s": round(setup_s, 1)}
 
 
 def ku_fourier_map(X, seed, mean=2e5, std=5e4, modes=16):
@@ -842,12 +912,12 @@ def fem_nnz(spx, X, T, dm):
     return nnz, nnzI
 
 
-def accuracy_vs_f64(spx, X, T, H0, m0, mfin, hef, a, export=False):
+def accuracy_vs_f64(spx, X, T, H0, m0, mfin, hef, a, export=False, keep=False):
     """Against an all-FP64 field (FP64 vectors, operators and H-matrix factors, rtol 1e-10):
     (1) the relative L2 error of the working-precision demag field at the final state;
     (2) max |m - m_f64| after a.drift_steps RK4 steps from m0 (both runs from the same
     state, same dt); (3) with `export`, the FP64 H-matrix in the reference's cache schema
-    (for the CPU baseline)."""
+    (for the CPU baseline); (4) with `keep`, the FP64 effective field itself (else None)."""
     import torch
     hef64 = spx.EffectiveField(
         X, T, 8e5, Aex=1.3e-11, alpha=0.02, gamma=2.211e5, H0_static=H0, use_demag=True, precision="f64",
@@ -870,9 +940,11 @@ def accuracy_vs_f64(spx, X, T, H0, m0, mfin, hef, a, export=False):
         d = float((hef.get_state() - hef64.get_state()).abs().max().item())
         drift = {"steps": a.drift_steps, "max_abs_dm": d, "bar": 1e-5}
     arrays = hef64.demag_field.B_hmatrix_gpu.cache_arrays() if export else None
+    if keep:
+        return e, drift, arrays, hef64
     del hef64
     torch.cuda.synchronize()
-    return e, drift, arrays
+    return e, drift, arrays, None
 
 
 def finish(ws):
@@ -1110,6 +1182,9 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="film: films of the same mesh integrated together")
     ap.add_argument("--tensor-cores", type=int, default=0, help="batch: far field of the shared H-matrix on tcgen05")
     ap.add_argument("--compare-single", type=int, default=1, help="batch: also time the film alone")
+    ap.add_argument("--batched", type=int, default=8,
+                    help="film (N=1): also time this many films of the mesh integrated together (0: off)")
+    ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--workload", default="film", choices=["film", "adjoint", "ensemble"],
                     help="film: LLG steps/s on the 0.48M-node film (the headline); adjoint: trajectory gradient "
                          "on the 100x100x2 film")

@@ -513,6 +513,25 @@ __device__ __forceinline__ void store_r(float* __restrict__ v, int64_t c, const 
   }
 }
 
+// R interleaved FP64 entries of row c ([row][R], R even): 16-byte loads and stores
+template <int R>
+__device__ __forceinline__ void load_r64(const double* __restrict__ v, int64_t c, double (&g)[R]) {
+  static_assert(R % 2 == 0, "R even");
+  const double2* p = reinterpret_cast<const double2*>(v + c * R);
+#pragma unroll
+  for (int h = 0; h < R / 2; ++h) {
+    const double2 a = p[h];
+    g[2 * h] = a.x;
+    g[2 * h + 1] = a.y;
+  }
+}
+template <int R>
+__device__ __forceinline__ void store_r64(double* __restrict__ v, int64_t c, const double (&g)[R]) {
+  double2* p = reinterpret_cast<double2*>(v + c * R);
+#pragma unroll
+  for (int h = 0; h < R / 2; ++h) p[h] = make_double2(g[2 * h], g[2 * h + 1]);
+}
+
 template <int R>
 __device__ __forceinline__ void sell_dot_r(const int64_t* __restrict__ sp, const int32_t* __restrict__ col,
                                            const float* __restrict__ val, int64_t sl, int lane,
@@ -1277,17 +1296,23 @@ __global__ void __launch_bounds__(PCG_BLOCK_R, PCG_CTAS_PER_SM) k_pcg_amg_r(PcgP
       PCG_ROWS_BEGIN
         const float di0 = dinv0[row];
         const double sd = P.sdinv[row], dg = P.diag[row];
+        double pv[R], rv[R], qv[R];
+        load_r64<R>(P.p, row, pv);
+        load_r64<R>(P.r, row, rv);
+        load_r64<R>(P.q, row, qv);
+        float bf[R], dbf[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int64_t j = row * R + r;
-          P.y[r * n + row] += alpha * P.p[j];
-          const double rv = P.r[j] - alpha * P.q[j];
-          P.r[j] = rv;
-          const float rf = static_cast<float>(rv / sd);
-          b0[j] = rf;
-          db0[j] = di0 * rf;
-          rh += dg * rv * rv;
+          P.y[r * n + row] += alpha * pv[r];
+          rv[r] -= alpha * qv[r];
+          const float rf = static_cast<float>(rv[r] / sd);
+          bf[r] = rf;
+          dbf[r] = di0 * rf;
+          rh += dg * rv[r] * rv[r];
         }
+        store_r64<R>(P.r, row, rv);
+        store_r<R>(b0, row, bf);
+        store_r<R>(db0, row, dbf);
       PCG_ROWS_END
       cta_partial(P.part, 0, rh, 0.0, 0.0, 0.0, sh);
       if (!grid_barrier(cnt, gen, nb, P.err)) return;

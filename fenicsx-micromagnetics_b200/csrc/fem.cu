@@ -132,17 +132,47 @@ __global__ void k_dense_gemv(int64_t Nb, const double* __restrict__ B, const TV*
   }
 }
 
-// remove each component's mean from a projected solution (x = y sdinv when the FP64 state y
-// is kept; one CTA per component)
+// Component means of ensembles (node offsets `off`), in two passes over chunks of SEG_CH
+// entries so that every component, however large, is spread over many CTAs: k_seg_sum writes
+// the chunk sums part[seg][c]; the apply kernels sum a component's chunk sums in a fixed order
+// (the same mean in every CTA, deterministic) and remove the mean from their chunk.
+constexpr int SEG_CH = 8192;
+
+// chunk sums of x (or of y sdinv when y is given: the FP64 state), or of b when x is null
 template <class TV>
-__global__ void k_seg_center(const int64_t* __restrict__ off, TV* __restrict__ x, double* __restrict__ y,
-                             const double* __restrict__ sdinv) {
+__global__ void k_seg_sum(const int64_t* __restrict__ off, int maxch, const TV* __restrict__ x,
+                          const double* __restrict__ y, const double* __restrict__ sdinv, double* __restrict__ part) {
   __shared__ double sh[32];
-  const int64_t a = off[blockIdx.x], b = off[blockIdx.x + 1];
+  const int seg = blockIdx.y, c = blockIdx.x;
+  const int64_t a = off[seg] + static_cast<int64_t>(c) * SEG_CH, end = off[seg + 1];
+  if (a >= end) return;  // uniform per CTA
+  const int64_t e = min(end, a + SEG_CH);
+  double v = 0.0;
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) v += y ? y[i] * sdinv[i] : static_cast<double>(x[i]);
+  v = block_sum(v, sh);
+  if (threadIdx.x == 0) part[static_cast<int64_t>(seg) * maxch + c] = v;
+}
+
+__device__ __forceinline__ double seg_mean(const int64_t* __restrict__ off, int maxch, const double* __restrict__ part,
+                                           int seg) {
+  const int64_t len = off[seg + 1] - off[seg];
+  const int nch = static_cast<int>((len + SEG_CH - 1) / SEG_CH);
   double s = 0.0;
-  for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) s += y ? y[i] * sdinv[i] : static_cast<double>(x[i]);
-  const double mean = block_sum(s, sh) / static_cast<double>(b - a);
-  for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) {
+  for (int c = 0; c < nch; ++c) s += part[static_cast<int64_t>(seg) * maxch + c];
+  return s / static_cast<double>(len);
+}
+
+// remove each component's mean from a projected solution (x = y sdinv when the FP64 state y
+// is kept)
+template <class TV>
+__global__ void k_seg_center(const int64_t* __restrict__ off, int maxch, const double* __restrict__ part,
+                             TV* __restrict__ x, double* __restrict__ y, const double* __restrict__ sdinv) {
+  const int seg = blockIdx.y;
+  const int64_t a = off[seg] + static_cast<int64_t>(blockIdx.x) * SEG_CH, end = off[seg + 1];
+  if (a >= end) return;
+  const int64_t e = min(end, a + SEG_CH);
+  const double mean = seg_mean(off, maxch, part, seg);
+  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) {
     if (y) {
       const double xv = y[i] * sdinv[i] - mean;
       x[i] = static_cast<TV>(xv);
@@ -153,26 +183,27 @@ __global__ void k_seg_center(const int64_t* __restrict__ off, TV* __restrict__ x
   }
 }
 
-// bh = (b minus its mean over each component) * sdinv, in FP64 (one CTA per component)
+// bh = (b minus its mean over each component) * sdinv, in FP64
 template <class TV>
-__global__ void k_seg_center_bh(const int64_t* __restrict__ off, const TV* __restrict__ b,
-                                const double* __restrict__ sdinv, double* __restrict__ bh) {
-  __shared__ double sh[32];
-  const int64_t a = off[blockIdx.x], e = off[blockIdx.x + 1];
-  double s = 0.0;
-  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) s += static_cast<double>(b[i]);
-  const double mean = block_sum(s, sh) / static_cast<double>(e - a);
+__global__ void k_seg_center_bh(const int64_t* __restrict__ off, int maxch, const double* __restrict__ part,
+                                const TV* __restrict__ b, const double* __restrict__ sdinv, double* __restrict__ bh) {
+  const int seg = blockIdx.y;
+  const int64_t a = off[seg] + static_cast<int64_t>(blockIdx.x) * SEG_CH, end = off[seg + 1];
+  if (a >= end) return;
+  const int64_t e = min(end, a + SEG_CH);
+  const double mean = seg_mean(off, maxch, part, seg);
   for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) bh[i] = (static_cast<double>(b[i]) - mean) * sdinv[i];
 }
 
-// out = b minus its mean over each component (one CTA per component)
+// out = b minus its mean over each component
 template <class TV>
-__global__ void k_seg_center_b(const int64_t* __restrict__ off, const TV* __restrict__ b, TV* __restrict__ out) {
-  __shared__ double sh[32];
-  const int64_t a = off[blockIdx.x], e = off[blockIdx.x + 1];
-  double s = 0.0;
-  for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) s += static_cast<double>(b[i]);
-  const double mean = block_sum(s, sh) / static_cast<double>(e - a);
+__global__ void k_seg_center_b(const int64_t* __restrict__ off, int maxch, const double* __restrict__ part,
+                               const TV* __restrict__ b, TV* __restrict__ out) {
+  const int seg = blockIdx.y;
+  const int64_t a = off[seg] + static_cast<int64_t>(blockIdx.x) * SEG_CH, end = off[seg + 1];
+  if (a >= end) return;
+  const int64_t e = min(end, a + SEG_CH);
+  const double mean = seg_mean(off, maxch, part, seg);
   for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) out[i] = static_cast<TV>(static_cast<double>(b[i]) - mean);
 }
 
@@ -696,13 +727,18 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   // ensembles: every component's right-hand side projected on its own (FP64 for the solvers
   // that keep an FP64 state, so that no FP32 rounding leaves a component inconsistent)
   const bool seg = project && seg_off.n > 1;
+  const dim3 sgrid(static_cast<unsigned>(std::max(seg_maxch, 1)), static_cast<unsigned>(seg_off.n > 1 ? seg_off.n - 1 : 1));
+  if (seg) {
+    k_seg_sum<TV><<<sgrid, 256, 0, st>>>(seg_off.p, seg_maxch, b, nullptr, nullptr, seg_part.p);
+    SPX_LAUNCH_CHECK();
+  }
   if (seg && ir) {
-    k_seg_center_bh<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, b, sdinv64.p, bh64.p);
+    k_seg_center_bh<TV><<<sgrid, 256, 0, st>>>(seg_off.p, seg_maxch, seg_part.p, b, sdinv64.p, bh64.p);
     SPX_LAUNCH_CHECK();
   } else if (seg) {
     if (bseg.n < n * sizeof(TV)) bseg.alloc(n * sizeof(TV));
     TV* bc = reinterpret_cast<TV*>(bseg.p);
-    k_seg_center_b<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, b, bc);
+    k_seg_center_b<TV><<<sgrid, 256, 0, st>>>(seg_off.p, seg_maxch, seg_part.p, b, bc);
     SPX_LAUNCH_CHECK();
     b = bc;
   }
@@ -740,8 +776,9 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     SPX_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(k_cg), dim3(grid), dim3(block), args, 0, st));
   }
   if (project && seg_off.n > 1) {
-    k_seg_center<TV><<<static_cast<unsigned>(seg_off.n - 1), 256, 0, st>>>(seg_off.p, x, ir ? y64.p : nullptr,
-                                                                           sdinv64.p);
+    k_seg_sum<TV><<<sgrid, 256, 0, st>>>(seg_off.p, seg_maxch, x, ir ? y64.p : nullptr, sdinv64.p, seg_part.p);
+    SPX_LAUNCH_CHECK();
+    k_seg_center<TV><<<sgrid, 256, 0, st>>>(seg_off.p, seg_maxch, seg_part.p, x, ir ? y64.p : nullptr, sdinv64.p);
     SPX_LAUNCH_CHECK();
   }
   if (slot == 0 && stage_correct && have_pred0) {  // stage 1's prediction error
@@ -773,6 +810,16 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     out.converged = (h_res <= rtol || h_it < maxit) ? 1 : 0;
   }
   return out;
+}
+
+template <class TM>
+void CgSystem<TM>::set_segments(const std::vector<int64_t>& offsets, cudaStream_t s) {
+  seg_off.upload(offsets, s);
+  int64_t mx = 0;
+  for (size_t k = 0; k + 1 < offsets.size(); ++k) mx = std::max<int64_t>(mx, offsets[k + 1] - offsets[k]);
+  seg_maxch = static_cast<int>((mx + SEG_CH - 1) / SEG_CH);
+  const int64_t nseg = offsets.size() > 1 ? static_cast<int64_t>(offsets.size()) - 1 : 1;
+  seg_part.alloc(static_cast<size_t>(nseg * std::max(seg_maxch, 1)));
 }
 
 template struct CgSystem<double>;
@@ -886,7 +933,7 @@ void DemagCtx<TV, TM>::create(const double* X, int64_t N_, const int32_t* tets, 
     bd.dense_B(Bdense.p, s);
   } else if (opt.backend == 2) {
     block_boundary_build<TM>(blk, bd, X, N, tets, E, opt, s);
-    cg1.seg_off.upload(opt.sample_offsets, s);
+    cg1.set_segments(opt.sample_offsets, s);
   } else {
     if (opt.preset) {
       SPX_CHECK(opt.preset->Nb == Nb && opt.preset->packed, "the given H-matrix does not belong to this boundary");

@@ -110,6 +110,9 @@ struct CgSystem {
   // the components; a projected solve removes every component's mean from the right-hand
   // side (each component's system must be consistent on its own) and from the solution
   DevBuf<int64_t> seg_off;
+  int seg_maxch = 0;          // chunks of the largest component (component-mean kernels)
+  DevBuf<double> seg_part;    // chunk sums [components][seg_maxch]
+  void set_segments(const std::vector<int64_t>& offsets, cudaStream_t s);
   DevBuf<char> bseg;  // right-hand side with every component's mean removed (TV)
   DevBuf<double> pred0, delta;
   double inner_rtol = 1e-3;
