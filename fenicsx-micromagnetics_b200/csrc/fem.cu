@@ -207,7 +207,7 @@ __global__ void k_seg_center_b(const int64_t* __restrict__ off, int maxch, const
   for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) out[i] = static_cast<TV>(static_cast<double>(b[i]) - mean);
 }
 
-// starting guess: quadratic / linear / constant extrapolation of stored solutions
+// starting guess: cubic / quadratic / linear / constant extrapolation of stored solutions
 __global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                            double* __restrict__ out, int mode) {  // mode 0: out = a - b; 1: out += a
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -217,11 +217,13 @@ __global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double
 
 template <class T>
 __global__ void k_extrap(int64_t n, const double* __restrict__ h0, const double* __restrict__ h1,
-                         const double* __restrict__ h2, int cnt, T* __restrict__ out) {
+                         const double* __restrict__ h2, const double* __restrict__ h3, int cnt,
+                         T* __restrict__ out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double v;
-  if (cnt >= 3) v = 3.0 * h0[i] - 3.0 * h1[i] + h2[i];
+  if (cnt >= 4) v = 4.0 * h0[i] - 6.0 * h1[i] + 4.0 * h2[i] - h3[i];
+  else if (cnt == 3) v = 3.0 * h0[i] - 3.0 * h1[i] + h2[i];
   else if (cnt == 2) v = 2.0 * h0[i] - h1[i];
   else v = h0[i];
   out[i] = static_cast<T>(v);
@@ -701,13 +703,15 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
   SPX_CHECK(ir || sizeof(TV) == sizeof(double), "FP64 CG needs FP64 vectors");
   if (slot >= 0) {
     SPX_CHECK(slot < CG_SLOTS, "extrapolation slot out of range");
-    for (int k = 0; k < 3; ++k)
+    for (int k = 0; k < CG_HIST; ++k)
       if (!hist[slot][k].n) hist[slot][k].alloc(n);
     if (hcount[slot] > 0) {
-      const int h0 = (hhead[slot] + 2) % 3, h1 = (hhead[slot] + 1) % 3, h2 = hhead[slot];
+      const int hh = hhead[slot];  // newest entry: hh - 1
+      const int h0 = (hh + CG_HIST - 1) % CG_HIST, h1 = (hh + CG_HIST - 2) % CG_HIST,
+                h2 = (hh + CG_HIST - 3) % CG_HIST, h3 = (hh + CG_HIST - 4) % CG_HIST;
       double* target = ir ? y64.p : reinterpret_cast<double*>(x);
       k_extrap<double><<<grid_for(n, 256), 256, 0, st>>>(n, hist[slot][h0].p, hist[slot][h1].p, hist[slot][h2].p,
-                                                         hcount[slot], target);
+                                                         hist[slot][h3].p, hcount[slot], target);
       SPX_LAUNCH_CHECK();
       warm = true;
       if (stage_correct) {
@@ -793,8 +797,8 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     double* dst = hist[slot][hhead[slot]].p;
     const double* src = ir ? y64.p : reinterpret_cast<const double*>(x);
     SPX_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    hhead[slot] = (hhead[slot] + 1) % 3;
-    hcount[slot] = std::min(3, hcount[slot] + 1);
+    hhead[slot] = (hhead[slot] + 1) % CG_HIST;
+    hcount[slot] = std::min(CG_HIST, hcount[slot] + 1);
   }
   CgStats out;
   if (sync_stats) {

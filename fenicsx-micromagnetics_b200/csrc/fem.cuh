@@ -72,12 +72,14 @@ struct Profiler {
 // FP32 single-reduction CG inside FP64 iterative refinement (FP64 values kept for the
 // true residual, FP64 solution state kept between calls).
 //
-// Starting guesses: with `slot` >= 0 the solver keeps the last three solutions returned
-// for that slot (e.g. one slot per RK stage) and starts from their quadratic
-// extrapolation 3 x1 - 3 x2 + x3 (linear / constant while fewer are stored).  The stopping
+// Starting guesses: with `slot` >= 0 the solver keeps the last four solutions returned
+// for that slot (e.g. one slot per RK stage) and starts from their cubic extrapolation
+// 4 x1 - 6 x2 + 4 x3 - x4 (quadratic / linear / constant while fewer are stored; measured
+// on the 400x400x2 film: 6.4 u1 iterations per solve against 7.3 with the quadratic one).  The stopping
 // rule does not change; only the iteration count does.  Slots 0-3: forward RK stages,
 // 4-7: adjoint stages, 8-11: tangent stages (CG_SLOTS).
 constexpr int CG_SLOTS = 12;
+constexpr int CG_HIST = 4;  // stored solutions per slot (cubic extrapolation)
 
 template <class TM>
 struct CgSystem {
@@ -98,7 +100,7 @@ struct CgSystem {
   DevBuf<double> resid;
   DevBuf<unsigned long long> iters_acc;  // [0] inner iterations, [1] refinement steps, [2] solves
   DevBuf<double> res_acc;                // [0] sum of initial, [1] sum of final relative residuals
-  DevBuf<double> hist[CG_SLOTS][3];
+  DevBuf<double> hist[CG_SLOTS][CG_HIST];
   int hcount[CG_SLOTS] = {}, hhead[CG_SLOTS] = {};
   // stage correction: slots 1..3 add slot 0's last prediction error (solution - guess)
   bool stage_correct = false, have_pred0 = false, have_delta = false;

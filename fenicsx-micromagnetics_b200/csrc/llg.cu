@@ -659,7 +659,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
     const int64_t ep = use_demag ? demag->epoch : 0;
     if (graph_ok && (dt != gdt || ep != gepoch)) graph_reset();
     if (!graph_ok) {
-      if (gwarm < 3) {  // fill the extrapolation rings (and every lazily allocated buffer) first
+      if (gwarm < CG_HIST) {  // fill the extrapolation rings (and every lazily allocated buffer) first
         step_once(dt, s);
         ++gwarm;
         continue;
@@ -667,7 +667,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
       if (!gstream) SPX_CUDA(cudaStreamCreateWithFlags(&gstream, cudaStreamNonBlocking));
       const int64_t st0 = steps, re0 = rhs_evals, la0 = launches;
       try {
-        for (int p = 0; p < 3; ++p) {
+        for (int p = 0; p < CG_HIST; ++p) {
           cudaGraph_t g = nullptr;
           SPX_CUDA(cudaStreamBeginCapture(gstream, cudaStreamCaptureModeThreadLocal));
           try {
@@ -692,7 +692,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
         step_once(dt, s);
         continue;
       }
-      // the three captures advanced the rings by three steps: back to the same phase
+      // the CG_HIST captures advanced the rings by one period: back to the same phase
       launches = la0;
       steps = st0;
       rhs_evals = re0;
@@ -702,7 +702,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
       gepoch = use_demag ? demag->epoch : 0;
     }
     SPX_CUDA(cudaGraphLaunch(gexec[gphase], s));
-    gphase = (gphase + 1) % 3;
+    gphase = (gphase + 1) % CG_HIST;
     ++graph_replays;
     ++steps;
     rhs_evals += 4;

@@ -126,12 +126,12 @@ struct LLGCtx {
   DevBuf<double> red;
   int64_t steps = 0, rhs_evals = 0;
   mutable int64_t launches = 0;
-  // CUDA graphs of one RK4 step (set_graph): three captures, one per phase of the Krylov
-  // extrapolation ring (each step advances every slot's ring by one, period 3), replayed in
-  // turn; dropped when dt, a field parameter or the solver state outside the graphs changes
+  // CUDA graphs of one RK4 step (set_graph): CG_HIST captures, one per phase of the Krylov
+  // extrapolation ring (each step advances every slot's ring by one, period CG_HIST), replayed
+  // in turn; dropped when dt, a field parameter or the solver state outside the graphs changes
   bool graph_on = false, graph_ok = false;
   cudaStream_t gstream = nullptr;
-  cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t gexec[CG_HIST] = {};
   int gphase = 0, gwarm = 0;
   double gdt = 0.0;
   int64_t gepoch = -1, graph_replays = 0;
