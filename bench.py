@@ -329,7 +329,11 @@ def run_ours(a):
         hout = torch.empty(3 * N, dtype=torch.float64).pin_memory()
         hin.copy_(mfin.cpu())
         ke = max(1, min(a.steps, a.e2e_steps))
-        hef.run_host(hin, a.dt, 1, out=hout)  # warm
+        # warm: the accuracy check above ran other trajectories through the same solvers, and
+        # each RK stage's Krylov start extrapolates from its last four solutions
+        for _ in range(max(a.warmup, 5)):
+            hef.run_host(hin, a.dt, 1, out=hout)
+            hin, hout = hout, hin
         barrier(ws)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
@@ -453,7 +457,7 @@ def batched_film_steps(spx, a, X, T, H0, R, ref_demag=None):
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     ens.set_state(m0s)
-    ens.step(a.dt, max(a.warmup, 3))
+    ens.step(a.dt, max(a.warmup, 5))  # the Krylov starts extrapolate from four solutions per stage
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -1150,7 +1154,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["f32", "f64", "mixed"])
     ap.add_argument("--hmatrix-precision", default=None, choices=["f64", "f32", "bf16", "f32_f16"])
