@@ -102,6 +102,14 @@ struct CgSystem {
   DevBuf<double> res_acc;                // [0] sum of initial, [1] sum of final relative residuals
   DevBuf<double> hist[CG_SLOTS][CG_HIST];
   int hcount[CG_SLOTS] = {}, hhead[CG_SLOTS] = {};
+  // the ring bookkeeping of `count` slots from `first` as a solve on each leaves it (a replayed
+  // CUDA graph runs the solves' kernels without this host code)
+  void advance_slots(int first, int count) {
+    for (int s = first; s < first + count && s < CG_SLOTS; ++s) {
+      hhead[s] = (hhead[s] + 1) % CG_HIST;
+      hcount[s] = hcount[s] + 1 < CG_HIST ? hcount[s] + 1 : CG_HIST;
+    }
+  }
   // stage correction: slots 1..3 add slot 0's last prediction error (solution - guess)
   bool stage_correct = false, have_pred0 = false, have_delta = false;
   // kind of the last solve (0 forward, 1 adjoint, 2 tangent): a warm start from the solver
@@ -243,6 +251,14 @@ struct DemagCtx {
               cudaStream_t s);
   // potential phi = u1 + u2 for magnetisation m (AoS, TV); slot: RK stage for extrapolated starts
   void potential(const TV* m, cudaStream_t s, bool sync_stats, int slot = -1);
+  // host bookkeeping of one RK4 step's four stage solves (slots 0-3) for a step replayed
+  // from a CUDA graph, so that later captures and ordinary steps see the rings as they are
+  void replay_step_advance() {
+    if (opt.warm_start >= 2) {
+      cg1.advance_slots(0, 4);
+      cg2.advance_slots(0, 4);
+    }
+  }
   // H_demag = G phi / vol (AoS)
   void field(TV* H, cudaStream_t s);
   // out (+)= D^T w for the linear map D: m -> H_demag (AoS, 3N); slot: adjoint RK stage (4-7)

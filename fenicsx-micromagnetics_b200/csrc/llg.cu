@@ -703,6 +703,7 @@ void LLGCtx<TV, TM>::step_rk4(double dt, int64_t nsteps, cudaStream_t s) {
     }
     SPX_CUDA(cudaGraphLaunch(gexec[gphase], s));
     gphase = (gphase + 1) % CG_HIST;
+    if (use_demag) demag->replay_step_advance();
     ++graph_replays;
     ++steps;
     rhs_evals += 4;
