@@ -201,11 +201,13 @@ SPX_API int spx_hmat_apply_noalloc(spx_hmat h, const double* x, double* y, spx_s
 SPX_API int spx_hmat_apply_multi(spx_hmat h, const double* X, double* Y, int32_t nrhs, spx_stream_t s);
 /* Tensor cores for spx_hmat_apply_multi (no counterpart in the reference): with enable != 0,
  * batches of 8 states run their far field as two block-sparse GEMMs on tcgen05 (column
- * clusters: Z = V X; row clusters: Y += U Z; kind::tf32 with a three-term hi/lo split, FP32
- * accumulation per tile of at most 2048 K elements, FP64 sums of the tiles), the near field
- * and diagonal on the CUDA cores.  Builds the packed factors (about the FP32 factor bytes
- * again; *plan_bytes = device bytes of the plan); enable = 0 drops them.  Needs the H-matrix's
- * FP64 factors (built or imported, not merged).  spx_hmat_tc_status returns (and clears) the
+ * clusters: Z = V X; row clusters: Y += U Z) with exact integer products: the FP32 factors as
+ * 31-bit fixed-point values per tile row and the FP64 states as 47-bit fixed-point values,
+ * cut into base-256 int8 digits (kind::i8, exact int32 digit-pair sums per tile of at most
+ * 2048 K elements, FP64 combination and FP64 sums of the tiles); the near field and diagonal
+ * on the CUDA cores.  Builds the digit plan (about the FP32 factor bytes plus tile padding;
+ * *plan_bytes = device bytes of the plan); enable = 0 drops it.  Needs the H-matrix's FP64
+ * factors (built or imported, not merged).  spx_hmat_tc_status returns (and clears) the
  * timeout flag of its kernels (SPX_ERR_TIMEOUT if a bounded wait ran out, else SPX_OK). */
 /* enable = 2 autotunes: one 8-state apply is timed on the CUDA-core kernels and on tensor-core
  * tiles of 512 and of 2048 K elements, and the fastest is kept (*plan_bytes = 0 when the
