@@ -330,7 +330,7 @@ def run_ours(a):
         hin.copy_(mfin.cpu())
         ke = max(1, min(a.steps, a.e2e_steps))
         # warm: the accuracy check above ran other trajectories through the same solvers, and
-        # each RK stage's Krylov start extrapolates from its last four solutions
+        # each RK stage's Krylov start extrapolates from its last five solutions
         for _ in range(max(a.warmup, 5)):
             hef.run_host(hin, a.dt, 1, out=hout)
             hin, hout = hout, hin
@@ -457,7 +457,7 @@ def batched_film_steps(spx, a, X, T, H0, R, ref_demag=None):
     torch.cuda.synchronize()
     setup_s = time.time() - t0
     ens.set_state(m0s)
-    ens.step(a.dt, max(a.warmup, 5))  # the Krylov starts extrapolate from four solutions per stage
+    ens.step(a.dt, max(a.warmup, 5))  # the Krylov starts extrapolate from five solutions per stage
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

@@ -207,7 +207,7 @@ __global__ void k_seg_center_b(const int64_t* __restrict__ off, int maxch, const
   for (int64_t i = a + threadIdx.x; i < e; i += blockDim.x) out[i] = static_cast<TV>(static_cast<double>(b[i]) - mean);
 }
 
-// starting guess: cubic / quadratic / linear / constant extrapolation of stored solutions
+// starting guess: polynomial extrapolation of the stored solutions (order cnt - 1)
 __global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                            double* __restrict__ out, int mode) {  // mode 0: out = a - b; 1: out += a
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -215,17 +215,22 @@ __global__ void k_axpy_sub(int64_t n, const double* __restrict__ a, const double
   out[i] = mode == 0 ? a[i] - b[i] : out[i] + a[i];
 }
 
+// the stored solutions of a slot, newest first, and the extrapolation weights
+// (-1)^k C(cnt, k + 1): the polynomial through the last cnt solutions at the next step
+struct ExtrapArgs {
+  const double* h[CG_HIST];
+  double w[CG_HIST];
+  int cnt;
+};
+
 template <class T>
-__global__ void k_extrap(int64_t n, const double* __restrict__ h0, const double* __restrict__ h1,
-                         const double* __restrict__ h2, const double* __restrict__ h3, int cnt,
-                         T* __restrict__ out) {
+__global__ void k_extrap(int64_t n, ExtrapArgs a, T* __restrict__ out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double v;
-  if (cnt >= 4) v = 4.0 * h0[i] - 6.0 * h1[i] + 4.0 * h2[i] - h3[i];
-  else if (cnt == 3) v = 3.0 * h0[i] - 3.0 * h1[i] + h2[i];
-  else if (cnt == 2) v = 2.0 * h0[i] - h1[i];
-  else v = h0[i];
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < CG_HIST; ++k)
+    if (k < a.cnt) v += a.w[k] * a.h[k][i];
   out[i] = static_cast<T>(v);
 }
 
@@ -706,12 +711,16 @@ CgStats CgSystem<TM>::solve(const TV* b, TV* x, double rtol, double atol, int ma
     for (int k = 0; k < CG_HIST; ++k)
       if (!hist[slot][k].n) hist[slot][k].alloc(n);
     if (hcount[slot] > 0) {
-      const int hh = hhead[slot];  // newest entry: hh - 1
-      const int h0 = (hh + CG_HIST - 1) % CG_HIST, h1 = (hh + CG_HIST - 2) % CG_HIST,
-                h2 = (hh + CG_HIST - 3) % CG_HIST, h3 = (hh + CG_HIST - 4) % CG_HIST;
+      ExtrapArgs ea{};
+      ea.cnt = hcount[slot];
+      double binom = 1.0;  // C(cnt, k + 1), built up term by term
+      for (int k = 0; k < CG_HIST; ++k) {
+        ea.h[k] = hist[slot][(hhead[slot] + 2 * CG_HIST - 1 - k) % CG_HIST].p;  // newest first
+        binom = binom * (ea.cnt - k) / (k + 1);
+        ea.w[k] = k < ea.cnt ? ((k % 2) ? -binom : binom) : 0.0;
+      }
       double* target = ir ? y64.p : reinterpret_cast<double*>(x);
-      k_extrap<double><<<grid_for(n, 256), 256, 0, st>>>(n, hist[slot][h0].p, hist[slot][h1].p, hist[slot][h2].p,
-                                                         hist[slot][h3].p, hcount[slot], target);
+      k_extrap<double><<<grid_for(n, 256), 256, 0, st>>>(n, ea, target);
       SPX_LAUNCH_CHECK();
       warm = true;
       if (stage_correct) {

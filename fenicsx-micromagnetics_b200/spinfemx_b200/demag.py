@@ -36,7 +36,7 @@ class DemagFieldLindholmGPU:
         hmatrix_precision  factor storage 'f64' | 'f32' | 'bf16' (default: 'f64' for
                            precision='f64', 'f32' otherwise)
         warm_start         False: zero start (the reference); True: previous solution;
-                           'extrapolate': per-RK-stage cubic extrapolation (time loop);
+                           'extrapolate': per-RK-stage quartic extrapolation (time loop);
                            'extrapolate_corrected': the same, stages 2-4 shifted by stage 1's
                            prediction error
         u1_preconditioner  'amg' (smoothed aggregation, as the reference's PC "gamg") or

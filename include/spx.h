@@ -455,8 +455,8 @@ SPX_API int spx_llg_min_eval(spx_llg l, double* m, double* d, int32_t normalize,
 SPX_API int spx_llg_min_trial(spx_llg l, const double* m_old, const double* d_old, double alpha, double* m_trial,
                               double* d_trial, double* out5, spx_stream_t s);
 /* CUDA graphs for spx_llg_step (no counterpart in the reference): with enable != 0, each RK4
- * step is replayed from captured graphs (four captures, one per phase of the per-stage Krylov
- * extrapolation history) after four ordinary steps; the graphs are recaptured when dt, the
+ * step is replayed from captured graphs (five captures, one per phase of the per-stage Krylov
+ * extrapolation history) after five ordinary steps; the graphs are recaptured when dt, the
  * applied field, the Ku map or the solver tolerances change or when any other call used the
  * demag solvers.  Results are those of ordinary steps.  spx_llg_graph_stats reports the steps
  * replayed from graphs and whether graphs are active; if capture failed, stepping continues

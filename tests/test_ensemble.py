@@ -129,15 +129,15 @@ def test_graph_replayed_steps_equal_ordinary_steps(spx, precision):
                               precision=precision, demag_kwargs=dk)
         ens.hef.set_graph(graph)
         ens.set_state([_m0(Xs.shape[0], 30 + k) for k, (Xs, _) in enumerate(ms)])
-        ens.step(2e-14, 13)  # 9 replays: not a multiple of the ring period before the recapture
+        ens.step(2e-14, 13)  # 8 replays: not a multiple of the ring period before the recapture
         a = ens.get_state().cpu().numpy()
         ens.hef.set_uniform_field(0.0, 1e5, 0.0)
         ens.step(2e-14, 7)
         runs.append((a, ens.get_state().cpu().numpy(), ens.hef.graph_stats()))
     assert np.array_equal(runs[0][0], runs[1][0])
     assert np.array_equal(runs[0][1], runs[1][1])
-    # four ordinary steps fill the four-deep extrapolation rings, then every step is replayed
-    assert runs[1][2]["replayed_steps"] == 9 + 7 and runs[1][2]["active"]
+    # five ordinary steps fill the five-deep extrapolation rings, then every step is replayed
+    assert runs[1][2]["replayed_steps"] == 8 + 7 and runs[1][2]["active"]
     assert runs[0][2]["replayed_steps"] == 0
 
 
