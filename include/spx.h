@@ -206,8 +206,10 @@ SPX_API int spx_hmat_apply_multi(spx_hmat h, const double* X, double* Y, int32_t
  * cut into base-256 int8 digits (kind::i8, exact int32 digit-pair sums per tile of at most
  * 2048 K elements, FP64 combination and FP64 sums of the tiles); the near field and diagonal
  * on the CUDA cores.  Builds the digit plan (about the FP32 factor bytes plus tile padding;
- * *plan_bytes = device bytes of the plan); enable = 0 drops it.  Needs the H-matrix's FP64
- * factors (built or imported, not merged).  spx_hmat_tc_status returns (and clears) the
+ * *plan_bytes = device bytes of the plan); enable = 0 drops it.  The plan holds the factors
+ * rounded to FP32 whatever the packing (with an FP64 packing the tensor-core far field is
+ * that of the FP32 packing).  Needs the H-matrix's FP64 factors (built or imported, not
+ * merged); spx_hmat_recompress drops the plan.  spx_hmat_tc_status returns (and clears) the
  * timeout flag of its kernels (SPX_ERR_TIMEOUT if a bounded wait ran out, else SPX_OK). */
 /* enable = 2 autotunes: one 8-state apply is timed on the CUDA-core kernels and on tensor-core
  * tiles of 512 and of 2048 K elements, and the fastest is kept (*plan_bytes = 0 when the
