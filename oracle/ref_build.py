@@ -10,9 +10,9 @@ lie, pulls each kernel's parameter lists and body out of the Python AST, wraps
 each body in a C loop over arrays and compiles the result with gcc into
 ``oracle/_ref/libref_elementwise.so``.  Nothing from the reference is copied
 into the repository: the generated C file and the library live only under
-``oracle/_ref/`` (git-ignored).  The library is used to make golden fixtures
-and by the CPU tests that compare the oracle with the reference's kernels; on a
-machine without the reference checkout it is absent and those tests skip.
+``oracle/_ref/`` (git-ignored).  The library is used to make the golden fixtures
+under ``tests/golden/`` (``make_golden.py``); the tests read those fixtures, so they
+run where the reference checkout is absent.
 
 The reference's CPU Jv kernel (``cpu/solvers/llg_module.py:25-74``) is a numba
 function inside a module that needs DOLFINx to import; ``load_cpu_jv`` pulls
