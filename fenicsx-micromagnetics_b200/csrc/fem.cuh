@@ -12,6 +12,8 @@
 
 #include <memory>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "amg.cuh"
 #include "hmat.cuh"
 
@@ -24,8 +26,14 @@ struct CgStats {
 };
 
 // Per-category CUDA-event timing of the demag/LLG pipeline (enabled on demand; events
-// are recorded on the launching stream around each kernel group).
+// are recorded on the launching stream around each kernel group).  Every group is also an
+// NVTX range of the same name (seen by Nsight Systems / Compute; a no-op without a tool).
 enum ProfCat : int { PC_DIV = 0, PC_CG1 = 1, PC_BND = 2, PC_U2RHS = 3, PC_CG2 = 4, PC_PHI = 5, PC_STAGE = 6, PC_N = 8 };
+inline const char* prof_cat_name(int c) {
+  static const char* const names[PC_N] = {"div", "u1_solve", "boundary_apply", "u2_rhs", "u2_solve", "phi", "stage",
+                                          "other"};
+  return c >= 0 && c < PC_N ? names[c] : "other";
+}
 struct Profiler {
   bool on = false;
   std::vector<cudaEvent_t> pool;
@@ -33,7 +41,13 @@ struct Profiler {
   size_t used = 0;
   int64_t launches[PC_N] = {};
   int64_t groups[PC_N] = {};
+  bool nvtx_open[PC_N] = {};
   void mark(int c, cudaStream_t s) {  // call before and after a group: pairs (start, stop)
+    if (c >= 0 && c < PC_N) {  // groups do not nest: a push on the start mark, a pop on the stop
+      if (nvtx_open[c]) nvtxRangePop();
+      else nvtxRangePushA(prof_cat_name(c));
+      nvtx_open[c] = !nvtx_open[c];
+    }
     if (!on) return;
     if ((used & 1) == 0) groups[c]++;
     if (used == pool.size()) {
